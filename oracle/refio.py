@@ -1,0 +1,157 @@
+"""Test infrastructure (oracle): run the reference's own TreePM through
+oracle/_ref/treepm_ref (built by oracle/Makefile.ref from the reference's
+sources) and read its results back as numpy arrays.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline arm use this
+module; the product never does.
+"""
+from __future__ import annotations
+
+import os
+import struct
+import subprocess
+import tempfile
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_BINARY = os.path.join(HERE, "_ref", "treepm_ref")
+
+
+@dataclass
+class RefProblem:
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    m: np.ndarray
+    box: tuple = (1.0, 1.0, 1.0)
+    mesh: tuple = (16, 16, 16)
+    asmth: float = 1.25
+    rcut: float = 6.25
+    theta: float = 0.5
+    g: float = 1.0
+    eps: float = 0.0
+    scale_factor: float = 1.0
+    leaf: int = 16
+    scheme: int = 0          # 0 CIC, 1 TSC
+    deconv: int = 0
+    criterion: int = 1       # 0 geometric, 1 com_distance, 2 relative
+    order: int = 2           # 0 monopole, 2 quadrupole
+    active: np.ndarray | None = None
+    dump_tree: int = 1
+    dump_density: int = 0
+    kdk: int = 0
+    repeats: int = 0
+    ewald: int = 0
+    drift: float = 0.0
+    kick1: float = 0.0
+    kick2: float = 0.0
+    drag1: float = 1.0
+    drag2: float = 1.0
+    vx: np.ndarray | None = None
+    vy: np.ndarray | None = None
+    vz: np.ndarray | None = None
+
+
+def write_problem(path: str, p: RefProblem) -> None:
+    n = len(p.x)
+    zeros = np.zeros(n)
+    active = np.asarray(p.active if p.active is not None else [], dtype=np.uint32)
+    with open(path, "wb") as f:
+        f.write(b"CHUIIN01")
+        f.write(struct.pack("<q", n))
+        f.write(struct.pack("<3d", *p.box))
+        f.write(struct.pack("<3q", *p.mesh))
+        f.write(struct.pack("<6d", p.asmth, p.rcut, p.theta, p.g, p.eps, p.scale_factor))
+        f.write(struct.pack("<11q", p.leaf, p.scheme, p.deconv, p.criterion, p.order,
+                            len(active), p.dump_tree, p.dump_density, p.kdk, p.repeats, p.ewald))
+        f.write(struct.pack("<5d", p.drift, p.kick1, p.kick2, p.drag1, p.drag2))
+        for a in (p.x, p.y, p.z, p.m,
+                  p.vx if p.vx is not None else zeros,
+                  p.vy if p.vy is not None else zeros,
+                  p.vz if p.vz is not None else zeros):
+            f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+        f.write(active.tobytes())
+
+
+class _Buf:
+    def __init__(self, data: bytes):
+        self.d = data
+        self.o = 0
+
+    def arr(self, dtype, count):
+        a = np.frombuffer(self.d, dtype=dtype, count=count, offset=self.o).copy()
+        self.o += a.nbytes
+        return a
+
+    def q(self):
+        return int(self.arr(np.int64, 1)[0])
+
+
+def read_result(path: str) -> dict:
+    with open(path, "rb") as f:
+        b = _Buf(f.read())
+    assert b.d[:8] == b"CHUIOUT1"
+    b.o = 8
+    n = b.q()
+    na = b.q()
+    r: dict = {"n": n, "n_active": na}
+    for k in ("ax", "ay", "az", "pm_ax", "pm_ay", "pm_az"):
+        r[k] = b.arr(np.float64, na)
+    for k in ("tree_ax", "tree_ay", "tree_az", "nearest_r2"):
+        r[k] = b.arr(np.float64, n)
+    r["first_ms"], r["pm_ms"], r["build_ms"], r["walk_ms"] = b.arr(np.float64, 4)
+    reps = b.q()
+    r["repeat_ms"] = b.arr(np.float64, reps)
+    keys = ("visited", "accepted", "opened", "pairs", "pruned", "pair_skips", "multipoles", "leaves")
+    r["counters"] = dict(zip(keys, (int(v) for v in b.arr(np.uint64, 8))))
+    nn = b.q()
+    r["n_nodes"] = nn
+    if nn:
+        for k in ("ux", "uy", "uz"):
+            r[k] = b.arr(np.float64, n)
+        r["anchors"] = b.arr(np.float64, 3)
+        r["morton_key"] = b.arr(np.uint64, n)
+        r["sorted_index"] = b.arr(np.uint32, n)
+        for k in ("center_x", "center_y", "center_z", "half", "mass", "com_x", "com_y", "com_z",
+                  "qxx", "qxy", "qxz", "qyy", "qyz", "qzz", "trace"):
+            r[k] = b.arr(np.float64, nn)
+        r["child_count"] = b.arr(np.uint32, nn)
+        r["child_index"] = b.arr(np.uint32, 8 * nn)
+        r["particle_begin"] = b.arr(np.uint32, nn)
+        r["particle_count"] = b.arr(np.uint32, nn)
+    cells = b.q()
+    if cells:
+        r["density"] = b.arr(np.float64, cells)
+    kdk = b.q()
+    if kdk:
+        for k in ("kdk_x", "kdk_y", "kdk_z", "kdk_vx", "kdk_vy", "kdk_vz"):
+            r[k] = b.arr(np.float64, n)
+        for k in ("kdk_ax", "kdk_ay", "kdk_az"):
+            r[k] = b.arr(np.float64, na)
+    ew = b.q()
+    if ew:
+        nt = min(ew, na)
+        for k in ("ewald_ax", "ewald_ay", "ewald_az"):
+            r[k] = b.arr(np.float64, nt)
+    return r
+
+
+def available() -> bool:
+    return os.path.isfile(REF_BINARY) and os.access(REF_BINARY, os.X_OK)
+
+
+def run(p: RefProblem, threads: int | None = None, timeout: float | None = None) -> dict:
+    """Run the reference TreePM on problem `p` and return its outputs."""
+    if not available():
+        raise FileNotFoundError(f"reference oracle binary missing: {REF_BINARY}")
+    env = dict(os.environ)
+    if threads is not None:
+        env["OMP_NUM_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        fout = os.path.join(td, "out.bin")
+        write_problem(fin, p)
+        subprocess.run([REF_BINARY, fin, fout], check=True, env=env, timeout=timeout)
+        return read_result(fout)

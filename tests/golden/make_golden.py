@@ -1,0 +1,127 @@
+"""Generate the golden fixtures in tests/golden/ by running the reference's own
+TreePM (oracle/_ref/treepm_ref, compiled from the reference's sources by
+oracle/Makefile.ref) on seeded synthetic inputs.
+
+    make -f oracle/Makefile.ref REF=<reference checkout> -j8
+    python tests/golden/make_golden.py
+
+The reference has no stored golden vectors for this path; these fixtures are
+its outputs on the same inputs, committed so the oracle and the CUDA path can
+be checked without the reference present.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "chui-dev_b200"))
+
+import refio  # noqa: E402
+from chui_treepm import ics  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+TREE_KEYS = ("ux", "uy", "uz", "anchors", "morton_key", "sorted_index", "center_x", "center_y",
+             "center_z", "half", "mass", "com_x", "com_y", "com_z", "qxx", "qxy", "qxz", "qyy",
+             "qyz", "qzz", "trace", "child_count", "child_index", "particle_begin", "particle_count")
+
+
+def save(name: str, p: refio.RefProblem, r: dict, extra: dict | None = None, keep_tree=True):
+    d = {
+        "x": p.x, "y": p.y, "z": p.z, "m": p.m,
+        "vx": p.vx if p.vx is not None else np.zeros_like(p.x),
+        "vy": p.vy if p.vy is not None else np.zeros_like(p.x),
+        "vz": p.vz if p.vz is not None else np.zeros_like(p.x),
+        "active": np.asarray(p.active if p.active is not None else [], dtype=np.uint32),
+        "box": np.array(p.box), "mesh": np.array(p.mesh, dtype=np.int64),
+        "params": np.array([p.asmth, p.rcut, p.theta, p.g, p.eps]),
+        "iparams": np.array([p.leaf, p.scheme, p.deconv, p.criterion, p.order], dtype=np.int64),
+        "kdk_factors": np.array([p.drift, p.kick1, p.kick2, p.drag1, p.drag2]),
+        "counters": np.array([r["counters"][k] for k in ("visited", "accepted", "opened", "pairs",
+                                                         "pruned", "pair_skips", "multipoles", "leaves")],
+                             dtype=np.uint64),
+    }
+    for k in ("ax", "ay", "az", "pm_ax", "pm_ay", "pm_az", "tree_ax", "tree_ay", "tree_az", "nearest_r2"):
+        d[k] = r[k]
+    if keep_tree and r.get("n_nodes"):
+        for k in TREE_KEYS:
+            d[k] = r[k]
+    if "density" in r:
+        d["density"] = r["density"]
+    for k in ("kdk_x", "kdk_y", "kdk_z", "kdk_vx", "kdk_vy", "kdk_vz", "kdk_ax", "kdk_ay", "kdk_az",
+              "ewald_ax", "ewald_ay", "ewald_az"):
+        if k in r:
+            d[k] = r[k]
+    if extra:
+        d.update(extra)
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **d)
+    print(name, len(p.x), "nodes", r.get("n_nodes"), "counters", r["counters"])
+
+
+def main():
+    # 1. 16^3 Zel'dovich lattice, CIC, no deconvolution, unsoftened, one KDK step
+    x, y, z, vx, vy, vz = ics.zeldovich_lattice(16, 10.0, 0.2, seed=11)
+    m = np.full(len(x), 1.0 / len(x))
+    p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(16,) * 3, theta=0.5, leaf=16,
+                         dump_density=1, kdk=1, drift=0.02, kick1=0.01, kick2=0.01,
+                         vx=vx, vy=vy, vz=vz, ewald=32)
+    save("lattice16_cic", p, refio.run(p))
+
+    # 2. clustered: lattice + NFW halos, TSC + deconvolution, softened (accepted multipoles)
+    x, y, z, vx, vy, vz = ics.zeldovich_lattice(20, 50.0, 0.3, seed=12)
+    hx, hy, hz = ics.nfw_halos(3000, 6, 50.0, 2.0, seed=13, total_particles=len(x) + 3000)
+    x, y, z = np.concatenate([x, hx]), np.concatenate([y, hy]), np.concatenate([z, hz])
+    m = np.full(len(x), 2.0 / len(x))
+    p = refio.RefProblem(x, y, z, m, box=(50.0,) * 3, mesh=(16,) * 3, theta=0.7, leaf=16, eps=0.05,
+                         scheme=1, deconv=1, dump_density=1)
+    save("clustered_tsc", p, refio.run(p))
+
+    # 3. rectangular box, non-power-of-two mesh, non-canonical coordinates, active subset
+    rng = np.random.default_rng(14)
+    n = 3000
+    box = (10.0, 8.0, 12.0)
+    x = rng.uniform(-2.0, 12.0, n)
+    y = rng.uniform(0.0, 8.0, n)
+    z = rng.uniform(0.0, 12.0, n)
+    x[:5] = [0.0, 10.0 - 1e-13, -1e-300, 5.0, 5.0]  # seam and coincident samples
+    y[:5] = [0.0, 8.0 - 1e-12, 4.0, 4.0, 4.0]
+    z[:5] = [0.0, 12.0 - 1e-12, 6.0, 6.0, 6.0]
+    m = rng.uniform(0.5, 1.5, n) / n
+    active = np.sort(rng.choice(n, 700, replace=False)).astype(np.uint32)
+    active[:3] = [0, 3, 4]
+    p = refio.RefProblem(x, y, z, m, box=box, mesh=(12, 10, 16), theta=0.5, leaf=8, eps=0.02, rcut=4.5,
+                         active=active, dump_density=1)
+    save("rect_active", p, refio.run(p))
+
+    # 4. tiny cases: two-body, 24-particle quasi-uniform, duplicates deeper than a leaf
+    p = refio.RefProblem(np.array([1.0, 1.7]), np.array([2.0, 2.1]), np.array([3.0, 2.6]),
+                         np.array([1.0, 0.5]), box=(10.0,) * 3, mesh=(16,) * 3, theta=0.5, leaf=1)
+    save("two_body", p, refio.run(p))
+    rng = np.random.default_rng(15)
+    x, y, z = (rng.uniform(0, 4.0, 24) for _ in range(3))
+    p = refio.RefProblem(x, y, z, np.full(24, 1.0 / 24), box=(4.0,) * 3, mesh=(8,) * 3, theta=0.5,
+                         leaf=4, eps=0.01, rcut=3.9)
+    save("quasi24", p, refio.run(p))
+    x = np.concatenate([np.full(20, 1.25), rng.uniform(0, 5.0, 200)])
+    y = np.concatenate([np.full(20, 2.5), rng.uniform(0, 5.0, 200)])
+    z = np.concatenate([np.full(20, 3.75), rng.uniform(0, 5.0, 200)])
+    p = refio.RefProblem(x, y, z, np.full(220, 1.0 / 220), box=(5.0,) * 3, mesh=(8,) * 3, theta=0.5,
+                         leaf=4, eps=0.02, rcut=3.9)
+    save("duplicates", p, refio.run(p))
+
+    # 5. the 32^3 configuration: L = 10 Mpc/h, lattice + Zel'dovich (P ~ k^-2, rms 0.2
+    #    spacing), mesh 64^3, r_s = 1.25 cells, theta = 0.5, leaf 16, CIC, unsoftened,
+    #    one KDK step, Ewald on 8 targets
+    x, y, z, vx, vy, vz = ics.zeldovich_lattice(32, 10.0, 0.2, seed=1)
+    m = np.full(len(x), 1.0 / len(x))
+    p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(64,) * 3, theta=0.5, leaf=16,
+                         kdk=1, drift=0.02, kick1=0.01, kick2=0.01, vx=vx, vy=vy, vz=vz, ewald=8)
+    save("config32", p, refio.run(p))
+
+
+if __name__ == "__main__":
+    main()
