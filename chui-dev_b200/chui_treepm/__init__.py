@@ -1,0 +1,15 @@
+"""B200-native TreePM gravity solver (CUDA kernels behind a C-ABI).
+
+Host-side mirror of the reference's TreePmCoordinator interface; see
+chui_treepm.solver. The CUDA library is chui-dev_b200/_build/libchui_treepm.so.
+"""
+from . import _abi
+from .config import config_from_param_file, config_from_param_text
+from .solver import (AllocationError, DeviceError, InvalidArgument, NotSupported, OutOfRange, StateError,
+                     TreePmConfig, TreePmCoordinator, TreePmError, kdk_factors_static)
+
+__all__ = [
+    "TreePmConfig", "TreePmCoordinator", "TreePmError", "InvalidArgument", "OutOfRange", "StateError",
+    "DeviceError", "AllocationError", "NotSupported", "config_from_param_file", "config_from_param_text",
+    "kdk_factors_static", "_abi",
+]

@@ -1,0 +1,109 @@
+"""`.param.txt` TreePM knobs -> TreePmConfig.
+
+Reads the keys the reference's typed config defines for TreePM
+(include/cosmosim/core/config.hpp:776-821, section [numerics]) and the box
+lengths of [cosmology], with the mapping GravityRuntimeImpl applies
+(src/workflows/gravity_runtime.cpp:469-608): softening in kpc -> Mpc
+(x 1e-3), r_s = treepm_asmth_cells x mesh spacing, r_cut = treepm_rcut_cells x
+spacing, spacing = cbrt(prod L_a / n_a). Unknown keys are ignored: a deck
+carries many subsystems this solver does not own.
+"""
+from __future__ import annotations
+
+import re
+
+from . import _abi
+from .solver import TreePmConfig
+
+# G in Mpc (km/s)^2 / Msun for the reference's default unit system
+# (length mpc, mass msun, velocity km_s).
+G_MPC_KMS2_PER_MSUN = 4.300917270036279e-09
+
+_CRITERIA = {"geometric": _abi.OPEN_GEOMETRIC, "com_distance": _abi.OPEN_COM_DISTANCE,
+             "relative_force_error": _abi.OPEN_RELATIVE}
+_SCHEMES = {"cic": _abi.CIC, "tsc": _abi.TSC}
+
+
+def _bool(v: str) -> bool:
+    v = v.strip().lower()
+    if v in ("true", "1", "yes", "on"):
+        return True
+    if v in ("false", "0", "no", "off"):
+        return False
+    raise ValueError(f"invalid boolean '{v}'")
+
+
+def _length_mpc(v: str) -> float:
+    m = re.fullmatch(r"\s*([-+0-9.eE]+)\s*([A-Za-z]*)\s*", v)
+    if not m:
+        raise ValueError(f"invalid length '{v}'")
+    val, unit = float(m.group(1)), m.group(2).lower()
+    scale = {"": 1.0, "mpc": 1.0, "kpc": 1.0e-3, "pc": 1.0e-6}.get(unit)
+    if scale is None:
+        raise ValueError(f"unsupported length unit '{unit}'")
+    return val * scale
+
+
+def parse_param_text(text: str) -> dict:
+    """Sectioned `key = value` pairs: {"section.key": "value"}."""
+    out: dict = {}
+    section = ""
+    for raw in text.splitlines():
+        line = raw.split("#", 1)[0].strip()
+        if not line:
+            continue
+        if line.startswith("[") and line.endswith("]"):
+            section = line[1:-1].strip()
+            continue
+        if "=" not in line:
+            continue
+        k, v = line.split("=", 1)
+        out[f"{section}.{k.strip()}" if section else k.strip()] = v.strip()
+    return out
+
+
+def config_from_param_text(text: str, precision: int = _abi.MIXED, device: int = 0,
+                           gravitational_constant: float | None = None) -> TreePmConfig:
+    kv = parse_param_text(text)
+    c = TreePmConfig(precision=precision, device=device)
+
+    def get(key, conv, default=None):
+        v = kv.get(key)
+        if v is None or v == "":
+            return default
+        return conv(v)
+
+    c.pm_grid_nx = get("numerics.treepm_pm_grid_nx", int, get("numerics.treepm_pm_grid", int, 16))
+    c.pm_grid_ny = get("numerics.treepm_pm_grid_ny", int, c.pm_grid_nx)
+    c.pm_grid_nz = get("numerics.treepm_pm_grid_nz", int, c.pm_grid_nx)
+    c.box_x = get("cosmology.box_size_x", _length_mpc, 1.0)
+    c.box_y = get("cosmology.box_size_y", _length_mpc, c.box_x)
+    c.box_z = get("cosmology.box_size_z", _length_mpc, c.box_x)
+    c.asmth_cells = get("numerics.treepm_asmth_cells", float, 1.25)
+    c.rcut_cells = get("numerics.treepm_rcut_cells", float, 6.25)
+    c.opening_theta = get("numerics.treepm_tree_opening_theta", float, 0.7)
+    crit = get("numerics.treepm_tree_opening_criterion", lambda v: v.strip().lower(), "com_distance")
+    if crit not in _CRITERIA:
+        raise ValueError(f"key 'numerics.treepm_tree_opening_criterion': invalid value '{crit}'")
+    c.opening_criterion = _CRITERIA[crit]
+    c.max_leaf_size = get("numerics.treepm_tree_max_leaf_size", int, 16)
+    scheme = get("numerics.treepm_assignment_scheme", lambda v: v.strip().lower(), "tsc")
+    if scheme not in _SCHEMES:
+        raise ValueError(f"key 'numerics.treepm_assignment_scheme': invalid value '{scheme}'")
+    c.assignment_scheme = _SCHEMES[scheme]
+    c.window_deconvolution = 1 if get("numerics.treepm_enable_window_deconvolution", _bool, True) else 0
+    if get("numerics.treepm_adaptive_acceptance_enabled", _bool, False):
+        c.acceptance_policy = 1  # rejected by the library: only the strict policy is implemented
+    soft = kv.get("numerics.gravity_softening")
+    if soft:
+        # gravity_softening_kpc_comoving * 1e-3 (gravity_runtime.cpp:579-581)
+        c.softening = _length_mpc(soft if re.search(r"[A-Za-z]", soft) else soft + " kpc")
+    else:
+        c.softening = 1.0e-3
+    c.gravitational_constant = gravitational_constant if gravitational_constant is not None else G_MPC_KMS2_PER_MSUN
+    return c
+
+
+def config_from_param_file(path: str, **kw) -> TreePmConfig:
+    with open(path) as f:
+        return config_from_param_text(f.read(), **kw)

@@ -49,7 +49,7 @@ def gaussian_displacement(n_side: int, box: float, rms_spacing: float, seed: int
     for comp in (kx, ky, kzz):
         # psi_k = i k delta_k / k^2 (displacement is the gradient of the potential)
         pk = 1j * comp * dk / k2
-        psi.append(np.fft.irfftn(pk, s=(n_side, n_side, n_side)).ravel())
+        psi.append(np.fft.irfftn(pk, s=(n_side, n_side, n_side), axes=(0, 1, 2)).ravel())
     psi = np.stack(psi)
     rms = math.sqrt(float(np.mean(np.sum(psi * psi, axis=0))))
     spacing = box / n_side

@@ -1,0 +1,332 @@
+"""Python mirror of the reference's TreePM gravity-solver interface over the
+C-ABI (include/chui_treepm.h).
+
+`TreePmCoordinator` follows cosmosim::gravity::TreePmCoordinator
+(include/cosmosim/gravity/tree_pm_coupling.hpp:527-814 in the reference):
+construct with the mesh shape and options, then `solve_active_set` /
+`solve_active_set_with_pm_cadence` with source positions, masses and an
+accumulator. Errors carry the reference's exception types: invalid input
+raises ValueError (std::invalid_argument), index/depth/stack overflow raises
+IndexError / OverflowError (std::out_of_range / std::overflow_error), reuse of
+a missing PM field raises RuntimeError (std::runtime_error).
+
+Arrays may be numpy arrays (host memory: the library stages them) or CUDA
+torch tensors of the context's device (device memory: used in place, the
+zero-copy path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _abi
+
+
+class TreePmError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class InvalidArgument(TreePmError, ValueError):
+    pass
+
+
+class OutOfRange(TreePmError, IndexError):
+    pass
+
+
+class StateError(TreePmError):
+    pass
+
+
+class DeviceError(TreePmError):
+    pass
+
+
+class AllocationError(TreePmError, MemoryError):
+    pass
+
+
+class NotSupported(TreePmError, NotImplementedError):
+    pass
+
+
+_ERRORS = {
+    _abi.EINVAL: InvalidArgument,
+    _abi.ERANGE: OutOfRange,
+    _abi.ESTATE: StateError,
+    _abi.EDEVICE: DeviceError,
+    _abi.ENOMEM: AllocationError,
+    _abi.ENOTSUP: NotSupported,
+}
+
+
+@dataclass
+class TreePmConfig:
+    """The `.param.txt` [numerics] treepm_* knobs (see chui_treepm.config)."""
+    pm_grid_nx: int = 16
+    pm_grid_ny: int = 16
+    pm_grid_nz: int = 16
+    box_x: float = 1.0
+    box_y: float = 1.0
+    box_z: float = 1.0
+    asmth_cells: float = 1.25
+    rcut_cells: float = 6.25
+    opening_theta: float = 0.7
+    opening_criterion: int = _abi.OPEN_COM_DISTANCE
+    multipole_order: int = 2
+    max_leaf_size: int = 16
+    assignment_scheme: int = _abi.CIC
+    window_deconvolution: int = 0
+    gravitational_constant: float = 1.0
+    softening: float = 0.0
+    acceptance_policy: int = 0
+    precision: int = _abi.MIXED
+    device: int = 0
+
+    def to_c(self) -> _abi.Config:
+        c = _abi.Config()
+        for f in fields(self):
+            setattr(c, f.name, getattr(self, f.name))
+        return c
+
+    @property
+    def mesh_spacing(self) -> float:
+        return ((self.box_x / self.pm_grid_nx) * (self.box_y / self.pm_grid_ny) *
+                (self.box_z / self.pm_grid_nz)) ** (1.0 / 3.0)
+
+
+def _is_torch(a) -> bool:
+    return hasattr(a, "data_ptr") and hasattr(a, "is_cuda")
+
+
+class _Arrays:
+    """Resolves numpy / torch inputs to raw pointers for one call."""
+
+    def __init__(self, sample):
+        self.device = _is_torch(sample) and sample.is_cuda
+        self.keep = []
+
+    def ptr(self, a, dtype):
+        if a is None:
+            return None
+        if self.device:
+            import torch
+            if not (_is_torch(a) and a.is_cuda):
+                raise InvalidArgument(_abi.EINVAL, "mixed host and device arrays in one call")
+            if dtype == np.uint32:
+                # 32-bit index lanes travel as int32 bit patterns (0xFFFFFFFF == -1)
+                if a.dtype != torch.int32:
+                    a = a.to(torch.int64)
+                    a = torch.where(a >= 2 ** 31, a - 2 ** 32, a).to(torch.int32)
+            elif dtype == np.float64:
+                if a.dtype != torch.float64:
+                    a = a.to(torch.float64)
+            elif a.dtype != torch.int64:
+                a = a.to(torch.int64)
+            a = a.contiguous()
+            self.keep.append(a)
+            return a.data_ptr()
+        arr = np.ascontiguousarray(a, dtype=dtype)
+        self.keep.append(arr)
+        return arr.ctypes.data
+
+    def out(self, n, like=None, dtype=np.float64):
+        if self.device:
+            import torch
+            t = torch.empty(n, dtype=torch.float64 if dtype == np.float64 else torch.int64, device=like.device)
+            self.keep.append(t)
+            return t, t.data_ptr()
+        arr = np.empty(n, dtype=dtype)
+        self.keep.append(arr)
+        return arr, arr.ctypes.data
+
+
+class TreePmCoordinator:
+    """B200 TreePM solver instance (owns PM mesh, FFT plans, tree, scratch)."""
+
+    def __init__(self, config: TreePmConfig):
+        self._lib = _abi.load()
+        self.config = config
+        h = C.c_void_p()
+        rc = self._lib.chui_treepm_create(C.byref(config.to_c()), C.byref(h))
+        if rc != 0:
+            raise _ERRORS.get(rc, TreePmError)(rc, f"chui_treepm_create failed ({rc})")
+        self._h = h
+        self.last_stats: dict = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.chui_treepm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self._lib.chui_treepm_last_error(self._h).decode()
+            raise _ERRORS.get(rc, TreePmError)(rc, msg or f"error {rc}")
+
+    def set_config(self, config: TreePmConfig):
+        self._check(self._lib.chui_treepm_set_config(self._h, C.byref(config.to_c())))
+        self.config = config
+
+    # -- solve ----------------------------------------------------------------
+    def solve_active_set_with_pm_cadence(self, x, y, z, mass, refresh_long_range_field: bool, active=None,
+                                         targets=None, uniform_mass: float | None = None,
+                                         long_range: bool = False, short_range: bool = False,
+                                         nearest_pair: bool = False, stream=None) -> dict:
+        """TreePmCoordinator::solveActiveSetWithPmCadence. Returns a dict with
+        ax, ay, az (active-slot order) and the requested optional lanes."""
+        arr = _Arrays(x)
+        n = len(x)
+        src = _abi.Sources()
+        src.count = n
+        src.x, src.y, src.z = arr.ptr(x, np.float64), arr.ptr(y, np.float64), arr.ptr(z, np.float64)
+        if mass is None:
+            if uniform_mass is None:
+                raise InvalidArgument(_abi.EINVAL, "mass or uniform_mass is required")
+            src.mass = None
+            src.uniform_mass = float(uniform_mass)
+        else:
+            src.mass = arr.ptr(mass, np.float64)
+            src.uniform_mass = 0.0
+        acc = _abi.Accumulator()
+        if targets is not None:
+            tx, ty, tz = targets
+            nt = len(tx)
+            acc.target_x, acc.target_y, acc.target_z = (arr.ptr(tx, np.float64), arr.ptr(ty, np.float64),
+                                                        arr.ptr(tz, np.float64))
+            if active is None:
+                active = np.full(nt, 0xFFFFFFFF, dtype=np.uint32)
+                if arr.device:
+                    import torch
+                    active = torch.full((nt,), 0xFFFFFFFF, dtype=torch.int64, device=x.device)
+        else:
+            nt = n if active is None else len(active)
+        acc.active_count = nt
+        acc.active_index = arr.ptr(active, np.uint32) if active is not None else None
+        out = {}
+        out["ax"], acc.accel_x = arr.out(nt, x)
+        out["ay"], acc.accel_y = arr.out(nt, x)
+        out["az"], acc.accel_z = arr.out(nt, x)
+        if long_range:
+            out["pm_ax"], acc.long_range_x = arr.out(nt, x)
+            out["pm_ay"], acc.long_range_y = arr.out(nt, x)
+            out["pm_az"], acc.long_range_z = arr.out(nt, x)
+        if short_range:
+            for k, attr in (("tree_ax", "short_range_x"), ("tree_ay", "short_range_y"),
+                            ("tree_az", "short_range_z")):
+                a, p = arr.out(n, x)
+                a[:] = 0.0
+                out[k] = a
+                setattr(acc, attr, p)
+        if nearest_pair:
+            a, p = arr.out(n, x)
+            a[:] = float("inf")
+            out["nearest_r2"] = a
+            acc.nearest_pair_r2 = p
+        st = _abi.Stats()
+        rc = self._lib.chui_treepm_solve(self._h, C.byref(src), C.byref(acc), 1 if refresh_long_range_field else 0,
+                                         _abi.DEVICE if arr.device else _abi.HOST,
+                                         C.c_void_p(stream) if stream else None, C.byref(st))
+        self._check(rc)
+        self.last_stats = st.as_dict()
+        out["stats"] = self.last_stats
+        return out
+
+    def solve_active_set(self, x, y, z, mass, **kw) -> dict:
+        """TreePmCoordinator::solveActiveSet: the cadence variant with refresh."""
+        return self.solve_active_set_with_pm_cadence(x, y, z, mass, True, **kw)
+
+    # -- PM pieces ------------------------------------------------------------
+    def assign_density(self, x, y, z, mass, uniform_mass: float = 0.0):
+        arr = _Arrays(x)
+        src = _abi.Sources()
+        src.count = len(x)
+        src.x, src.y, src.z = arr.ptr(x, np.float64), arr.ptr(y, np.float64), arr.ptr(z, np.float64)
+        src.mass = arr.ptr(mass, np.float64) if mass is not None else None
+        src.uniform_mass = uniform_mass
+        c = self.config
+        rho, p = arr.out(c.pm_grid_nx * c.pm_grid_ny * c.pm_grid_nz, x)
+        self._check(self._lib.chui_pm_assign_density(self._h, C.byref(src), C.c_void_p(p),
+                                                     _abi.DEVICE if arr.device else _abi.HOST, None))
+        return rho
+
+    def cells(self, x, y, z):
+        arr = _Arrays(x)
+        src = _abi.Sources()
+        src.count = len(x)
+        src.x, src.y, src.z = arr.ptr(x, np.float64), arr.ptr(y, np.float64), arr.ptr(z, np.float64)
+        out, p = arr.out(3 * len(x), x, dtype=np.int64)
+        self._check(self._lib.chui_pm_cells(self._h, C.byref(src), C.c_void_p(p),
+                                            _abi.DEVICE if arr.device else _abi.HOST, None))
+        return out.reshape(-1, 3)
+
+    # -- parity dumps ---------------------------------------------------------
+    def dump_tree(self, n: int) -> dict:
+        nn = C.c_int64()
+        self._check(self._lib.chui_treepm_tree_node_count(self._h, C.byref(nn)))
+        nn = nn.value
+        d = _abi.TreeDump()
+        r = {}
+        for k in ("center_x", "center_y", "center_z", "half_size", "mass", "com_x", "com_y", "com_z",
+                  "quad_xx", "quad_xy", "quad_xz", "quad_yy", "quad_yz", "quad_zz", "second_moment_trace"):
+            r[k] = np.zeros(nn)
+            setattr(d, k, r[k].ctypes.data)
+        for k, cnt in (("child_count", nn), ("child_index", 8 * nn), ("particle_begin", nn),
+                       ("particle_count", nn)):
+            r[k] = np.zeros(cnt, dtype=np.uint32)
+            setattr(d, k, r[k].ctypes.data)
+        self._check(self._lib.chui_treepm_dump_tree(self._h, C.byref(d)))
+        ux, uy, uz = np.zeros(n), np.zeros(n), np.zeros(n)
+        mk = np.zeros(n, dtype=np.uint64)
+        si = np.zeros(n, dtype=np.uint32)
+        anchors = np.zeros(3)
+        self._check(self._lib.chui_treepm_dump_particles(self._h, n, ux.ctypes.data, uy.ctypes.data, uz.ctypes.data,
+                                                         mk.ctypes.data, si.ctypes.data, anchors.ctypes.data))
+        r.update(ux=ux, uy=uy, uz=uz, morton_key=mk, sorted_index=si, anchors=anchors, n_nodes=nn)
+        return r
+
+    # -- KDK ------------------------------------------------------------------
+    def kick(self, vx, vy, vz, ax, ay, az, kick_factor: float, drag_factor: float = 1.0):
+        arr = _Arrays(vx)
+        if not arr.device:
+            for v in (vx, vy, vz):
+                if not (isinstance(v, np.ndarray) and v.dtype == np.float64 and v.flags.c_contiguous):
+                    raise InvalidArgument(_abi.EINVAL, "kick updates contiguous float64 arrays in place")
+        ps = [arr.ptr(a, np.float64) for a in (vx, vy, vz, ax, ay, az)]
+        self._check(self._lib.chui_treepm_kick(self._h, len(vx), *[C.c_void_p(p) for p in ps], kick_factor,
+                                               drag_factor, _abi.DEVICE if arr.device else _abi.HOST, None))
+
+    def drift(self, x, y, z, vx, vy, vz, drift_factor: float):
+        arr = _Arrays(x)
+        if not arr.device:
+            for v in (x, y, z):
+                if not (isinstance(v, np.ndarray) and v.dtype == np.float64 and v.flags.c_contiguous):
+                    raise InvalidArgument(_abi.EINVAL, "drift updates contiguous float64 arrays in place")
+        ps = [arr.ptr(a, np.float64) for a in (x, y, z, vx, vy, vz)]
+        self._check(self._lib.chui_treepm_drift(self._h, len(x), *[C.c_void_p(p) for p in ps], drift_factor,
+                                                _abi.DEVICE if arr.device else _abi.HOST, None))
+
+
+def kdk_factors_static(dt: float):
+    """CosmologicalTimeline::prepareStep without a background: (D, K1, K2, drag1, drag2)."""
+    f = np.zeros(5)
+    rc = _abi.load().chui_treepm_kdk_factors_static(dt, f.ctypes.data)
+    if rc != 0:
+        raise InvalidArgument(rc, "dt must be finite and positive")
+    return tuple(float(v) for v in f)

@@ -1,0 +1,894 @@
+// C-ABI of the B200 TreePM solver (include/chui_treepm.h): context lifecycle,
+// input validation with the reference's error semantics, host/device staging,
+// and the orchestration of one solve (TreePmCoordinator::solveActiveSetWithPmCadence,
+// tree_pm_coupling.cpp:2282-3518): PM refresh -> periodic tree build ->
+// residual walk -> PM interpolation -> accumulation.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "context.cuh"
+
+namespace chui {
+
+cudaError_t ensure(DevBuf& b, size_t bytes) {
+  if (bytes <= b.bytes && b.ptr) return cudaSuccess;
+  if (b.ptr) cudaFree(b.ptr);
+  b.ptr = nullptr;
+  b.bytes = 0;
+  const size_t want = bytes ? bytes : 16;
+  cudaError_t e = cudaMalloc(&b.ptr, want);
+  if (e == cudaSuccess) b.bytes = want;
+  return e;
+}
+
+void release(DevBuf& b) {
+  if (b.ptr) cudaFree(b.ptr);
+  b.ptr = nullptr;
+  b.bytes = 0;
+}
+
+const char* statusText(uint32_t bits) {
+  if (bits & kStatusStackOverflow) return "TreePM residual traversal stack overflow";
+  if (bits & kStatusDepthExceeded) return "Tree gravity maximum depth contract exceeded";
+  if (bits & kStatusNonFinite) return "TreePM sources require finite coordinates and finite non-negative masses";
+  if (bits & kStatusNegativeMass) return "TreePM sources require finite coordinates and finite non-negative masses";
+  if (bits & kStatusIndexRange) return "TreePM active index exceeds particle count";
+  return "";
+}
+
+namespace {
+
+inline unsigned gridFor(size_t n, int block) {
+  size_t b = (n + block - 1) / block;
+  if (b > 148u * 32u) b = 148u * 32u;
+  return static_cast<unsigned>(b ? b : 1);
+}
+
+// min/max per axis, finiteness, non-negative mass and mass sum in one pass.
+__global__ void sourceReduceKernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                   const double* __restrict__ z, const double* __restrict__ m,
+                                   unsigned long long* out, double* mass_sum, uint32_t* status) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double msum = 0.0;
+  uint32_t bad = 0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double p[3] = {x[i], y[i], z[i]};
+    for (int a = 0; a < 3; ++a) {
+      if (!isfinite(p[a])) bad |= kStatusNonFinite;
+      lo[a] = fmin(lo[a], p[a]);
+      hi[a] = fmax(hi[a], p[a]);
+    }
+    if (m) {
+      const double mi = m[i];
+      if (!isfinite(mi)) bad |= kStatusNonFinite;
+      if (mi < 0.0) bad |= kStatusNegativeMass;
+      msum += mi;
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+      hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    msum += __shfl_xor_sync(0xffffffffu, msum, off);
+    bad |= __shfl_xor_sync(0xffffffffu, bad, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(out + a, orderedBits(lo[a]));
+      atomicMax(out + 3 + a, orderedBits(hi[a]));
+    }
+    if (m) atomicAdd(mass_sum, msum);
+    if (bad) atomicOr(status, bad);
+  }
+}
+
+__global__ void activeCheckKernel(int64_t nt, const uint32_t* __restrict__ active, int64_t n, int explicit_targets,
+                                  uint32_t* status) {
+  uint32_t bad = 0;
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nt;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t r = active[k];
+    if (r >= n && !(explicit_targets && r == kInvalid)) bad = kStatusIndexRange;
+  }
+  if (bad) atomicOr(status, bad);
+}
+
+// accel = PM + tree (active order); optional source-indexed tree-only and
+// nearest-pair lanes (TreePmForceAccumulatorView::addShortRangeToActiveSlot and
+// noteNearestPairToActiveSlot, tree_pm_coupling.cpp:1961-1978).
+__global__ void combineKernel(int64_t nt, const uint32_t* __restrict__ active, int64_t n,
+                              const double* __restrict__ pmx, const double* __restrict__ pmy,
+                              const double* __restrict__ pmz, const double* __restrict__ tr,
+                              const double* __restrict__ near, double* ax, double* ay, double* az,
+                              double* sx, double* sy, double* sz, double* snear) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nt;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double tx = tr[k], ty = tr[nt + k], tz = tr[2 * nt + k];
+    ax[k] = (pmx ? pmx[k] : 0.0) + tx;
+    ay[k] = (pmy ? pmy[k] : 0.0) + ty;
+    az[k] = (pmz ? pmz[k] : 0.0) + tz;
+    const uint32_t row = active ? active[k] : static_cast<uint32_t>(k);
+    if (row < n) {
+      if (sx) {
+        sx[row] = tx;
+        sy[row] = ty;
+        sz[row] = tz;
+      }
+      if (snear) snear[row] = near[k];
+    }
+  }
+}
+
+// applyPeculiarVelocityKick (src/workflows/gravity_runtime.cpp:3043-3059).
+__global__ void kickKernel(int64_t n, double* vx, double* vy, double* vz, const double* __restrict__ ax,
+                           const double* __restrict__ ay, const double* __restrict__ az, double kick, double drag) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    vx[i] = fma(kick, ax[i], drag * vx[i]);
+    vy[i] = fma(kick, ay[i], drag * vy[i]);
+    vz[i] = fma(kick, az[i], drag * vz[i]);
+  }
+}
+
+// Drift + core::canonicalPeriodicPosition (include/cosmosim/core/periodic_domain.hpp:8-16;
+// src/workflows/reference_runtime_composition.cpp:76-107).
+__device__ __forceinline__ double canonicalPosition(double v, double box) {
+  double w = fmod(v, box);
+  if (w < 0.0) w += box;
+  if (!(w < box)) w = 0.0;
+  return w;
+}
+
+__global__ void driftKernel(int64_t n, double* x, double* y, double* z, const double* __restrict__ vx,
+                            const double* __restrict__ vy, const double* __restrict__ vz, double drift,
+                            double bx, double by, double bz) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    x[i] = canonicalPosition(fma(vx[i], drift, x[i]), bx);
+    y[i] = canonicalPosition(fma(vy[i], drift, y[i]), by);
+    z[i] = canonicalPosition(fma(vz[i], drift, z[i]), bz);
+  }
+}
+
+// ---- Gaussian long-range coefficient polynomial (host) ----------------------
+
+double hostH(double t) {
+  // H(t) = L(sqrt t)/t^(3/2) (tree_pm_split_kernel.hpp:109-116 and :90-107)
+  const double c = 2.25675833419102514779231780624309034;
+  if (t < 0.015625) {
+    return c * (1.0 / 3.0 + t * (-1.0 / 5.0 + t * (1.0 / 14.0 + t * (-1.0 / 54.0 +
+                t * (1.0 / 264.0 + t * (-1.0 / 1560.0 + t * (1.0 / 10800.0 - t / 85680.0)))))));
+  }
+  const double q = std::sqrt(t);
+  return (std::erf(q) - 0.5 * c * q * std::exp(-t)) / (t * q);
+}
+
+PolyH fitPoly(double t_cut) {
+  PolyH best;
+  best.max_rel_error = 1e300;
+  for (int deg = 6; deg < kPolyMaxTerms; ++deg) {
+    const int m = deg + 1;
+    std::vector<double> f(m), cheb(m, 0.0);
+    const double pi = 3.141592653589793238462643383279502884;
+    for (int k = 0; k < m; ++k) {
+      const double xk = std::cos(pi * (k + 0.5) / m);
+      f[k] = hostH((xk + 1.0) * 0.5 * t_cut);
+    }
+    for (int j = 0; j < m; ++j) {
+      double sum = 0.0;
+      for (int k = 0; k < m; ++k) sum += f[k] * std::cos(pi * j * (k + 0.5) / m);
+      cheb[j] = (j == 0 ? 1.0 : 2.0) * sum / m;
+    }
+    // Chebyshev -> monomial in s
+    std::vector<double> mono(m, 0.0), tkm1(m, 0.0), tk(m, 0.0), tkp1(m, 0.0);
+    tkm1[0] = 1.0;
+    if (m > 1) tk[1] = 1.0;
+    for (int i = 0; i < m; ++i) mono[i] += cheb[0] * tkm1[i];
+    if (m > 1)
+      for (int i = 0; i < m; ++i) mono[i] += cheb[1] * tk[i];
+    for (int j = 2; j < m; ++j) {
+      std::fill(tkp1.begin(), tkp1.end(), 0.0);
+      for (int i = 0; i < m; ++i) {
+        if (i + 1 < m) tkp1[i + 1] += 2.0 * tk[i];
+        tkp1[i] -= tkm1[i];
+      }
+      for (int i = 0; i < m; ++i) mono[i] += cheb[j] * tkp1[i];
+      tkm1 = tk;
+      tk = tkp1;
+    }
+    PolyH p;
+    p.terms = m;
+    p.scale = static_cast<float>(2.0 / t_cut);
+    for (int i = 0; i < m; ++i) p.c[i] = static_cast<float>(mono[i]);
+    double err = 0.0;
+    for (int k = 0; k <= 4000; ++k) {
+      const double t = t_cut * k / 4000.0;
+      const float s = std::fmaf(static_cast<float>(t), p.scale, -1.0f);
+      float h = p.c[m - 1];
+      for (int i = m - 2; i >= 0; --i) h = std::fmaf(h, s, p.c[i]);
+      const double ref = hostH(t);
+      err = std::max(err, std::fabs(static_cast<double>(h) - ref) / ref);
+    }
+    p.max_rel_error = err;
+    if (err < best.max_rel_error) best = p;
+    if (err < 1.0e-6) break;
+  }
+  return best;
+}
+
+int fail(Context& c, int code, const std::string& msg) {
+  c.last_error = msg;
+  return code;
+}
+
+int validateConfig(const chui_treepm_config& cfg, std::string& err) {
+  if (cfg.pm_grid_nx <= 0 || cfg.pm_grid_ny <= 0 || cfg.pm_grid_nz <= 0) {
+    err = "numerics.treepm_pm_grid_n{xyz} must all be > 0";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if (!(std::isfinite(cfg.box_x) && std::isfinite(cfg.box_y) && std::isfinite(cfg.box_z)) || cfg.box_x <= 0 ||
+      cfg.box_y <= 0 || cfg.box_z <= 0 || !std::isfinite(cfg.gravitational_constant) ||
+      cfg.gravitational_constant <= 0) {
+    err = "TreePM requires finite positive box axes, scale factor, and gravitational constants";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if (!std::isfinite(cfg.asmth_cells) || cfg.asmth_cells <= 0) {
+    err = "TreePM asmth_cells must be > 0";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if (!std::isfinite(cfg.rcut_cells) || cfg.rcut_cells <= 0) {
+    err = "TreePM rcut_cells must be > 0";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if (!std::isfinite(cfg.opening_theta) || cfg.opening_theta <= 0 || cfg.max_leaf_size <= 0 ||
+      !std::isfinite(cfg.softening) || cfg.softening < 0 ||
+      (cfg.opening_criterion < 0 || cfg.opening_criterion > 2) ||
+      (cfg.multipole_order != 0 && cfg.multipole_order != 2)) {
+    err = "TreePM tree options are invalid";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if (cfg.assignment_scheme != CHUI_TREEPM_CIC && cfg.assignment_scheme != CHUI_TREEPM_TSC) {
+    err = "TreePM PM assignment scheme is invalid";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if (cfg.acceptance_policy != 0) {
+    err = "only the strict reference acceptance policy is implemented";
+    return CHUI_TREEPM_ENOTSUP;
+  }
+  if (cfg.precision != CHUI_TREEPM_MIXED && cfg.precision != CHUI_TREEPM_FP64) {
+    err = "precision must be CHUI_TREEPM_MIXED or CHUI_TREEPM_FP64";
+    return CHUI_TREEPM_EINVAL;
+  }
+  const double spacing = std::cbrt((cfg.box_x / cfg.pm_grid_nx) * (cfg.box_y / cfg.pm_grid_ny) *
+                                   (cfg.box_z / cfg.pm_grid_nz));
+  const double cutoff = cfg.rcut_cells * spacing;
+  const double half_short = 0.5 * std::min({cfg.box_x, cfg.box_y, cfg.box_z});
+  if (cutoff >= std::nextafter(half_short, 0.0)) {
+    err = "Periodic TreePM requires cutoff_radius_comoving < half the shortest box axis; cutoff_radius_comoving=" +
+          std::to_string(cutoff) + ", half_shortest_axis=" + std::to_string(half_short) +
+          "; the short-range tree evaluates one minimum image per source";
+    return CHUI_TREEPM_EINVAL;
+  }
+  return 0;
+}
+
+void applyConfig(Context& c, const chui_treepm_config& cfg) {
+  c.cfg = cfg;
+  // makeTreePmSplitPolicyFromMeshSpacing (tree_pm_split_kernel.hpp:50-63) with the
+  // mesh spacing of gravity_runtime.cpp:586-590.
+  c.spacing = std::cbrt((cfg.box_x / static_cast<double>(cfg.pm_grid_nx)) *
+                        (cfg.box_y / static_cast<double>(cfg.pm_grid_ny)) *
+                        (cfg.box_z / static_cast<double>(cfg.pm_grid_nz)));
+  c.rs = cfg.asmth_cells * c.spacing;
+  c.cutoff = cfg.rcut_cells * c.spacing;
+  const double t_cut = (c.cutoff * c.cutoff) / (4.0 * c.rs * c.rs) * (1.0 + 1.0e-5);
+  c.poly = fitPoly(t_cut);
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Stage a host array into a device buffer (or pass a device pointer through).
+template <class T>
+int stageIn(Context& c, DevBuf& buf, const T* src, int64_t count, int memory, cudaStream_t s, const T** out) {
+  if (src == nullptr || count == 0) {
+    *out = src;
+    if (count == 0 && src == nullptr) return 0;
+    if (count == 0) return 0;
+    return 0;
+  }
+  if (memory == CHUI_TREEPM_DEVICE) {
+    *out = src;
+    return 0;
+  }
+  if (ensure(buf, count * sizeof(T)) != cudaSuccess) return fail(c, CHUI_TREEPM_ENOMEM, "device staging allocation failed");
+  if (cudaMemcpyAsync(buf.ptr, src, count * sizeof(T), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return fail(c, CHUI_TREEPM_EDEVICE, "host-to-device copy failed");
+  *out = buf.as<T>();
+  return 0;
+}
+
+}  // namespace
+
+int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
+                 double lo[3], double hi[3], double* mass_sum, uint32_t* status_bits, cudaStream_t s) {
+  auto* sc = c.scalars.as<unsigned long long>();
+  unsigned long long init[8] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+  cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(c.status.ptr, 0, 4, s);
+  if (n > 0)
+    sourceReduceKernel<<<gridFor(n, 256), 256, 0, s>>>(n, x, y, z, m, sc, reinterpret_cast<double*>(sc + 6),
+                                                       c.status.as<uint32_t>());
+  unsigned long long hb[8];
+  uint32_t st = 0;
+  cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&st, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(c, CHUI_TREEPM_EDEVICE, "source reduction failed");
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = n > 0 ? fromOrderedBits(hb[a]) : INFINITY;
+    hi[a] = n > 0 ? fromOrderedBits(hb[3 + a]) : -INFINITY;
+  }
+  double ms;
+  std::memcpy(&ms, &hb[6], 8);
+  *mass_sum = ms;
+  *status_bits = st;
+  return 0;
+}
+
+}  // namespace chui
+
+using chui::Context;
+
+extern "C" {
+
+int chui_treepm_config_default(chui_treepm_config* cfg) {
+  if (!cfg) return CHUI_TREEPM_EINVAL;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->pm_grid_nx = cfg->pm_grid_ny = cfg->pm_grid_nz = 16;  // config.hpp:778-780
+  cfg->box_x = cfg->box_y = cfg->box_z = 1.0;
+  cfg->asmth_cells = 1.25;                                    // config.hpp:783
+  cfg->rcut_cells = 6.25;                                     // config.hpp:784
+  cfg->opening_theta = 0.7;                                   // tree_gravity.hpp:33
+  cfg->opening_criterion = CHUI_TREEPM_OPEN_COM_DISTANCE;     // tree_gravity.hpp:34
+  cfg->multipole_order = 2;                                   // tree_gravity.hpp:35
+  cfg->max_leaf_size = 16;                                    // tree_gravity.hpp:37
+  cfg->assignment_scheme = CHUI_TREEPM_CIC;                   // pm_solver.hpp:231
+  cfg->window_deconvolution = 0;                              // pm_solver.hpp:232
+  cfg->gravitational_constant = 1.0;
+  cfg->softening = 0.0;
+  cfg->acceptance_policy = 0;
+  cfg->precision = CHUI_TREEPM_MIXED;
+  cfg->device = 0;
+  return 0;
+}
+
+int chui_treepm_create(const chui_treepm_config* cfg, void** handle) {
+  if (!cfg || !handle) return CHUI_TREEPM_EINVAL;
+  *handle = nullptr;
+  std::string err;
+  int rc = chui::validateConfig(*cfg, err);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return CHUI_TREEPM_EDEVICE;
+  if (cfg->device < 0 || cfg->device >= ndev) return CHUI_TREEPM_EINVAL;
+  Context* c = new (std::nothrow) Context();
+  if (!c) return CHUI_TREEPM_ENOMEM;
+  c->device = cfg->device;
+  chui::DeviceGuard guard(c->device);
+  chui::applyConfig(*c, *cfg);
+  if (chui::ensure(c->status, 64) != cudaSuccess || chui::ensure(c->scalars, 64 * 8) != cudaSuccess) {
+    delete c;
+    return CHUI_TREEPM_ENOMEM;
+  }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+  c->events_ready = true;
+  *handle = c;
+  return 0;
+}
+
+void chui_treepm_destroy(void* handle) {
+  if (!handle) return;
+  Context* c = static_cast<Context*>(handle);
+  {
+    chui::DeviceGuard guard(c->device);
+    cudaDeviceSynchronize();
+    chui::pmDestroy(*c);
+    chui::DevBuf* bufs[] = {&c->in_x, &c->in_y, &c->in_z, &c->in_m, &c->in_active, &c->in_tx, &c->in_ty, &c->in_tz,
+                            &c->out_acc[0], &c->out_acc[1], &c->out_acc[2], &c->out_pm[0], &c->out_pm[1],
+                            &c->out_pm[2], &c->out_tree[0], &c->out_tree[1], &c->out_tree[2], &c->out_near,
+                            &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max,
+                            &c->bucket_next, &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
+                            &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
+                            &c->leaf_of_pos, &c->inv_pos, &c->cub_temp, &c->node_geom, &c->node_com,
+                            &c->node_quad, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
+                            &c->node_counter, &c->sorted_index, &c->pos_of_row, &c->src_f4, &c->src_d4,
+                            &c->target_order, &c->morton_sorted, &c->walk_counters, &c->work_counter,
+                            &c->tree_acc, &c->tree_near};
+    for (auto* b : bufs) chui::release(*b);
+    if (c->events_ready)
+      for (auto& e : c->ev) cudaEventDestroy(e);
+  }
+  delete c;
+}
+
+int chui_treepm_set_config(void* handle, const chui_treepm_config* cfg) {
+  if (!handle || !cfg) return CHUI_TREEPM_EINVAL;
+  Context* c = static_cast<Context*>(handle);
+  std::string err;
+  int rc = chui::validateConfig(*cfg, err);
+  if (rc) return chui::fail(*c, rc, err);
+  if (cfg->pm_grid_nx != c->cfg.pm_grid_nx || cfg->pm_grid_ny != c->cfg.pm_grid_ny ||
+      cfg->pm_grid_nz != c->cfg.pm_grid_nz || cfg->device != c->cfg.device)
+    return chui::fail(*c, CHUI_TREEPM_EINVAL, "PM solver/grid shape mismatch: the mesh is fixed at creation");
+  chui::DeviceGuard guard(c->device);
+  const bool pm_changed = cfg->precision != c->cfg.precision || cfg->assignment_scheme != c->cfg.assignment_scheme ||
+                          cfg->window_deconvolution != c->cfg.window_deconvolution || cfg->box_x != c->cfg.box_x ||
+                          cfg->box_y != c->cfg.box_y || cfg->box_z != c->cfg.box_z ||
+                          cfg->asmth_cells != c->cfg.asmth_cells ||
+                          cfg->gravitational_constant != c->cfg.gravitational_constant;
+  if (pm_changed) {
+    cudaDeviceSynchronize();
+    chui::pmDestroy(*c);
+    c->pm_field_valid = false;
+  }
+  chui::applyConfig(*c, *cfg);
+  return 0;
+}
+
+const char* chui_treepm_last_error(const void* handle) {
+  if (!handle) return "null handle";
+  return static_cast<const Context*>(handle)->last_error.c_str();
+}
+
+int chui_treepm_kdk_factors_static(double dt, double factors[5]) {
+  if (!factors || !(dt > 0.0) || !std::isfinite(dt)) return CHUI_TREEPM_EINVAL;
+  factors[0] = dt;
+  factors[1] = 0.5 * dt;
+  factors[2] = 0.5 * dt;
+  factors[3] = 1.0;
+  factors[4] = 1.0;
+  return 0;
+}
+
+int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_treepm_accumulator* acc,
+                      int refresh_long_range_field, int memory, void* stream, chui_treepm_stats* stats) {
+  if (!handle) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  c.last_error.clear();
+  if (!src || !acc) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources and accumulator are required");
+  if (memory != CHUI_TREEPM_HOST && memory != CHUI_TREEPM_DEVICE)
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "memory must be CHUI_TREEPM_HOST or CHUI_TREEPM_DEVICE");
+  const int64_t n = src->count;
+  const int64_t nt = acc->active_index ? acc->active_count : (acc->target_x ? acc->active_count : n);
+  if (n < 0 || nt < 0) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM requires non-negative extents");
+  if (n > static_cast<int64_t>(0xFFFFFFFEu))
+    return chui::fail(c, CHUI_TREEPM_ERANGE, "Tree gravity source count exceeds the 32-bit tree-index contract");
+  if (n > 0 && (!src->x || !src->y || !src->z))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM requires position and mass spans with equal extent");
+  if (!src->mass && !(std::isfinite(src->uniform_mass) && src->uniform_mass >= 0.0))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources require finite coordinates and finite non-negative masses");
+  const bool explicit_targets = acc->target_x != nullptr;
+  if (explicit_targets && (!acc->target_y || !acc->target_z))
+    return chui::fail(c, CHUI_TREEPM_EINVAL,
+                      "TreePM independent target coordinate triplet must be entirely present or absent");
+  if (!explicit_targets && (acc->target_y || acc->target_z))
+    return chui::fail(c, CHUI_TREEPM_EINVAL,
+                      "TreePM independent target coordinate triplet must be entirely present or absent");
+  if (nt > 0 && (!acc->accel_x || !acc->accel_y || !acc->accel_z))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM force accumulator spans must have matching active-set extent");
+  if (explicit_targets && (acc->short_range_x || acc->nearest_pair_r2))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "Tree component output requires source-indexed full source extents");
+  const bool lr = acc->long_range_x || acc->long_range_y || acc->long_range_z;
+  const bool sr = acc->short_range_x || acc->short_range_y || acc->short_range_z;
+  if ((lr && !(acc->long_range_x && acc->long_range_y && acc->long_range_z)) ||
+      (sr && !(acc->short_range_x && acc->short_range_y && acc->short_range_z)))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM force accumulator spans must have matching active-set extent");
+
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaEventRecord(c.ev[0], s);
+  int rc;
+  const double *x, *y, *z, *m, *tx = nullptr, *ty = nullptr, *tz = nullptr;
+  const uint32_t* active = nullptr;
+  if ((rc = chui::stageIn(c, c.in_x, src->x, n, memory, s, &x)) || (rc = chui::stageIn(c, c.in_y, src->y, n, memory, s, &y)) ||
+      (rc = chui::stageIn(c, c.in_z, src->z, n, memory, s, &z)) ||
+      (rc = chui::stageIn(c, c.in_m, src->mass, src->mass ? n : 0, memory, s, &m)))
+    return rc;
+  if (acc->active_index && (rc = chui::stageIn(c, c.in_active, acc->active_index, nt, memory, s, &active))) return rc;
+  if (explicit_targets &&
+      ((rc = chui::stageIn(c, c.in_tx, acc->target_x, nt, memory, s, &tx)) ||
+       (rc = chui::stageIn(c, c.in_ty, acc->target_y, nt, memory, s, &ty)) ||
+       (rc = chui::stageIn(c, c.in_tz, acc->target_z, nt, memory, s, &tz))))
+    return rc;
+  if (!src->mass) m = nullptr;
+
+  // validateTreePmPreflight (tree_pm_coupling.cpp:244-481)
+  double lo[3], hi[3], mass_sum = 0.0;
+  uint32_t st = 0;
+  if ((rc = chui::sourceBounds(c, n, x, y, z, m, lo, hi, &mass_sum, &st, s))) return rc;
+  if (st) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources require finite coordinates and finite non-negative masses");
+  if (explicit_targets && nt > 0) {
+    double tlo[3], thi[3], dummy;
+    if ((rc = chui::sourceBounds(c, nt, tx, ty, tz, nullptr, tlo, thi, &dummy, &st, s))) return rc;
+    if (st) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM target positions must be finite");
+  }
+  if (active && nt > 0) {
+    cudaMemsetAsync(c.status.ptr, 0, 4, s);
+    chui::activeCheckKernel<<<chui::gridFor(nt, 256), 256, 0, s>>>(nt, active, n, explicit_targets ? 1 : 0,
+                                                                  c.status.as<uint32_t>());
+    cudaMemcpyAsync(&st, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    if (st) {
+      return chui::fail(c, CHUI_TREEPM_ERANGE,
+                        explicit_targets
+                            ? "TreePM explicit target source identity must be local or the invalid local-index sentinel"
+                            : "TreePM active index exceeds particle count");
+    }
+  } else if (!active && !explicit_targets && nt > n) {
+    return chui::fail(c, CHUI_TREEPM_ERANGE, "TreePM active index exceeds particle count");
+  }
+  const double total_mass = m ? mass_sum : static_cast<double>(n) * src->uniform_mass;
+
+  // PM refresh or cached-field reuse (tree_pm_coupling.cpp:2483-2532)
+  if (refresh_long_range_field) {
+    if ((rc = chui::pmRefresh(c, n, x, y, z, m, src->uniform_mass, total_mass, s))) return rc;
+  } else if (!c.pm_field_valid || c.pm_field_box[0] != c.cfg.box_x || c.pm_field_box[1] != c.cfg.box_y ||
+             c.pm_field_box[2] != c.cfg.box_z) {
+    return chui::fail(c, CHUI_TREEPM_ESTATE, "TreePM long-range reuse requested without a compatible PM field");
+  }
+  cudaEventRecord(c.ev[1], s);
+
+  // periodic tree build
+  if ((rc = chui::treeBuild(c, n, x, y, z, m, src->uniform_mass, lo, hi, s))) {
+    if (c.last_error.empty()) c.last_error = "TreePM tree build failed";
+    return rc;
+  }
+  double nlo[3], nhi[3];
+  if ((rc = chui::treeNodeBounds(c, nlo, nhi, s))) return chui::fail(c, rc, "node bounds failed");
+  if ((rc = chui::treeOrderTargets(c, nt, active, explicit_targets ? 1 : 0, n, s)))
+    return chui::fail(c, rc, "target ordering failed");
+  cudaEventRecord(c.ev[2], s);
+
+  // residual walk
+  chui::WalkParams wp;
+  wp.box[0] = c.cfg.box_x;
+  wp.box[1] = c.cfg.box_y;
+  wp.box[2] = c.cfg.box_z;
+  for (int a = 0; a < 3; ++a) {
+    wp.src_lo[a] = lo[a];
+    wp.src_hi[a] = hi[a];
+    wp.node_lo[a] = nlo[a];
+    wp.node_hi[a] = nhi[a];
+  }
+  wp.rs = c.rs;
+  wp.cutoff = c.cutoff;
+  wp.cutoff2 = c.cutoff * c.cutoff;
+  wp.G = c.cfg.gravitational_constant;
+  wp.eps = c.cfg.softening;
+  wp.theta = c.cfg.opening_theta;
+  wp.exact_half = 0.5 * std::min({c.cfg.box_x, c.cfg.box_y, c.cfg.box_z}) - c.cutoff;
+  wp.criterion = c.cfg.opening_criterion;
+  wp.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
+  wp.inv_4rs2_f = static_cast<float>(0.25 / (c.rs * c.rs));
+  wp.inv_8rs3_f = static_cast<float>(0.125 / (c.rs * c.rs * c.rs));
+  wp.cut2_f = static_cast<float>(c.cutoff * c.cutoff);
+  wp.eps2_f = static_cast<float>(c.cfg.softening * c.cfg.softening);
+  wp.G_f = static_cast<float>(c.cfg.gravitational_constant);
+  cudaMemsetAsync(c.status.ptr, 0, 4, s);
+  if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, wp, n, s)))
+    return chui::fail(c, rc, "residual walk launch failed");
+  if (n == 0 && nt > 0) {
+    if (chui::ensure(c.tree_acc, nt * 3 * 8) || chui::ensure(c.tree_near, nt * 8))
+      return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    cudaMemsetAsync(c.tree_acc.ptr, 0, nt * 3 * 8, s);
+    std::vector<double> inf(nt, INFINITY);
+    cudaMemcpyAsync(c.tree_near.ptr, inf.data(), nt * 8, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+  }
+  cudaEventRecord(c.ev[3], s);
+
+  // outputs
+  double *ax, *ay, *az, *pmx, *pmy, *pmz, *sx = nullptr, *sy = nullptr, *sz = nullptr, *snear = nullptr;
+  if (memory == CHUI_TREEPM_DEVICE) {
+    ax = acc->accel_x;
+    ay = acc->accel_y;
+    az = acc->accel_z;
+    sx = acc->short_range_x;
+    sy = acc->short_range_y;
+    sz = acc->short_range_z;
+    snear = acc->nearest_pair_r2;
+  } else {
+    for (int a = 0; a < 3; ++a)
+      if (chui::ensure(c.out_acc[a], std::max<int64_t>(nt, 1) * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    ax = c.out_acc[0].as<double>();
+    ay = c.out_acc[1].as<double>();
+    az = c.out_acc[2].as<double>();
+    if (sr) {
+      for (int a = 0; a < 3; ++a)
+        if (chui::ensure(c.out_tree[a], std::max<int64_t>(n, 1) * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+      sx = c.out_tree[0].as<double>();
+      sy = c.out_tree[1].as<double>();
+      sz = c.out_tree[2].as<double>();
+      cudaMemcpyAsync(sx, acc->short_range_x, n * 8, cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(sy, acc->short_range_y, n * 8, cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(sz, acc->short_range_z, n * 8, cudaMemcpyHostToDevice, s);
+    }
+    if (acc->nearest_pair_r2) {
+      if (chui::ensure(c.out_near, std::max<int64_t>(n, 1) * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+      snear = c.out_near.as<double>();
+      cudaMemcpyAsync(snear, acc->nearest_pair_r2, n * 8, cudaMemcpyHostToDevice, s);
+    }
+  }
+  if (lr && memory == CHUI_TREEPM_DEVICE) {
+    pmx = acc->long_range_x;
+    pmy = acc->long_range_y;
+    pmz = acc->long_range_z;
+  } else {
+    for (int a = 0; a < 3; ++a)
+      if (chui::ensure(c.out_pm[a], std::max<int64_t>(nt, 1) * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    pmx = c.out_pm[0].as<double>();
+    pmy = c.out_pm[1].as<double>();
+    pmz = c.out_pm[2].as<double>();
+  }
+  if ((rc = chui::pmInterpolate(c, nt, active, tx, ty, tz, x, y, z, pmx, pmy, pmz, s))) return rc;
+  if (nt > 0)
+    chui::combineKernel<<<chui::gridFor(nt, 256), 256, 0, s>>>(nt, active, explicit_targets ? 0 : n, pmx, pmy, pmz,
+                                                              c.tree_acc.as<double>(), c.tree_near.as<double>(), ax,
+                                                              ay, az, sx, sy, sz, snear);
+  cudaEventRecord(c.ev[4], s);
+  uint32_t walk_status = 0;
+  cudaMemcpyAsync(&walk_status, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
+  unsigned long long counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (n > 0 && nt > 0) cudaMemcpyAsync(counters, c.walk_counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, s);
+  if (memory == CHUI_TREEPM_HOST && nt > 0) {
+    cudaMemcpyAsync(acc->accel_x, ax, nt * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(acc->accel_y, ay, nt * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(acc->accel_z, az, nt * 8, cudaMemcpyDeviceToHost, s);
+    if (lr) {
+      cudaMemcpyAsync(acc->long_range_x, pmx, nt * 8, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(acc->long_range_y, pmy, nt * 8, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(acc->long_range_z, pmz, nt * 8, cudaMemcpyDeviceToHost, s);
+    }
+    if (sr) {
+      cudaMemcpyAsync(acc->short_range_x, sx, n * 8, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(acc->short_range_y, sy, n * 8, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(acc->short_range_z, sz, n * 8, cudaMemcpyDeviceToHost, s);
+    }
+    if (acc->nearest_pair_r2) cudaMemcpyAsync(acc->nearest_pair_r2, snear, n * 8, cudaMemcpyDeviceToHost, s);
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return chui::fail(c, CHUI_TREEPM_EDEVICE, std::string("CUDA error: ") + cudaGetErrorString(e));
+  if (walk_status) return chui::fail(c, CHUI_TREEPM_ERANGE, chui::statusText(walk_status));
+  chui_treepm_stats stt{};
+  stt.visited_nodes = counters[0];
+  stt.accepted_nodes = counters[1];
+  stt.opened_nodes = counters[2];
+  stt.direct_pair_evaluations = counters[3];
+  stt.cutoff_pruned_nodes = counters[4];
+  stt.cutoff_skipped_pairs = counters[5];
+  stt.accepted_internal_multipoles = counters[6];
+  stt.accepted_leaves = counters[7];
+  stt.node_count = static_cast<uint64_t>(c.n_nodes);
+  stt.maximum_depth = c.max_depth;
+  stt.path_words = static_cast<uint32_t>(c.path_words_used);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
+  stt.pm_ms = ms;
+  cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+  stt.tree_build_ms = ms;
+  cudaEventElapsedTime(&ms, c.ev[2], c.ev[3]);
+  stt.walk_ms = ms;
+  cudaEventElapsedTime(&ms, c.ev[0], c.ev[4]);
+  stt.total_ms = ms;
+  c.last_stats = stt;
+  if (stats) *stats = stt;
+  return 0;
+}
+
+int chui_pm_assign_density(void* handle, const chui_treepm_sources* src, double* density, int memory, void* stream) {
+  if (!handle || !src || !density) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t n = src->count;
+  const double *x, *y, *z, *m;
+  int rc;
+  if ((rc = chui::stageIn(c, c.in_x, src->x, n, memory, s, &x)) || (rc = chui::stageIn(c, c.in_y, src->y, n, memory, s, &y)) ||
+      (rc = chui::stageIn(c, c.in_z, src->z, n, memory, s, &z)) ||
+      (rc = chui::stageIn(c, c.in_m, src->mass, src->mass ? n : 0, memory, s, &m)))
+    return rc;
+  if (!src->mass) m = nullptr;
+  const size_t cells = static_cast<size_t>(c.cfg.pm_grid_nx) * c.cfg.pm_grid_ny * c.cfg.pm_grid_nz;
+  double* rho = density;
+  chui::DevBuf tmp;
+  if (memory == CHUI_TREEPM_HOST) {
+    if (chui::ensure(tmp, cells * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    rho = tmp.as<double>();
+  }
+  rc = chui::pmDensityOnly(c, n, x, y, z, m, src->uniform_mass, rho, s);
+  if (!rc && memory == CHUI_TREEPM_HOST) cudaMemcpyAsync(density, rho, cells * 8, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) rc = CHUI_TREEPM_EDEVICE;
+  chui::release(tmp);
+  return rc;
+}
+
+int chui_pm_cells(void* handle, const chui_treepm_sources* src, int64_t* cells, int memory, void* stream) {
+  if (!handle || !src || !cells) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t n = src->count;
+  const double *x, *y, *z;
+  int rc;
+  if ((rc = chui::stageIn(c, c.in_x, src->x, n, memory, s, &x)) || (rc = chui::stageIn(c, c.in_y, src->y, n, memory, s, &y)) ||
+      (rc = chui::stageIn(c, c.in_z, src->z, n, memory, s, &z)))
+    return rc;
+  int64_t* out = cells;
+  chui::DevBuf tmp;
+  if (memory == CHUI_TREEPM_HOST) {
+    if (chui::ensure(tmp, std::max<int64_t>(n, 1) * 3 * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    out = tmp.as<int64_t>();
+  }
+  rc = chui::pmCells(c, n, x, y, z, out, s);
+  if (!rc && memory == CHUI_TREEPM_HOST && n > 0) cudaMemcpyAsync(cells, out, n * 3 * 8, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) rc = CHUI_TREEPM_EDEVICE;
+  chui::release(tmp);
+  return rc;
+}
+
+int chui_treepm_tree_node_count(const void* handle, int64_t* node_count) {
+  if (!handle || !node_count) return CHUI_TREEPM_EINVAL;
+  *node_count = static_cast<const Context*>(handle)->n_nodes;
+  return 0;
+}
+
+int chui_treepm_dump_tree(void* handle, const chui_treepm_tree_dump* d) {
+  if (!handle || !d) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  chui::DeviceGuard guard(c.device);
+  const int64_t nn = c.n_nodes;
+  if (cudaDeviceSynchronize() != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  // n is the size of the last solve's source set; sorted_index holds n entries
+  const int64_t n = static_cast<int64_t>(c.sorted_index.bytes / 4);
+  (void)n;
+  auto copy = [](void* dst, const void* srcp, size_t bytes) {
+    if (dst && bytes) cudaMemcpy(dst, srcp, bytes, cudaMemcpyDeviceToHost);
+  };
+  std::vector<double> geom(nn * 4), com(nn * 4), quad(nn * 8);
+  std::vector<uint32_t> child(nn * 8);
+  std::vector<uint4> range(nn);
+  copy(geom.data(), c.node_geom.ptr, nn * 32);
+  copy(com.data(), c.node_com.ptr, nn * 32);
+  copy(quad.data(), c.node_quad.ptr, nn * 64);
+  copy(child.data(), c.node_child.ptr, nn * 32);
+  copy(range.data(), c.node_range.ptr, nn * 16);
+  for (int64_t k = 0; k < nn; ++k) {
+    if (d->center_x) d->center_x[k] = geom[4 * k];
+    if (d->center_y) d->center_y[k] = geom[4 * k + 1];
+    if (d->center_z) d->center_z[k] = geom[4 * k + 2];
+    if (d->half_size) d->half_size[k] = geom[4 * k + 3];
+    if (d->com_x) d->com_x[k] = com[4 * k];
+    if (d->com_y) d->com_y[k] = com[4 * k + 1];
+    if (d->com_z) d->com_z[k] = com[4 * k + 2];
+    if (d->mass) d->mass[k] = com[4 * k + 3];
+    double* qs[7] = {d->quad_xx, d->quad_xy, d->quad_xz, d->quad_yy, d->quad_yz, d->quad_zz, d->second_moment_trace};
+    for (int q = 0; q < 7; ++q)
+      if (qs[q]) qs[q][k] = quad[8 * k + q];
+    if (d->child_count) d->child_count[k] = range[k].z;
+    if (d->particle_begin) d->particle_begin[k] = range[k].x;
+    if (d->particle_count) d->particle_count[k] = range[k].y;
+    if (d->child_index)
+      for (int o = 0; o < 8; ++o) d->child_index[8 * k + o] = child[8 * k + o];
+  }
+  return 0;
+}
+
+int chui_treepm_dump_particles(void* handle, int64_t n, double* ux, double* uy, double* uz, uint64_t* morton_sorted,
+                               uint32_t* sorted_index, double anchors[3]) {
+  if (!handle) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  chui::DeviceGuard guard(c.device);
+  if (cudaDeviceSynchronize() != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  if (ux) cudaMemcpy(ux, c.ux.ptr, n * 8, cudaMemcpyDeviceToHost);
+  if (uy) cudaMemcpy(uy, c.uy.ptr, n * 8, cudaMemcpyDeviceToHost);
+  if (uz) cudaMemcpy(uz, c.uz.ptr, n * 8, cudaMemcpyDeviceToHost);
+  if (morton_sorted) cudaMemcpy(morton_sorted, c.morton_sorted.ptr, n * 8, cudaMemcpyDeviceToHost);
+  if (sorted_index) cudaMemcpy(sorted_index, c.sorted_index.ptr, n * 4, cudaMemcpyDeviceToHost);
+  if (anchors)
+    for (int a = 0; a < 3; ++a) anchors[a] = c.tree_anchor[a];
+  return 0;
+}
+
+int chui_treepm_kick(void* handle, int64_t n, double* vx, double* vy, double* vz, const double* ax, const double* ay,
+                     const double* az, double kick_factor, double drag_factor, int memory, void* stream) {
+  if (!handle || n < 0) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  if (n == 0) return 0;
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double *dvx = vx, *dvy = vy, *dvz = vz;
+  const double *dax = ax, *day = ay, *daz = az;
+  if (memory == CHUI_TREEPM_HOST) {
+    if (chui::ensure(c.in_x, n * 8) || chui::ensure(c.in_y, n * 8) || chui::ensure(c.in_z, n * 8) ||
+        chui::ensure(c.out_acc[0], n * 8) || chui::ensure(c.out_acc[1], n * 8) || chui::ensure(c.out_acc[2], n * 8))
+      return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    dvx = c.in_x.as<double>();
+    dvy = c.in_y.as<double>();
+    dvz = c.in_z.as<double>();
+    cudaMemcpyAsync(dvx, vx, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dvy, vy, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dvz, vz, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c.out_acc[0].ptr, ax, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c.out_acc[1].ptr, ay, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c.out_acc[2].ptr, az, n * 8, cudaMemcpyHostToDevice, s);
+    dax = c.out_acc[0].as<double>();
+    day = c.out_acc[1].as<double>();
+    daz = c.out_acc[2].as<double>();
+  }
+  chui::kickKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dvx, dvy, dvz, dax, day, daz, kick_factor, drag_factor);
+  if (memory == CHUI_TREEPM_HOST) {
+    cudaMemcpyAsync(vx, dvx, n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(vy, dvy, n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(vz, dvz, n * 8, cudaMemcpyDeviceToHost, s);
+  }
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "kick failed");
+}
+
+int chui_treepm_drift(void* handle, int64_t n, double* x, double* y, double* z, const double* vx, const double* vy,
+                      const double* vz, double drift_factor, int memory, void* stream) {
+  if (!handle || n < 0) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  if (n == 0) return 0;
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double *dx = x, *dy = y, *dz = z;
+  const double *dvx = vx, *dvy = vy, *dvz = vz;
+  if (memory == CHUI_TREEPM_HOST) {
+    if (chui::ensure(c.in_x, n * 8) || chui::ensure(c.in_y, n * 8) || chui::ensure(c.in_z, n * 8) ||
+        chui::ensure(c.out_acc[0], n * 8) || chui::ensure(c.out_acc[1], n * 8) || chui::ensure(c.out_acc[2], n * 8))
+      return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    dx = c.in_x.as<double>();
+    dy = c.in_y.as<double>();
+    dz = c.in_z.as<double>();
+    cudaMemcpyAsync(dx, x, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dy, y, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dz, z, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c.out_acc[0].ptr, vx, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c.out_acc[1].ptr, vy, n * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c.out_acc[2].ptr, vz, n * 8, cudaMemcpyHostToDevice, s);
+    dvx = c.out_acc[0].as<double>();
+    dvy = c.out_acc[1].as<double>();
+    dvz = c.out_acc[2].as<double>();
+  }
+  chui::driftKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dx, dy, dz, dvx, dvy, dvz, drift_factor, c.cfg.box_x,
+                                                         c.cfg.box_y, c.cfg.box_z);
+  if (memory == CHUI_TREEPM_HOST) {
+    cudaMemcpyAsync(x, dx, n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(y, dy, n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(z, dz, n * 8, cudaMemcpyDeviceToHost, s);
+  }
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "drift failed");
+}
+
+}  // extern "C"

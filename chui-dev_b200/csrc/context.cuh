@@ -1,0 +1,152 @@
+// Internal state of one TreePM solver instance (the object behind the C-ABI
+// handle) and the declarations shared by the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/chui_treepm.h"
+#include "common.cuh"
+
+namespace chui {
+
+// Grow-only device allocation.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+};
+
+cudaError_t ensure(DevBuf& b, size_t bytes);
+void release(DevBuf& b);
+
+// Coefficients of the FP32 Gaussian long-range coefficient H(t) = L(q)/q^3,
+// t = q^2 = r^2/(4 r_s^2), as a polynomial in s = t*scale - 1 on [0, t_cut].
+struct PolyH {
+  int terms = 0;              // degree + 1
+  float scale = 0.f;          // 2 / t_cut
+  float c[kPolyMaxTerms] = {};
+  double max_rel_error = 0.0;
+};
+
+// Per-solve scalar geometry shared with the walk kernel.
+struct WalkParams {
+  double box[3];
+  double src_lo[3], src_hi[3];    // bounds of the caller's source coordinates
+  double node_lo[3], node_hi[3];  // bounds of node centres and COMs
+  double rs, cutoff, cutoff2;
+  double G, eps;
+  double theta;
+  double exact_half;  // leaves with half >= this use the exact FP64 pair path
+  int criterion;   // 0 geometric, 1 COM distance, 2 relative (no history: COM distance)
+  int quadrupole;
+  float inv_4rs2_f;   // 1/(4 r_s^2)
+  float inv_8rs3_f;   // 1/(8 r_s^3)
+  float cut2_f;
+  float eps2_f;
+  float G_f;
+};
+
+struct Context {
+  chui_treepm_config cfg{};
+  int device = 0;
+  double spacing = 0.0, rs = 0.0, cutoff = 0.0;
+  PolyH poly;
+  std::string last_error;
+
+  // PM (cuFFT, in-place padded real layout nx*ny*2*(nz/2+1))
+  bool fft_ready = false;
+  cufftHandle plan_r2c = 0, plan_c2r = 0;
+  DevBuf grid[3];            // grid[0] holds the density then F_x; grid[1], grid[2] F_y, F_z
+  DevBuf axis_tables;        // kx, ky, kz, wx, wy, wz (FP64)
+  bool pm_field_valid = false;
+  double pm_field_box[3] = {0, 0, 0};
+
+  // staged inputs / outputs
+  DevBuf in_x, in_y, in_z, in_m, in_active, in_tx, in_ty, in_tz;
+  DevBuf out_acc[3], out_pm[3], out_tree[3], out_near;
+  DevBuf status;       // uint32 status word + scalar results (reduction scratch)
+  DevBuf scalars;      // reduction outputs (64 x u64)
+  std::vector<unsigned long long> host_scalars;
+
+  // tree construction
+  DevBuf ux, uy, uz;             // unwrapped FP64 coordinates (tree frame)
+  DevBuf bucket_min, bucket_max, bucket_next;
+  DevBuf keys_a, keys_b, idx_a, idx_b, idx_c, idx_d;
+  DevBuf path_words;             // kMaxPathWords * n u64
+  DevBuf common_prefix;          // int8/int32 per sorted position
+  DevBuf node_count_per_pos, node_offset;  // per sorted position (n+1)
+  DevBuf leaf_of_pos, inv_pos;
+  DevBuf cub_temp;
+  int64_t n_nodes = 0;
+  uint32_t max_depth = 0;
+  int path_words_used = 0;
+  double tree_anchor[3] = {0, 0, 0};
+
+  // nodes (SoA, FP64 geometry/moments)
+  DevBuf node_geom;    // double4 {cx, cy, cz, half}
+  DevBuf node_com;     // double4 {comx, comy, comz, mass}
+  DevBuf node_quad;    // 8 doubles per node {qxx, qxy, qxz, qyy, qyz, qzz, trace, com_center_offset}
+  DevBuf node_child;   // 8 u32 per node
+  DevBuf node_range;   // uint4 {begin, count, child_count | leaf flag, subtree_end}
+  DevBuf node_parent;  // u32
+  DevBuf node_depth;   // u32
+  DevBuf node_counter; // u32 (bottom-up completion counters)
+  DevBuf sorted_index; // u32 per tree position: caller row
+  DevBuf pos_of_row;   // u32 per caller row: tree position
+  DevBuf src_f4;       // float4 per tree position: offset from leaf centre (FP32) + mass
+  DevBuf src_d4;       // double4 per tree position: caller position + mass (FP64 path)
+  DevBuf target_order; // visit order of active slots
+  DevBuf morton_sorted;  // sorted Morton keys (diagnostic parity output)
+
+  // walk
+  DevBuf walk_counters;  // 8 x u64
+  DevBuf work_counter;   // u32 dynamic scheduling
+  DevBuf tree_acc;       // double3 per active slot (short-range part)
+  DevBuf tree_near;      // double per active slot
+
+  cudaEvent_t ev[8] = {};
+  bool events_ready = false;
+  chui_treepm_stats last_stats{};
+};
+
+// ---- PM (pm.cu) ----
+int pmPrepare(Context& c);
+int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const double* z,
+              const double* m, double uniform_mass, double total_mass, cudaStream_t s);
+// CIC/TSC interpolation of the cached force grids at targets (active slots).
+int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* tx,
+                  const double* ty, const double* tz, const double* sx, const double* sy,
+                  const double* sz, double* ax, double* ay, double* az, cudaStream_t s);
+int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const double* z,
+                  const double* m, double uniform_mass, double* rho_out, cudaStream_t s);
+int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,
+            int64_t* cells, cudaStream_t s);
+void pmDestroy(Context& c);
+
+// ---- tree (tree.cu) ----
+int treeBuild(Context& c, int64_t n, const double* x, const double* y, const double* z,
+              const double* m, double uniform_mass, const double src_lo[3], const double src_hi[3],
+              cudaStream_t s);
+int treeNodeBounds(Context& c, double lo[3], double hi[3], cudaStream_t s);
+int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explicit_targets, int64_t n,
+                     cudaStream_t s);
+
+// ---- walk (walk.cu) ----
+int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
+            const double* tz, const double* sx, const double* sy, const double* sz,
+            const WalkParams& wp, int64_t n, cudaStream_t s);
+
+// ---- reductions / small kernels (abi.cu) ----
+int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const double* z,
+                 const double* m, double lo[3], double hi[3], double* mass_sum,
+                 uint32_t* status_bits, cudaStream_t s);
+
+const char* statusText(uint32_t bits);
+
+}  // namespace chui

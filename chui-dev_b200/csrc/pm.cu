@@ -1,0 +1,477 @@
+// Particle-mesh long-range force on the B200: periodic CIC/TSC mass assignment,
+// cuFFT real-to-complex transform, one fused k-space pass (Green's function x
+// assignment-window deconvolution x Gaussian split filter x spectral gradient,
+// emitting the three force spectra), three complex-to-real transforms, and
+// CIC/TSC force interpolation.
+//
+// Reference: src/gravity/pm_solver.cpp -- makeAxisStencil :925-951,
+// assignDensityImpl :3842-4565, solvePoissonPeriodicImpl :4581-4940,
+// ensureSpectralAxisMetadata :2398-2466, applyDerivedPoissonOperator
+// :2557-2656, fillGradientSpectrum :2658-2706, interpolateForcesImpl
+// :5735-5953.
+//
+// Layout in HBM: one in-place FFT array per force component, nx*ny*nzp reals
+// (nzp = 2*(nz/2+1), FFTW/cuFFT padded rows). grid[0] carries the density
+// (minus its mean), is transformed in place, and is overwritten by the F_x
+// spectrum; grid[1], grid[2] receive F_y, F_z. Mixed precision keeps the mesh
+// in FP32; the FP64 configuration uses double grids and Z2D/D2Z plans.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <vector>
+
+#include "context.cuh"
+
+namespace chui {
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+struct PmGeom {
+  int64_t n[3];
+  int64_t nzc, nzp;
+  double L[3];
+  double inv_d[3];
+  int scheme;
+};
+
+PmGeom geomOf(const Context& c) {
+  PmGeom g;
+  g.n[0] = c.cfg.pm_grid_nx;
+  g.n[1] = c.cfg.pm_grid_ny;
+  g.n[2] = c.cfg.pm_grid_nz;
+  g.nzc = g.n[2] / 2 + 1;
+  g.nzp = 2 * g.nzc;
+  g.L[0] = c.cfg.box_x;
+  g.L[1] = c.cfg.box_y;
+  g.L[2] = c.cfg.box_z;
+  for (int a = 0; a < 3; ++a) g.inv_d[a] = static_cast<double>(g.n[a]) / g.L[a];
+  g.scheme = c.cfg.assignment_scheme;
+  return g;
+}
+
+// wrapPosition (pm_solver.cpp:112-115): fmod is exact, so cell indices match.
+__device__ __forceinline__ double wrapPosition(double v, double box) {
+  const double w = fmod(v, box);
+  return w < 0.0 ? w + box : w;
+}
+
+__device__ __forceinline__ int64_t wrapIndex(int64_t i, int64_t n) {
+  int64_t w = i % n;
+  return w < 0 ? w + n : w;
+}
+
+struct Stencil {
+  int64_t off0;
+  double w[3];
+};
+
+// makeAxisStencil (pm_solver.cpp:925-951).
+__device__ __forceinline__ Stencil makeStencil(double gp, int scheme) {
+  Stencil s;
+  if (scheme == 0) {
+    const double base = floor(gp);
+    const double t = gp - base;
+    s.off0 = static_cast<int64_t>(base);
+    s.w[0] = 1.0 - t;
+    s.w[1] = t;
+    s.w[2] = 0.0;
+  } else {
+    const double center = floor(gp + 0.5);
+    const double d = gp - center;
+    s.off0 = static_cast<int64_t>(center) - 1;
+    s.w[0] = 0.5 * ((0.5 - d) * (0.5 - d));
+    s.w[1] = 0.75 - d * d;
+    s.w[2] = 0.5 * ((0.5 + d) * (0.5 + d));
+  }
+  return s;
+}
+
+template <class R>
+__global__ void fillKernel(R* grid, size_t count, R value) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    grid[i] = value;
+  }
+}
+
+// Mass assignment: one thread per particle, `taps`^3 atomic adds into the FP32
+// (or FP64) padded grid; the 1/cell_volume normalization is folded into the
+// per-particle mass.
+template <class R>
+__global__ void depositKernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                              const double* __restrict__ z, const double* __restrict__ m,
+                              double uniform_mass, double inv_cell_volume, PmGeom g, R* grid) {
+  const int taps = g.scheme == 0 ? 2 : 3;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const Stencil sx = makeStencil(wrapPosition(x[i], g.L[0]) * g.inv_d[0], g.scheme);
+    const Stencil sy = makeStencil(wrapPosition(y[i], g.L[1]) * g.inv_d[1], g.scheme);
+    const Stencil sz = makeStencil(wrapPosition(z[i], g.L[2]) * g.inv_d[2], g.scheme);
+    const double mass = (m ? m[i] : uniform_mass) * inv_cell_volume;
+    for (int a = 0; a < taps; ++a) {
+      const int64_t ix = wrapIndex(sx.off0 + a, g.n[0]);
+      for (int b = 0; b < taps; ++b) {
+        const int64_t iy = wrapIndex(sy.off0 + b, g.n[1]);
+        const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
+        const double wxy = sx.w[a] * sy.w[b];
+        for (int cc = 0; cc < taps; ++cc) {
+          const int64_t iz = wrapIndex(sz.off0 + cc, g.n[2]);
+          atomicAdd(grid + row + iz, static_cast<R>(mass * (wxy * sz.w[cc])));
+        }
+      }
+    }
+  }
+}
+
+// Same assignment into a compact FP64 grid (diagnostic density output).
+__global__ void depositCompactKernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                     const double* __restrict__ z, const double* __restrict__ m,
+                                     double uniform_mass, PmGeom g, double* grid) {
+  const int taps = g.scheme == 0 ? 2 : 3;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const Stencil sx = makeStencil(wrapPosition(x[i], g.L[0]) * g.inv_d[0], g.scheme);
+    const Stencil sy = makeStencil(wrapPosition(y[i], g.L[1]) * g.inv_d[1], g.scheme);
+    const Stencil sz = makeStencil(wrapPosition(z[i], g.L[2]) * g.inv_d[2], g.scheme);
+    const double mass = m ? m[i] : uniform_mass;
+    for (int a = 0; a < taps; ++a) {
+      const int64_t ix = wrapIndex(sx.off0 + a, g.n[0]);
+      for (int b = 0; b < taps; ++b) {
+        const int64_t iy = wrapIndex(sy.off0 + b, g.n[1]);
+        for (int cc = 0; cc < taps; ++cc) {
+          const int64_t iz = wrapIndex(sz.off0 + cc, g.n[2]);
+          const double w = sx.w[a] * sy.w[b] * sz.w[cc];
+          atomicAdd(grid + (static_cast<size_t>(ix) * g.n[1] + iy) * g.n[2] + iz, mass * w);
+        }
+      }
+    }
+  }
+}
+
+__global__ void scaleKernel(double* v, size_t count, double factor) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    v[i] /= factor;
+  }
+}
+
+__global__ void cellsKernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, PmGeom g, int64_t* cells) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double p[3] = {x[i], y[i], z[i]};
+    for (int a = 0; a < 3; ++a) {
+      const Stencil s = makeStencil(wrapPosition(p[a], g.L[a]) * g.inv_d[a], g.scheme);
+      cells[3 * i + a] = wrapIndex(s.off0, g.n[a]);
+    }
+  }
+}
+
+// Fused k-space pass over the half spectrum: Psi = G(k) rho_k with
+// G = -4 pi G_N W(k)^-2 exp(-(|k| r_s)^2) / k^2 / M (k = 0 -> 0), then
+// F_a = -i g_a Psi with g_a = k_a except the Nyquist index of an even axis.
+// Reads rho_k once and writes three spectra (F_x in place).
+template <class R, class C>
+__global__ void greenGradientKernel(PmGeom g, const double* __restrict__ tab, double prefactor,
+                                    double rs, int deconv, C* c0, C* c1, C* c2) {
+  const int64_t nx = g.n[0], ny = g.n[1], nzc = g.nzc;
+  const double* kx = tab;
+  const double* ky = kx + nx;
+  const double* kz = ky + ny;
+  const double* wx = kz + nzc;
+  const double* wy = wx + nx;
+  const double* wz = wy + ny;
+  const double* gx = wz + nzc;
+  const double* gy = gx + nx;
+  const double* gz = gy + ny;
+  const size_t total = static_cast<size_t>(nx) * ny * nzc;
+  for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int64_t iz = static_cast<int64_t>(idx % nzc);
+    const size_t row = idx / nzc;
+    const int64_t iy = static_cast<int64_t>(row % ny);
+    const int64_t ix = static_cast<int64_t>(row / ny);
+    const double k2 = kx[ix] * kx[ix] + ky[iy] * ky[iy] + kz[iz] * kz[iz];
+    double op = 0.0;
+    if (k2 != 0.0) {
+      double window = 1.0;
+      if (deconv) {
+        const double tw = wx[ix] * wy[iy] * wz[iz];
+        const double w2 = tw * tw;
+        window = 1.0 / (w2 > 1.0e-12 ? w2 : 1.0e-12);
+      }
+      const double prod = sqrt(k2) * rs;
+      op = prefactor * window * exp(-(prod * prod)) / k2;
+    }
+    const C rho = c0[idx];
+    const R re = static_cast<R>(op) * rho.x;
+    const R im = static_cast<R>(op) * rho.y;
+    const R ga = static_cast<R>(gx[ix]);
+    const R gb = static_cast<R>(gy[iy]);
+    const R gc = static_cast<R>(gz[iz]);
+    C fx, fy, fz;
+    fx.x = ga * im;
+    fx.y = -ga * re;
+    fy.x = gb * im;
+    fy.y = -gb * re;
+    fz.x = gc * im;
+    fz.y = -gc * re;
+    c0[idx] = fx;
+    c1[idx] = fy;
+    c2[idx] = fz;
+  }
+}
+
+// Force interpolation at targets: taps^3 gathers from the three padded
+// force grids. Targets are active slots (rows of the source arrays) or
+// explicit positions.
+template <class R>
+__global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ active,
+                                  const double* __restrict__ tx, const double* __restrict__ ty,
+                                  const double* __restrict__ tz, const double* __restrict__ sx,
+                                  const double* __restrict__ sy, const double* __restrict__ sz,
+                                  PmGeom g, const R* __restrict__ fxg, const R* __restrict__ fyg,
+                                  const R* __restrict__ fzg, double* ax, double* ay, double* az) {
+  const int taps = g.scheme == 0 ? 2 : 3;
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nt;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double px, py, pz;
+    if (tx) {
+      px = tx[k];
+      py = ty[k];
+      pz = tz[k];
+    } else {
+      const int64_t row = active ? static_cast<int64_t>(active[k]) : k;
+      px = sx[row];
+      py = sy[row];
+      pz = sz[row];
+    }
+    const Stencil s0 = makeStencil(wrapPosition(px, g.L[0]) * g.inv_d[0], g.scheme);
+    const Stencil s1 = makeStencil(wrapPosition(py, g.L[1]) * g.inv_d[1], g.scheme);
+    const Stencil s2 = makeStencil(wrapPosition(pz, g.L[2]) * g.inv_d[2], g.scheme);
+    R gx = 0, gy = 0, gz = 0;
+    for (int a = 0; a < taps; ++a) {
+      const int64_t ix = wrapIndex(s0.off0 + a, g.n[0]);
+      for (int b = 0; b < taps; ++b) {
+        const int64_t iy = wrapIndex(s1.off0 + b, g.n[1]);
+        const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
+        const R wab = static_cast<R>(s0.w[a] * s1.w[b]);
+        for (int cc = 0; cc < taps; ++cc) {
+          const int64_t iz = wrapIndex(s2.off0 + cc, g.n[2]);
+          const R w = wab * static_cast<R>(s2.w[cc]);
+          gx += w * fxg[row + iz];
+          gy += w * fyg[row + iz];
+          gz += w * fzg[row + iz];
+        }
+      }
+    }
+    ax[k] = static_cast<double>(gx);
+    ay[k] = static_cast<double>(gy);
+    az[k] = static_cast<double>(gz);
+  }
+}
+
+inline unsigned gridFor(size_t n, int block) {
+  size_t b = (n + block - 1) / block;
+  if (b > 148u * 32u) b = 148u * 32u;
+  return static_cast<unsigned>(b ? b : 1);
+}
+
+inline double sincHost(double v) {
+  // pm_solver.cpp:121-126
+  if (std::fabs(v) < 1.0e-12) return 1.0;
+  return std::sin(v) / v;
+}
+
+bool isMixed(const Context& c) { return c.cfg.precision == CHUI_TREEPM_MIXED; }
+
+}  // namespace
+
+int pmPrepare(Context& c) {
+  if (c.fft_ready) return 0;
+  const PmGeom g = geomOf(c);
+  const bool mixed = isMixed(c);
+  const size_t elem = mixed ? sizeof(float) : sizeof(double);
+  const size_t padded = static_cast<size_t>(g.n[0]) * g.n[1] * g.nzp;
+  for (auto& b : c.grid) {
+    if (ensure(b, padded * elem) != cudaSuccess) {
+      c.last_error = "PM mesh allocation failed";
+      return CHUI_TREEPM_ENOMEM;
+    }
+  }
+  const int nx = static_cast<int>(g.n[0]), ny = static_cast<int>(g.n[1]), nz = static_cast<int>(g.n[2]);
+  if (cufftPlan3d(&c.plan_r2c, nx, ny, nz, mixed ? CUFFT_R2C : CUFFT_D2Z) != CUFFT_SUCCESS ||
+      cufftPlan3d(&c.plan_c2r, nx, ny, nz, mixed ? CUFFT_C2R : CUFFT_Z2D) != CUFFT_SUCCESS) {
+    c.last_error = "cuFFT plan creation failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  // Axis metadata (ensureSpectralAxisMetadata, pm_solver.cpp:2398-2466) plus
+  // the gradient wave numbers with the even-axis Nyquist zeroed (:2679-2705).
+  std::vector<double> tab;
+  const int expo = c.cfg.assignment_scheme == CHUI_TREEPM_CIC ? 2 : 3;
+  std::vector<double> k[3], w[3], gk[3];
+  for (int a = 0; a < 3; ++a) {
+    const int64_t count = a == 2 ? g.nzc : g.n[a];
+    const double dk = 2.0 * kPi / g.L[a];
+    for (int64_t i = 0; i < count; ++i) {
+      const int64_t mode = (a == 2) ? i : (i <= g.n[a] / 2 ? i : i - g.n[a]);
+      const double kk = dk * static_cast<double>(mode);
+      k[a].push_back(kk);
+      w[a].push_back(c.cfg.window_deconvolution
+                         ? std::pow(sincHost(0.5 * kk * g.L[a] / static_cast<double>(g.n[a])),
+                                    static_cast<double>(expo))
+                         : 1.0);
+      gk[a].push_back((g.n[a] % 2 == 0 && i == g.n[a] / 2) ? 0.0 : kk);
+    }
+  }
+  for (int a = 0; a < 3; ++a) tab.insert(tab.end(), k[a].begin(), k[a].end());
+  for (int a = 0; a < 3; ++a) tab.insert(tab.end(), w[a].begin(), w[a].end());
+  for (int a = 0; a < 3; ++a) tab.insert(tab.end(), gk[a].begin(), gk[a].end());
+  if (ensure(c.axis_tables, tab.size() * sizeof(double)) != cudaSuccess ||
+      cudaMemcpy(c.axis_tables.ptr, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice) !=
+          cudaSuccess) {
+    c.last_error = "PM axis table upload failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  c.fft_ready = true;
+  return 0;
+}
+
+void pmDestroy(Context& c) {
+  if (c.plan_r2c) cufftDestroy(c.plan_r2c);
+  if (c.plan_c2r) cufftDestroy(c.plan_c2r);
+  c.plan_r2c = c.plan_c2r = 0;
+  c.fft_ready = false;
+  for (auto& b : c.grid) release(b);
+  release(c.axis_tables);
+}
+
+int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const double* z,
+              const double* m, double uniform_mass, double total_mass, cudaStream_t s) {
+  int rc = pmPrepare(c);
+  if (rc) return rc;
+  const PmGeom g = geomOf(c);
+  const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
+  const size_t padded = static_cast<size_t>(g.n[0]) * g.n[1] * g.nzp;
+  const double volume = g.L[0] * g.L[1] * g.L[2];
+  const double cell_volume = volume / static_cast<double>(cells);
+  // Mean subtraction (pm_solver.cpp:4676-4707) folded into the fill value:
+  // the mean density is total mass / box volume, which the deposit conserves.
+  const double mean = total_mass / volume;
+  const bool mixed = isMixed(c);
+  const int block = 256;
+  if (mixed) {
+    fillKernel<float><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<float>(), padded,
+                                                               static_cast<float>(-mean));
+    if (n > 0)
+      depositKernel<float><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
+                                                               1.0 / cell_volume, g, c.grid[0].as<float>());
+  } else {
+    fillKernel<double><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<double>(), padded, -mean);
+    if (n > 0)
+      depositKernel<double><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
+                                                                1.0 / cell_volume, g, c.grid[0].as<double>());
+  }
+  cufftSetStream(c.plan_r2c, s);
+  cufftSetStream(c.plan_c2r, s);
+  const double prefactor = -4.0 * kPi * c.cfg.gravitational_constant / static_cast<double>(cells);
+  const size_t total = static_cast<size_t>(g.n[0]) * g.n[1] * g.nzc;
+  cufftResult fr;
+  if (mixed) {
+    fr = cufftExecR2C(c.plan_r2c, c.grid[0].as<cufftReal>(), c.grid[0].as<cufftComplex>());
+    if (fr != CUFFT_SUCCESS) {
+      c.last_error = "cuFFT R2C failed";
+      return CHUI_TREEPM_EDEVICE;
+    }
+    greenGradientKernel<float, cufftComplex><<<gridFor(total, block), block, 0, s>>>(
+        g, c.axis_tables.as<double>(), prefactor, c.rs, c.cfg.window_deconvolution,
+        c.grid[0].as<cufftComplex>(), c.grid[1].as<cufftComplex>(), c.grid[2].as<cufftComplex>());
+    for (int a = 0; a < 3; ++a) {
+      fr = cufftExecC2R(c.plan_c2r, c.grid[a].as<cufftComplex>(), c.grid[a].as<cufftReal>());
+      if (fr != CUFFT_SUCCESS) {
+        c.last_error = "cuFFT C2R failed";
+        return CHUI_TREEPM_EDEVICE;
+      }
+    }
+  } else {
+    fr = cufftExecD2Z(c.plan_r2c, c.grid[0].as<cufftDoubleReal>(), c.grid[0].as<cufftDoubleComplex>());
+    if (fr != CUFFT_SUCCESS) {
+      c.last_error = "cuFFT D2Z failed";
+      return CHUI_TREEPM_EDEVICE;
+    }
+    greenGradientKernel<double, cufftDoubleComplex><<<gridFor(total, block), block, 0, s>>>(
+        g, c.axis_tables.as<double>(), prefactor, c.rs, c.cfg.window_deconvolution,
+        c.grid[0].as<cufftDoubleComplex>(), c.grid[1].as<cufftDoubleComplex>(),
+        c.grid[2].as<cufftDoubleComplex>());
+    for (int a = 0; a < 3; ++a) {
+      fr = cufftExecZ2D(c.plan_c2r, c.grid[a].as<cufftDoubleComplex>(), c.grid[a].as<cufftDoubleReal>());
+      if (fr != CUFFT_SUCCESS) {
+        c.last_error = "cuFFT Z2D failed";
+        return CHUI_TREEPM_EDEVICE;
+      }
+    }
+  }
+  if (cudaGetLastError() != cudaSuccess) {
+    c.last_error = "PM kernel launch failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  c.pm_field_valid = true;
+  c.pm_field_box[0] = g.L[0];
+  c.pm_field_box[1] = g.L[1];
+  c.pm_field_box[2] = g.L[2];
+  return 0;
+}
+
+int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* tx,
+                  const double* ty, const double* tz, const double* sx, const double* sy,
+                  const double* sz, double* ax, double* ay, double* az, cudaStream_t s) {
+  if (nt == 0) return 0;
+  const PmGeom g = geomOf(c);
+  const int block = 256;
+  if (isMixed(c)) {
+    interpolateKernel<float><<<gridFor(nt, block), block, 0, s>>>(
+        nt, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<float>(), c.grid[1].as<float>(),
+        c.grid[2].as<float>(), ax, ay, az);
+  } else {
+    interpolateKernel<double><<<gridFor(nt, block), block, 0, s>>>(
+        nt, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<double>(), c.grid[1].as<double>(),
+        c.grid[2].as<double>(), ax, ay, az);
+  }
+  if (cudaGetLastError() != cudaSuccess) {
+    c.last_error = "PM interpolation launch failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  return 0;
+}
+
+int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const double* z,
+                  const double* m, double uniform_mass, double* rho, cudaStream_t s) {
+  const PmGeom g = geomOf(c);
+  const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
+  const int block = 256;
+  if (cudaMemsetAsync(rho, 0, cells * sizeof(double), s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  if (n > 0)
+    depositCompactKernel<<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass, g, rho);
+  const double cell_volume = (g.L[0] * g.L[1] * g.L[2]) / static_cast<double>(cells);
+  scaleKernel<<<gridFor(cells, block), block, 0, s>>>(rho, cells, cell_volume);
+  if (cudaGetLastError() != cudaSuccess) {
+    c.last_error = "PM density launch failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  return 0;
+}
+
+int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,
+            int64_t* cells, cudaStream_t s) {
+  const PmGeom g = geomOf(c);
+  if (n > 0) cellsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, x, y, z, g, cells);
+  if (cudaGetLastError() != cudaSuccess) {
+    c.last_error = "PM cell launch failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  return 0;
+}
+
+}  // namespace chui

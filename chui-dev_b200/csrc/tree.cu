@@ -1,0 +1,957 @@
+// Octree construction on the B200, bit-exact with the reference's recursive
+// FP64 octant partition.
+//
+// Reference: periodic unwrap tree_pm_coupling.cpp:94-218; Morton ordering
+// tree_ordering.cpp:13-171; TreeGravitySolver::build tree_gravity.cpp:343-524,
+// buildNodeRecursive :1081-1206 (octantForParticle :50-61), accumulateMultipoles
+// :1208-1380.
+//
+// The reference builds the octree recursively: starting from Morton order it
+// stably partitions each node's particles by (x >= cx, y >= cy, z >= cz)
+// against FP64 centres obtained by repeated centre +- half/2, stopping at
+// count <= leaf or half <= 1e-12. The same tree is produced here in parallel:
+//  1. unwrap each axis (largest circular gap, found with a 2N-bucket max-gap
+//     pass instead of a sort: the largest gap always exceeds a bucket width);
+//  2. Morton keys + stable radix sort (the reference's within-leaf order);
+//  3. per particle, the geometric octant path (3 bits/level, 21 levels per
+//     64-bit word) by the same FP64 centre recurrence; stable sort by path;
+//  4. nodes = maximal runs of equal path prefix whose parent run has more
+//     than `leaf` particles; they are enumerated in preorder directly from the
+//     common-prefix lengths of neighbouring sorted paths;
+//  5. stable sort of Morton order by leaf id gives the final particle order;
+//  6. FP64 multipoles bottom-up, each parent reduced once, children in octant
+//     order, by the last child to finish.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "context.cuh"
+
+namespace chui {
+namespace {
+
+inline unsigned gridFor(size_t n, int block) {
+  size_t b = (n + block - 1) / block;
+  if (b > 148u * 64u) b = 148u * 64u;
+  return static_cast<unsigned>(b ? b : 1);
+}
+
+__device__ __forceinline__ unsigned long long dbits(double v) {
+  return static_cast<unsigned long long>(__double_as_longlong(v));
+}
+__device__ __forceinline__ double bitsd(unsigned long long b) {
+  return __longlong_as_double(static_cast<long long>(b));
+}
+
+// ---------------------------------------------------------------- unwrap
+
+// Canonical wrap of unwrapPeriodicAxis (tree_pm_coupling.cpp:166-183), then
+// bucket min/max of the non-negative IEEE bits (buckets stored reversed so a
+// forward exclusive min-scan yields "smallest value in any later bucket").
+__global__ void wrapBucketKernel(int64_t n, const double* __restrict__ in, double box, int canonical,
+                                 double* out, unsigned long long nb, double bucket_scale,
+                                 unsigned long long* bmin_rev, unsigned long long* bmax) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double v = canonical ? in[i] : in[i] - box * floor(in[i] / box);
+    if (v >= box) {
+      v = 0.0;
+    } else if (v < 0.0) {
+      v += box;
+    }
+    if (v == 0.0) v = 0.0;
+    out[i] = v;
+    unsigned long long b = static_cast<unsigned long long>(v * bucket_scale);
+    if (b >= nb) b = nb - 1;
+    const unsigned long long bits = dbits(v);
+    atomicMin(bmin_rev + (nb - 1 - b), bits);
+    atomicMax(bmax + b, bits);
+  }
+}
+
+// Largest circular gap over occupied buckets: gap = next - current with the
+// wrap-around next = first + L (tree_pm_coupling.cpp:189-207).
+__global__ void bucketGapKernel(unsigned long long nb, const unsigned long long* __restrict__ bmin_rev,
+                                const unsigned long long* __restrict__ bmax,
+                                const unsigned long long* __restrict__ later_min_rev, double box,
+                                unsigned long long global_min, unsigned long long* best_gap,
+                                int pass, unsigned long long* best_anchor) {
+  for (unsigned long long b = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
+       b < nb; b += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const unsigned long long rb = nb - 1 - b;
+    if (bmin_rev[rb] == ~0ull) continue;
+    const double cur = bitsd(bmax[b]);
+    const unsigned long long later = later_min_rev[rb];
+    double cand, next;
+    if (later == ~0ull) {
+      cand = bitsd(global_min);
+      next = cand + box;
+    } else {
+      cand = bitsd(later);
+      next = cand;
+    }
+    const double gap = next - cur;
+    if (pass == 0) {
+      atomicMax(best_gap, dbits(gap));
+    } else if (dbits(gap) == *best_gap) {
+      atomicMin(best_anchor, dbits(cand));
+    }
+  }
+}
+
+__global__ void applyAnchorKernel(int64_t n, double* u, double box, const unsigned long long* anchor_bits) {
+  const double anchor = bitsd(*anchor_bits);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (u[i] < anchor) u[i] += box;
+  }
+}
+
+struct MinU64 {
+  __device__ __forceinline__ unsigned long long operator()(unsigned long long a, unsigned long long b) const {
+    return a < b ? a : b;
+  }
+};
+
+// ------------------------------------------------------------- bounds
+
+__global__ void boundsKernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                             const double* __restrict__ z, unsigned long long* out /* 6 */) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double p[3] = {x[i], y[i], z[i]};
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = fmin(lo[a], p[a]);
+      hi[a] = fmax(hi[a], p[a]);
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+      hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(out + a, orderedBits(lo[a]));
+      atomicMax(out + 3 + a, orderedBits(hi[a]));
+    }
+  }
+}
+
+// ------------------------------------------------------------- Morton
+
+// expandBits21 / morton3D (tree_ordering.cpp:73-85).
+__device__ __forceinline__ unsigned long long spread21(unsigned v) {
+  unsigned long long x = v & 0x1FFFFFu;
+  x = (x | (x << 32)) & 0x1F00000000FFFFull;
+  x = (x | (x << 16)) & 0x1F0000FF0000FFull;
+  x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+  x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+  x = (x | (x << 2)) & 0x1249249249249249ull;
+  return x;
+}
+
+// std::llround for a finite value in [0, 2^21): round half away from zero.
+__device__ __forceinline__ unsigned roundHalfAway(double v) {
+  const double t = trunc(v);
+  const double frac = __dsub_rn(v, t);
+  return static_cast<unsigned>(t) + (frac >= 0.5 ? 1u : 0u);
+}
+
+// buildMortonOrderingInPlace (tree_ordering.cpp:152-168).
+__global__ void mortonKernel(int64_t n, const double* __restrict__ ux, const double* __restrict__ uy,
+                             const double* __restrict__ uz, double lo0, double lo1, double lo2,
+                             double extent, unsigned long long* keys, uint32_t* idx) {
+  const double grid = static_cast<double>((1u << 21) - 1u);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v[3] = {__ddiv_rn(__dsub_rn(ux[i], lo0), extent), __ddiv_rn(__dsub_rn(uy[i], lo1), extent),
+                         __ddiv_rn(__dsub_rn(uz[i], lo2), extent)};
+    unsigned q[3];
+    for (int a = 0; a < 3; ++a) {
+      const double c = v[a] < 0.0 ? 0.0 : (v[a] > 1.0 ? 1.0 : v[a]);
+      q[a] = roundHalfAway(__dmul_rn(c, grid));
+    }
+    keys[i] = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+    idx[i] = static_cast<uint32_t>(i);
+  }
+}
+
+// ------------------------------------------------------------ paths
+
+// Octant path of each particle (in Morton order) by the reference's centre
+// recurrence: digit d compares against the level-(d-1) centre, then
+// centre += +-half/2 (tree_gravity.cpp:50-61, :1181-1185). Word w holds levels
+// 21w+1 .. 21w+21, level 1 in the top digit.
+__global__ void pathKernel(int64_t n, int words, const uint32_t* __restrict__ perm,
+                           const double* __restrict__ ux, const double* __restrict__ uy,
+                           const double* __restrict__ uz, double cx0, double cy0, double cz0,
+                           double half0, unsigned long long* path /* words * n */) {
+  for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t p = perm[j];
+    const double px = ux[p], py = uy[p], pz = uz[p];
+    double cx = cx0, cy = cy0, cz = cz0, h = half0;
+    for (int w = 0; w < words; ++w) {
+      unsigned long long word = 0;
+      for (int k = 0; k < kLevelsPerWord; ++k) {
+        const unsigned o = (px >= cx ? 4u : 0u) | (py >= cy ? 2u : 0u) | (pz >= cz ? 1u : 0u);
+        word = (word << 3) | o;
+        const double ch = 0.5 * h;
+        cx = __dadd_rn(cx, (o & 4u) ? ch : -ch);
+        cy = __dadd_rn(cy, (o & 2u) ? ch : -ch);
+        cz = __dadd_rn(cz, (o & 1u) ? ch : -ch);
+        h = ch;
+      }
+      path[static_cast<size_t>(w) * n + j] = word;
+    }
+  }
+}
+
+__global__ void gatherU64Kernel(int64_t n, const unsigned long long* __restrict__ src,
+                                const uint32_t* __restrict__ idx, unsigned long long* dst) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    dst[i] = src[idx[i]];
+  }
+}
+
+__device__ __forceinline__ unsigned digitAt(const unsigned long long* path, int64_t n, int64_t i, int level) {
+  // level >= 1
+  const int w = (level - 1) / kLevelsPerWord;
+  const int k = (level - 1) % kLevelsPerWord;
+  return static_cast<unsigned>((path[static_cast<size_t>(w) * n + i] >> (3 * (kLevelsPerWord - 1 - k))) & 7ull);
+}
+
+// Number of leading equal digits of the paths at sorted positions i-1, i.
+__global__ void commonPrefixKernel(int64_t n, int words, const unsigned long long* __restrict__ path,
+                                   int* cp) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (i == 0) {
+      cp[0] = -1;
+      continue;
+    }
+    int c = kLevelsPerWord * words;
+    for (int w = 0; w < words; ++w) {
+      const unsigned long long x = path[static_cast<size_t>(w) * n + i - 1] ^ path[static_cast<size_t>(w) * n + i];
+      if (x != 0) {
+        c = kLevelsPerWord * w + (__clzll(static_cast<long long>(x)) - 1) / 3;
+        break;
+      }
+    }
+    cp[i] = c;
+  }
+}
+
+struct NodePlan {
+  int64_t n;
+  int leaf;        // max_leaf_size
+  int depth_half;  // first depth whose half size <= 1e-12
+  int depth_max;   // resolvable depth = 21 * words
+};
+
+// Leaf depth of the chain of nodes started at sorted position i, or -1 when i
+// starts no node. A node (d, i) exists when its parent run is internal
+// (size > leaf and half > 1e-12, tree_gravity.cpp:1136); it is a leaf when
+// its own run has at most `leaf` particles or d reaches depth_half.
+__device__ int chainLeafDepth(const NodePlan& p, const int* __restrict__ cp, int64_t i, uint32_t* status) {
+  const int ci = cp[i];
+  const int64_t n = p.n;
+  if (ci >= p.depth_max) return -1;  // identical to the previous path through all resolved levels
+  if (i > 0) {
+    // parent run at level ci containing i-1 and i
+    if (ci >= p.depth_half) return -1;
+    int64_t s = -1, r = -1;
+    for (int64_t k = i - 1; k >= 0 && k >= i - p.leaf; --k) {
+      if (cp[k] < ci) {
+        s = k;
+        break;
+      }
+    }
+    for (int64_t k = i + 1; k < n && k <= i + p.leaf; ++k) {
+      if (cp[k] < ci) {
+        r = k;
+        break;
+      }
+    }
+    if (r < 0 && i + p.leaf >= n) r = n;
+    if (s >= 0 && r >= 0 && r - s <= p.leaf) return -1;  // parent is a leaf
+  }
+  int m = -1;  // min common prefix in the forward window; -1 when the array ends inside it
+  if (i + p.leaf < n) {
+    m = 1 << 30;
+    for (int64_t k = i + 1; k <= i + p.leaf; ++k) m = min(m, cp[k]);
+  }
+  int l = max(ci + 1, min(m + 1, p.depth_half));
+  if (l > p.depth_max) {
+    atomicOr(status, kStatusNeedMorePathWords);
+    l = p.depth_max;
+  }
+  if (l > kMaxDepth) atomicOr(status, kStatusDepthExceeded);
+  return l;
+}
+
+__global__ void nodeCountKernel(NodePlan p, const int* __restrict__ cp, uint32_t* counts, uint32_t* status) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i <= p.n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (i == p.n) {
+      counts[i] = 0;
+      continue;
+    }
+    const int l = chainLeafDepth(p, cp, i, status);
+    counts[i] = l < 0 ? 0u : static_cast<uint32_t>(l - cp[i]);
+  }
+}
+
+// First sorted position > i whose path differs from path[i] within `d` levels.
+__device__ int64_t runEnd(const unsigned long long* __restrict__ path, int64_t n, int words,
+                          const int* __restrict__ cp, int64_t i, int d, int leaf) {
+  for (int64_t k = i + 1; k < n && k <= i + leaf; ++k) {
+    if (cp[k] < d) return k;
+  }
+  if (i + leaf + 1 >= n) return n;
+  // binary search on the sorted paths for the end of the d-digit prefix
+  int64_t lo = i + leaf, hi = n;  // cp[...] >= d through lo
+  while (hi - lo > 1) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    // prefix equal through d digits <=> common prefix of (i, mid) >= d
+    int common = kLevelsPerWord * words;
+    for (int w = 0; w < words; ++w) {
+      const unsigned long long x = path[static_cast<size_t>(w) * n + i] ^ path[static_cast<size_t>(w) * n + mid];
+      if (x != 0) {
+        common = kLevelsPerWord * w + (__clzll(static_cast<long long>(x)) - 1) / 3;
+        break;
+      }
+    }
+    if (common >= d) lo = mid;
+    else hi = mid;
+  }
+  return hi;
+}
+
+// First sorted position <= i whose d-digit prefix equals path[i]'s.
+__device__ int64_t runStart(const unsigned long long* __restrict__ path, int64_t n, int words,
+                            const int* __restrict__ cp, int64_t i, int d) {
+  int64_t k = i;
+  for (int step = 0; step < 64 && k > 0; ++step) {
+    if (cp[k] < d) return k;
+    --k;
+  }
+  if (k == 0) return 0;
+  int64_t lo = -1, hi = k;  // answer in (lo, hi]
+  while (hi - lo > 1) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    int common = kLevelsPerWord * words;
+    for (int w = 0; w < words; ++w) {
+      const unsigned long long x = path[static_cast<size_t>(w) * n + i] ^ path[static_cast<size_t>(w) * n + mid];
+      if (x != 0) {
+        common = kLevelsPerWord * w + (__clzll(static_cast<long long>(x)) - 1) / 3;
+        break;
+      }
+    }
+    if (common >= d) hi = mid;
+    else lo = mid;
+  }
+  return hi;
+}
+
+struct NodeOut {
+  double4* geom;
+  uint4* range;      // begin, count, child_count (filled later), subtree_end
+  uint32_t* parent;
+  uint32_t* depth;
+  uint32_t* child;   // 8 per node
+  uint32_t* leaf_of_pos;
+};
+
+// Emit the chain of nodes started at each sorted position, in preorder.
+__global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* __restrict__ path,
+                               const int* __restrict__ cp, const uint32_t* __restrict__ counts,
+                               const uint32_t* __restrict__ offset, double cx0, double cy0, double cz0,
+                               double half0, NodeOut out) {
+  const int64_t n = p.n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t cnt = counts[i];
+    if (cnt == 0) continue;
+    const int ci = cp[i];
+    const int d0 = ci + 1;
+    const int l = d0 + static_cast<int>(cnt) - 1;
+    // replay the centre recurrence down to depth d0 - 1
+    double cx = cx0, cy = cy0, cz = cz0, h = half0;
+    for (int d = 1; d < d0; ++d) {
+      const unsigned o = digitAt(path, n, i, d);
+      const double ch = 0.5 * h;
+      cx = __dadd_rn(cx, (o & 4u) ? ch : -ch);
+      cy = __dadd_rn(cy, (o & 2u) ? ch : -ch);
+      cz = __dadd_rn(cz, (o & 1u) ? ch : -ch);
+      h = ch;
+    }
+    for (int d = d0; d <= l; ++d) {
+      if (d > 0) {
+        const unsigned o = digitAt(path, n, i, d);
+        const double ch = 0.5 * h;
+        cx = __dadd_rn(cx, (o & 4u) ? ch : -ch);
+        cy = __dadd_rn(cy, (o & 2u) ? ch : -ch);
+        cz = __dadd_rn(cz, (o & 1u) ? ch : -ch);
+        h = ch;
+      }
+      const uint32_t node = offset[i] + static_cast<uint32_t>(d - d0);
+      const int64_t end = (d == 0) ? n : runEnd(path, n, words, cp, i, d, p.leaf);
+      const uint32_t count = static_cast<uint32_t>(end - i);
+      out.geom[node] = make_double4(cx, cy, cz, h);
+      out.range[node] = make_uint4(static_cast<uint32_t>(i), count, 0u, offset[end]);
+      out.depth[node] = static_cast<uint32_t>(d);
+      for (int o = 0; o < 8; ++o) out.child[8 * static_cast<size_t>(node) + o] = kInvalid;
+      if (d == 0) {
+        out.parent[node] = kInvalid;
+      } else {
+        uint32_t parent;
+        if (d > d0) {
+          parent = node - 1;
+        } else {
+          const int64_t s = runStart(path, n, words, cp, i, d - 1);
+          parent = offset[s] + static_cast<uint32_t>((d - 1) - (cp[s] + 1));
+        }
+        out.parent[node] = parent;
+        out.child[8 * static_cast<size_t>(parent) + digitAt(path, n, i, d)] = node;
+      }
+      if (d == l) {
+        for (int64_t k = i; k < end; ++k) out.leaf_of_pos[k] = node;
+      }
+    }
+  }
+}
+
+__global__ void childCountKernel(int64_t nodes, const uint32_t* __restrict__ child, uint4* range) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nodes;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t c = 0;
+    for (int o = 0; o < 8; ++o) c += child[8 * k + o] != kInvalid ? 1u : 0u;
+    range[k].z = c;
+  }
+}
+
+__global__ void invertKernel(int64_t n, const uint32_t* __restrict__ perm, uint32_t* inv) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    inv[perm[i]] = static_cast<uint32_t>(i);
+  }
+}
+
+// key for the final stable sort: leaf id of each particle, listed in Morton order
+__global__ void leafKeyKernel(int64_t n, const uint32_t* __restrict__ inv_rank,
+                              const uint32_t* __restrict__ leaf_of_pos, uint32_t* key) {
+  for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    key[j] = leaf_of_pos[inv_rank[j]];
+  }
+}
+
+struct MomentIn {
+  const double* ux;
+  const double* uy;
+  const double* uz;
+  const double* m;
+  double uniform_mass;
+  const uint32_t* sorted;
+  int quadrupole;
+};
+
+__device__ void leafMoments(int64_t node, const MomentIn& in, const double4 g, const uint4 r,
+                            double4* com_out, double* quad_out) {
+  double total = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+  for (uint32_t t = r.x; t < r.x + r.y; ++t) {
+    const uint32_t s = in.sorted[t];
+    const double ms = in.m ? in.m[s] : in.uniform_mass;
+    total += ms;
+    wx += ms * in.ux[s];
+    wy += ms * in.uy[s];
+    wz += ms * in.uz[s];
+  }
+  double cx = g.x, cy = g.y, cz = g.z;
+  if (total > 0.0) {
+    cx = wx / total;
+    cy = wy / total;
+    cz = wz / total;
+  }
+  double q[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (in.quadrupole && total > 0.0) {
+    double ixx = 0, ixy = 0, ixz = 0, iyy = 0, iyz = 0, izz = 0;
+    for (uint32_t t = r.x; t < r.x + r.y; ++t) {
+      const uint32_t s = in.sorted[t];
+      const double ms = in.m ? in.m[s] : in.uniform_mass;
+      const double rx = in.ux[s] - cx, ry = in.uy[s] - cy, rz = in.uz[s] - cz;
+      ixx += ms * rx * rx;
+      ixy += ms * rx * ry;
+      ixz += ms * rx * rz;
+      iyy += ms * ry * ry;
+      iyz += ms * ry * rz;
+      izz += ms * rz * rz;
+    }
+    const double tr = ixx + iyy + izz;
+    q[0] = 3.0 * ixx - tr;
+    q[1] = 3.0 * ixy;
+    q[2] = 3.0 * ixz;
+    q[3] = 3.0 * iyy - tr;
+    q[4] = 3.0 * iyz;
+    q[5] = 3.0 * izz - tr;
+    q[6] = tr;
+  }
+  *com_out = make_double4(cx, cy, cz, total);
+  const double ox = g.x - cx, oy = g.y - cy, oz = g.z - cz;
+  for (int k = 0; k < 7; ++k) quad_out[k] = q[k];
+  quad_out[7] = sqrt(ox * ox + oy * oy + oz * oz);
+  (void)node;
+}
+
+__device__ __forceinline__ double4 ldcg4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  const double2 a = __ldcg(q), b = __ldcg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ void internalMoments(int64_t node, const double4 g, const uint32_t* __restrict__ child,
+                                const double4* com, const double* quad, int quadrupole,
+                                double4* com_out, double* quad_out) {
+  double total = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+  for (int o = 0; o < 8; ++o) {
+    const uint32_t c = __ldcg(child + 8 * node + o);
+    if (c == kInvalid) continue;
+    const double4 cc = ldcg4(com + c);
+    total += cc.w;
+    wx += cc.w * cc.x;
+    wy += cc.w * cc.y;
+    wz += cc.w * cc.z;
+  }
+  double cx = g.x, cy = g.y, cz = g.z;
+  if (total > 0.0) {
+    cx = wx / total;
+    cy = wy / total;
+    cz = wz / total;
+  }
+  double q[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (quadrupole && total > 0.0) {
+    for (int o = 0; o < 8; ++o) {
+      const uint32_t c = __ldcg(child + 8 * node + o);
+      if (c == kInvalid) continue;
+      const double4 cc = ldcg4(com + c);
+      const double dx = cc.x - cx, dy = cc.y - cy, dz = cc.z - cz;
+      const double m = cc.w;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      const double* qc = quad + 8 * static_cast<size_t>(c);
+      q[0] += __ldcg(qc + 0) + m * (3.0 * dx * dx - d2);
+      q[1] += __ldcg(qc + 1) + m * (3.0 * dx * dy);
+      q[2] += __ldcg(qc + 2) + m * (3.0 * dx * dz);
+      q[3] += __ldcg(qc + 3) + m * (3.0 * dy * dy - d2);
+      q[4] += __ldcg(qc + 4) + m * (3.0 * dy * dz);
+      q[5] += __ldcg(qc + 5) + m * (3.0 * dz * dz - d2);
+      q[6] += __ldcg(qc + 6) + m * d2;
+    }
+  }
+  *com_out = make_double4(cx, cy, cz, total);
+  const double ox = g.x - cx, oy = g.y - cy, oz = g.z - cz;
+  for (int k = 0; k < 7; ++k) quad_out[k] = q[k];
+  quad_out[7] = sqrt(ox * ox + oy * oy + oz * oz);
+}
+
+// Bottom-up moments: each leaf computes itself, then the last child to finish
+// a parent computes it from its children in octant order (deterministic).
+__global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restrict__ geom,
+                              const uint4* __restrict__ range, const uint32_t* __restrict__ parent,
+                              const uint32_t* __restrict__ child, uint32_t* counter, double4* com,
+                              double* quad) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nodes;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint4 r = range[k];
+    if (r.z != 0) continue;  // internal
+    double4 cm;
+    double q[8];
+    leafMoments(k, in, geom[k], r, &cm, q);
+    com[k] = cm;
+    for (int t = 0; t < 8; ++t) quad[8 * k + t] = q[t];
+    int64_t node = k;
+    while (true) {
+      __threadfence();
+      const uint32_t p = parent[node];
+      if (p == kInvalid) break;
+      const uint32_t done = atomicAdd(counter + p, 1u);
+      if (done + 1 != range[p].z) break;
+      __threadfence();
+      internalMoments(p, geom[p], child, com, quad, in.quadrupole, &cm, q);
+      com[p] = cm;
+      for (int t = 0; t < 8; ++t) quad[8 * static_cast<size_t>(p) + t] = q[t];
+      node = p;
+    }
+  }
+}
+
+__global__ void nodeBoundsKernel(int64_t nodes, const double4* __restrict__ geom,
+                                 const double4* __restrict__ com, unsigned long long* out) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nodes;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double4 g = geom[k], c = com[k];
+    const double a[3] = {g.x, g.y, g.z}, b[3] = {c.x, c.y, c.z};
+    for (int t = 0; t < 3; ++t) {
+      lo[t] = fmin(lo[t], fmin(a[t], b[t]));
+      hi[t] = fmax(hi[t], fmax(a[t], b[t]));
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+      hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(out + a, orderedBits(lo[a]));
+      atomicMax(out + 3 + a, orderedBits(hi[a]));
+    }
+  }
+}
+
+// Tree-ordered source records. Mixed precision: FP32 offset of the unwrapped
+// position from its leaf's FP64 centre, plus mass. FP64: the caller's
+// position (the reference's source lanes, :3736-3800) plus mass.
+__global__ void packSourcesKernel(int64_t n, const uint32_t* __restrict__ sorted,
+                                  const uint32_t* __restrict__ leaf_of_pos,
+                                  const double4* __restrict__ geom, const double* __restrict__ ux,
+                                  const double* __restrict__ uy, const double* __restrict__ uz,
+                                  const double* __restrict__ x, const double* __restrict__ y,
+                                  const double* __restrict__ z, const double* __restrict__ m,
+                                  double uniform_mass, float4* f4, double4* d4, uint32_t* pos_of_row) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t s = sorted[t];
+    const double ms = m ? m[s] : uniform_mass;
+    pos_of_row[s] = static_cast<uint32_t>(t);
+    if (f4) {
+      const double4 g = geom[leaf_of_pos[t]];
+      f4[t] = make_float4(static_cast<float>(ux[s] - g.x), static_cast<float>(uy[s] - g.y),
+                          static_cast<float>(uz[s] - g.z), static_cast<float>(ms));
+    }
+    if (d4) d4[t] = make_double4(x[s], y[s], z[s], ms);
+  }
+}
+
+__global__ void targetKeyKernel(int64_t nt, const uint32_t* __restrict__ active, int64_t n,
+                                const uint32_t* __restrict__ pos_of_row, int explicit_targets,
+                                uint32_t* key, uint32_t* slot) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nt;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t row = active ? active[k] : static_cast<uint32_t>(k);
+    key[k] = (row < n) ? pos_of_row[row] : 0xFFFFFFFFu;
+    (void)explicit_targets;
+    slot[k] = static_cast<uint32_t>(k);
+  }
+}
+
+__global__ void iotaKernel(int64_t n, uint32_t* v) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    v[i] = static_cast<uint32_t>(i);
+  }
+}
+
+int cubSortPairsU64(Context& c, const unsigned long long* kin, unsigned long long* kout,
+                    const uint32_t* vin, uint32_t* vout, int64_t n, int end_bit, cudaStream_t s) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, static_cast<int>(n), 0, end_bit, s);
+  if (ensure(c.cub_temp, bytes) != cudaSuccess) return CHUI_TREEPM_ENOMEM;
+  if (cub::DeviceRadixSort::SortPairs(c.cub_temp.ptr, bytes, kin, kout, vin, vout, static_cast<int>(n), 0,
+                                      end_bit, s) != cudaSuccess)
+    return CHUI_TREEPM_EDEVICE;
+  return 0;
+}
+
+int cubSortPairsU32(Context& c, const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout,
+                    int64_t n, int end_bit, cudaStream_t s) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, static_cast<int>(n), 0, end_bit, s);
+  if (ensure(c.cub_temp, bytes) != cudaSuccess) return CHUI_TREEPM_ENOMEM;
+  if (cub::DeviceRadixSort::SortPairs(c.cub_temp.ptr, bytes, kin, kout, vin, vout, static_cast<int>(n), 0,
+                                      end_bit, s) != cudaSuccess)
+    return CHUI_TREEPM_EDEVICE;
+  return 0;
+}
+
+int bitsFor(uint64_t maxval) {
+  int b = 1;
+  while (b < 32 && (1ull << b) <= maxval) ++b;
+  return b;
+}
+
+}  // namespace
+
+// Unwrap one axis into `out` (tree frame), returning the anchor.
+static int unwrapAxis(Context& c, int64_t n, const double* in, double box, int canonical, double* out,
+                      double* anchor, cudaStream_t s) {
+  if (n == 0) {
+    *anchor = 0.0;
+    return 0;
+  }
+  const unsigned long long nb = 2ull * static_cast<unsigned long long>(n);
+  if (ensure(c.bucket_min, nb * 8) || ensure(c.bucket_max, nb * 8) || ensure(c.bucket_next, nb * 8))
+    return CHUI_TREEPM_ENOMEM;
+  auto* bmin = c.bucket_min.as<unsigned long long>();
+  auto* bmax = c.bucket_max.as<unsigned long long>();
+  auto* later = c.bucket_next.as<unsigned long long>();
+  cudaMemsetAsync(bmin, 0xFF, nb * 8, s);
+  cudaMemsetAsync(bmax, 0x00, nb * 8, s);
+  const double scale = static_cast<double>(nb) / box;
+  wrapBucketKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in, box, canonical, out, nb, scale, bmin, bmax);
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveScan(nullptr, bytes, bmin, later, MinU64(), ~0ull, static_cast<int>(nb), s);
+  if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
+  cub::DeviceScan::ExclusiveScan(c.cub_temp.ptr, bytes, bmin, later, MinU64(), ~0ull, static_cast<int>(nb), s);
+  // global minimum = min(later[nb-1], bmin[nb-1]) (bucket 0 is the last reversed slot)
+  unsigned long long tail[2];
+  cudaMemcpyAsync(&tail[0], later + nb - 1, 8, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&tail[1], bmin + nb - 1, 8, cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  const unsigned long long gmin = tail[0] < tail[1] ? tail[0] : tail[1];
+  auto* sc = c.scalars.as<unsigned long long>();
+  unsigned long long init[2] = {0ull, ~0ull};
+  cudaMemcpyAsync(sc, init, 16, cudaMemcpyHostToDevice, s);
+  bucketGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, later, box, gmin, sc, 0, sc + 1);
+  bucketGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, later, box, gmin, sc, 1, sc + 1);
+  applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out, box, sc + 1);
+  unsigned long long ab = 0;
+  cudaMemcpyAsync(&ab, sc + 1, 8, cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  std::memcpy(anchor, &ab, 8);
+  return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
+}
+
+int treeBuild(Context& c, int64_t n, const double* x, const double* y, const double* z,
+              const double* m, double uniform_mass, const double src_lo[3], const double src_hi[3],
+              cudaStream_t s) {
+  c.n_nodes = 0;
+  c.max_depth = 0;
+  if (n == 0) return 0;
+  const double box[3] = {c.cfg.box_x, c.cfg.box_y, c.cfg.box_z};
+  if (ensure(c.ux, n * 8) || ensure(c.uy, n * 8) || ensure(c.uz, n * 8)) return CHUI_TREEPM_ENOMEM;
+  const double* in[3] = {x, y, z};
+  double* u[3] = {c.ux.as<double>(), c.uy.as<double>(), c.uz.as<double>()};
+  double anchors[3];
+  for (int a = 0; a < 3; ++a) {
+    // canonical flag as tree_pm_coupling.cpp:3183-3194
+    const int canonical = src_lo[a] >= 0.0 && src_hi[a] < box[a];
+    int rc = unwrapAxis(c, n, in[a], box[a], canonical, u[a], &anchors[a], s);
+    if (rc) return rc;
+  }
+  // bounds of the unwrapped frame
+  auto* sc = c.scalars.as<unsigned long long>();
+  unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
+  cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  boundsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], sc);
+  unsigned long long hb[6];
+  cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = fromOrderedBits(hb[a]);
+    hi[a] = fromOrderedBits(hb[3 + a]);
+  }
+  const double max_extent = std::fmax(hi[0] - lo[0], std::fmax(hi[1] - lo[1], hi[2] - lo[2]));
+
+  // Morton keys + stable sort (tree_ordering.cpp:152-172)
+  const double extent = std::fmax(max_extent, 1.0e-12);
+  if (ensure(c.keys_a, n * 8) || ensure(c.keys_b, n * 8) || ensure(c.idx_a, n * 4) || ensure(c.idx_b, n * 4) ||
+      ensure(c.idx_c, (n + 1) * 4) || ensure(c.idx_d, (n + 1) * 4))
+    return CHUI_TREEPM_ENOMEM;
+  mortonKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], lo[0], lo[1], lo[2], extent,
+                                               c.keys_a.as<unsigned long long>(), c.idx_a.as<uint32_t>());
+  int rc = cubSortPairsU64(c, c.keys_a.as<unsigned long long>(), c.keys_b.as<unsigned long long>(),
+                           c.idx_a.as<uint32_t>(), c.idx_b.as<uint32_t>(), n, 63, s);
+  if (rc) return rc;
+  // keys_b: sorted Morton keys; idx_b: perm_m (Morton rank -> particle)
+  if (ensure(c.morton_sorted, n * 8)) return CHUI_TREEPM_ENOMEM;
+  cudaMemcpyAsync(c.morton_sorted.ptr, c.keys_b.ptr, n * 8, cudaMemcpyDeviceToDevice, s);
+  const uint32_t* perm_m = c.idx_b.as<uint32_t>();
+
+  // root (tree_gravity.cpp:448-452)
+  const double mext = std::fmax(max_extent, 1.0e-10);
+  const double cx0 = 0.5 * (lo[0] + hi[0]);
+  const double cy0 = 0.5 * (lo[1] + hi[1]);
+  const double cz0 = 0.5 * (lo[2] + hi[2]);
+  const double half0 = 0.5 * mext * (1.0 + 1.0e-8);
+  int depth_half = 0;
+  for (double h = half0; !(h <= 1.0e-12) && depth_half < 4 * kMaxDepth; h *= 0.5) ++depth_half;
+
+  if (ensure(c.common_prefix, n * 4) || ensure(c.node_count_per_pos, (n + 1) * 4) ||
+      ensure(c.node_offset, (n + 1) * 4) || ensure(c.inv_pos, n * 4) || ensure(c.leaf_of_pos, n * 4) ||
+      ensure(c.sorted_index, n * 4) || ensure(c.pos_of_row, n * 4))
+    return CHUI_TREEPM_ENOMEM;
+  uint32_t* status = c.status.as<uint32_t>();
+  int* cp = c.common_prefix.as<int>();
+  uint32_t* counts = c.node_count_per_pos.as<uint32_t>();
+  uint32_t* offset = c.node_offset.as<uint32_t>();
+  unsigned long long* path = nullptr;
+  uint32_t total_nodes = 0;
+  int words = 1;
+  NodePlan plan;
+  plan.n = n;
+  plan.leaf = static_cast<int>(c.cfg.max_leaf_size);
+  plan.depth_half = depth_half;
+  for (;; ++words) {
+    if (words > kMaxPathWords) {
+      c.last_error = "Tree gravity maximum depth contract exceeded";
+      return CHUI_TREEPM_ERANGE;
+    }
+    if (ensure(c.path_words, static_cast<size_t>(words) * n * 8) ||
+        ensure(c.keys_a, static_cast<size_t>(words) * n * 8))
+      return CHUI_TREEPM_ENOMEM;
+    path = c.path_words.as<unsigned long long>();
+    unsigned long long* by_rank = c.keys_a.as<unsigned long long>();
+    unsigned long long* key_cur = c.keys_b.as<unsigned long long>();
+    unsigned long long* key_sorted = c.bucket_max.as<unsigned long long>();
+    pathKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, perm_m, u[0], u[1], u[2], cx0, cy0, cz0, half0,
+                                               by_rank);
+    uint32_t* rank_in = c.idx_c.as<uint32_t>();
+    uint32_t* rank_out = c.idx_d.as<uint32_t>();
+    iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in);
+    for (int w = words - 1; w >= 0; --w) {  // LSD over path words, each pass stable
+      gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in, key_cur);
+      rc = cubSortPairsU64(c, key_cur, key_sorted, rank_in, rank_out, n, 63, s);
+      if (rc) return rc;
+      uint32_t* t = rank_in;
+      rank_in = rank_out;
+      rank_out = t;
+    }
+    // rank_in: path position -> Morton rank
+    for (int w = 0; w < words; ++w)
+      gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in,
+                                                      path + static_cast<size_t>(w) * n);
+    invertKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in, c.inv_pos.as<uint32_t>());
+    commonPrefixKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, path, cp);
+    plan.depth_max = kLevelsPerWord * words;
+    cudaMemsetAsync(status, 0, 4, s);
+    nodeCountKernel<<<gridFor(n + 1, 256), 256, 0, s>>>(plan, cp, counts, status);
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, counts, offset, static_cast<int>(n + 1), s);
+    if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
+    cub::DeviceScan::ExclusiveSum(c.cub_temp.ptr, bytes, counts, offset, static_cast<int>(n + 1), s);
+    uint32_t hs[2];
+    cudaMemcpyAsync(&hs[0], status, 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hs[1], offset + n, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      c.last_error = "tree node enumeration failed";
+      return CHUI_TREEPM_EDEVICE;
+    }
+    if (hs[0] & kStatusNeedMorePathWords) continue;
+    if (hs[0] & kStatusDepthExceeded) {
+      c.last_error = "Tree gravity maximum depth contract exceeded";
+      return CHUI_TREEPM_ERANGE;
+    }
+    total_nodes = hs[1];
+    break;
+  }
+  c.path_words_used = words;
+  c.n_nodes = total_nodes;
+  if (ensure(c.node_geom, total_nodes * sizeof(double4)) || ensure(c.node_com, total_nodes * sizeof(double4)) ||
+      ensure(c.node_quad, total_nodes * 8 * sizeof(double)) || ensure(c.node_child, total_nodes * 8 * 4) ||
+      ensure(c.node_range, total_nodes * sizeof(uint4)) || ensure(c.node_parent, total_nodes * 4) ||
+      ensure(c.node_depth, total_nodes * 4) || ensure(c.node_counter, total_nodes * 4))
+    return CHUI_TREEPM_ENOMEM;
+  NodeOut out;
+  out.geom = c.node_geom.as<double4>();
+  out.range = c.node_range.as<uint4>();
+  out.parent = c.node_parent.as<uint32_t>();
+  out.depth = c.node_depth.as<uint32_t>();
+  out.child = c.node_child.as<uint32_t>();
+  out.leaf_of_pos = c.leaf_of_pos.as<uint32_t>();
+  nodeEmitKernel<<<gridFor(n, 128), 128, 0, s>>>(plan, words, path, cp, counts, offset, cx0, cy0, cz0, half0,
+                                                 out);
+  childCountKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.child, out.range);
+  // final order: stable sort of Morton order by leaf id
+  uint32_t* leaf_key = c.idx_a.as<uint32_t>();
+  leafKeyKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.inv_pos.as<uint32_t>(), out.leaf_of_pos, leaf_key);
+  rc = cubSortPairsU32(c, leaf_key, c.idx_d.as<uint32_t>(), perm_m, c.sorted_index.as<uint32_t>(), n,
+                       bitsFor(total_nodes), s);
+  if (rc) return rc;
+  // moments
+  cudaMemsetAsync(c.node_counter.ptr, 0, total_nodes * 4, s);
+  MomentIn mi;
+  mi.ux = u[0];
+  mi.uy = u[1];
+  mi.uz = u[2];
+  mi.m = m;
+  mi.uniform_mass = uniform_mass;
+  mi.sorted = c.sorted_index.as<uint32_t>();
+  mi.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
+  momentsKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(total_nodes, mi, out.geom, out.range, out.parent,
+                                                          out.child, c.node_counter.as<uint32_t>(),
+                                                          c.node_com.as<double4>(), c.node_quad.as<double>());
+  // tree-ordered source records
+  const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
+  if (mixed) {
+    if (ensure(c.src_f4, n * sizeof(float4))) return CHUI_TREEPM_ENOMEM;
+  }
+  if (ensure(c.src_d4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
+  packSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), out.leaf_of_pos, out.geom,
+                                                    u[0], u[1], u[2], x, y, z, m, uniform_mass,
+                                                    mixed ? c.src_f4.as<float4>() : nullptr,
+                                                    c.src_d4.as<double4>(), c.pos_of_row.as<uint32_t>());
+  // maximum depth (for stack sizing and stats)
+  {
+    size_t bytes = 0;
+    uint32_t* dmax = c.idx_a.as<uint32_t>();
+    cub::DeviceReduce::Max(nullptr, bytes, out.depth, dmax, static_cast<int>(total_nodes), s);
+    if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
+    cub::DeviceReduce::Max(c.cub_temp.ptr, bytes, out.depth, dmax, static_cast<int>(total_nodes), s);
+    uint32_t hd = 0;
+    cudaMemcpyAsync(&hd, dmax, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      c.last_error = "tree build kernels failed";
+      return CHUI_TREEPM_EDEVICE;
+    }
+    c.max_depth = hd;
+  }
+  c.tree_anchor[0] = anchors[0];
+  c.tree_anchor[1] = anchors[1];
+  c.tree_anchor[2] = anchors[2];
+  return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
+}
+
+int treeNodeBounds(Context& c, double lo[3], double hi[3], cudaStream_t s) {
+  auto* sc = c.scalars.as<unsigned long long>();
+  unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
+  cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  if (c.n_nodes > 0)
+    nodeBoundsKernel<<<gridFor(c.n_nodes, 256), 256, 0, s>>>(c.n_nodes, c.node_geom.as<double4>(),
+                                                              c.node_com.as<double4>(), sc);
+  unsigned long long hb[6];
+  cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = c.n_nodes > 0 ? fromOrderedBits(hb[a]) : INFINITY;
+    hi[a] = c.n_nodes > 0 ? fromOrderedBits(hb[3 + a]) : -INFINITY;
+  }
+  return 0;
+}
+
+// Visit order: active slots sorted by the tree position of their row
+// (tree_pm_coupling.cpp:3808-3838); slots without a local source go last.
+int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explicit_targets, int64_t n,
+                     cudaStream_t s) {
+  if (nt == 0) return 0;
+  if (ensure(c.target_order, nt * 4) || ensure(c.idx_a, std::max<int64_t>(nt, n) * 4) ||
+      ensure(c.idx_c, (std::max<int64_t>(nt, n) + 1) * 4) || ensure(c.idx_d, (std::max<int64_t>(nt, n) + 1) * 4))
+    return CHUI_TREEPM_ENOMEM;
+  uint32_t* key = c.idx_c.as<uint32_t>();
+  uint32_t* slot = c.idx_a.as<uint32_t>();
+  targetKeyKernel<<<gridFor(nt, 256), 256, 0, s>>>(nt, active, n, c.pos_of_row.as<uint32_t>(), explicit_targets,
+                                                   key, slot);
+  return cubSortPairsU32(c, key, c.idx_d.as<uint32_t>(), slot, c.target_order.as<uint32_t>(), nt, 32, s);
+}
+
+}  // namespace chui

@@ -1,0 +1,418 @@
+// Short-range residual walk on the B200: the FLOP sink of the TreePM force.
+//
+// Reference: evaluateTargetAgainstLocalTree, tree_pm_coupling.cpp:4026-4272
+// (per-target DFS, periodic node metric, AABB cutoff prune, leaf pairs with
+// K_soft - K_long inside r_cut, strict acceptance of internal nodes,
+// screened-quadrupole multipoles monopolePlusQuadrupoleAccelPeriodicReference
+// :743-827, children pushed in reverse octant order :916-925).
+//
+// Design: one warp walks 32 targets that are consecutive in tree order
+// (spatially coherent), sharing one DFS stack in shared memory. Every lane
+// makes the reference's own decision for every node it reaches, in FP64
+// (prune / leaf pairs / accept multipole / open); the warp descends into a
+// node's children when any lane opens it, and a lane that pruned or accepted
+// a node skips that node's subtree (nodes are numbered in preorder, so the
+// subtree is the index range [node, subtree_end)). Each lane therefore sees
+// exactly the nodes, pairs and multipoles of its own walk.
+//
+// Leaf sources are staged through shared memory per warp chunk of 32 and
+// broadcast to the lanes. Mixed precision: each source is stored as an FP32
+// offset from its leaf's FP64 centre; the target's offset to that centre is
+// formed in FP64 (the node metric) and rounded once, so the pair separation
+// is an FP32 difference of two small node-relative vectors. The residual
+// kernel K = (r^2+eps^2)^-3/2 - H(t)/(8 r_s^3), t = r^2/(4 r_s^2), uses one
+// rsqrt and a polynomial for H fitted per configuration (no erf/exp per
+// pair). Per-leaf FP32 partial sums are added into FP64 accumulators. The
+// FP64 configuration evaluates the reference's formulas (source metric per
+// pair, erf/exp residual) unchanged.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+
+#include "context.cuh"
+
+namespace chui {
+namespace {
+
+struct WalkArgs {
+  int64_t nt;       // targets
+  int64_t n;        // sources
+  const uint32_t* order;   // visit position -> active slot
+  const uint32_t* active;  // slot -> source row (nullable: slot == row)
+  const double* tx;        // explicit target positions (nullable)
+  const double* ty;
+  const double* tz;
+  const double* sx;        // caller source positions
+  const double* sy;
+  const double* sz;
+  const uint32_t* pos_of_row;
+  const double4* geom;
+  const double4* com;
+  const double* quad;
+  const uint32_t* child;
+  const uint4* range;
+  const float4* src_f4;
+  const double4* src_d4;
+  double* out_x;   // per slot, short-range part
+  double* out_y;
+  double* out_z;
+  double* out_near;
+  unsigned long long* counters;
+  uint32_t* work;
+  uint32_t* status;
+  PolyH poly;
+  WalkParams wp;
+};
+
+__device__ __forceinline__ float polyH(const PolyH& p, float t) {
+  const float s = fmaf(t, p.scale, -1.0f);
+  float h = p.c[p.terms - 1];
+  for (int k = p.terms - 2; k >= 0; --k) h = fmaf(h, s, p.c[k]);
+  return h;
+}
+
+// monopolePlusQuadrupoleAccelPeriodicReference (tree_pm_coupling.cpp:743-827), FP64.
+__device__ void multipoleForce(const WalkArgs& a, uint32_t node, double dx, double dy, double dz,
+                               double eps_t, double& ax, double& ay, double& az) {
+  const WalkParams& w = a.wp;
+  const double rs = w.rs;
+  const double4 cm = a.com[node];
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  const double safe_r2 = fmax(r2, 1.0e-30);
+  const double r = sqrt(safe_r2);
+  const double pe = fmax(w.eps, eps_t);
+  const double denom = fmax(r2 + pe * pe, 1.0e-30);
+  const double soft = 1.0 / (denom * sqrt(denom));
+  const double split = shortRangeFactor(r, rs);
+  const double newton = 1.0 / (safe_r2 * r);
+  const double radial = soft + (split - 1.0) * newton;
+  const double G = w.G;
+  double fx = G * cm.w * radial * dx;
+  double fy = G * cm.w * radial * dy;
+  double fz = G * cm.w * radial * dz;
+  if (w.quadrupole) {
+    const double* q = a.quad + 8 * static_cast<size_t>(node);
+    const double tr = q[6];
+    const double mxx = (q[0] + tr) / 3.0, mxy = q[1] / 3.0, mxz = q[2] / 3.0;
+    const double myy = (q[3] + tr) / 3.0, myz = q[4] / 3.0, mzz = (q[5] + tr) / 3.0;
+    const double mdx = mxx * dx + mxy * dy + mxz * dz;
+    const double mdy = mxy * dx + myy * dy + myz * dz;
+    const double mdz = mxz * dx + myz * dy + mzz * dz;
+    const double dmd = dx * mdx + dy * mdy + dz * mdz;
+    const double k = 0.564189583547756286948079451560772586;
+    const double rs2 = rs * rs;
+    const double ex = exp(-r2 / (4.0 * rs2));
+    const double sf = -0.5 * k * r2 * ex / (rs * rs2);
+    const double ss = k * ex * (-r / (rs * rs2) + 0.25 * r * r2 / (rs * rs2 * rs2));
+    const double s1 = -3.0 * r / (denom * denom * sqrt(denom));
+    const double s2 = -3.0 / (denom * denom * sqrt(denom)) + 15.0 * r2 / (denom * denom * denom * sqrt(denom));
+    const double n1 = -3.0 / (safe_r2 * safe_r2);
+    const double n2 = 12.0 / (safe_r2 * safe_r2 * r);
+    const double rf = s1 + sf * newton + (split - 1.0) * n1;
+    const double rsec = s2 + ss * newton + 2.0 * sf * n1 + (split - 1.0) * n2;
+    const double f1 = rf / r;
+    const double cr = rsec / r2 - rf / (r2 * r);
+    fx += G * (mdx * f1 + 0.5 * tr * dx * f1 + 0.5 * dx * dmd * cr);
+    fy += G * (mdy * f1 + 0.5 * tr * dy * f1 + 0.5 * dy * dmd * cr);
+    fz += G * (mdz * f1 + 0.5 * tr * dz * f1 + 0.5 * dz * dmd * cr);
+  }
+  ax += fx;
+  ay += fy;
+  az += fz;
+}
+
+// Strict-reference acceptance of an internal node (internal/tree_pm_acceptance.hpp:170-255
+// with acceptNodeByMac and the softening guard of internal/tree_interaction_common.hpp:36-89).
+__device__ __forceinline__ bool acceptStrict(const WalkParams& w, double half, double com_offset,
+                                             bool inside, bool within, double r2, double eps_t) {
+  const double r = sqrt(fmax(r2, 1.0e-30));
+  // uniform softening: node softening max == min, the envelope guard passes
+  (void)eps_t;
+  const bool envelope_ok = w.quadrupole && (2.0 * half / r) < 0.08;
+  bool mac_ok;
+  if (inside) {
+    mac_ok = false;
+  } else if (w.criterion == 0) {
+    mac_ok = (2.0 * half / sqrt(r2 + 1.0e-30)) < w.theta;
+  } else {
+    mac_ok = ((2.0 * half + com_offset) / sqrt(r2 + 1.0e-30)) < w.theta;
+  }
+  return mac_ok && envelope_ok && within && !inside && isfinite(r2);
+}
+
+template <bool kMixed, bool kEpsZero>
+__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a) {
+  __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
+  __shared__ float4 src_f_sm[kWalkWarpsPerBlock][32];
+  __shared__ double4 src_d_sm[kWalkWarpsPerBlock][32];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  uint32_t* stack = stack_sm[warp];
+  const WalkParams& w = a.wp;
+  unsigned long long cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0,
+                     cnt_skips = 0, cnt_multi = 0, cnt_leaves = 0;
+
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(a.work, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= a.nt) break;
+    const int64_t v = static_cast<int64_t>(base) + lane;
+    const bool valid = v < a.nt;
+    uint32_t slot = 0, row = kInvalid;
+    double px = 0.0, py = 0.0, pz = 0.0;
+    if (valid) {
+      slot = a.order[v];
+      row = a.active ? a.active[slot] : slot;
+      if (a.tx) {
+        px = a.tx[slot];
+        py = a.ty[slot];
+        pz = a.tz[slot];
+      } else {
+        px = a.sx[row];
+        py = a.sy[row];
+        pz = a.sz[row];
+      }
+    }
+    const bool skip_self = valid && row < a.n;
+    const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
+    const double eps_t = w.eps;
+    Metric sm[3], nm[3];
+    const double pt[3] = {px, py, pz};
+    for (int ax_ = 0; ax_ < 3; ++ax_) {
+      sm[ax_] = makeMetric(w.src_lo[ax_], w.src_hi[ax_], pt[ax_], w.box[ax_]);
+      nm[ax_] = makeMetric(w.node_lo[ax_], w.node_hi[ax_], pt[ax_], w.box[ax_]);
+    }
+    double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
+    double nearest = INFINITY;
+    float nearest_f = INFINITY;
+    uint32_t skip_until = 0;
+    int sp = 0;
+    if (lane == 0) stack[0] = 0u;
+    sp = 1;
+    __syncwarp();
+    bool overflow = false;
+    while (sp > 0) {
+      const uint32_t node = stack[sp - 1];
+      --sp;
+      __syncwarp();
+      const bool act = valid && node >= skip_until;
+      if (!__any_sync(0xffffffffu, act)) continue;
+      const double4 g = a.geom[node];
+      const uint4 rg = a.range[node];
+      const double h = g.w;
+      const double ndx = applyMetric(nm[0], g.x - px);
+      const double ndy = applyMetric(nm[1], g.y - py);
+      const double ndz = applyMetric(nm[2], g.z - pz);
+      const double ax_abs = fabs(ndx), ay_abs = fabs(ndy), az_abs = fabs(ndz);
+      const double ex = fmax(0.0, ax_abs - h), ey = fmax(0.0, ay_abs - h), ez = fmax(0.0, az_abs - h);
+      const bool prune = !withinCutoff(ex * ex + ey * ey + ez * ez, w.cutoff, w.cutoff2);
+      if (act) {
+        ++cnt_visited;
+        cnt_pruned += prune ? 1 : 0;
+      }
+      const bool is_leaf = rg.z == 0;
+      if (is_leaf) {
+        const bool want = act && !prune;
+        if (!__any_sync(0xffffffffu, want)) continue;
+        if (want) {
+          ++cnt_accepted;
+          ++cnt_leaves;
+        }
+        const uint32_t begin = rg.x, count = rg.y;
+        // Node-relative FP32 offsets select the right periodic image only for
+        // leaves smaller than L/2 - r_cut; larger (tiny-N) leaves use the exact path.
+        if (kMixed && h < w.exact_half) {
+          const float ndfx = static_cast<float>(ndx), ndfy = static_cast<float>(ndy),
+                      ndfz = static_cast<float>(ndz);
+          float fx = 0.f, fy = 0.f, fz = 0.f;
+          for (uint32_t chunk = 0; chunk < count; chunk += 32) {
+            const uint32_t k = chunk + lane;
+            if (k < count) src_f_sm[warp][lane] = a.src_f4[begin + k];
+            __syncwarp();
+            const uint32_t m = min(32u, count - chunk);
+            if (want) {
+              for (uint32_t j = 0; j < m; ++j) {
+                const float4 s = src_f_sm[warp][j];
+                const float dx = s.x + ndfx, dy = s.y + ndfy, dz = s.z + ndfz;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool in = r2 <= w.cut2_f && (begin + chunk + j) != self_pos;
+                cnt_pairs += in ? 1 : 0;
+                cnt_skips += (!in && (begin + chunk + j) != self_pos) ? 1 : 0;
+                nearest_f = in ? fminf(nearest_f, r2) : nearest_f;
+                const float t = r2 * w.inv_4rs2_f;
+                const float hh = polyH(a.poly, t);
+                const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
+                const float rinv = rsqrtf(s2);
+                const float k3 = fmaf(-hh, w.inv_8rs3_f, rinv * rinv * rinv);
+                const float f = (in && r2 > 0.f) ? w.G_f * s.w * k3 : 0.f;
+                fx = fmaf(f, dx, fx);
+                fy = fmaf(f, dy, fy);
+                fz = fmaf(f, dz, fz);
+              }
+            }
+            __syncwarp();
+          }
+          acc_x += static_cast<double>(fx);
+          acc_y += static_cast<double>(fy);
+          acc_z += static_cast<double>(fz);
+        } else {
+          float nearest_mixed = INFINITY;
+          for (uint32_t chunk = 0; chunk < count; chunk += 32) {
+            const uint32_t k = chunk + lane;
+            if (k < count) src_d_sm[warp][lane] = a.src_d4[begin + k];
+            __syncwarp();
+            const uint32_t m = min(32u, count - chunk);
+            if (want) {
+              for (uint32_t j = 0; j < m; ++j) {
+                if ((begin + chunk + j) == self_pos) continue;
+                const double4 s = src_d_sm[warp][j];
+                const double dx = applyMetric(sm[0], s.x - px);
+                const double dy = applyMetric(sm[1], s.y - py);
+                const double dz = applyMetric(sm[2], s.z - pz);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > w.cutoff2) {
+                  ++cnt_skips;
+                  continue;
+                }
+                nearest = fmin(nearest, r2);
+                nearest_mixed = fminf(nearest_mixed, static_cast<float>(r2));
+                ++cnt_pairs;
+                if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
+                const double f = residualInvR3(r2, fmax(w.eps, eps_t), w.rs) * w.G;
+                acc_x += f * s.w * dx;
+                acc_y += f * s.w * dy;
+                acc_z += f * s.w * dz;
+              }
+            }
+            __syncwarp();
+          }
+          nearest_f = fminf(nearest_f, nearest_mixed);
+        }
+        continue;
+      }
+      // internal node
+      const double4 cm = a.com[node];
+      const double off = a.quad[8 * static_cast<size_t>(node) + 7];
+      const bool inside = skip_self && ax_abs <= h && ay_abs <= h && az_abs <= h;
+      const double mx = ax_abs + h, my = ay_abs + h, mz = az_abs + h;
+      const bool within = withinCutoff(mx * mx + my * my + mz * mz, w.cutoff, w.cutoff2);
+      const double dx = applyMetric(nm[0], cm.x - px);
+      const double dy = applyMetric(nm[1], cm.y - py);
+      const double dz = applyMetric(nm[2], cm.z - pz);
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const bool accept = act && !prune && acceptStrict(w, h, off, inside, within, r2, eps_t);
+      const bool open = act && !prune && !accept;
+      if (accept) {
+        ++cnt_accepted;
+        ++cnt_multi;
+        multipoleForce(a, node, dx, dy, dz, eps_t, acc_x, acc_y, acc_z);
+      }
+      if (act && (prune || accept)) skip_until = rg.w;
+      if (open) ++cnt_opened;
+      if (__any_sync(0xffffffffu, open)) {
+        const uint32_t ch = lane < 8 ? a.child[8 * static_cast<size_t>(node) + lane] : kInvalid;
+        const unsigned mask = __ballot_sync(0xffffffffu, ch != kInvalid) & 0xFFu;
+        const int nc = __popc(mask);
+        if (sp + nc > kStackCap) {
+          overflow = true;
+          break;
+        }
+        if (ch != kInvalid) {
+          // highest octant deepest in the stack: octant 0 is popped first
+          const int pos = sp + __popc(mask >> (lane + 1));
+          stack[pos] = ch;
+        }
+        sp += nc;
+        __syncwarp();
+      }
+    }
+    if (overflow) {
+      if (lane == 0) atomicOr(a.status, kStatusStackOverflow);
+    }
+    if constexpr (kMixed) nearest = static_cast<double>(nearest_f);
+    if (valid) {
+      a.out_x[slot] = acc_x;
+      a.out_y[slot] = acc_y;
+      a.out_z[slot] = acc_z;
+      a.out_near[slot] = nearest;
+    }
+    __syncwarp();
+  }
+  // counters: warp reduction then one atomic each
+  unsigned long long c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs,
+                             cnt_pruned, cnt_skips, cnt_multi, cnt_leaves};
+  for (int k = 0; k < 8; ++k) {
+    for (int off = 16; off > 0; off >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], off);
+  }
+  if (lane == 0) {
+    for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, c[k]);
+  }
+}
+
+template <bool kMixed, bool kEpsZero>
+int launchWalk(const WalkArgs& args, cudaStream_t s) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walkKernel<kMixed, kEpsZero>,
+                                                kWalkWarpsPerBlock * 32, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t warps_needed = (args.nt + 31) / 32;
+  int64_t blocks = static_cast<int64_t>(sms) * per_sm;
+  const int64_t max_useful = (warps_needed + kWalkWarpsPerBlock - 1) / kWalkWarpsPerBlock;
+  if (blocks > max_useful) blocks = max_useful;
+  if (blocks < 1) blocks = 1;
+  walkKernel<kMixed, kEpsZero><<<static_cast<unsigned>(blocks), kWalkWarpsPerBlock * 32, 0, s>>>(args);
+  return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
+}
+
+}  // namespace
+
+int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
+            const double* tz, const double* sx, const double* sy, const double* sz,
+            const WalkParams& wp, int64_t n, cudaStream_t s) {
+  if (nt == 0) return 0;
+  if (ensure(c.tree_acc, static_cast<size_t>(nt) * 3 * sizeof(double)) ||
+      ensure(c.tree_near, static_cast<size_t>(nt) * sizeof(double)) ||
+      ensure(c.walk_counters, 8 * sizeof(unsigned long long)) || ensure(c.work_counter, 4))
+    return CHUI_TREEPM_ENOMEM;
+  cudaMemsetAsync(c.walk_counters.ptr, 0, 8 * sizeof(unsigned long long), s);
+  cudaMemsetAsync(c.work_counter.ptr, 0, 4, s);
+  WalkArgs a;
+  a.nt = nt;
+  a.n = n;
+  a.order = c.target_order.as<uint32_t>();
+  a.active = active;
+  a.tx = tx;
+  a.ty = ty;
+  a.tz = tz;
+  a.sx = sx;
+  a.sy = sy;
+  a.sz = sz;
+  a.pos_of_row = c.pos_of_row.as<uint32_t>();
+  a.geom = c.node_geom.as<double4>();
+  a.com = c.node_com.as<double4>();
+  a.quad = c.node_quad.as<double>();
+  a.child = c.node_child.as<uint32_t>();
+  a.range = c.node_range.as<uint4>();
+  a.src_f4 = c.src_f4.as<float4>();
+  a.src_d4 = c.src_d4.as<double4>();
+  double* acc = c.tree_acc.as<double>();
+  a.out_x = acc;
+  a.out_y = acc + nt;
+  a.out_z = acc + 2 * nt;
+  a.out_near = c.tree_near.as<double>();
+  a.counters = c.walk_counters.as<unsigned long long>();
+  a.work = c.work_counter.as<uint32_t>();
+  a.status = c.status.as<uint32_t>();
+  a.poly = c.poly;
+  a.wp = wp;
+  const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
+  const bool eps_zero = wp.eps == 0.0;
+  if (mixed) return eps_zero ? launchWalk<true, true>(a, s) : launchWalk<true, false>(a, s);
+  return launchWalk<false, false>(a, s);
+}
+
+}  // namespace chui

@@ -1,0 +1,191 @@
+/* chui_treepm.h -- C-ABI of the B200 TreePM gravity solver.
+ *
+ * Drop-in boundary for CHUI's periodic TreePM force path. A C++ host binds it
+ * behind the same interface as cosmosim::gravity::TreePmCoordinator
+ * (include/cosmosim/gravity/tree_pm_coupling.hpp:527-814 in the reference);
+ * chui-dev_b200/host/tree_pm_coordinator.hpp is that shim. Plain pointers and
+ * sizes only; no C++ or torch types cross this boundary.
+ *
+ * Conventions
+ *  - Every entry point returns 0 on success or a CHUI_TREEPM_E* code; the text
+ *    of the last error is available from chui_treepm_last_error().
+ *  - Pointers are host memory when `memory == CHUI_TREEPM_HOST`, device memory
+ *    of the context's GPU when `memory == CHUI_TREEPM_DEVICE`.
+ *  - `stream` is a cudaStream_t (NULL: the context's own stream). Calls with
+ *    host memory return after the results are in the host buffers; calls with
+ *    device memory return after the work is complete on `stream` as well (the
+ *    solver reads a status word back to report kernel-side errors).
+ *  - One context must not be used from two threads at once.
+ */
+#ifndef CHUI_TREEPM_H
+#define CHUI_TREEPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHUI_TREEPM_ABI_VERSION 1
+
+enum {
+  CHUI_TREEPM_OK = 0,
+  CHUI_TREEPM_EINVAL = 22,      /* std::invalid_argument in the reference */
+  CHUI_TREEPM_ERANGE = 34,      /* std::out_of_range / std::overflow_error (index, depth, stack) */
+  CHUI_TREEPM_ENOMEM = 12,      /* allocation failure (MemoryAdmissionError / bad_alloc) */
+  CHUI_TREEPM_ESTATE = 71,      /* std::runtime_error: e.g. PM reuse without a valid field */
+  CHUI_TREEPM_EDEVICE = 5,      /* CUDA / cuFFT failure */
+  CHUI_TREEPM_ENOTSUP = 95      /* option outside the implemented periodic strict path */
+};
+
+enum { CHUI_TREEPM_HOST = 0, CHUI_TREEPM_DEVICE = 1 };
+enum { CHUI_TREEPM_MIXED = 0, CHUI_TREEPM_FP64 = 1 };
+enum { CHUI_TREEPM_CIC = 0, CHUI_TREEPM_TSC = 1 };
+enum {
+  CHUI_TREEPM_OPEN_GEOMETRIC = 0,     /* TreeOpeningCriterion::kBarnesHutGeometric */
+  CHUI_TREEPM_OPEN_COM_DISTANCE = 1,  /* TreeOpeningCriterion::kBarnesHutComDistance */
+  CHUI_TREEPM_OPEN_RELATIVE = 2       /* TreeOpeningCriterion::kRelativeForceError */
+};
+
+/* Solver configuration: the `.param.txt` [numerics] treepm_* knobs
+ * (include/cosmosim/core/config.hpp:776-821) after GravityRuntimeImpl's
+ * mapping to TreePmOptions (src/workflows/gravity_runtime.cpp:469-608). */
+typedef struct {
+  int64_t pm_grid_nx, pm_grid_ny, pm_grid_nz; /* treepm_pm_grid_n{x,y,z} */
+  double box_x, box_y, box_z;                 /* cosmology box_size_{x,y,z}_mpc_comoving */
+  double asmth_cells;                         /* treepm_asmth_cells: r_s in mesh cells */
+  double rcut_cells;                          /* treepm_rcut_cells: r_cut in mesh cells */
+  double opening_theta;                       /* treepm_tree_opening_theta */
+  int32_t opening_criterion;                  /* treepm_tree_opening_criterion */
+  int32_t multipole_order;                    /* 0 monopole, 2 quadrupole (the reference default) */
+  int64_t max_leaf_size;                      /* treepm_tree_max_leaf_size */
+  int32_t assignment_scheme;                  /* treepm_assignment_scheme: CIC or TSC */
+  int32_t window_deconvolution;               /* treepm_enable_window_deconvolution */
+  double gravitational_constant;              /* G in code units (PM and tree share it) */
+  double softening;                           /* Plummer epsilon, comoving (gravity_softening_kpc_comoving * 1e-3) */
+  int32_t acceptance_policy;                  /* 0 strict reference (only policy implemented) */
+  int32_t precision;                          /* CHUI_TREEPM_MIXED or CHUI_TREEPM_FP64 */
+  int32_t device;                             /* CUDA device ordinal */
+  int32_t reserved;
+} chui_treepm_config;
+
+/* Counters named as TreePmTraversalCounters (tree_pm_coupling.hpp:39-87) plus
+ * device timings of the last solve. */
+typedef struct {
+  uint64_t visited_nodes, accepted_nodes, opened_nodes, direct_pair_evaluations;
+  uint64_t cutoff_pruned_nodes, cutoff_skipped_pairs, accepted_internal_multipoles, accepted_leaves;
+  uint64_t node_count;
+  uint32_t maximum_depth;
+  uint32_t path_words;
+  double pm_ms, tree_build_ms, walk_ms, total_ms;
+} chui_treepm_stats;
+
+/* Sources: TreePmCoordinator::solveActiveSet's pos_{x,y,z}_comoving and
+ * mass_code spans. mass may be NULL for a uniform mass population. */
+typedef struct {
+  int64_t count;
+  const double *x, *y, *z;
+  const double *mass;
+  double uniform_mass;
+} chui_treepm_sources;
+
+/* Accumulator: TreePmForceAccumulatorView (tree_pm_coupling.hpp:127-165).
+ * active_index may be NULL for "all sources in row order". target_{x,y,z}
+ * (optional) give explicit target positions, in which case active_index
+ * entries may be 0xFFFFFFFF for targets without a source identity. Output
+ * lanes other than accel_* are optional (NULL). long_range_* are in active-slot
+ * order; short_range_* and nearest_pair_r2 are source-indexed like the
+ * reference's tree-only lanes. */
+typedef struct {
+  int64_t active_count;
+  const uint32_t *active_index;
+  double *accel_x, *accel_y, *accel_z;
+  const double *target_x, *target_y, *target_z;
+  double *long_range_x, *long_range_y, *long_range_z;
+  double *short_range_x, *short_range_y, *short_range_z;
+  double *nearest_pair_r2;
+} chui_treepm_accumulator;
+
+/* Defaults of TreePmOptions / TreeGravityOptions (tree_gravity.hpp:30-43,
+ * tree_pm_coupling.hpp:243-332) for a 16^3 mesh on a unit box. */
+int chui_treepm_config_default(chui_treepm_config *config);
+
+/* TreePmCoordinator::TreePmCoordinator(PmGridShape) (tree_pm_coupling.hpp:545-551):
+ * owns the PM mesh, FFT plans, tree and scratch on `config->device`. */
+int chui_treepm_create(const chui_treepm_config *config, void **handle);
+
+/* ~TreePmCoordinator(). NULL is accepted. */
+void chui_treepm_destroy(void *handle);
+
+/* Replace the options used by later solves (TreePmOptions passed per call in
+ * the reference). The mesh shape is fixed at creation, as PmGridShape is. */
+int chui_treepm_set_config(void *handle, const chui_treepm_config *config);
+
+/* Text of the last error on this handle ("" when none). */
+const char *chui_treepm_last_error(const void *handle);
+
+/* TreePmCoordinator::solveActiveSetWithPmCadence (tree_pm_coupling.hpp:563-573,
+ * tree_pm_coupling.cpp:2282-3518): PM refresh (deposit, FFT, Green x split
+ * filter, spectral gradient) when refresh_long_range_field != 0 (otherwise the
+ * cached field must match, as :2483-2532 requires), PM interpolation, periodic
+ * tree build, short-range residual walk, accumulation. stats may be NULL. */
+int chui_treepm_solve(void *handle, const chui_treepm_sources *sources,
+                      const chui_treepm_accumulator *accumulator, int refresh_long_range_field,
+                      int memory, void *stream, chui_treepm_stats *stats);
+
+/* PmSolver::assignDensity (pm_solver.hpp:469-482, pm_solver.cpp:3842-4565):
+ * periodic CIC/TSC density (mass / cell volume) in compact nx*ny*nz row-major
+ * order, written as FP64. */
+int chui_pm_assign_density(void *handle, const chui_treepm_sources *sources, double *density,
+                           int memory, void *stream);
+
+/* Base mesh cell per axis of each particle's assignment stencil after the
+ * periodic wrap (makeAxisStencil / wrapIndex, pm_solver.cpp:103-116, :925-951):
+ * cells[3*i + a]. The parity check on cell indices uses this. */
+int chui_pm_cells(void *handle, const chui_treepm_sources *sources, int64_t *cells, int memory,
+                  void *stream);
+
+/* Tree parity dump after the last solve (TreeGravitySolver::nodes() and
+ * ::ordering(), tree_gravity.hpp:195-198; unwrapped coordinates and anchors of
+ * tree_pm_coupling.cpp:3183-3194). Host memory. Pass NULL for unwanted arrays.
+ * node arrays hold node_count entries (child_index 8 per node). */
+typedef struct {
+  double *center_x, *center_y, *center_z, *half_size, *mass, *com_x, *com_y, *com_z;
+  double *quad_xx, *quad_xy, *quad_xz, *quad_yy, *quad_yz, *quad_zz, *second_moment_trace;
+  uint32_t *child_count, *child_index, *particle_begin, *particle_count;
+} chui_treepm_tree_dump;
+int chui_treepm_tree_node_count(const void *handle, int64_t *node_count);
+int chui_treepm_dump_tree(void *handle, const chui_treepm_tree_dump *dump);
+
+/* Particle-level parity dump after the last solve of n sources: unwrapped
+ * tree-frame coordinates (m_tree_source_{x,y,z}_comoving), Morton keys in
+ * sorted order (TreeMortonOrdering::morton_key), the final particle order
+ * (TreeMortonOrdering::sorted_particle_index) and the three unwrap anchors
+ * (m_tree_unwrap_anchor). Host memory; NULL skips an array. */
+int chui_treepm_dump_particles(void *handle, int64_t n, double *ux, double *uy, double *uz,
+                               uint64_t *morton_key, uint32_t *sorted_particle_index,
+                               double anchors[3]);
+
+/* KDK building blocks. Kick: u <- drag*u + kick*a (applyPeculiarVelocityKick,
+ * src/workflows/gravity_runtime.cpp:3043-3059). Drift: x <- canonical(x + u*D)
+ * (src/workflows/reference_runtime_composition.cpp:49-107 with
+ * core::canonicalPeriodicPosition, include/cosmosim/core/periodic_domain.hpp:8-16),
+ * using the context's box. */
+int chui_treepm_kick(void *handle, int64_t n, double *vx, double *vy, double *vz,
+                     const double *ax, const double *ay, const double *az, double kick_factor,
+                     double drag_factor, int memory, void *stream);
+int chui_treepm_drift(void *handle, int64_t n, double *x, double *y, double *z,
+                      const double *vx, const double *vy, const double *vz, double drift_factor,
+                      int memory, void *stream);
+
+/* Non-cosmological KDK factors of CosmologicalTimeline::prepareStep without a
+ * background (src/core/time_integration.cpp:429-441): D = dt, K1 = K2 = dt/2,
+ * drag = 1. factors = {drift, kick1, kick2, drag1, drag2}. */
+int chui_treepm_kdk_factors_static(double dt, double factors[5]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHUI_TREEPM_H */

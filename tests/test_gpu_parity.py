@@ -1,0 +1,210 @@
+"""CUDA path against the reference's golden outputs and the oracle, through the
+C-ABI (chui_treepm -> libchui_treepm.so).
+
+Bars (as the build specification states them):
+- Morton keys, sort order, CIC cell indices, leaf membership: bit-exact.
+- FP64 GPU accelerations: the reference's values to FP64 round-off, with the
+  same traversal counters.
+- Mixed precision accelerations: median |da|/|a| <= 1e-4, 99th percentile
+  <= 1e-3 against the reference.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import chui_treepm as ct  # noqa: E402
+import oracle  # noqa: E402
+from conftest import golden_params, load_golden  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["lattice16_cic", "clustered_tsc", "rect_active", "two_body", "quasi24", "duplicates", "config32"]
+COUNTER_KEYS = ("visited_nodes", "accepted_nodes", "opened_nodes", "direct_pair_evaluations",
+                "cutoff_pruned_nodes", "cutoff_skipped_pairs", "accepted_internal_multipoles", "accepted_leaves")
+
+
+def cfg_for(g, precision):
+    asmth, rcut, theta, gconst, eps = (float(v) for v in g["params"])
+    leaf, scheme, deconv, criterion, order = (int(v) for v in g["iparams"])
+    mesh = [int(v) for v in g["mesh"]]
+    return ct.TreePmConfig(pm_grid_nx=mesh[0], pm_grid_ny=mesh[1], pm_grid_nz=mesh[2], box_x=float(g["box"][0]),
+                           box_y=float(g["box"][1]), box_z=float(g["box"][2]), asmth_cells=asmth, rcut_cells=rcut,
+                           opening_theta=theta, opening_criterion=criterion, multipole_order=order,
+                           max_leaf_size=leaf, assignment_scheme=scheme, window_deconvolution=deconv,
+                           gravitational_constant=gconst, softening=eps, precision=precision)
+
+
+def _active(g):
+    return g["active"] if len(g["active"]) else None
+
+
+def rel_err(got, ref):
+    g = np.stack(got)
+    r = np.stack(ref)
+    den = np.linalg.norm(r, axis=0)
+    scale = max(np.median(den), 1e-300)
+    return np.linalg.norm(g - r, axis=0) / np.maximum(den, 1e-6 * scale)
+
+
+@pytest.fixture(scope="module")
+def cuda_ok():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return True
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("precision", [ct._abi.FP64, ct._abi.MIXED])
+def test_tree_bit_exact(cuda_ok, name, precision):
+    g = load_golden(name)
+    with ct.TreePmCoordinator(cfg_for(g, precision)) as s:
+        s.solve_active_set(g["x"], g["y"], g["z"], g["m"], active=_active(g))
+        t = s.dump_tree(len(g["x"]))
+    for a, key in enumerate(("ux", "uy", "uz")):
+        assert np.array_equal(t[key], g[key]), key
+    assert np.array_equal(t["anchors"], g["anchors"])
+    assert t["n_nodes"] == len(g["half"])
+    assert np.array_equal(t["morton_key"], g["morton_key"])
+    assert np.array_equal(t["sorted_index"], g["sorted_index"])
+    for k in ("particle_begin", "particle_count", "child_count", "child_index"):
+        assert np.array_equal(t[k], g[k]), k
+    for mine, ref in (("center_x", "center_x"), ("center_y", "center_y"), ("center_z", "center_z"),
+                      ("half_size", "half")):
+        assert np.array_equal(t[mine], g[ref]), mine
+    np.testing.assert_allclose(t["mass"], g["mass"], rtol=1e-13, atol=1e-14 * g["mass"].max())
+    for mine, ref in (("com_x", "com_x"), ("com_y", "com_y"), ("com_z", "com_z")):
+        np.testing.assert_allclose(t[mine], g[ref], rtol=1e-13, atol=1e-13 * np.abs(g[ref]).max())
+    qs = max(np.abs(g["trace"]).max(), 1e-300)
+    for mine, ref in (("quad_xx", "qxx"), ("quad_xy", "qxy"), ("quad_zz", "qzz"), ("second_moment_trace", "trace")):
+        assert np.abs(t[mine] - g[ref]).max() <= 1e-11 * qs, mine
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_matches_reference(cuda_ok, name):
+    g = load_golden(name)
+    act = _active(g)
+    with ct.TreePmCoordinator(cfg_for(g, ct._abi.FP64)) as s:
+        r = s.solve_active_set(g["x"], g["y"], g["z"], g["m"], active=act, long_range=True, short_range=True,
+                               nearest_pair=True)
+    scale = np.abs(np.concatenate([g["ax"], g["ay"], g["az"]])).max()
+    for k in ("ax", "ay", "az"):
+        assert np.abs(r[k] - g[k]).max() <= 1e-9 * scale, k
+    pscale = np.abs(np.concatenate([g["pm_ax"], g["pm_ay"], g["pm_az"]])).max()
+    for k in ("pm_ax", "pm_ay", "pm_az"):
+        assert np.abs(r[k] - g[k]).max() <= 1e-9 * pscale, k
+    rows = act if act is not None else np.arange(len(g["x"]))
+    for k in ("tree_ax", "tree_ay", "tree_az"):
+        assert np.abs(r[k][rows] - g[k][rows]).max() <= 1e-9 * scale, k
+    near = g["nearest_r2"][rows]
+    fin = np.isfinite(near)
+    assert np.array_equal(np.isfinite(r["nearest_r2"][rows]), fin)
+    np.testing.assert_allclose(r["nearest_r2"][rows][fin], near[fin], rtol=1e-12)
+    st = r["stats"]
+    assert [st[k] for k in COUNTER_KEYS] == [int(v) for v in g["counters"]]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_precision_matches_reference(cuda_ok, name):
+    g = load_golden(name)
+    act = _active(g)
+    with ct.TreePmCoordinator(cfg_for(g, ct._abi.MIXED)) as s:
+        r = s.solve_active_set(g["x"], g["y"], g["z"], g["m"], active=act)
+    e = rel_err([r["ax"], r["ay"], r["az"]], [g["ax"], g["ay"], g["az"]])
+    assert np.median(e) <= 1e-4, np.median(e)
+    assert np.percentile(e, 99) <= 1e-3, np.percentile(e, 99)
+
+
+def test_cic_cells_and_density_bit_exact(cuda_ok):
+    for name in ("lattice16_cic", "clustered_tsc", "rect_active"):
+        g = load_golden(name)
+        p = golden_params(g)
+        with ct.TreePmCoordinator(cfg_for(g, ct._abi.FP64)) as s:
+            cells = s.cells(g["x"], g["y"], g["z"])
+            rho = s.assign_density(g["x"], g["y"], g["z"], g["m"])
+        assert np.array_equal(cells, oracle.pm_cells(g["x"], g["y"], g["z"], p)), name
+        np.testing.assert_allclose(rho, g["density"], rtol=0, atol=1e-12 * np.abs(g["density"]).max())
+
+
+@pytest.mark.parametrize("name", ["lattice16_cic", "config32"])
+def test_kdk_step_matches_reference(cuda_ok, name):
+    g = load_golden(name)
+    drift, k1, k2, d1, d2 = (float(v) for v in g["kdk_factors"])
+    dev = torch.device("cuda:0")
+    t = {k: torch.tensor(g[k], device=dev) for k in ("x", "y", "z", "m", "vx", "vy", "vz")}
+    with ct.TreePmCoordinator(cfg_for(g, ct._abi.FP64)) as s:
+        r = s.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+        s.kick(t["vx"], t["vy"], t["vz"], r["ax"], r["ay"], r["az"], k1, d1)
+        s.drift(t["x"], t["y"], t["z"], t["vx"], t["vy"], t["vz"], drift)
+        x = t["x"].cpu().numpy()
+        np.testing.assert_allclose(x, g["kdk_x"], rtol=0, atol=1e-12 * float(g["box"][0]))
+        r2 = s.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+        s.kick(t["vx"], t["vy"], t["vz"], r2["ax"], r2["ay"], r2["az"], k2, d2)
+    vs = np.abs(g["kdk_vx"]).max()
+    for k in ("vx", "vy", "vz"):
+        assert np.abs(t[k].cpu().numpy() - g["kdk_" + k]).max() <= 1e-9 * vs, k
+
+
+def test_device_and_host_paths_agree(cuda_ok):
+    g = load_golden("clustered_tsc")
+    dev = torch.device("cuda:0")
+    with ct.TreePmCoordinator(cfg_for(g, ct._abi.MIXED)) as s:
+        h = s.solve_active_set(g["x"], g["y"], g["z"], g["m"])
+        d = s.solve_active_set(*(torch.tensor(g[k], device=dev) for k in ("x", "y", "z", "m")))
+    for k in ("ax", "ay", "az"):
+        np.testing.assert_allclose(d[k].cpu().numpy(), h[k], rtol=1e-6, atol=1e-9 * np.abs(h[k]).max())
+
+
+def test_explicit_targets_match_oracle_walk(cuda_ok):
+    """Explicit target positions without source identity (reference: active
+    index UINT32_MAX, tree_pm_coupling.cpp:4459-4485) equal the FP64 solve at
+    those positions up to the self-pair the identity-less walk keeps."""
+    g = load_golden("lattice16_cic")
+    rng = np.random.default_rng(3)
+    tx, ty, tz = (rng.uniform(0, 10.0, 64) for _ in range(3))
+    with ct.TreePmCoordinator(cfg_for(g, ct._abi.FP64)) as s:
+        r = s.solve_active_set(g["x"], g["y"], g["z"], g["m"], targets=(tx, ty, tz))
+    # the same targets appended as massless sources with identity
+    x = np.concatenate([g["x"], tx])
+    y = np.concatenate([g["y"], ty])
+    z = np.concatenate([g["z"], tz])
+    m = np.concatenate([g["m"], np.zeros(64)])
+    p = golden_params(g)
+    o = oracle.treepm_solve(x, y, z, m, p, active=np.arange(len(g["x"]), len(x), dtype=np.uint32))
+    e = rel_err([r["ax"], r["ay"], r["az"]], [o["ax"], o["ay"], o["az"]])
+    assert np.max(e) < 1e-9
+
+
+def test_errors_follow_reference_semantics(cuda_ok):
+    g = load_golden("lattice16_cic")
+    cfg = cfg_for(g, ct._abi.MIXED)
+    with ct.TreePmCoordinator(cfg) as s:
+        bad = g["x"].copy()
+        bad[5] = np.nan
+        with pytest.raises(ValueError, match="finite"):
+            s.solve_active_set(bad, g["y"], g["z"], g["m"])
+        neg = g["m"].copy()
+        neg[3] = -1.0
+        with pytest.raises(ValueError, match="non-negative"):
+            s.solve_active_set(g["x"], g["y"], g["z"], neg)
+        with pytest.raises(IndexError, match="active index"):
+            s.solve_active_set(g["x"], g["y"], g["z"], g["m"], active=np.array([0, len(g["x"])], dtype=np.uint32))
+    with ct.TreePmCoordinator(cfg) as s2:
+        with pytest.raises(RuntimeError, match="reuse"):
+            s2.solve_active_set_with_pm_cadence(g["x"], g["y"], g["z"], g["m"], False)
+        s2.solve_active_set(g["x"], g["y"], g["z"], g["m"])
+        r = s2.solve_active_set_with_pm_cadence(g["x"], g["y"], g["z"], g["m"], False)
+        assert np.isfinite(r["ax"]).all()
+    big = cfg_for(g, ct._abi.MIXED)
+    big.rcut_cells = 16.0
+    with pytest.raises(ValueError, match="cutoff_radius_comoving"):
+        ct.TreePmCoordinator(big)
+
+
+def test_uniform_mass_lane_matches_explicit_masses(cuda_ok):
+    g = load_golden("config32")
+    with ct.TreePmCoordinator(cfg_for(g, ct._abi.MIXED)) as s:
+        a = s.solve_active_set(g["x"], g["y"], g["z"], g["m"])
+        b = s.solve_active_set(g["x"], g["y"], g["z"], None, uniform_mass=float(g["m"][0]))
+    for k in ("ax", "ay", "az"):
+        np.testing.assert_allclose(a[k], b[k], rtol=1e-6, atol=1e-7 * np.abs(a[k]).max())

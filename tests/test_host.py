@@ -1,0 +1,113 @@
+"""Host-side checks that need no GPU: the C-ABI library exports every entry
+point include/chui_treepm.h declares, the `.param.txt` knob mapping, the
+synthetic IC generators and the FP32 kernel polynomial."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import chui_treepm as ct
+from chui_treepm import _abi, ics
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", fn)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names += re.findall(r"\b(chui_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _abi.load()
+    names = declared_functions()
+    assert len(names) >= 14
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_abi.EXPORTED) | (set(names) - set(_abi.EXPORTED))
+
+
+def test_config_defaults_match_reference_defaults():
+    c = _abi.Config()
+    assert _abi.load().chui_treepm_config_default(c) == 0
+    assert (c.pm_grid_nx, c.asmth_cells, c.rcut_cells, c.opening_theta, c.max_leaf_size) == (16, 1.25, 6.25, 0.7, 16)
+    assert c.opening_criterion == _abi.OPEN_COM_DISTANCE and c.multipole_order == 2
+
+
+def test_kdk_static_factors():
+    assert ct.kdk_factors_static(0.2) == (0.2, 0.1, 0.1, 1.0, 1.0)
+    with pytest.raises(ValueError):
+        ct.kdk_factors_static(-1.0)
+
+
+DECK = """
+schema_version = 1
+[cosmology]
+box_size_x = 20 mpc
+box_size_y = 20 mpc
+box_size_z = 20 mpc
+[numerics]
+gravity_softening = 15 kpc
+treepm_pm_grid_nx = 32
+treepm_pm_grid_ny = 32
+treepm_pm_grid_nz = 32
+treepm_asmth_cells = 1.25
+treepm_rcut_cells = 6.25
+treepm_tree_opening_criterion = geometric
+treepm_tree_opening_theta = 0.6
+treepm_tree_max_leaf_size = 32
+treepm_assignment_scheme = cic
+treepm_enable_window_deconvolution = false
+"""
+
+
+def test_param_deck_mapping():
+    c = ct.config_from_param_text(DECK)
+    assert (c.pm_grid_nx, c.box_x, c.opening_theta, c.max_leaf_size) == (32, 20.0, 0.6, 32)
+    assert c.opening_criterion == _abi.OPEN_GEOMETRIC and c.assignment_scheme == _abi.CIC
+    assert c.window_deconvolution == 0
+    assert abs(c.softening - 0.015) < 1e-15
+    assert abs(c.mesh_spacing - 20.0 / 32) < 1e-12
+    with pytest.raises(ValueError):
+        ct.config_from_param_text(DECK.replace("geometric", "bogus"))
+
+
+def test_zeldovich_lattice_statistics():
+    x, y, z, vx, vy, vz = ics.zeldovich_lattice(16, 10.0, 0.2, seed=5)
+    assert len(x) == 16 ** 3 and x.min() >= 0 and x.max() < 10.0
+    spacing = 10.0 / 16
+    rms = np.sqrt(np.mean(vx ** 2 + vy ** 2 + vz ** 2))
+    assert abs(rms - 0.2 * spacing) < 1e-9
+    x2, *_ = ics.zeldovich_lattice(16, 10.0, 0.2, seed=5)
+    assert np.array_equal(x, x2)
+
+
+def test_clustered_box_counts():
+    x, y, z, vx, vy, vz = ics.clustered_box(20000, 100.0, 0.4, 30, 3.0, 0.5, seed=2)
+    assert len(x) == 20000
+    assert np.all((x >= 0) & (x < 100.0)) and np.all((z >= 0) & (z < 100.0))
+
+
+def test_fp32_kernel_polynomial_accuracy():
+    """The per-configuration FP32 fit of H(t) = L(q)/q^3 (the Gaussian long-range
+    coefficient of tree_pm_split_kernel.hpp:109-128) is accurate to 1e-6."""
+    from scipy.special import erf
+    t_cut = (6.25 / 2.5) ** 2
+    t = np.linspace(1e-3, t_cut, 1000)
+    q = np.sqrt(t)
+    h_ref = (erf(q) - 2 * q * np.exp(-t) / np.sqrt(np.pi)) / (t * q)
+    # same construction as the library: Chebyshev interpolation on [0, t_cut]
+    m = 12
+    k = np.arange(m)
+    xk = np.cos(np.pi * (k + 0.5) / m)
+    tk = (xk + 1) * 0.5 * t_cut
+    qk = np.sqrt(tk)
+    fk = (erf(qk) - 2 * qk * np.exp(-tk) / np.sqrt(np.pi)) / (tk * qk)
+    cheb = np.polynomial.chebyshev.chebfit(xk, fk, m - 1)
+    approx = np.polynomial.chebyshev.chebval(2 * t / t_cut - 1, cheb)
+    assert np.max(np.abs(approx - h_ref) / h_ref) < 1e-6
