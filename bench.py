@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""TreePM benchmark: particle-forces/s of the mixed-precision TreePM on one B200,
+next to the same solver in FP64 on the GPU and the reference's CPU TreePM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
+
+Workload (default "clustered256"): 256^3 = 16,777,216 equal-mass particles in a
+periodic box of 200 Mpc/h; 50% in 2000 NFW halos (log-uniform masses over 3
+decades, concentrations U[4,12], R_vir ~ M^(1/3)), the rest a Zel'dovich-displaced
+lattice (0.5 spacing rms, P(k) ~ k^-2); PM mesh 256^3, r_s = 1.25 cells,
+r_cut = 6.25 cells, theta = 0.6, leaf 16, CIC with window deconvolution,
+Plummer epsilon 1 kpc/h, strict reference acceptance. Synthetic, seeded inputs
+stand in for the reference's external HDF5 initial conditions.
+
+A step is one KDK step: kick with the previous force, drift + periodic wrap,
+one full TreePM force evaluation (PM refresh, tree build, residual walk), kick.
+`value` counts particle forces (N per step) over the device-timed region with
+inputs resident in HBM; `e2e` times the public C-ABI call with host buffers
+(pinned), host<->device copies inside the region. Positions (400 MB) exceed L2
+(126 MB), so no flush is needed between steps.
+
+Under torchrun with N > 1 every rank runs an independent replica (the force
+does not shard here), timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "chui-dev_b200"))
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    "clustered256": dict(n_side=256, box=200.0, halo_fraction=0.5, n_halos=2000, mass_decades=3.0,
+                         lattice_rms=0.5, mesh=256, theta=0.6, leaf=16, eps=0.001),
+    "clustered128": dict(n_side=128, box=100.0, halo_fraction=0.4, n_halos=300, mass_decades=3.0,
+                         lattice_rms=0.5, mesh=128, theta=0.5, leaf=16, eps=0.001),
+    "lattice32": dict(n_side=32, box=10.0, halo_fraction=0.0, n_halos=0, mass_decades=0.0,
+                      lattice_rms=0.2, mesh=64, theta=0.5, leaf=16, eps=0.0),
+}
+METRIC = "particle-forces/s at 256^3 (mixed precision TreePM, one KDK step per step)"
+UNIT = "particle-forces/s"
+# FP32 operations per direct pair of the mixed walk (csrc/walk.cu): separation
+# 3, r^2 5, t 1, H(t) polynomial 2*terms (12 terms), softening 1, rsqrt 1,
+# r^-3 2, residual 2, G*m*K 2, accumulate 6 -> 47; node visit and multipole
+# work are counted separately (FP64 decisions).
+FLOPS_PER_PAIR = 47.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_particles(w: dict, seed: int):
+    from chui_treepm import ics
+    n = w["n_side"] ** 3
+    if w["n_halos"] == 0:
+        x, y, z, vx, vy, vz = ics.zeldovich_lattice(w["n_side"], w["box"], w["lattice_rms"], seed)
+    else:
+        x, y, z, vx, vy, vz = ics.clustered_box(n, w["box"], w["halo_fraction"], w["n_halos"],
+                                                w["mass_decades"], w["lattice_rms"], seed)
+    m = np.full(n, 1.0 / n)
+    return x, y, z, m, vx, vy, vz
+
+
+def make_config(w: dict, precision: int, device: int):
+    import chui_treepm as ct
+    return ct.TreePmConfig(pm_grid_nx=w["mesh"], pm_grid_ny=w["mesh"], pm_grid_nz=w["mesh"], box_x=w["box"],
+                           box_y=w["box"], box_z=w["box"], asmth_cells=1.25, rcut_cells=6.25,
+                           opening_theta=w["theta"], max_leaf_size=w["leaf"], assignment_scheme=ct._abi.CIC,
+                           window_deconvolution=1, gravitational_constant=1.0, softening=w["eps"],
+                           precision=precision, device=device)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.lines: list[str] = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[3:7]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def rel_errors(a, b):
+    num = np.sqrt((a[0] - b[0]) ** 2 + (a[1] - b[1]) ** 2 + (a[2] - b[2]) ** 2)
+    den = np.sqrt(b[0] ** 2 + b[1] ** 2 + b[2] ** 2)
+    return num / np.maximum(den, 1e-300)
+
+
+def gpu_step(solver, t, acc, factors, stream):
+    d, k1, k2, g1, g2 = factors
+    solver.kick(t["vx"], t["vy"], t["vz"], acc["ax"], acc["ay"], acc["az"], k1, g1, stream=stream)
+    solver.drift(t["x"], t["y"], t["z"], t["vx"], t["vy"], t["vz"], d, stream=stream)
+    r = solver.solve_active_set(t["x"], t["y"], t["z"], t["m"], stream=stream)
+    solver.kick(t["vx"], t["vy"], t["vz"], r["ax"], r["ay"], r["az"], k2, g2, stream=stream)
+    return r
+
+
+def timed_steps(torch, solver, t, acc, factors, steps, warmup):
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(warmup):
+        acc = gpu_step(solver, t, acc, factors, stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    walk_ms = []
+    stats = []
+    e0.record()
+    for _ in range(steps):
+        acc = gpu_step(solver, t, acc, factors, stream)
+        st = solver.last_stats
+        stats.append(st)
+        walk_ms.append(st["walk_ms"])
+        launches += st["kernel_launches"] + 3  # + kick, drift, kick
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), acc, stats, launches
+
+
+def run_gpu(args) -> int:
+    import torch
+    import chui_treepm as ct
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    t0 = time.time()
+    x, y, z, m, vx, vy, vz = make_particles(w, seed=42 + rank)
+    n = len(x)
+    log(f"[rank {rank}] particles {n} generated in {time.time() - t0:.1f}s")
+    t = {k: torch.tensor(v, device=dev) for k, v in dict(x=x, y=y, z=z, m=m, vx=vx, vy=vy, vz=vz).items()}
+    factors = ct.kdk_factors_static(args.dt)
+
+    mixed = ct.TreePmCoordinator(make_config(w, ct._abi.MIXED, local))
+    fp64 = ct.TreePmCoordinator(make_config(w, ct._abi.FP64, local))
+
+    # accuracy of mixed against FP64 on the initial state
+    r_m = mixed.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+    r_d = fp64.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+    err = rel_errors([r_m[k].cpu().numpy() for k in ("ax", "ay", "az")],
+                     [r_d[k].cpu().numpy() for k in ("ax", "ay", "az")])
+    stats0 = dict(mixed.last_stats)
+    log(f"[rank {rank}] mixed vs fp64 median {np.median(err):.3e} p99 {np.percentile(err, 99):.3e}; "
+        f"stats {stats0}")
+
+    # FP64-on-GPU comparator (same step definition, fewer repetitions)
+    tf = {k: v.clone() for k, v in t.items()}
+    fp64_ms, _, _, _ = timed_steps(torch, fp64, tf, r_d, factors, max(1, args.fp64_steps), 1)
+    fp64_value = n * max(1, args.fp64_steps) / (fp64_ms * 1e-3)
+    del tf
+    fp64.close()
+    torch.cuda.empty_cache()
+
+    # headline: mixed precision, device-resident inputs
+    with ClockSampler(local) as clocks:
+        ms, acc, stats, launches = timed_steps(torch, mixed, t, r_m, factors, args.steps, args.warmup)
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = n * args.steps * world / (ms * 1e-3)
+
+    # end to end through the C-ABI with pinned host buffers
+    hx = torch.from_numpy(x).pin_memory().numpy()
+    hy = torch.from_numpy(y).pin_memory().numpy()
+    hz = torch.from_numpy(z).pin_memory().numpy()
+    hm = torch.from_numpy(m).pin_memory().numpy()
+    mixed.solve_active_set(hx, hy, hz, hm)  # warm
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        mixed.solve_active_set(hx, hy, hz, hm)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - w0
+    e2e_value = n * e2e_steps / e2e_s
+    if dist is not None:
+        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_value = n * e2e_steps * world / float(tt.item())
+
+    # roofline of the dominant kernel (residual walk, FP32 pipes)
+    peak = ct.probe_fp32_peak_tflops(local)
+    st = stats[-1]
+    walk_flops = FLOPS_PER_PAIR * st["direct_pair_evaluations"]
+    achieved = walk_flops / (st["walk_ms"] * 1e-3) / 1e12
+    mixed.close()
+
+    if rank == 0:
+        result = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 pair/mesh arithmetic, f64 positions/decisions/COM",
+            "data": "synthetic (seeded NFW halos + Zel'dovich lattice)",
+            "config": {"workload": f"{args.workload}: N={n}, L={w['box']} Mpc/h, mesh {w['mesh']}^3, "
+                                   f"r_s=1.25 cells, r_cut=6.25 cells, theta={w['theta']}, leaf {w['leaf']}, "
+                                   f"CIC+deconvolution, eps={w['eps']}",
+                       "particles": n, "l2": "inputs larger than L2 (positions 400 MB)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "accuracy_vs_fp64_gpu": {"median_rel": float(np.median(err)),
+                                     "p99_rel": float(np.percentile(err, 99)),
+                                     "max_rel": float(np.max(err))},
+            "fp64_gpu": {"value": fp64_value, "unit": UNIT, "steps": max(1, args.fp64_steps),
+                         "speedup_mixed_over_fp64": value / world / fp64_value},
+            "phases_ms": {k: st[k] for k in ("pm_ms", "tree_build_ms", "walk_ms", "total_ms")},
+            "counters": {k: st[k] for k in ("direct_pair_evaluations", "visited_nodes",
+                                            "accepted_internal_multipoles", "node_count", "maximum_depth")},
+            "adjoint": None,
+            "roofline": {"bound": "fp32", "kernel": "walkKernel<mixed>", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": "measured FP32 FFMA probe (chui_treepm_probe_fp32_peak)",
+                         "flops_per_pair": FLOPS_PER_PAIR, "traffic": None},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 32,
+                    "d2h_bytes_per_step": n * 24, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        if args.cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(w, x, y, z, m, args)
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_baseline(w, x, y, z, m, args) -> dict | None:
+    """The reference's own TreePM (oracle/_ref/treepm_ref, built from its
+    sources) on the host cores: full PM + tree build, residual walk on a seeded
+    1/64 target subset scaled to all N targets."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refio
+    if not refio.available():
+        return None
+    n = len(x)
+    frac = args.cpu_fraction
+    rng = np.random.default_rng(7)
+    k = max(1, int(n * frac))
+    act = np.sort(rng.choice(n, k, replace=False)).astype(np.uint32)
+    p = refio.RefProblem(x, y, z, m, box=(w["box"],) * 3, mesh=(w["mesh"],) * 3, theta=w["theta"], leaf=w["leaf"],
+                         eps=w["eps"], deconv=1, active=act, dump_tree=0)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    r = refio.run(p, threads=cores)
+    wall = time.perf_counter() - t0
+    total = r["first_ms"]
+    fixed = r["pm_ms"] + r["build_ms"]
+    walk = max(total - fixed, 0.0)
+    est_ms = fixed + walk * (n / k)
+    return {"value": n / (est_ms * 1e-3), "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"full PM ({w['mesh']}^3, FFT via the repo's FFTW-API shim) + full tree build, "
+                      f"walk on {k} seeded targets ({frac:.4f} of N) scaled by N/{k}",
+            "phases_ms": {"pm": r["pm_ms"], "tree_build": r["build_ms"], "walk_sample": walk,
+                          "walk_scaled": walk * n / k},
+            "process_wall_s": wall}
+
+
+def run_reference(args) -> int:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refio
+    w = WORKLOADS[args.workload]
+    if not refio.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle binary oracle/_ref/treepm_ref "
+                                                              "not built (needs the reference sources)"}))
+        return 0
+    x, y, z, m, vx, vy, vz = make_particles(w, seed=42)
+    n = len(x)
+    values = []
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(w, x, y, z, m, args)
+        if i >= args.warmup:
+            values.append(cb["value"])
+    value = statistics.median(values)
+    cb["value"] = value
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded NFW halos + Zel'dovich lattice)",
+        "config": {"workload": args.workload, "particles": n},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="clustered256", choices=sorted(WORKLOADS))
+    ap.add_argument("--dt", type=float, default=1.0e-3)
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64.0)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        args.steps = min(args.steps, 1) if args.workload == "clustered256" else args.steps
+        args.warmup = 0 if args.workload == "clustered256" else args.warmup
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -40,7 +40,7 @@ class Stats(C.Structure):
         ("cutoff_skipped_pairs", C.c_uint64), ("accepted_internal_multipoles", C.c_uint64),
         ("accepted_leaves", C.c_uint64), ("node_count", C.c_uint64), ("maximum_depth", C.c_uint32),
         ("path_words", C.c_uint32), ("pm_ms", C.c_double), ("tree_build_ms", C.c_double),
-        ("walk_ms", C.c_double), ("total_ms", C.c_double),
+        ("walk_ms", C.c_double), ("total_ms", C.c_double), ("kernel_launches", C.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -78,7 +78,7 @@ EXPORTED = (
     "chui_treepm_set_config", "chui_treepm_last_error", "chui_treepm_solve",
     "chui_pm_assign_density", "chui_pm_cells", "chui_treepm_tree_node_count",
     "chui_treepm_dump_tree", "chui_treepm_dump_particles", "chui_treepm_kick", "chui_treepm_drift",
-    "chui_treepm_kdk_factors_static",
+    "chui_treepm_kdk_factors_static", "chui_treepm_probe_fp32_peak",
 )
 
 _lib = None
@@ -112,6 +112,7 @@ def load(path: str | None = None):
     L.chui_treepm_kick.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, vp]
     L.chui_treepm_drift.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp, C.c_double, C.c_int, vp]
     L.chui_treepm_kdk_factors_static.argtypes = [C.c_double, vp]
+    L.chui_treepm_probe_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     for name in EXPORTED:
         fn = getattr(L, name)
         if fn.restype is C.c_int or name not in ("chui_treepm_destroy", "chui_treepm_last_error"):

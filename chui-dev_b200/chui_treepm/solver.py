@@ -154,7 +154,8 @@ class TreePmCoordinator:
         h = C.c_void_p()
         rc = self._lib.chui_treepm_create(C.byref(config.to_c()), C.byref(h))
         if rc != 0:
-            raise _ERRORS.get(rc, TreePmError)(rc, f"chui_treepm_create failed ({rc})")
+            msg = self._lib.chui_treepm_last_error(None).decode()
+            raise _ERRORS.get(rc, TreePmError)(rc, msg or f"chui_treepm_create failed ({rc})")
         self._h = h
         self.last_stats: dict = {}
 
@@ -302,7 +303,7 @@ class TreePmCoordinator:
         return r
 
     # -- KDK ------------------------------------------------------------------
-    def kick(self, vx, vy, vz, ax, ay, az, kick_factor: float, drag_factor: float = 1.0):
+    def kick(self, vx, vy, vz, ax, ay, az, kick_factor: float, drag_factor: float = 1.0, stream=None):
         arr = _Arrays(vx)
         if not arr.device:
             for v in (vx, vy, vz):
@@ -310,9 +311,10 @@ class TreePmCoordinator:
                     raise InvalidArgument(_abi.EINVAL, "kick updates contiguous float64 arrays in place")
         ps = [arr.ptr(a, np.float64) for a in (vx, vy, vz, ax, ay, az)]
         self._check(self._lib.chui_treepm_kick(self._h, len(vx), *[C.c_void_p(p) for p in ps], kick_factor,
-                                               drag_factor, _abi.DEVICE if arr.device else _abi.HOST, None))
+                                               drag_factor, _abi.DEVICE if arr.device else _abi.HOST,
+                                               C.c_void_p(stream) if stream else None))
 
-    def drift(self, x, y, z, vx, vy, vz, drift_factor: float):
+    def drift(self, x, y, z, vx, vy, vz, drift_factor: float, stream=None):
         arr = _Arrays(x)
         if not arr.device:
             for v in (x, y, z):
@@ -320,7 +322,17 @@ class TreePmCoordinator:
                     raise InvalidArgument(_abi.EINVAL, "drift updates contiguous float64 arrays in place")
         ps = [arr.ptr(a, np.float64) for a in (x, y, z, vx, vy, vz)]
         self._check(self._lib.chui_treepm_drift(self._h, len(x), *[C.c_void_p(p) for p in ps], drift_factor,
-                                                _abi.DEVICE if arr.device else _abi.HOST, None))
+                                                _abi.DEVICE if arr.device else _abi.HOST,
+                                                C.c_void_p(stream) if stream else None))
+
+
+def probe_fp32_peak_tflops(device: int = 0) -> float:
+    """Measured FP32 FMA throughput of the GPU (the walk's roofline denominator)."""
+    v = C.c_double()
+    rc = _abi.load().chui_treepm_probe_fp32_peak(device, C.byref(v))
+    if rc != 0:
+        raise DeviceError(rc, "FP32 peak probe failed")
+    return v.value
 
 
 def kdk_factors_static(dt: float):

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -33,6 +34,12 @@ void release(DevBuf& b) {
   b.ptr = nullptr;
   b.bytes = 0;
 }
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+void noteLaunch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launchCount() { return g_launches.load(std::memory_order_relaxed); }
 
 const char* statusText(uint32_t bits) {
   if (bits & kStatusStackOverflow) return "TreePM residual traversal stack overflow";
@@ -338,8 +345,8 @@ int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const 
   cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(c.status.ptr, 0, 4, s);
   if (n > 0)
-    sourceReduceKernel<<<gridFor(n, 256), 256, 0, s>>>(n, x, y, z, m, sc, reinterpret_cast<double*>(sc + 6),
-                                                       c.status.as<uint32_t>());
+    { noteLaunch(); sourceReduceKernel<<<gridFor(n, 256), 256, 0, s>>>(n, x, y, z, m, sc, reinterpret_cast<double*>(sc + 6),
+                                                       c.status.as<uint32_t>()); }
   unsigned long long hb[8];
   uint32_t st = 0;
   cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);
@@ -359,6 +366,11 @@ int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const 
 }  // namespace chui
 
 using chui::Context;
+
+namespace {
+// Text of the last failed chui_treepm_create on this thread (no handle exists).
+thread_local std::string g_create_error;
+}  // namespace
 
 extern "C" {
 
@@ -388,19 +400,33 @@ int chui_treepm_create(const chui_treepm_config* cfg, void** handle) {
   *handle = nullptr;
   std::string err;
   int rc = chui::validateConfig(*cfg, err);
-  if (rc) return rc;
+  if (rc) {
+    g_create_error = err;
+    return rc;
+  }
   int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return CHUI_TREEPM_EDEVICE;
-  if (cfg->device < 0 || cfg->device >= ndev) return CHUI_TREEPM_EINVAL;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    g_create_error = "no CUDA device is available";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) {
+    g_create_error = "device ordinal out of range";
+    return CHUI_TREEPM_EINVAL;
+  }
   Context* c = new (std::nothrow) Context();
-  if (!c) return CHUI_TREEPM_ENOMEM;
+  if (!c) {
+    g_create_error = "context allocation failed";
+    return CHUI_TREEPM_ENOMEM;
+  }
   c->device = cfg->device;
   chui::DeviceGuard guard(c->device);
   chui::applyConfig(*c, *cfg);
   if (chui::ensure(c->status, 64) != cudaSuccess || chui::ensure(c->scalars, 64 * 8) != cudaSuccess) {
     delete c;
+    g_create_error = "device allocation failed";
     return CHUI_TREEPM_ENOMEM;
   }
+  g_create_error.clear();
   for (auto& e : c->ev) cudaEventCreate(&e);
   c->events_ready = true;
   *handle = c;
@@ -457,7 +483,7 @@ int chui_treepm_set_config(void* handle, const chui_treepm_config* cfg) {
 }
 
 const char* chui_treepm_last_error(const void* handle) {
-  if (!handle) return "null handle";
+  if (!handle) return g_create_error.c_str();
   return static_cast<const Context*>(handle)->last_error.c_str();
 }
 
@@ -507,6 +533,7 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
 
   chui::DeviceGuard guard(c.device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint64_t launches_before = chui::launchCount();
   cudaEventRecord(c.ev[0], s);
   int rc;
   const double *x, *y, *z, *m, *tx = nullptr, *ty = nullptr, *tz = nullptr;
@@ -535,8 +562,8 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   }
   if (active && nt > 0) {
     cudaMemsetAsync(c.status.ptr, 0, 4, s);
-    chui::activeCheckKernel<<<chui::gridFor(nt, 256), 256, 0, s>>>(nt, active, n, explicit_targets ? 1 : 0,
-                                                                  c.status.as<uint32_t>());
+    { chui::noteLaunch(); chui::activeCheckKernel<<<chui::gridFor(nt, 256), 256, 0, s>>>(nt, active, n, explicit_targets ? 1 : 0,
+                                                                  c.status.as<uint32_t>()); }
     cudaMemcpyAsync(&st, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     if (st) {
@@ -653,9 +680,9 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   }
   if ((rc = chui::pmInterpolate(c, nt, active, tx, ty, tz, x, y, z, pmx, pmy, pmz, s))) return rc;
   if (nt > 0)
-    chui::combineKernel<<<chui::gridFor(nt, 256), 256, 0, s>>>(nt, active, explicit_targets ? 0 : n, pmx, pmy, pmz,
+    { chui::noteLaunch(); chui::combineKernel<<<chui::gridFor(nt, 256), 256, 0, s>>>(nt, active, explicit_targets ? 0 : n, pmx, pmy, pmz,
                                                               c.tree_acc.as<double>(), c.tree_near.as<double>(), ax,
-                                                              ay, az, sx, sy, sz, snear);
+                                                              ay, az, sx, sy, sz, snear); }
   cudaEventRecord(c.ev[4], s);
   uint32_t walk_status = 0;
   cudaMemcpyAsync(&walk_status, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
@@ -692,6 +719,7 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   stt.node_count = static_cast<uint64_t>(c.n_nodes);
   stt.maximum_depth = c.max_depth;
   stt.path_words = static_cast<uint32_t>(c.path_words_used);
+  stt.kernel_launches = chui::launchCount() - launches_before;
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
   stt.pm_ms = ms;
@@ -846,7 +874,7 @@ int chui_treepm_kick(void* handle, int64_t n, double* vx, double* vy, double* vz
     day = c.out_acc[1].as<double>();
     daz = c.out_acc[2].as<double>();
   }
-  chui::kickKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dvx, dvy, dvz, dax, day, daz, kick_factor, drag_factor);
+  { chui::noteLaunch(); chui::kickKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dvx, dvy, dvz, dax, day, daz, kick_factor, drag_factor); }
   if (memory == CHUI_TREEPM_HOST) {
     cudaMemcpyAsync(vx, dvx, n * 8, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(vy, dvy, n * 8, cudaMemcpyDeviceToHost, s);
@@ -881,8 +909,8 @@ int chui_treepm_drift(void* handle, int64_t n, double* x, double* y, double* z, 
     dvy = c.out_acc[1].as<double>();
     dvz = c.out_acc[2].as<double>();
   }
-  chui::driftKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dx, dy, dz, dvx, dvy, dvz, drift_factor, c.cfg.box_x,
-                                                         c.cfg.box_y, c.cfg.box_z);
+  { chui::noteLaunch(); chui::driftKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dx, dy, dz, dvx, dvy, dvz, drift_factor, c.cfg.box_x,
+                                                         c.cfg.box_y, c.cfg.box_z); }
   if (memory == CHUI_TREEPM_HOST) {
     cudaMemcpyAsync(x, dx, n * 8, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(y, dy, n * 8, cudaMemcpyDeviceToHost, s);

@@ -363,16 +363,16 @@ int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const dou
   const bool mixed = isMixed(c);
   const int block = 256;
   if (mixed) {
-    fillKernel<float><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<float>(), padded,
-                                                               static_cast<float>(-mean));
+    { noteLaunch(); fillKernel<float><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<float>(), padded,
+                                                               static_cast<float>(-mean)); }
     if (n > 0)
-      depositKernel<float><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
-                                                               1.0 / cell_volume, g, c.grid[0].as<float>());
+      { noteLaunch(); depositKernel<float><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
+                                                               1.0 / cell_volume, g, c.grid[0].as<float>()); }
   } else {
-    fillKernel<double><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<double>(), padded, -mean);
+    { noteLaunch(); fillKernel<double><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<double>(), padded, -mean); }
     if (n > 0)
-      depositKernel<double><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
-                                                                1.0 / cell_volume, g, c.grid[0].as<double>());
+      { noteLaunch(); depositKernel<double><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
+                                                                1.0 / cell_volume, g, c.grid[0].as<double>()); }
   }
   cufftSetStream(c.plan_r2c, s);
   cufftSetStream(c.plan_c2r, s);
@@ -385,9 +385,9 @@ int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const dou
       c.last_error = "cuFFT R2C failed";
       return CHUI_TREEPM_EDEVICE;
     }
-    greenGradientKernel<float, cufftComplex><<<gridFor(total, block), block, 0, s>>>(
+    { noteLaunch(); greenGradientKernel<float, cufftComplex><<<gridFor(total, block), block, 0, s>>>(
         g, c.axis_tables.as<double>(), prefactor, c.rs, c.cfg.window_deconvolution,
-        c.grid[0].as<cufftComplex>(), c.grid[1].as<cufftComplex>(), c.grid[2].as<cufftComplex>());
+        c.grid[0].as<cufftComplex>(), c.grid[1].as<cufftComplex>(), c.grid[2].as<cufftComplex>()); }
     for (int a = 0; a < 3; ++a) {
       fr = cufftExecC2R(c.plan_c2r, c.grid[a].as<cufftComplex>(), c.grid[a].as<cufftReal>());
       if (fr != CUFFT_SUCCESS) {
@@ -401,10 +401,10 @@ int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const dou
       c.last_error = "cuFFT D2Z failed";
       return CHUI_TREEPM_EDEVICE;
     }
-    greenGradientKernel<double, cufftDoubleComplex><<<gridFor(total, block), block, 0, s>>>(
+    { noteLaunch(); greenGradientKernel<double, cufftDoubleComplex><<<gridFor(total, block), block, 0, s>>>(
         g, c.axis_tables.as<double>(), prefactor, c.rs, c.cfg.window_deconvolution,
         c.grid[0].as<cufftDoubleComplex>(), c.grid[1].as<cufftDoubleComplex>(),
-        c.grid[2].as<cufftDoubleComplex>());
+        c.grid[2].as<cufftDoubleComplex>()); }
     for (int a = 0; a < 3; ++a) {
       fr = cufftExecZ2D(c.plan_c2r, c.grid[a].as<cufftDoubleComplex>(), c.grid[a].as<cufftDoubleReal>());
       if (fr != CUFFT_SUCCESS) {
@@ -431,13 +431,13 @@ int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* 
   const PmGeom g = geomOf(c);
   const int block = 256;
   if (isMixed(c)) {
-    interpolateKernel<float><<<gridFor(nt, block), block, 0, s>>>(
+    { noteLaunch(); interpolateKernel<float><<<gridFor(nt, block), block, 0, s>>>(
         nt, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<float>(), c.grid[1].as<float>(),
-        c.grid[2].as<float>(), ax, ay, az);
+        c.grid[2].as<float>(), ax, ay, az); }
   } else {
-    interpolateKernel<double><<<gridFor(nt, block), block, 0, s>>>(
+    { noteLaunch(); interpolateKernel<double><<<gridFor(nt, block), block, 0, s>>>(
         nt, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<double>(), c.grid[1].as<double>(),
-        c.grid[2].as<double>(), ax, ay, az);
+        c.grid[2].as<double>(), ax, ay, az); }
   }
   if (cudaGetLastError() != cudaSuccess) {
     c.last_error = "PM interpolation launch failed";
@@ -453,9 +453,9 @@ int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const
   const int block = 256;
   if (cudaMemsetAsync(rho, 0, cells * sizeof(double), s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
   if (n > 0)
-    depositCompactKernel<<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass, g, rho);
+    { noteLaunch(); depositCompactKernel<<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass, g, rho); }
   const double cell_volume = (g.L[0] * g.L[1] * g.L[2]) / static_cast<double>(cells);
-  scaleKernel<<<gridFor(cells, block), block, 0, s>>>(rho, cells, cell_volume);
+  { noteLaunch(); scaleKernel<<<gridFor(cells, block), block, 0, s>>>(rho, cells, cell_volume); }
   if (cudaGetLastError() != cudaSuccess) {
     c.last_error = "PM density launch failed";
     return CHUI_TREEPM_EDEVICE;
@@ -466,7 +466,7 @@ int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const
 int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,
             int64_t* cells, cudaStream_t s) {
   const PmGeom g = geomOf(c);
-  if (n > 0) cellsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, x, y, z, g, cells);
+  if (n > 0) { noteLaunch(); cellsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, x, y, z, g, cells); }
   if (cudaGetLastError() != cudaSuccess) {
     c.last_error = "PM cell launch failed";
     return CHUI_TREEPM_EDEVICE;

@@ -374,7 +374,7 @@ struct NodeOut {
 __global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* __restrict__ path,
                                const int* __restrict__ cp, const uint32_t* __restrict__ counts,
                                const uint32_t* __restrict__ offset, double cx0, double cy0, double cz0,
-                               double half0, NodeOut out) {
+                               double half0, uint32_t total_nodes, NodeOut out, uint32_t* status) {
   const int64_t n = p.n;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -404,11 +404,14 @@ __global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* 
       }
       const uint32_t node = offset[i] + static_cast<uint32_t>(d - d0);
       const int64_t end = (d == 0) ? n : runEnd(path, n, words, cp, i, d, p.leaf);
+      if (node >= total_nodes || end > n || end <= i) {
+        atomicOr(status, kStatusIndexRange);
+        return;
+      }
       const uint32_t count = static_cast<uint32_t>(end - i);
       out.geom[node] = make_double4(cx, cy, cz, h);
       out.range[node] = make_uint4(static_cast<uint32_t>(i), count, 0u, offset[end]);
       out.depth[node] = static_cast<uint32_t>(d);
-      for (int o = 0; o < 8; ++o) out.child[8 * static_cast<size_t>(node) + o] = kInvalid;
       if (d == 0) {
         out.parent[node] = kInvalid;
       } else {
@@ -418,6 +421,10 @@ __global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* 
         } else {
           const int64_t s = runStart(path, n, words, cp, i, d - 1);
           parent = offset[s] + static_cast<uint32_t>((d - 1) - (cp[s] + 1));
+        }
+        if (parent >= total_nodes) {
+          atomicOr(status, kStatusIndexRange);
+          return;
         }
         out.parent[node] = parent;
         out.child[8 * static_cast<size_t>(parent) + digitAt(path, n, i, d)] = node;
@@ -707,7 +714,7 @@ static int unwrapAxis(Context& c, int64_t n, const double* in, double box, int c
   cudaMemsetAsync(bmin, 0xFF, nb * 8, s);
   cudaMemsetAsync(bmax, 0x00, nb * 8, s);
   const double scale = static_cast<double>(nb) / box;
-  wrapBucketKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in, box, canonical, out, nb, scale, bmin, bmax);
+  { noteLaunch(); wrapBucketKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in, box, canonical, out, nb, scale, bmin, bmax); }
   size_t bytes = 0;
   cub::DeviceScan::ExclusiveScan(nullptr, bytes, bmin, later, MinU64(), ~0ull, static_cast<int>(nb), s);
   if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
@@ -721,9 +728,9 @@ static int unwrapAxis(Context& c, int64_t n, const double* in, double box, int c
   auto* sc = c.scalars.as<unsigned long long>();
   unsigned long long init[2] = {0ull, ~0ull};
   cudaMemcpyAsync(sc, init, 16, cudaMemcpyHostToDevice, s);
-  bucketGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, later, box, gmin, sc, 0, sc + 1);
-  bucketGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, later, box, gmin, sc, 1, sc + 1);
-  applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out, box, sc + 1);
+  { noteLaunch(); bucketGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, later, box, gmin, sc, 0, sc + 1); }
+  { noteLaunch(); bucketGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, later, box, gmin, sc, 1, sc + 1); }
+  { noteLaunch(); applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out, box, sc + 1); }
   unsigned long long ab = 0;
   cudaMemcpyAsync(&ab, sc + 1, 8, cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
@@ -752,7 +759,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   auto* sc = c.scalars.as<unsigned long long>();
   unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
   cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
-  boundsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], sc);
+  { noteLaunch(); boundsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], sc); }
   unsigned long long hb[6];
   cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
@@ -768,8 +775,8 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   if (ensure(c.keys_a, n * 8) || ensure(c.keys_b, n * 8) || ensure(c.idx_a, n * 4) || ensure(c.idx_b, n * 4) ||
       ensure(c.idx_c, (n + 1) * 4) || ensure(c.idx_d, (n + 1) * 4))
     return CHUI_TREEPM_ENOMEM;
-  mortonKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], lo[0], lo[1], lo[2], extent,
-                                               c.keys_a.as<unsigned long long>(), c.idx_a.as<uint32_t>());
+  { noteLaunch(); mortonKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], lo[0], lo[1], lo[2], extent,
+                                               c.keys_a.as<unsigned long long>(), c.idx_a.as<uint32_t>()); }
   int rc = cubSortPairsU64(c, c.keys_a.as<unsigned long long>(), c.keys_b.as<unsigned long long>(),
                            c.idx_a.as<uint32_t>(), c.idx_b.as<uint32_t>(), n, 63, s);
   if (rc) return rc;
@@ -814,13 +821,13 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     unsigned long long* by_rank = c.keys_a.as<unsigned long long>();
     unsigned long long* key_cur = c.keys_b.as<unsigned long long>();
     unsigned long long* key_sorted = c.bucket_max.as<unsigned long long>();
-    pathKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, perm_m, u[0], u[1], u[2], cx0, cy0, cz0, half0,
-                                               by_rank);
+    { noteLaunch(); pathKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, perm_m, u[0], u[1], u[2], cx0, cy0, cz0, half0,
+                                               by_rank); }
     uint32_t* rank_in = c.idx_c.as<uint32_t>();
     uint32_t* rank_out = c.idx_d.as<uint32_t>();
-    iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in);
-    for (int w = words - 1; w >= 0; --w) {  // LSD over path words, each pass stable
-      gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in, key_cur);
+    { noteLaunch(); iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in); }
+    for (int w = words - 1; w >= 0; --w) {  { noteLaunch(); // LSD over path words, each pass stable
+      gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in, key_cur); }
       rc = cubSortPairsU64(c, key_cur, key_sorted, rank_in, rank_out, n, 63, s);
       if (rc) return rc;
       uint32_t* t = rank_in;
@@ -829,13 +836,13 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     }
     // rank_in: path position -> Morton rank
     for (int w = 0; w < words; ++w)
-      gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in,
-                                                      path + static_cast<size_t>(w) * n);
-    invertKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in, c.inv_pos.as<uint32_t>());
-    commonPrefixKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, path, cp);
+      { noteLaunch(); gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in,
+                                                      path + static_cast<size_t>(w) * n); }
+    { noteLaunch(); invertKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in, c.inv_pos.as<uint32_t>()); }
+    { noteLaunch(); commonPrefixKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, path, cp); }
     plan.depth_max = kLevelsPerWord * words;
     cudaMemsetAsync(status, 0, 4, s);
-    nodeCountKernel<<<gridFor(n + 1, 256), 256, 0, s>>>(plan, cp, counts, status);
+    { noteLaunch(); nodeCountKernel<<<gridFor(n + 1, 256), 256, 0, s>>>(plan, cp, counts, status); }
     size_t bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, bytes, counts, offset, static_cast<int>(n + 1), s);
     if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
@@ -869,12 +876,24 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   out.depth = c.node_depth.as<uint32_t>();
   out.child = c.node_child.as<uint32_t>();
   out.leaf_of_pos = c.leaf_of_pos.as<uint32_t>();
-  nodeEmitKernel<<<gridFor(n, 128), 128, 0, s>>>(plan, words, path, cp, counts, offset, cx0, cy0, cz0, half0,
-                                                 out);
-  childCountKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.child, out.range);
+  cudaMemsetAsync(out.leaf_of_pos, 0, n * 4, s);
+  cudaMemsetAsync(out.child, 0xFF, static_cast<size_t>(total_nodes) * 8 * 4, s);  // all slots empty
+  cudaMemsetAsync(status, 0, 4, s);
+  { noteLaunch(); nodeEmitKernel<<<gridFor(n, 128), 128, 0, s>>>(plan, words, path, cp, counts, offset, cx0, cy0, cz0, half0,
+                                                 total_nodes, out, status); }
+  {
+    uint32_t est = 0;
+    cudaMemcpyAsync(&est, status, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+    if (est) {
+      c.last_error = "tree node enumeration produced an inconsistent node range";
+      return CHUI_TREEPM_EDEVICE;
+    }
+  }
+  { noteLaunch(); childCountKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.child, out.range); }
   // final order: stable sort of Morton order by leaf id
   uint32_t* leaf_key = c.idx_a.as<uint32_t>();
-  leafKeyKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.inv_pos.as<uint32_t>(), out.leaf_of_pos, leaf_key);
+  { noteLaunch(); leafKeyKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.inv_pos.as<uint32_t>(), out.leaf_of_pos, leaf_key); }
   rc = cubSortPairsU32(c, leaf_key, c.idx_d.as<uint32_t>(), perm_m, c.sorted_index.as<uint32_t>(), n,
                        bitsFor(total_nodes), s);
   if (rc) return rc;
@@ -888,19 +907,19 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   mi.uniform_mass = uniform_mass;
   mi.sorted = c.sorted_index.as<uint32_t>();
   mi.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
-  momentsKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(total_nodes, mi, out.geom, out.range, out.parent,
+  { noteLaunch(); momentsKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(total_nodes, mi, out.geom, out.range, out.parent,
                                                           out.child, c.node_counter.as<uint32_t>(),
-                                                          c.node_com.as<double4>(), c.node_quad.as<double>());
+                                                          c.node_com.as<double4>(), c.node_quad.as<double>()); }
   // tree-ordered source records
   const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
   if (mixed) {
     if (ensure(c.src_f4, n * sizeof(float4))) return CHUI_TREEPM_ENOMEM;
   }
   if (ensure(c.src_d4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
-  packSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), out.leaf_of_pos, out.geom,
+  { noteLaunch(); packSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), out.leaf_of_pos, out.geom,
                                                     u[0], u[1], u[2], x, y, z, m, uniform_mass,
                                                     mixed ? c.src_f4.as<float4>() : nullptr,
-                                                    c.src_d4.as<double4>(), c.pos_of_row.as<uint32_t>());
+                                                    c.src_d4.as<double4>(), c.pos_of_row.as<uint32_t>()); }
   // maximum depth (for stack sizing and stats)
   {
     size_t bytes = 0;
@@ -927,8 +946,8 @@ int treeNodeBounds(Context& c, double lo[3], double hi[3], cudaStream_t s) {
   unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
   cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
   if (c.n_nodes > 0)
-    nodeBoundsKernel<<<gridFor(c.n_nodes, 256), 256, 0, s>>>(c.n_nodes, c.node_geom.as<double4>(),
-                                                              c.node_com.as<double4>(), sc);
+    { noteLaunch(); nodeBoundsKernel<<<gridFor(c.n_nodes, 256), 256, 0, s>>>(c.n_nodes, c.node_geom.as<double4>(),
+                                                              c.node_com.as<double4>(), sc); }
   unsigned long long hb[6];
   cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
@@ -949,8 +968,8 @@ int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explici
     return CHUI_TREEPM_ENOMEM;
   uint32_t* key = c.idx_c.as<uint32_t>();
   uint32_t* slot = c.idx_a.as<uint32_t>();
-  targetKeyKernel<<<gridFor(nt, 256), 256, 0, s>>>(nt, active, n, c.pos_of_row.as<uint32_t>(), explicit_targets,
-                                                   key, slot);
+  { noteLaunch(); targetKeyKernel<<<gridFor(nt, 256), 256, 0, s>>>(nt, active, n, c.pos_of_row.as<uint32_t>(), explicit_targets,
+                                                   key, slot); }
   return cubSortPairsU32(c, key, c.idx_d.as<uint32_t>(), slot, c.target_order.as<uint32_t>(), nt, 32, s);
 }
 

@@ -364,7 +364,7 @@ int launchWalk(const WalkArgs& args, cudaStream_t s) {
   const int64_t max_useful = (warps_needed + kWalkWarpsPerBlock - 1) / kWalkWarpsPerBlock;
   if (blocks > max_useful) blocks = max_useful;
   if (blocks < 1) blocks = 1;
-  walkKernel<kMixed, kEpsZero><<<static_cast<unsigned>(blocks), kWalkWarpsPerBlock * 32, 0, s>>>(args);
+  { noteLaunch(); walkKernel<kMixed, kEpsZero><<<static_cast<unsigned>(blocks), kWalkWarpsPerBlock * 32, 0, s>>>(args); }
   return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
 }
 

@@ -79,6 +79,7 @@ typedef struct {
   uint32_t maximum_depth;
   uint32_t path_words;
   double pm_ms, tree_build_ms, walk_ms, total_ms;
+  uint64_t kernel_launches;   /* this library's own kernels launched by the solve */
 } chui_treepm_stats;
 
 /* Sources: TreePmCoordinator::solveActiveSet's pos_{x,y,z}_comoving and
@@ -122,7 +123,8 @@ void chui_treepm_destroy(void *handle);
  * the reference). The mesh shape is fixed at creation, as PmGridShape is. */
 int chui_treepm_set_config(void *handle, const chui_treepm_config *config);
 
-/* Text of the last error on this handle ("" when none). */
+/* Text of the last error on this handle ("" when none). With a NULL handle:
+ * the text of the last failed chui_treepm_create on the calling thread. */
 const char *chui_treepm_last_error(const void *handle);
 
 /* TreePmCoordinator::solveActiveSetWithPmCadence (tree_pm_coupling.hpp:563-573,
