@@ -327,6 +327,24 @@ def cpu_baseline(w, x, y, z, m, args) -> dict | None:
             "process_wall_s": wall}
 
 
+def run_profile(args) -> int:
+    """Two mixed-precision force evaluations of the workload (the second is the
+    one an ncu capture selects with -s/-c), nothing else: for launch lists and
+    single-kernel captures."""
+    import torch
+    import chui_treepm as ct
+    w = WORKLOADS[args.workload]
+    x, y, z, m, vx, vy, vz = make_particles(w, seed=42)
+    dev = torch.device("cuda", 0)
+    t = {k: torch.tensor(v, device=dev) for k, v in dict(x=x, y=y, z=z, m=m).items()}
+    with ct.TreePmCoordinator(make_config(w, ct._abi.MIXED, 0)) as s:
+        for _ in range(2):
+            s.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+        torch.cuda.synchronize()
+        log(json.dumps(s.last_stats))
+    return 0
+
+
 def run_reference(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -370,7 +388,10 @@ def main() -> int:
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile"])
     args = ap.parse_args()
+    if args.mode == "profile":
+        return run_profile(args)
     if args.impl == "reference":
         args.steps = min(args.steps, 1) if args.workload == "clustered256" else args.steps
         args.warmup = 0 if args.workload == "clustered256" else args.warmup

@@ -184,7 +184,9 @@ double hostH(double t) {
 PolyH fitPoly(double t_cut) {
   PolyH best;
   best.max_rel_error = 1e300;
-  for (int deg = 6; deg < kPolyMaxTerms; ++deg) {
+  // The walk kernel evaluates either 12 terms or kPolyMaxTerms terms (unused
+  // high coefficients are zero); try 12 first, then the longest form.
+  for (int deg : {11, kPolyMaxTerms - 1}) {
     const int m = deg + 1;
     std::vector<double> f(m), cheb(m, 0.0);
     const double pi = 3.141592653589793238462643383279502884;
@@ -229,7 +231,7 @@ PolyH fitPoly(double t_cut) {
     }
     p.max_rel_error = err;
     if (err < best.max_rel_error) best = p;
-    if (err < 1.0e-6) break;
+    if (err < 2.0e-6) break;
   }
   return best;
 }

@@ -72,6 +72,16 @@ __device__ __forceinline__ float polyH(const PolyH& p, float t) {
   return h;
 }
 
+// Fixed-length Horner form (coefficients beyond p.terms are zero).
+template <int kTerms>
+__device__ __forceinline__ float polyHFixed(const PolyH& p, float t) {
+  const float s = fmaf(t, p.scale, -1.0f);
+  float h = p.c[kTerms - 1];
+#pragma unroll
+  for (int k = kTerms - 2; k >= 0; --k) h = fmaf(h, s, p.c[k]);
+  return h;
+}
+
 // monopolePlusQuadrupoleAccelPeriodicReference (tree_pm_coupling.cpp:743-827), FP64.
 __device__ void multipoleForce(const WalkArgs& a, uint32_t node, double dx, double dy, double dz,
                                double eps_t, double& ax, double& ay, double& az) {
@@ -351,6 +361,266 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
   }
 }
 
+constexpr int kQueue = 64;  // sources per warp batch
+
+// Mixed-precision walk with batched leaf sources.
+//
+// The traversal and every per-lane decision are those of walkKernel. Instead
+// of evaluating each accepted leaf on its own, the warp appends the leaf's
+// sources to a shared-memory queue, each tagged with the ballot of lanes that
+// accepted the leaf, and evaluates the queue 64 sources at a time: all lanes
+// stay busy across small leaves and the unrolled source loop gives the FP32
+// pipes independent dependency chains. Sources and targets are expressed as
+// FP32 offsets from one FP64 reference point per warp (its first target): the
+// offset of a source is (u_s - leaf centre) + (leaf centre image nearest the
+// reference - reference), formed in FP64 and rounded once. The image is the
+// pair's nearest image whenever r_cut + leaf half size + group radius < L/2;
+// leaves failing that test (tiny boxes) take the exact FP64 path.
+template <bool kEpsZero, int kTerms>
+__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(WalkArgs a) {
+  __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
+  __shared__ float4 q_src[kWalkWarpsPerBlock][kQueue];
+  __shared__ uint2 q_meta[kWalkWarpsPerBlock][kQueue];
+  __shared__ double4 exact_sm[kWalkWarpsPerBlock][32];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t lane_bit = 1u << lane;
+  uint32_t* stack = stack_sm[warp];
+  const WalkParams& w = a.wp;
+  const double half_min_box = 0.5 * fmin(w.box[0], fmin(w.box[1], w.box[2]));
+  unsigned long long cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0,
+                     cnt_skips = 0, cnt_multi = 0, cnt_leaves = 0;
+
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(a.work, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= a.nt) break;
+    const int64_t v = static_cast<int64_t>(base) + lane;
+    const bool valid = v < a.nt;
+    uint32_t slot = 0, row = kInvalid;
+    double px = 0.0, py = 0.0, pz = 0.0;
+    if (valid) {
+      slot = a.order[v];
+      row = a.active ? a.active[slot] : slot;
+      if (a.tx) {
+        px = a.tx[slot];
+        py = a.ty[slot];
+        pz = a.tz[slot];
+      } else {
+        px = a.sx[row];
+        py = a.sy[row];
+        pz = a.sz[row];
+      }
+    }
+    // lane 0 is always valid (base < nt): its target is the warp reference
+    const double rx = __shfl_sync(0xffffffffu, px, 0);
+    const double ry = __shfl_sync(0xffffffffu, py, 0);
+    const double rz = __shfl_sync(0xffffffffu, pz, 0);
+    double ox = px - rx, oy = py - ry, oz = pz - rz;
+    ox -= w.box[0] * rint(ox / w.box[0]);
+    oy -= w.box[1] * rint(oy / w.box[1]);
+    oz -= w.box[2] * rint(oz / w.box[2]);
+    double rg = valid ? fmax(fabs(ox), fmax(fabs(oy), fabs(oz))) : 0.0;
+    for (int off = 16; off > 0; off >>= 1) rg = fmax(rg, __shfl_xor_sync(0xffffffffu, rg, off));
+    const float tfx = static_cast<float>(ox), tfy = static_cast<float>(oy), tfz = static_cast<float>(oz);
+    const bool skip_self = valid && row < a.n;
+    const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
+    const double eps_t = w.eps;
+    Metric sm[3], nm[3];
+    const double pt[3] = {px, py, pz};
+    for (int ax_ = 0; ax_ < 3; ++ax_) {
+      sm[ax_] = makeMetric(w.src_lo[ax_], w.src_hi[ax_], pt[ax_], w.box[ax_]);
+      nm[ax_] = makeMetric(w.node_lo[ax_], w.node_hi[ax_], pt[ax_], w.box[ax_]);
+    }
+    double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
+    float nearest_f = INFINITY;
+    uint32_t skip_until = 0;
+    int qn = 0;
+    if (lane == 0) stack[0] = 0u;
+    int sp = 1;
+    __syncwarp();
+    bool overflow = false;
+
+    auto flush = [&]() {
+      float fx = 0.f, fy = 0.f, fz = 0.f;
+      uint32_t pairs = 0, skips = 0;
+#pragma unroll 4
+      for (int k = 0; k < qn; ++k) {
+        const float4 e = q_src[warp][k];
+        const uint2 meta = q_meta[warp][k];
+        const float dx = e.x - tfx, dy = e.y - tfy, dz = e.z - tfz;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const bool mine = (meta.x & lane_bit) != 0u && meta.y != self_pos;
+        const bool in = mine && r2 <= w.cut2_f;
+        pairs += in ? 1u : 0u;
+        skips += (mine && !in) ? 1u : 0u;
+        nearest_f = in ? fminf(nearest_f, r2) : nearest_f;
+        const float hh = polyHFixed<kTerms>(a.poly, r2 * w.inv_4rs2_f);
+        const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
+        const float rinv = rsqrtf(s2);
+        const float k3 = fmaf(-hh, w.inv_8rs3_f, rinv * rinv * rinv);
+        const float f = (in && r2 > 0.f) ? e.w * k3 : 0.f;
+        fx = fmaf(f, dx, fx);
+        fy = fmaf(f, dy, fy);
+        fz = fmaf(f, dz, fz);
+      }
+      acc_x += static_cast<double>(w.G_f * fx);
+      acc_y += static_cast<double>(w.G_f * fy);
+      acc_z += static_cast<double>(w.G_f * fz);
+      cnt_pairs += pairs;
+      cnt_skips += skips;
+      qn = 0;
+      __syncwarp();
+    };
+
+    while (sp > 0) {
+      const uint32_t node = stack[sp - 1];
+      --sp;
+      __syncwarp();
+      const bool act = valid && node >= skip_until;
+      if (!__any_sync(0xffffffffu, act)) continue;
+      const double4 g = a.geom[node];
+      const uint4 rg4 = a.range[node];
+      const double h = g.w;
+      const double ndx = applyMetric(nm[0], g.x - px);
+      const double ndy = applyMetric(nm[1], g.y - py);
+      const double ndz = applyMetric(nm[2], g.z - pz);
+      const double ax_abs = fabs(ndx), ay_abs = fabs(ndy), az_abs = fabs(ndz);
+      const double ex = fmax(0.0, ax_abs - h), ey = fmax(0.0, ay_abs - h), ez = fmax(0.0, az_abs - h);
+      const bool prune = !withinCutoff(ex * ex + ey * ey + ez * ez, w.cutoff, w.cutoff2);
+      if (act) {
+        ++cnt_visited;
+        cnt_pruned += prune ? 1 : 0;
+      }
+      if (rg4.z == 0) {  // leaf
+        const bool want = act && !prune;
+        const uint32_t mask = __ballot_sync(0xffffffffu, want);
+        if (mask == 0u) continue;
+        if (want) {
+          ++cnt_accepted;
+          ++cnt_leaves;
+        }
+        const uint32_t begin = rg4.x, count = rg4.y;
+        if (w.cutoff + h + rg < half_min_box && h < w.exact_half) {
+          double cdx = g.x - rx, cdy = g.y - ry, cdz = g.z - rz;
+          cdx -= w.box[0] * rint(cdx / w.box[0]);
+          cdy -= w.box[1] * rint(cdy / w.box[1]);
+          cdz -= w.box[2] * rint(cdz / w.box[2]);
+          for (uint32_t chunk = 0; chunk < count; chunk += 32) {
+            const int c = static_cast<int>(min(32u, count - chunk));
+            if (qn + c > kQueue) flush();
+            if (lane < c) {
+              const float4 s = a.src_f4[begin + chunk + lane];
+              q_src[warp][qn + lane] = make_float4(static_cast<float>(static_cast<double>(s.x) + cdx),
+                                                   static_cast<float>(static_cast<double>(s.y) + cdy),
+                                                   static_cast<float>(static_cast<double>(s.z) + cdz), s.w);
+              q_meta[warp][qn + lane] = make_uint2(mask, begin + chunk + lane);
+            }
+            __syncwarp();
+            qn += c;
+          }
+        } else {
+          // exact FP64 pairs (reference formulas) for leaves the shared frame cannot serve
+          for (uint32_t chunk = 0; chunk < count; chunk += 32) {
+            const uint32_t k = chunk + lane;
+            if (k < count) exact_sm[warp][lane] = a.src_d4[begin + k];
+            __syncwarp();
+            const uint32_t m = min(32u, count - chunk);
+            if (want) {
+              for (uint32_t j = 0; j < m; ++j) {
+                if ((begin + chunk + j) == self_pos) continue;
+                const double4 sv = exact_sm[warp][j];
+                const double dx = applyMetric(sm[0], sv.x - px);
+                const double dy = applyMetric(sm[1], sv.y - py);
+                const double dz = applyMetric(sm[2], sv.z - pz);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > w.cutoff2) {
+                  ++cnt_skips;
+                  continue;
+                }
+                nearest_f = fminf(nearest_f, static_cast<float>(r2));
+                ++cnt_pairs;
+                if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
+                const double f = residualInvR3(r2, fmax(w.eps, eps_t), w.rs) * w.G;
+                acc_x += f * sv.w * dx;
+                acc_y += f * sv.w * dy;
+                acc_z += f * sv.w * dz;
+              }
+            }
+            __syncwarp();
+          }
+        }
+        continue;
+      }
+      // internal node
+      const double4 cm = a.com[node];
+      const double off = a.quad[8 * static_cast<size_t>(node) + 7];
+      const bool inside = skip_self && ax_abs <= h && ay_abs <= h && az_abs <= h;
+      const double mx = ax_abs + h, my = ay_abs + h, mz = az_abs + h;
+      const bool within = withinCutoff(mx * mx + my * my + mz * mz, w.cutoff, w.cutoff2);
+      const double dx = applyMetric(nm[0], cm.x - px);
+      const double dy = applyMetric(nm[1], cm.y - py);
+      const double dz = applyMetric(nm[2], cm.z - pz);
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const bool accept = act && !prune && acceptStrict(w, h, off, inside, within, r2, eps_t);
+      const bool open = act && !prune && !accept;
+      if (accept) {
+        ++cnt_accepted;
+        ++cnt_multi;
+        multipoleForce(a, node, dx, dy, dz, eps_t, acc_x, acc_y, acc_z);
+      }
+      if (act && (prune || accept)) skip_until = rg4.w;
+      if (open) ++cnt_opened;
+      if (__any_sync(0xffffffffu, open)) {
+        const uint32_t ch = lane < 8 ? a.child[8 * static_cast<size_t>(node) + lane] : kInvalid;
+        const unsigned mask = __ballot_sync(0xffffffffu, ch != kInvalid) & 0xFFu;
+        const int nc = __popc(mask);
+        if (sp + nc > kStackCap) {
+          overflow = true;
+          break;
+        }
+        if (ch != kInvalid) stack[sp + __popc(mask >> (lane + 1))] = ch;
+        sp += nc;
+        __syncwarp();
+      }
+    }
+    if (qn > 0) flush();
+    if (overflow && lane == 0) atomicOr(a.status, kStatusStackOverflow);
+    if (valid) {
+      a.out_x[slot] = acc_x;
+      a.out_y[slot] = acc_y;
+      a.out_z[slot] = acc_z;
+      a.out_near[slot] = static_cast<double>(nearest_f);
+    }
+    __syncwarp();
+  }
+  unsigned long long c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs,
+                             cnt_pruned, cnt_skips, cnt_multi, cnt_leaves};
+  for (int k = 0; k < 8; ++k) {
+    for (int off = 16; off > 0; off >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], off);
+  }
+  if (lane == 0) {
+    for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, c[k]);
+  }
+}
+
+template <class Kernel>
+int launchPersistent(Kernel kernel, const WalkArgs& args, cudaStream_t s) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWalkWarpsPerBlock * 32, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t warps_needed = (args.nt + 31) / 32;
+  int64_t blocks = static_cast<int64_t>(sms) * per_sm;
+  const int64_t max_useful = (warps_needed + kWalkWarpsPerBlock - 1) / kWalkWarpsPerBlock;
+  if (blocks > max_useful) blocks = max_useful;
+  if (blocks < 1) blocks = 1;
+  { noteLaunch(); kernel<<<static_cast<unsigned>(blocks), kWalkWarpsPerBlock * 32, 0, s>>>(args); }
+  return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
+}
+
 template <bool kMixed, bool kEpsZero>
 int launchWalk(const WalkArgs& args, cudaStream_t s) {
   int dev = 0, sms = 148, per_sm = 1;
@@ -411,7 +681,13 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.wp = wp;
   const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
   const bool eps_zero = wp.eps == 0.0;
-  if (mixed) return eps_zero ? launchWalk<true, true>(a, s) : launchWalk<true, false>(a, s);
+  if (mixed) {
+    if (c.poly.terms <= 12)
+      return eps_zero ? launchPersistent(walkQueuedKernel<true, 12>, a, s)
+                      : launchPersistent(walkQueuedKernel<false, 12>, a, s);
+    return eps_zero ? launchPersistent(walkQueuedKernel<true, kPolyMaxTerms>, a, s)
+                    : launchPersistent(walkQueuedKernel<false, kPolyMaxTerms>, a, s);
+  }
   return launchWalk<false, false>(a, s);
 }
 
