@@ -29,7 +29,7 @@ class Config(C.Structure):
         ("assignment_scheme", C.c_int32), ("window_deconvolution", C.c_int32),
         ("gravitational_constant", C.c_double), ("softening", C.c_double),
         ("acceptance_policy", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
-        ("reserved", C.c_int32),
+        ("diagnostics", C.c_int32),
     ]
 
 

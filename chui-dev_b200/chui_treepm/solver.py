@@ -86,6 +86,7 @@ class TreePmConfig:
     acceptance_policy: int = 0
     precision: int = _abi.MIXED
     device: int = 0
+    diagnostics: int = 1
 
     def to_c(self) -> _abi.Config:
         c = _abi.Config()

@@ -54,6 +54,7 @@ struct WalkArgs {
   const uint4* range;
   const float4* src_f4;
   const double4* src_d4;
+  const float4* node_f4;
   double* out_x;   // per slot, short-range part
   double* out_y;
   double* out_z;
@@ -363,21 +364,127 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
 
 constexpr int kQueue = 64;  // sources per warp batch
 
-// Mixed-precision walk with batched leaf sources.
+// H(t) in Estrin form: same polynomial as polyHFixed<12>, dependency depth 5.
+__device__ __forceinline__ float polyH12(const PolyH& p, float t) {
+  const float s = fmaf(t, p.scale, -1.0f);
+  const float s2 = s * s;
+  const float s4 = s2 * s2;
+  const float s8 = s4 * s4;
+  const float a0 = fmaf(p.c[1], s, p.c[0]);
+  const float a1 = fmaf(p.c[3], s, p.c[2]);
+  const float a2 = fmaf(p.c[5], s, p.c[4]);
+  const float a3 = fmaf(p.c[7], s, p.c[6]);
+  const float a4 = fmaf(p.c[9], s, p.c[8]);
+  const float a5 = fmaf(p.c[11], s, p.c[10]);
+  const float b0 = fmaf(a1, s2, a0);
+  const float b1 = fmaf(a3, s2, a2);
+  const float b2 = fmaf(a5, s2, a4);
+  return fmaf(b2, s8, fmaf(b1, s4, b0));
+}
+
+template <int kTerms>
+__device__ __forceinline__ float evalH(const PolyH& p, float t) {
+  if constexpr (kTerms == 12) return polyH12(p, t);
+  return polyHFixed<kTerms>(p, t);
+}
+
+// Exact (FP64, reference formulas) decision for one lane at one node: prune,
+// and for internal nodes accept/open, plus the COM offset for a multipole.
+struct ExactDecision {
+  bool prune, accept;
+  double dx, dy, dz;
+};
+
+__device__ __forceinline__ ExactDecision exactNodeDecision(const WalkArgs& a, uint32_t node, double px, double py,
+                                                        double pz, bool skip_self) {
+  const WalkParams& w = a.wp;
+  ExactDecision d{};
+  const double4 g = a.geom[node];
+  const uint4 rg4 = a.range[node];
+  const Metric mx = makeMetric(w.node_lo[0], w.node_hi[0], px, w.box[0]);
+  const Metric my = makeMetric(w.node_lo[1], w.node_hi[1], py, w.box[1]);
+  const Metric mz = makeMetric(w.node_lo[2], w.node_hi[2], pz, w.box[2]);
+  const double h = g.w;
+  const double ndx = applyMetric(mx, g.x - px), ndy = applyMetric(my, g.y - py), ndz = applyMetric(mz, g.z - pz);
+  const double ax = fabs(ndx), ay = fabs(ndy), az = fabs(ndz);
+  const double ex = fmax(0.0, ax - h), ey = fmax(0.0, ay - h), ez = fmax(0.0, az - h);
+  d.prune = !withinCutoff(ex * ex + ey * ey + ez * ez, w.cutoff, w.cutoff2);
+  d.accept = false;
+  if (d.prune || rg4.z == 0) return d;
+  const double4 cm = a.com[node];
+  const double off = a.quad[8 * static_cast<size_t>(node) + 7];
+  const bool inside = skip_self && ax <= h && ay <= h && az <= h;
+  const double qx = ax + h, qy = ay + h, qz = az + h;
+  const bool within = withinCutoff(qx * qx + qy * qy + qz * qz, w.cutoff, w.cutoff2);
+  d.dx = applyMetric(mx, cm.x - px);
+  d.dy = applyMetric(my, cm.y - py);
+  d.dz = applyMetric(mz, cm.z - pz);
+  const double r2 = d.dx * d.dx + d.dy * d.dy + d.dz * d.dz;
+  d.accept = acceptStrict(w, h, off, inside, within, r2, w.eps);
+  return d;
+}
+
+// Exact FP64 pairs of one leaf for the lanes in `want` (reference formulas,
+// per-pair source metric): used where the shared FP32 frame cannot serve.
+__device__ __forceinline__ void exactLeafPairs(const WalkArgs& a, double4* stage, uint32_t begin, uint32_t count,
+                                            bool want, double px, double py, double pz, uint32_t self_pos,
+                                            double& ax, double& ay, double& az, float& nearest,
+                                            unsigned long long& pairs, unsigned long long& skips) {
+  const WalkParams& w = a.wp;
+  const int lane = threadIdx.x & 31;
+  const Metric mx = makeMetric(w.src_lo[0], w.src_hi[0], px, w.box[0]);
+  const Metric my = makeMetric(w.src_lo[1], w.src_hi[1], py, w.box[1]);
+  const Metric mz = makeMetric(w.src_lo[2], w.src_hi[2], pz, w.box[2]);
+  for (uint32_t chunk = 0; chunk < count; chunk += 32) {
+    const uint32_t k = chunk + lane;
+    if (k < count) stage[lane] = a.src_d4[begin + k];
+    __syncwarp();
+    const uint32_t m = min(32u, count - chunk);
+    if (want) {
+      for (uint32_t j = 0; j < m; ++j) {
+        if ((begin + chunk + j) == self_pos) continue;
+        const double4 sv = stage[j];
+        const double dx = applyMetric(mx, sv.x - px), dy = applyMetric(my, sv.y - py), dz = applyMetric(mz, sv.z - pz);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > w.cutoff2) {
+          ++skips;
+          continue;
+        }
+        nearest = fminf(nearest, static_cast<float>(r2));
+        ++pairs;
+        if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
+        const double f = residualInvR3(r2, w.eps, w.rs) * w.G;
+        ax += f * sv.w * dx;
+        ay += f * sv.w * dy;
+        az += f * sv.w * dz;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Comparison a < b decided in FP32 with a relative guard band: returns
+// +1 (certainly true), -1 (certainly false) or 0 (too close to call in FP32).
+__device__ __forceinline__ int certainLess(float a, float b) {
+  const float band = 2.0e-5f * (fabsf(a) + fabsf(b)) + 1.0e-30f;
+  if (a < b - band) return 1;
+  if (a > b + band) return -1;
+  return 0;
+}
+
+// Mixed-precision walk (the product path).
 //
-// The traversal and every per-lane decision are those of walkKernel. Instead
-// of evaluating each accepted leaf on its own, the warp appends the leaf's
-// sources to a shared-memory queue, each tagged with the ballot of lanes that
-// accepted the leaf, and evaluates the queue 64 sources at a time: all lanes
-// stay busy across small leaves and the unrolled source loop gives the FP32
-// pipes independent dependency chains. Sources and targets are expressed as
-// FP32 offsets from one FP64 reference point per warp (its first target): the
-// offset of a source is (u_s - leaf centre) + (leaf centre image nearest the
-// reference - reference), formed in FP64 and rounded once. The image is the
-// pair's nearest image whenever r_cut + leaf half size + group radius < L/2;
-// leaves failing that test (tiny boxes) take the exact FP64 path.
-template <bool kEpsZero, int kTerms>
-__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(WalkArgs a) {
+// Traversal order and every per-lane decision are those of the reference's
+// evaluateTargetAgainstLocalTree. Each warp works in one FP64 reference frame
+// (its first target): a node's centre offset is formed once in FP64 and
+// rounded, and each lane decides prune / accept / open in FP32 with a guard
+// band; only lanes whose FP32 test lands inside the band re-decide with the
+// exact FP64 reference arithmetic, so decisions equal the reference's.
+// Accepted leaves are appended to a shared-memory queue (sources outside the
+// group's cutoff sphere are dropped at enqueue) tagged with the ballot of
+// accepting lanes, and evaluated 64 sources at a time in FP32.
+template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous>
+__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(WalkArgs a) {
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
   __shared__ float4 q_src[kWalkWarpsPerBlock][kQueue];
   __shared__ uint2 q_meta[kWalkWarpsPerBlock][kQueue];
@@ -388,10 +495,13 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(W
   uint32_t* stack = stack_sm[warp];
   const WalkParams& w = a.wp;
   const double half_min_box = 0.5 * fmin(w.box[0], fmin(w.box[1], w.box[2]));
-  unsigned long long cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0,
-                     cnt_skips = 0, cnt_multi = 0, cnt_leaves = 0;
+  const float cut2 = w.cut2_f;
+  const float env2 = 0.0064f;  // 0.08^2
+  const float theta2 = static_cast<float>(w.theta * w.theta);
 
   while (true) {
+    uint32_t cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0, cnt_skips = 0,
+             cnt_multi = 0, cnt_leaves = 0;
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(a.work, 32u);
     base = __shfl_sync(0xffffffffu, base, 0);
@@ -413,7 +523,6 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(W
         pz = a.sz[row];
       }
     }
-    // lane 0 is always valid (base < nt): its target is the warp reference
     const double rx = __shfl_sync(0xffffffffu, px, 0);
     const double ry = __shfl_sync(0xffffffffu, py, 0);
     const double rz = __shfl_sync(0xffffffffu, pz, 0);
@@ -421,18 +530,17 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(W
     ox -= w.box[0] * rint(ox / w.box[0]);
     oy -= w.box[1] * rint(oy / w.box[1]);
     oz -= w.box[2] * rint(oz / w.box[2]);
-    double rg = valid ? fmax(fabs(ox), fmax(fabs(oy), fabs(oz))) : 0.0;
-    for (int off = 16; off > 0; off >>= 1) rg = fmax(rg, __shfl_xor_sync(0xffffffffu, rg, off));
+    double rga = valid ? fmax(fabs(ox), fmax(fabs(oy), fabs(oz))) : 0.0;
+    double rg2 = valid ? ox * ox + oy * oy + oz * oz : 0.0;
+    for (int off = 16; off > 0; off >>= 1) {
+      rga = fmax(rga, __shfl_xor_sync(0xffffffffu, rga, off));
+      rg2 = fmax(rg2, __shfl_xor_sync(0xffffffffu, rg2, off));
+    }
     const float tfx = static_cast<float>(ox), tfy = static_cast<float>(oy), tfz = static_cast<float>(oz);
+    const float cull = static_cast<float>(w.cutoff + sqrt(rg2));
+    const float cull2 = cull * cull * 1.0001f;
     const bool skip_self = valid && row < a.n;
     const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
-    const double eps_t = w.eps;
-    Metric sm[3], nm[3];
-    const double pt[3] = {px, py, pz};
-    for (int ax_ = 0; ax_ < 3; ++ax_) {
-      sm[ax_] = makeMetric(w.src_lo[ax_], w.src_hi[ax_], pt[ax_], w.box[ax_]);
-      nm[ax_] = makeMetric(w.node_lo[ax_], w.node_hi[ax_], pt[ax_], w.box[ax_]);
-    }
     double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
     float nearest_f = INFINITY;
     uint32_t skip_until = 0;
@@ -445,18 +553,20 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(W
     auto flush = [&]() {
       float fx = 0.f, fy = 0.f, fz = 0.f;
       uint32_t pairs = 0, skips = 0;
-#pragma unroll 4
+#pragma unroll 2
       for (int k = 0; k < qn; ++k) {
         const float4 e = q_src[warp][k];
         const uint2 meta = q_meta[warp][k];
         const float dx = e.x - tfx, dy = e.y - tfy, dz = e.z - tfz;
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const bool mine = (meta.x & lane_bit) != 0u && meta.y != self_pos;
-        const bool in = mine && r2 <= w.cut2_f;
-        pairs += in ? 1u : 0u;
-        skips += (mine && !in) ? 1u : 0u;
-        nearest_f = in ? fminf(nearest_f, r2) : nearest_f;
-        const float hh = polyHFixed<kTerms>(a.poly, r2 * w.inv_4rs2_f);
+        const bool mine = kContiguous ? (meta.x & lane_bit) != 0u : ((meta.x & lane_bit) != 0u && meta.y != self_pos);
+        const bool in = mine && r2 <= cut2;
+        if constexpr (kDiag) {
+          pairs += in ? 1u : 0u;
+          skips += (mine && !in) ? 1u : 0u;
+          nearest_f = in ? fminf(nearest_f, r2) : nearest_f;
+        }
+        const float hh = evalH<kTerms>(a.poly, r2 * w.inv_4rs2_f);
         const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
         const float rinv = rsqrtf(s2);
         const float k3 = fmaf(-hh, w.inv_8rs3_f, rinv * rinv * rinv);
@@ -483,17 +593,69 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(W
       const double4 g = a.geom[node];
       const uint4 rg4 = a.range[node];
       const double h = g.w;
-      const double ndx = applyMetric(nm[0], g.x - px);
-      const double ndy = applyMetric(nm[1], g.y - py);
-      const double ndz = applyMetric(nm[2], g.z - pz);
-      const double ax_abs = fabs(ndx), ay_abs = fabs(ndy), az_abs = fabs(ndz);
-      const double ex = fmax(0.0, ax_abs - h), ey = fmax(0.0, ay_abs - h), ez = fmax(0.0, az_abs - h);
-      const bool prune = !withinCutoff(ex * ex + ey * ey + ez * ez, w.cutoff, w.cutoff2);
+      const bool is_leaf = rg4.z == 0;
+      // warp-uniform FP64 centre offset from the reference target
+      double cdx = g.x - rx, cdy = g.y - ry, cdz = g.z - rz;
+      cdx -= w.box[0] * rint(cdx / w.box[0]);
+      cdy -= w.box[1] * rint(cdy / w.box[1]);
+      cdz -= w.box[2] * rint(cdz / w.box[2]);
+      const bool fast_frame = h < 64.0 * w.cutoff &&
+                              fmax(fabs(cdx), fmax(fabs(cdy), fabs(cdz))) + rga < half_min_box * (1.0 - 1.0e-9);
+      bool prune = false, accept = false, need_exact = !fast_frame;
+      float ndx = 0.f, ndy = 0.f, ndz = 0.f;
+      if (act && fast_frame) {
+        const float hf = static_cast<float>(h);
+        ndx = static_cast<float>(cdx) - tfx;
+        ndy = static_cast<float>(cdy) - tfy;
+        ndz = static_cast<float>(cdz) - tfz;
+        const float ax = fabsf(ndx), ay = fabsf(ndy), az = fabsf(ndz);
+        const float ex = fmaxf(0.f, ax - hf), ey = fmaxf(0.f, ay - hf), ez = fmaxf(0.f, az - hf);
+        const int keep = certainLess(fmaf(ex, ex, fmaf(ey, ey, ez * ez)), cut2);
+        if (keep == 0) {
+          need_exact = true;
+        } else {
+          prune = keep < 0;
+          if (!prune && !is_leaf) {
+            // inside (target within the node cube), cutoff containment, envelope, MAC
+            int cin = 1;
+            if (skip_self) {
+              const int ix = certainLess(ax, hf), iy = certainLess(ay, hf), iz = certainLess(az, hf);
+              if (ix == 0 || iy == 0 || iz == 0) cin = 0;
+              else cin = (ix > 0 && iy > 0 && iz > 0) ? 1 : -1;  // +1 inside, -1 outside
+            } else {
+              cin = -1;
+            }
+            const float qx = ax + hf, qy = ay + hf, qz = az + hf;
+            const int within = certainLess(fmaf(qx, qx, fmaf(qy, qy, qz * qz)), cut2);
+            const float4 nf = a.node_f4[node];
+            const float dxc = ndx + nf.x, dyc = ndy + nf.y, dzc = ndz + nf.z;
+            const float r2c = fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc));
+            const float w2 = 4.0f * hf * hf;
+            const int env = w.quadrupole ? certainLess(w2, env2 * r2c) : -1;
+            const float macl = (w.criterion == 0) ? w2 : (2.0f * hf + nf.w) * (2.0f * hf + nf.w);
+            const int mac = certainLess(macl, theta2 * r2c);
+            if (cin == 0 || within == 0 || env == 0 || mac == 0) {
+              need_exact = true;
+            } else {
+              accept = cin < 0 && within > 0 && env > 0 && mac > 0;
+            }
+          }
+        }
+      }
+      double mdx = 0.0, mdy = 0.0, mdz = 0.0;
+      if (act && need_exact) {
+        const ExactDecision d = exactNodeDecision(a, node, px, py, pz, skip_self);
+        prune = d.prune;
+        accept = d.accept;
+        mdx = d.dx;
+        mdy = d.dy;
+        mdz = d.dz;
+      }
       if (act) {
         ++cnt_visited;
         cnt_pruned += prune ? 1 : 0;
       }
-      if (rg4.z == 0) {  // leaf
+      if (is_leaf) {
         const bool want = act && !prune;
         const uint32_t mask = __ballot_sync(0xffffffffu, want);
         if (mask == 0u) continue;
@@ -502,85 +664,69 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(W
           ++cnt_leaves;
         }
         const uint32_t begin = rg4.x, count = rg4.y;
-        if (w.cutoff + h + rg < half_min_box && h < w.exact_half) {
-          double cdx = g.x - rx, cdy = g.y - ry, cdz = g.z - rz;
-          cdx -= w.box[0] * rint(cdx / w.box[0]);
-          cdy -= w.box[1] * rint(cdy / w.box[1]);
-          cdz -= w.box[2] * rint(cdz / w.box[2]);
+        if (w.cutoff + h + rga < half_min_box && h < w.exact_half) {
           for (uint32_t chunk = 0; chunk < count; chunk += 32) {
-            const int c = static_cast<int>(min(32u, count - chunk));
+            const uint32_t k = chunk + lane;
+            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+            bool keep = false;
+            if (k < count) {
+              const float4 sv = a.src_f4[begin + k];
+              e = make_float4(static_cast<float>(static_cast<double>(sv.x) + cdx),
+                              static_cast<float>(static_cast<double>(sv.y) + cdy),
+                              static_cast<float>(static_cast<double>(sv.z) + cdz), sv.w);
+              keep = fmaf(e.x, e.x, fmaf(e.y, e.y, e.z * e.z)) <= cull2;
+            }
+            const uint32_t keep_mask = __ballot_sync(0xffffffffu, keep);
+            const int c = __popc(keep_mask);
             if (qn + c > kQueue) flush();
-            if (lane < c) {
-              const float4 s = a.src_f4[begin + chunk + lane];
-              q_src[warp][qn + lane] = make_float4(static_cast<float>(static_cast<double>(s.x) + cdx),
-                                                   static_cast<float>(static_cast<double>(s.y) + cdy),
-                                                   static_cast<float>(static_cast<double>(s.z) + cdz), s.w);
-              q_meta[warp][qn + lane] = make_uint2(mask, begin + chunk + lane);
+            if (keep) {
+              const int slot_q = qn + __popc(keep_mask & (lane_bit - 1u));
+              uint32_t m = mask;
+              if constexpr (kContiguous) {
+                // targets are tree positions base..base+31: drop the source's own lane
+                const uint32_t rel = begin + k - base;
+                if (rel < 32u) m &= ~(1u << rel);
+              }
+              q_src[warp][slot_q] = e;
+              q_meta[warp][slot_q] = make_uint2(m, begin + k);
             }
             __syncwarp();
             qn += c;
           }
         } else {
-          // exact FP64 pairs (reference formulas) for leaves the shared frame cannot serve
-          for (uint32_t chunk = 0; chunk < count; chunk += 32) {
-            const uint32_t k = chunk + lane;
-            if (k < count) exact_sm[warp][lane] = a.src_d4[begin + k];
-            __syncwarp();
-            const uint32_t m = min(32u, count - chunk);
-            if (want) {
-              for (uint32_t j = 0; j < m; ++j) {
-                if ((begin + chunk + j) == self_pos) continue;
-                const double4 sv = exact_sm[warp][j];
-                const double dx = applyMetric(sm[0], sv.x - px);
-                const double dy = applyMetric(sm[1], sv.y - py);
-                const double dz = applyMetric(sm[2], sv.z - pz);
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 > w.cutoff2) {
-                  ++cnt_skips;
-                  continue;
-                }
-                nearest_f = fminf(nearest_f, static_cast<float>(r2));
-                ++cnt_pairs;
-                if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
-                const double f = residualInvR3(r2, fmax(w.eps, eps_t), w.rs) * w.G;
-                acc_x += f * sv.w * dx;
-                acc_y += f * sv.w * dy;
-                acc_z += f * sv.w * dz;
-              }
-            }
-            __syncwarp();
-          }
+          unsigned long long p = 0, sk = 0;
+          exactLeafPairs(a, exact_sm[warp], begin, count, want, px, py, pz, self_pos, acc_x, acc_y, acc_z,
+                         nearest_f, p, sk);
+          cnt_pairs += static_cast<uint32_t>(p);
+          cnt_skips += static_cast<uint32_t>(sk);
         }
         continue;
       }
       // internal node
-      const double4 cm = a.com[node];
-      const double off = a.quad[8 * static_cast<size_t>(node) + 7];
-      const bool inside = skip_self && ax_abs <= h && ay_abs <= h && az_abs <= h;
-      const double mx = ax_abs + h, my = ay_abs + h, mz = az_abs + h;
-      const bool within = withinCutoff(mx * mx + my * my + mz * mz, w.cutoff, w.cutoff2);
-      const double dx = applyMetric(nm[0], cm.x - px);
-      const double dy = applyMetric(nm[1], cm.y - py);
-      const double dz = applyMetric(nm[2], cm.z - pz);
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      const bool accept = act && !prune && acceptStrict(w, h, off, inside, within, r2, eps_t);
+      const bool do_accept = act && !prune && accept;
       const bool open = act && !prune && !accept;
-      if (accept) {
+      if (do_accept) {
         ++cnt_accepted;
         ++cnt_multi;
-        multipoleForce(a, node, dx, dy, dz, eps_t, acc_x, acc_y, acc_z);
+        if (!need_exact) {
+          const ExactDecision d = exactNodeDecision(a, node, px, py, pz, skip_self);
+          mdx = d.dx;
+          mdy = d.dy;
+          mdz = d.dz;
+        }
+        multipoleForce(a, node, mdx, mdy, mdz, w.eps, acc_x, acc_y, acc_z);
       }
       if (act && (prune || accept)) skip_until = rg4.w;
       if (open) ++cnt_opened;
       if (__any_sync(0xffffffffu, open)) {
         const uint32_t ch = lane < 8 ? a.child[8 * static_cast<size_t>(node) + lane] : kInvalid;
-        const unsigned mask = __ballot_sync(0xffffffffu, ch != kInvalid) & 0xFFu;
-        const int nc = __popc(mask);
+        const unsigned cmask = __ballot_sync(0xffffffffu, ch != kInvalid) & 0xFFu;
+        const int nc = __popc(cmask);
         if (sp + nc > kStackCap) {
           overflow = true;
           break;
         }
-        if (ch != kInvalid) stack[sp + __popc(mask >> (lane + 1))] = ch;
+        if (ch != kInvalid) stack[sp + __popc(cmask >> (lane + 1))] = ch;
         sp += nc;
         __syncwarp();
       }
@@ -591,17 +737,16 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkQueuedKernel(W
       a.out_x[slot] = acc_x;
       a.out_y[slot] = acc_y;
       a.out_z[slot] = acc_z;
-      a.out_near[slot] = static_cast<double>(nearest_f);
+      a.out_near[slot] = kDiag ? static_cast<double>(nearest_f) : INFINITY;
+    }
+    uint32_t c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs, cnt_pruned, cnt_skips, cnt_multi, cnt_leaves};
+    for (int k = 0; k < 8; ++k) {
+      for (int off = 16; off > 0; off >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], off);
+    }
+    if (lane == 0) {
+      for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, static_cast<unsigned long long>(c[k]));
     }
     __syncwarp();
-  }
-  unsigned long long c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs,
-                             cnt_pruned, cnt_skips, cnt_multi, cnt_leaves};
-  for (int k = 0; k < 8; ++k) {
-    for (int off = 16; off > 0; off >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], off);
-  }
-  if (lane == 0) {
-    for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, c[k]);
   }
 }
 
@@ -669,6 +814,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.range = c.node_range.as<uint4>();
   a.src_f4 = c.src_f4.as<float4>();
   a.src_d4 = c.src_d4.as<double4>();
+  a.node_f4 = c.node_f4.as<float4>();
   double* acc = c.tree_acc.as<double>();
   a.out_x = acc;
   a.out_y = acc + nt;
@@ -682,11 +828,22 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
   const bool eps_zero = wp.eps == 0.0;
   if (mixed) {
-    if (c.poly.terms <= 12)
-      return eps_zero ? launchPersistent(walkQueuedKernel<true, 12>, a, s)
-                      : launchPersistent(walkQueuedKernel<false, 12>, a, s);
-    return eps_zero ? launchPersistent(walkQueuedKernel<true, kPolyMaxTerms>, a, s)
-                    : launchPersistent(walkQueuedKernel<false, kPolyMaxTerms>, a, s);
+    // full solves visit targets in tree order, so a warp's targets are tree
+    // positions base..base+31 and self pairs are excluded by the lane mask
+    const bool contiguous = active == nullptr && tx == nullptr && nt == n;
+    const bool diag = c.cfg.diagnostics != 0;
+#define CHUI_WALK_DISPATCH(EPS, TERMS)                                                               \
+    if (diag) return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, true, true>, a, s)     \
+                                : launchPersistent(walkFastKernel<EPS, TERMS, true, false>, a, s);   \
+    return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, false, true>, a, s)              \
+                      : launchPersistent(walkFastKernel<EPS, TERMS, false, false>, a, s);
+    if (c.poly.terms <= 12) {
+      if (eps_zero) { CHUI_WALK_DISPATCH(true, 12) }
+      CHUI_WALK_DISPATCH(false, 12)
+    }
+    if (eps_zero) { CHUI_WALK_DISPATCH(true, kPolyMaxTerms) }
+    CHUI_WALK_DISPATCH(false, kPolyMaxTerms)
+#undef CHUI_WALK_DISPATCH
   }
   return launchWalk<false, false>(a, s);
 }

@@ -67,7 +67,8 @@ typedef struct {
   int32_t acceptance_policy;                  /* 0 strict reference (only policy implemented) */
   int32_t precision;                          /* CHUI_TREEPM_MIXED or CHUI_TREEPM_FP64 */
   int32_t device;                             /* CUDA device ordinal */
-  int32_t reserved;
+  int32_t diagnostics;                        /* 1: per-pair counters and nearest-pair r^2 (default);
+                                                 0: skipped in the walk (production timing) */
 } chui_treepm_config;
 
 /* Counters named as TreePmTraversalCounters (tree_pm_coupling.hpp:39-87) plus
