@@ -40,9 +40,21 @@ int main(int argc, char** argv) {
     std::iota(active.begin(), active.end(), 0u);
     std::vector<double> ax(n), ay(n), az(n), bx(n), by(n), bz(n);
     cb::TreePmForceAccumulatorView acc{active, ax, ay, az};
-    coordinator.solveActiveSet(x, y, z, m, acc, options);
+    cb::TreePmProfileEvent profile;
+    cb::TreePmDiagnostics diag;
+    coordinator.solveActiveSet(x, y, z, m, acc, options, &profile, &diag);
+    if (diag.pm_solve_count != 1 || diag.pm_reuse_count != 0 || diag.local_traversal.targets != static_cast<std::uint64_t>(n) ||
+        diag.local_traversal.visited_nodes == 0 || profile.tree_profile.actual_node_count == 0) {
+      std::fprintf(stderr, "unexpected diagnostics after a refresh solve\n");
+      return 4;
+    }
     cb::TreePmForceAccumulatorView acc2{active, bx, by, bz};
-    coordinator.solveActiveSetWithPmCadence(x, y, z, m, acc2, options, false);
+    coordinator.solveActiveSetWithPmCadence(x, y, z, m, acc2, options, false, nullptr, &diag);
+    // the integrator's cadence check (gravity_runtime.cpp:2418-2424)
+    if (diag.pm_solve_count != 0 || diag.pm_reuse_count != 1) {
+      std::fprintf(stderr, "unexpected PM cadence diagnostics after a reuse solve\n");
+      return 5;
+    }
     std::FILE* o = std::fopen(argv[2], "wb");
     for (auto* v : {&ax, &ay, &az, &bx, &by, &bz}) std::fwrite(v->data(), 8, n, o);
     std::fclose(o);

@@ -13,6 +13,7 @@
 // std::runtime_error, std::bad_alloc).
 #pragma once
 
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <new>
@@ -97,9 +98,80 @@ struct TreePmForceAccumulatorView {
   std::span<double> short_range_nearest_pair_r2_comoving{};
 };
 
-// The counters of TreePmTraversalCounters plus the phase timings.
+// The TreePmTraversalCounters fields the periodic strict walk produces
+// (tree_pm_coupling.hpp:39-60); counts are equal to the reference's.
+struct TreePmTraversalCounters {
+  std::uint64_t visited_nodes = 0;
+  std::uint64_t accepted_nodes = 0;
+  std::uint64_t opened_nodes = 0;
+  std::uint64_t direct_pair_evaluations = 0;
+  std::uint64_t cutoff_pruned_nodes = 0;
+  std::uint64_t cutoff_skipped_pairs = 0;
+  std::uint64_t accepted_internal_multipoles = 0;
+  std::uint64_t accepted_leaves = 0;
+  std::uint64_t targets = 0;
+};
+
+// The subset of TreePmDiagnostics (tree_pm_coupling.hpp:334-470) a
+// single-device periodic solve defines. GravityRuntimeImpl checks
+// pm_solve_count / pm_reuse_count against its cadence decision right after
+// the call (src/workflows/gravity_runtime.cpp:2418-2424).
 struct TreePmDiagnostics {
-  chui_treepm_stats stats{};
+  TreePmTraversalCounters local_traversal{};
+  std::uint64_t local_source_count = 0;
+  std::uint64_t local_active_target_count = 0;
+  std::uint64_t local_tree_node_count = 0;
+  std::uint64_t pm_solve_count = 0;
+  std::uint64_t pm_reuse_count = 0;
+  double mesh_spacing_comoving = 0.0;
+  double asmth_cells = 0.0;
+  double rcut_cells = 0.0;
+  double split_scale_comoving = 0.0;
+  double cutoff_radius_comoving = 0.0;
+  std::uint64_t residual_pruned_nodes = 0;
+  std::uint64_t residual_pair_skips_cutoff = 0;
+  std::uint64_t residual_pair_evaluations = 0;
+  std::uint64_t local_pair_evaluations = 0;
+  chui_treepm_stats stats{};  // raw C-ABI record (maximum depth, launches, ...)
+};
+
+// Phase timings in the shape of TreePmProfileEvent (tree_pm_coupling.hpp:505-524)
+// and TreeGravityProfile (tree_gravity.hpp:45-59); device times from CUDA events.
+struct TreeGravityProfile {
+  double build_ms = 0.0;
+  double multipole_ms = 0.0;
+  double traversal_ms = 0.0;
+  std::uint64_t build_count = 0;
+  std::uint64_t visited_nodes = 0;
+  std::uint64_t accepted_nodes = 0;
+  std::uint64_t opened_nodes = 0;
+  std::uint64_t particle_particle_interactions = 0;
+  std::uint64_t traversed_target_count = 0;
+  std::uint64_t actual_node_count = 0;
+};
+
+struct TreePmProfileEvent {
+  double pm_ms = 0.0;  // PM refresh (deposit, FFTs, Green, gradient) and interpolation
+  TreeGravityProfile tree_profile{};
+  double tree_short_range_ms = 0.0;
+  double coupling_overhead_ms = 0.0;
+  double source_preprocess_ms = 0.0;
+};
+
+// tree_softening.hpp:31-47. Only uniform softening (options) is supported;
+// a non-empty per-particle view is rejected.
+struct TreeSofteningView {
+  std::span<const std::uint32_t> source_species_tag{};
+  std::span<const double> source_particle_epsilon_comoving{};
+  std::span<const std::uint8_t> source_particle_epsilon_override_mask{};
+  std::span<const std::uint32_t> target_species_tag{};
+  std::span<const double> target_particle_epsilon_comoving{};
+  std::span<const std::uint8_t> target_particle_epsilon_override_mask{};
+  [[nodiscard]] bool empty() const noexcept {
+    return source_species_tag.empty() && source_particle_epsilon_comoving.empty() &&
+           source_particle_epsilon_override_mask.empty() && target_species_tag.empty() &&
+           target_particle_epsilon_comoving.empty() && target_particle_epsilon_override_mask.empty();
+  }
 };
 
 class TreePmCoordinator {
@@ -114,7 +186,12 @@ class TreePmCoordinator {
   void solveActiveSetWithPmCadence(std::span<const double> pos_x_comoving, std::span<const double> pos_y_comoving,
                                    std::span<const double> pos_z_comoving, std::span<const double> mass_code,
                                    const TreePmForceAccumulatorView& accumulator, const TreePmOptions& options,
-                                   bool refresh_long_range_field, TreePmDiagnostics* diagnostics = nullptr) {
+                                   bool refresh_long_range_field, TreePmProfileEvent* profile = nullptr,
+                                   TreePmDiagnostics* diagnostics = nullptr,
+                                   const TreeSofteningView& softening_view = {}) {
+    if (!softening_view.empty()) {
+      throw std::invalid_argument("B200 TreePM supports uniform softening only (per-particle softening view given)");
+    }
     if (pos_x_comoving.size() != pos_y_comoving.size() || pos_x_comoving.size() != pos_z_comoving.size() ||
         pos_x_comoving.size() != mass_code.size()) {
       throw std::invalid_argument("TreePM requires position and mass spans with equal extent");
@@ -123,6 +200,11 @@ class TreePmCoordinator {
     if (accumulator.accel_x_comoving.size() != targets || accumulator.accel_y_comoving.size() != targets ||
         accumulator.accel_z_comoving.size() != targets) {
       throw std::invalid_argument("TreePM force accumulator spans must have matching active-set extent");
+    }
+    if (!accumulator.previous_acceleration_magnitude_code.empty() &&
+        options.tree_options.opening_criterion == TreeOpeningCriterion::kRelativeForceError) {
+      throw std::invalid_argument(
+          "B200 TreePM implements the relative-force-error criterion only without previous accelerations");
     }
     configure(options);
     chui_treepm_sources src{};
@@ -169,18 +251,66 @@ class TreePmCoordinator {
     chui_treepm_stats stats{};
     check(chui_treepm_solve(m_handle, &src, &acc, refresh_long_range_field ? 1 : 0, CHUI_TREEPM_HOST, nullptr,
                             &stats));
-    if (diagnostics != nullptr) diagnostics->stats = stats;
+    if (diagnostics != nullptr) fillDiagnostics(stats, pos_x_comoving.size(), targets, refresh_long_range_field, *diagnostics);
+    if (profile != nullptr) {
+      *profile = TreePmProfileEvent{};
+      profile->pm_ms = stats.pm_ms;
+      profile->source_preprocess_ms = stats.tree_build_ms;
+      profile->tree_short_range_ms = stats.walk_ms;
+      profile->coupling_overhead_ms = stats.total_ms - stats.pm_ms - stats.tree_build_ms - stats.walk_ms;
+      TreeGravityProfile& t = profile->tree_profile;
+      t.build_ms = stats.tree_build_ms;
+      t.traversal_ms = stats.walk_ms;
+      t.build_count = 1;
+      t.visited_nodes = stats.visited_nodes;
+      t.accepted_nodes = stats.accepted_nodes;
+      t.opened_nodes = stats.opened_nodes;
+      t.particle_particle_interactions = stats.direct_pair_evaluations;
+      t.traversed_target_count = targets;
+      t.actual_node_count = stats.node_count;
+    }
   }
 
   void solveActiveSet(std::span<const double> pos_x_comoving, std::span<const double> pos_y_comoving,
                       std::span<const double> pos_z_comoving, std::span<const double> mass_code,
                       const TreePmForceAccumulatorView& accumulator, const TreePmOptions& options,
-                      TreePmDiagnostics* diagnostics = nullptr) {
+                      TreePmProfileEvent* profile = nullptr, TreePmDiagnostics* diagnostics = nullptr,
+                      const TreeSofteningView& softening_view = {}) {
     solveActiveSetWithPmCadence(pos_x_comoving, pos_y_comoving, pos_z_comoving, mass_code, accumulator, options,
-                                true, diagnostics);
+                                true, profile, diagnostics, softening_view);
   }
 
  private:
+  void fillDiagnostics(const chui_treepm_stats& s, std::size_t sources, std::size_t targets, bool refresh,
+                       TreePmDiagnostics& d) const {
+    d = TreePmDiagnostics{};
+    d.stats = s;
+    TreePmTraversalCounters& c = d.local_traversal;
+    c.visited_nodes = s.visited_nodes;
+    c.accepted_nodes = s.accepted_nodes;
+    c.opened_nodes = s.opened_nodes;
+    c.direct_pair_evaluations = s.direct_pair_evaluations;
+    c.cutoff_pruned_nodes = s.cutoff_pruned_nodes;
+    c.cutoff_skipped_pairs = s.cutoff_skipped_pairs;
+    c.accepted_internal_multipoles = s.accepted_internal_multipoles;
+    c.accepted_leaves = s.accepted_leaves;
+    c.targets = targets;
+    d.local_source_count = sources;
+    d.local_active_target_count = targets;
+    d.local_tree_node_count = s.node_count;
+    d.pm_solve_count = refresh ? 1U : 0U;
+    d.pm_reuse_count = refresh ? 0U : 1U;
+    d.mesh_spacing_comoving = m_spacing;
+    d.asmth_cells = m_asmth;
+    d.rcut_cells = m_rcut;
+    d.split_scale_comoving = m_asmth * m_spacing;
+    d.cutoff_radius_comoving = m_rcut * m_spacing;
+    d.residual_pruned_nodes = s.cutoff_pruned_nodes;
+    d.residual_pair_skips_cutoff = s.cutoff_skipped_pairs;
+    d.residual_pair_evaluations = s.direct_pair_evaluations;
+    d.local_pair_evaluations = s.direct_pair_evaluations;
+  }
+
   void configure(const TreePmOptions& o) {
     chui_treepm_config c{};
     chui_treepm_config_default(&c);
@@ -207,6 +337,10 @@ class TreePmCoordinator {
     c.acceptance_policy = o.acceptance_policy == TreePmAcceptancePolicy::kStrictReference ? 0 : 1;
     c.precision = o.precision == Precision::kFp64 ? CHUI_TREEPM_FP64 : CHUI_TREEPM_MIXED;
     c.device = o.device;
+    // split scale and cutoff are in units of the mean mesh spacing (gravity_runtime.cpp:586-590)
+    m_spacing = std::cbrt((c.box_x / c.pm_grid_nx) * (c.box_y / c.pm_grid_ny) * (c.box_z / c.pm_grid_nz));
+    m_asmth = c.asmth_cells;
+    m_rcut = c.rcut_cells;
     if (m_handle == nullptr) {
       check(chui_treepm_create(&c, &m_handle));
     } else {
@@ -235,6 +369,9 @@ class TreePmCoordinator {
 
   PmGridShape m_shape;
   void* m_handle = nullptr;
+  double m_spacing = 0.0;
+  double m_asmth = 0.0;
+  double m_rcut = 0.0;
 };
 
 }  // namespace chui::b200
