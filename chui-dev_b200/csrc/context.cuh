@@ -93,6 +93,7 @@ struct Context {
   DevBuf node_com;     // double4 {comx, comy, comz, mass}
   DevBuf node_quad;    // 8 doubles per node {qxx, qxy, qxz, qyy, qyz, qzz, trace, com_center_offset}
   DevBuf node_f4;      // float4 {com - centre (x, y, z), |centre - com|}: FP32 node frame of the walk
+  DevBuf node_hmin;    // float: smallest half-size of an internal descendant (rounded down; +inf if none)
   DevBuf node_child;   // 8 u32 per node
   DevBuf node_range;   // uint4 {begin, count, child_count | leaf flag, subtree_end}
   DevBuf node_parent;  // u32
@@ -102,6 +103,7 @@ struct Context {
   DevBuf pos_of_row;   // u32 per caller row: tree position
   DevBuf src_f4;       // float4 per tree position: offset from leaf centre (FP32) + mass
   DevBuf src_d4;       // double4 per tree position: caller position + mass (FP64 path)
+  DevBuf src_u4;       // double4 per tree position: unwrapped (tree frame) position + mass (mixed path)
   DevBuf target_order; // visit order of active slots
   DevBuf morton_sorted;  // sorted Morton keys (diagnostic parity output)
 

@@ -570,10 +570,23 @@ __device__ void internalMoments(int64_t node, const double4 g, const uint32_t* _
 
 // Bottom-up moments: each leaf computes itself, then the last child to finish
 // a parent computes it from its children in octant order (deterministic).
+// Smallest half-size among the internal descendants of `node` (children are
+// complete when this runs), rounded toward zero so that it bounds from below.
+__device__ float descendantHalfMin(int64_t node, const double4* __restrict__ geom, const uint4* __restrict__ range,
+                                   const uint32_t* child, const float* hmin) {
+  float v = INFINITY;
+  for (int o = 0; o < 8; ++o) {
+    const uint32_t c = __ldcg(child + 8 * node + o);
+    if (c == kInvalid || range[c].z == 0) continue;
+    v = fminf(v, fminf(__double2float_rz(geom[c].w), __ldcg(hmin + c)));
+  }
+  return v;
+}
+
 __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restrict__ geom,
                               const uint4* __restrict__ range, const uint32_t* __restrict__ parent,
                               const uint32_t* __restrict__ child, uint32_t* counter, double4* com,
-                              double* quad) {
+                              double* quad, float* hmin) {
   for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nodes;
        k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const uint4 r = range[k];
@@ -583,6 +596,7 @@ __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restr
     leafMoments(k, in, geom[k], r, &cm, q);
     com[k] = cm;
     for (int t = 0; t < 8; ++t) quad[8 * k + t] = q[t];
+    hmin[k] = INFINITY;
     int64_t node = k;
     while (true) {
       __threadfence();
@@ -594,6 +608,7 @@ __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restr
       internalMoments(p, geom[p], child, com, quad, in.quadrupole, &cm, q);
       com[p] = cm;
       for (int t = 0; t < 8; ++t) quad[8 * static_cast<size_t>(p) + t] = q[t];
+      hmin[p] = descendantHalfMin(p, geom, range, child, hmin);
       node = p;
     }
   }
@@ -646,7 +661,8 @@ __global__ void packSourcesKernel(int64_t n, const uint32_t* __restrict__ sorted
                                   const double* __restrict__ uy, const double* __restrict__ uz,
                                   const double* __restrict__ x, const double* __restrict__ y,
                                   const double* __restrict__ z, const double* __restrict__ m,
-                                  double uniform_mass, float4* f4, double4* d4, uint32_t* pos_of_row) {
+                                  double uniform_mass, float4* f4, double4* d4, double4* u4,
+                                  uint32_t* pos_of_row) {
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < n;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const uint32_t s = sorted[t];
@@ -658,6 +674,7 @@ __global__ void packSourcesKernel(int64_t n, const uint32_t* __restrict__ sorted
                           static_cast<float>(uz[s] - g.z), static_cast<float>(ms));
     }
     if (d4) d4[t] = make_double4(x[s], y[s], z[s], ms);
+    if (u4) u4[t] = make_double4(ux[s], uy[s], uz[s], ms);
   }
 }
 
@@ -879,7 +896,8 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   if (ensure(c.node_geom, total_nodes * sizeof(double4)) || ensure(c.node_com, total_nodes * sizeof(double4)) ||
       ensure(c.node_quad, total_nodes * 8 * sizeof(double)) || ensure(c.node_child, total_nodes * 8 * 4) ||
       ensure(c.node_range, total_nodes * sizeof(uint4)) || ensure(c.node_parent, total_nodes * 4) ||
-      ensure(c.node_depth, total_nodes * 4) || ensure(c.node_counter, total_nodes * 4))
+      ensure(c.node_depth, total_nodes * 4) || ensure(c.node_counter, total_nodes * 4) ||
+      ensure(c.node_hmin, total_nodes * sizeof(float)))
     return CHUI_TREEPM_ENOMEM;
   NodeOut out;
   out.geom = c.node_geom.as<double4>();
@@ -921,7 +939,8 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   mi.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
   { noteLaunch(); momentsKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(total_nodes, mi, out.geom, out.range, out.parent,
                                                           out.child, c.node_counter.as<uint32_t>(),
-                                                          c.node_com.as<double4>(), c.node_quad.as<double>()); }
+                                                          c.node_com.as<double4>(), c.node_quad.as<double>(),
+                                                          c.node_hmin.as<float>()); }
   if (ensure(c.node_f4, total_nodes * sizeof(float4))) return CHUI_TREEPM_ENOMEM;
   { noteLaunch(); nodeFrameKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.geom, c.node_com.as<double4>(),
                                                             c.node_quad.as<double>(), c.node_f4.as<float4>()); }
@@ -931,10 +950,12 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     if (ensure(c.src_f4, n * sizeof(float4))) return CHUI_TREEPM_ENOMEM;
   }
   if (ensure(c.src_d4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
+  if (mixed && ensure(c.src_u4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
   { noteLaunch(); packSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), out.leaf_of_pos, out.geom,
                                                     u[0], u[1], u[2], x, y, z, m, uniform_mass,
                                                     mixed ? c.src_f4.as<float4>() : nullptr,
-                                                    c.src_d4.as<double4>(), c.pos_of_row.as<uint32_t>()); }
+                                                    c.src_d4.as<double4>(), mixed ? c.src_u4.as<double4>() : nullptr,
+                                                    c.pos_of_row.as<uint32_t>()); }
   // maximum depth (for stack sizing and stats)
   {
     size_t bytes = 0;

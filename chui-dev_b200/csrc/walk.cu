@@ -25,6 +25,14 @@
 // pair). Per-leaf FP32 partial sums are added into FP64 accumulators. The
 // FP64 configuration evaluates the reference's formulas (source metric per
 // pair, erf/exp residual) unchanged.
+//
+// With diagnostics on, the walk reproduces the reference's traversal counters
+// exactly. With diagnostics off (production), an opened node whose internal
+// descendants provably fail the strict envelope for every opening lane is
+// evaluated as one block of sources instead of being descended: the lane's
+// pair set (every source within r_cut outside accepted multipoles) is the
+// same, the number of warp traversal steps drops several-fold, and no
+// counters are kept.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -55,6 +63,8 @@ struct WalkArgs {
   const float4* src_f4;
   const double4* src_d4;
   const float4* node_f4;
+  const float* hmin;       // smallest internal-descendant half-size per node
+  const double4* src_u4;   // tree-ordered unwrapped positions + mass (mixed)
   double* out_x;   // per slot, short-range part
   double* out_y;
   double* out_z;
@@ -364,6 +374,22 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
 
 constexpr int kQueue = 64;  // sources per warp batch
 
+// Subtree blocks of the production walk (diagnostics off): an opened node
+// with at most kBulkCount sources and half-size at most kBulkHalf * r_cut is
+// evaluated as one block of sources when no internal descendant can pass the
+// strict envelope for any lane that opened it.
+#ifndef CHUI_BULK_COUNT
+#define CHUI_BULK_COUNT 1024
+#endif
+#ifndef CHUI_BULK_HALF
+#define CHUI_BULK_HALF 1.0
+#endif
+#ifndef CHUI_WALK_MIN_BLOCKS
+#define CHUI_WALK_MIN_BLOCKS 5  // resident blocks per SM the register budget is sized for
+#endif
+constexpr uint32_t kBulkCount = CHUI_BULK_COUNT;
+constexpr double kBulkHalf = CHUI_BULK_HALF;
+
 // H(t) in Estrin form: same polynomial as polyHFixed<12>, dependency depth 5.
 __device__ __forceinline__ float polyH12(const PolyH& p, float t) {
   const float s = fmaf(t, p.scale, -1.0f);
@@ -484,7 +510,7 @@ __device__ __forceinline__ int certainLess(float a, float b) {
 // group's cutoff sphere are dropped at enqueue) tagged with the ballot of
 // accepting lanes, and evaluated 64 sources at a time in FP32.
 template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous>
-__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(WalkArgs a) {
+__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS) walkFastKernel(WalkArgs a) {
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
   __shared__ float4 q_src[kWalkWarpsPerBlock][kQueue];
   __shared__ uint2 q_meta[kWalkWarpsPerBlock][kQueue];
@@ -498,6 +524,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(Wal
   const float cut2 = w.cut2_f;
   const float env2 = 0.0064f;  // 0.08^2
   const float theta2 = static_cast<float>(w.theta * w.theta);
+  const double bulk_half = kBulkHalf * w.cutoff;
 
   while (true) {
     uint32_t cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0, cnt_skips = 0,
@@ -584,6 +611,49 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(Wal
       __syncwarp();
     };
 
+    // Append sources [begin, begin+count) for the lanes in `mask`, as FP32
+    // offsets from the warp's reference target; sources outside the group's
+    // cutoff sphere are dropped. Leaf records are offsets from the leaf centre
+    // (src_f4); subtree blocks read tree-frame FP64 positions (src_u4). Either
+    // way the offset is formed in FP64 and rounded once.
+    auto enqueue = [&](uint32_t begin, uint32_t count, uint32_t mask, bool whole, const double4& g, double cdx,
+                       double cdy, double cdz) {
+      for (uint32_t chunk = 0; chunk < count; chunk += 32) {
+        const uint32_t k = chunk + lane;
+        float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool keep = false;
+        if (k < count) {
+          if (whole) {
+            const double4 u = a.src_u4[begin + k];
+            e = make_float4(static_cast<float>((u.x - g.x) + cdx), static_cast<float>((u.y - g.y) + cdy),
+                            static_cast<float>((u.z - g.z) + cdz), static_cast<float>(u.w));
+          } else {
+            const float4 sv = a.src_f4[begin + k];
+            e = make_float4(static_cast<float>(static_cast<double>(sv.x) + cdx),
+                            static_cast<float>(static_cast<double>(sv.y) + cdy),
+                            static_cast<float>(static_cast<double>(sv.z) + cdz), sv.w);
+          }
+          keep = fmaf(e.x, e.x, fmaf(e.y, e.y, e.z * e.z)) <= cull2;
+        }
+        const uint32_t keep_mask = __ballot_sync(0xffffffffu, keep);
+        const int c = __popc(keep_mask);
+        if (qn + c > kQueue) flush();
+        if (keep) {
+          const int slot_q = qn + __popc(keep_mask & (lane_bit - 1u));
+          uint32_t m = mask;
+          if constexpr (kContiguous) {
+            // targets are tree positions base..base+31: drop the source's own lane
+            const uint32_t rel = begin + k - base;
+            if (rel < 32u) m &= ~(1u << rel);
+          }
+          q_src[warp][slot_q] = e;
+          q_meta[warp][slot_q] = make_uint2(m, begin + k);
+        }
+        __syncwarp();
+        qn += c;
+      }
+    };
+
     while (sp > 0) {
       const uint32_t node = stack[sp - 1];
       --sp;
@@ -651,7 +721,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(Wal
         mdy = d.dy;
         mdz = d.dz;
       }
-      if (act) {
+      if (kDiag && act) {
         ++cnt_visited;
         cnt_pruned += prune ? 1 : 0;
       }
@@ -659,40 +729,13 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(Wal
         const bool want = act && !prune;
         const uint32_t mask = __ballot_sync(0xffffffffu, want);
         if (mask == 0u) continue;
-        if (want) {
+        if (kDiag && want) {
           ++cnt_accepted;
           ++cnt_leaves;
         }
         const uint32_t begin = rg4.x, count = rg4.y;
         if (w.cutoff + h + rga < half_min_box && h < w.exact_half) {
-          for (uint32_t chunk = 0; chunk < count; chunk += 32) {
-            const uint32_t k = chunk + lane;
-            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-            bool keep = false;
-            if (k < count) {
-              const float4 sv = a.src_f4[begin + k];
-              e = make_float4(static_cast<float>(static_cast<double>(sv.x) + cdx),
-                              static_cast<float>(static_cast<double>(sv.y) + cdy),
-                              static_cast<float>(static_cast<double>(sv.z) + cdz), sv.w);
-              keep = fmaf(e.x, e.x, fmaf(e.y, e.y, e.z * e.z)) <= cull2;
-            }
-            const uint32_t keep_mask = __ballot_sync(0xffffffffu, keep);
-            const int c = __popc(keep_mask);
-            if (qn + c > kQueue) flush();
-            if (keep) {
-              const int slot_q = qn + __popc(keep_mask & (lane_bit - 1u));
-              uint32_t m = mask;
-              if constexpr (kContiguous) {
-                // targets are tree positions base..base+31: drop the source's own lane
-                const uint32_t rel = begin + k - base;
-                if (rel < 32u) m &= ~(1u << rel);
-              }
-              q_src[warp][slot_q] = e;
-              q_meta[warp][slot_q] = make_uint2(m, begin + k);
-            }
-            __syncwarp();
-            qn += c;
-          }
+          enqueue(begin, count, mask, false, g, cdx, cdy, cdz);
         } else {
           unsigned long long p = 0, sk = 0;
           exactLeafPairs(a, exact_sm[warp], begin, count, want, px, py, pz, self_pos, acc_x, acc_y, acc_z,
@@ -706,8 +749,10 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(Wal
       const bool do_accept = act && !prune && accept;
       const bool open = act && !prune && !accept;
       if (do_accept) {
-        ++cnt_accepted;
-        ++cnt_multi;
+        if constexpr (kDiag) {
+          ++cnt_accepted;
+          ++cnt_multi;
+        }
         if (!need_exact) {
           const ExactDecision d = exactNodeDecision(a, node, px, py, pz, skip_self);
           mdx = d.dx;
@@ -717,8 +762,32 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(Wal
         multipoleForce(a, node, mdx, mdy, mdz, w.eps, acc_x, acc_y, acc_z);
       }
       if (act && (prune || accept)) skip_until = rg4.w;
-      if (open) ++cnt_opened;
+      if (kDiag && open) ++cnt_opened;
       if (__any_sync(0xffffffffu, open)) {
+        if constexpr (!kDiag) {
+          // Subtree block: every source of this node within r_cut of an
+          // opening lane is one of that lane's reference pairs unless an
+          // internal descendant would be accepted as a multipole, which the
+          // strict envelope 2h/r < 0.08 rules out when 2 h_min >= 0.08 R,
+          // h_min the smallest internal-descendant half-size and R the
+          // largest target-to-cube distance (an upper bound on every
+          // descendant COM distance). Pairs beyond r_cut are dropped per pair
+          // as in the leaf path, so the lane's sum is the reference's.
+          if (fast_frame && rg4.y <= kBulkCount && h <= bulk_half && w.cutoff + h + rga < half_min_box &&
+              h < w.exact_half) {
+            bool ok = true;
+            if (open && w.quadrupole) {
+              const float hf = static_cast<float>(h);
+              const float qx = fabsf(ndx) + hf, qy = fabsf(ndy) + hf, qz = fabsf(ndz) + hf;
+              const float hm = a.hmin[node];
+              ok = 4.0f * hm * hm >= 0.0064f * 1.001f * fmaf(qx, qx, fmaf(qy, qy, qz * qz));
+            }
+            if (__all_sync(0xffffffffu, ok)) {
+              enqueue(rg4.x, rg4.y, __ballot_sync(0xffffffffu, open), true, g, cdx, cdy, cdz);
+              continue;
+            }
+          }
+        }
         const uint32_t ch = lane < 8 ? a.child[8 * static_cast<size_t>(node) + lane] : kInvalid;
         const unsigned cmask = __ballot_sync(0xffffffffu, ch != kInvalid) & 0xFFu;
         const int nc = __popc(cmask);
@@ -739,12 +808,14 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkFastKernel(Wal
       a.out_z[slot] = acc_z;
       a.out_near[slot] = kDiag ? static_cast<double>(nearest_f) : INFINITY;
     }
-    uint32_t c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs, cnt_pruned, cnt_skips, cnt_multi, cnt_leaves};
-    for (int k = 0; k < 8; ++k) {
-      for (int off = 16; off > 0; off >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], off);
-    }
-    if (lane == 0) {
-      for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, static_cast<unsigned long long>(c[k]));
+    if constexpr (kDiag) {
+      uint32_t c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs, cnt_pruned, cnt_skips, cnt_multi, cnt_leaves};
+      for (int k = 0; k < 8; ++k) {
+        for (int off = 16; off > 0; off >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], off);
+      }
+      if (lane == 0) {
+        for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, static_cast<unsigned long long>(c[k]));
+      }
     }
     __syncwarp();
   }
@@ -815,6 +886,8 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.src_f4 = c.src_f4.as<float4>();
   a.src_d4 = c.src_d4.as<double4>();
   a.node_f4 = c.node_f4.as<float4>();
+  a.hmin = c.node_hmin.as<float>();
+  a.src_u4 = c.src_u4.as<double4>();
   double* acc = c.tree_acc.as<double>();
   a.out_x = acc;
   a.out_y = acc + nt;

@@ -105,14 +105,43 @@ def test_fp64_matches_reference(cuda_ok, name):
 
 
 @pytest.mark.parametrize("name", CASES)
-def test_mixed_precision_matches_reference(cuda_ok, name):
+@pytest.mark.parametrize("diagnostics", [1, 0])
+def test_mixed_precision_matches_reference(cuda_ok, name, diagnostics):
+    """diagnostics=0 is the production walk (subtree blocks, no counters)."""
     g = load_golden(name)
     act = _active(g)
-    with ct.TreePmCoordinator(cfg_for(g, ct._abi.MIXED)) as s:
+    cfg = cfg_for(g, ct._abi.MIXED)
+    cfg.diagnostics = diagnostics
+    with ct.TreePmCoordinator(cfg) as s:
         r = s.solve_active_set(g["x"], g["y"], g["z"], g["m"], active=act)
     e = rel_err([r["ax"], r["ay"], r["az"]], [g["ax"], g["ay"], g["az"]])
     assert np.median(e) <= 1e-4, np.median(e)
     assert np.percentile(e, 99) <= 1e-3, np.percentile(e, 99)
+
+
+@pytest.mark.parametrize("n_side,halos", [(48, 60), (64, 120)])
+def test_production_walk_matches_diagnostic_walk(cuda_ok, n_side, halos):
+    """Clustered boxes where many opened nodes qualify as subtree blocks: the
+    production walk sums the same pairs as the per-node walk (FP32 summation
+    order differs), and both agree with the FP64 walk to the mixed bar."""
+    from chui_treepm import ics
+    box = 50.0
+    x, y, z, *_ = ics.clustered_box(n_side ** 3, box, 0.6, halos, 3.0, 0.5, 7)
+    m = np.full(len(x), 1.0 / len(x))
+    res = {}
+    for key, prec, diag in (("d1", ct._abi.MIXED, 1), ("d0", ct._abi.MIXED, 0), ("f64", ct._abi.FP64, 1)):
+        cfg = ct.TreePmConfig(pm_grid_nx=n_side, pm_grid_ny=n_side, pm_grid_nz=n_side, box_x=box, box_y=box,
+                              box_z=box, opening_theta=0.6, max_leaf_size=16, softening=0.002, precision=prec,
+                              diagnostics=diag)
+        with ct.TreePmCoordinator(cfg) as s:
+            r = s.solve_active_set(x, y, z, m, short_range=True)
+            res[key] = [r["tree_ax"], r["tree_ay"], r["tree_az"]]
+    e_order = rel_err(res["d0"], res["d1"])
+    assert np.median(e_order) <= 1e-5, np.median(e_order)
+    assert np.percentile(e_order, 99) <= 1e-4, np.percentile(e_order, 99)
+    e64 = rel_err(res["d0"], res["f64"])
+    assert np.median(e64) <= 1e-4, np.median(e64)
+    assert np.percentile(e64, 99) <= 1e-3, np.percentile(e64, 99)
 
 
 def test_cic_cells_and_density_bit_exact(cuda_ok):
