@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -920,6 +921,90 @@ int chui_treepm_drift(void* handle, int64_t n, double* x, double* y, double* z, 
     cudaMemcpyAsync(z, dz, n * 8, cudaMemcpyDeviceToHost, s);
   }
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "drift failed");
+}
+
+}  // extern "C"
+
+// ---- allocation-free density (chui_pm_assign_density_static) ----
+
+// Accumulation grid of chui_pm_assign_density_static, one per device (module
+// globals are per device). Zero at module load; every call zeroes it again
+// before depositing.
+static __device__ __align__(256) double g_static_density[CHUI_PM_STATIC_MAX_CELLS];
+
+namespace {
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mutex;                              // one call at a time per process
+void* g_static_density_ptr[kStaticMaxDevices] = {};     // device address, looked up on first use
+
+bool onDevice(const void* p, int device) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == device;
+}
+
+int staticFail(int code, const std::string& msg) {
+  g_create_error = msg;
+  return code;
+}
+}  // namespace
+
+extern "C" {
+
+int chui_pm_assign_density_static(const chui_treepm_config* cfg, const chui_treepm_sources* src, double* density,
+                                  int density_memory, void* stream) {
+  if (!cfg || !src || !density) return staticFail(CHUI_TREEPM_EINVAL, "config, sources and density must be non-null");
+  std::string err;
+  int rc = chui::validateConfig(*cfg, err);
+  if (rc) return staticFail(rc, err);
+  const double cells_d = static_cast<double>(cfg->pm_grid_nx) * static_cast<double>(cfg->pm_grid_ny) *
+                         static_cast<double>(cfg->pm_grid_nz);
+  if (cells_d > static_cast<double>(CHUI_PM_STATIC_MAX_CELLS)) {
+    return staticFail(CHUI_TREEPM_ERANGE, "PM mesh of " + std::to_string(static_cast<long long>(cells_d)) +
+                                              " cells exceeds the static scratch grid of " +
+                                              std::to_string(CHUI_PM_STATIC_MAX_CELLS) + " cells");
+  }
+  const size_t cells = static_cast<size_t>(cells_d);
+  if (density_memory != CHUI_TREEPM_HOST && density_memory != CHUI_TREEPM_DEVICE)
+    return staticFail(CHUI_TREEPM_EINVAL, "density_memory must be CHUI_TREEPM_HOST or CHUI_TREEPM_DEVICE");
+  const int64_t n = src->count;
+  if (n < 0) return staticFail(CHUI_TREEPM_EINVAL, "source count must be >= 0");
+  if (n > 0 && (!src->x || !src->y || !src->z))
+    return staticFail(CHUI_TREEPM_EINVAL, "source positions must be non-null");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return staticFail(CHUI_TREEPM_EDEVICE, "no CUDA device is available");
+  if (cfg->device < 0 || cfg->device >= ndev || cfg->device >= kStaticMaxDevices)
+    return staticFail(CHUI_TREEPM_EINVAL, "device ordinal out of range");
+
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  chui::DeviceGuard guard(cfg->device);
+  if (n > 0 && (!onDevice(src->x, cfg->device) || !onDevice(src->y, cfg->device) ||
+                !onDevice(src->z, cfg->device) || (src->mass && !onDevice(src->mass, cfg->device))))
+    return staticFail(CHUI_TREEPM_EINVAL, "positions and masses must be device memory on the configured device");
+  if (density_memory == CHUI_TREEPM_DEVICE && !onDevice(density, cfg->device))
+    return staticFail(CHUI_TREEPM_EINVAL, "density must be device memory on the configured device");
+  void*& scratch = g_static_density_ptr[cfg->device];
+  if (scratch == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_density);
+    if (e != cudaSuccess || p == nullptr)
+      return staticFail(CHUI_TREEPM_EDEVICE, std::string("static scratch lookup failed: ") + cudaGetErrorString(e));
+    scratch = p;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* grid = static_cast<double*>(scratch);
+  rc = chui::pmDensityInto(*cfg, n, src->x, src->y, src->z, src->mass, src->uniform_mass, grid, s);
+  if (rc) return staticFail(rc, "PM density launch failed");
+  if (cudaMemcpyAsync(density, grid, cells * sizeof(double),
+                      density_memory == CHUI_TREEPM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                      s) != cudaSuccess)
+    return staticFail(CHUI_TREEPM_EDEVICE, "density copy failed");
+  if (cudaStreamSynchronize(s) != cudaSuccess) return staticFail(CHUI_TREEPM_EDEVICE, "PM density kernels failed");
+  return 0;
 }
 
 }  // extern "C"

@@ -130,6 +130,9 @@ int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const
                   const double* m, double uniform_mass, double* rho_out, cudaStream_t s);
 int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,
             int64_t* cells, cudaStream_t s);
+// Density into a caller-provided compact grid of nx*ny*nz doubles; no allocation.
+int pmDensityInto(const chui_treepm_config& cfg, int64_t n, const double* x, const double* y, const double* z,
+                  const double* m, double uniform_mass, double* rho, cudaStream_t s);
 void pmDestroy(Context& c);
 
 // ---- tree (tree.cu) ----

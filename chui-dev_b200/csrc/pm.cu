@@ -463,6 +463,32 @@ int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const
   return 0;
 }
 
+// Density into a caller-provided compact FP64 grid, with no allocation (the
+// allocation-free entry point): zero the grid, deposit, divide by the cell
+// volume. Same kernels and arithmetic as pmDensityOnly.
+int pmDensityInto(const chui_treepm_config& cfg, int64_t n, const double* x, const double* y, const double* z,
+                  const double* m, double uniform_mass, double* rho, cudaStream_t s) {
+  PmGeom g;
+  g.n[0] = cfg.pm_grid_nx;
+  g.n[1] = cfg.pm_grid_ny;
+  g.n[2] = cfg.pm_grid_nz;
+  g.nzc = g.n[2] / 2 + 1;
+  g.nzp = 2 * g.nzc;
+  g.L[0] = cfg.box_x;
+  g.L[1] = cfg.box_y;
+  g.L[2] = cfg.box_z;
+  for (int a = 0; a < 3; ++a) g.inv_d[a] = static_cast<double>(g.n[a]) / g.L[a];
+  g.scheme = cfg.assignment_scheme;
+  const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
+  const int block = 256;
+  if (cudaMemsetAsync(rho, 0, cells * sizeof(double), s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  if (n > 0)
+    { noteLaunch(); depositCompactKernel<<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass, g, rho); }
+  const double cell_volume = (g.L[0] * g.L[1] * g.L[2]) / static_cast<double>(cells);
+  { noteLaunch(); scaleKernel<<<gridFor(cells, block), block, 0, s>>>(rho, cells, cell_volume); }
+  return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
+}
+
 int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,
             int64_t* cells, cudaStream_t s) {
   const PmGeom g = geomOf(c);

@@ -143,6 +143,30 @@ int chui_treepm_solve(void *handle, const chui_treepm_sources *sources,
 int chui_pm_assign_density(void *handle, const chui_treepm_sources *sources, double *density,
                            int memory, void *stream);
 
+/* Allocation-free form of chui_pm_assign_density. No counterpart in the
+ * reference, which always allocates its mesh.
+ *
+ * For callers that must not allocate device memory during the call: code
+ * running while another allocator (a framework's caching pool) holds the
+ * device's free memory, where cudaMalloc would fail, and code that must not
+ * pay cudaFree's device-wide synchronisation between steps. It takes no
+ * handle (creating one allocates). The accumulation grid is a fixed scratch
+ * array inside the library, CHUI_PM_STATIC_MAX_CELLS doubles (2 MiB) per
+ * device, so meshes with nx*ny*nz above that fail with CHUI_TREEPM_ERANGE.
+ * Positions and masses (mass may be NULL: uniform_mass) must be device memory
+ * on config->device; density (nx*ny*nz doubles, row-major, mass / cell volume)
+ * is host or device memory as density_memory says. The call zeroes the
+ * scratch grid itself; nothing has to start at zero.
+ *
+ * The first call on a device looks up the scratch address (per-device set-up);
+ * make it before any stream capture on that device. All calls on a device in
+ * one process share the scratch grid and overlapping calls would race, so each
+ * call holds a process-wide lock and waits for its stream before returning.
+ * Errors: chui_treepm_last_error(NULL) describes the last failure. */
+#define CHUI_PM_STATIC_MAX_CELLS 262144
+int chui_pm_assign_density_static(const chui_treepm_config *config, const chui_treepm_sources *sources,
+                                  double *density, int density_memory, void *stream);
+
 /* Base mesh cell per axis of each particle's assignment stencil after the
  * periodic wrap (makeAxisStencil / wrapIndex, pm_solver.cpp:103-116, :925-951):
  * cells[3*i + a]. The parity check on cell indices uses this. */
