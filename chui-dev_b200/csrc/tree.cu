@@ -73,12 +73,17 @@ __global__ void wrapBucketKernel(int64_t n, const double* __restrict__ in, doubl
 }
 
 // Largest circular gap over occupied buckets: gap = next - current with the
-// wrap-around next = first + L (tree_pm_coupling.cpp:189-207).
-__global__ void bucketGapKernel(unsigned long long nb, const unsigned long long* __restrict__ bmin_rev,
+// wrap-around next = first + L (tree_pm_coupling.cpp:189-207). Pass 0 finds
+// the largest gap (gaps are >= 0, so their bit patterns order like the
+// values; reduced per block, one atomic per block); pass 1 takes the smallest
+// anchor among the buckets whose gap equals it.
+__global__ void __launch_bounds__(256) bucketGapKernel(unsigned long long nb, const unsigned long long* __restrict__ bmin_rev,
                                 const unsigned long long* __restrict__ bmax,
                                 const unsigned long long* __restrict__ later_min_rev, double box,
                                 unsigned long long global_min, unsigned long long* best_gap,
                                 int pass, unsigned long long* best_anchor) {
+  unsigned long long local = 0ull;
+  const unsigned long long target = pass == 0 ? 0ull : *best_gap;
   for (unsigned long long b = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
        b < nb; b += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
     const unsigned long long rb = nb - 1 - b;
@@ -95,10 +100,25 @@ __global__ void bucketGapKernel(unsigned long long nb, const unsigned long long*
     }
     const double gap = next - cur;
     if (pass == 0) {
-      atomicMax(best_gap, dbits(gap));
-    } else if (dbits(gap) == *best_gap) {
+      const unsigned long long g = dbits(gap);
+      local = g > local ? g : local;
+    } else if (dbits(gap) == target) {
       atomicMin(best_anchor, dbits(cand));
     }
+  }
+  if (pass != 0) return;
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(0xffffffffu, local, off);
+    local = o > local ? o : local;
+  }
+  __shared__ unsigned long long warp_max[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) warp_max[warp] = local;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long v = 0ull;
+    for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) v = warp_max[k] > v ? warp_max[k] : v;
+    if (v != 0ull) atomicMax(best_gap, v);
   }
 }
 
