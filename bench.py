@@ -49,11 +49,19 @@ WORKLOADS = {
 }
 METRIC = "particle-forces/s at 256^3 (mixed precision TreePM, one KDK step per step)"
 UNIT = "particle-forces/s"
-# FP32 operations per direct pair of the mixed walk (csrc/walk.cu): separation
-# 3, r^2 5, t 1, H(t) polynomial 2*terms (12 terms), softening 1, rsqrt 1,
-# r^-3 2, residual 2, G*m*K 2, accumulate 6 -> 47; node visit and multipole
-# work are counted separately (FP64 decisions).
-FLOPS_PER_PAIR = 47.0
+# Algorithmic FLOP convention of the walk (fixed, independent of how a kernel
+# evaluates the kernel function): 28 per direct pair (3 sub, r^2 5, +eps^2 1,
+# rsqrt 1, r^-3 2, residual ~10, accumulate 6), 90 per accepted multipole
+# (screened quadrupole), 12 per node visit. Counts are the reference's
+# traversal counters for the timed state (the FP64 walk reproduces them).
+FLOPS_PER_PAIR = 28.0
+FLOPS_PER_MULTIPOLE = 90.0
+FLOPS_PER_VISIT = 12.0
+# The differentiable case: 64^3 lattice + Zel'dovich (P ~ k^-2, 0.3 spacing
+# rms) in a box of 50, mesh 64^3, theta 0.5, 10 KDK steps of 0.05 at unit mean
+# density (G = 1), softening 0.1 spacing, loss = MSE(CIC density of the final
+# positions, target).
+ADJOINT = dict(n_side=64, box=50.0, steps=10, dt=0.05, theta=0.5, eps_spacing=0.1)
 
 
 def log(*a):
@@ -147,6 +155,71 @@ def gpu_step(solver, t, acc, factors, stream):
     r = solver.solve_active_set(t["x"], t["y"], t["z"], t["m"], stream=stream)
     solver.kick(t["vx"], t["vy"], t["vz"], r["ax"], r["ay"], r["az"], k2, g2, stream=stream)
     return r
+
+
+def adjoint_bench(torch, ct, dev, local: int) -> dict:
+    """Forward (10 KDK steps with one checkpoint per step, then the density
+    loss) and backward (the gradient with respect to the initial
+    displacements) through chui_treepm.adjoint, timed with CUDA events."""
+    from chui_treepm import adjoint, ics
+    a = ADJOINT
+    n_side, box = a["n_side"], a["box"]
+    spacing = box / n_side
+    g = (np.arange(n_side) + 0.5) * spacing
+    q = [torch.tensor(v.ravel(), device=dev) for v in np.meshgrid(g, g, g, indexing="ij")]
+    _, _, _, sx, sy, sz = ics.zeldovich_lattice(n_side, box, 0.3, 101)
+    _, _, _, tx, ty, tz = ics.zeldovich_lattice(n_side, box, 0.3, 202)
+    mass = torch.full((n_side ** 3,), box ** 3 / n_side ** 3, dtype=torch.float64, device=dev)
+
+    def cfg(precision):
+        return ct.TreePmConfig(pm_grid_nx=n_side, pm_grid_ny=n_side, pm_grid_nz=n_side, box_x=box, box_y=box,
+                               box_z=box, opening_theta=a["theta"], max_leaf_size=16,
+                               softening=a["eps_spacing"] * spacing,
+                               assignment_scheme=ct._abi.CIC, window_deconvolution=1, precision=precision,
+                               device=local, diagnostics=0)
+
+    with ct.TreePmCoordinator(cfg(ct._abi.MIXED)) as solver, ct.TreePmCoordinator(cfg(ct._abi.MIXED)) as dens:
+        target = dens.assign_density(*[q[k] + torch.tensor(v, device=dev) for k, v in enumerate((tx, ty, tz))],
+                                     mass).reshape(n_side, n_side, n_side)
+        times = []
+        for _ in range(3):
+            s = [torch.tensor(v, device=dev, requires_grad=True) for v in (sx, sy, sz)]
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            torch.cuda.synchronize()
+            e[0].record()
+            xn = adjoint.kdk(solver, *[q[k] + s[k] for k in range(3)], *s, mass, a["steps"], a["dt"])
+            rho = adjoint.cic_density(dens, xn[0], xn[1], xn[2], mass)
+            loss = ((rho - target) ** 2).mean()
+            e[1].record()
+            loss.backward()
+            e[2].record()
+            torch.cuda.synchronize()
+            times.append((e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])))
+        fwd, bwd = min(t[0] for t in times), min(t[1] for t in times)
+    return {"workload": f"{n_side}^3 lattice+ZA, L={box}, mesh {n_side}^3, theta {a['theta']}, "
+                        f"eps {a['eps_spacing']} spacing, {a['steps']} KDK steps dt={a['dt']}, "
+                        f"loss MSE(CIC density)",
+            "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+            "checkpoints": a["steps"] + 1, "precision": "mixed (FP32 pair/mesh, FP64 positions)"}
+
+
+def vjp_vs_force(torch, solver, t) -> dict:
+    """One force VJP against one force evaluation at the same positions."""
+    solver.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+    cot = [torch.randn_like(t["x"]) for _ in range(3)]
+    solver.force_vjp(t["x"], t["y"], t["z"], t["m"], *cot)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    solver.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+    e[1].record()
+    solver.force_vjp(t["x"], t["y"], t["z"], t["m"], *cot)
+    e[2].record()
+    torch.cuda.synchronize()
+    f, b = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    st = solver.last_vjp_stats
+    return {"force_ms": f, "vjp_ms": b, "vjp_over_force": b / f,
+            "vjp_phases_ms": {k: st[k] for k in ("pm_ms", "tree_build_ms", "walk_ms", "total_ms")}}
 
 
 def timed_steps(torch, solver, t, acc, factors, steps, warmup):
@@ -248,11 +321,25 @@ def run_gpu(args) -> int:
     # roofline of the dominant kernel (residual walk, FP32 pipes)
     peak = ct.probe_fp32_peak_tflops(local)
     st = stats[-1]
-    # algorithmic work: the reference's pairs inside r_cut for the timed state
+    # algorithmic work: the reference's traversal counters for the timed state
     # (the first step's counts; positions move by far less than a leaf per step)
-    walk_flops = FLOPS_PER_PAIR * stats0["direct_pair_evaluations"]
+    walk_flops = (FLOPS_PER_PAIR * stats0["direct_pair_evaluations"] +
+                  FLOPS_PER_MULTIPOLE * stats0["accepted_internal_multipoles"] +
+                  FLOPS_PER_VISIT * stats0["visited_nodes"])
     achieved = walk_flops / (st["walk_ms"] * 1e-3) / 1e12
+    checks = mixed.momentum_energy(t["m"], t["vx"], t["vy"], t["vz"], acc["ax"], acc["ay"], acc["az"])
+    try:
+        adj_step = vjp_vs_force(torch, mixed, t)
+    except Exception as exc:  # reported, not fatal to the headline
+        adj_step = {"error": repr(exc)}
     mixed.close()
+    del t, acc
+    torch.cuda.empty_cache()
+    try:
+        adj = adjoint_bench(torch, ct, dev, local)
+        adj["one_step_at_workload"] = adj_step
+    except Exception as exc:
+        adj = {"error": repr(exc), "one_step_at_workload": adj_step}
 
     if rank == 0:
         result = {
@@ -281,11 +368,16 @@ def run_gpu(args) -> int:
             "phases_ms": {k: st[k] for k in ("pm_ms", "tree_build_ms", "walk_ms", "total_ms")},
             "counters": {k: stats0[k] for k in ("direct_pair_evaluations", "visited_nodes",
                                                 "accepted_internal_multipoles", "node_count", "maximum_depth")},
-            "adjoint": None,
-            "roofline": {"bound": "fp32", "kernel": "walkKernel<mixed>", "achieved": achieved,
+            "adjoint": adj,
+            "fp64_checks_end": {"momentum": [float(v) for v in checks["momentum"]],
+                                "net_force": [float(v) for v in checks["net_force"]],
+                                "kinetic_energy": checks["kinetic_energy"], "mass": checks["mass"]},
+            "roofline": {"bound": "fp32", "kernel": "walkFastKernel (production walk)", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "measured FP32 FFMA probe (chui_treepm_probe_fp32_peak)",
-                         "flops_per_pair": FLOPS_PER_PAIR, "traffic": None},
+                         "flops_convention": {"pair": FLOPS_PER_PAIR, "multipole": FLOPS_PER_MULTIPOLE,
+                                              "visit": FLOPS_PER_VISIT},
+                         "traffic": None},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 32,
                     "d2h_bytes_per_step": n * 24, "steps": e2e_steps},
             "gpu_launches": launches,

@@ -327,6 +327,74 @@ class TreePmCoordinator:
                                                 C.c_void_p(stream) if stream else None))
 
 
+def _adjoint_methods():
+    """Reverse-mode entry points, attached to TreePmCoordinator below."""
+
+    def force_vjp(self, x, y, z, mass, cot_x, cot_y, cot_z, uniform_mass: float = 0.0):
+        """J_a(x)^T cot for the full-set TreePM acceleration (chui_treepm_force_vjp)."""
+        arr = _Arrays(x)
+        src = _abi.Sources()
+        src.count = len(x)
+        src.x, src.y, src.z = arr.ptr(x, np.float64), arr.ptr(y, np.float64), arr.ptr(z, np.float64)
+        src.mass = arr.ptr(mass, np.float64) if mass is not None else None
+        src.uniform_mass = uniform_mass
+        cps = [arr.ptr(c, np.float64) for c in (cot_x, cot_y, cot_z)]
+        outs = [arr.out(len(x), x) for _ in range(3)]
+        st = _abi.Stats()
+        self._check(self._lib.chui_treepm_force_vjp(self._h, C.byref(src), *[C.c_void_p(p) for p in cps],
+                                                    *[C.c_void_p(o[1]) for o in outs],
+                                                    _abi.DEVICE if arr.device else _abi.HOST, None, C.byref(st)))
+        self.last_vjp_stats = st.as_dict()
+        return tuple(o[0] for o in outs)
+
+    def density_vjp(self, x, y, z, mass, rho_bar, uniform_mass: float = 0.0):
+        """Transpose of assign_density for a flat cotangent grid (chui_pm_density_vjp)."""
+        arr = _Arrays(x)
+        src = _abi.Sources()
+        src.count = len(x)
+        src.x, src.y, src.z = arr.ptr(x, np.float64), arr.ptr(y, np.float64), arr.ptr(z, np.float64)
+        src.mass = arr.ptr(mass, np.float64) if mass is not None else None
+        src.uniform_mass = uniform_mass
+        rb = arr.ptr(rho_bar, np.float64)
+        outs = [arr.out(len(x), x) for _ in range(3)]
+        self._check(self._lib.chui_pm_density_vjp(self._h, C.byref(src), C.c_void_p(rb),
+                                                  *[C.c_void_p(o[1]) for o in outs],
+                                                  _abi.DEVICE if arr.device else _abi.HOST, None))
+        return tuple(o[0] for o in outs)
+
+    def kdk_adjoint(self, gx, gy, gz, xb, yb, zb, vxb, vyb, vzb, axb, ayb, azb, drift, kick1, kick2, drag1, drag2,
+                    first_step: bool, stream=None):
+        """In-place transpose of one KDK step on CUDA float64 tensors (chui_treepm_kdk_adjoint)."""
+        import torch
+        ts = (gx, gy, gz, xb, yb, zb, vxb, vyb, vzb, axb, ayb, azb)
+        for t in ts:
+            if not (_is_torch(t) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise InvalidArgument(_abi.EINVAL, "kdk_adjoint works in place on contiguous CUDA float64 tensors")
+        self._check(self._lib.chui_treepm_kdk_adjoint(self._h, len(gx), *[C.c_void_p(t.data_ptr()) for t in ts],
+                                                      drift, kick1, kick2, drag1, drag2, 1 if first_step else 0,
+                                                      C.c_void_p(stream) if stream else None))
+
+    def momentum_energy(self, mass, vx, vy, vz, ax=None, ay=None, az=None, uniform_mass: float = 0.0) -> dict:
+        """FP64 global checks on the device: momentum, net force, kinetic energy, total mass."""
+        arr = _Arrays(vx)
+        mp = arr.ptr(mass, np.float64) if mass is not None else None
+        vs = [arr.ptr(v, np.float64) for v in (vx, vy, vz)]
+        acc = [arr.ptr(a, np.float64) if a is not None else None for a in (ax, ay, az)]
+        out = np.zeros(8)
+        self._check(self._lib.chui_treepm_momentum_energy(
+            self._h, len(vx), C.c_void_p(mp) if mp else None, uniform_mass, *[C.c_void_p(p) for p in vs],
+            *[C.c_void_p(p) if p else None for p in acc], _abi.DEVICE if arr.device else _abi.HOST, None,
+            out.ctypes.data))
+        return {"momentum": out[0:3].copy(), "net_force": out[3:6].copy(), "kinetic_energy": float(out[6]),
+                "mass": float(out[7])}
+
+    return force_vjp, density_vjp, kdk_adjoint, momentum_energy
+
+
+(TreePmCoordinator.force_vjp, TreePmCoordinator.density_vjp, TreePmCoordinator.kdk_adjoint,
+ TreePmCoordinator.momentum_energy) = _adjoint_methods()
+
+
 def probe_fp32_peak_tflops(device: int = 0) -> float:
     """Measured FP32 FMA throughput of the GPU (the walk's roofline denominator)."""
     v = C.c_double()

@@ -149,6 +149,84 @@ __global__ void kickKernel(int64_t n, double* vx, double* vy, double* vz, const 
   }
 }
 
+// FP64 global checks: out = {sum m v (3), sum m a (3), sum m v^2 / 2, sum m}.
+// Block partial sums in FP64, one atomicAdd per block and quantity.
+__global__ void momentumEnergyKernel(int64_t n, const double* __restrict__ m, double uniform_mass,
+                                     const double* __restrict__ vx, const double* __restrict__ vy,
+                                     const double* __restrict__ vz, const double* __restrict__ ax,
+                                     const double* __restrict__ ay, const double* __restrict__ az, double* out) {
+  double q[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double mi = m ? m[i] : uniform_mass;
+    const double u[3] = {vx[i], vy[i], vz[i]};
+    q[0] += mi * u[0];
+    q[1] += mi * u[1];
+    q[2] += mi * u[2];
+    if (ax) {
+      q[3] += mi * ax[i];
+      q[4] += mi * ay[i];
+      q[5] += mi * az[i];
+    }
+    q[6] += 0.5 * mi * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    q[7] += mi;
+  }
+  __shared__ double part[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < 8; ++k) {
+    for (int off = 16; off > 0; off >>= 1) q[k] += __shfl_xor_sync(0xffffffffu, q[k], off);
+    if (lane == 0) part[k][warp] = q[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int warps = blockDim.x >> 5;
+    for (int k = 0; k < 8; ++k) {
+      double v = lane < warps ? part[k][lane] : 0.0;
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if (lane == 0) atomicAdd(out + k, v);
+    }
+  }
+}
+
+// g += t (the short-range part of the force VJP onto the PM part).
+__global__ void addKernel(int64_t n, double* gx, double* gy, double* gz, const double* __restrict__ t) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    gx[i] += t[i];
+    gy[i] += t[n + i];
+    gz[i] += t[2 * n + i];
+  }
+}
+
+// Transpose of one KDK step (kick K1 with drag1, drift D, kick K2 with drag2)
+// applied after the force VJP g at the step's end positions:
+//   x_bar += g;  vh_bar = drag2 v_bar + D x_bar;  v_bar = drag1 vh_bar;
+//   a_bar = K1 vh_bar (+ K2 v_bar from the previous step's closing kick,
+//   which acts at the same positions, unless this is the first step).
+__global__ void kdkAdjointKernel(int64_t n, const double* __restrict__ gx, const double* __restrict__ gy,
+                                 const double* __restrict__ gz, double* xb, double* yb, double* zb, double* vxb,
+                                 double* vyb, double* vzb, double* axb, double* ayb, double* azb, double D,
+                                 double K1, double K2, double drag1, double drag2, int first_step) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double px = xb[i] + gx[i], py = yb[i] + gy[i], pz = zb[i] + gz[i];
+    const double hx = fma(D, px, drag2 * vxb[i]);
+    const double hy = fma(D, py, drag2 * vyb[i]);
+    const double hz = fma(D, pz, drag2 * vzb[i]);
+    const double vx = drag1 * hx, vy = drag1 * hy, vz = drag1 * hz;
+    xb[i] = px;
+    yb[i] = py;
+    zb[i] = pz;
+    vxb[i] = vx;
+    vyb[i] = vy;
+    vzb[i] = vz;
+    const double k2 = first_step ? 0.0 : K2;
+    axb[i] = fma(K1, hx, k2 * vx);
+    ayb[i] = fma(K1, hy, k2 * vy);
+    azb[i] = fma(K1, hz, k2 * vz);
+  }
+}
+
 // Drift + core::canonicalPeriodicPosition (include/cosmosim/core/periodic_domain.hpp:8-16;
 // src/workflows/reference_runtime_composition.cpp:76-107).
 __device__ __forceinline__ double canonicalPosition(double v, double box) {
@@ -182,7 +260,28 @@ double hostH(double t) {
   return (std::erf(q) - 0.5 * c * q * std::exp(-t)) / (t * q);
 }
 
-PolyH fitPoly(double t_cut) {
+// H'(t) (the adjoint's kernel derivative): Taylor series below t = 1, closed
+// form above (see residualDerivOverR).
+double hostHp(double t) {
+  if (t < 1.0) {
+    double sum = 0.0, term = 1.0;
+    for (int k = 0; k <= 20; ++k) {
+      const double v = term / (2.0 * k + 5.0);
+      sum += (k & 1) ? v : -v;
+      term *= t / (k + 1.0);
+    }
+    return 2.25675833419102514779231780624309034 * sum;
+  }
+  const double q = std::sqrt(t);
+  const double e = std::exp(-t);
+  const double L = std::erf(q) - 1.12837916709551257389615890312154517 * q * e;
+  return 1.12837916709551257389615890312154517 * e / t - 1.5 * L / (t * t * q);
+}
+
+// Chebyshev interpolation of f on [0, t_cut] rewritten as a polynomial in
+// s = t * 2 / t_cut - 1 (FP32 coefficients).
+template <class F>
+PolyH fitChebyshev(F func, double t_cut) {
   PolyH best;
   best.max_rel_error = 1e300;
   // The walk kernel evaluates either 12 terms or kPolyMaxTerms terms (unused
@@ -193,7 +292,7 @@ PolyH fitPoly(double t_cut) {
     const double pi = 3.141592653589793238462643383279502884;
     for (int k = 0; k < m; ++k) {
       const double xk = std::cos(pi * (k + 0.5) / m);
-      f[k] = hostH((xk + 1.0) * 0.5 * t_cut);
+      f[k] = func((xk + 1.0) * 0.5 * t_cut);
     }
     for (int j = 0; j < m; ++j) {
       double sum = 0.0;
@@ -227,8 +326,8 @@ PolyH fitPoly(double t_cut) {
       const float s = std::fmaf(static_cast<float>(t), p.scale, -1.0f);
       float h = p.c[m - 1];
       for (int i = m - 2; i >= 0; --i) h = std::fmaf(h, s, p.c[i]);
-      const double ref = hostH(t);
-      err = std::max(err, std::fabs(static_cast<double>(h) - ref) / ref);
+      const double ref = func(t);
+      err = std::max(err, std::fabs(static_cast<double>(h) - ref) / std::fabs(ref));
     }
     p.max_rel_error = err;
     if (err < best.max_rel_error) best = p;
@@ -236,6 +335,8 @@ PolyH fitPoly(double t_cut) {
   }
   return best;
 }
+
+PolyH fitPoly(double t_cut) { return fitChebyshev(hostH, t_cut); }
 
 int fail(Context& c, int code, const std::string& msg) {
   c.last_error = msg;
@@ -304,6 +405,7 @@ void applyConfig(Context& c, const chui_treepm_config& cfg) {
   c.cutoff = cfg.rcut_cells * c.spacing;
   const double t_cut = (c.cutoff * c.cutoff) / (4.0 * c.rs * c.rs) * (1.0 + 1.0e-5);
   c.poly = fitPoly(t_cut);
+  c.dpoly = fitChebyshev(hostHp, t_cut);
 }
 
 struct DeviceGuard {
@@ -452,7 +554,7 @@ void chui_treepm_destroy(void* handle) {
                             &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
                             &c->leaf_of_pos, &c->inv_pos, &c->cub_temp, &c->node_geom, &c->node_com,
                             &c->node_quad, &c->node_f4, &c->node_hmin, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
-                            &c->node_counter, &c->sorted_index, &c->pos_of_row, &c->src_f4, &c->src_d4, &c->src_u4,
+                            &c->node_counter, &c->sorted_index, &c->pos_of_row, &c->src_f4, &c->src_d4, &c->src_u4, &c->src_cot,
                             &c->target_order, &c->morton_sorted, &c->walk_counters, &c->work_counter,
                             &c->tree_acc, &c->tree_near};
     for (auto* b : bufs) chui::release(*b);
@@ -736,6 +838,205 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   c.last_stats = stt;
   if (stats) *stats = stt;
   return 0;
+}
+
+int chui_treepm_force_vjp(void* handle, const chui_treepm_sources* src, const double* cot_x, const double* cot_y,
+                          const double* cot_z, double* grad_x, double* grad_y, double* grad_z, int memory,
+                          void* stream, chui_treepm_stats* stats) {
+  if (!handle) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  c.last_error.clear();
+  if (!src) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources are required");
+  if (memory != CHUI_TREEPM_HOST && memory != CHUI_TREEPM_DEVICE)
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "memory must be CHUI_TREEPM_HOST or CHUI_TREEPM_DEVICE");
+  const int64_t n = src->count;
+  if (n < 0) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM requires non-negative extents");
+  if (n > static_cast<int64_t>(0xFFFFFFFEu))
+    return chui::fail(c, CHUI_TREEPM_ERANGE, "Tree gravity source count exceeds the 32-bit tree-index contract");
+  if (n > 0 && (!src->x || !src->y || !src->z || !cot_x || !cot_y || !cot_z || !grad_x || !grad_y || !grad_z))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "force VJP requires positions, cotangents and gradients of equal extent");
+  if (!src->mass && !(std::isfinite(src->uniform_mass) && src->uniform_mass >= 0.0))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources require finite coordinates and finite non-negative masses");
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint64_t launches_before = chui::launchCount();
+  cudaEventRecord(c.ev[0], s);
+  int rc;
+  const double *x, *y, *z, *m, *cx, *cy, *cz;
+  if ((rc = chui::stageIn(c, c.in_x, src->x, n, memory, s, &x)) || (rc = chui::stageIn(c, c.in_y, src->y, n, memory, s, &y)) ||
+      (rc = chui::stageIn(c, c.in_z, src->z, n, memory, s, &z)) ||
+      (rc = chui::stageIn(c, c.in_m, src->mass, src->mass ? n : 0, memory, s, &m)) ||
+      (rc = chui::stageIn(c, c.in_tx, cot_x, n, memory, s, &cx)) ||
+      (rc = chui::stageIn(c, c.in_ty, cot_y, n, memory, s, &cy)) ||
+      (rc = chui::stageIn(c, c.in_tz, cot_z, n, memory, s, &cz)))
+    return rc;
+  if (!src->mass) m = nullptr;
+  double lo[3], hi[3], mass_sum = 0.0;
+  uint32_t st = 0;
+  if ((rc = chui::sourceBounds(c, n, x, y, z, m, lo, hi, &mass_sum, &st, s))) return rc;
+  if (st) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources require finite coordinates and finite non-negative masses");
+  const double total_mass = m ? mass_sum : static_cast<double>(n) * src->uniform_mass;
+  double *gx = grad_x, *gy = grad_y, *gz = grad_z;
+  if (memory == CHUI_TREEPM_HOST) {
+    for (int a = 0; a < 3; ++a)
+      if (chui::ensure(c.out_acc[a], std::max<int64_t>(n, 1) * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    gx = c.out_acc[0].as<double>();
+    gy = c.out_acc[1].as<double>();
+    gz = c.out_acc[2].as<double>();
+  }
+  // PM part (refreshes the PM field at these positions)
+  if ((rc = chui::pmForceVjp(c, n, x, y, z, m, src->uniform_mass, total_mass, cx, cy, cz, gx, gy, gz, s)))
+    return chui::fail(c, rc, c.last_error.empty() ? "PM adjoint failed" : c.last_error);
+  cudaEventRecord(c.ev[1], s);
+  // tree for these positions, every particle a target in tree order
+  if (n > 0) {
+    if ((rc = chui::treeBuild(c, n, x, y, z, m, src->uniform_mass, lo, hi, s))) {
+      if (c.last_error.empty()) c.last_error = "TreePM tree build failed";
+      return rc;
+    }
+    if ((rc = chui::treeOrderTargets(c, n, nullptr, 0, n, s))) return chui::fail(c, rc, "target ordering failed");
+  }
+  cudaEventRecord(c.ev[2], s);
+  chui::WalkParams wp{};
+  wp.box[0] = c.cfg.box_x;
+  wp.box[1] = c.cfg.box_y;
+  wp.box[2] = c.cfg.box_z;
+  wp.rs = c.rs;
+  wp.cutoff = c.cutoff;
+  wp.cutoff2 = c.cutoff * c.cutoff;
+  wp.G = c.cfg.gravitational_constant;
+  wp.eps = c.cfg.softening;
+  wp.inv_4rs2_f = static_cast<float>(0.25 / (c.rs * c.rs));
+  wp.inv_8rs3_f = static_cast<float>(0.125 / (c.rs * c.rs * c.rs));
+  wp.cut2_f = static_cast<float>(c.cutoff * c.cutoff);
+  wp.eps2_f = static_cast<float>(c.cfg.softening * c.cfg.softening);
+  wp.G_f = static_cast<float>(c.cfg.gravitational_constant);
+  cudaMemsetAsync(c.status.ptr, 0, 4, s);
+  if (n > 0) {
+    if (chui::ensure(c.tree_acc, static_cast<size_t>(n) * 3 * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    double* t = c.tree_acc.as<double>();
+    if ((rc = chui::walkVjpRun(c, n, x, y, z, m, src->uniform_mass, cx, cy, cz, wp, t, t + n, t + 2 * n, s)))
+      return chui::fail(c, rc, "adjoint walk launch failed");
+    cudaEventRecord(c.ev[3], s);
+    { chui::noteLaunch(); chui::addKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, gx, gy, gz, t); }
+  } else {
+    cudaEventRecord(c.ev[3], s);
+  }
+  cudaEventRecord(c.ev[4], s);
+  uint32_t walk_status = 0;
+  cudaMemcpyAsync(&walk_status, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
+  if (memory == CHUI_TREEPM_HOST && n > 0) {
+    cudaMemcpyAsync(grad_x, gx, n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(grad_y, gy, n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(grad_z, gz, n * 8, cudaMemcpyDeviceToHost, s);
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return chui::fail(c, CHUI_TREEPM_EDEVICE, std::string("CUDA error: ") + cudaGetErrorString(e));
+  if (walk_status) return chui::fail(c, CHUI_TREEPM_ERANGE, chui::statusText(walk_status));
+  if (stats) {
+    chui_treepm_stats stt{};
+    stt.node_count = static_cast<uint64_t>(c.n_nodes);
+    stt.maximum_depth = c.max_depth;
+    stt.path_words = static_cast<uint32_t>(c.path_words_used);
+    stt.kernel_launches = chui::launchCount() - launches_before;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
+    stt.pm_ms = ms;
+    cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+    stt.tree_build_ms = ms;
+    cudaEventElapsedTime(&ms, c.ev[2], c.ev[3]);
+    stt.walk_ms = ms;
+    cudaEventElapsedTime(&ms, c.ev[0], c.ev[4]);
+    stt.total_ms = ms;
+    *stats = stt;
+  }
+  return 0;
+}
+
+int chui_pm_density_vjp(void* handle, const chui_treepm_sources* src, const double* rho_bar, double* grad_x,
+                        double* grad_y, double* grad_z, int memory, void* stream) {
+  if (!handle) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  if (!src || !rho_bar || (src->count > 0 && (!src->x || !src->y || !src->z || !grad_x || !grad_y || !grad_z)))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "density VJP requires positions, a cotangent grid and gradients");
+  if (memory != CHUI_TREEPM_HOST && memory != CHUI_TREEPM_DEVICE)
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "memory must be CHUI_TREEPM_HOST or CHUI_TREEPM_DEVICE");
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t n = src->count;
+  const size_t cells = static_cast<size_t>(c.cfg.pm_grid_nx) * c.cfg.pm_grid_ny * c.cfg.pm_grid_nz;
+  const double *x, *y, *z, *m, *rb;
+  int rc;
+  if ((rc = chui::stageIn(c, c.in_x, src->x, n, memory, s, &x)) || (rc = chui::stageIn(c, c.in_y, src->y, n, memory, s, &y)) ||
+      (rc = chui::stageIn(c, c.in_z, src->z, n, memory, s, &z)) ||
+      (rc = chui::stageIn(c, c.in_m, src->mass, src->mass ? n : 0, memory, s, &m)) ||
+      (rc = chui::stageIn(c, c.in_tx, rho_bar, static_cast<int64_t>(cells), memory, s, &rb)))
+    return rc;
+  if (!src->mass) m = nullptr;
+  double *gx = grad_x, *gy = grad_y, *gz = grad_z;
+  if (memory == CHUI_TREEPM_HOST) {
+    for (int a = 0; a < 3; ++a)
+      if (chui::ensure(c.out_acc[a], std::max<int64_t>(n, 1) * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+    gx = c.out_acc[0].as<double>();
+    gy = c.out_acc[1].as<double>();
+    gz = c.out_acc[2].as<double>();
+  }
+  if ((rc = chui::pmDensityVjp(c, n, x, y, z, m, src->uniform_mass, rb, gx, gy, gz, s))) return rc;
+  if (memory == CHUI_TREEPM_HOST && n > 0) {
+    cudaMemcpyAsync(grad_x, gx, n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(grad_y, gy, n * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(grad_z, gz, n * 8, cudaMemcpyDeviceToHost, s);
+  }
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "density VJP failed");
+}
+
+int chui_treepm_kdk_adjoint(void* handle, int64_t n, const double* gx, const double* gy, const double* gz,
+                            double* x_bar_x, double* x_bar_y, double* x_bar_z, double* v_bar_x, double* v_bar_y,
+                            double* v_bar_z, double* a_bar_x, double* a_bar_y, double* a_bar_z, double drift_factor,
+                            double kick1, double kick2, double drag1, double drag2, int first_step, void* stream) {
+  if (!handle) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  if (n < 0 || (n > 0 && (!gx || !gy || !gz || !x_bar_x || !x_bar_y || !x_bar_z || !v_bar_x || !v_bar_y ||
+                          !v_bar_z || !a_bar_x || !a_bar_y || !a_bar_z)))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "KDK adjoint requires device arrays of equal extent");
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n > 0)
+    { chui::noteLaunch(); chui::kdkAdjointKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(
+        n, gx, gy, gz, x_bar_x, x_bar_y, x_bar_z, v_bar_x, v_bar_y, v_bar_z, a_bar_x, a_bar_y, a_bar_z,
+        drift_factor, kick1, kick2, drag1, drag2, first_step); }
+  return cudaGetLastError() == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "KDK adjoint launch failed");
+}
+
+int chui_treepm_momentum_energy(void* handle, int64_t n, const double* mass, double uniform_mass, const double* vx,
+                                const double* vy, const double* vz, const double* ax, const double* ay,
+                                const double* az, int memory, void* stream, double out[8]) {
+  if (!handle || !out) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  if (n < 0 || (n > 0 && (!vx || !vy || !vz)) || ((ax || ay || az) && !(ax && ay && az)))
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "momentum/energy check requires velocity arrays (and all or no accelerations)");
+  if (memory != CHUI_TREEPM_HOST && memory != CHUI_TREEPM_DEVICE)
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "memory must be CHUI_TREEPM_HOST or CHUI_TREEPM_DEVICE");
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const double *m, *u[3], *a[3] = {nullptr, nullptr, nullptr};
+  int rc;
+  if ((rc = chui::stageIn(c, c.in_m, mass, mass ? n : 0, memory, s, &m)) ||
+      (rc = chui::stageIn(c, c.in_x, vx, n, memory, s, &u[0])) || (rc = chui::stageIn(c, c.in_y, vy, n, memory, s, &u[1])) ||
+      (rc = chui::stageIn(c, c.in_z, vz, n, memory, s, &u[2])))
+    return rc;
+  if (ax && ((rc = chui::stageIn(c, c.in_tx, ax, n, memory, s, &a[0])) ||
+             (rc = chui::stageIn(c, c.in_ty, ay, n, memory, s, &a[1])) ||
+             (rc = chui::stageIn(c, c.in_tz, az, n, memory, s, &a[2]))))
+    return rc;
+  if (!mass) m = nullptr;
+  double* d = c.scalars.as<double>();
+  cudaMemsetAsync(d, 0, 8 * sizeof(double), s);
+  if (n > 0)
+    { chui::noteLaunch(); chui::momentumEnergyKernel<<<std::min<unsigned>(chui::gridFor(n, 256), 148u * 4u), 256, 0, s>>>(
+        n, m, uniform_mass, u[0], u[1], u[2], a[0], a[1], a[2], d); }
+  cudaMemcpyAsync(out, d, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "momentum/energy check failed");
 }
 
 int chui_pm_assign_density(void* handle, const chui_treepm_sources* src, double* density, int memory, void* stream) {

@@ -136,4 +136,32 @@ __device__ inline double residualInvR3(double r2, double eps, double rs) {
   return softenedInvR3(r2, eps) - longRangeInvR3(sqrt(r2), rs);
 }
 
+// (dK/dr) / r of K = K_soft - K_long at r^2 = r2 > 0, FP64. K_long = H(t) / (8 r_s^3)
+// with H(t) = L(q) / q^3, t = q^2 = r^2 / (4 r_s^2), L(q) = erf(q) - 2 q e^{-q^2} / sqrt(pi),
+// so dK_long/dr / r = H'(t) / (16 r_s^5). H'(t) from its Taylor series
+// (4/sqrt(pi)) sum_m (-1)^{m+1} t^m / (m! (2m+5)) for t < 1, else from
+// H'(t) = (2/sqrt(pi)) e^{-t} / t - 1.5 L(sqrt t) / t^{5/2}.
+__device__ inline double residualDerivOverR(double r2, double eps, double rs) {
+  const double s2 = r2 + eps * eps;
+  const double soft = -3.0 / (s2 * s2 * sqrt(s2));
+  const double t = r2 / (4.0 * rs * rs);
+  double hp;
+  if (t < 1.0) {
+    double sum = 0.0, term = 1.0;  // term = t^m / m!
+    for (int k = 0; k <= 20; ++k) {
+      const double v = term / (2.0 * k + 5.0);
+      sum += (k & 1) ? v : -v;
+      term *= t / (k + 1.0);
+    }
+    hp = 2.25675833419102514779231780624309034 * sum;
+  } else {
+    const double q = sqrt(t);
+    const double e = exp(-t);
+    const double L = erf(q) - 1.12837916709551257389615890312154517 * q * e;
+    hp = 1.12837916709551257389615890312154517 * e / t - 1.5 * L / (t * t * q);
+  }
+  const double rs2 = rs * rs;
+  return soft - hp / (16.0 * rs2 * rs2 * rs);
+}
+
 }  // namespace chui

@@ -57,12 +57,14 @@ struct Context {
   int device = 0;
   double spacing = 0.0, rs = 0.0, cutoff = 0.0;
   PolyH poly;
+  PolyH dpoly;  // H'(t) for the adjoint walk
   std::string last_error;
 
   // PM (cuFFT, in-place padded real layout nx*ny*2*(nz/2+1))
   bool fft_ready = false;
   cufftHandle plan_r2c = 0, plan_c2r = 0;
   DevBuf grid[3];            // grid[0] holds the density then F_x; grid[1], grid[2] F_y, F_z
+  DevBuf adj_grid[3];        // adjoint: cotangent grids B_x, B_y, B_z; adj_grid[0] then holds rho_bar
   DevBuf axis_tables;        // kx, ky, kz, wx, wy, wz (FP64)
   bool pm_field_valid = false;
   double pm_field_box[3] = {0, 0, 0};
@@ -104,6 +106,7 @@ struct Context {
   DevBuf src_f4;       // float4 per tree position: offset from leaf centre (FP32) + mass
   DevBuf src_d4;       // double4 per tree position: caller position + mass (FP64 path)
   DevBuf src_u4;       // double4 per tree position: unwrapped (tree frame) position + mass (mixed path)
+  DevBuf src_cot;      // double4 per tree position: force cotangent (adjoint walk)
   DevBuf target_order; // visit order of active slots
   DevBuf morton_sorted;  // sorted Morton keys (diagnostic parity output)
 
@@ -130,6 +133,14 @@ int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const
                   const double* m, double uniform_mass, double* rho_out, cudaStream_t s);
 int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,
             int64_t* cells, cudaStream_t s);
+// Adjoint of the PM force at positions (x, y, z) for cotangents c: g = J_pm^T c
+// (refreshes the PM field at these positions first).
+int pmForceVjp(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
+               double uniform_mass, double total_mass, const double* cx, const double* cy, const double* cz,
+               double* gx, double* gy, double* gz, cudaStream_t s);
+// Adjoint of the compact FP64 density for a cotangent grid rho_bar.
+int pmDensityVjp(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
+                 double uniform_mass, const double* rho_bar, double* gx, double* gy, double* gz, cudaStream_t s);
 // Density into a caller-provided compact grid of nx*ny*nz doubles; no allocation.
 int pmDensityInto(const chui_treepm_config& cfg, int64_t n, const double* x, const double* y, const double* z,
                   const double* m, double uniform_mass, double* rho, cudaStream_t s);
@@ -147,6 +158,13 @@ int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explici
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
             const WalkParams& wp, int64_t n, cudaStream_t s);
+
+// Adjoint of the short-range force for all n particles (targets in tree
+// order, after treeBuild and treeOrderTargets with the full set):
+// g = G sum_j M(d) (m_k c_j - m_j c_k) per row.
+int walkVjpRun(Context& c, int64_t n, const double* sx, const double* sy, const double* sz, const double* m,
+               double uniform_mass, const double* cx, const double* cy, const double* cz, const WalkParams& wp,
+               double* gx, double* gy, double* gz, cudaStream_t s);
 
 // ---- reductions / small kernels (abi.cu) ----
 int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const double* z,

@@ -287,6 +287,172 @@ inline double sincHost(double v) {
 
 bool isMixed(const Context& c) { return c.cfg.precision == CHUI_TREEPM_MIXED; }
 
+// ---- adjoint (transposes of the PM force map) ----
+
+// Derivatives of the stencil weights with respect to the grid coordinate gp
+// (same base cell as makeStencil).
+__device__ __forceinline__ Stencil makeStencilGrad(double gp, int scheme) {
+  Stencil s;
+  if (scheme == 0) {
+    s.off0 = static_cast<int64_t>(floor(gp));
+    s.w[0] = -1.0;
+    s.w[1] = 1.0;
+    s.w[2] = 0.0;
+  } else {
+    const double center = floor(gp + 0.5);
+    const double d = gp - center;
+    s.off0 = static_cast<int64_t>(center) - 1;
+    s.w[0] = -(0.5 - d);
+    s.w[1] = -2.0 * d;
+    s.w[2] = 0.5 + d;
+  }
+  return s;
+}
+
+// Transpose of the interpolation a_k = sum_c W(x_k - c) F(c) for cotangents
+// a_bar: position gradient sum_b a_bar_b sum_c grad W F_b(c) (written to g),
+// and the cotangent grids B_b(c) += W(x_k - c) a_bar_b (atomics).
+template <class R>
+__global__ void pmInterpAdjointKernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                      const double* __restrict__ z, const double* __restrict__ cx,
+                                      const double* __restrict__ cy, const double* __restrict__ cz, PmGeom g,
+                                      const R* __restrict__ f0, const R* __restrict__ f1, const R* __restrict__ f2,
+                                      R* b0, R* b1, R* b2, double* gx, double* gy, double* gz) {
+  const int taps = g.scheme == 0 ? 2 : 3;
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double gp0 = wrapPosition(x[k], g.L[0]) * g.inv_d[0];
+    const double gp1 = wrapPosition(y[k], g.L[1]) * g.inv_d[1];
+    const double gp2 = wrapPosition(z[k], g.L[2]) * g.inv_d[2];
+    const Stencil s0 = makeStencil(gp0, g.scheme), s1 = makeStencil(gp1, g.scheme), s2 = makeStencil(gp2, g.scheme);
+    const Stencil d0 = makeStencilGrad(gp0, g.scheme), d1 = makeStencilGrad(gp1, g.scheme),
+                  d2 = makeStencilGrad(gp2, g.scheme);
+    const double ax = cx[k], ay = cy[k], az = cz[k];
+    double ox = 0.0, oy = 0.0, oz = 0.0;
+    for (int a = 0; a < taps; ++a) {
+      const int64_t ix = wrapIndex(s0.off0 + a, g.n[0]);
+      for (int b = 0; b < taps; ++b) {
+        const int64_t iy = wrapIndex(s1.off0 + b, g.n[1]);
+        const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
+        for (int cc = 0; cc < taps; ++cc) {
+          const int64_t iz = wrapIndex(s2.off0 + cc, g.n[2]);
+          const size_t at = row + iz;
+          const double dot = ax * static_cast<double>(f0[at]) + ay * static_cast<double>(f1[at]) +
+                             az * static_cast<double>(f2[at]);
+          ox += d0.w[a] * s1.w[b] * s2.w[cc] * dot;
+          oy += s0.w[a] * d1.w[b] * s2.w[cc] * dot;
+          oz += s0.w[a] * s1.w[b] * d2.w[cc] * dot;
+          const double w = s0.w[a] * s1.w[b] * s2.w[cc];
+          atomicAdd(b0 + at, static_cast<R>(w * ax));
+          atomicAdd(b1 + at, static_cast<R>(w * ay));
+          atomicAdd(b2 + at, static_cast<R>(w * az));
+        }
+      }
+    }
+    gx[k] = ox * g.inv_d[0];
+    gy[k] = oy * g.inv_d[1];
+    gz[k] = oz * g.inv_d[2];
+  }
+}
+
+// Transpose of the three gradient operators F_b = C2R(-i g_b op R2C(rho)):
+// each is a real circulant with an odd kernel, so its transpose is its
+// negative and rho_bar = -sum_b C2R(-i g_b op B_b^) = C2R(sum_b i g_b op B_b^).
+// Writes that spectrum into c0 (in place of B_0^).
+template <class R, class C>
+__global__ void pmSpectrumAdjointKernel(PmGeom g, const double* __restrict__ tab, double prefactor, double rs,
+                                        int deconv, C* c0, const C* __restrict__ c1, const C* __restrict__ c2) {
+  const int64_t nx = g.n[0], ny = g.n[1], nzc = g.nzc;
+  const double* kx = tab;
+  const double* ky = kx + nx;
+  const double* kz = ky + ny;
+  const double* wx = kz + nzc;
+  const double* wy = wx + nx;
+  const double* wz = wy + ny;
+  const double* gx = wz + nzc;
+  const double* gy = gx + nx;
+  const double* gz = gy + ny;
+  const size_t total = static_cast<size_t>(nx) * ny * nzc;
+  for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int64_t iz = static_cast<int64_t>(idx % nzc);
+    const size_t row = idx / nzc;
+    const int64_t iy = static_cast<int64_t>(row % ny);
+    const int64_t ix = static_cast<int64_t>(row / ny);
+    const double k2 = kx[ix] * kx[ix] + ky[iy] * ky[iy] + kz[iz] * kz[iz];
+    double op = 0.0;
+    if (k2 != 0.0) {
+      double window = 1.0;
+      if (deconv) {
+        const double tw = wx[ix] * wy[iy] * wz[iz];
+        const double w2 = tw * tw;
+        window = 1.0 / (w2 > 1.0e-12 ? w2 : 1.0e-12);
+      }
+      const double prod = sqrt(k2) * rs;
+      op = prefactor * window * exp(-(prod * prod)) / k2;
+    }
+    const C v0 = c0[idx], v1 = c1[idx], v2 = c2[idx];
+    // sum_b g_b (re_b + i im_b) = (sr + i si); times i op -> (-op si, op sr)
+    const double sr = gx[ix] * static_cast<double>(v0.x) + gy[iy] * static_cast<double>(v1.x) +
+                      gz[iz] * static_cast<double>(v2.x);
+    const double si = gx[ix] * static_cast<double>(v0.y) + gy[iy] * static_cast<double>(v1.y) +
+                      gz[iz] * static_cast<double>(v2.y);
+    C out;
+    out.x = static_cast<R>(-op * si);
+    out.y = static_cast<R>(op * sr);
+    c0[idx] = out;
+  }
+}
+
+// Transpose of the mass deposit rho(c) = sum_j m_j W(x_j - c) / V_cell:
+// g_j += (m_j / V_cell) sum_c rho_bar(c) grad W(x_j - c). The grid's row
+// stride is g.nzp (padded FFT layout or compact nz).
+template <class R>
+__global__ void pmDepositAdjointKernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                       const double* __restrict__ z, const double* __restrict__ m,
+                                       double uniform_mass, double inv_cell_volume, PmGeom g,
+                                       const R* __restrict__ rho_bar, int accumulate, double* gx, double* gy,
+                                       double* gz) {
+  const int taps = g.scheme == 0 ? 2 : 3;
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double gp0 = wrapPosition(x[k], g.L[0]) * g.inv_d[0];
+    const double gp1 = wrapPosition(y[k], g.L[1]) * g.inv_d[1];
+    const double gp2 = wrapPosition(z[k], g.L[2]) * g.inv_d[2];
+    const Stencil s0 = makeStencil(gp0, g.scheme), s1 = makeStencil(gp1, g.scheme), s2 = makeStencil(gp2, g.scheme);
+    const Stencil d0 = makeStencilGrad(gp0, g.scheme), d1 = makeStencilGrad(gp1, g.scheme),
+                  d2 = makeStencilGrad(gp2, g.scheme);
+    double ox = 0.0, oy = 0.0, oz = 0.0;
+    for (int a = 0; a < taps; ++a) {
+      const int64_t ix = wrapIndex(s0.off0 + a, g.n[0]);
+      for (int b = 0; b < taps; ++b) {
+        const int64_t iy = wrapIndex(s1.off0 + b, g.n[1]);
+        const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
+        for (int cc = 0; cc < taps; ++cc) {
+          const int64_t iz = wrapIndex(s2.off0 + cc, g.n[2]);
+          const double v = static_cast<double>(rho_bar[row + iz]);
+          ox += d0.w[a] * s1.w[b] * s2.w[cc] * v;
+          oy += s0.w[a] * d1.w[b] * s2.w[cc] * v;
+          oz += s0.w[a] * s1.w[b] * d2.w[cc] * v;
+        }
+      }
+    }
+    const double f = (m ? m[k] : uniform_mass) * inv_cell_volume;
+    ox *= f * g.inv_d[0];
+    oy *= f * g.inv_d[1];
+    oz *= f * g.inv_d[2];
+    if (accumulate) {
+      gx[k] += ox;
+      gy[k] += oy;
+      gz[k] += oz;
+    } else {
+      gx[k] = ox;
+      gy[k] = oy;
+      gz[k] = oz;
+    }
+  }
+}
+
 }  // namespace
 
 int pmPrepare(Context& c) {
@@ -345,6 +511,7 @@ void pmDestroy(Context& c) {
   c.plan_r2c = c.plan_c2r = 0;
   c.fft_ready = false;
   for (auto& b : c.grid) release(b);
+  for (auto& b : c.adj_grid) release(b);
   release(c.axis_tables);
 }
 
@@ -487,6 +654,94 @@ int pmDensityInto(const chui_treepm_config& cfg, int64_t n, const double* x, con
   const double cell_volume = (g.L[0] * g.L[1] * g.L[2]) / static_cast<double>(cells);
   { noteLaunch(); scaleKernel<<<gridFor(cells, block), block, 0, s>>>(rho, cells, cell_volume); }
   return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
+}
+
+// PM part of the force VJP at positions (x, y, z): refreshes the PM field at
+// these positions, then g = J_pm^T a_bar (written, not accumulated).
+int pmForceVjp(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
+               double uniform_mass, double total_mass, const double* cx, const double* cy, const double* cz,
+               double* gx, double* gy, double* gz, cudaStream_t s) {
+  int rc = pmRefresh(c, n, x, y, z, m, uniform_mass, total_mass, s);
+  if (rc) return rc;
+  if (n == 0) return 0;
+  const PmGeom g = geomOf(c);
+  const bool mixed = isMixed(c);
+  const size_t elem = mixed ? sizeof(float) : sizeof(double);
+  const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
+  const size_t padded = static_cast<size_t>(g.n[0]) * g.n[1] * g.nzp;
+  const size_t total = static_cast<size_t>(g.n[0]) * g.n[1] * g.nzc;
+  const double cell_volume = (g.L[0] * g.L[1] * g.L[2]) / static_cast<double>(cells);
+  const double prefactor = -4.0 * kPi * c.cfg.gravitational_constant / static_cast<double>(cells);
+  for (auto& b : c.adj_grid) {
+    if (ensure(b, padded * elem) != cudaSuccess) {
+      c.last_error = "PM adjoint mesh allocation failed";
+      return CHUI_TREEPM_ENOMEM;
+    }
+    cudaMemsetAsync(b.ptr, 0, padded * elem, s);
+  }
+  const int block = 256;
+  cufftSetStream(c.plan_r2c, s);
+  cufftSetStream(c.plan_c2r, s);
+  cufftResult fr = CUFFT_SUCCESS;
+  if (mixed) {
+    { noteLaunch(); pmInterpAdjointKernel<float><<<gridFor(n, block), block, 0, s>>>(
+        n, x, y, z, cx, cy, cz, g, c.grid[0].as<float>(), c.grid[1].as<float>(), c.grid[2].as<float>(),
+        c.adj_grid[0].as<float>(), c.adj_grid[1].as<float>(), c.adj_grid[2].as<float>(), gx, gy, gz); }
+    for (int a = 0; a < 3 && fr == CUFFT_SUCCESS; ++a)
+      fr = cufftExecR2C(c.plan_r2c, c.adj_grid[a].as<cufftReal>(), c.adj_grid[a].as<cufftComplex>());
+    if (fr == CUFFT_SUCCESS) {
+      { noteLaunch(); pmSpectrumAdjointKernel<float, cufftComplex><<<gridFor(total, block), block, 0, s>>>(
+          g, c.axis_tables.as<double>(), prefactor, c.rs, c.cfg.window_deconvolution,
+          c.adj_grid[0].as<cufftComplex>(), c.adj_grid[1].as<cufftComplex>(), c.adj_grid[2].as<cufftComplex>()); }
+      fr = cufftExecC2R(c.plan_c2r, c.adj_grid[0].as<cufftComplex>(), c.adj_grid[0].as<cufftReal>());
+    }
+    if (fr == CUFFT_SUCCESS)
+      { noteLaunch(); pmDepositAdjointKernel<float><<<gridFor(n, block), block, 0, s>>>(
+          n, x, y, z, m, uniform_mass, 1.0 / cell_volume, g, c.adj_grid[0].as<float>(), 1, gx, gy, gz); }
+  } else {
+    { noteLaunch(); pmInterpAdjointKernel<double><<<gridFor(n, block), block, 0, s>>>(
+        n, x, y, z, cx, cy, cz, g, c.grid[0].as<double>(), c.grid[1].as<double>(), c.grid[2].as<double>(),
+        c.adj_grid[0].as<double>(), c.adj_grid[1].as<double>(), c.adj_grid[2].as<double>(), gx, gy, gz); }
+    for (int a = 0; a < 3 && fr == CUFFT_SUCCESS; ++a)
+      fr = cufftExecD2Z(c.plan_r2c, c.adj_grid[a].as<cufftDoubleReal>(), c.adj_grid[a].as<cufftDoubleComplex>());
+    if (fr == CUFFT_SUCCESS) {
+      { noteLaunch(); pmSpectrumAdjointKernel<double, cufftDoubleComplex><<<gridFor(total, block), block, 0, s>>>(
+          g, c.axis_tables.as<double>(), prefactor, c.rs, c.cfg.window_deconvolution,
+          c.adj_grid[0].as<cufftDoubleComplex>(), c.adj_grid[1].as<cufftDoubleComplex>(),
+          c.adj_grid[2].as<cufftDoubleComplex>()); }
+      fr = cufftExecZ2D(c.plan_c2r, c.adj_grid[0].as<cufftDoubleComplex>(), c.adj_grid[0].as<cufftDoubleReal>());
+    }
+    if (fr == CUFFT_SUCCESS)
+      { noteLaunch(); pmDepositAdjointKernel<double><<<gridFor(n, block), block, 0, s>>>(
+          n, x, y, z, m, uniform_mass, 1.0 / cell_volume, g, c.adj_grid[0].as<double>(), 1, gx, gy, gz); }
+  }
+  if (fr != CUFFT_SUCCESS) {
+    c.last_error = "cuFFT failed in the PM adjoint";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  if (cudaGetLastError() != cudaSuccess) {
+    c.last_error = "PM adjoint launch failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  return 0;
+}
+
+// Transpose of the density (mass / cell volume, compact FP64 grid):
+// g_j = (m_j / V_cell) sum_c rho_bar(c) grad W(x_j - c).
+int pmDensityVjp(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
+                 double uniform_mass, const double* rho_bar, double* gx, double* gy, double* gz, cudaStream_t s) {
+  if (n == 0) return 0;
+  PmGeom g = geomOf(c);
+  g.nzp = g.n[2];  // compact rows
+  const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
+  const double cell_volume = (g.L[0] * g.L[1] * g.L[2]) / static_cast<double>(cells);
+  { noteLaunch(); pmDepositAdjointKernel<double><<<gridFor(n, 256), 256, 0, s>>>(
+      n, x, y, z, m, uniform_mass, 1.0 / cell_volume, g, rho_bar, 0, gx, gy, gz); }
+  if (cudaGetLastError() != cudaSuccess) {
+    c.last_error = "PM density adjoint launch failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  return 0;
 }
 
 int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,

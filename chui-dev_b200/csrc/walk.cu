@@ -35,6 +35,7 @@
 // counters are kept.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 
@@ -821,6 +822,291 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   }
 }
 
+// ---- adjoint: vector-Jacobian product of the short-range force ----------
+
+struct VjpArgs {
+  int64_t n;                    // particles (every particle is a target)
+  const uint32_t* order;        // visit position -> row (tree order)
+  const double* sx;             // caller positions
+  const double* sy;
+  const double* sz;
+  const double* m;              // masses (nullable: uniform_mass)
+  double uniform_mass;
+  const double* cx;             // cotangents a_bar per row
+  const double* cy;
+  const double* cz;
+  const double4* geom;
+  const uint4* range;
+  const uint32_t* child;
+  const double4* src_d4;        // tree order: caller position + mass
+  const double4* src_c4;        // tree order: cotangent
+  double* out_x;                // per row: x_bar of the short-range force (times G)
+  double* out_y;
+  double* out_z;
+  uint32_t* work;
+  uint32_t* status;
+  PolyH poly;
+  PolyH dpoly;
+  WalkParams wp;
+  float inv_16rs5_f;
+};
+
+template <class Real>
+struct VjpQueue;
+template <>
+struct VjpQueue<float> {
+  using V4 = float4;
+};
+template <>
+struct VjpQueue<double> {
+  using V4 = double4;
+};
+
+// x_bar_k = G sum_j M(d) (m_k a_bar_j - m_j a_bar_k), d = x_j - x_k, over every
+// source j within r_cut of target k (j != k, d != 0), M(d) = K I + (K'/r) d d^T
+// the Jacobian of the pair force d -> K(|d|) d. Because M is even in d and the
+// pair set {|d| <= r_cut} is symmetric, this gathers both the target-side and
+// the source-side derivatives without scattering.
+//
+// Traversal: a node is kept while the r_cut sphere of some lane may reach its
+// cube (each lane with its own minimum image, so groups of targets that are
+// far apart in the box still prune); leaves and nodes of at most kBulkCount
+// sources are enqueued whole, keeping sources inside the sphere of the lanes
+// that need the node; every pair decision is the per-pair cutoff test. Queue
+// entries are FP64-formed minimum-image offsets from the warp's reference
+// target; when r_cut plus the group radius reaches half the box, each pair
+// takes its own minimum image.
+template <class Real, bool kEpsZero, int kTerms>
+__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpArgs a) {
+  using V4 = typename VjpQueue<Real>::V4;
+  __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
+  __shared__ V4 q_pos[kWalkWarpsPerBlock][kQueue];
+  __shared__ V4 q_cot[kWalkWarpsPerBlock][kQueue];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  uint32_t* stack = stack_sm[warp];
+  const WalkParams& w = a.wp;
+  const double half_min_box = 0.5 * fmin(w.box[0], fmin(w.box[1], w.box[2]));
+  const double inv_box[3] = {1.0 / w.box[0], 1.0 / w.box[1], 1.0 / w.box[2]};
+  const Real cut2 = static_cast<Real>(w.cutoff2);
+  const Real box_r[3] = {static_cast<Real>(w.box[0]), static_cast<Real>(w.box[1]), static_cast<Real>(w.box[2])};
+  const Real inv_box_r[3] = {static_cast<Real>(inv_box[0]), static_cast<Real>(inv_box[1]),
+                             static_cast<Real>(inv_box[2])};
+  const double bulk_half = kBulkHalf * w.cutoff;
+
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(a.work, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= a.n) break;
+    const int64_t v = static_cast<int64_t>(base) + lane;
+    const bool valid = v < a.n;
+    uint32_t row = 0;
+    double px = 0.0, py = 0.0, pz = 0.0, mk = 0.0, ckx = 0.0, cky = 0.0, ckz = 0.0;
+    if (valid) {
+      row = a.order[v];
+      px = a.sx[row];
+      py = a.sy[row];
+      pz = a.sz[row];
+      mk = a.m ? a.m[row] : a.uniform_mass;
+      ckx = a.cx[row];
+      cky = a.cy[row];
+      ckz = a.cz[row];
+    }
+    const double rx = __shfl_sync(0xffffffffu, px, 0);
+    const double ry = __shfl_sync(0xffffffffu, py, 0);
+    const double rz = __shfl_sync(0xffffffffu, pz, 0);
+    double ox = px - rx, oy = py - ry, oz = pz - rz;
+    ox -= w.box[0] * rint(ox * inv_box[0]);
+    oy -= w.box[1] * rint(oy * inv_box[1]);
+    oz -= w.box[2] * rint(oz * inv_box[2]);
+    double rg2 = valid ? ox * ox + oy * oy + oz * oz : 0.0;
+    for (int off = 16; off > 0; off >>= 1) rg2 = fmax(rg2, __shfl_xor_sync(0xffffffffu, rg2, off));
+    const double reach = w.cutoff + sqrt(rg2);       // group sphere radius
+    const bool pair_image = reach >= half_min_box * (1.0 - 1.0e-9);
+    const Real tx = static_cast<Real>(ox), ty = static_cast<Real>(oy), tz = static_cast<Real>(oz);
+    const Real mkr = static_cast<Real>(mk);
+    const Real ckxr = static_cast<Real>(ckx), ckyr = static_cast<Real>(cky), ckzr = static_cast<Real>(ckz);
+    double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
+    int qn = 0;
+    if (lane == 0) stack[0] = 0u;
+    int sp = 1;
+    __syncwarp();
+    bool overflow = false;
+
+    auto flush = [&]() {
+      Real gx = 0, gy = 0, gz = 0;
+#pragma unroll 2
+      for (int k = 0; k < qn; ++k) {
+        const V4 e = q_pos[warp][k];
+        const V4 cj = q_cot[warp][k];
+        Real dx = static_cast<Real>(e.x) - tx, dy = static_cast<Real>(e.y) - ty, dz = static_cast<Real>(e.z) - tz;
+        if (pair_image) {
+          dx -= box_r[0] * rint(dx * inv_box_r[0]);
+          dy -= box_r[1] * rint(dy * inv_box_r[1]);
+          dz -= box_r[2] * rint(dz * inv_box_r[2]);
+        }
+        const Real r2 = dx * dx + dy * dy + dz * dz;
+        const bool in = valid && r2 <= cut2 && r2 > Real(0);
+        Real K, Kp;
+        if constexpr (sizeof(Real) == 4) {
+          const float t = r2 * w.inv_4rs2_f;
+          const float hh = evalH<kTerms>(a.poly, t);
+          const float hp = polyHFixed<kTerms>(a.dpoly, t);
+          const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
+          const float rinv = rsqrtf(s2);
+          const float rinv2 = rinv * rinv;
+          const float rinv3 = rinv2 * rinv;
+          K = fmaf(-hh, w.inv_8rs3_f, rinv3);
+          Kp = fmaf(-hp, a.inv_16rs5_f, -3.0f * rinv3 * rinv2);
+        } else {
+          const double rr = in ? r2 : 1.0;
+          K = residualInvR3(rr, w.eps, w.rs);
+          Kp = residualDerivOverR(rr, w.eps, w.rs);
+        }
+        const Real c0 = mkr * static_cast<Real>(cj.x) - static_cast<Real>(e.w) * ckxr;
+        const Real c1 = mkr * static_cast<Real>(cj.y) - static_cast<Real>(e.w) * ckyr;
+        const Real c2 = mkr * static_cast<Real>(cj.z) - static_cast<Real>(e.w) * ckzr;
+        const Real dc = (dx * c0 + dy * c1 + dz * c2) * Kp;
+        // select, not multiply: K and K' are infinite for the excluded self pair
+        gx += in ? K * c0 + dc * dx : Real(0);
+        gy += in ? K * c1 + dc * dy : Real(0);
+        gz += in ? K * c2 + dc * dz : Real(0);
+      }
+      acc_x += static_cast<double>(gx);
+      acc_y += static_cast<double>(gy);
+      acc_z += static_cast<double>(gz);
+      qn = 0;
+      __syncwarp();
+    };
+
+    auto enqueue = [&](uint32_t begin, uint32_t count, uint32_t mask) {
+      // sphere of the lanes that need the node (their offsets, FP64)
+      const int first = __ffs(mask) - 1;
+      const double scx = __shfl_sync(0xffffffffu, ox, first);
+      const double scy = __shfl_sync(0xffffffffu, oy, first);
+      const double scz = __shfl_sync(0xffffffffu, oz, first);
+      double d2 = 0.0;
+      if ((mask >> lane) & 1u) {
+        const double ux = ox - scx, uy = oy - scy, uz = oz - scz;
+        d2 = ux * ux + uy * uy + uz * uz;
+      }
+      for (int off = 16; off > 0; off >>= 1) d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, off));
+      const double sr = w.cutoff + sqrt(d2);
+      const double sr2 = sr * sr * (1.0 + 1.0e-6);
+      for (uint32_t chunk = 0; chunk < count; chunk += 32) {
+        const uint32_t k = chunk + lane;
+        bool keep = false;
+        double ex = 0.0, ey = 0.0, ez = 0.0;
+        double4 sv = make_double4(0.0, 0.0, 0.0, 0.0), cv = sv;
+        if (k < count) {
+          sv = a.src_d4[begin + k];
+          ex = sv.x - rx;
+          ey = sv.y - ry;
+          ez = sv.z - rz;
+          ex -= w.box[0] * rint(ex * inv_box[0]);
+          ey -= w.box[1] * rint(ey * inv_box[1]);
+          ez -= w.box[2] * rint(ez * inv_box[2]);
+          const double qx = ex - scx, qy = ey - scy, qz = ez - scz;
+          keep = qx * qx + qy * qy + qz * qz <= sr2;
+          if (keep) cv = a.src_c4[begin + k];
+        }
+        const uint32_t keep_mask = __ballot_sync(0xffffffffu, keep);
+        const int c = __popc(keep_mask);
+        if (qn + c > kQueue) flush();
+        if (keep) {
+          const int slot_q = qn + __popc(keep_mask & ((1u << lane) - 1u));
+          V4 e, cj;
+          e.x = static_cast<Real>(ex);
+          e.y = static_cast<Real>(ey);
+          e.z = static_cast<Real>(ez);
+          e.w = static_cast<Real>(sv.w);
+          cj.x = static_cast<Real>(cv.x);
+          cj.y = static_cast<Real>(cv.y);
+          cj.z = static_cast<Real>(cv.z);
+          cj.w = Real(0);
+          q_pos[warp][slot_q] = e;
+          q_cot[warp][slot_q] = cj;
+        }
+        __syncwarp();
+        qn += c;
+      }
+    };
+
+    while (sp > 0) {
+      const uint32_t node = stack[sp - 1];
+      --sp;
+      __syncwarp();
+      const double4 g = a.geom[node];
+      const uint4 rg4 = a.range[node];
+      const double h = g.w;
+      // lanes whose r_cut sphere may reach the node cube: each lane takes its
+      // own minimum image of the cube centre, so the test holds however far
+      // apart the warp's targets are (only cubes with h + r_cut >= L/2, near
+      // the root, are never pruned)
+      bool need = valid;
+      if (valid && h + w.cutoff < half_min_box * (1.0 - 1.0e-9)) {
+        double dx = g.x - px, dy = g.y - py, dz = g.z - pz;
+        dx -= w.box[0] * rint(dx * inv_box[0]);
+        dy -= w.box[1] * rint(dy * inv_box[1]);
+        dz -= w.box[2] * rint(dz * inv_box[2]);
+        const double ex = fmax(0.0, fabs(dx) - h), ey = fmax(0.0, fabs(dy) - h), ez = fmax(0.0, fabs(dz) - h);
+        need = ex * ex + ey * ey + ez * ez <= w.cutoff2 * (1.0 + 1.0e-9);
+      }
+      const uint32_t need_mask = __ballot_sync(0xffffffffu, need);
+      if (need_mask == 0u) continue;
+      if (rg4.z == 0 || (rg4.y <= kBulkCount && h <= bulk_half)) {
+        enqueue(rg4.x, rg4.y, need_mask);
+        continue;
+      }
+      const uint32_t ch = lane < 8 ? a.child[8 * static_cast<size_t>(node) + lane] : kInvalid;
+      const unsigned cmask = __ballot_sync(0xffffffffu, ch != kInvalid) & 0xFFu;
+      const int nc = __popc(cmask);
+      if (sp + nc > kStackCap) {
+        overflow = true;
+        break;
+      }
+      if (ch != kInvalid) stack[sp + __popc(cmask >> (lane + 1))] = ch;
+      sp += nc;
+      __syncwarp();
+    }
+    if (qn > 0) flush();
+    if (overflow && lane == 0) atomicOr(a.status, kStatusStackOverflow);
+    if (valid) {
+      a.out_x[row] = w.G * acc_x;
+      a.out_y[row] = w.G * acc_y;
+      a.out_z[row] = w.G * acc_z;
+    }
+    __syncwarp();
+  }
+}
+
+// Cotangents gathered into tree order (double4 {a_bar, 0}).
+__global__ void packCotangentKernel(int64_t n, const uint32_t* __restrict__ sorted, const double* __restrict__ cx,
+                                    const double* __restrict__ cy, const double* __restrict__ cz, double4* out) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t s = sorted[t];
+    out[t] = make_double4(cx[s], cy[s], cz[s], 0.0);
+  }
+}
+
+template <class Kernel>
+int launchVjp(Kernel kernel, const VjpArgs& args, cudaStream_t s) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWalkWarpsPerBlock * 32, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t warps_needed = (args.n + 31) / 32;
+  int64_t blocks = static_cast<int64_t>(sms) * per_sm;
+  const int64_t max_useful = (warps_needed + kWalkWarpsPerBlock - 1) / kWalkWarpsPerBlock;
+  if (blocks > max_useful) blocks = max_useful;
+  if (blocks < 1) blocks = 1;
+  { noteLaunch(); kernel<<<static_cast<unsigned>(blocks), kWalkWarpsPerBlock * 32, 0, s>>>(args); }
+  return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
+}
+
 template <class Kernel>
 int launchPersistent(Kernel kernel, const WalkArgs& args, cudaStream_t s) {
   int dev = 0, sms = 148, per_sm = 1;
@@ -919,6 +1205,51 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
 #undef CHUI_WALK_DISPATCH
   }
   return launchWalk<false, false>(a, s);
+}
+
+int walkVjpRun(Context& c, int64_t n, const double* sx, const double* sy, const double* sz, const double* m,
+               double uniform_mass, const double* cx, const double* cy, const double* cz, const WalkParams& wp,
+               double* gx, double* gy, double* gz, cudaStream_t s) {
+  if (n == 0) return 0;
+  if (ensure(c.src_cot, static_cast<size_t>(n) * sizeof(double4)) || ensure(c.work_counter, 4))
+    return CHUI_TREEPM_ENOMEM;
+  { noteLaunch(); packCotangentKernel<<<static_cast<unsigned>(std::min<int64_t>((n + 255) / 256, 148 * 32)), 256, 0, s>>>(
+      n, c.sorted_index.as<uint32_t>(), cx, cy, cz, c.src_cot.as<double4>()); }
+  cudaMemsetAsync(c.work_counter.ptr, 0, 4, s);
+  VjpArgs a;
+  a.n = n;
+  a.order = c.target_order.as<uint32_t>();
+  a.sx = sx;
+  a.sy = sy;
+  a.sz = sz;
+  a.m = m;
+  a.uniform_mass = uniform_mass;
+  a.cx = cx;
+  a.cy = cy;
+  a.cz = cz;
+  a.geom = c.node_geom.as<double4>();
+  a.range = c.node_range.as<uint4>();
+  a.child = c.node_child.as<uint32_t>();
+  a.src_d4 = c.src_d4.as<double4>();
+  a.src_c4 = c.src_cot.as<double4>();
+  a.out_x = gx;
+  a.out_y = gy;
+  a.out_z = gz;
+  a.work = c.work_counter.as<uint32_t>();
+  a.status = c.status.as<uint32_t>();
+  a.poly = c.poly;
+  a.dpoly = c.dpoly;
+  a.wp = wp;
+  const double rs2 = c.rs * c.rs;
+  a.inv_16rs5_f = static_cast<float>(1.0 / (16.0 * rs2 * rs2 * c.rs));
+  const bool eps_zero = wp.eps == 0.0;
+  if (c.cfg.precision == CHUI_TREEPM_MIXED) {
+    if (c.poly.terms <= 12 && c.dpoly.terms <= 12)
+      return eps_zero ? launchVjp(walkVjpKernel<float, true, 12>, a, s) : launchVjp(walkVjpKernel<float, false, 12>, a, s);
+    return eps_zero ? launchVjp(walkVjpKernel<float, true, kPolyMaxTerms>, a, s)
+                    : launchVjp(walkVjpKernel<float, false, kPolyMaxTerms>, a, s);
+  }
+  return launchVjp(walkVjpKernel<double, false, 12>, a, s);
 }
 
 }  // namespace chui

@@ -211,6 +211,45 @@ int chui_treepm_drift(void *handle, int64_t n, double *x, double *y, double *z,
  * drag = 1. factors = {drift, kick1, kick2, drag1, drag2}. */
 int chui_treepm_kdk_factors_static(double dt, double factors[5]);
 
+/* Global FP64 momentum and energy checks over n particles: out = {sum m v_x,
+ * sum m v_y, sum m v_z, sum m a_x, sum m a_y, sum m a_z, sum m |v|^2 / 2,
+ * sum m}. mass may be NULL (uniform_mass); a_* may all be NULL. Reductions run
+ * in FP64 on the device. */
+int chui_treepm_momentum_energy(void *handle, int64_t n, const double *mass, double uniform_mass,
+                                const double *vx, const double *vy, const double *vz, const double *ax,
+                                const double *ay, const double *az, int memory, void *stream, double out[8]);
+
+/* ---- Adjoint (no counterpart in the reference) ----------------------------
+ * Reverse-mode building blocks for gradients of a loss on final positions or
+ * density with respect to initial conditions. */
+
+/* grad = J^T cot for the full TreePM acceleration a(x) of all sources (every
+ * particle a target): PM part transposed exactly (interpolation, k-space
+ * gradient operators, deposit); short-range part over the tree rebuilt for
+ * these positions, as the pair-force Jacobian of every pair inside r_cut
+ * (accepted strict multipoles are differentiated as the pairs they stand
+ * for). cot and grad are source-indexed. The PM field cached for cadence
+ * reuse afterwards holds these positions' field. stats may be NULL. */
+int chui_treepm_force_vjp(void *handle, const chui_treepm_sources *sources, const double *cot_x,
+                          const double *cot_y, const double *cot_z, double *grad_x, double *grad_y,
+                          double *grad_z, int memory, void *stream, chui_treepm_stats *stats);
+
+/* grad_j = sum_c rho_bar(c) d rho(c) / d x_j for the density of
+ * chui_pm_assign_density (compact nx*ny*nz row-major cotangent). */
+int chui_pm_density_vjp(void *handle, const chui_treepm_sources *sources, const double *rho_bar,
+                        double *grad_x, double *grad_y, double *grad_z, int memory, void *stream);
+
+/* Transpose of one KDK step (kick1/drag1, drift, kick2/drag2), in place on
+ * device arrays, given g = chui_treepm_force_vjp at the step's end positions
+ * for the pending force cotangent a_bar:
+ *   x_bar += g; vh = drag2 v_bar + D x_bar; v_bar = drag1 vh;
+ *   a_bar = kick1 vh + (first_step ? 0 : kick2 v_bar)   (cotangent at the start positions). */
+int chui_treepm_kdk_adjoint(void *handle, int64_t n, const double *gx, const double *gy, const double *gz,
+                            double *x_bar_x, double *x_bar_y, double *x_bar_z, double *v_bar_x,
+                            double *v_bar_y, double *v_bar_z, double *a_bar_x, double *a_bar_y,
+                            double *a_bar_z, double drift_factor, double kick1, double kick2, double drag1,
+                            double drag2, int first_step, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
