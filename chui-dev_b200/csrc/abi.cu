@@ -683,16 +683,14 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   }
   const double total_mass = m ? mass_sum : static_cast<double>(n) * src->uniform_mass;
 
-  // PM refresh or cached-field reuse (tree_pm_coupling.cpp:2483-2532)
-  if (refresh_long_range_field) {
-    if ((rc = chui::pmRefresh(c, n, x, y, z, m, src->uniform_mass, total_mass, s))) return rc;
-  } else if (!c.pm_field_valid || c.pm_field_box[0] != c.cfg.box_x || c.pm_field_box[1] != c.cfg.box_y ||
-             c.pm_field_box[2] != c.cfg.box_z) {
+  // cached-field reuse needs a compatible field (tree_pm_coupling.cpp:2483-2532)
+  if (!refresh_long_range_field &&
+      (!c.pm_field_valid || c.pm_field_box[0] != c.cfg.box_x || c.pm_field_box[1] != c.cfg.box_y ||
+       c.pm_field_box[2] != c.cfg.box_z)) {
     return chui::fail(c, CHUI_TREEPM_ESTATE, "TreePM long-range reuse requested without a compatible PM field");
   }
-  cudaEventRecord(c.ev[1], s);
 
-  // periodic tree build
+  // periodic tree build (first: the PM deposit reads the tree-ordered sources)
   if ((rc = chui::treeBuild(c, n, x, y, z, m, src->uniform_mass, lo, hi, s))) {
     if (c.last_error.empty()) c.last_error = "TreePM tree build failed";
     return rc;
@@ -701,6 +699,13 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   if ((rc = chui::treeNodeBounds(c, nlo, nhi, s))) return chui::fail(c, rc, "node bounds failed");
   if ((rc = chui::treeOrderTargets(c, nt, active, explicit_targets ? 1 : 0, n, s)))
     return chui::fail(c, rc, "target ordering failed");
+  cudaEventRecord(c.ev[1], s);
+
+  // PM refresh (tiled deposit over the tree-ordered sources)
+  if (refresh_long_range_field &&
+      (rc = chui::pmRefresh(c, n, x, y, z, m, src->uniform_mass, total_mass, s,
+                            n > 0 ? c.src_d4.as<double4>() : nullptr)))
+    return rc;
   cudaEventRecord(c.ev[2], s);
 
   // residual walk
@@ -828,9 +833,9 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   stt.kernel_launches = chui::launchCount() - launches_before;
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
-  stt.pm_ms = ms;
-  cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
   stt.tree_build_ms = ms;
+  cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+  stt.pm_ms = ms;
   cudaEventElapsedTime(&ms, c.ev[2], c.ev[3]);
   stt.walk_ms = ms;
   cudaEventElapsedTime(&ms, c.ev[0], c.ev[4]);
@@ -884,10 +889,6 @@ int chui_treepm_force_vjp(void* handle, const chui_treepm_sources* src, const do
     gy = c.out_acc[1].as<double>();
     gz = c.out_acc[2].as<double>();
   }
-  // PM part (refreshes the PM field at these positions)
-  if ((rc = chui::pmForceVjp(c, n, x, y, z, m, src->uniform_mass, total_mass, cx, cy, cz, gx, gy, gz, s)))
-    return chui::fail(c, rc, c.last_error.empty() ? "PM adjoint failed" : c.last_error);
-  cudaEventRecord(c.ev[1], s);
   // tree for these positions, every particle a target in tree order
   if (n > 0) {
     if ((rc = chui::treeBuild(c, n, x, y, z, m, src->uniform_mass, lo, hi, s))) {
@@ -896,6 +897,11 @@ int chui_treepm_force_vjp(void* handle, const chui_treepm_sources* src, const do
     }
     if ((rc = chui::treeOrderTargets(c, n, nullptr, 0, n, s))) return chui::fail(c, rc, "target ordering failed");
   }
+  cudaEventRecord(c.ev[1], s);
+  // PM part (refreshes the PM field at these positions)
+  if ((rc = chui::pmForceVjp(c, n, x, y, z, m, src->uniform_mass, total_mass, cx, cy, cz, gx, gy, gz, s,
+                             n > 0 ? c.src_d4.as<double4>() : nullptr)))
+    return chui::fail(c, rc, c.last_error.empty() ? "PM adjoint failed" : c.last_error);
   cudaEventRecord(c.ev[2], s);
   chui::WalkParams wp{};
   wp.box[0] = c.cfg.box_x;
@@ -941,9 +947,9 @@ int chui_treepm_force_vjp(void* handle, const chui_treepm_sources* src, const do
     stt.kernel_launches = chui::launchCount() - launches_before;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
-    stt.pm_ms = ms;
-    cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
     stt.tree_build_ms = ms;
+    cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+    stt.pm_ms = ms;
     cudaEventElapsedTime(&ms, c.ev[2], c.ev[3]);
     stt.walk_ms = ms;
     cudaEventElapsedTime(&ms, c.ev[0], c.ev[4]);

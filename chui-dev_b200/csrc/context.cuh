@@ -123,8 +123,11 @@ struct Context {
 
 // ---- PM (pm.cu) ----
 int pmPrepare(Context& c);
+// tree_sources (nullable): the same sources in tree order as double4
+// {position, mass} (Context::src_d4 after treeBuild); selects the tiled deposit.
 int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const double* z,
-              const double* m, double uniform_mass, double total_mass, cudaStream_t s);
+              const double* m, double uniform_mass, double total_mass, cudaStream_t s,
+              const double4* tree_sources = nullptr);
 // CIC/TSC interpolation of the cached force grids at targets (active slots).
 int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* tx,
                   const double* ty, const double* tz, const double* sx, const double* sy,
@@ -137,7 +140,7 @@ int pmCells(Context& c, int64_t n, const double* x, const double* y, const doubl
 // (refreshes the PM field at these positions first).
 int pmForceVjp(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
                double uniform_mass, double total_mass, const double* cx, const double* cy, const double* cz,
-               double* gx, double* gy, double* gz, cudaStream_t s);
+               double* gx, double* gy, double* gz, cudaStream_t s, const double4* tree_sources = nullptr);
 // Adjoint of the compact FP64 density for a cotangent grid rho_bar.
 int pmDensityVjp(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
                  double uniform_mass, const double* rho_bar, double* gx, double* gy, double* gz, cudaStream_t s);

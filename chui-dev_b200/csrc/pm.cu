@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <vector>
 
@@ -122,6 +124,123 @@ __global__ void depositKernel(int64_t n, const double* __restrict__ x, const dou
         }
       }
     }
+  }
+}
+
+// Mass assignment over tree-ordered sources (double4 {position, mass}),
+// accumulated per block in a shared-memory tile. A block takes chunks of
+// kDepositChunk consecutive tree positions, which occupy a compact region;
+// it finds the chunk's base-cell bounding box, and when the stencil box fits
+// the tile it deposits with shared-memory atomics and then adds the tile's
+// nonzero cells to the grid (one global atomic per touched cell instead of
+// taps^3 per particle). Chunks that straddle the periodic boundary or are too
+// spread out deposit with global atomics. Weights and cells are those of
+// depositKernel (same stencil arithmetic); only the summation order differs.
+#ifndef CHUI_DEPOSIT_CHUNK
+#define CHUI_DEPOSIT_CHUNK 1024
+#endif
+constexpr int kDepositChunk = CHUI_DEPOSIT_CHUNK;
+constexpr int kDepositTileBytes = 32768;
+
+template <class R>
+__global__ void __launch_bounds__(256) depositTiledKernel(int64_t n, const double4* __restrict__ src,
+                                                          double inv_cell_volume, PmGeom g, R* grid) {
+  __shared__ __align__(16) unsigned char tile_raw[kDepositTileBytes];
+  __shared__ int box_lo[3], box_hi[3];
+  R* tile = reinterpret_cast<R*>(tile_raw);
+  constexpr int kTileCells = kDepositTileBytes / static_cast<int>(sizeof(R));
+  const int taps = g.scheme == 0 ? 2 : 3;
+  const int64_t chunks = (n + kDepositChunk - 1) / kDepositChunk;
+  for (int64_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x) {
+    const int64_t begin = chunk * kDepositChunk;
+    const int count = static_cast<int>(n - begin < kDepositChunk ? n - begin : kDepositChunk);
+    if (threadIdx.x < 3) {
+      box_lo[threadIdx.x] = INT_MAX;
+      box_hi[threadIdx.x] = INT_MIN;
+    }
+    __syncthreads();
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (int i = threadIdx.x; i < count; i += blockDim.x) {
+      const double4 p = src[begin + i];
+      const double v[3] = {p.x, p.y, p.z};
+      for (int a = 0; a < 3; ++a) {
+        const int o = static_cast<int>(makeStencil(wrapPosition(v[a], g.L[a]) * g.inv_d[a], g.scheme).off0);
+        lo[a] = min(lo[a], o);
+        hi[a] = max(hi[a], o);
+      }
+    }
+    for (int a = 0; a < 3; ++a) {
+      for (int off = 16; off > 0; off >>= 1) {
+        lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+        hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+      }
+    }
+    if ((threadIdx.x & 31) == 0) {
+      for (int a = 0; a < 3; ++a) {
+        atomicMin(box_lo + a, lo[a]);
+        atomicMax(box_hi + a, hi[a]);
+      }
+    }
+    __syncthreads();
+    const int b0 = box_lo[0], b1 = box_lo[1], b2 = box_lo[2];
+    const int e0 = box_hi[0] - b0 + taps, e1 = box_hi[1] - b1 + taps, e2 = box_hi[2] - b2 + taps;
+    const int64_t cells = static_cast<int64_t>(e0) * e1 * e2;
+    if (cells <= kTileCells) {
+      const int tc = static_cast<int>(cells);
+      for (int t = threadIdx.x; t < tc; t += blockDim.x) tile[t] = R(0);
+      __syncthreads();
+      for (int i = threadIdx.x; i < count; i += blockDim.x) {
+        const double4 p = src[begin + i];
+        const Stencil s0 = makeStencil(wrapPosition(p.x, g.L[0]) * g.inv_d[0], g.scheme);
+        const Stencil s1 = makeStencil(wrapPosition(p.y, g.L[1]) * g.inv_d[1], g.scheme);
+        const Stencil s2 = makeStencil(wrapPosition(p.z, g.L[2]) * g.inv_d[2], g.scheme);
+        const double mass = p.w * inv_cell_volume;
+        for (int a = 0; a < taps; ++a) {
+          const int lx = static_cast<int>(s0.off0) - b0 + a;
+          for (int b = 0; b < taps; ++b) {
+            const int ly = static_cast<int>(s1.off0) - b1 + b;
+            const double wxy = s0.w[a] * s1.w[b];
+            for (int cc = 0; cc < taps; ++cc) {
+              const int lz = static_cast<int>(s2.off0) - b2 + cc;
+              atomicAdd(tile + (lx * e1 + ly) * e2 + lz, static_cast<R>(mass * (wxy * s2.w[cc])));
+            }
+          }
+        }
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < tc; t += blockDim.x) {
+        const R v = tile[t];
+        if (v == R(0)) continue;
+        const int lz = t % e2;
+        const int ly = (t / e2) % e1;
+        const int lx = t / (e1 * e2);
+        const int64_t ix = wrapIndex(b0 + lx, g.n[0]);
+        const int64_t iy = wrapIndex(b1 + ly, g.n[1]);
+        const int64_t iz = wrapIndex(b2 + lz, g.n[2]);
+        atomicAdd(grid + (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp + iz, v);
+      }
+    } else {
+      for (int i = threadIdx.x; i < count; i += blockDim.x) {
+        const double4 p = src[begin + i];
+        const Stencil s0 = makeStencil(wrapPosition(p.x, g.L[0]) * g.inv_d[0], g.scheme);
+        const Stencil s1 = makeStencil(wrapPosition(p.y, g.L[1]) * g.inv_d[1], g.scheme);
+        const Stencil s2 = makeStencil(wrapPosition(p.z, g.L[2]) * g.inv_d[2], g.scheme);
+        const double mass = p.w * inv_cell_volume;
+        for (int a = 0; a < taps; ++a) {
+          const int64_t ix = wrapIndex(s0.off0 + a, g.n[0]);
+          for (int b = 0; b < taps; ++b) {
+            const int64_t iy = wrapIndex(s1.off0 + b, g.n[1]);
+            const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
+            const double wxy = s0.w[a] * s1.w[b];
+            for (int cc = 0; cc < taps; ++cc) {
+              const int64_t iz = wrapIndex(s2.off0 + cc, g.n[2]);
+              atomicAdd(grid + row + iz, static_cast<R>(mass * (wxy * s2.w[cc])));
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -516,7 +635,8 @@ void pmDestroy(Context& c) {
 }
 
 int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const double* z,
-              const double* m, double uniform_mass, double total_mass, cudaStream_t s) {
+              const double* m, double uniform_mass, double total_mass, cudaStream_t s,
+              const double4* tree_sources) {
   int rc = pmPrepare(c);
   if (rc) return rc;
   const PmGeom g = geomOf(c);
@@ -532,12 +652,18 @@ int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const dou
   if (mixed) {
     { noteLaunch(); fillKernel<float><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<float>(), padded,
                                                                static_cast<float>(-mean)); }
-    if (n > 0)
+    if (n > 0 && tree_sources)
+      { noteLaunch(); depositTiledKernel<float><<<static_cast<unsigned>(std::min<int64_t>((n + kDepositChunk - 1) / kDepositChunk, 148 * 8)), 256, 0, s>>>(
+          n, tree_sources, 1.0 / cell_volume, g, c.grid[0].as<float>()); }
+    else if (n > 0)
       { noteLaunch(); depositKernel<float><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
                                                                1.0 / cell_volume, g, c.grid[0].as<float>()); }
   } else {
     { noteLaunch(); fillKernel<double><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<double>(), padded, -mean); }
-    if (n > 0)
+    if (n > 0 && tree_sources)
+      { noteLaunch(); depositTiledKernel<double><<<static_cast<unsigned>(std::min<int64_t>((n + kDepositChunk - 1) / kDepositChunk, 148 * 8)), 256, 0, s>>>(
+          n, tree_sources, 1.0 / cell_volume, g, c.grid[0].as<double>()); }
+    else if (n > 0)
       { noteLaunch(); depositKernel<double><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
                                                                 1.0 / cell_volume, g, c.grid[0].as<double>()); }
   }
@@ -660,8 +786,8 @@ int pmDensityInto(const chui_treepm_config& cfg, int64_t n, const double* x, con
 // these positions, then g = J_pm^T a_bar (written, not accumulated).
 int pmForceVjp(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
                double uniform_mass, double total_mass, const double* cx, const double* cy, const double* cz,
-               double* gx, double* gy, double* gz, cudaStream_t s) {
-  int rc = pmRefresh(c, n, x, y, z, m, uniform_mass, total_mass, s);
+               double* gx, double* gy, double* gz, cudaStream_t s, const double4* tree_sources) {
+  int rc = pmRefresh(c, n, x, y, z, m, uniform_mass, total_mass, s, tree_sources);
   if (rc) return rc;
   if (n == 0) return 0;
   const PmGeom g = geomOf(c);

@@ -994,6 +994,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpA
       for (int off = 16; off > 0; off >>= 1) d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, off));
       const double sr = w.cutoff + sqrt(d2);
       const double sr2 = sr * sr * (1.0 + 1.0e-6);
+      // a sphere reaching half the box keeps everything; in warps whose pairs
+      // take their own minimum image, the distance to its centre is wrapped too
+      const bool keep_all = sr >= half_min_box * (1.0 - 1.0e-9);
       for (uint32_t chunk = 0; chunk < count; chunk += 32) {
         const uint32_t k = chunk + lane;
         bool keep = false;
@@ -1007,8 +1010,13 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpA
           ex -= w.box[0] * rint(ex * inv_box[0]);
           ey -= w.box[1] * rint(ey * inv_box[1]);
           ez -= w.box[2] * rint(ez * inv_box[2]);
-          const double qx = ex - scx, qy = ey - scy, qz = ez - scz;
-          keep = qx * qx + qy * qy + qz * qz <= sr2;
+          double qx = ex - scx, qy = ey - scy, qz = ez - scz;
+          if (pair_image) {
+            qx -= w.box[0] * rint(qx * inv_box[0]);
+            qy -= w.box[1] * rint(qy * inv_box[1]);
+            qz -= w.box[2] * rint(qz * inv_box[2]);
+          }
+          keep = keep_all || qx * qx + qy * qy + qz * qz <= sr2;
           if (keep) cv = a.src_c4[begin + k];
         }
         const uint32_t keep_mask = __ballot_sync(0xffffffffu, keep);

@@ -140,16 +140,17 @@ def test_kdk_gradient_matches_finite_differences(dev):
     0.05 at unit mean density with softening 0.1 spacing (unsoftened close
     encounters make the trajectory chaotic, and no gradient check is then
     meaningful): FP64 adjoint gradient vs central differences of the FP64
-    forward on 64 random components (h = 1e-4 spacing); mixed adjoint vs FP64
+    forward (deterministic) on 64 random components; mixed adjoint vs FP64
     adjoint.
 
-    The residual pair force is cut off at r_cut, where it is ~2.5e-4 of the
-    Newtonian force, so the forward map jumps whenever a pair crosses r_cut;
-    with h = 1e-4 spacing about half of the perturbed particles have such a
-    crossing inside the difference interval. Each component is therefore also
-    differenced with h/2: where the two estimates agree (no crossing) the
-    adjoint must match them tightly, and all components must match to the
-    size of the jumps."""
+    With h = 1e-4 spacing the differences straddle the forward map's jumps:
+    the residual pair force is cut off at r_cut, where it is ~2.5e-4 of the
+    Newtonian force, and CIC weights have kinks at cell faces, so those
+    components are compared against the gradient's scale (its largest
+    component over all particles). With h = 1e-6 spacing almost no interval
+    contains a jump, and components are compared one by one; a few may differ
+    by the strict-multipole truncation, which the adjoint differentiates as
+    the pairs it stands for."""
     n_side, box, steps, dt = 64, 50.0, 10, 0.05
     spacing = box / n_side
     eps = 0.1 * spacing
@@ -168,10 +169,11 @@ def test_kdk_gradient_matches_finite_differences(dev):
             grads[prec] = [g.cpu().numpy() for g in torch.autograd.grad(loss, s)]
     g64 = grads[ct._abi.FP64]
     assert rel(grads[ct._abi.MIXED], g64) <= 1e-3
+    scale = max(float(np.abs(g).max()) for g in g64)
+    assert math.isfinite(scale) and scale > 0
 
     rng = np.random.default_rng(13)
     comps = [(int(rng.integers(3)), int(rng.integers(len(m)))) for _ in range(64)]
-    h = 1e-4 * spacing
 
     def central(solver, dsol, axis, i, step):
         vals = []
@@ -182,19 +184,16 @@ def test_kdk_gradient_matches_finite_differences(dev):
                 vals.append(density_loss(solver, dsol, q, s, mass, target, steps, dt).item())
         return (vals[0] - vals[1]) / (2 * step)
 
-    fd, fd2, ad = [], [], []
+    fd4, fd6, ad = [], [], []
     with make_solver(n_side, box, ct._abi.FP64, eps=eps) as solver, \
             make_solver(n_side, box, ct._abi.FP64) as dsol:
         for axis, i in comps:
-            fd.append(central(solver, dsol, axis, i, h))
-            fd2.append(central(solver, dsol, axis, i, 0.5 * h))
+            fd4.append(central(solver, dsol, axis, i, 1e-4 * spacing))
+            fd6.append(central(solver, dsol, axis, i, 1e-6 * spacing))
             ad.append(g64[axis][i])
-    fd, fd2, ad = np.array(fd), np.array(fd2), np.array(ad)
-    scale = np.abs(ad).max()
-    assert math.isfinite(scale) and scale > 0
-    err = np.abs(fd - ad) / scale
-    smooth = np.abs(fd - fd2) <= 1e-5 * scale
-    err_smooth = np.abs(fd2 - ad)[smooth] / scale
-    assert smooth.sum() >= 16, smooth.sum()
-    assert np.median(err_smooth) <= 1e-5 and err_smooth.max() <= 1e-4, (np.median(err_smooth), err_smooth.max())
-    assert np.median(err) <= 2e-3 and err.max() <= 2e-2, (np.median(err), err.max())
+    fd4, fd6, ad = np.array(fd4), np.array(fd6), np.array(ad)
+    err4 = np.abs(fd4 - ad) / scale
+    assert np.median(err4) <= 1e-4 and err4.max() <= 1e-3, (np.median(err4), err4.max())
+    err6 = np.abs(fd6 - ad) / np.maximum(np.abs(ad), 1e-3 * scale)
+    assert np.median(err6) <= 1e-4, np.median(err6)
+    assert np.quantile(err6, 0.9) <= 1e-3, np.quantile(err6, 0.9)
