@@ -147,10 +147,8 @@ def test_kdk_gradient_matches_finite_differences(dev):
     the residual pair force is cut off at r_cut, where it is ~2.5e-4 of the
     Newtonian force, and CIC weights have kinks at cell faces, so those
     components are compared against the gradient's scale (its largest
-    component over all particles). With h = 1e-6 spacing almost no interval
-    contains a jump, and components are compared one by one; a few may differ
-    by the strict-multipole truncation, which the adjoint differentiates as
-    the pairs it stands for."""
+    component over all particles). With h = 1e-6 spacing no interval contains
+    a jump here, and every component must match on its own."""
     n_side, box, steps, dt = 64, 50.0, 10, 0.05
     spacing = box / n_side
     eps = 0.1 * spacing
@@ -195,5 +193,4 @@ def test_kdk_gradient_matches_finite_differences(dev):
     err4 = np.abs(fd4 - ad) / scale
     assert np.median(err4) <= 1e-4 and err4.max() <= 1e-3, (np.median(err4), err4.max())
     err6 = np.abs(fd6 - ad) / np.maximum(np.abs(ad), 1e-3 * scale)
-    assert np.median(err6) <= 1e-4, np.median(err6)
-    assert np.quantile(err6, 0.9) <= 1e-3, np.quantile(err6, 0.9)
+    assert np.median(err6) <= 1e-4 and err6.max() <= 1e-3, (np.median(err6), err6.max())
