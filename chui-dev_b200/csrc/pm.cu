@@ -131,25 +131,41 @@ __global__ void depositKernel(int64_t n, const double* __restrict__ x, const dou
 // accumulated per block in a shared-memory tile. A block takes chunks of
 // kDepositChunk consecutive tree positions, which occupy a compact region;
 // it finds the chunk's base-cell bounding box, and when the stencil box fits
-// the tile it deposits with shared-memory atomics and then adds the tile's
-// nonzero cells to the grid (one global atomic per touched cell instead of
-// taps^3 per particle). Chunks that straddle the periodic boundary or are too
+// the tile it deposits into shared memory and then adds the tile's nonzero
+// cells to the grid (one global atomic per touched cell instead of taps^3 per
+// particle). Each thread takes a contiguous run of the chunk and sums the
+// stencils of consecutive particles with the same base cell in registers
+// (dense regions repeat base cells along tree order), so shared-memory
+// atomics are issued once per run of equal cells and lanes of a warp work in
+// different places. Chunks that straddle the periodic boundary or are too
 // spread out deposit with global atomics. Weights and cells are those of
 // depositKernel (same stencil arithmetic); only the summation order differs.
 #ifndef CHUI_DEPOSIT_CHUNK
-#define CHUI_DEPOSIT_CHUNK 1024
+#define CHUI_DEPOSIT_CHUNK 2048
 #endif
 constexpr int kDepositChunk = CHUI_DEPOSIT_CHUNK;
 constexpr int kDepositTileBytes = 32768;
 
-template <class R>
+template <class R, int kTaps>
+__device__ __forceinline__ void tileFlush(R* tile, int e1, int e2, int lx, int ly, int lz, const R (&acc)[kTaps * kTaps * kTaps]) {
+#pragma unroll
+  for (int a = 0; a < kTaps; ++a)
+#pragma unroll
+    for (int b = 0; b < kTaps; ++b)
+#pragma unroll
+      for (int c = 0; c < kTaps; ++c) {
+        const R v = acc[(a * kTaps + b) * kTaps + c];
+        if (v != R(0)) atomicAdd(tile + ((lx + a) * e1 + (ly + b)) * e2 + (lz + c), v);
+      }
+}
+
+template <class R, int kTaps>
 __global__ void __launch_bounds__(256) depositTiledKernel(int64_t n, const double4* __restrict__ src,
                                                           double inv_cell_volume, PmGeom g, R* grid) {
   __shared__ __align__(16) unsigned char tile_raw[kDepositTileBytes];
   __shared__ int box_lo[3], box_hi[3];
   R* tile = reinterpret_cast<R*>(tile_raw);
   constexpr int kTileCells = kDepositTileBytes / static_cast<int>(sizeof(R));
-  const int taps = g.scheme == 0 ? 2 : 3;
   const int64_t chunks = (n + kDepositChunk - 1) / kDepositChunk;
   for (int64_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x) {
     const int64_t begin = chunk * kDepositChunk;
@@ -183,30 +199,46 @@ __global__ void __launch_bounds__(256) depositTiledKernel(int64_t n, const doubl
     }
     __syncthreads();
     const int b0 = box_lo[0], b1 = box_lo[1], b2 = box_lo[2];
-    const int e0 = box_hi[0] - b0 + taps, e1 = box_hi[1] - b1 + taps, e2 = box_hi[2] - b2 + taps;
+    const int e0 = box_hi[0] - b0 + kTaps, e1 = box_hi[1] - b1 + kTaps, e2 = box_hi[2] - b2 + kTaps;
     const int64_t cells = static_cast<int64_t>(e0) * e1 * e2;
     if (cells <= kTileCells) {
       const int tc = static_cast<int>(cells);
       for (int t = threadIdx.x; t < tc; t += blockDim.x) tile[t] = R(0);
       __syncthreads();
-      for (int i = threadIdx.x; i < count; i += blockDim.x) {
+      // contiguous run per thread, equal base cells summed in registers
+      const int per = (count + static_cast<int>(blockDim.x) - 1) / static_cast<int>(blockDim.x);
+      const int i0 = static_cast<int>(threadIdx.x) * per;
+      const int i1 = min(i0 + per, count);
+      R acc[kTaps * kTaps * kTaps];
+#pragma unroll
+      for (int t = 0; t < kTaps * kTaps * kTaps; ++t) acc[t] = R(0);
+      int cx = INT_MIN, cy = 0, cz = 0;
+      for (int i = i0; i < i1; ++i) {
         const double4 p = src[begin + i];
         const Stencil s0 = makeStencil(wrapPosition(p.x, g.L[0]) * g.inv_d[0], g.scheme);
         const Stencil s1 = makeStencil(wrapPosition(p.y, g.L[1]) * g.inv_d[1], g.scheme);
         const Stencil s2 = makeStencil(wrapPosition(p.z, g.L[2]) * g.inv_d[2], g.scheme);
-        const double mass = p.w * inv_cell_volume;
-        for (int a = 0; a < taps; ++a) {
-          const int lx = static_cast<int>(s0.off0) - b0 + a;
-          for (int b = 0; b < taps; ++b) {
-            const int ly = static_cast<int>(s1.off0) - b1 + b;
-            const double wxy = s0.w[a] * s1.w[b];
-            for (int cc = 0; cc < taps; ++cc) {
-              const int lz = static_cast<int>(s2.off0) - b2 + cc;
-              atomicAdd(tile + (lx * e1 + ly) * e2 + lz, static_cast<R>(mass * (wxy * s2.w[cc])));
-            }
-          }
+        const int lx = static_cast<int>(s0.off0) - b0, ly = static_cast<int>(s1.off0) - b1,
+                  lz = static_cast<int>(s2.off0) - b2;
+        if (lx != cx || ly != cy || lz != cz) {
+          if (cx != INT_MIN) tileFlush<R, kTaps>(tile, e1, e2, cx, cy, cz, acc);
+#pragma unroll
+          for (int t = 0; t < kTaps * kTaps * kTaps; ++t) acc[t] = R(0);
+          cx = lx;
+          cy = ly;
+          cz = lz;
         }
+        const double mass = p.w * inv_cell_volume;
+#pragma unroll
+        for (int a = 0; a < kTaps; ++a)
+#pragma unroll
+          for (int b = 0; b < kTaps; ++b) {
+            const double wxy = s0.w[a] * s1.w[b];
+#pragma unroll
+            for (int c = 0; c < kTaps; ++c) acc[(a * kTaps + b) * kTaps + c] += static_cast<R>(mass * (wxy * s2.w[c]));
+          }
       }
+      if (cx != INT_MIN) tileFlush<R, kTaps>(tile, e1, e2, cx, cy, cz, acc);
       __syncthreads();
       for (int t = threadIdx.x; t < tc; t += blockDim.x) {
         const R v = tile[t];
@@ -226,13 +258,13 @@ __global__ void __launch_bounds__(256) depositTiledKernel(int64_t n, const doubl
         const Stencil s1 = makeStencil(wrapPosition(p.y, g.L[1]) * g.inv_d[1], g.scheme);
         const Stencil s2 = makeStencil(wrapPosition(p.z, g.L[2]) * g.inv_d[2], g.scheme);
         const double mass = p.w * inv_cell_volume;
-        for (int a = 0; a < taps; ++a) {
+        for (int a = 0; a < kTaps; ++a) {
           const int64_t ix = wrapIndex(s0.off0 + a, g.n[0]);
-          for (int b = 0; b < taps; ++b) {
+          for (int b = 0; b < kTaps; ++b) {
             const int64_t iy = wrapIndex(s1.off0 + b, g.n[1]);
             const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
             const double wxy = s0.w[a] * s1.w[b];
-            for (int cc = 0; cc < taps; ++cc) {
+            for (int cc = 0; cc < kTaps; ++cc) {
               const int64_t iz = wrapIndex(s2.off0 + cc, g.n[2]);
               atomicAdd(grid + row + iz, static_cast<R>(mass * (wxy * s2.w[cc])));
             }
@@ -241,6 +273,18 @@ __global__ void __launch_bounds__(256) depositTiledKernel(int64_t n, const doubl
       }
     }
     __syncthreads();
+  }
+}
+
+template <class R>
+void launchDepositTiled(int64_t n, const double4* src, double inv_cell_volume, const PmGeom& g, R* grid,
+                        cudaStream_t s) {
+  const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((n + kDepositChunk - 1) / kDepositChunk, 148 * 8));
+  noteLaunch();
+  if (g.scheme == 0) {
+    depositTiledKernel<R, 2><<<blocks, 256, 0, s>>>(n, src, inv_cell_volume, g, grid);
+  } else {
+    depositTiledKernel<R, 3><<<blocks, 256, 0, s>>>(n, src, inv_cell_volume, g, grid);
   }
 }
 
@@ -653,16 +697,14 @@ int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const dou
     { noteLaunch(); fillKernel<float><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<float>(), padded,
                                                                static_cast<float>(-mean)); }
     if (n > 0 && tree_sources)
-      { noteLaunch(); depositTiledKernel<float><<<static_cast<unsigned>(std::min<int64_t>((n + kDepositChunk - 1) / kDepositChunk, 148 * 8)), 256, 0, s>>>(
-          n, tree_sources, 1.0 / cell_volume, g, c.grid[0].as<float>()); }
+      launchDepositTiled<float>(n, tree_sources, 1.0 / cell_volume, g, c.grid[0].as<float>(), s);
     else if (n > 0)
       { noteLaunch(); depositKernel<float><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
                                                                1.0 / cell_volume, g, c.grid[0].as<float>()); }
   } else {
     { noteLaunch(); fillKernel<double><<<gridFor(padded, block), block, 0, s>>>(c.grid[0].as<double>(), padded, -mean); }
     if (n > 0 && tree_sources)
-      { noteLaunch(); depositTiledKernel<double><<<static_cast<unsigned>(std::min<int64_t>((n + kDepositChunk - 1) / kDepositChunk, 148 * 8)), 256, 0, s>>>(
-          n, tree_sources, 1.0 / cell_volume, g, c.grid[0].as<double>()); }
+      launchDepositTiled<double>(n, tree_sources, 1.0 / cell_volume, g, c.grid[0].as<double>(), s);
     else if (n > 0)
       { noteLaunch(); depositKernel<double><<<gridFor(n, block), block, 0, s>>>(n, x, y, z, m, uniform_mass,
                                                                 1.0 / cell_volume, g, c.grid[0].as<double>()); }
