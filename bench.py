@@ -42,6 +42,8 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     "clustered256": dict(n_side=256, box=200.0, halo_fraction=0.5, n_halos=2000, mass_decades=3.0,
                          lattice_rms=0.5, mesh=256, theta=0.6, leaf=16, eps=0.001),
+    "clustered512": dict(n_side=512, box=500.0, halo_fraction=0.6, n_halos=20000, mass_decades=4.0,
+                         lattice_rms=0.5, mesh=512, theta=0.7, leaf=32, eps=0.001),
     "clustered128": dict(n_side=128, box=100.0, halo_fraction=0.4, n_halos=300, mass_decades=3.0,
                          lattice_rms=0.5, mesh=128, theta=0.5, leaf=16, eps=0.001),
     "lattice32": dict(n_side=32, box=10.0, halo_fraction=0.0, n_halos=0, mass_decades=0.0,
@@ -222,11 +224,22 @@ def vjp_vs_force(torch, solver, t) -> dict:
             "vjp_phases_ms": {k: st[k] for k in ("pm_ms", "tree_build_ms", "walk_ms", "total_ms")}}
 
 
-def timed_steps(torch, solver, t, acc, factors, steps, warmup):
+def max_over_ranks(torch, dist, value: float, device) -> float:
+    """The largest value over all ranks (the job's time is its slowest rank's)."""
+    if dist is None:
+        return value
+    tt = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def timed_steps(torch, solver, t, acc, factors, steps, warmup, dist=None):
     stream = torch.cuda.current_stream().cuda_stream
     for _ in range(warmup):
         acc = gpu_step(solver, t, acc, factors, stream)
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     launches = 0
@@ -241,6 +254,8 @@ def timed_steps(torch, solver, t, acc, factors, steps, warmup):
         launches += st["kernel_launches"] + 3  # + kick, drift, kick
     e1.record()
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     return e0.elapsed_time(e1), acc, stats, launches
 
 
@@ -292,11 +307,8 @@ def run_gpu(args) -> int:
 
     # headline: mixed precision, device-resident inputs
     with ClockSampler(local) as clocks:
-        ms, acc, stats, launches = timed_steps(torch, mixed, t, r_m, factors, args.steps, args.warmup)
-    if dist is not None:
-        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+        ms, acc, stats, launches = timed_steps(torch, mixed, t, r_m, factors, args.steps, args.warmup, dist)
+    ms = max_over_ranks(torch, dist, ms, dev)
     value = n * args.steps * world / (ms * 1e-3)
 
     # end to end through the C-ABI with pinned host buffers
@@ -312,11 +324,7 @@ def run_gpu(args) -> int:
         mixed.solve_active_set(hx, hy, hz, hm)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - w0
-    e2e_value = n * e2e_steps / e2e_s
-    if dist is not None:
-        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_value = n * e2e_steps * world / float(tt.item())
+    e2e_value = n * e2e_steps * world / max_over_ranks(torch, dist, e2e_s, dev)
 
     # roofline of the dominant kernel (residual walk, FP32 pipes)
     peak = ct.probe_fp32_peak_tflops(local)
@@ -473,6 +481,92 @@ def run_reference(args) -> int:
     return 0
 
 
+def run_large(args) -> int:
+    """The large configuration (default clustered512: 512^3 = 134M particles,
+    L = 500, 60 % in 20000 halos over 4 decades, mesh 512^3, theta 0.7, leaf
+    32): one production force, the traversal counters (per-node walk), the
+    mixed-vs-FP64 force error on a seeded 1/256 target subset, and the adjoint
+    of one KDK step (forward, then the gradient of sum(w . x_1) with respect
+    to the initial positions). Prints one JSON record (not the headline)."""
+    import torch
+    import chui_treepm as ct
+    from chui_treepm import adjoint
+    w = WORKLOADS[args.workload]
+    dev = torch.device("cuda", 0)
+    t0 = time.time()
+    x, y, z, m, vx, vy, vz = make_particles(w, seed=42)
+    n = len(x)
+    log(f"particles {n} generated in {time.time() - t0:.1f}s")
+    t = {k: torch.tensor(v, device=dev) for k, v in dict(x=x, y=y, z=z, m=m, vx=vx, vy=vy, vz=vz).items()}
+    del x, y, z, vx, vy, vz
+    rec = {"workload": args.workload, "particles": n, "config": w}
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    with ct.TreePmCoordinator(make_config(w, ct._abi.MIXED, 0, diagnostics=0)) as s:
+        s.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+        r, ms = timed(lambda: s.solve_active_set(t["x"], t["y"], t["z"], t["m"]))
+        st = dict(s.last_stats)
+        rec["force"] = {"ms": ms, "particle_forces_per_s": n / (ms * 1e-3),
+                        "phases_ms": {k: st[k] for k in ("pm_ms", "tree_build_ms", "walk_ms", "total_ms")}}
+        rng = np.random.default_rng(7)
+        sub = np.sort(rng.choice(n, n // 256, replace=False)).astype(np.uint32)
+        mixed_sub = np.stack([r[k].cpu().numpy()[sub] for k in ("ax", "ay", "az")])
+        del r
+        # PM algorithmic bytes (deposit 24N + 8M, R2C + 3 C2R, Green 32 Mc, interpolation 24N + 12M + 12N)
+        mesh = w["mesh"]
+        cells = mesh ** 3
+        mc = mesh * mesh * (mesh // 2 + 1)
+        pm_bytes = (24 * n + 8 * cells) + 4 * (4 * cells + 8 * mc) + 32 * mc
+        rec["pm_refresh_effective_gbs"] = pm_bytes / (st["pm_ms"] * 1e-3) / 1e9
+    torch.cuda.empty_cache()
+    with ct.TreePmCoordinator(make_config(w, ct._abi.MIXED, 0, diagnostics=1)) as s:
+        s.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+        c = dict(s.last_stats)
+        rec["counters"] = {k: c[k] for k in ("direct_pair_evaluations", "visited_nodes",
+                                             "accepted_internal_multipoles", "node_count", "maximum_depth")}
+        flops = (FLOPS_PER_PAIR * c["direct_pair_evaluations"] + FLOPS_PER_MULTIPOLE *
+                 c["accepted_internal_multipoles"] + FLOPS_PER_VISIT * c["visited_nodes"])
+        rec["walk_achieved_tflops"] = flops / (rec["force"]["phases_ms"]["walk_ms"] * 1e-3) / 1e12
+        rec["walk_fraction_of_fp32_peak"] = rec["walk_achieved_tflops"] / ct.probe_fp32_peak_tflops(0)
+    torch.cuda.empty_cache()
+    with ct.TreePmCoordinator(make_config(w, ct._abi.FP64, 0, diagnostics=1)) as s:
+        sub_t = torch.tensor(sub.astype(np.int64), device=dev)
+        r, ms64 = timed(lambda: s.solve_active_set(t["x"], t["y"], t["z"], t["m"], active=sub_t))
+        ref = np.stack([r[k].cpu().numpy() for k in ("ax", "ay", "az")])
+        e = rel_errors(mixed_sub, ref)
+        rec["accuracy_vs_fp64_subset"] = {"targets": int(len(sub)), "median_rel": float(np.median(e)),
+                                          "p99_rel": float(np.percentile(e, 99)), "max_rel": float(np.max(e)),
+                                          "fp64_subset_ms": ms64}
+        del r
+    torch.cuda.empty_cache()
+    # adjoint of one KDK step
+    with ct.TreePmCoordinator(make_config(w, ct._abi.MIXED, 0, diagnostics=0)) as s:
+        g = torch.Generator(device="cpu").manual_seed(3)
+        wts = [torch.randn(n, generator=g, dtype=torch.float64).to(dev) for _ in range(3)]
+        pos = [t[k].clone().requires_grad_(True) for k in ("x", "y", "z")]
+
+        def fwd():
+            out = adjoint.kdk(s, *pos, t["vx"], t["vy"], t["vz"], t["m"], 1, args.dt)
+            return sum((out[k] * wts[k]).sum() for k in range(3))
+
+        loss, fwd_ms = timed(fwd)
+        _, bwd_ms = timed(lambda: loss.backward())
+        gnorm = float(sum((p.grad ** 2).sum() for p in pos).sqrt())
+        rec["adjoint_one_kdk_step"] = {"forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                                       "backward_over_forward": bwd_ms / fwd_ms, "grad_norm": gnorm,
+                                       "finite": bool(np.isfinite(gnorm))}
+    print(json.dumps(rec), flush=True)
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -484,10 +578,14 @@ def main() -> int:
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile"])
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "large"])
     args = ap.parse_args()
     if args.mode == "profile":
         return run_profile(args)
+    if args.mode == "large":
+        if args.workload == "clustered256":
+            args.workload = "clustered512"
+        return run_large(args)
     if args.impl == "reference":
         args.steps = min(args.steps, 1) if args.workload == "clustered256" else args.steps
         args.warmup = 0 if args.workload == "clustered256" else args.warmup
