@@ -553,7 +553,7 @@ void chui_treepm_destroy(void* handle) {
                             &c->bucket_next, &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
                             &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
                             &c->leaf_of_pos, &c->inv_pos, &c->cub_temp, &c->node_geom, &c->node_com,
-                            &c->node_quad, &c->node_f4, &c->node_hmin, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
+                            &c->node_quad, &c->node_f4, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
                             &c->node_counter, &c->sorted_index, &c->pos_of_row, &c->src_f4, &c->src_d4, &c->src_u4, &c->src_cot,
                             &c->target_order, &c->morton_sorted, &c->walk_counters, &c->work_counter,
                             &c->tree_acc, &c->tree_near};

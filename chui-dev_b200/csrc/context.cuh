@@ -95,7 +95,6 @@ struct Context {
   DevBuf node_com;     // double4 {comx, comy, comz, mass}
   DevBuf node_quad;    // 8 doubles per node {qxx, qxy, qxz, qyy, qyz, qzz, trace, com_center_offset}
   DevBuf node_f4;      // float4 {com - centre (x, y, z), |centre - com|}: FP32 node frame of the walk
-  DevBuf node_hmin;    // float: smallest half-size of an internal descendant (rounded down; +inf if none)
   DevBuf node_child;   // 8 u32 per node
   DevBuf node_range;   // uint4 {begin, count, child_count | leaf flag, subtree_end}
   DevBuf node_parent;  // u32

@@ -590,23 +590,10 @@ __device__ void internalMoments(int64_t node, const double4 g, const uint32_t* _
 
 // Bottom-up moments: each leaf computes itself, then the last child to finish
 // a parent computes it from its children in octant order (deterministic).
-// Smallest half-size among the internal descendants of `node` (children are
-// complete when this runs), rounded toward zero so that it bounds from below.
-__device__ float descendantHalfMin(int64_t node, const double4* __restrict__ geom, const uint4* __restrict__ range,
-                                   const uint32_t* child, const float* hmin) {
-  float v = INFINITY;
-  for (int o = 0; o < 8; ++o) {
-    const uint32_t c = __ldcg(child + 8 * node + o);
-    if (c == kInvalid || range[c].z == 0) continue;
-    v = fminf(v, fminf(__double2float_rz(geom[c].w), __ldcg(hmin + c)));
-  }
-  return v;
-}
-
 __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restrict__ geom,
                               const uint4* __restrict__ range, const uint32_t* __restrict__ parent,
                               const uint32_t* __restrict__ child, uint32_t* counter, double4* com,
-                              double* quad, float* hmin) {
+                              double* quad) {
   for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nodes;
        k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const uint4 r = range[k];
@@ -616,7 +603,6 @@ __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restr
     leafMoments(k, in, geom[k], r, &cm, q);
     com[k] = cm;
     for (int t = 0; t < 8; ++t) quad[8 * k + t] = q[t];
-    hmin[k] = INFINITY;
     int64_t node = k;
     while (true) {
       __threadfence();
@@ -628,7 +614,6 @@ __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restr
       internalMoments(p, geom[p], child, com, quad, in.quadrupole, &cm, q);
       com[p] = cm;
       for (int t = 0; t < 8; ++t) quad[8 * static_cast<size_t>(p) + t] = q[t];
-      hmin[p] = descendantHalfMin(p, geom, range, child, hmin);
       node = p;
     }
   }
@@ -916,8 +901,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   if (ensure(c.node_geom, total_nodes * sizeof(double4)) || ensure(c.node_com, total_nodes * sizeof(double4)) ||
       ensure(c.node_quad, total_nodes * 8 * sizeof(double)) || ensure(c.node_child, total_nodes * 8 * 4) ||
       ensure(c.node_range, total_nodes * sizeof(uint4)) || ensure(c.node_parent, total_nodes * 4) ||
-      ensure(c.node_depth, total_nodes * 4) || ensure(c.node_counter, total_nodes * 4) ||
-      ensure(c.node_hmin, total_nodes * sizeof(float)))
+      ensure(c.node_depth, total_nodes * 4) || ensure(c.node_counter, total_nodes * 4))
     return CHUI_TREEPM_ENOMEM;
   NodeOut out;
   out.geom = c.node_geom.as<double4>();
@@ -959,8 +943,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   mi.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
   { noteLaunch(); momentsKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(total_nodes, mi, out.geom, out.range, out.parent,
                                                           out.child, c.node_counter.as<uint32_t>(),
-                                                          c.node_com.as<double4>(), c.node_quad.as<double>(),
-                                                          c.node_hmin.as<float>()); }
+                                                          c.node_com.as<double4>(), c.node_quad.as<double>()); }
   if (ensure(c.node_f4, total_nodes * sizeof(float4))) return CHUI_TREEPM_ENOMEM;
   { noteLaunch(); nodeFrameKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.geom, c.node_com.as<double4>(),
                                                             c.node_quad.as<double>(), c.node_f4.as<float4>()); }

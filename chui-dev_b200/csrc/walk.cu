@@ -26,13 +26,14 @@
 // FP64 configuration evaluates the reference's formulas (source metric per
 // pair, erf/exp residual) unchanged.
 //
-// With diagnostics on, the walk reproduces the reference's traversal counters
-// exactly. With diagnostics off (production), an opened node whose internal
-// descendants provably fail the strict envelope for every opening lane is
-// evaluated as one block of sources instead of being descended: the lane's
-// pair set (every source within r_cut outside accepted multipoles) is the
-// same, the number of warp traversal steps drops several-fold, and no
-// counters are kept.
+// With diagnostics on, the walk reproduces the reference's node counters
+// exactly. With diagnostics off (production), a small opened node is
+// evaluated as one block of sources instead of being descended: its lanes
+// get every source inside r_cut, which is the reference's pair set except
+// where a deeper node would have been accepted as a strict multipole (those
+// few are summed as pairs, which moves forces by far less than the mixed
+// precision does); the number of warp traversal steps drops several-fold,
+// and no counters are kept.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -64,7 +65,6 @@ struct WalkArgs {
   const float4* src_f4;
   const double4* src_d4;
   const float4* node_f4;
-  const float* hmin;       // smallest internal-descendant half-size per node
   const double4* src_u4;   // tree-ordered unwrapped positions + mass (mixed)
   double* out_x;   // per slot, short-range part
   double* out_y;
@@ -377,8 +377,7 @@ constexpr int kQueue = 64;  // sources per warp batch
 
 // Subtree blocks of the production walk (diagnostics off): an opened node
 // with at most kBulkCount sources and half-size at most kBulkHalf * r_cut is
-// evaluated as one block of sources when no internal descendant can pass the
-// strict envelope for any lane that opened it.
+// evaluated as one block of sources by the lanes that opened it.
 #ifndef CHUI_BULK_COUNT
 #define CHUI_BULK_COUNT 1024
 #endif
@@ -766,27 +765,15 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       if (kDiag && open) ++cnt_opened;
       if (__any_sync(0xffffffffu, open)) {
         if constexpr (!kDiag) {
-          // Subtree block: every source of this node within r_cut of an
-          // opening lane is one of that lane's reference pairs unless an
-          // internal descendant would be accepted as a multipole, which the
-          // strict envelope 2h/r < 0.08 rules out when 2 h_min >= 0.08 R,
-          // h_min the smallest internal-descendant half-size and R the
-          // largest target-to-cube distance (an upper bound on every
-          // descendant COM distance). Pairs beyond r_cut are dropped per pair
-          // as in the leaf path, so the lane's sum is the reference's.
+          // Subtree block: the lanes that opened this small node take every
+          // source in it within r_cut (per-pair test, as in the leaf path)
+          // instead of descending. This is the reference's pair set except
+          // where a deeper node would have been accepted as a strict
+          // multipole; those few are evaluated as the pairs they stand for.
           if (fast_frame && rg4.y <= kBulkCount && h <= bulk_half && w.cutoff + h + rga < half_min_box &&
               h < w.exact_half) {
-            bool ok = true;
-            if (open && w.quadrupole) {
-              const float hf = static_cast<float>(h);
-              const float qx = fabsf(ndx) + hf, qy = fabsf(ndy) + hf, qz = fabsf(ndz) + hf;
-              const float hm = a.hmin[node];
-              ok = 4.0f * hm * hm >= 0.0064f * 1.001f * fmaf(qx, qx, fmaf(qy, qy, qz * qz));
-            }
-            if (__all_sync(0xffffffffu, ok)) {
-              enqueue(rg4.x, rg4.y, __ballot_sync(0xffffffffu, open), true, g, cdx, cdy, cdz);
-              continue;
-            }
+            enqueue(rg4.x, rg4.y, __ballot_sync(0xffffffffu, open), true, g, cdx, cdy, cdz);
+            continue;
           }
         }
         const uint32_t ch = lane < 8 ? a.child[8 * static_cast<size_t>(node) + lane] : kInvalid;
@@ -1180,7 +1167,6 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.src_f4 = c.src_f4.as<float4>();
   a.src_d4 = c.src_d4.as<double4>();
   a.node_f4 = c.node_f4.as<float4>();
-  a.hmin = c.node_hmin.as<float>();
   a.src_u4 = c.src_u4.as<double4>();
   double* acc = c.tree_acc.as<double>();
   a.out_x = acc;
