@@ -390,28 +390,17 @@ constexpr int kQueue = 64;  // sources per warp batch
 constexpr uint32_t kBulkCount = CHUI_BULK_COUNT;
 constexpr double kBulkHalf = CHUI_BULK_HALF;
 
-// H(t) in Estrin form: same polynomial as polyHFixed<12>, dependency depth 5.
-__device__ __forceinline__ float polyH12(const PolyH& p, float t) {
-  const float s = fmaf(t, p.scale, -1.0f);
-  const float s2 = s * s;
-  const float s4 = s2 * s2;
-  const float s8 = s4 * s4;
-  const float a0 = fmaf(p.c[1], s, p.c[0]);
-  const float a1 = fmaf(p.c[3], s, p.c[2]);
-  const float a2 = fmaf(p.c[5], s, p.c[4]);
-  const float a3 = fmaf(p.c[7], s, p.c[6]);
-  const float a4 = fmaf(p.c[9], s, p.c[8]);
-  const float a5 = fmaf(p.c[11], s, p.c[10]);
-  const float b0 = fmaf(a1, s2, a0);
-  const float b1 = fmaf(a3, s2, a2);
-  const float b2 = fmaf(a5, s2, a4);
-  return fmaf(b2, s8, fmaf(b1, s4, b0));
-}
-
+// The fitted polynomial at t = r^2 / (4 r_s^2), straight from r^2: s =
+// r^2 * sc - 1 with sc = scale / (4 r_s^2), then Horner (kTerms - 1 FMAs).
+// The walk is issue-bound, so the fewest instructions win over a shorter
+// dependency chain (the unrolled queue loop supplies the parallelism).
 template <int kTerms>
-__device__ __forceinline__ float evalH(const PolyH& p, float t) {
-  if constexpr (kTerms == 12) return polyH12(p, t);
-  return polyHFixed<kTerms>(p, t);
+__device__ __forceinline__ float hornerR2(const PolyH& p, float r2, float sc) {
+  const float s = fmaf(r2, sc, -1.0f);
+  float h = p.c[kTerms - 1];
+#pragma unroll
+  for (int k = kTerms - 2; k >= 0; --k) h = fmaf(h, s, p.c[k]);
+  return h;
 }
 
 // Exact (FP64, reference formulas) decision for one lane at one node: prune,
@@ -525,6 +514,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   const float env2 = 0.0064f;  // 0.08^2
   const float theta2 = static_cast<float>(w.theta * w.theta);
   const double bulk_half = kBulkHalf * w.cutoff;
+  const float sc_r2 = w.inv_4rs2_f * a.poly.scale;
 
   while (true) {
     uint32_t cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0, cnt_skips = 0,
@@ -580,7 +570,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     auto flush = [&]() {
       float fx = 0.f, fy = 0.f, fz = 0.f;
       uint32_t pairs = 0, skips = 0;
-#pragma unroll 2
+#pragma unroll 4
       for (int k = 0; k < qn; ++k) {
         const float4 e = q_src[warp][k];
         const uint2 meta = q_meta[warp][k];
@@ -593,7 +583,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
           skips += (mine && !in) ? 1u : 0u;
           nearest_f = in ? fminf(nearest_f, r2) : nearest_f;
         }
-        const float hh = evalH<kTerms>(a.poly, r2 * w.inv_4rs2_f);
+        const float hh = hornerR2<kTerms>(a.poly, r2, sc_r2);
         const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
         const float rinv = rsqrtf(s2);
         const float k3 = fmaf(-hh, w.inv_8rs3_f, rinv * rinv * rinv);
@@ -937,9 +927,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpA
         const bool in = valid && r2 <= cut2 && r2 > Real(0);
         Real K, Kp;
         if constexpr (sizeof(Real) == 4) {
-          const float t = r2 * w.inv_4rs2_f;
-          const float hh = evalH<kTerms>(a.poly, t);
-          const float hp = polyHFixed<kTerms>(a.dpoly, t);
+          const float hh = hornerR2<kTerms>(a.poly, r2, w.inv_4rs2_f * a.poly.scale);
+          const float hp = hornerR2<kTerms>(a.dpoly, r2, w.inv_4rs2_f * a.dpoly.scale);
           const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
           const float rinv = rsqrtf(s2);
           const float rinv2 = rinv * rinv;
