@@ -587,7 +587,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
         const float rinv = rsqrtf(s2);
         const float k3 = fmaf(-hh, w.inv_8rs3_f, rinv * rinv * rinv);
-        const float f = (in && r2 > 0.f) ? e.w * k3 : 0.f;
+        // coincident sources contribute nothing: with eps > 0 the kernel is
+        // finite there and d = 0; with eps = 0 the zero-distance test avoids inf * 0
+        const float f = (kEpsZero ? (in && r2 > 0.f) : in) ? e.w * k3 : 0.f;
         fx = fmaf(f, dx, fx);
         fy = fmaf(f, dy, fy);
         fz = fmaf(f, dz, fz);
