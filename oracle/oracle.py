@@ -29,6 +29,13 @@ class Params(C.Structure):
         ("deconvolution", C.c_int32),
         ("criterion", C.c_int32),
         ("quadrupole", C.c_int32),
+        ("policy", C.c_int32),
+        ("estimator", C.c_int32),
+        ("cutoff_policy", C.c_int32),
+        ("reserved", C.c_int32),
+        ("adaptive_angle", C.c_double),
+        ("rel_tol", C.c_double),
+        ("accel_floor", C.c_double),
     ]
 
 
@@ -38,7 +45,11 @@ class Counters(C.Structure):
 
 
 def make_params(box=(1.0, 1.0, 1.0), mesh=(16, 16, 16), asmth=1.25, rcut=6.25, theta=0.5, g=1.0,
-                eps=0.0, leaf=16, scheme=0, deconv=0, criterion=1, quadrupole=1) -> Params:
+                eps=0.0, leaf=16, scheme=0, deconv=0, criterion=1, quadrupole=1, policy=0, estimator=0,
+                cutoff_policy=0, adaptive_angle=0.25, rel_tol=0.005, accel_floor=1e-30) -> Params:
+    """Defaults are TreePmOptions' (include/cosmosim/gravity/tree_pm_coupling.hpp:243-332):
+    strict-reference policy; the adaptive fields apply with policy=1 (estimator 0 residual
+    derivative / 1 relative monopole, cutoff_policy 0 contain node / 1 COM distance)."""
     p = Params()
     p.box = (C.c_double * 3)(*box)
     p.mesh = (C.c_int64 * 3)(*mesh)
@@ -52,6 +63,12 @@ def make_params(box=(1.0, 1.0, 1.0), mesh=(16, 16, 16), asmth=1.25, rcut=6.25, t
     p.deconvolution = deconv
     p.criterion = criterion
     p.quadrupole = quadrupole
+    p.policy = policy
+    p.estimator = estimator
+    p.cutoff_policy = cutoff_policy
+    p.adaptive_angle = adaptive_angle
+    p.rel_tol = rel_tol
+    p.accel_floor = accel_floor
     return p
 
 
@@ -71,6 +88,7 @@ def lib():
         L = C.CDLL(LIB_PATH)
         dp = C.POINTER(C.c_double)
         L.oracle_treepm_solve.restype = C.c_int
+        L.oracle_treepm_solve2.restype = C.c_int
         L.oracle_tree_build.restype = C.c_void_p
         L.oracle_tree_build.argtypes = [C.c_int64, dp, dp, dp, dp, C.POINTER(Params), C.POINTER(C.c_int)]
         L.oracle_tree_node_count.restype = C.c_int64
@@ -99,17 +117,22 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
-def treepm_solve(x, y, z, m, params: Params, active=None) -> dict:
+def treepm_solve(x, y, z, m, params: Params, active=None, prev_acc=None) -> dict:
+    """prev_acc: per active target |a_previous| (the acceleration history of the
+    relative criteria), or None for no history."""
     x, y, z, m = _f64(x), _f64(y), _f64(z), _f64(m)
     n = len(x)
     act = None if active is None else np.ascontiguousarray(active, dtype=np.uint32)
     na = n if act is None else len(act)
+    prev = None if prev_acc is None else _f64(prev_acc)
+    if prev is not None and len(prev) != na:
+        raise ValueError("prev_acc needs one entry per active target")
     out = {k: np.zeros(na) for k in ("ax", "ay", "az", "pm_ax", "pm_ay", "pm_az",
                                       "tree_ax", "tree_ay", "tree_az", "nearest_r2")}
     cnt = Counters()
-    rc = lib().oracle_treepm_solve(
+    rc = lib().oracle_treepm_solve2(
         C.c_int64(n), _p(x), _p(y), _p(z), _p(m), C.c_int64(na),
-        None if act is None else _p(act, C.c_uint32), C.byref(params),
+        None if act is None else _p(act, C.c_uint32), C.byref(params), None if prev is None else _p(prev),
         *[_p(out[k]) for k in ("ax", "ay", "az", "pm_ax", "pm_ay", "pm_az",
                                "tree_ax", "tree_ay", "tree_az", "nearest_r2")],
         C.byref(cnt))

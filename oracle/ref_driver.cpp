@@ -99,6 +99,10 @@ struct Problem {
   double drift = 0, kick1 = 0, kick2 = 0, drag1 = 1, drag2 = 1;
   std::vector<double> x, y, z, m, vx, vy, vz;
   std::vector<std::uint32_t> active;
+  // optional trailing "CHUIADP1" block: acceptance policy and acceleration history
+  std::int64_t policy = 0, estimator = 0, cutoff_policy = 0, has_prev = 0;
+  double adaptive_angle = 0.25, rel_tol = 0.005, accel_floor = 1.0e-30;
+  std::vector<double> prev;
 };
 
 Problem readProblem(const char* path) {
@@ -144,6 +148,18 @@ Problem readProblem(const char* path) {
   p.vy = r.vec<double>(n);
   p.vz = r.vec<double>(n);
   p.active = r.vec<std::uint32_t>(static_cast<std::size_t>(p.n_active));
+  char tail[8];
+  if (std::fread(tail, 1, 8, f) == 8) {
+    if (std::memcmp(tail, "CHUIADP1", 8) != 0) throw std::runtime_error("bad trailing block");
+    p.policy = r.get<std::int64_t>();
+    p.estimator = r.get<std::int64_t>();
+    p.cutoff_policy = r.get<std::int64_t>();
+    p.has_prev = r.get<std::int64_t>();
+    p.adaptive_angle = r.get<double>();
+    p.rel_tol = r.get<double>();
+    p.accel_floor = r.get<double>();
+    if (p.has_prev) p.prev = r.vec<double>(static_cast<std::size_t>(p.n_active ? p.n_active : p.n));
+  }
   std::fclose(f);
   return p;
 }
@@ -166,7 +182,15 @@ cg::TreePmOptions makeOptions(const Problem& p) {
   o.tree_options.multipole_order = p.order == 0 ? cg::TreeMultipoleOrder::kMonopole : cg::TreeMultipoleOrder::kQuadrupole;
   o.tree_options.max_leaf_size = static_cast<std::size_t>(p.leaf);
   o.tree_options.softening.epsilon_comoving = p.eps;
-  o.acceptance_policy = cg::TreePmAcceptancePolicy::kStrictReference;
+  o.tree_options.relative_force_tolerance = p.rel_tol;
+  o.tree_options.relative_force_acceleration_floor_code = p.accel_floor;
+  o.acceptance_policy = p.policy == 1 ? cg::TreePmAcceptancePolicy::kAdaptiveRelative
+                                      : cg::TreePmAcceptancePolicy::kStrictReference;
+  o.adaptive_maximum_opening_angle = p.adaptive_angle;
+  o.adaptive_error_estimator = p.estimator == 1 ? cg::TreePmAdaptiveErrorEstimator::kRelativeMonopole
+                                                : cg::TreePmAdaptiveErrorEstimator::kResidualDerivative;
+  o.cutoff_node_policy = p.cutoff_policy == 1 ? cg::TreePmCutoffNodePolicy::kComDistance
+                                              : cg::TreePmCutoffNodePolicy::kContainNode;
   o.split_policy = cg::makeTreePmSplitPolicyFromMeshSpacing(
       p.asmth, p.rcut,
       std::cbrt((p.box[0] / static_cast<double>(p.mesh[0])) * (p.box[1] / static_cast<double>(p.mesh[1])) *
@@ -202,6 +226,7 @@ int main(int argc, char** argv) {
     acc.short_range_accel_y_comoving = sy;
     acc.short_range_accel_z_comoving = sz;
     acc.short_range_nearest_pair_r2_comoving = nearest;
+    if (p.has_prev) acc.previous_acceleration_magnitude_code = p.prev;
 
     cg::TreePmProfileEvent profile{};
     cg::TreePmDiagnostics diagnostics{};

@@ -52,6 +52,14 @@ class RefProblem:
     vx: np.ndarray | None = None
     vy: np.ndarray | None = None
     vz: np.ndarray | None = None
+    # acceptance policy (TreePmOptions): 0 strict reference, 1 adaptive relative
+    policy: int = 0
+    estimator: int = 0       # adaptive: 0 residual derivative, 1 relative monopole
+    cutoff_policy: int = 0   # adaptive: 0 contain node, 1 COM distance
+    adaptive_angle: float = 0.25
+    rel_tol: float = 0.005
+    accel_floor: float = 1e-30
+    prev_acc: np.ndarray | None = None  # per active target |a_previous|
 
 
 def write_problem(path: str, p: RefProblem) -> None:
@@ -73,6 +81,15 @@ def write_problem(path: str, p: RefProblem) -> None:
                   p.vz if p.vz is not None else zeros):
             f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
         f.write(active.tobytes())
+        if p.policy or p.prev_acc is not None or p.rel_tol != 0.005 or p.accel_floor != 1e-30:
+            f.write(b"CHUIADP1")
+            f.write(struct.pack("<4q", p.policy, p.estimator, p.cutoff_policy, int(p.prev_acc is not None)))
+            f.write(struct.pack("<3d", p.adaptive_angle, p.rel_tol, p.accel_floor))
+            if p.prev_acc is not None:
+                prev = np.ascontiguousarray(p.prev_acc, dtype=np.float64)
+                if len(prev) != (len(active) if len(active) else n):
+                    raise ValueError("prev_acc needs one entry per active target")
+                f.write(prev.tobytes())
 
 
 class _Buf:

@@ -747,41 +747,122 @@ static void multipole_force(const walk_ctx *w, uint32_t node, double dx, double 
   acc[2] += az;
 }
 
+static double com_center_offset(const oracle_tree *t, uint32_t node) {
+  const double ox = t->cx[node] - t->comx[node];
+  const double oy = t->cy[node] - t->comy[node];
+  const double oz = t->cz[node] - t->comz[node];
+  return sqrt(ox * ox + oy * oy + oz * oz);
+}
+
+/* acceptNodeByComDistanceMac, internal/tree_interaction_common.hpp:36-43 */
+static int com_distance_mac(double theta, double h, double off, double r2) {
+  const double r = sqrt(r2 + 1.0e-30);
+  return ((2.0 * h + off) / r) < theta;
+}
+
+/* passesSofteningEnvelopeGuard, internal/tree_interaction_common.hpp:77-89 */
+static int softening_ok(const oracle_tree *t, uint32_t node, double r, double eps_t) {
+  if (t->smax[node] - t->smin[node] <= 1.0e-12) return 1;
+  const double pe = t->smax[node] > eps_t ? t->smax[node] : eps_t;
+  return r > (2.0 * t->half[node] + 2.0 * pe);
+}
+
 /* Strict-reference acceptance, internal/tree_pm_acceptance.hpp:170-255 with
- * acceptNodeByMac / passesSofteningEnvelopeGuard of
- * internal/tree_interaction_common.hpp:36-89 (no acceleration history). */
+ * acceptNodeByMac (internal/tree_interaction_common.hpp:45-75): COM-distance
+ * or geometric MAC, or the relative-force criterion when the target has an
+ * acceleration history. */
 static int accept_strict(const walk_ctx *w, uint32_t node, int inside, int within, double r2,
-                         double eps_t) {
+                         double eps_t, int prev_avail, double prev_mag) {
   const oracle_tree *t = w->t;
   const double h = t->half[node];
   const double r = sqrt(r2 > 1.0e-30 ? r2 : 1.0e-30);
-  int soft_ok = 1;
-  if (!(t->smax[node] - t->smin[node] <= 1.0e-12)) {
-    const double pe = t->smax[node] > eps_t ? t->smax[node] : eps_t;
-    soft_ok = r > (2.0 * h + 2.0 * pe);
-  }
+  const int soft_ok = softening_ok(t, node, r, eps_t);
   const int envelope_ok = w->p->quadrupole && (2.0 * h / r) < 0.08;
   int mac_ok;
   if (inside) {
     mac_ok = 0;
   } else if (w->p->criterion == 0) {
     mac_ok = (2.0 * h / sqrt(r2 + 1.0e-30)) < w->p->theta;
+  } else if (w->p->criterion == 1 || !prev_avail) {
+    mac_ok = com_distance_mac(w->p->theta, h, com_center_offset(t, node), r2);
   } else {
-    const double ox = t->cx[node] - t->comx[node];
-    const double oy = t->cy[node] - t->comy[node];
-    const double oz = t->cz[node] - t->comz[node];
-    const double off = sqrt(ox * ox + oy * oy + oz * oz);
-    const double rr = sqrt(r2 + 1.0e-30);
-    mac_ok = ((2.0 * h + off) / rr) < w->p->theta;
+    const double scale = fabs(prev_mag) > w->p->accel_floor ? fabs(prev_mag) : w->p->accel_floor;
+    const double width = 2.0 * h;
+    const double estimated = w->p->G * t->mass[node] * width * width;
+    const double allowed = w->p->rel_tol * scale * r2 * r2;
+    mac_ok = estimated <= allowed;
   }
   return mac_ok && envelope_ok && soft_ok && within && !inside && isfinite(r2);
+}
+
+/* residualAccuracyProxy, internal/tree_pm_acceptance.hpp:20-51 (same order of
+ * operations: the proxy is compared with alpha |a_previous|). */
+static double residual_proxy(const walk_ctx *w, uint32_t node, double r2, double eps_t) {
+  const oracle_tree *t = w->t;
+  if (!(r2 > 0.0) || !isfinite(r2)) return INFINITY;
+  const double rs = w->rs;
+  const double r = sqrt(r2);
+  const double eps = t->smax[node] > eps_t ? t->smax[node] : eps_t;
+  const double d = r2 + eps * eps;
+  const double inv_d5 = 1.0 / (d * d * sqrt(d));
+  const double inv_r3 = 1.0 / (r2 * r);
+  const double inv_r4 = 1.0 / (r2 * r2);
+  const double long_factor = oracle_long_range_factor(r, rs);
+  const double q = r / (2.0 * rs);
+  const double exponential = exp(-q * q);
+  const double scale3 = rs * rs * rs;
+  const double s_first = -0.5 * k_inv_sqrt_pi * r2 * exponential / scale3;
+  const double s_second = k_inv_sqrt_pi * exponential * (-r / scale3 + 0.25 * r * r2 / (scale3 * rs * rs));
+  const double first = -3.0 * r * inv_d5 + s_first * inv_r3 - 3.0 * (-long_factor) * inv_r4;
+  const double second = -3.0 * inv_d5 + 15.0 * r2 * inv_d5 / d + s_second * inv_r3 - 6.0 * s_first * inv_r4 +
+                        12.0 * (-long_factor) * inv_r4 / r;
+  const double width = 2.0 * t->half[node];
+  const double rho = sqrt(3.0) * t->half[node] + com_center_offset(t, node);
+  const double a = width * width * inv_r4;
+  const double b = 0.5 * rho * rho * (3.0 * fabs(first) + fabs(r * second - first));
+  const double proxy = w->p->G * t->mass[node] * (a > b ? a : b);
+  return isfinite(proxy) && proxy >= 0.0 ? proxy : INFINITY;
+}
+
+/* Adaptive-relative acceptance, internal/tree_pm_acceptance.hpp:170-255:
+ * opening-angle envelope, then the relative monopole (or residual-derivative)
+ * estimate against alpha |a_previous|, or the COM-distance MAC without history. */
+static int accept_adaptive(const walk_ctx *w, uint32_t node, int inside, int within, double r2, double eps_t,
+                           int prev_avail, double prev_mag) {
+  const oracle_tree *t = w->t;
+  const double h = t->half[node];
+  const double r = sqrt(r2 > 1.0e-30 ? r2 : 1.0e-30);
+  const int soft_ok = softening_ok(t, node, r, eps_t);
+  const int envelope_ok = (2.0 * h / r) < w->p->adaptive_angle;
+  if (!envelope_ok || !soft_ok || inside || !within || !isfinite(r2)) return 0;
+  const int history_ok = prev_avail && isfinite(prev_mag) && prev_mag > w->p->accel_floor;
+  int mac_ok;
+  if (history_ok) {
+    const double allowance = w->p->rel_tol * prev_mag;
+    const double width = 2.0 * h;
+    const double inv_r4 = 1.0 / (r2 * r2);
+    const double lower = w->p->G * t->mass[node] * (width * width * inv_r4);
+    if (isfinite(allowance) && isfinite(lower) && lower > allowance) {
+      mac_ok = 0;
+    } else if (w->p->estimator == 1) {
+      mac_ok = isfinite(allowance) && isfinite(lower);
+    } else {
+      const double est = residual_proxy(w, node, r2, eps_t);
+      mac_ok = isfinite(est) && isfinite(allowance) && est <= allowance;
+    }
+  } else {
+    mac_ok = com_distance_mac(w->p->theta, h, com_center_offset(t, node), r2);
+  }
+  return mac_ok;
 }
 
 /* evaluateTargetAgainstLocalTree, tree_pm_coupling.cpp:4026-4272 (no lookup
  * tables, no SIMD staging: the reference defaults). */
 static void walk_target(const walk_ctx *w, double px, double py, double pz, uint32_t self,
-                        int skip_self, double eps_t, uint32_t *stack, size_t stack_cap,
-                        double out[4], oracle_counters *cnt) {
+                        int skip_self, double eps_t, int prev_avail, double prev_mag, uint32_t *stack,
+                        size_t stack_cap, double out[4], oracle_counters *cnt) {
+  const int adaptive = w->p->policy == 1;
+  const int com_cutoff = adaptive && w->p->cutoff_policy == 1;
   const oracle_tree *t = w->t;
   double acc[3] = {0.0, 0.0, 0.0};
   double nearest = INFINITY;
@@ -818,14 +899,21 @@ static void walk_target(const walk_ctx *w, double px, double py, double pz, uint
     int accept = is_leaf;
     double dx = 0.0, dy = 0.0, dz = 0.0;
     if (!is_leaf) {
-      const int inside = skip_self && ax_ <= h && ay_ <= h && az_ <= h;
+      /* the adaptive policy tests containment for every target (:4090-4092) */
+      const int inside = (skip_self || adaptive) && ax_ <= h && ay_ <= h && az_ <= h;
       const double mx = ax_ + h, my = ay_ + h, mz = az_ + h;
-      const int within = within_cutoff(mx * mx + my * my + mz * mz, w->cutoff, w->cutoff2);
+      const int within = com_cutoff || within_cutoff(mx * mx + my * my + mz * mz, w->cutoff, w->cutoff2);
       dx = metric_apply(nm[0], t->comx[node] - px);
       dy = metric_apply(nm[1], t->comy[node] - py);
       dz = metric_apply(nm[2], t->comz[node] - pz);
       const double r2 = dx * dx + dy * dy + dz * dz;
-      accept = accept_strict(w, node, inside, within, r2, eps_t);
+      accept = adaptive ? accept_adaptive(w, node, inside, within, r2, eps_t, prev_avail, prev_mag)
+                        : accept_strict(w, node, inside, within, r2, eps_t, prev_avail, prev_mag);
+      /* kComDistance: an accepted node whose COM lies beyond r_cut is pruned (:4129-4132) */
+      if (accept && com_cutoff && r2 > w->cutoff2) {
+        ++cnt->pruned;
+        continue;
+      }
     }
     if (accept) {
       ++cnt->accepted;
@@ -878,6 +966,16 @@ int oracle_treepm_solve(int64_t n, const double *x, const double *y, const doubl
                         double *pm_ax, double *pm_ay, double *pm_az, double *tree_ax,
                         double *tree_ay, double *tree_az, double *nearest_r2,
                         oracle_counters *counters) {
+  return oracle_treepm_solve2(n, x, y, z, m, n_active, active, p, NULL, ax, ay, az, pm_ax, pm_ay, pm_az,
+                              tree_ax, tree_ay, tree_az, nearest_r2, counters);
+}
+
+int oracle_treepm_solve2(int64_t n, const double *x, const double *y, const double *z,
+                         const double *m, int64_t n_active, const uint32_t *active,
+                         const oracle_params *p, const double *prev_acc, double *ax, double *ay,
+                         double *az, double *pm_ax, double *pm_ay, double *pm_az, double *tree_ax,
+                         double *tree_ay, double *tree_az, double *nearest_r2,
+                         oracle_counters *counters) {
   const int64_t na = active ? n_active : n;
   const double delta = oracle_mesh_spacing(p);
   const double rs = p->asmth_cells * delta;
@@ -985,7 +1083,10 @@ int oracle_treepm_solve(int64_t n, const double *x, const double *y, const doubl
     for (int64_t k = 0; k < na; ++k) {
       const uint32_t self = active ? active[k] : (uint32_t)k;
       double res[4];
-      walk_target(&w, tx[k], ty[k], tz[k], self, 1, p->epsilon, stack, stack_cap, res, &local);
+      /* history per active slot: present and finite (tree_pm_coupling.cpp:4467-4472) */
+      const int avail = prev_acc != NULL && isfinite(prev_acc[k]);
+      walk_target(&w, tx[k], ty[k], tz[k], self, 1, p->epsilon, avail, avail ? prev_acc[k] : 0.0, stack,
+                  stack_cap, res, &local);
       if (ax) ax[k] = lx[k] + res[0];
       if (ay) ay[k] = ly[k] + res[1];
       if (az) az[k] = lz[k] + res[2];

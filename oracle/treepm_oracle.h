@@ -30,6 +30,14 @@ typedef struct {
   int32_t deconvolution; /* assignment-window deconvolution on/off */
   int32_t criterion;     /* 0 geometric, 1 COM distance, 2 relative force */
   int32_t quadrupole;    /* 1 quadrupole multipoles, 0 monopole */
+  /* TreePmOptions acceptance policy (tree_pm_coupling.hpp:243-332) */
+  int32_t policy;        /* 0 strict reference, 1 adaptive relative */
+  int32_t estimator;     /* adaptive: 0 residual derivative, 1 relative monopole */
+  int32_t cutoff_policy; /* adaptive: 0 contain node, 1 COM distance */
+  int32_t reserved;
+  double adaptive_angle; /* adaptive_maximum_opening_angle */
+  double rel_tol;        /* tree relative_force_tolerance (alpha) */
+  double accel_floor;    /* tree relative_force_acceleration_floor_code */
 } oracle_params;
 
 typedef struct {
@@ -73,6 +81,16 @@ int oracle_treepm_solve(int64_t n, const double *x, const double *y, const doubl
                         double *pm_ax, double *pm_ay, double *pm_az, double *tree_ax,
                         double *tree_ay, double *tree_az, double *nearest_r2,
                         oracle_counters *counters);
+
+/* As oracle_treepm_solve, with the previous-step acceleration magnitudes of
+ * the targets (active-slot order; NULL: no history), which the relative
+ * criterion and the adaptive policy read. */
+int oracle_treepm_solve2(int64_t n, const double *x, const double *y, const double *z,
+                         const double *m, int64_t n_active, const uint32_t *active,
+                         const oracle_params *p, const double *prev_acc, double *ax, double *ay,
+                         double *az, double *pm_ax, double *pm_ay, double *pm_az, double *tree_ax,
+                         double *tree_ay, double *tree_az, double *nearest_r2,
+                         oracle_counters *counters);
 
 /* KDK pieces (src/workflows/gravity_runtime.cpp:3043-3059,
  * src/workflows/reference_runtime_composition.cpp:76-107) */

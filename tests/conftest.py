@@ -31,9 +31,16 @@ def golden_params(g):
     import oracle
     asmth, rcut, theta, gconst, eps = (float(v) for v in g["params"])
     leaf, scheme, deconv, criterion, order = (int(v) for v in g["iparams"])
+    adaptive = {}
+    if "adaptive" in g:
+        policy, estimator, cutoff_policy = (int(v) for v in g["adaptive"])
+        angle, rel_tol, floor = (float(v) for v in g["adaptive_f"])
+        adaptive = dict(policy=policy, estimator=estimator, cutoff_policy=cutoff_policy,
+                        adaptive_angle=angle, rel_tol=rel_tol, accel_floor=floor)
     return oracle.make_params(box=tuple(g["box"]), mesh=tuple(int(v) for v in g["mesh"]), asmth=asmth,
                               rcut=rcut, theta=theta, g=gconst, eps=eps, leaf=leaf, scheme=scheme,
-                              deconv=deconv, criterion=criterion, quadrupole=1 if order == 2 else 0)
+                              deconv=deconv, criterion=criterion, quadrupole=1 if order == 2 else 0,
+                              **adaptive)
 
 
 @pytest.fixture(scope="session")

@@ -3,7 +3,7 @@ TreePM (oracle/_ref/treepm_ref, compiled from the reference's sources by
 oracle/Makefile.ref) on seeded synthetic inputs.
 
     make -f oracle/Makefile.ref REF=<reference checkout> -j8
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]   # all fixtures, or only the named ones
 
 The reference has no stored golden vectors for this path; these fixtures are
 its outputs on the same inputs, committed so the oracle and the CUDA path can
@@ -30,7 +30,12 @@ TREE_KEYS = ("ux", "uy", "uz", "anchors", "morton_key", "sorted_index", "center_
              "qyz", "qzz", "trace", "child_count", "child_index", "particle_begin", "particle_count")
 
 
+ONLY = set(sys.argv[1:])
+
+
 def save(name: str, p: refio.RefProblem, r: dict, extra: dict | None = None, keep_tree=True):
+    if ONLY and name not in ONLY:
+        return
     d = {
         "x": p.x, "y": p.y, "z": p.z, "m": p.m,
         "vx": p.vx if p.vx is not None else np.zeros_like(p.x),
@@ -56,6 +61,11 @@ def save(name: str, p: refio.RefProblem, r: dict, extra: dict | None = None, kee
               "ewald_ax", "ewald_ay", "ewald_az"):
         if k in r:
             d[k] = r[k]
+    if p.policy or p.prev_acc is not None:
+        d["adaptive"] = np.array([p.policy, p.estimator, p.cutoff_policy], dtype=np.int64)
+        d["adaptive_f"] = np.array([p.adaptive_angle, p.rel_tol, p.accel_floor])
+        if p.prev_acc is not None:
+            d["prev_acc"] = np.asarray(p.prev_acc, dtype=np.float64)
     if extra:
         d.update(extra)
     np.savez_compressed(os.path.join(OUT, name + ".npz"), **d)
@@ -121,6 +131,33 @@ def main():
     p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(64,) * 3, theta=0.5, leaf=16,
                          kdk=1, drift=0.02, kick1=0.01, kick2=0.01, vx=vx, vy=vy, vz=vz, ewald=8)
     save("config32", p, refio.run(p))
+
+    # 6. adaptive relative policy (TreePmOptions::acceptance_policy = kAdaptiveRelative) on a
+    #    clustered box: lattice + NFW halos, softened, leaf 8. The acceleration history is the
+    #    reference's own strict-policy |a| on the same snapshot; a few entries are NaN (no
+    #    history: COM-distance fallback), zero or below the floor (also the fallback).
+    x, y, z, _, _, _ = ics.zeldovich_lattice(24, 20.0, 0.3, seed=21)
+    hx, hy, hz = ics.nfw_halos(6000, 12, 20.0, 2.5, seed=22, total_particles=len(x) + 6000)
+    x, y, z = np.concatenate([x, hx]), np.concatenate([y, hy]), np.concatenate([z, hz])
+    m = np.full(len(x), 1.0 / len(x))
+    common = dict(box=(20.0,) * 3, mesh=(32,) * 3, theta=0.5, leaf=8, eps=0.01, dump_tree=0)
+    r0 = refio.run(refio.RefProblem(x, y, z, m, **common))
+    prev = np.sqrt(r0["ax"] ** 2 + r0["ay"] ** 2 + r0["az"] ** 2)
+    rng = np.random.default_rng(23)
+    prev[rng.choice(len(x), 300, replace=False)] = np.nan
+    prev[rng.choice(len(x), 40, replace=False)] = 0.0
+    prev[rng.choice(len(x), 20, replace=False)] = 1e-31
+    #    the production fast deck: relative monopole, COM-distance cutoff nodes,
+    #    alpha 0.0025, maximum angle 1.0
+    p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=1, cutoff_policy=1,
+                         adaptive_angle=1.0, rel_tol=0.0025, prev_acc=prev)
+    save("adaptive_monopole", p, refio.run(p))
+    #    the default adaptive estimator: residual derivative, contain nodes, alpha 0.005,
+    #    maximum angle 0.5; an active subset carries its own history slots
+    active = np.sort(rng.choice(len(x), 5000, replace=False)).astype(np.uint32)
+    p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=0, cutoff_policy=0,
+                         adaptive_angle=0.5, rel_tol=0.005, prev_acc=prev[active], active=active)
+    save("adaptive_residual", p, refio.run(p))
 
 
 if __name__ == "__main__":

@@ -12,7 +12,8 @@ import pytest
 import oracle
 from conftest import golden_params, load_golden
 
-CASES = ["lattice16_cic", "clustered_tsc", "rect_active", "two_body", "quasi24", "duplicates", "config32"]
+CASES = ["lattice16_cic", "clustered_tsc", "rect_active", "two_body", "quasi24", "duplicates", "config32",
+         "adaptive_monopole", "adaptive_residual"]
 COUNTER_KEYS = ("visited", "accepted", "opened", "pairs", "pruned", "pair_skips", "multipoles", "leaves")
 
 
@@ -30,7 +31,7 @@ def _active(g):
 def test_oracle_accelerations_match_reference(name):
     g = load_golden(name)
     p = golden_params(g)
-    o = oracle.treepm_solve(g["x"], g["y"], g["z"], g["m"], p, active=_active(g))
+    o = oracle.treepm_solve(g["x"], g["y"], g["z"], g["m"], p, active=_active(g), prev_acc=g.get("prev_acc"))
     act = _active(g)
     for prefix in ("", "pm_", "tree_"):
         ref = [g[prefix + "ax"], g[prefix + "ay"], g[prefix + "az"]]
