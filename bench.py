@@ -59,6 +59,10 @@ UNIT = "particle-forces/s"
 FLOPS_PER_PAIR = 28.0
 FLOPS_PER_MULTIPOLE = 90.0
 FLOPS_PER_VISIT = 12.0
+# DRAM bytes of one production walk launch on the workload (ncu
+# dram__bytes_read.sum + dram__bytes_write.sum, one capture of
+# `bench.py --mode profile --workload clustered256`, first walkFast launch)
+WALK_DRAM_BYTES = {"clustered256": 11645360896 + 2439870976}
 # The differentiable case: 64^3 lattice + Zel'dovich (P ~ k^-2, 0.3 spacing
 # rms) in a box of 50, mesh 64^3, theta 0.5, 10 KDK steps of 0.05 at unit mean
 # density (G = 1), softening 0.1 spacing, loss = MSE(CIC density of the final
@@ -385,7 +389,8 @@ def run_gpu(args) -> int:
                          "peak_source": "measured FP32 FFMA probe (chui_treepm_probe_fp32_peak)",
                          "flops_convention": {"pair": FLOPS_PER_PAIR, "multipole": FLOPS_PER_MULTIPOLE,
                                               "visit": FLOPS_PER_VISIT},
-                         "traffic": None},
+                         "traffic": WALK_DRAM_BYTES.get(args.workload),
+                         "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 32,
                     "d2h_bytes_per_step": n * 24, "steps": e2e_steps},
             "gpu_launches": launches,
@@ -434,7 +439,8 @@ def cpu_baseline(w, x, y, z, m, args) -> dict | None:
 def run_profile(args) -> int:
     """Two production (mixed precision, diagnostics off) force evaluations of
     the workload (the second is the one an ncu capture selects with -s/-c),
-    nothing else: for launch lists and single-kernel captures."""
+    nothing else: for launch lists and single-kernel captures. --mode
+    profile-vjp runs two force VJPs instead."""
     import torch
     import chui_treepm as ct
     w = WORKLOADS[args.workload]
@@ -442,6 +448,15 @@ def run_profile(args) -> int:
     dev = torch.device("cuda", 0)
     t = {k: torch.tensor(v, device=dev) for k, v in dict(x=x, y=y, z=z, m=m).items()}
     with ct.TreePmCoordinator(make_config(w, ct._abi.MIXED, 0, diagnostics=0)) as s:
+        if args.mode == "profile-vjp":
+            # two force VJPs with seeded Gaussian cotangents (the adjoint's hot call)
+            g = torch.Generator(device="cpu").manual_seed(1)
+            cot = [torch.randn(len(x), generator=g, dtype=torch.float64).to(dev) for _ in range(3)]
+            for _ in range(2):
+                s.force_vjp(t["x"], t["y"], t["z"], t["m"], *cot)
+            torch.cuda.synchronize()
+            log(json.dumps(s.last_vjp_stats))
+            return 0
         for _ in range(2):
             s.solve_active_set(t["x"], t["y"], t["z"], t["m"])
         torch.cuda.synchronize()
@@ -578,9 +593,9 @@ def main() -> int:
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "large"])
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "profile-vjp", "large"])
     args = ap.parse_args()
-    if args.mode == "profile":
+    if args.mode in ("profile", "profile-vjp"):
         return run_profile(args)
     if args.mode == "large":
         if args.workload == "clustered256":
