@@ -17,6 +17,9 @@ HOST, DEVICE = 0, 1
 MIXED, FP64 = 0, 1
 CIC, TSC = 0, 1
 OPEN_GEOMETRIC, OPEN_COM_DISTANCE, OPEN_RELATIVE = 0, 1, 2
+POLICY_STRICT, POLICY_ADAPTIVE = 0, 1
+ESTIMATOR_RESIDUAL_DERIVATIVE, ESTIMATOR_RELATIVE_MONOPOLE = 0, 1
+CUTOFF_CONTAIN_NODE, CUTOFF_COM_DISTANCE = 0, 1
 
 
 class Config(C.Structure):
@@ -30,6 +33,9 @@ class Config(C.Structure):
         ("gravitational_constant", C.c_double), ("softening", C.c_double),
         ("acceptance_policy", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
         ("diagnostics", C.c_int32),
+        ("adaptive_error_estimator", C.c_int32), ("cutoff_node_policy", C.c_int32),
+        ("adaptive_maximum_opening_angle", C.c_double), ("relative_force_tolerance", C.c_double),
+        ("relative_force_acceleration_floor", C.c_double),
     ]
 
 
@@ -62,7 +68,7 @@ class Accumulator(C.Structure):
                 ("target_x", C.c_void_p), ("target_y", C.c_void_p), ("target_z", C.c_void_p),
                 ("long_range_x", C.c_void_p), ("long_range_y", C.c_void_p), ("long_range_z", C.c_void_p),
                 ("short_range_x", C.c_void_p), ("short_range_y", C.c_void_p), ("short_range_z", C.c_void_p),
-                ("nearest_pair_r2", C.c_void_p)]
+                ("nearest_pair_r2", C.c_void_p), ("previous_acceleration_magnitude", C.c_void_p)]
 
 
 class TreeDump(C.Structure):

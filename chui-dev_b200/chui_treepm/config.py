@@ -22,6 +22,9 @@ G_MPC_KMS2_PER_MSUN = 4.300917270036279e-09
 _CRITERIA = {"geometric": _abi.OPEN_GEOMETRIC, "com_distance": _abi.OPEN_COM_DISTANCE,
              "relative_force_error": _abi.OPEN_RELATIVE}
 _SCHEMES = {"cic": _abi.CIC, "tsc": _abi.TSC}
+_ESTIMATORS = {"residual_derivative": _abi.ESTIMATOR_RESIDUAL_DERIVATIVE,
+               "relative_monopole": _abi.ESTIMATOR_RELATIVE_MONOPOLE}
+_CUTOFF_POLICIES = {"contain": _abi.CUTOFF_CONTAIN_NODE, "com_distance": _abi.CUTOFF_COM_DISTANCE}
 
 
 def _bool(v: str) -> bool:
@@ -92,8 +95,19 @@ def config_from_param_text(text: str, precision: int = _abi.MIXED, device: int =
         raise ValueError(f"key 'numerics.treepm_assignment_scheme': invalid value '{scheme}'")
     c.assignment_scheme = _SCHEMES[scheme]
     c.window_deconvolution = 1 if get("numerics.treepm_enable_window_deconvolution", _bool, True) else 0
+    c.relative_force_tolerance = get("numerics.treepm_tree_relative_force_tolerance", float, 0.005)
+    c.relative_force_acceleration_floor = get("numerics.treepm_tree_relative_force_acceleration_floor", float, 1e-30)
     if get("numerics.treepm_adaptive_acceptance_enabled", _bool, False):
-        c.acceptance_policy = 1  # rejected by the library: only the strict policy is implemented
+        c.acceptance_policy = _abi.POLICY_ADAPTIVE
+    c.adaptive_maximum_opening_angle = get("numerics.treepm_adaptive_maximum_opening_angle", float, 0.25)
+    est = get("numerics.treepm_adaptive_error_estimator", lambda v: v.strip().lower(), "residual_derivative")
+    if est not in _ESTIMATORS:
+        raise ValueError(f"key 'numerics.treepm_adaptive_error_estimator': invalid value '{est}'")
+    c.adaptive_error_estimator = _ESTIMATORS[est]
+    cut = get("numerics.treepm_cutoff_node_policy", lambda v: v.strip().lower(), "contain")
+    if cut not in _CUTOFF_POLICIES:
+        raise ValueError(f"key 'numerics.treepm_cutoff_node_policy': invalid value '{cut}'")
+    c.cutoff_node_policy = _CUTOFF_POLICIES[cut]
     soft = kv.get("numerics.gravity_softening")
     if soft:
         # gravity_softening_kpc_comoving * 1e-3 (gravity_runtime.cpp:579-581)

@@ -83,10 +83,15 @@ class TreePmConfig:
     window_deconvolution: int = 0
     gravitational_constant: float = 1.0
     softening: float = 0.0
-    acceptance_policy: int = 0
+    acceptance_policy: int = _abi.POLICY_STRICT
     precision: int = _abi.MIXED
     device: int = 0
     diagnostics: int = 1
+    adaptive_error_estimator: int = _abi.ESTIMATOR_RESIDUAL_DERIVATIVE
+    cutoff_node_policy: int = _abi.CUTOFF_CONTAIN_NODE
+    adaptive_maximum_opening_angle: float = 0.25
+    relative_force_tolerance: float = 0.005
+    relative_force_acceleration_floor: float = 1.0e-30
 
     def to_c(self) -> _abi.Config:
         c = _abi.Config()
@@ -190,9 +195,12 @@ class TreePmCoordinator:
     def solve_active_set_with_pm_cadence(self, x, y, z, mass, refresh_long_range_field: bool, active=None,
                                          targets=None, uniform_mass: float | None = None,
                                          long_range: bool = False, short_range: bool = False,
-                                         nearest_pair: bool = False, stream=None) -> dict:
+                                         nearest_pair: bool = False, previous_acceleration=None,
+                                         stream=None) -> dict:
         """TreePmCoordinator::solveActiveSetWithPmCadence. Returns a dict with
-        ax, ay, az (active-slot order) and the requested optional lanes."""
+        ax, ay, az (active-slot order) and the requested optional lanes.
+        previous_acceleration: per active slot |a_previous| for the relative
+        criteria (NaN entries: no history for that target), or None."""
         arr = _Arrays(x)
         n = len(x)
         src = _abi.Sources()
@@ -221,6 +229,10 @@ class TreePmCoordinator:
             nt = n if active is None else len(active)
         acc.active_count = nt
         acc.active_index = arr.ptr(active, np.uint32) if active is not None else None
+        if previous_acceleration is not None:
+            if len(previous_acceleration) != nt:
+                raise InvalidArgument(_abi.EINVAL, "TreePM force accumulator spans must have matching active-set extent")
+            acc.previous_acceleration_magnitude = arr.ptr(previous_acceleration, np.float64)
         out = {}
         out["ax"], acc.accel_x = arr.out(nt, x)
         out["ay"], acc.accel_y = arr.out(nt, x)

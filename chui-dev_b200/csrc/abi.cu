@@ -278,10 +278,29 @@ double hostHp(double t) {
   return 1.12837916709551257389615890312154517 * e / t - 1.5 * L / (t * t * q);
 }
 
+// H''(t): Taylor series (4/sqrt(pi)) sum_k (-1)^k t^k / (k! (2k+7)) below
+// t = 1, closed form -(2/sqrt(pi)) e^{-t} (1/t + 2.5/t^2) + 3.75 L(sqrt t) / t^{7/2}
+// above (the derivative of H'(t) above).
+double hostHpp(double t) {
+  if (t < 1.0) {
+    double sum = 0.0, term = 1.0;
+    for (int k = 0; k <= 20; ++k) {
+      const double v = term / (2.0 * k + 7.0);
+      sum += (k & 1) ? -v : v;
+      term *= t / (k + 1.0);
+    }
+    return 2.25675833419102514779231780624309034 * sum;
+  }
+  const double q = std::sqrt(t);
+  const double e = std::exp(-t);
+  const double L = std::erf(q) - 1.12837916709551257389615890312154517 * q * e;
+  return -1.12837916709551257389615890312154517 * e * (1.0 / t + 2.5 / (t * t)) + 3.75 * L / (t * t * t * q);
+}
+
 // Chebyshev interpolation of f on [0, t_cut] rewritten as a polynomial in
 // s = t * 2 / t_cut - 1 (FP32 coefficients).
 template <class F>
-PolyH fitChebyshev(F func, double t_cut) {
+PolyH fitChebyshev(F func, double t_cut, double tolerance = 2.0e-6) {
   PolyH best;
   best.max_rel_error = 1e300;
   // The walk kernel evaluates either 12 terms or kPolyMaxTerms terms (unused
@@ -331,7 +350,7 @@ PolyH fitChebyshev(F func, double t_cut) {
     }
     p.max_rel_error = err;
     if (err < best.max_rel_error) best = p;
-    if (err < 2.0e-6) break;
+    if (err < tolerance) break;
   }
   return best;
 }
@@ -373,9 +392,24 @@ int validateConfig(const chui_treepm_config& cfg, std::string& err) {
     err = "TreePM PM assignment scheme is invalid";
     return CHUI_TREEPM_EINVAL;
   }
-  if (cfg.acceptance_policy != 0) {
-    err = "only the strict reference acceptance policy is implemented";
-    return CHUI_TREEPM_ENOTSUP;
+  // validateTreePmOptions (tree_pm_coupling.cpp:300-340)
+  if (!std::isfinite(cfg.relative_force_tolerance) || cfg.relative_force_tolerance <= 0.0 ||
+      !std::isfinite(cfg.relative_force_acceleration_floor) || cfg.relative_force_acceleration_floor <= 0.0 ||
+      !std::isfinite(cfg.adaptive_maximum_opening_angle) || cfg.adaptive_maximum_opening_angle <= 0.0 ||
+      cfg.adaptive_maximum_opening_angle > 1.0) {
+    err = "TreePM tree options are invalid";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if (cfg.acceptance_policy != CHUI_TREEPM_POLICY_STRICT && cfg.acceptance_policy != CHUI_TREEPM_POLICY_ADAPTIVE) {
+    err = "TreePM acceptance policy is invalid";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if ((cfg.adaptive_error_estimator != CHUI_TREEPM_ESTIMATOR_RESIDUAL_DERIVATIVE &&
+       cfg.adaptive_error_estimator != CHUI_TREEPM_ESTIMATOR_RELATIVE_MONOPOLE) ||
+      (cfg.cutoff_node_policy != CHUI_TREEPM_CUTOFF_CONTAIN_NODE &&
+       cfg.cutoff_node_policy != CHUI_TREEPM_CUTOFF_COM_DISTANCE)) {
+    err = "TreePM adaptive estimator or cutoff-node policy is invalid";
+    return CHUI_TREEPM_EINVAL;
   }
   if (cfg.precision != CHUI_TREEPM_MIXED && cfg.precision != CHUI_TREEPM_FP64) {
     err = "precision must be CHUI_TREEPM_MIXED or CHUI_TREEPM_FP64";
@@ -406,6 +440,8 @@ void applyConfig(Context& c, const chui_treepm_config& cfg) {
   const double t_cut = (c.cutoff * c.cutoff) / (4.0 * c.rs * c.rs) * (1.0 + 1.0e-5);
   c.poly = fitPoly(t_cut);
   c.dpoly = fitChebyshev(hostHp, t_cut);
+  // H'' scales the quadrupole's second-derivative term only: 1e-5 suffices
+  c.ddpoly = fitChebyshev(hostHpp, t_cut, 1.0e-5);
 }
 
 struct DeviceGuard {
@@ -494,10 +530,15 @@ int chui_treepm_config_default(chui_treepm_config* cfg) {
   cfg->window_deconvolution = 0;                              // pm_solver.hpp:232
   cfg->gravitational_constant = 1.0;
   cfg->softening = 0.0;
-  cfg->acceptance_policy = 0;
+  cfg->acceptance_policy = CHUI_TREEPM_POLICY_STRICT;            // tree_pm_coupling.hpp:247
   cfg->precision = CHUI_TREEPM_MIXED;
   cfg->device = 0;
   cfg->diagnostics = 1;
+  cfg->adaptive_error_estimator = CHUI_TREEPM_ESTIMATOR_RESIDUAL_DERIVATIVE;  // tree_pm_coupling.hpp:249
+  cfg->cutoff_node_policy = CHUI_TREEPM_CUTOFF_CONTAIN_NODE;                  // tree_pm_coupling.hpp:250
+  cfg->adaptive_maximum_opening_angle = 0.25;                                 // tree_pm_coupling.hpp:248
+  cfg->relative_force_tolerance = 0.005;                                      // tree_gravity.hpp:39
+  cfg->relative_force_acceleration_floor = 1.0e-30;                           // tree_gravity.hpp:40
   return 0;
 }
 
@@ -546,14 +587,14 @@ void chui_treepm_destroy(void* handle) {
     chui::DeviceGuard guard(c->device);
     cudaDeviceSynchronize();
     chui::pmDestroy(*c);
-    chui::DevBuf* bufs[] = {&c->in_x, &c->in_y, &c->in_z, &c->in_m, &c->in_active, &c->in_tx, &c->in_ty, &c->in_tz,
+    chui::DevBuf* bufs[] = {&c->in_x, &c->in_y, &c->in_z, &c->in_m, &c->in_active, &c->in_tx, &c->in_ty, &c->in_tz, &c->in_prev,
                             &c->out_acc[0], &c->out_acc[1], &c->out_acc[2], &c->out_pm[0], &c->out_pm[1],
                             &c->out_pm[2], &c->out_tree[0], &c->out_tree[1], &c->out_tree[2], &c->out_near,
                             &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max,
                             &c->bucket_next, &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
                             &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
                             &c->leaf_of_pos, &c->inv_pos, &c->cub_temp, &c->node_geom, &c->node_com,
-                            &c->node_quad, &c->node_f4, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
+                            &c->node_quad, &c->node_f4, &c->node_mq, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
                             &c->node_counter, &c->sorted_index, &c->pos_of_row, &c->src_f4, &c->src_d4, &c->src_u4, &c->src_cot,
                             &c->target_order, &c->morton_sorted, &c->walk_counters, &c->work_counter,
                             &c->tree_acc, &c->tree_near};
@@ -649,6 +690,10 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
       (rc = chui::stageIn(c, c.in_m, src->mass, src->mass ? n : 0, memory, s, &m)))
     return rc;
   if (acc->active_index && (rc = chui::stageIn(c, c.in_active, acc->active_index, nt, memory, s, &active))) return rc;
+  const double* prev = nullptr;
+  if (acc->previous_acceleration_magnitude &&
+      (rc = chui::stageIn(c, c.in_prev, acc->previous_acceleration_magnitude, nt, memory, s, &prev)))
+    return rc;
   if (explicit_targets &&
       ((rc = chui::stageIn(c, c.in_tx, acc->target_x, nt, memory, s, &tx)) ||
        (rc = chui::stageIn(c, c.in_ty, acc->target_y, nt, memory, s, &ty)) ||
@@ -728,13 +773,20 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   wp.exact_half = 0.5 * std::min({c.cfg.box_x, c.cfg.box_y, c.cfg.box_z}) - c.cutoff;
   wp.criterion = c.cfg.opening_criterion;
   wp.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
+  wp.policy = c.cfg.acceptance_policy;
+  wp.estimator = c.cfg.adaptive_error_estimator;
+  wp.com_cutoff = c.cfg.acceptance_policy == CHUI_TREEPM_POLICY_ADAPTIVE &&
+                  c.cfg.cutoff_node_policy == CHUI_TREEPM_CUTOFF_COM_DISTANCE;
+  wp.angle = c.cfg.adaptive_maximum_opening_angle;
+  wp.rel_tol = c.cfg.relative_force_tolerance;
+  wp.floor_ = c.cfg.relative_force_acceleration_floor;
   wp.inv_4rs2_f = static_cast<float>(0.25 / (c.rs * c.rs));
   wp.inv_8rs3_f = static_cast<float>(0.125 / (c.rs * c.rs * c.rs));
   wp.cut2_f = static_cast<float>(c.cutoff * c.cutoff);
   wp.eps2_f = static_cast<float>(c.cfg.softening * c.cfg.softening);
   wp.G_f = static_cast<float>(c.cfg.gravitational_constant);
   cudaMemsetAsync(c.status.ptr, 0, 4, s);
-  if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, wp, n, s)))
+  if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, prev, wp, n, s)))
     return chui::fail(c, rc, "residual walk launch failed");
   if (n == 0 && nt > 0) {
     if (chui::ensure(c.tree_acc, nt * 3 * 8) || chui::ensure(c.tree_near, nt * 8))

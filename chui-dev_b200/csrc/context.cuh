@@ -45,6 +45,12 @@ struct WalkParams {
   double exact_half;  // leaves with half >= this use the exact FP64 pair path
   int criterion;   // 0 geometric, 1 COM distance, 2 relative (no history: COM distance)
   int quadrupole;
+  int policy;      // 0 strict reference, 1 adaptive relative
+  int estimator;   // adaptive: 0 residual derivative, 1 relative monopole
+  int com_cutoff;  // adaptive with COM-distance cutoff nodes
+  double angle;    // adaptive_maximum_opening_angle
+  double rel_tol;  // relative_force_tolerance
+  double floor_;   // relative_force_acceleration_floor_code
   float inv_4rs2_f;   // 1/(4 r_s^2)
   float inv_8rs3_f;   // 1/(8 r_s^3)
   float cut2_f;
@@ -57,7 +63,8 @@ struct Context {
   int device = 0;
   double spacing = 0.0, rs = 0.0, cutoff = 0.0;
   PolyH poly;
-  PolyH dpoly;  // H'(t) for the adjoint walk
+  PolyH dpoly;   // H'(t): the adjoint walk and FP32 multipoles
+  PolyH ddpoly;  // H''(t): FP32 quadrupoles
   std::string last_error;
 
   // PM (cuFFT, in-place padded real layout nx*ny*2*(nz/2+1))
@@ -70,7 +77,7 @@ struct Context {
   double pm_field_box[3] = {0, 0, 0};
 
   // staged inputs / outputs
-  DevBuf in_x, in_y, in_z, in_m, in_active, in_tx, in_ty, in_tz;
+  DevBuf in_x, in_y, in_z, in_m, in_active, in_tx, in_ty, in_tz, in_prev;
   DevBuf out_acc[3], out_pm[3], out_tree[3], out_near;
   DevBuf status;       // uint32 status word + scalar results (reduction scratch)
   DevBuf scalars;      // reduction outputs (64 x u64)
@@ -94,6 +101,7 @@ struct Context {
   DevBuf node_geom;    // double4 {cx, cy, cz, half}
   DevBuf node_com;     // double4 {comx, comy, comz, mass}
   DevBuf node_quad;    // 8 doubles per node {qxx, qxy, qxz, qyy, qyz, qzz, trace, com_center_offset}
+  DevBuf node_mq;      // 2 x float4 per node: {mass, Mxx, Mxy, Mxz}, {Myy, Myz, Mzz, trace}, M = (Q + tr I)/3
   DevBuf node_f4;      // float4 {com - centre (x, y, z), |centre - com|}: FP32 node frame of the walk
   DevBuf node_child;   // 8 u32 per node
   DevBuf node_range;   // uint4 {begin, count, child_count | leaf flag, subtree_end}
@@ -159,7 +167,7 @@ int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explici
 // ---- walk (walk.cu) ----
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
-            const WalkParams& wp, int64_t n, cudaStream_t s);
+            const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s);
 
 // Adjoint of the short-range force for all n particles (targets in tree
 // order, after treeBuild and treeOrderTargets with the full set):

@@ -622,12 +622,19 @@ __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restr
 // FP32 COM offset from the node centre and |centre - COM| for the walk's
 // single-precision acceptance tests.
 __global__ void nodeFrameKernel(int64_t nodes, const double4* __restrict__ geom, const double4* __restrict__ com,
-                                const double* __restrict__ quad, float4* f4) {
+                                const double* __restrict__ quad, float4* f4, float4* mq) {
   for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nodes;
        k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const double4 g = geom[k], c = com[k];
+    const double* q = quad + 8 * k;
     f4[k] = make_float4(static_cast<float>(c.x - g.x), static_cast<float>(c.y - g.y), static_cast<float>(c.z - g.z),
-                        static_cast<float>(quad[8 * k + 7]));
+                        static_cast<float>(q[7]));
+    // the screened-quadrupole tensor M = (Q + tr I) / 3 of the multipole force
+    const double tr = q[6];
+    mq[2 * k] = make_float4(static_cast<float>(c.w), static_cast<float>((q[0] + tr) / 3.0),
+                            static_cast<float>(q[1] / 3.0), static_cast<float>(q[2] / 3.0));
+    mq[2 * k + 1] = make_float4(static_cast<float>((q[3] + tr) / 3.0), static_cast<float>(q[4] / 3.0),
+                                static_cast<float>((q[5] + tr) / 3.0), static_cast<float>(tr));
   }
 }
 
@@ -944,9 +951,11 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   { noteLaunch(); momentsKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(total_nodes, mi, out.geom, out.range, out.parent,
                                                           out.child, c.node_counter.as<uint32_t>(),
                                                           c.node_com.as<double4>(), c.node_quad.as<double>()); }
-  if (ensure(c.node_f4, total_nodes * sizeof(float4))) return CHUI_TREEPM_ENOMEM;
+  if (ensure(c.node_f4, total_nodes * sizeof(float4)) || ensure(c.node_mq, total_nodes * 2 * sizeof(float4)))
+    return CHUI_TREEPM_ENOMEM;
   { noteLaunch(); nodeFrameKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.geom, c.node_com.as<double4>(),
-                                                            c.node_quad.as<double>(), c.node_f4.as<float4>()); }
+                                                            c.node_quad.as<double>(), c.node_f4.as<float4>(),
+                                                            c.node_mq.as<float4>()); }
   // tree-ordered source records
   const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
   if (mixed) {

@@ -65,7 +65,9 @@ struct WalkArgs {
   const float4* src_f4;
   const double4* src_d4;
   const float4* node_f4;
+  const float4* node_mq;   // per node 2 x float4: {mass, Mxx, Mxy, Mxz}, {Myy, Myz, Mzz, trace}
   const double4* src_u4;   // tree-ordered unwrapped positions + mass (mixed)
+  const double* prev;      // per slot |a_previous| (nullable: no history)
   double* out_x;   // per slot, short-range part
   double* out_y;
   double* out_z;
@@ -74,6 +76,12 @@ struct WalkArgs {
   uint32_t* work;
   uint32_t* status;
   PolyH poly;
+  PolyH dpoly;     // H'(t)
+  PolyH ddpoly;    // H''(t)
+  float inv_16rs5_f;
+  float inv_32rs7_f;
+  int mult_f32;    // accepted multipoles in FP32 (the split constants are normal floats)
+  int mpoly12;     // H' and H'' fits have at most 12 terms
   WalkParams wp;
 };
 
@@ -95,7 +103,7 @@ __device__ __forceinline__ float polyHFixed(const PolyH& p, float t) {
 }
 
 // monopolePlusQuadrupoleAccelPeriodicReference (tree_pm_coupling.cpp:743-827), FP64.
-__device__ void multipoleForce(const WalkArgs& a, uint32_t node, double dx, double dy, double dz,
+__device__ __forceinline__ void multipoleForce(const WalkArgs& a, uint32_t node, double dx, double dy, double dz,
                                double eps_t, double& ax, double& ay, double& az) {
   const WalkParams& w = a.wp;
   const double rs = w.rs;
@@ -144,23 +152,94 @@ __device__ void multipoleForce(const WalkArgs& a, uint32_t node, double dx, doub
   az += fz;
 }
 
-// Strict-reference acceptance of an internal node (internal/tree_pm_acceptance.hpp:170-255
-// with acceptNodeByMac and the softening guard of internal/tree_interaction_common.hpp:36-89).
-__device__ __forceinline__ bool acceptStrict(const WalkParams& w, double half, double com_offset,
-                                             bool inside, bool within, double r2, double eps_t) {
-  const double r = sqrt(fmax(r2, 1.0e-30));
-  // uniform softening: node softening max == min, the envelope guard passes
-  (void)eps_t;
-  const bool envelope_ok = w.quadrupole && (2.0 * half / r) < 0.08;
-  bool mac_ok;
-  if (inside) {
-    mac_ok = false;
-  } else if (w.criterion == 0) {
-    mac_ok = (2.0 * half / sqrt(r2 + 1.0e-30)) < w.theta;
-  } else {
-    mac_ok = ((2.0 * half + com_offset) / sqrt(r2 + 1.0e-30)) < w.theta;
+// |d|^2 summed as the reference does, ((dx dx + dy dy) + dz dz) with every
+// operation rounded on its own (no FMA contraction), so acceptance decisions
+// see the reference's exact value.
+__device__ __forceinline__ double norm2rn(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// Per-target acceleration history: present and finite
+// (tree_pm_coupling.cpp:4467-4472); magnitude 0 when absent.
+struct History {
+  bool avail;
+  double mag;
+};
+
+__device__ __forceinline__ History loadHistory(const double* prev, uint32_t slot, bool valid) {
+  History h{false, 0.0};
+  if (prev && valid) {
+    const double v = prev[slot];
+    h.avail = isfinite(v);
+    h.mag = h.avail ? v : 0.0;
   }
-  return mac_ok && envelope_ok && within && !inside && isfinite(r2);
+  return h;
+}
+
+// residualAccuracyProxy (internal/tree_pm_acceptance.hpp:20-51) with uniform
+// softening (node softening max = the target's). Scalars by value: a
+// reference into the kernel's parameter block would force a local copy of it.
+__device__ __noinline__ double residualProxy(double G, double eps, double rs, double half, double com_offset,
+                                            double mass, double r2) {
+  if (!(r2 > 0.0) || !isfinite(r2)) return INFINITY;
+  const double r = sqrt(r2);
+  const double d = r2 + eps * eps;
+  const double inv_d5 = 1.0 / (d * d * sqrt(d));
+  const double inv_r3 = 1.0 / (r2 * r);
+  const double inv_r4 = 1.0 / (r2 * r2);
+  const double long_factor = longRangeFactor(r, rs);
+  const double q = r / (2.0 * rs);
+  const double exponential = exp(-q * q);
+  const double k_inv_sqrt_pi = 0.564189583547756286948079451560772586;
+  const double scale3 = rs * rs * rs;
+  const double s_first = -0.5 * k_inv_sqrt_pi * r2 * exponential / scale3;
+  const double s_second = k_inv_sqrt_pi * exponential * (-r / scale3 + 0.25 * r * r2 / (scale3 * rs * rs));
+  const double first = -3.0 * r * inv_d5 + s_first * inv_r3 - 3.0 * (-long_factor) * inv_r4;
+  const double second = -3.0 * inv_d5 + 15.0 * r2 * inv_d5 / d + s_second * inv_r3 - 6.0 * s_first * inv_r4 +
+                        12.0 * (-long_factor) * inv_r4 / r;
+  const double width = 2.0 * half;
+  const double rho = sqrt(3.0) * half + com_offset;
+  const double proxy =
+      G * mass * fmax(width * width * inv_r4, 0.5 * rho * rho * (3.0 * fabs(first) + fabs(r * second - first)));
+  return isfinite(proxy) && proxy >= 0.0 ? proxy : INFINITY;
+}
+
+// Acceptance of an internal node (acceptTreePmNode, internal/tree_pm_acceptance.hpp:53-139,
+// with acceptNodeByMac and acceptNodeByComDistanceMac of
+// internal/tree_interaction_common.hpp:36-75). Softening is uniform, so the
+// softening envelope guard passes.
+template <bool kAdaptive>
+__device__ __forceinline__ bool acceptNode(const WalkParams& w, double half, double com_offset, double mass,
+                                           bool inside, bool within, double r2, const History& hist) {
+  const double r = sqrt(fmax(r2, 1.0e-30));
+  const double width = 2.0 * half;
+  if constexpr (!kAdaptive) {
+    const bool envelope_ok = w.quadrupole && (width / r) < 0.08;
+    bool mac_ok;
+    if (inside) {
+      mac_ok = false;
+    } else if (w.criterion == 0) {
+      mac_ok = (width / sqrt(r2 + 1.0e-30)) < w.theta;
+    } else if (w.criterion == 1 || !hist.avail) {
+      mac_ok = ((width + com_offset) / sqrt(r2 + 1.0e-30)) < w.theta;
+    } else {
+      const double scale = fmax(fabs(hist.mag), w.floor_);
+      mac_ok = w.G * mass * width * width <= w.rel_tol * scale * r2 * r2;
+    }
+    return mac_ok && envelope_ok && within && !inside && isfinite(r2);
+  }
+  const bool envelope_ok = (width / r) < w.angle;
+  if (!envelope_ok || inside || !within || !isfinite(r2)) return false;
+  if (hist.avail && hist.mag > w.floor_) {
+    const double allowance = w.rel_tol * hist.mag;
+    const double inv_r4 = 1.0 / (r2 * r2);
+    const double lower = w.G * mass * (width * width * inv_r4);
+    if (isfinite(allowance) && isfinite(lower) && lower > allowance) return false;
+    if (w.estimator == 1) return isfinite(allowance) && isfinite(lower);
+    const double est = residualProxy(w.G, w.eps, w.rs, half, com_offset, mass, r2);
+    return isfinite(est) && isfinite(allowance) && est <= allowance;
+  }
+  return ((width + com_offset) / sqrt(r2 + 1.0e-30)) < w.theta;
 }
 
 template <bool kMixed, bool kEpsZero>
@@ -200,6 +279,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
     const bool skip_self = valid && row < a.n;
     const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
     const double eps_t = w.eps;
+    const History hist = loadHistory(a.prev, slot, valid);
     Metric sm[3], nm[3];
     const double pt[3] = {px, py, pz};
     for (int ax_ = 0; ax_ < 3; ++ax_) {
@@ -229,7 +309,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
       const double ndz = applyMetric(nm[2], g.z - pz);
       const double ax_abs = fabs(ndx), ay_abs = fabs(ndy), az_abs = fabs(ndz);
       const double ex = fmax(0.0, ax_abs - h), ey = fmax(0.0, ay_abs - h), ez = fmax(0.0, az_abs - h);
-      const bool prune = !withinCutoff(ex * ex + ey * ey + ez * ez, w.cutoff, w.cutoff2);
+      bool prune = !withinCutoff(ex * ex + ey * ey + ez * ez, w.cutoff, w.cutoff2);
       if (act) {
         ++cnt_visited;
         cnt_pruned += prune ? 1 : 0;
@@ -317,14 +397,23 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
       // internal node
       const double4 cm = a.com[node];
       const double off = a.quad[8 * static_cast<size_t>(node) + 7];
-      const bool inside = skip_self && ax_abs <= h && ay_abs <= h && az_abs <= h;
+      // the adaptive policy tests containment for every target (tree_pm_coupling.cpp:4090-4092)
+      const bool inside = (skip_self || w.policy == 1) && ax_abs <= h && ay_abs <= h && az_abs <= h;
       const double mx = ax_abs + h, my = ay_abs + h, mz = az_abs + h;
-      const bool within = withinCutoff(mx * mx + my * my + mz * mz, w.cutoff, w.cutoff2);
+      const bool within = w.com_cutoff || withinCutoff(mx * mx + my * my + mz * mz, w.cutoff, w.cutoff2);
       const double dx = applyMetric(nm[0], cm.x - px);
       const double dy = applyMetric(nm[1], cm.y - py);
       const double dz = applyMetric(nm[2], cm.z - pz);
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      const bool accept = act && !prune && acceptStrict(w, h, off, inside, within, r2, eps_t);
+      const double r2 = norm2rn(dx, dy, dz);
+      bool accept = act && !prune &&
+                    (w.policy == 1 ? acceptNode<true>(w, h, off, cm.w, inside, within, r2, hist)
+                                   : acceptNode<false>(w, h, off, cm.w, inside, within, r2, hist));
+      // COM-distance cutoff nodes: accepted beyond r_cut means pruned (:4129-4132)
+      if (accept && w.com_cutoff && r2 > w.cutoff2) {
+        accept = false;
+        prune = true;
+        ++cnt_pruned;
+      }
       const bool open = act && !prune && !accept;
       if (accept) {
         ++cnt_accepted;
@@ -373,7 +462,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
   }
 }
 
-constexpr int kQueue = 64;  // sources per warp batch
+constexpr int kQueue = 64;   // sources per warp batch
+constexpr int kMultList = 8; // accepted multipoles per lane before a flush
 
 // Subtree blocks of the production walk (diagnostics off): an opened node
 // with at most kBulkCount sources and half-size at most kBulkHalf * r_cut is
@@ -387,7 +477,14 @@ constexpr int kQueue = 64;  // sources per warp batch
 #ifndef CHUI_WALK_MIN_BLOCKS
 #define CHUI_WALK_MIN_BLOCKS 5  // resident blocks per SM the register budget is sized for
 #endif
+// Under the adaptive policy most opened nodes have deeper accepted
+// multipoles, so blocks pay only for small nodes; evaluating their sources as
+// pairs is at least as accurate as the multipoles it replaces.
+#ifndef CHUI_BULK_COUNT_ADAPTIVE
+#define CHUI_BULK_COUNT_ADAPTIVE 256
+#endif
 constexpr uint32_t kBulkCount = CHUI_BULK_COUNT;
+constexpr uint32_t kBulkCountAdaptive = CHUI_BULK_COUNT_ADAPTIVE;
 constexpr double kBulkHalf = CHUI_BULK_HALF;
 
 // The fitted polynomial at t = r^2 / (4 r_s^2), straight from r^2: s =
@@ -403,6 +500,46 @@ __device__ __forceinline__ float hornerR2(const PolyH& p, float r2, float sc) {
   return h;
 }
 
+// monopolePlusQuadrupoleAccelPeriodicReference (tree_pm_coupling.cpp:743-827)
+// in FP32, without the G factor, added to (fx, fy, fz). With t = r^2/(4 r_s^2)
+// and H the fitted long-range kernel: K = (r^2+eps^2)^-3/2 - H(t)/(8 r_s^3),
+// K'/r = -3 (r^2+eps^2)^-5/2 - H'(t)/(16 r_s^5) and
+// (K'' - K'/r)/r^2 = 15 (r^2+eps^2)^-7/2 - H''(t)/(32 r_s^7); the force is
+// M K d + f1 (Md + tr d / 2) + cr (d.Md) d / 2 with f1 = K'/r, cr the last.
+template <bool kEpsZero, int kTerms>
+__device__ __forceinline__ void multipoleF32(const WalkArgs& a, uint32_t node, float dx, float dy, float dz, float sc,
+                                             float& fx, float& fy, float& fz) {
+  const float4 q0 = a.node_mq[2 * static_cast<size_t>(node)];
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float den = kEpsZero ? r2 : r2 + a.wp.eps2_f;
+  const float rinv = rsqrtf(den);
+  const float rinv2 = rinv * rinv;
+  const float rinv3 = rinv2 * rinv;
+  const float k = fmaf(-hornerR2<kTerms>(a.poly, r2, sc), a.wp.inv_8rs3_f, rinv3);
+  float s = q0.x * k;
+  if (a.wp.quadrupole) {
+    const float4 q1 = a.node_mq[2 * static_cast<size_t>(node) + 1];
+    const float rinv5 = rinv3 * rinv2;
+    // H' and H'' have their own fitted lengths (warp-uniform choice)
+    const float h1 = a.mpoly12 ? hornerR2<12>(a.dpoly, r2, sc) : hornerR2<kPolyMaxTerms>(a.dpoly, r2, sc);
+    const float h2 = a.mpoly12 ? hornerR2<12>(a.ddpoly, r2, sc) : hornerR2<kPolyMaxTerms>(a.ddpoly, r2, sc);
+    const float f1 = fmaf(-h1, a.inv_16rs5_f, -3.0f * rinv5);
+    const float cr = fmaf(-h2, a.inv_32rs7_f, 15.0f * rinv5 * rinv2);
+    const float mdx = fmaf(q0.y, dx, fmaf(q0.z, dy, q0.w * dz));
+    const float mdy = fmaf(q0.z, dx, fmaf(q1.x, dy, q1.y * dz));
+    const float mdz = fmaf(q0.w, dx, fmaf(q1.y, dy, q1.z * dz));
+    const float dmd = fmaf(dx, mdx, fmaf(dy, mdy, dz * mdz));
+    s = fmaf(0.5f, fmaf(q1.w, f1, dmd * cr), s);
+    fx = fmaf(mdx, f1, fmaf(s, dx, fx));
+    fy = fmaf(mdy, f1, fmaf(s, dy, fy));
+    fz = fmaf(mdz, f1, fmaf(s, dz, fz));
+  } else {
+    fx = fmaf(s, dx, fx);
+    fy = fmaf(s, dy, fy);
+    fz = fmaf(s, dz, fz);
+  }
+}
+
 // Exact (FP64, reference formulas) decision for one lane at one node: prune,
 // and for internal nodes accept/open, plus the COM offset for a multipole.
 struct ExactDecision {
@@ -410,8 +547,9 @@ struct ExactDecision {
   double dx, dy, dz;
 };
 
+template <bool kAdaptive>
 __device__ __forceinline__ ExactDecision exactNodeDecision(const WalkArgs& a, uint32_t node, double px, double py,
-                                                        double pz, bool skip_self) {
+                                                        double pz, bool skip_self, const History& hist) {
   const WalkParams& w = a.wp;
   ExactDecision d{};
   const double4 g = a.geom[node];
@@ -428,14 +566,18 @@ __device__ __forceinline__ ExactDecision exactNodeDecision(const WalkArgs& a, ui
   if (d.prune || rg4.z == 0) return d;
   const double4 cm = a.com[node];
   const double off = a.quad[8 * static_cast<size_t>(node) + 7];
-  const bool inside = skip_self && ax <= h && ay <= h && az <= h;
+  const bool inside = (skip_self || kAdaptive) && ax <= h && ay <= h && az <= h;
   const double qx = ax + h, qy = ay + h, qz = az + h;
-  const bool within = withinCutoff(qx * qx + qy * qy + qz * qz, w.cutoff, w.cutoff2);
+  const bool within = (kAdaptive && w.com_cutoff) || withinCutoff(qx * qx + qy * qy + qz * qz, w.cutoff, w.cutoff2);
   d.dx = applyMetric(mx, cm.x - px);
   d.dy = applyMetric(my, cm.y - py);
   d.dz = applyMetric(mz, cm.z - pz);
-  const double r2 = d.dx * d.dx + d.dy * d.dy + d.dz * d.dz;
-  d.accept = acceptStrict(w, h, off, inside, within, r2, w.eps);
+  const double r2 = norm2rn(d.dx, d.dy, d.dz);
+  d.accept = acceptNode<kAdaptive>(w, h, off, cm.w, inside, within, r2, hist);
+  if (kAdaptive && d.accept && w.com_cutoff && r2 > w.cutoff2) {  // accepted beyond r_cut: pruned
+    d.accept = false;
+    d.prune = true;
+  }
   return d;
 }
 
@@ -478,10 +620,11 @@ __device__ __forceinline__ void exactLeafPairs(const WalkArgs& a, double4* stage
   }
 }
 
-// Comparison a < b decided in FP32 with a relative guard band: returns
-// +1 (certainly true), -1 (certainly false) or 0 (too close to call in FP32).
-__device__ __forceinline__ int certainLess(float a, float b) {
-  const float band = 2.0e-5f * (fabsf(a) + fabsf(b)) + 1.0e-30f;
+// Comparison a < b decided in FP32 with a guard band (relative, plus an
+// absolute bound `err` on the inputs' own error): returns +1 (certainly true),
+// -1 (certainly false) or 0 (too close to call in FP32).
+__device__ __forceinline__ int certainLess(float a, float b, float err = 0.f) {
+  const float band = fmaf(2.0e-5f, fabsf(a) + fabsf(b), err) + 1.0e-30f;
   if (a < b - band) return 1;
   if (a > b + band) return -1;
   return 0;
@@ -498,11 +641,17 @@ __device__ __forceinline__ int certainLess(float a, float b) {
 // Accepted leaves are appended to a shared-memory queue (sources outside the
 // group's cutoff sphere are dropped at enqueue) tagged with the ballot of
 // accepting lanes, and evaluated 64 sources at a time in FP32.
-template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous>
+// kMode: 0 strict policy without acceleration history, 1 strict policy with
+// the relative-force MAC and history, 2 adaptive-relative policy.
+template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS) walkFastKernel(WalkArgs a) {
+  constexpr bool kAdaptive = kMode == 2;
+  constexpr bool kHistory = kMode != 0;
+  constexpr int kList = kAdaptive ? kMultList : 1;
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
   __shared__ float4 q_src[kWalkWarpsPerBlock][kQueue];
   __shared__ uint2 q_meta[kWalkWarpsPerBlock][kQueue];
+  __shared__ float4 m_list[kWalkWarpsPerBlock][kList][32];
   __shared__ double4 exact_sm[kWalkWarpsPerBlock][32];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -511,8 +660,10 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   const WalkParams& w = a.wp;
   const double half_min_box = 0.5 * fmin(w.box[0], fmin(w.box[1], w.box[2]));
   const float cut2 = w.cut2_f;
+  const float cut_f = static_cast<float>(w.cutoff);
   const float env2 = 0.0064f;  // 0.08^2
   const float theta2 = static_cast<float>(w.theta * w.theta);
+  const float angle2 = static_cast<float>(w.angle * w.angle);
   const double bulk_half = kBulkHalf * w.cutoff;
   const float sc_r2 = w.inv_4rs2_f * a.poly.scale;
 
@@ -556,12 +707,24 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     const float tfx = static_cast<float>(ox), tfy = static_cast<float>(oy), tfz = static_cast<float>(oz);
     const float cull = static_cast<float>(w.cutoff + sqrt(rg2));
     const float cull2 = cull * cull * 1.0001f;
+    const float rga_f = static_cast<float>(rga);
     const bool skip_self = valid && row < a.n;
     const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
+    const History hist = loadHistory(kHistory ? a.prev : nullptr, slot, valid);
+    // relative criterion in FP32: the allowance alpha |a_prev| (adaptive, with
+    // usable history) or alpha max(|a_prev|, floor) (strict relative MAC, any
+    // finite history); FP32 tests are used only where it is a normal float
+    const bool rel_test = kAdaptive ? (hist.avail && hist.mag > w.floor_) : (kHistory && hist.avail);
+    float allow_f = 0.f;
+    if (rel_test) {
+      allow_f = static_cast<float>(kAdaptive ? w.rel_tol * hist.mag : w.rel_tol * fmax(fabs(hist.mag), w.floor_));
+      if (!(allow_f >= FLT_MIN && allow_f <= FLT_MAX)) allow_f = 0.f;  // FP32 cannot decide: exact path
+    }
     double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
     float nearest_f = INFINITY;
     uint32_t skip_until = 0;
-    int qn = 0;
+    int qn = 0;  // warp's source queue length
+    int mn = 0;  // this lane's multipole list length
     if (lane == 0) stack[0] = 0u;
     int sp = 1;
     __syncwarp();
@@ -600,6 +763,25 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       cnt_pairs += pairs;
       cnt_skips += skips;
       qn = 0;
+      __syncwarp();
+    };
+
+    // Accepted multipoles wait in a per-lane list and are evaluated together:
+    // the lanes step through their own lists in lockstep, so a warp pays for
+    // the longest list rather than for every node some lane accepted.
+    auto mflush = [&]() {
+      const int kmax = __reduce_max_sync(0xffffffffu, mn);
+      float fx = 0.f, fy = 0.f, fz = 0.f;
+      for (int k = 0; k < kmax; ++k) {
+        if (k < mn) {
+          const float4 e = m_list[warp][k][lane];
+          multipoleF32<kEpsZero, kTerms>(a, __float_as_uint(e.w), e.x, e.y, e.z, sc_r2, fx, fy, fz);
+        }
+      }
+      acc_x += static_cast<double>(w.G_f * fx);
+      acc_y += static_cast<double>(w.G_f * fy);
+      acc_z += static_cast<double>(w.G_f * fz);
+      mn = 0;
       __syncwarp();
     };
 
@@ -661,57 +843,95 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       cdx -= w.box[0] * rint(cdx / w.box[0]);
       cdy -= w.box[1] * rint(cdy / w.box[1]);
       cdz -= w.box[2] * rint(cdz / w.box[2]);
-      const bool fast_frame = h < 64.0 * w.cutoff &&
-                              fmax(fabs(cdx), fmax(fabs(cdy), fabs(cdz))) + rga < half_min_box * (1.0 - 1.0e-9);
+      const double cmax = fmax(fabs(cdx), fmax(fabs(cdy), fabs(cdz)));
+      const bool fast_frame = h < 64.0 * w.cutoff && cmax + rga < half_min_box * (1.0 - 1.0e-9);
       bool prune = false, accept = false, need_exact = !fast_frame;
-      float ndx = 0.f, ndy = 0.f, ndz = 0.f;
+      float dxc = 0.f, dyc = 0.f, dzc = 0.f;  // COM offset of an accepted node (FP32)
       if (act && fast_frame) {
         const float hf = static_cast<float>(h);
-        ndx = static_cast<float>(cdx) - tfx;
-        ndy = static_cast<float>(cdy) - tfy;
-        ndz = static_cast<float>(cdz) - tfz;
+        // bound on the error of each FP32 offset component below (centre and
+        // target offsets rounded once, one subtraction, the COM offset added)
+        const float fe = 2.4e-7f * (static_cast<float>(cmax) + rga_f + hf);
+        const float cut_e = 4.0f * cut_f * fe;
+        const float ndx = static_cast<float>(cdx) - tfx;
+        const float ndy = static_cast<float>(cdy) - tfy;
+        const float ndz = static_cast<float>(cdz) - tfz;
         const float ax = fabsf(ndx), ay = fabsf(ndy), az = fabsf(ndz);
         const float ex = fmaxf(0.f, ax - hf), ey = fmaxf(0.f, ay - hf), ez = fmaxf(0.f, az - hf);
-        const int keep = certainLess(fmaf(ex, ex, fmaf(ey, ey, ez * ez)), cut2);
+        const int keep = certainLess(fmaf(ex, ex, fmaf(ey, ey, ez * ez)), cut2, cut_e);
         if (keep == 0) {
           need_exact = true;
         } else {
           prune = keep < 0;
           if (!prune && !is_leaf) {
-            // inside (target within the node cube), cutoff containment, envelope, MAC
-            int cin = 1;
-            if (skip_self) {
-              const int ix = certainLess(ax, hf), iy = certainLess(ay, hf), iz = certainLess(az, hf);
-              if (ix == 0 || iy == 0 || iz == 0) cin = 0;
-              else cin = (ix > 0 && iy > 0 && iz > 0) ? 1 : -1;  // +1 inside, -1 outside
-            } else {
-              cin = -1;
+            // inside (target within the node cube), cutoff containment, envelope, MAC;
+            // each +1 certainly true, -1 certainly false, 0 too close to call in FP32
+            int cin = -1;
+            if (skip_self || kAdaptive) {
+              const int ix = certainLess(ax, hf, fe), iy = certainLess(ay, hf, fe), iz = certainLess(az, hf, fe);
+              if (ix < 0 || iy < 0 || iz < 0) cin = -1;  // outside on some axis
+              else cin = (ix > 0 && iy > 0 && iz > 0) ? 1 : 0;
             }
-            const float qx = ax + hf, qy = ay + hf, qz = az + hf;
-            const int within = certainLess(fmaf(qx, qx, fmaf(qy, qy, qz * qz)), cut2);
+            int within = 1;
+            if (!(kAdaptive && w.com_cutoff)) {
+              const float qx = ax + hf, qy = ay + hf, qz = az + hf;
+              within = certainLess(fmaf(qx, qx, fmaf(qy, qy, qz * qz)), cut2, cut_e);
+            }
             const float4 nf = a.node_f4[node];
-            const float dxc = ndx + nf.x, dyc = ndy + nf.y, dzc = ndz + nf.z;
+            dxc = ndx + nf.x;
+            dyc = ndy + nf.y;
+            dzc = ndz + nf.z;
             const float r2c = fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc));
             const float w2 = 4.0f * hf * hf;
-            const int env = w.quadrupole ? certainLess(w2, env2 * r2c) : -1;
-            const float macl = (w.criterion == 0) ? w2 : (2.0f * hf + nf.w) * (2.0f * hf + nf.w);
-            const int mac = certainLess(macl, theta2 * r2c);
-            if (cin == 0 || within == 0 || env == 0 || mac == 0) {
+            const float r2c_e = 4.0f * sqrtf(r2c) * fe;  // bound on the error of r2c
+            int env, mac;
+            if constexpr (kAdaptive) {
+              env = certainLess(w2, angle2 * r2c, angle2 * r2c_e);
+            } else {
+              env = w.quadrupole ? certainLess(w2, env2 * r2c, env2 * r2c_e) : -1;
+            }
+            if (rel_test) {
+              // G M w^2 / r^4 against the allowance (relative monopole: lower <= allowance
+              // accepts; residual derivative: lower > allowance rejects, else the FP64 proxy)
+              const float gm = w.G_f * a.node_mq[2 * static_cast<size_t>(node)].x;
+              const float lower = gm * ((w2 / r2c) / r2c);
+              const int over = (allow_f > 0.f && isfinite(lower))
+                                   ? certainLess(allow_f, lower, 2.0f * lower * (r2c_e / r2c))
+                                   : 0;
+              if (!kAdaptive || w.estimator == 1) mac = -over;
+              else mac = over > 0 ? -1 : 0;
+            } else {
+              const float macl = (!kAdaptive && w.criterion == 0) ? w2 : (2.0f * hf + nf.w) * (2.0f * hf + nf.w);
+              mac = certainLess(macl, theta2 * r2c, theta2 * r2c_e);
+            }
+            if (cin > 0 || within < 0 || env < 0 || mac < 0) {
+              accept = false;  // some condition certainly fails
+            } else if (cin == 0 || within == 0 || env == 0 || mac == 0) {
               need_exact = true;
             } else {
-              accept = cin < 0 && within > 0 && env > 0 && mac > 0;
+              accept = true;
+              if (kAdaptive && w.com_cutoff) {
+                // accepted with its COM beyond r_cut: pruned (tree_pm_coupling.cpp:4129-4132)
+                const int beyond = certainLess(cut2, r2c, r2c_e);
+                if (beyond > 0) {
+                  accept = false;
+                  prune = true;
+                } else if (beyond == 0) {
+                  accept = false;
+                  need_exact = true;
+                }
+              }
             }
           }
         }
       }
-      double mdx = 0.0, mdy = 0.0, mdz = 0.0;
       if (act && need_exact) {
-        const ExactDecision d = exactNodeDecision(a, node, px, py, pz, skip_self);
+        const ExactDecision d = exactNodeDecision<kAdaptive>(a, node, px, py, pz, skip_self, hist);
         prune = d.prune;
         accept = d.accept;
-        mdx = d.dx;
-        mdy = d.dy;
-        mdz = d.dz;
+        dxc = static_cast<float>(d.dx);
+        dyc = static_cast<float>(d.dy);
+        dzc = static_cast<float>(d.dz);
       }
       if (kDiag && act) {
         ++cnt_visited;
@@ -745,24 +965,39 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
           ++cnt_accepted;
           ++cnt_multi;
         }
-        if (!need_exact) {
-          const ExactDecision d = exactNodeDecision(a, node, px, py, pz, skip_self);
-          mdx = d.dx;
-          mdy = d.dy;
-          mdz = d.dz;
+        if (a.mult_f32 && fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc)) >= fmaxf(1.0e-8f * cut2, 1.0e-10f)) {
+          if constexpr (kAdaptive) {
+            m_list[warp][mn][lane] = make_float4(dxc, dyc, dzc, __uint_as_float(node));
+            ++mn;
+          } else {
+            // few multipoles under the strict policy: evaluated where accepted
+            float fx = 0.f, fy = 0.f, fz = 0.f;
+            multipoleF32<kEpsZero, kTerms>(a, node, dxc, dyc, dzc, sc_r2, fx, fy, fz);
+            acc_x += static_cast<double>(w.G_f * fx);
+            acc_y += static_cast<double>(w.G_f * fy);
+            acc_z += static_cast<double>(w.G_f * fz);
+          }
+        } else {
+          // FP64 multipole: FP32 powers of 1/r could overflow this close to the
+          // COM, or the FP32 split constants are out of range for this r_s
+          const ExactDecision d = exactNodeDecision<kAdaptive>(a, node, px, py, pz, skip_self, hist);
+          multipoleForce(a, node, d.dx, d.dy, d.dz, w.eps, acc_x, acc_y, acc_z);
         }
-        multipoleForce(a, node, mdx, mdy, mdz, w.eps, acc_x, acc_y, acc_z);
+      }
+      if constexpr (kAdaptive) {
+        if (__any_sync(0xffffffffu, mn == kList)) mflush();
       }
       if (act && (prune || accept)) skip_until = rg4.w;
       if (kDiag && open) ++cnt_opened;
       if (__any_sync(0xffffffffu, open)) {
-        if constexpr (!kDiag) {
+        constexpr uint32_t kBlock = kAdaptive ? kBulkCountAdaptive : kBulkCount;
+        if constexpr (!kDiag && kBlock > 0) {
           // Subtree block: the lanes that opened this small node take every
           // source in it within r_cut (per-pair test, as in the leaf path)
           // instead of descending. This is the reference's pair set except
           // where a deeper node would have been accepted as a strict
           // multipole; those few are evaluated as the pairs they stand for.
-          if (fast_frame && rg4.y <= kBulkCount && h <= bulk_half && w.cutoff + h + rga < half_min_box &&
+          if (fast_frame && rg4.y <= kBlock && h <= bulk_half && w.cutoff + h + rga < half_min_box &&
               h < w.exact_half) {
             enqueue(rg4.x, rg4.y, __ballot_sync(0xffffffffu, open), true, g, cdx, cdy, cdz);
             continue;
@@ -781,6 +1016,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       }
     }
     if (qn > 0) flush();
+    if constexpr (kAdaptive) {
+      if (__any_sync(0xffffffffu, mn > 0)) mflush();
+    }
     if (overflow && lane == 0) atomicOr(a.status, kStatusStackOverflow);
     if (valid) {
       a.out_x[slot] = acc_x;
@@ -1130,7 +1368,7 @@ int launchWalk(const WalkArgs& args, cudaStream_t s) {
 
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
-            const WalkParams& wp, int64_t n, cudaStream_t s) {
+            const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s) {
   if (nt == 0) return 0;
   if (ensure(c.tree_acc, static_cast<size_t>(nt) * 3 * sizeof(double)) ||
       ensure(c.tree_near, static_cast<size_t>(nt) * sizeof(double)) ||
@@ -1158,7 +1396,9 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.src_f4 = c.src_f4.as<float4>();
   a.src_d4 = c.src_d4.as<double4>();
   a.node_f4 = c.node_f4.as<float4>();
+  a.node_mq = c.node_mq.as<float4>();
   a.src_u4 = c.src_u4.as<double4>();
+  a.prev = prev_acc;
   double* acc = c.tree_acc.as<double>();
   a.out_x = acc;
   a.out_y = acc + nt;
@@ -1168,6 +1408,16 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.work = c.work_counter.as<uint32_t>();
   a.status = c.status.as<uint32_t>();
   a.poly = c.poly;
+  a.dpoly = c.dpoly;
+  a.ddpoly = c.ddpoly;
+  {
+    const double rs2 = c.rs * c.rs;
+    const double i5 = 1.0 / (16.0 * rs2 * rs2 * c.rs), i7 = 1.0 / (32.0 * rs2 * rs2 * rs2 * c.rs);
+    a.inv_16rs5_f = static_cast<float>(i5);
+    a.inv_32rs7_f = static_cast<float>(i7);
+    a.mult_f32 = (i5 >= FLT_MIN && i5 <= 1.0e30 && i7 >= FLT_MIN && i7 <= 1.0e30) ? 1 : 0;
+    a.mpoly12 = (c.dpoly.terms <= 12 && c.ddpoly.terms <= 12) ? 1 : 0;
+  }
   a.wp = wp;
   const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
   const bool eps_zero = wp.eps == 0.0;
@@ -1176,11 +1426,16 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     // positions base..base+31 and self pairs are excluded by the lane mask
     const bool contiguous = active == nullptr && tx == nullptr && nt == n;
     const bool diag = c.cfg.diagnostics != 0;
-#define CHUI_WALK_DISPATCH(EPS, TERMS)                                                               \
-    if (diag) return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, true, true>, a, s)     \
-                                : launchPersistent(walkFastKernel<EPS, TERMS, true, false>, a, s);   \
-    return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, false, true>, a, s)              \
-                      : launchPersistent(walkFastKernel<EPS, TERMS, false, false>, a, s);
+    const int mode = wp.policy == CHUI_TREEPM_POLICY_ADAPTIVE ? 2 : (wp.criterion == 2 && prev_acc ? 1 : 0);
+#define CHUI_WALK_DISPATCH2(EPS, TERMS, ADP)                                                           \
+    if (diag) return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, true, true, ADP>, a, s)     \
+                                : launchPersistent(walkFastKernel<EPS, TERMS, true, false, ADP>, a, s);   \
+    return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP>, a, s)              \
+                      : launchPersistent(walkFastKernel<EPS, TERMS, false, false, ADP>, a, s);
+#define CHUI_WALK_DISPATCH(EPS, TERMS)                  \
+    if (mode == 2) { CHUI_WALK_DISPATCH2(EPS, TERMS, 2) } \
+    if (mode == 1) { CHUI_WALK_DISPATCH2(EPS, TERMS, 1) } \
+    CHUI_WALK_DISPATCH2(EPS, TERMS, 0)
     if (c.poly.terms <= 12) {
       if (eps_zero) { CHUI_WALK_DISPATCH(true, 12) }
       CHUI_WALK_DISPATCH(false, 12)
@@ -1188,6 +1443,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     if (eps_zero) { CHUI_WALK_DISPATCH(true, kPolyMaxTerms) }
     CHUI_WALK_DISPATCH(false, kPolyMaxTerms)
 #undef CHUI_WALK_DISPATCH
+#undef CHUI_WALK_DISPATCH2
   }
   return launchWalk<false, false>(a, s);
 }

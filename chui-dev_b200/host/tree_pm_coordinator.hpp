@@ -38,6 +38,8 @@ enum class PmAssignmentScheme { kCic, kTsc };
 enum class TreeOpeningCriterion { kBarnesHutGeometric, kBarnesHutComDistance, kRelativeForceError };
 enum class TreeMultipoleOrder { kMonopole = 0, kQuadrupole = 2 };
 enum class TreePmAcceptancePolicy { kStrictReference, kAdaptiveRelative };
+enum class TreePmAdaptiveErrorEstimator { kResidualDerivative, kRelativeMonopole };
+enum class TreePmCutoffNodePolicy { kContainNode, kComDistance };
 enum class Precision { kMixed, kFp64 };
 
 // The option fields the periodic TreePM path consumes (tree_pm_coupling.hpp:243-332,
@@ -62,6 +64,8 @@ struct TreeGravityOptions {
   TreeMultipoleOrder multipole_order = TreeMultipoleOrder::kQuadrupole;
   double gravitational_constant_code = 1.0;
   std::size_t max_leaf_size = 16;
+  double relative_force_tolerance = 0.005;
+  double relative_force_acceleration_floor_code = 1.0e-30;
   TreeSofteningPolicy softening{};
 };
 
@@ -75,6 +79,9 @@ struct TreePmOptions {
   TreeGravityOptions tree_options{};
   TreePmSplitPolicy split_policy{};
   TreePmAcceptancePolicy acceptance_policy = TreePmAcceptancePolicy::kStrictReference;
+  double adaptive_maximum_opening_angle = 0.25;
+  TreePmAdaptiveErrorEstimator adaptive_error_estimator = TreePmAdaptiveErrorEstimator::kResidualDerivative;
+  TreePmCutoffNodePolicy cutoff_node_policy = TreePmCutoffNodePolicy::kContainNode;
   Precision precision = Precision::kMixed;  // B200 extension: FP64 runs the same solver in double
   int device = 0;
 };
@@ -202,9 +209,8 @@ class TreePmCoordinator {
       throw std::invalid_argument("TreePM force accumulator spans must have matching active-set extent");
     }
     if (!accumulator.previous_acceleration_magnitude_code.empty() &&
-        options.tree_options.opening_criterion == TreeOpeningCriterion::kRelativeForceError) {
-      throw std::invalid_argument(
-          "B200 TreePM implements the relative-force-error criterion only without previous accelerations");
+        accumulator.previous_acceleration_magnitude_code.size() != targets) {
+      throw std::invalid_argument("TreePM force accumulator spans must have matching active-set extent");
     }
     configure(options);
     chui_treepm_sources src{};
@@ -219,6 +225,9 @@ class TreePmCoordinator {
     acc.accel_x = accumulator.accel_x_comoving.data();
     acc.accel_y = accumulator.accel_y_comoving.data();
     acc.accel_z = accumulator.accel_z_comoving.data();
+    if (!accumulator.previous_acceleration_magnitude_code.empty()) {
+      acc.previous_acceleration_magnitude = accumulator.previous_acceleration_magnitude_code.data();
+    }
     if (!accumulator.target_pos_x_comoving.empty()) {
       acc.target_x = accumulator.target_pos_x_comoving.data();
       acc.target_y = accumulator.target_pos_y_comoving.data();
@@ -334,7 +343,17 @@ class TreePmCoordinator {
     c.assignment_scheme = o.pm_options.assignment_scheme == PmAssignmentScheme::kTsc ? CHUI_TREEPM_TSC : CHUI_TREEPM_CIC;
     c.window_deconvolution = o.pm_options.enable_window_deconvolution ? 1 : 0;
     c.softening = o.tree_options.softening.epsilon_comoving;
-    c.acceptance_policy = o.acceptance_policy == TreePmAcceptancePolicy::kStrictReference ? 0 : 1;
+    c.acceptance_policy = o.acceptance_policy == TreePmAcceptancePolicy::kStrictReference ? CHUI_TREEPM_POLICY_STRICT
+                                                                                        : CHUI_TREEPM_POLICY_ADAPTIVE;
+    c.adaptive_error_estimator = o.adaptive_error_estimator == TreePmAdaptiveErrorEstimator::kRelativeMonopole
+                                     ? CHUI_TREEPM_ESTIMATOR_RELATIVE_MONOPOLE
+                                     : CHUI_TREEPM_ESTIMATOR_RESIDUAL_DERIVATIVE;
+    c.cutoff_node_policy = o.cutoff_node_policy == TreePmCutoffNodePolicy::kComDistance
+                               ? CHUI_TREEPM_CUTOFF_COM_DISTANCE
+                               : CHUI_TREEPM_CUTOFF_CONTAIN_NODE;
+    c.adaptive_maximum_opening_angle = o.adaptive_maximum_opening_angle;
+    c.relative_force_tolerance = o.tree_options.relative_force_tolerance;
+    c.relative_force_acceleration_floor = o.tree_options.relative_force_acceleration_floor_code;
     c.precision = o.precision == Precision::kFp64 ? CHUI_TREEPM_FP64 : CHUI_TREEPM_MIXED;
     c.device = o.device;
     // split scale and cutoff are in units of the mean mesh spacing (gravity_runtime.cpp:586-590)

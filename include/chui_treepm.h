@@ -47,6 +47,11 @@ enum {
   CHUI_TREEPM_OPEN_COM_DISTANCE = 1,  /* TreeOpeningCriterion::kBarnesHutComDistance */
   CHUI_TREEPM_OPEN_RELATIVE = 2       /* TreeOpeningCriterion::kRelativeForceError */
 };
+/* TreePmAcceptancePolicy, TreePmAdaptiveErrorEstimator, TreePmCutoffNodePolicy
+ * (include/cosmosim/gravity/tree_pm_coupling.hpp:172-199) */
+enum { CHUI_TREEPM_POLICY_STRICT = 0, CHUI_TREEPM_POLICY_ADAPTIVE = 1 };
+enum { CHUI_TREEPM_ESTIMATOR_RESIDUAL_DERIVATIVE = 0, CHUI_TREEPM_ESTIMATOR_RELATIVE_MONOPOLE = 1 };
+enum { CHUI_TREEPM_CUTOFF_CONTAIN_NODE = 0, CHUI_TREEPM_CUTOFF_COM_DISTANCE = 1 };
 
 /* Solver configuration: the `.param.txt` [numerics] treepm_* knobs
  * (include/cosmosim/core/config.hpp:776-821) after GravityRuntimeImpl's
@@ -64,11 +69,18 @@ typedef struct {
   int32_t window_deconvolution;               /* treepm_enable_window_deconvolution */
   double gravitational_constant;              /* G in code units (PM and tree share it) */
   double softening;                           /* Plummer epsilon, comoving (gravity_softening_kpc_comoving * 1e-3) */
-  int32_t acceptance_policy;                  /* 0 strict reference (only policy implemented) */
+  int32_t acceptance_policy;                  /* CHUI_TREEPM_POLICY_*: treepm_adaptive_acceptance_enabled */
   int32_t precision;                          /* CHUI_TREEPM_MIXED or CHUI_TREEPM_FP64 */
   int32_t device;                             /* CUDA device ordinal */
   int32_t diagnostics;                        /* 1: per-pair counters and nearest-pair r^2 (default);
                                                  0: skipped in the walk (production timing) */
+  /* adaptive-relative policy (TreePmOptions, tree_pm_coupling.hpp:243-332) */
+  int32_t adaptive_error_estimator;           /* CHUI_TREEPM_ESTIMATOR_*: treepm_adaptive_error_estimator */
+  int32_t cutoff_node_policy;                 /* CHUI_TREEPM_CUTOFF_*: treepm_cutoff_node_policy */
+  double adaptive_maximum_opening_angle;      /* (0, 1]; 0.25 */
+  /* relative criteria (TreeGravityOptions, tree_gravity.hpp:30-43) */
+  double relative_force_tolerance;            /* alpha; 0.005 */
+  double relative_force_acceleration_floor;   /* code units; 1e-30 */
 } chui_treepm_config;
 
 /* Counters named as TreePmTraversalCounters (tree_pm_coupling.hpp:39-87) plus
@@ -107,6 +119,10 @@ typedef struct {
   double *long_range_x, *long_range_y, *long_range_z;
   double *short_range_x, *short_range_y, *short_range_z;
   double *nearest_pair_r2;
+  /* previous_acceleration_magnitude_code: per active slot |a_previous| for the
+   * relative criteria, or NULL (no history). Non-finite entries mean "no
+   * history" for that target: the COM-distance fallback. */
+  const double *previous_acceleration_magnitude;
 } chui_treepm_accumulator;
 
 /* Defaults of TreePmOptions / TreeGravityOptions (tree_gravity.hpp:30-43,

@@ -1,6 +1,7 @@
 """Host-side checks that need no GPU: the C-ABI library exports every entry
 point include/chui_treepm.h declares, the `.param.txt` knob mapping, the
 synthetic IC generators and the FP32 kernel polynomial."""
+import ctypes as C
 import os
 import re
 
@@ -37,6 +38,34 @@ def test_config_defaults_match_reference_defaults():
     assert _abi.load().chui_treepm_config_default(c) == 0
     assert (c.pm_grid_nx, c.asmth_cells, c.rcut_cells, c.opening_theta, c.max_leaf_size) == (16, 1.25, 6.25, 0.7, 16)
     assert c.opening_criterion == _abi.OPEN_COM_DISTANCE and c.multipole_order == 2
+    # TreePmOptions / TreeGravityOptions defaults (tree_pm_coupling.hpp:243-332, tree_gravity.hpp:30-43)
+    assert c.acceptance_policy == _abi.POLICY_STRICT
+    assert c.adaptive_error_estimator == _abi.ESTIMATOR_RESIDUAL_DERIVATIVE
+    assert c.cutoff_node_policy == _abi.CUTOFF_CONTAIN_NODE
+    assert (c.adaptive_maximum_opening_angle, c.relative_force_tolerance,
+            c.relative_force_acceleration_floor) == (0.25, 0.005, 1e-30)
+    # the Python mirror carries the same defaults
+    py = ct.TreePmConfig().to_c()
+    for name, _ in _abi.Config._fields_:
+        if name not in ("pm_grid_nx", "pm_grid_ny", "pm_grid_nz", "box_x", "box_y", "box_z", "window_deconvolution",
+                        "diagnostics"):
+            assert getattr(py, name) == getattr(c, name), name
+
+
+@pytest.mark.parametrize("field,value", [("adaptive_maximum_opening_angle", 1.5),
+                                         ("adaptive_maximum_opening_angle", 0.0),
+                                         ("relative_force_tolerance", -1.0),
+                                         ("relative_force_acceleration_floor", 0.0),
+                                         ("acceptance_policy", 2), ("adaptive_error_estimator", 5),
+                                         ("cutoff_node_policy", -1)])
+def test_invalid_adaptive_options_are_rejected(field, value):
+    # validateTreePmOptions (tree_pm_coupling.cpp:300-340) runs before any device work
+    c = _abi.Config()
+    lib = _abi.load()
+    lib.chui_treepm_config_default(c)
+    setattr(c, field, value)
+    h = C.c_void_p()
+    assert lib.chui_treepm_create(C.byref(c), C.byref(h)) == _abi.EINVAL
 
 
 def test_kdk_static_factors():
@@ -75,6 +104,28 @@ def test_param_deck_mapping():
     assert abs(c.mesh_spacing - 20.0 / 32) < 1e-12
     with pytest.raises(ValueError):
         ct.config_from_param_text(DECK.replace("geometric", "bogus"))
+    assert c.acceptance_policy == _abi.POLICY_STRICT
+
+
+FAST_DECK = DECK + """treepm_adaptive_acceptance_enabled = true
+treepm_adaptive_error_estimator = relative_monopole
+treepm_cutoff_node_policy = com_distance
+treepm_adaptive_maximum_opening_angle = 1.0
+treepm_tree_relative_force_tolerance = 0.0025
+"""
+
+
+def test_param_deck_adaptive_keys():
+    c = ct.config_from_param_text(FAST_DECK)
+    assert c.acceptance_policy == _abi.POLICY_ADAPTIVE
+    assert c.adaptive_error_estimator == _abi.ESTIMATOR_RELATIVE_MONOPOLE
+    assert c.cutoff_node_policy == _abi.CUTOFF_COM_DISTANCE
+    assert (c.adaptive_maximum_opening_angle, c.relative_force_tolerance) == (1.0, 0.0025)
+    assert c.relative_force_acceleration_floor == 1e-30
+    with pytest.raises(ValueError):
+        ct.config_from_param_text(FAST_DECK.replace("relative_monopole", "bogus"))
+    with pytest.raises(ValueError):
+        ct.config_from_param_text(FAST_DECK.replace("= com_distance", "= bogus"))
 
 
 def test_zeldovich_lattice_statistics():
