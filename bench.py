@@ -263,6 +263,35 @@ def timed_steps(torch, solver, t, acc, factors, steps, warmup, dist=None):
     return e0.elapsed_time(e1), acc, stats, launches
 
 
+def adaptive_fast_deck(torch, ct, w, device, t, r_ref, repeats=3) -> dict:
+    """One force under the adaptive relative policy (the reference's
+    configs/treepm_evolved_snapshot_fast deck settings), production walk:
+    device time of the solve and its error against the strict FP64 forces."""
+    cfg = make_config(w, ct._abi.MIXED, device, diagnostics=0)
+    cfg.acceptance_policy = ct._abi.POLICY_ADAPTIVE
+    cfg.adaptive_error_estimator = ct._abi.ESTIMATOR_RELATIVE_MONOPOLE
+    cfg.cutoff_node_policy = ct._abi.CUTOFF_COM_DISTANCE
+    cfg.adaptive_maximum_opening_angle = 1.0
+    cfg.relative_force_tolerance = 0.0025
+    prev = torch.sqrt(r_ref["ax"] ** 2 + r_ref["ay"] ** 2 + r_ref["az"] ** 2)
+    n = len(t["x"])
+    with ct.TreePmCoordinator(cfg) as s:
+        r = s.solve_active_set(t["x"], t["y"], t["z"], t["m"], previous_acceleration=prev)
+        total, walk = [], []
+        for _ in range(repeats):
+            r = s.solve_active_set(t["x"], t["y"], t["z"], t["m"], previous_acceleration=prev)
+            total.append(s.last_stats["total_ms"])
+            walk.append(s.last_stats["walk_ms"])
+    e = rel_errors([r[k].cpu().numpy() for k in ("ax", "ay", "az")],
+                   [r_ref[k].cpu().numpy() for k in ("ax", "ay", "az")])
+    ms = float(np.median(total))
+    return {"deck": "adaptive relative_monopole, cutoff nodes com_distance, alpha 0.0025, max angle 1.0",
+            "value": n / (ms * 1e-3), "unit": "particle-forces/s (one force, device time)",
+            "force_ms": ms, "walk_ms": float(np.median(walk)),
+            "vs_fp64_strict": {"median_rel": float(np.median(e)), "p99_rel": float(np.percentile(e, 99)),
+                               "p9999_rel": float(np.percentile(e, 99.99)), "max_rel": float(np.max(e))}}
+
+
 def run_gpu(args) -> int:
     import torch
     import chui_treepm as ct
@@ -300,6 +329,12 @@ def run_gpu(args) -> int:
     stats0 = dict(fp64.last_stats)
     log(f"[rank {rank}] mixed vs fp64 median {np.median(err):.3e} p99 {np.percentile(err, 99):.3e}; "
         f"stats {stats0}")
+
+    # the reference's production fast deck on the same state: adaptive relative
+    # monopole, COM-distance cutoff nodes, alpha 0.0025, maximum angle 1.0, with
+    # the FP64 strict solve's |a| as the acceleration history
+    adaptive = adaptive_fast_deck(torch, ct, w, local, t, r_d)
+    log(f"[rank {rank}] adaptive fast deck {adaptive}")
 
     # FP64-on-GPU comparator (same step definition, fewer repetitions)
     tf = {k: v.clone() for k, v in t.items()}
@@ -381,6 +416,7 @@ def run_gpu(args) -> int:
             "counters": {k: stats0[k] for k in ("direct_pair_evaluations", "visited_nodes",
                                                 "accepted_internal_multipoles", "node_count", "maximum_depth")},
             "adjoint": adj,
+            "adaptive_fast_deck": adaptive,
             "fp64_checks_end": {"momentum": [float(v) for v in checks["momentum"]],
                                 "net_force": [float(v) for v in checks["net_force"]],
                                 "kinetic_energy": checks["kinetic_energy"], "mass": checks["mass"]},
