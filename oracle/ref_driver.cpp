@@ -103,6 +103,8 @@ struct Problem {
   std::int64_t policy = 0, estimator = 0, cutoff_policy = 0, has_prev = 0;
   double adaptive_angle = 0.25, rel_tol = 0.005, accel_floor = 1.0e-30;
   std::vector<double> prev;
+  // optional "CHUIGRP1" block after it: group walk and Gaussian pair lookup
+  std::int64_t group_walk = 0, gaussian_lookup = 0;
 };
 
 Problem readProblem(const char* path) {
@@ -159,6 +161,11 @@ Problem readProblem(const char* path) {
     p.rel_tol = r.get<double>();
     p.accel_floor = r.get<double>();
     if (p.has_prev) p.prev = r.vec<double>(static_cast<std::size_t>(p.n_active ? p.n_active : p.n));
+    if (std::fread(tail, 1, 8, f) == 8) {
+      if (std::memcmp(tail, "CHUIGRP1", 8) != 0) throw std::runtime_error("bad trailing block");
+      p.group_walk = r.get<std::int64_t>();
+      p.gaussian_lookup = r.get<std::int64_t>();
+    }
   }
   std::fclose(f);
   return p;
@@ -191,6 +198,8 @@ cg::TreePmOptions makeOptions(const Problem& p) {
                                                 : cg::TreePmAdaptiveErrorEstimator::kResidualDerivative;
   o.cutoff_node_policy = p.cutoff_policy == 1 ? cg::TreePmCutoffNodePolicy::kComDistance
                                               : cg::TreePmCutoffNodePolicy::kContainNode;
+  o.group_walk_enabled = p.group_walk != 0;
+  o.gaussian_pair_lookup_enabled = p.gaussian_lookup != 0;
   o.split_policy = cg::makeTreePmSplitPolicyFromMeshSpacing(
       p.asmth, p.rcut,
       std::cbrt((p.box[0] / static_cast<double>(p.mesh[0])) * (p.box[1] / static_cast<double>(p.mesh[1])) *

@@ -60,6 +60,8 @@ class RefProblem:
     rel_tol: float = 0.005
     accel_floor: float = 1e-30
     prev_acc: np.ndarray | None = None  # per active target |a_previous|
+    group_walk: int = 0       # TreePmOptions::group_walk_enabled
+    gaussian_lookup: int = 0  # TreePmOptions::gaussian_pair_lookup_enabled
 
 
 def write_problem(path: str, p: RefProblem) -> None:
@@ -81,7 +83,8 @@ def write_problem(path: str, p: RefProblem) -> None:
                   p.vz if p.vz is not None else zeros):
             f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
         f.write(active.tobytes())
-        if p.policy or p.prev_acc is not None or p.rel_tol != 0.005 or p.accel_floor != 1e-30:
+        grp = p.group_walk or p.gaussian_lookup
+        if p.policy or p.prev_acc is not None or p.rel_tol != 0.005 or p.accel_floor != 1e-30 or grp:
             f.write(b"CHUIADP1")
             f.write(struct.pack("<4q", p.policy, p.estimator, p.cutoff_policy, int(p.prev_acc is not None)))
             f.write(struct.pack("<3d", p.adaptive_angle, p.rel_tol, p.accel_floor))
@@ -90,6 +93,9 @@ def write_problem(path: str, p: RefProblem) -> None:
                 if len(prev) != (len(active) if len(active) else n):
                     raise ValueError("prev_acc needs one entry per active target")
                 f.write(prev.tobytes())
+            if grp:
+                f.write(b"CHUIGRP1")
+                f.write(struct.pack("<2q", p.group_walk, p.gaussian_lookup))
 
 
 class _Buf:

@@ -690,12 +690,60 @@ static int within_cutoff(double d2, double cutoff, double cutoff2) {
   return d2 <= cutoff2;
 }
 
+/* TreePmGaussianCoefficientTable (tree_pm_split_kernel.hpp:130-186): cubic
+ * Hermite interpolation of H(t) = L(sqrt t)/t^(3/2) on t in [0, 64], 4096 cells,
+ * slopes pre-scaled by the cell width. */
+#define GAUSS_CELLS 4096
+static const double k_gauss_step = 64.0 / GAUSS_CELLS;
+typedef struct {
+  double value[GAUSS_CELLS + 1];
+  double slope[GAUSS_CELLS + 1];
+} gauss_table;
+
+static void gauss_table_init(gauss_table *g) {
+  const double two_inv_sqrt_pi = 1.12837916709551257389615890312154517;
+  for (int i = 0; i <= GAUSS_CELLS; ++i) {
+    const double t = (double)i * k_gauss_step;
+    const double q = sqrt(t);
+    g->value[i] = i == 0 ? coefficient_series(0.0) : oracle_long_range_factor(q, 0.5) / (t * q);
+    const double derivative = i == 0 ? -4.0 * k_inv_sqrt_pi / 5.0 : (two_inv_sqrt_pi * exp(-t) - 1.5 * g->value[i]) / t;
+    g->slope[i] = k_gauss_step * derivative;
+  }
+}
+
+static double gauss_hermite(const gauss_table *g, double t) {
+  const double cell = t / k_gauss_step;
+  const size_t i = (size_t)cell;
+  const double u = cell - (double)i;
+  const double u2 = u * u;
+  const double u3 = u2 * u;
+  return (2 * u3 - 3 * u2 + 1) * g->value[i] + (u3 - 2 * u2 + u) * g->slope[i] + (-2 * u3 + 3 * u2) * g->value[i + 1] +
+         (u3 - u2) * g->slope[i + 1];
+}
+
+/* dimensionlessCoefficient (tree_pm_split_kernel.hpp:150-164) */
+static double gauss_coefficient(const gauss_table *g, double t) {
+  if (t < 0.015625) return coefficient_series(t);
+  if (!(t < 64.0)) return long_range_inv_r3(sqrt(t), 0.5);
+  return gauss_hermite(g, t);
+}
+
+/* longRangeInvR3 of the table (tree_pm_split_kernel.hpp:143-149) */
+static double gauss_long_inv_r3(const gauss_table *g, double r2, double a) {
+  const double t = 0.25 * (r2 / a) / a;
+  if (!(t >= 0.0) || t >= 64.0) return long_range_inv_r3(sqrt(r2), a);
+  return ((0.125 * gauss_coefficient(g, t) / a) / a) / a;
+}
+
 typedef struct {
   const oracle_tree *t;
   const oracle_params *p;
   const double *ox, *oy, *oz, *om; /* caller positions/masses gathered into tree order */
   double src_lo[3], src_hi[3], node_lo[3], node_hi[3];
   double rs, cutoff, cutoff2;
+  const gauss_table *gt;      /* Gaussian pair lookup (NULL: analytic) */
+  double inv_2a2, inv_8a3;    /* 1/(2 r_s)^2, 1/(8 r_s^3) */
+  int scaling_ok;             /* both normal (tree_pm_coupling.cpp:3922-3925) */
 } walk_ctx;
 
 /* monopolePlusQuadrupoleAccelPeriodicReference, tree_pm_coupling.cpp:743-827 */
@@ -934,7 +982,17 @@ static void walk_target(const walk_ctx *w, double px, double py, double pz, uint
           ++cnt->pairs;
           if (sx == 0.0 && sy == 0.0 && sz == 0.0) continue;
           const double pe = w->p->epsilon > eps_t ? w->p->epsilon : eps_t;
-          const double f = oracle_residual_inv_r3(sr2, pe, w->rs) * w->p->G;
+          double res;
+          if (w->gt != NULL && sr2 > 0.0) {
+            /* Gaussian pair lookup (tree_pm_coupling.cpp:4221-4226) */
+            const double gt_t = w->scaling_ok ? sr2 * w->inv_2a2 : 64.0;
+            const double long_inv_r3 =
+                gt_t < 64.0 ? gauss_coefficient(w->gt, gt_t) * w->inv_8a3 : gauss_long_inv_r3(w->gt, sr2, w->rs);
+            res = softened_inv_r3(sr2, pe) - long_inv_r3;
+          } else {
+            res = oracle_residual_inv_r3(sr2, pe, w->rs);
+          }
+          const double f = res * w->p->G;
           acc[0] += f * w->om[s] * sx;
           acc[1] += f * w->om[s] * sy;
           acc[2] += f * w->om[s] * sz;
@@ -955,6 +1013,230 @@ static void walk_target(const walk_ctx *w, double px, double py, double pz, uint
   out[1] = acc[1];
   out[2] = acc[2];
   out[3] = nearest;
+}
+
+
+/* ---------------------------------------------------------- group walk */
+/* Opt-in group walk (TreePmOptions::group_walk_enabled, adaptive relative
+ * monopole with the Gaussian pair table): internal/tree_pm_group_walk.hpp and
+ * its driver tree_pm_coupling.cpp:4287-4560. Legacy grouping only
+ * (group_walk_target_group_size = 0: the active targets of one source leaf,
+ * consecutive in visit order inside one residual block of 64). */
+
+/* treePmGroupNearestImage, tree_pm_group_walk.hpp:70-76 */
+static double group_nearest_image(double delta, double length) {
+  if (!(length > 0.0)) return delta;
+  return delta - length * nearbyint(delta / length);
+}
+
+typedef struct {
+  uint32_t *mult;
+  size_t n_mult;
+  uint32_t *leaf_begin, *leaf_end;
+  double *leaf_dx, *leaf_dy, *leaf_dz, *leaf_h;
+  size_t n_leaf;
+} group_list;
+
+/* buildTreePmGroupInteractionList, tree_pm_group_walk.hpp:78-154 */
+static void group_build_list(const walk_ctx *w, const double center[3], const double half[3], double a_min,
+                             uint32_t *stack, size_t stack_cap, group_list *out, oracle_counters *cnt) {
+  const oracle_tree *t = w->t;
+  const int contain = !(w->p->policy == 1 && w->p->cutoff_policy == 1);
+  const double rel_over_g = w->p->rel_tol / w->p->G;
+  const double angle2 = w->p->adaptive_angle * w->p->adaptive_angle;
+  out->n_mult = out->n_leaf = 0;
+  if (t->n_nodes == 0) return;
+  size_t sp = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    const uint32_t node = stack[--sp];
+    ++cnt->visited;
+    const double h = t->half[node];
+    const double dc[3] = {group_nearest_image(t->cx[node] - center[0], w->p->box[0]),
+                          group_nearest_image(t->cy[node] - center[1], w->p->box[1]),
+                          group_nearest_image(t->cz[node] - center[2], w->p->box[2])};
+    double gap2 = 0.0, far2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      const double ad = fabs(dc[a]);
+      const double gap = ad - h - half[a] > 0.0 ? ad - h - half[a] : 0.0;
+      const double far = ad + h + half[a];
+      gap2 += gap * gap;
+      far2 += far * far;
+    }
+    if (gap2 > w->cutoff2) {
+      ++cnt->pruned;
+      continue;
+    }
+    if (t->child_count[node] == 0) {
+      ++cnt->leaves;
+      ++cnt->accepted;
+      const size_t k = out->n_leaf++;
+      out->leaf_begin[k] = t->pbegin[node];
+      out->leaf_end[k] = t->pbegin[node] + t->pcount[node];
+      out->leaf_dx[k] = dc[0];
+      out->leaf_dy[k] = dc[1];
+      out->leaf_dz[k] = dc[2];
+      out->leaf_h[k] = h;
+      continue;
+    }
+    int accept = gap2 > 0.0 && (!contain || far2 <= w->cutoff2);
+    if (accept) {
+      const double dm[3] = {group_nearest_image(t->comx[node] - center[0], w->p->box[0]),
+                            group_nearest_image(t->comy[node] - center[1], w->p->box[1]),
+                            group_nearest_image(t->comz[node] - center[2], w->p->box[2])};
+      double r_min2 = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        const double gap = fabs(dm[a]) - half[a] > 0.0 ? fabs(dm[a]) - half[a] : 0.0;
+        r_min2 += gap * gap;
+      }
+      const double width2 = 4.0 * h * h;
+      accept = r_min2 > 0.0 && width2 < angle2 * r_min2 &&
+               t->mass[node] * width2 <= rel_over_g * a_min * r_min2 * r_min2;
+    }
+    if (accept) {
+      ++cnt->multipoles;
+      ++cnt->accepted;
+      out->mult[out->n_mult++] = node;
+    } else {
+      ++cnt->opened;
+      for (int o = 7; o >= 0; --o) {
+        const uint32_t c = t->child_index[8 * node + o];
+        if (c != 0xFFFFFFFFu && sp < stack_cap) stack[sp++] = c;
+      }
+    }
+  }
+}
+
+/* accumulateTreePmGroupPairsImpl, tree_pm_group_walk.hpp:191-246 (owned
+ * targets: the self pair excluded by source identity, distinct coincident
+ * sources counted) */
+static void group_pairs(const walk_ctx *w, double px, double py, double pz, size_t begin, size_t end,
+                        uint32_t self_row, double acc[3], uint64_t *pairs, double *nearest) {
+  const oracle_tree *t = w->t;
+  const double lx = w->p->box[0], ly = w->p->box[1], lz = w->p->box[2];
+  const double hx = 0.5 * lx, hy = 0.5 * ly, hz = 0.5 * lz;
+  const double t_limit = nextafter(64.0, 0.0);
+  const double eps2 = w->p->epsilon * w->p->epsilon;
+  double sx = 0.0, sy = 0.0, sz = 0.0, near = *nearest;
+  uint64_t counted = 0;
+  for (size_t j = begin; j < end; ++j) {
+    double dx = w->ox[j] - px, dy = w->oy[j] - py, dz = w->oz[j] - pz;
+    dx = dx > hx ? dx - lx : (dx < -hx ? dx + lx : dx);
+    dy = dy > hy ? dy - ly : (dy < -hy ? dy + ly : dy);
+    dz = dz > hz ? dz - lz : (dz < -hz ? dz + lz : dz);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const int is_self = self_row != 0xFFFFFFFFu && t->sorted[j] == self_row;
+    const int inside = !is_self && r2 <= w->cutoff2;
+    const double tt = r2 * w->inv_2a2 < t_limit ? r2 * w->inv_2a2 : t_limit;
+    const double coefficient_long = gauss_hermite(w->gt, tt) * w->inv_8a3;
+    const double d = r2 + eps2;
+    const double softened = 1.0 / (d * sqrt(d));
+    const double factor = inside && r2 > 0.0 ? (softened - coefficient_long) * w->p->G * w->om[j] : 0.0;
+    sx += factor * dx;
+    sy += factor * dy;
+    sz += factor * dz;
+    counted += inside ? 1u : 0u;
+    near = fmin(near, inside ? r2 : near);
+  }
+  *nearest = near;
+  acc[0] += sx;
+  acc[1] += sy;
+  acc[2] += sz;
+  *pairs += counted;
+}
+
+/* One group through the shared list (evaluate_target_group,
+ * tree_pm_coupling.cpp:4326-4422). Returns 0 when the group falls back to
+ * per-target walks (history or geometry), before any accumulation. */
+static int group_evaluate(const walk_ctx *w, const double *tx, const double *ty, const double *tz,
+                          const uint32_t *rows, const double *prev, const int64_t *slots, size_t count,
+                          uint32_t *stack, size_t stack_cap, group_list *list, double *res, oracle_counters *cnt) {
+  const double len[3] = {w->p->box[0], w->p->box[1], w->p->box[2]};
+  double a_min = INFINITY, ref[3] = {0, 0, 0}, low[3] = {0, 0, 0}, high[3] = {0, 0, 0};
+  for (size_t i = 0; i < count; ++i) {
+    const int64_t k = slots[i];
+    const double pv = prev ? prev[k] : NAN;
+    if (!(isfinite(pv) && pv > w->p->accel_floor)) return 0;
+    if (pv < a_min) a_min = pv;
+    const double pos[3] = {tx[k], ty[k], tz[k]};
+    for (int a = 0; a < 3; ++a) {
+      if (!metric_make(w->src_lo[a], w->src_hi[a], pos[a], len[a]).bounded) return 0;
+      if (i == 0) {
+        ref[a] = pos[a];
+        continue;
+      }
+      const double delta = group_nearest_image(pos[a] - ref[a], len[a]);
+      if (delta < low[a]) low[a] = delta;
+      if (delta > high[a]) high[a] = delta;
+    }
+  }
+  double center[3], half[3];
+  for (int a = 0; a < 3; ++a) {
+    center[a] = ref[a] + 0.5 * (low[a] + high[a]);
+    half[a] = 0.5 * (high[a] - low[a]);
+  }
+  group_build_list(w, center, half, a_min, stack, stack_cap, list, cnt);
+  const int com_cutoff = w->p->policy == 1 && w->p->cutoff_policy == 1;
+  const double cull2 = w->cutoff2 * (1.0 + 1.0e-9);
+  for (size_t i = 0; i < count; ++i) {
+    const int64_t k = slots[i];
+    const double px = tx[k], py = ty[k], pz = tz[k];
+    double acc[3] = {0.0, 0.0, 0.0}, nearest = INFINITY;
+    uint64_t pairs = 0;
+    const double toff[3] = {group_nearest_image(px - center[0], len[0]), group_nearest_image(py - center[1], len[1]),
+                            group_nearest_image(pz - center[2], len[2])};
+    /* accumulateTreePmGroupCulledLeaves, tree_pm_group_walk.hpp:284-341 */
+    size_t run_begin = 0, run_end = 0;
+    int run_open = 0;
+    for (size_t l = 0; l < list->n_leaf; ++l) {
+      const double h = list->leaf_h[l];
+      const double off[3] = {list->leaf_dx[l] - toff[0], list->leaf_dy[l] - toff[1], list->leaf_dz[l] - toff[2]};
+      double g2 = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        const double hl = 0.5 * len[a];
+        const double d = off[a] > hl ? off[a] - len[a] : (off[a] < -hl ? off[a] + len[a] : off[a]);
+        const double g = fabs(d) - h > 0.0 ? fabs(d) - h : 0.0;
+        g2 += g * g;
+      }
+      if (g2 > cull2) continue;
+      const size_t b = list->leaf_begin[l], e = list->leaf_end[l];
+      if (run_open && run_end == b) {
+        run_end = e;
+        continue;
+      }
+      if (run_open) group_pairs(w, px, py, pz, run_begin, run_end, rows[k], acc, &pairs, &nearest);
+      run_begin = b;
+      run_end = e;
+      run_open = 1;
+    }
+    if (run_open) group_pairs(w, px, py, pz, run_begin, run_end, rows[k], acc, &pairs, &nearest);
+    cnt->pairs += pairs;
+    metric nm[3];
+    const double pos[3] = {px, py, pz};
+    for (int a = 0; a < 3; ++a) nm[a] = metric_make(w->node_lo[a], w->node_hi[a], pos[a], len[a]);
+    const oracle_tree *t = w->t;
+    for (size_t q = 0; q < list->n_mult; ++q) {
+      const uint32_t node = list->mult[q];
+      const double dx = metric_apply(nm[0], t->comx[node] - px);
+      const double dy = metric_apply(nm[1], t->comy[node] - py);
+      const double dz = metric_apply(nm[2], t->comz[node] - pz);
+      if (com_cutoff && dx * dx + dy * dy + dz * dz > w->cutoff2) {
+        ++cnt->pruned;
+        continue;
+      }
+      multipole_force(w, node, dx, dy, dz, w->p->epsilon, acc);
+    }
+    res[4 * k + 0] = acc[0];
+    res[4 * k + 1] = acc[1];
+    res[4 * k + 2] = acc[2];
+    res[4 * k + 3] = nearest;
+  }
+  return 1;
+}
+
+static int cmp_visit(const void *a, const void *b) {
+  const uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+  return x < y ? -1 : (x > y ? 1 : 0);
 }
 
 /* solveActiveSetWithPmCadence (tree_pm_coupling.cpp:2282-3518) restricted to
@@ -1071,9 +1353,101 @@ int oracle_treepm_solve2(int64_t n, const double *x, const double *y, const doub
   w.oy = oy;
   w.oz = oz;
   w.om = om;
+  gauss_table *gt = NULL;
+  if (p->gaussian_lookup) {
+    gt = (gauss_table *)malloc(sizeof(gauss_table));
+    gauss_table_init(gt);
+  }
+  w.gt = gt;
+  w.inv_2a2 = (0.25 / rs) / rs;
+  w.inv_8a3 = ((0.125 / rs) / rs) / rs;
+  w.scaling_ok = isnormal(w.inv_2a2) && isnormal(w.inv_8a3);
   const size_t stack_cap = 1 + 7 * (size_t)t->max_depth;
   oracle_counters total;
   memset(&total, 0, sizeof(total));
+  double *res = (double *)malloc(sizeof(double) * 4 * (size_t)(na ? na : 1));
+  unsigned char *done = (unsigned char *)calloc((size_t)(na ? na : 1), 1);
+
+  /* group walk eligibility (tree_pm_coupling.cpp:3840-3870, 4282-4286) */
+  const double t_cut_group = (0.25 * w.cutoff2 / rs) / rs;
+  const int group_active = p->group_walk && p->policy == 1 && p->estimator == 1 && gt != NULL && t->n_nodes > 0 &&
+                           isfinite(t_cut_group) && t_cut_group < 63.0 && w.scaling_ok;
+  if (group_active) {
+    /* visit order: stable sort of active slots by the tree position of their row (:3808-3838) */
+    uint32_t *pos_of_row = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n ? n : 1));
+    for (int64_t s2 = 0; s2 < n; ++s2) pos_of_row[t->sorted[s2]] = (uint32_t)s2;
+    uint64_t *keyed = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(na ? na : 1));
+    uint32_t *rows = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(na ? na : 1));
+    for (int64_t k = 0; k < na; ++k) {
+      const uint32_t row = active ? active[k] : (uint32_t)k;
+      rows[k] = row;
+      const uint64_t key = (int64_t)row < n ? pos_of_row[row] : 0xFFFFFFFFu;
+      keyed[k] = (key << 32) | (uint64_t)k; /* ties keep slot order: a stable sort */
+    }
+    qsort(keyed, (size_t)na, sizeof(uint64_t), cmp_visit);
+    uint32_t *leaf_of_pos = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n ? n : 1));
+    for (int64_t s2 = 0; s2 < n; ++s2) leaf_of_pos[s2] = 0xFFFFFFFFu;
+    for (int64_t nd = 0; nd < t->n_nodes; ++nd) {
+      if (t->child_count[nd] != 0) continue;
+      for (uint32_t q = t->pbegin[nd]; q < t->pbegin[nd] + t->pcount[nd]; ++q) leaf_of_pos[q] = (uint32_t)nd;
+    }
+    const int64_t blocks = (na + 63) / 64;
+#pragma omp parallel
+    {
+      uint32_t *stack = (uint32_t *)malloc(sizeof(uint32_t) * (stack_cap + 8));
+      group_list list;
+      const size_t cap = (size_t)t->n_nodes;
+      list.mult = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+      list.leaf_begin = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+      list.leaf_end = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+      list.leaf_dx = (double *)malloc(sizeof(double) * cap);
+      list.leaf_dy = (double *)malloc(sizeof(double) * cap);
+      list.leaf_dz = (double *)malloc(sizeof(double) * cap);
+      list.leaf_h = (double *)malloc(sizeof(double) * cap);
+      int64_t slots[64];
+      oracle_counters local;
+      memset(&local, 0, sizeof(local));
+#pragma omp for schedule(dynamic, 1)
+      for (int64_t b = 0; b < blocks; ++b) {
+        const int64_t v_end = (b + 1) * 64 < na ? (b + 1) * 64 : na;
+        int64_t v = b * 64;
+        while (v < v_end) {
+          const int64_t k0 = (int64_t)(keyed[v] & 0xFFFFFFFFu);
+          const uint32_t r0 = rows[k0];
+          const uint32_t leaf = (int64_t)r0 < n ? leaf_of_pos[pos_of_row[r0]] : 0xFFFFFFFFu;
+          int64_t g_end = v + 1;
+          if (leaf != 0xFFFFFFFFu) {
+            while (g_end < v_end) {
+              const uint32_t rr = rows[(int64_t)(keyed[g_end] & 0xFFFFFFFFu)];
+              if (!((int64_t)rr < n && leaf_of_pos[pos_of_row[rr]] == leaf)) break;
+              ++g_end;
+            }
+            const size_t count = (size_t)(g_end - v);
+            for (size_t i = 0; i < count; ++i) slots[i] = (int64_t)(keyed[v + (int64_t)i] & 0xFFFFFFFFu);
+            if (group_evaluate(&w, tx, ty, tz, rows, prev_acc, slots, count, stack, stack_cap, &list, res, &local))
+              for (size_t i = 0; i < count; ++i) done[slots[i]] = 1;
+          }
+          v = g_end;
+        }
+      }
+#pragma omp critical
+      {
+        total.visited += local.visited;
+        total.accepted += local.accepted;
+        total.opened += local.opened;
+        total.pairs += local.pairs;
+        total.pruned += local.pruned;
+        total.pair_skips += local.pair_skips;
+        total.multipoles += local.multipoles;
+        total.leaves += local.leaves;
+      }
+      free(list.mult); free(list.leaf_begin); free(list.leaf_end);
+      free(list.leaf_dx); free(list.leaf_dy); free(list.leaf_dz); free(list.leaf_h);
+      free(stack);
+    }
+    free(pos_of_row); free(keyed); free(rows); free(leaf_of_pos);
+  }
+
 #pragma omp parallel
   {
     uint32_t *stack = (uint32_t *)malloc(sizeof(uint32_t) * (stack_cap + 8));
@@ -1081,19 +1455,12 @@ int oracle_treepm_solve2(int64_t n, const double *x, const double *y, const doub
     memset(&local, 0, sizeof(local));
 #pragma omp for schedule(dynamic, 64)
     for (int64_t k = 0; k < na; ++k) {
+      if (done[k]) continue;
       const uint32_t self = active ? active[k] : (uint32_t)k;
-      double res[4];
       /* history per active slot: present and finite (tree_pm_coupling.cpp:4467-4472) */
       const int avail = prev_acc != NULL && isfinite(prev_acc[k]);
       walk_target(&w, tx[k], ty[k], tz[k], self, 1, p->epsilon, avail, avail ? prev_acc[k] : 0.0, stack,
-                  stack_cap, res, &local);
-      if (ax) ax[k] = lx[k] + res[0];
-      if (ay) ay[k] = ly[k] + res[1];
-      if (az) az[k] = lz[k] + res[2];
-      if (tree_ax) tree_ax[k] = res[0];
-      if (tree_ay) tree_ay[k] = res[1];
-      if (tree_az) tree_az[k] = res[2];
-      if (nearest_r2) nearest_r2[k] = res[3];
+                  stack_cap, res + 4 * k, &local);
     }
 #pragma omp critical
     {
@@ -1108,6 +1475,18 @@ int oracle_treepm_solve2(int64_t n, const double *x, const double *y, const doub
     }
     free(stack);
   }
+  for (int64_t k = 0; k < na; ++k) {
+    if (ax) ax[k] = lx[k] + res[4 * k + 0];
+    if (ay) ay[k] = ly[k] + res[4 * k + 1];
+    if (az) az[k] = lz[k] + res[4 * k + 2];
+    if (tree_ax) tree_ax[k] = res[4 * k + 0];
+    if (tree_ay) tree_ay[k] = res[4 * k + 1];
+    if (tree_az) tree_az[k] = res[4 * k + 2];
+    if (nearest_r2) nearest_r2[k] = res[4 * k + 3];
+  }
+  free(res);
+  free(done);
+  free(gt);
   if (pm_ax) memcpy(pm_ax, lx, sizeof(double) * (size_t)na);
   if (pm_ay) memcpy(pm_ay, ly, sizeof(double) * (size_t)na);
   if (pm_az) memcpy(pm_az, lz, sizeof(double) * (size_t)na);

@@ -38,6 +38,8 @@ typedef struct {
   double adaptive_angle; /* adaptive_maximum_opening_angle */
   double rel_tol;        /* tree relative_force_tolerance (alpha) */
   double accel_floor;    /* tree relative_force_acceleration_floor_code */
+  int32_t group_walk;      /* TreePmOptions::group_walk_enabled (leaf grouping, blocks of 64) */
+  int32_t gaussian_lookup; /* TreePmOptions::gaussian_pair_lookup_enabled (Hermite pair table) */
 } oracle_params;
 
 typedef struct {

@@ -37,6 +37,8 @@ def golden_params(g):
         angle, rel_tol, floor = (float(v) for v in g["adaptive_f"])
         adaptive = dict(policy=policy, estimator=estimator, cutoff_policy=cutoff_policy,
                         adaptive_angle=angle, rel_tol=rel_tol, accel_floor=floor)
+    if "group" in g:
+        adaptive["group_walk"], adaptive["gaussian_lookup"] = (int(v) for v in g["group"])
     return oracle.make_params(box=tuple(g["box"]), mesh=tuple(int(v) for v in g["mesh"]), asmth=asmth,
                               rcut=rcut, theta=theta, g=gconst, eps=eps, leaf=leaf, scheme=scheme,
                               deconv=deconv, criterion=criterion, quadrupole=1 if order == 2 else 0,

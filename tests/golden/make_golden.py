@@ -66,6 +66,8 @@ def save(name: str, p: refio.RefProblem, r: dict, extra: dict | None = None, kee
         d["adaptive_f"] = np.array([p.adaptive_angle, p.rel_tol, p.accel_floor])
         if p.prev_acc is not None:
             d["prev_acc"] = np.asarray(p.prev_acc, dtype=np.float64)
+        if p.group_walk or p.gaussian_lookup:
+            d["group"] = np.array([p.group_walk, p.gaussian_lookup], dtype=np.int64)
     if extra:
         d.update(extra)
     np.savez_compressed(os.path.join(OUT, name + ".npz"), **d)
@@ -158,6 +160,15 @@ def main():
     p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=0, cutoff_policy=0,
                          adaptive_angle=0.5, rel_tol=0.005, prev_acc=prev[active], active=active)
     save("adaptive_residual", p, refio.run(p))
+    #    the group walk (one conservative walk per leaf of targets, Gaussian Hermite pair
+    #    table) on the fast deck, over all targets and over the active subset
+    p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=1, cutoff_policy=1,
+                         adaptive_angle=1.0, rel_tol=0.0025, prev_acc=prev, group_walk=1, gaussian_lookup=1)
+    save("group_walk", p, refio.run(p))
+    p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=1, cutoff_policy=0,
+                         adaptive_angle=0.5, rel_tol=0.005, prev_acc=prev[active], active=active,
+                         group_walk=1, gaussian_lookup=1)
+    save("group_walk_active", p, refio.run(p))
 
 
 if __name__ == "__main__":

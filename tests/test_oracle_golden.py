@@ -13,7 +13,7 @@ import oracle
 from conftest import golden_params, load_golden
 
 CASES = ["lattice16_cic", "clustered_tsc", "rect_active", "two_body", "quasi24", "duplicates", "config32",
-         "adaptive_monopole", "adaptive_residual"]
+         "adaptive_monopole", "adaptive_residual", "group_walk", "group_walk_active"]
 COUNTER_KEYS = ("visited", "accepted", "opened", "pairs", "pruned", "pair_skips", "multipoles", "leaves")
 
 
