@@ -36,6 +36,7 @@ class Config(C.Structure):
         ("adaptive_error_estimator", C.c_int32), ("cutoff_node_policy", C.c_int32),
         ("adaptive_maximum_opening_angle", C.c_double), ("relative_force_tolerance", C.c_double),
         ("relative_force_acceleration_floor", C.c_double),
+        ("group_walk_enabled", C.c_int32), ("gaussian_pair_lookup", C.c_int32),
     ]
 
 

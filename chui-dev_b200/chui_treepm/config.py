@@ -108,6 +108,8 @@ def config_from_param_text(text: str, precision: int = _abi.MIXED, device: int =
     if cut not in _CUTOFF_POLICIES:
         raise ValueError(f"key 'numerics.treepm_cutoff_node_policy': invalid value '{cut}'")
     c.cutoff_node_policy = _CUTOFF_POLICIES[cut]
+    c.group_walk_enabled = 1 if get("numerics.treepm_group_walk_enabled", _bool, False) else 0
+    c.gaussian_pair_lookup = 1 if get("numerics.treepm_gaussian_pair_lookup_enabled", _bool, False) else 0
     soft = kv.get("numerics.gravity_softening")
     if soft:
         # gravity_softening_kpc_comoving * 1e-3 (gravity_runtime.cpp:579-581)

@@ -92,6 +92,8 @@ class TreePmConfig:
     adaptive_maximum_opening_angle: float = 0.25
     relative_force_tolerance: float = 0.005
     relative_force_acceleration_floor: float = 1.0e-30
+    group_walk_enabled: int = 0
+    gaussian_pair_lookup: int = 0
 
     def to_c(self) -> _abi.Config:
         c = _abi.Config()

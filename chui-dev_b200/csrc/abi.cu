@@ -539,6 +539,8 @@ int chui_treepm_config_default(chui_treepm_config* cfg) {
   cfg->adaptive_maximum_opening_angle = 0.25;                                 // tree_pm_coupling.hpp:248
   cfg->relative_force_tolerance = 0.005;                                      // tree_gravity.hpp:39
   cfg->relative_force_acceleration_floor = 1.0e-30;                           // tree_gravity.hpp:40
+  cfg->group_walk_enabled = 0;                                                // tree_pm_coupling.hpp:257
+  cfg->gaussian_pair_lookup = 0;                                              // tree_pm_coupling.hpp:266
   return 0;
 }
 
@@ -588,6 +590,7 @@ void chui_treepm_destroy(void* handle) {
     cudaDeviceSynchronize();
     chui::pmDestroy(*c);
     chui::DevBuf* bufs[] = {&c->in_x, &c->in_y, &c->in_z, &c->in_m, &c->in_active, &c->in_tx, &c->in_ty, &c->in_tz, &c->in_prev,
+                            &c->grp_leaf, &c->grp_start, &c->grp_rec, &c->grp_list, &c->grp_done, &c->gauss_tab,
                             &c->out_acc[0], &c->out_acc[1], &c->out_acc[2], &c->out_pm[0], &c->out_pm[1],
                             &c->out_pm[2], &c->out_tree[0], &c->out_tree[1], &c->out_tree[2], &c->out_near,
                             &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max,
@@ -780,6 +783,16 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   wp.angle = c.cfg.adaptive_maximum_opening_angle;
   wp.rel_tol = c.cfg.relative_force_tolerance;
   wp.floor_ = c.cfg.relative_force_acceleration_floor;
+  wp.gauss_lookup = c.cfg.gaussian_pair_lookup ? 1 : 0;
+  {
+    // group walk eligibility (tree_pm_coupling.cpp:3840-3870, 3922-3925, 4282-4286)
+    const double inv_2a2 = (0.25 / c.rs) / c.rs, inv_8a3 = ((0.125 / c.rs) / c.rs) / c.rs;
+    const double t_cut = (0.25 * wp.cutoff2 / c.rs) / c.rs;
+    wp.group_walk = c.cfg.group_walk_enabled && c.cfg.acceptance_policy == CHUI_TREEPM_POLICY_ADAPTIVE &&
+                    c.cfg.adaptive_error_estimator == CHUI_TREEPM_ESTIMATOR_RELATIVE_MONOPOLE &&
+                    c.cfg.gaussian_pair_lookup && std::isnormal(inv_2a2) && std::isnormal(inv_8a3) &&
+                    std::isfinite(t_cut) && t_cut < 63.0;
+  }
   wp.inv_4rs2_f = static_cast<float>(0.25 / (c.rs * c.rs));
   wp.inv_8rs3_f = static_cast<float>(0.125 / (c.rs * c.rs * c.rs));
   wp.cut2_f = static_cast<float>(c.cutoff * c.cutoff);

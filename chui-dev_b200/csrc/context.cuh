@@ -48,6 +48,8 @@ struct WalkParams {
   int policy;      // 0 strict reference, 1 adaptive relative
   int estimator;   // adaptive: 0 residual derivative, 1 relative monopole
   int com_cutoff;  // adaptive with COM-distance cutoff nodes
+  int group_walk;  // the group walk is active for this solve
+  int gauss_lookup;  // Gaussian Hermite table for FP64 direct pairs
   double angle;    // adaptive_maximum_opening_angle
   double rel_tol;  // relative_force_tolerance
   double floor_;   // relative_force_acceleration_floor_code
@@ -78,6 +80,11 @@ struct Context {
 
   // staged inputs / outputs
   DevBuf in_x, in_y, in_z, in_m, in_active, in_tx, in_ty, in_tz, in_prev;
+  // group walk: leaf per tree position, per visit position the group start and
+  // the group record (centre + a_min, half + flags), the eligible group starts,
+  // per-slot "evaluated by a group" flags, the Gaussian Hermite table
+  DevBuf grp_leaf, grp_start, grp_rec, grp_list, grp_done, gauss_tab;
+  bool gauss_ready = false;
   DevBuf out_acc[3], out_pm[3], out_tree[3], out_near;
   DevBuf status;       // uint32 status word + scalar results (reduction scratch)
   DevBuf scalars;      // reduction outputs (64 x u64)

@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <vector>
 
 #include "context.cuh"
 
@@ -68,6 +69,13 @@ struct WalkArgs {
   const float4* node_mq;   // per node 2 x float4: {mass, Mxx, Mxy, Mxz}, {Myy, Myz, Mzz, trace}
   const double4* src_u4;   // tree-ordered unwrapped positions + mass (mixed)
   const double* prev;      // per slot |a_previous| (nullable: no history)
+  // group walk
+  const uint32_t* leaf_of_pos;  // tree position -> leaf node
+  uint32_t* grp_start;          // visit position -> visit position of its group's first target
+  double4* grp_rec;             // at a group start v: [2v] {centre, a_min}, [2v+1] {half, targets or 0 if ineligible}
+  uint32_t* grp_list;           // eligible group starts
+  unsigned char* grp_done;      // per slot: evaluated by the group walk
+  const double2* gauss;         // Gaussian Hermite table {value, slope} (4097 knots)
   double* out_x;   // per slot, short-range part
   double* out_y;
   double* out_z;
@@ -242,6 +250,320 @@ __device__ __forceinline__ bool acceptNode(const WalkParams& w, double half, dou
   return ((width + com_offset) / sqrt(r2 + 1.0e-30)) < w.theta;
 }
 
+// ---- Gaussian pair lookup and the group walk (FP64) ------------------------
+
+constexpr int kGaussCells = 4096;                  // tree_pm_split_kernel.hpp:136-138
+constexpr double kGaussStep = 64.0 / kGaussCells;
+
+// Cubic Hermite evaluation of H(t) from the reference's table
+// (TreePmGaussianCoefficientTable::dimensionlessCoefficient, :150-164).
+__device__ __forceinline__ double gaussHermite(const double2* g, double t) {
+  const double cell = t / kGaussStep;
+  const int i = static_cast<int>(cell);
+  const double u = cell - static_cast<double>(i);
+  const double u2 = u * u;
+  const double u3 = u2 * u;
+  const double2 k0 = g[i], k1 = g[i + 1];
+  return (2 * u3 - 3 * u2 + 1) * k0.x + (u3 - 2 * u2 + u) * k0.y + (-2 * u3 + 3 * u2) * k1.x + (u3 - u2) * k1.y;
+}
+
+// Per-target direct pair with the Gaussian lookup (tree_pm_coupling.cpp:4221-4226).
+__device__ __forceinline__ double gaussResidualInvR3(const WalkArgs& a, double r2, double eps) {
+  const double rs = a.wp.rs;
+  const double inv_2a2 = (0.25 / rs) / rs, inv_8a3 = ((0.125 / rs) / rs) / rs;
+  const double t = r2 * inv_2a2;
+  double long_inv_r3;
+  if (t < 64.0) {
+    const double coeff = t < 0.015625 ? coefficientSeries(t) : gaussHermite(a.gauss, t);
+    long_inv_r3 = coeff * inv_8a3;
+  } else {
+    long_inv_r3 = longRangeInvR3(sqrt(r2), rs);
+  }
+  return softenedInvR3(r2, eps) - long_inv_r3;
+}
+
+// treePmGroupNearestImage (internal/tree_pm_group_walk.hpp:70-76), unfused.
+__device__ __forceinline__ double groupImage(double delta, double length) {
+  if (!(length > 0.0)) return delta;
+  return __dsub_rn(delta, __dmul_rn(length, rint(__ddiv_rn(delta, length))));
+}
+
+struct GroupBox {
+  double c[3], h[3], a_min;
+};
+
+// Node decision of the group walk (buildTreePmGroupInteractionList,
+// internal/tree_pm_group_walk.hpp:78-154): 0 prune, 1 accept (leaf or
+// multipole), 2 open. The reference's FP64 arithmetic, unfused.
+__device__ __forceinline__ int groupDecision(const WalkArgs& a, uint32_t node, const GroupBox& gb) {
+  const WalkParams& w = a.wp;
+  const double4 g = a.geom[node];
+  const double h = g.w;
+  const double cc[3] = {g.x, g.y, g.z};
+  double gap2 = 0.0, far2 = 0.0;
+  for (int ax = 0; ax < 3; ++ax) {
+    const double d = fabs(groupImage(cc[ax] - gb.c[ax], w.box[ax]));
+    const double gap = fmax(0.0, __dsub_rn(__dsub_rn(d, h), gb.h[ax]));
+    const double far = __dadd_rn(__dadd_rn(d, h), gb.h[ax]);
+    gap2 = __dadd_rn(gap2, __dmul_rn(gap, gap));
+    far2 = __dadd_rn(far2, __dmul_rn(far, far));
+  }
+  if (gap2 > w.cutoff2) return 0;
+  if (a.range[node].z == 0) return 1;
+  bool accept = gap2 > 0.0 && (w.com_cutoff || far2 <= w.cutoff2);
+  if (accept) {
+    const double4 cm = a.com[node];
+    const double mc[3] = {cm.x, cm.y, cm.z};
+    double r_min2 = 0.0;
+    for (int ax = 0; ax < 3; ++ax) {
+      const double gap = fmax(0.0, __dsub_rn(fabs(groupImage(mc[ax] - gb.c[ax], w.box[ax])), gb.h[ax]));
+      r_min2 = __dadd_rn(r_min2, __dmul_rn(gap, gap));
+    }
+    const double width2 = 4.0 * h * h;
+    const double rel_over_g = w.rel_tol / w.G;
+    accept = r_min2 > 0.0 && width2 < (w.angle * w.angle) * r_min2 &&
+             cm.w * width2 <= rel_over_g * gb.a_min * r_min2 * r_min2;
+  }
+  return accept ? 1 : 2;
+}
+
+inline unsigned groupGrid(int64_t n, int block) {
+  const int64_t g = (n + block - 1) / block;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(g, 148 * 64)));
+}
+
+__global__ void leafOfPosKernel(int64_t nodes, const uint4* __restrict__ range, uint32_t* leaf_of_pos) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nodes;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint4 rg = range[k];
+    if (rg.z != 0) continue;
+    for (uint32_t q = rg.x; q < rg.x + rg.y; ++q) leaf_of_pos[q] = static_cast<uint32_t>(k);
+  }
+}
+
+__device__ __forceinline__ uint32_t leafOfVisit(const WalkArgs& a, int64_t v, uint32_t* slot_out, uint32_t* row_out) {
+  const uint32_t slot = a.order[v];
+  const uint32_t row = a.active ? a.active[slot] : slot;
+  *slot_out = slot;
+  *row_out = row;
+  return row < a.n ? a.leaf_of_pos[a.pos_of_row[row]] : kInvalid;
+}
+
+// Groups: maximal runs of visit positions with the same source leaf inside one
+// residual block of 64 (tree_pm_coupling.cpp:4498-4560, legacy grouping). At a
+// group start: the group box (reference = first target, nearest-image deltas),
+// the smallest previous |a|, and eligibility (every target with history above
+// the floor and a bounded source metric; :4326-4368).
+__global__ void groupSetupKernel(WalkArgs a, uint32_t* count) {
+  const WalkParams& w = a.wp;
+  for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < a.nt;
+       v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t slot, row;
+    const uint32_t leaf = leafOfVisit(a, v, &slot, &row);
+    const int64_t block0 = v & ~static_cast<int64_t>(63);
+    int64_t st = v;
+    if (leaf != kInvalid) {
+      uint32_t s2, r2;
+      while (st > block0 && leafOfVisit(a, st - 1, &s2, &r2) == leaf) --st;
+    }
+    a.grp_start[v] = static_cast<uint32_t>(st);
+    if (st != v) continue;
+    const int64_t block1 = min(block0 + 64, a.nt);
+    int64_t e = v + 1;
+    if (leaf != kInvalid) {
+      uint32_t s2, r2;
+      while (e < block1 && leafOfVisit(a, e, &s2, &r2) == leaf) ++e;
+    }
+    bool ok = leaf != kInvalid;
+    double ref[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, a_min = INFINITY;
+    for (int64_t q = v; q < e && ok; ++q) {
+      uint32_t sq, rq;
+      leafOfVisit(a, q, &sq, &rq);
+      const double pv = a.prev ? a.prev[sq] : NAN;
+      if (!(isfinite(pv) && pv > w.floor_)) {
+        ok = false;
+        break;
+      }
+      a_min = fmin(a_min, pv);
+      const double pos[3] = {a.tx ? a.tx[sq] : a.sx[rq], a.ty ? a.ty[sq] : a.sy[rq], a.tz ? a.tz[sq] : a.sz[rq]};
+      for (int ax = 0; ax < 3; ++ax) {
+        if (!makeMetric(w.src_lo[ax], w.src_hi[ax], pos[ax], w.box[ax]).bounded) ok = false;
+        if (q == v) {
+          ref[ax] = pos[ax];
+          continue;
+        }
+        const double d = groupImage(pos[ax] - ref[ax], w.box[ax]);
+        lo[ax] = fmin(lo[ax], d);
+        hi[ax] = fmax(hi[ax], d);
+      }
+    }
+    double c[3], h[3];
+    for (int ax = 0; ax < 3; ++ax) {
+      c[ax] = ref[ax] + 0.5 * (lo[ax] + hi[ax]);
+      h[ax] = 0.5 * (hi[ax] - lo[ax]);
+    }
+    a.grp_rec[2 * v] = make_double4(c[0], c[1], c[2], a_min);
+    a.grp_rec[2 * v + 1] = make_double4(h[0], h[1], h[2], ok ? static_cast<double>(e - v) : 0.0);
+    if (ok) a.grp_list[atomicAdd(count, 1u)] = static_cast<uint32_t>(v);
+  }
+}
+
+// The FP64 group walk: one warp per eligible group (its targets on the lanes,
+// 32 at a time), one warp-uniform walk building the shared list; each lane
+// evaluates the accepted leaves' pairs with the Hermite table (leaves whose
+// cell lies beyond r_cut are culled per target, as the reference does) and the
+// accepted multipoles at its own COM distance (pruned beyond r_cut under
+// COM-distance cutoff nodes), accumulateTreePmGroupCulledLeaves and
+// evaluate_target_group (tree_pm_coupling.cpp:4369-4420). Summation order:
+// leaves and multipoles as the walk meets them.
+__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) groupWalkKernel(WalkArgs a, const uint32_t* groups,
+                                                                           uint32_t n_groups) {
+  __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  uint32_t* stack = stack_sm[warp];
+  const WalkParams& w = a.wp;
+  const double lx = w.box[0], ly = w.box[1], lz = w.box[2];
+  const double inv_2a2 = (0.25 / w.rs) / w.rs, inv_8a3 = ((0.125 / w.rs) / w.rs) / w.rs;
+  const double t_limit = 63.99999999999999;  // nextafter(64, 0)
+  const double eps2 = w.eps * w.eps;
+  const double cull2 = w.cutoff2 * (1.0 + 1.0e-9);
+  unsigned long long cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0,
+                     cnt_multi = 0, cnt_leaves = 0;
+  for (uint32_t gi = blockIdx.x * kWalkWarpsPerBlock + warp; gi < n_groups; gi += gridDim.x * kWalkWarpsPerBlock) {
+    const uint32_t v0 = groups[gi];
+    const double4 r0 = a.grp_rec[2 * static_cast<size_t>(v0)], r1 = a.grp_rec[2 * static_cast<size_t>(v0) + 1];
+    GroupBox gb;
+    gb.c[0] = r0.x; gb.c[1] = r0.y; gb.c[2] = r0.z; gb.a_min = r0.w;
+    gb.h[0] = r1.x; gb.h[1] = r1.y; gb.h[2] = r1.z;
+    const int count = static_cast<int>(r1.w);
+    for (int chunk = 0; chunk < count; chunk += 32) {
+      const bool valid = chunk + lane < count;
+      uint32_t slot = 0, row = kInvalid;
+      double px = 0.0, py = 0.0, pz = 0.0;
+      if (valid) {
+        leafOfVisit(a, v0 + chunk + lane, &slot, &row);
+        px = a.tx ? a.tx[slot] : a.sx[row];
+        py = a.ty ? a.ty[slot] : a.sy[row];
+        pz = a.tz ? a.tz[slot] : a.sz[row];
+      }
+      const uint32_t self_pos = (valid && row < a.n) ? a.pos_of_row[row] : kInvalid;
+      const double toff[3] = {groupImage(px - gb.c[0], lx), groupImage(py - gb.c[1], ly), groupImage(pz - gb.c[2], lz)};
+      Metric nm[3];
+      const double pt[3] = {px, py, pz};
+      for (int ax = 0; ax < 3; ++ax) nm[ax] = makeMetric(w.node_lo[ax], w.node_hi[ax], pt[ax], w.box[ax]);
+      const bool count_walk = lane == 0 && chunk == 0;
+      double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0, nearest = INFINITY;
+      if (lane == 0) stack[0] = 0u;
+      int sp = 1;
+      __syncwarp();
+      bool overflow = false;
+      while (sp > 0) {
+        const uint32_t node = stack[sp - 1];
+        --sp;
+        __syncwarp();
+        const int d = groupDecision(a, node, gb);  // identical on every lane
+        if (count_walk) {
+          ++cnt_visited;
+          cnt_pruned += d == 0 ? 1 : 0;
+        }
+        if (d == 0) continue;
+        const uint4 rg = a.range[node];
+        if (d == 1 && rg.z == 0) {
+          if (count_walk) {
+            ++cnt_leaves;
+            ++cnt_accepted;
+          }
+          if (valid) {
+            const double4 g = a.geom[node];
+            const double h = g.w;
+            const double lc[3] = {groupImage(g.x - gb.c[0], lx), groupImage(g.y - gb.c[1], ly),
+                                  groupImage(g.z - gb.c[2], lz)};
+            double g2 = 0.0;
+            for (int ax = 0; ax < 3; ++ax) {
+              const double off = lc[ax] - toff[ax], hl = 0.5 * w.box[ax];
+              const double dd = off > hl ? off - w.box[ax] : (off < -hl ? off + w.box[ax] : off);
+              const double gg = fmax(0.0, fabs(dd) - h);
+              g2 = __dadd_rn(g2, __dmul_rn(gg, gg));
+            }
+            if (!(g2 > cull2)) {
+              double sx = 0.0, sy = 0.0, sz = 0.0;
+              for (uint32_t j = rg.x; j < rg.x + rg.y; ++j) {
+                const double4 sv = a.src_d4[j];
+                double dx = sv.x - px, dy = sv.y - py, dz = sv.z - pz;
+                dx = dx > 0.5 * lx ? dx - lx : (dx < -0.5 * lx ? dx + lx : dx);
+                dy = dy > 0.5 * ly ? dy - ly : (dy < -0.5 * ly ? dy + ly : dy);
+                dz = dz > 0.5 * lz ? dz - lz : (dz < -0.5 * lz ? dz + lz : dz);
+                const double r2 = norm2rn(dx, dy, dz);
+                const bool inside = j != self_pos && r2 <= w.cutoff2;
+                const double t = fmin(r2 * inv_2a2, t_limit);
+                const double coeff_long = gaussHermite(a.gauss, t) * inv_8a3;
+                const double dn = r2 + eps2;
+                const double softened = 1.0 / (dn * sqrt(dn));
+                const double factor = (inside && r2 > 0.0) ? (softened - coeff_long) * w.G * sv.w : 0.0;
+                sx += factor * dx;
+                sy += factor * dy;
+                sz += factor * dz;
+                cnt_pairs += inside ? 1 : 0;
+                nearest = inside ? fmin(nearest, r2) : nearest;
+              }
+              acc_x += sx;
+              acc_y += sy;
+              acc_z += sz;
+            }
+          }
+          continue;
+        }
+        if (d == 1) {
+          if (count_walk) {
+            ++cnt_multi;
+            ++cnt_accepted;
+          }
+          if (valid) {
+            const double4 cm = a.com[node];
+            const double dx = applyMetric(nm[0], cm.x - px);
+            const double dy = applyMetric(nm[1], cm.y - py);
+            const double dz = applyMetric(nm[2], cm.z - pz);
+            if (w.com_cutoff && norm2rn(dx, dy, dz) > w.cutoff2) {
+              ++cnt_pruned;
+            } else {
+              multipoleForce(a, node, dx, dy, dz, w.eps, acc_x, acc_y, acc_z);
+            }
+          }
+          continue;
+        }
+        if (count_walk) ++cnt_opened;
+        const uint32_t ch = lane < 8 ? a.child[8 * static_cast<size_t>(node) + lane] : kInvalid;
+        const unsigned cmask = __ballot_sync(0xffffffffu, ch != kInvalid) & 0xFFu;
+        const int nc = __popc(cmask);
+        if (sp + nc > kStackCap) {
+          overflow = true;
+          break;
+        }
+        if (ch != kInvalid) stack[sp + __popc(cmask >> (lane + 1))] = ch;
+        sp += nc;
+        __syncwarp();
+      }
+      if (overflow && lane == 0) atomicOr(a.status, kStatusStackOverflow);
+      if (valid) {
+        a.out_x[slot] = acc_x;
+        a.out_y[slot] = acc_y;
+        a.out_z[slot] = acc_z;
+        a.out_near[slot] = nearest;
+        a.grp_done[slot] = 1;
+      }
+      __syncwarp();
+    }
+  }
+  unsigned long long c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs, cnt_pruned, 0ull, cnt_multi, cnt_leaves};
+  for (int k = 0; k < 8; ++k) {
+    for (int off = 16; off > 0; off >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], off);
+  }
+  if (lane == 0) {
+    for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, c[k]);
+  }
+}
+
 template <bool kMixed, bool kEpsZero>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a) {
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
@@ -280,6 +602,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
     const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
     const double eps_t = w.eps;
     const History hist = loadHistory(a.prev, slot, valid);
+    // targets the group walk evaluated take no per-target walk
+    const bool grouped = valid && a.grp_done != nullptr && a.grp_done[slot] != 0;
     Metric sm[3], nm[3];
     const double pt[3] = {px, py, pz};
     for (int ax_ = 0; ax_ < 3; ++ax_) {
@@ -299,7 +623,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
       const uint32_t node = stack[sp - 1];
       --sp;
       __syncwarp();
-      const bool act = valid && node >= skip_until;
+      const bool act = valid && !grouped && node >= skip_until;
       if (!__any_sync(0xffffffffu, act)) continue;
       const double4 g = a.geom[node];
       const uint4 rg = a.range[node];
@@ -382,7 +706,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
                 nearest_mixed = fminf(nearest_mixed, static_cast<float>(r2));
                 ++cnt_pairs;
                 if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
-                const double f = residualInvR3(r2, fmax(w.eps, eps_t), w.rs) * w.G;
+                const double f = (w.gauss_lookup && r2 > 0.0 ? gaussResidualInvR3(a, r2, fmax(w.eps, eps_t))
+                                                             : residualInvR3(r2, fmax(w.eps, eps_t), w.rs)) *
+                                 w.G;
                 acc_x += f * s.w * dx;
                 acc_y += f * s.w * dy;
                 acc_z += f * s.w * dz;
@@ -443,7 +769,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
       if (lane == 0) atomicOr(a.status, kStatusStackOverflow);
     }
     if constexpr (kMixed) nearest = static_cast<double>(nearest_f);
-    if (valid) {
+    if (valid && !grouped) {
       a.out_x[slot] = acc_x;
       a.out_y[slot] = acc_y;
       a.out_z[slot] = acc_z;
@@ -642,10 +968,14 @@ __device__ __forceinline__ int certainLess(float a, float b, float err = 0.f) {
 // group's cutoff sphere are dropped at enqueue) tagged with the ballot of
 // accepting lanes, and evaluated 64 sources at a time in FP32.
 // kMode: 0 strict policy without acceleration history, 1 strict policy with
-// the relative-force MAC and history, 2 adaptive-relative policy.
+// the relative-force MAC and history, 2 adaptive-relative policy, 3 adaptive
+// with the group walk: lanes whose group is eligible take their group's
+// decision (made in FP64 by the group's first lane in the warp and broadcast),
+// the others the per-target adaptive decision.
 template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS) walkFastKernel(WalkArgs a) {
-  constexpr bool kAdaptive = kMode == 2;
+  constexpr bool kAdaptive = kMode >= 2;
+  constexpr bool kGroup = kMode == 3;
   constexpr bool kHistory = kMode != 0;
   constexpr int kList = kAdaptive ? kMultList : 1;
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
@@ -711,6 +1041,21 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     const bool skip_self = valid && row < a.n;
     const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
     const History hist = loadHistory(kHistory ? a.prev : nullptr, slot, valid);
+    // group walk: the lane's group (start visit position), eligibility, and the
+    // lane deciding for it in this warp (the group's first lane here); only the
+    // warp holding a group's first target counts the group walk's node counters
+    uint32_t g_start = 0;
+    bool in_group = false;
+    int leader = lane;
+    bool count_walk = false;
+    if constexpr (kGroup) {
+      g_start = valid ? a.grp_start[v] : 0xFFFFFFFFu;
+      in_group = valid && a.grp_rec[2 * static_cast<size_t>(g_start) + 1].w > 0.0;
+      const uint32_t up = __shfl_up_sync(0xffffffffu, g_start, 1);
+      const unsigned run_start = __ballot_sync(0xffffffffu, lane == 0 || up != g_start);
+      leader = 31 - __clz(run_start & ((2u << lane) - 1u));
+      count_walk = in_group && leader == lane && static_cast<int64_t>(g_start) == v;
+    }
     // relative criterion in FP32: the allowance alpha |a_prev| (adaptive, with
     // usable history) or alpha max(|a_prev|, floor) (strict relative MAC, any
     // finite history); FP32 tests are used only where it is a normal float
@@ -743,7 +1088,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         const bool in = mine && r2 <= cut2;
         if constexpr (kDiag) {
           pairs += in ? 1u : 0u;
-          skips += (mine && !in) ? 1u : 0u;
+          // the group walk's pair kernel counts no skipped pairs
+          skips += (mine && !in && !in_group) ? 1u : 0u;
           nearest_f = in ? fminf(nearest_f, r2) : nearest_f;
         }
         const float hh = hornerR2<kTerms>(a.poly, r2, sc_r2);
@@ -847,7 +1193,27 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       const bool fast_frame = h < 64.0 * w.cutoff && cmax + rga < half_min_box * (1.0 - 1.0e-9);
       bool prune = false, accept = false, need_exact = !fast_frame;
       float dxc = 0.f, dyc = 0.f, dzc = 0.f;  // COM offset of an accepted node (FP32)
-      if (act && fast_frame) {
+      if constexpr (kGroup) {
+        const bool lead = in_group && act && leader == lane;
+        int gd = 0;
+        if (__any_sync(0xffffffffu, lead)) {
+          if (lead) {
+            const double4 r0 = a.grp_rec[2 * static_cast<size_t>(g_start)];
+            const double4 r1 = a.grp_rec[2 * static_cast<size_t>(g_start) + 1];
+            GroupBox gb;
+            gb.c[0] = r0.x; gb.c[1] = r0.y; gb.c[2] = r0.z; gb.a_min = r0.w;
+            gb.h[0] = r1.x; gb.h[1] = r1.y; gb.h[2] = r1.z;
+            gd = groupDecision(a, node, gb);
+          }
+        }
+        gd = __shfl_sync(0xffffffffu, gd, leader);
+        if (in_group) {
+          need_exact = false;
+          prune = gd == 0;
+          accept = gd == 1;
+        }
+      }
+      if (act && fast_frame && !in_group) {
         const float hf = static_cast<float>(h);
         // bound on the error of each FP32 offset component below (centre and
         // target offsets rounded once, one subtraction, the COM offset added)
@@ -925,6 +1291,37 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
           }
         }
       }
+      // a group lane's accepted multipole: its own COM offset, and under
+      // COM-distance cutoff nodes no contribution beyond r_cut (the node stays
+      // accepted for the walk; the reference counts it pruned for this target)
+      bool com_skip = false;
+      if (kGroup && in_group && act && accept && !is_leaf) {
+        bool exact_com = !fast_frame;
+        if (fast_frame) {
+          const float4 nf = a.node_f4[node];
+          dxc = (static_cast<float>(cdx) - tfx) + nf.x;
+          dyc = (static_cast<float>(cdy) - tfy) + nf.y;
+          dzc = (static_cast<float>(cdz) - tfz) + nf.z;
+          if (w.com_cutoff) {
+            const float fe = 2.4e-7f * (static_cast<float>(cmax) + rga_f + static_cast<float>(h));
+            const float r2c = fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc));
+            const int beyond = certainLess(cut2, r2c, 4.0f * sqrtf(r2c) * fe);
+            if (beyond > 0) com_skip = true;
+            else if (beyond == 0) exact_com = true;
+          }
+        }
+        if (exact_com) {
+          const double4 cm = a.com[node];
+          const double ex = applyMetric(makeMetric(w.node_lo[0], w.node_hi[0], px, w.box[0]), cm.x - px);
+          const double ey = applyMetric(makeMetric(w.node_lo[1], w.node_hi[1], py, w.box[1]), cm.y - py);
+          const double ez = applyMetric(makeMetric(w.node_lo[2], w.node_hi[2], pz, w.box[2]), cm.z - pz);
+          com_skip = w.com_cutoff && norm2rn(ex, ey, ez) > w.cutoff2;
+          dxc = static_cast<float>(ex);
+          dyc = static_cast<float>(ey);
+          dzc = static_cast<float>(ez);
+        }
+        if (kDiag && com_skip) ++cnt_pruned;
+      }
       if (act && need_exact) {
         const ExactDecision d = exactNodeDecision<kAdaptive>(a, node, px, py, pz, skip_self, hist);
         prune = d.prune;
@@ -933,7 +1330,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         dyc = static_cast<float>(d.dy);
         dzc = static_cast<float>(d.dz);
       }
-      if (kDiag && act) {
+      // node counters: per lane, or once per group under the group walk
+      const bool count_node = !kGroup || !in_group || count_walk;
+      if (kDiag && act && count_node) {
         ++cnt_visited;
         cnt_pruned += prune ? 1 : 0;
       }
@@ -941,7 +1340,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         const bool want = act && !prune;
         const uint32_t mask = __ballot_sync(0xffffffffu, want);
         if (mask == 0u) continue;
-        if (kDiag && want) {
+        if (kDiag && want && count_node) {
           ++cnt_accepted;
           ++cnt_leaves;
         }
@@ -961,10 +1360,12 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       const bool do_accept = act && !prune && accept;
       const bool open = act && !prune && !accept;
       if (do_accept) {
-        if constexpr (kDiag) {
+        if (kDiag && count_node) {
           ++cnt_accepted;
           ++cnt_multi;
         }
+      }
+      if (do_accept && !com_skip) {
         if (a.mult_f32 && fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc)) >= fmaxf(1.0e-8f * cut2, 1.0e-10f)) {
           if constexpr (kAdaptive) {
             m_list[warp][mn][lane] = make_float4(dxc, dyc, dzc, __uint_as_float(node));
@@ -988,7 +1389,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         if (__any_sync(0xffffffffu, mn == kList)) mflush();
       }
       if (act && (prune || accept)) skip_until = rg4.w;
-      if (kDiag && open) ++cnt_opened;
+      if (kDiag && open && count_node) ++cnt_opened;
       if (__any_sync(0xffffffffu, open)) {
         constexpr uint32_t kBlock = kAdaptive ? kBulkCountAdaptive : kBulkCount;
         if constexpr (!kDiag && kBlock > 0) {
@@ -1364,6 +1765,41 @@ int launchWalk(const WalkArgs& args, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
 }
 
+// Host copy of the Gaussian long-range force factor L(q) for the table.
+double hostLongRangeFactor(double r, double rs) {
+  if (r <= 0.0) return 0.0;
+  const double q = (0.5 * r) / rs;
+  if (std::isinf(q)) return 1.0;
+  const double k = 0.564189583547756286948079451560772586;
+  if (q < 0.125) {
+    const double t = q * q;
+    const double h = 4.0 * k * (1.0 / 3.0 + t * (-1.0 / 5.0 + t * (1.0 / 14.0 + t * (-1.0 / 54.0 +
+                     t * (1.0 / 264.0 + t * (-1.0 / 1560.0 + t * (1.0 / 10800.0 - t / 85680.0)))))));
+    return q * q * q * h;
+  }
+  return std::erf(q) - 2.0 * k * q * std::exp(-q * q);
+}
+
+// TreePmGaussianCoefficientTable's knots (tree_pm_split_kernel.hpp:170-181),
+// uploaded once per context.
+int ensureGaussTable(Context& c, cudaStream_t s) {
+  if (c.gauss_ready) return 0;
+  if (ensure(c.gauss_tab, (kGaussCells + 1) * sizeof(double2))) return CHUI_TREEPM_ENOMEM;
+  std::vector<double2> tab(kGaussCells + 1);
+  const double k = 0.564189583547756286948079451560772586;
+  for (int i = 0; i <= kGaussCells; ++i) {
+    const double t = static_cast<double>(i) * kGaussStep;
+    const double q = std::sqrt(t);
+    const double value = i == 0 ? 4.0 * k / 3.0 : hostLongRangeFactor(q, 0.5) / (t * q);
+    const double derivative = i == 0 ? -4.0 * k / 5.0 : (2.0 * k * std::exp(-t) - 1.5 * value) / t;
+    tab[i] = make_double2(value, kGaussStep * derivative);
+  }
+  cudaMemcpyAsync(c.gauss_tab.ptr, tab.data(), tab.size() * sizeof(double2), cudaMemcpyHostToDevice, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  c.gauss_ready = true;
+  return 0;
+}
+
 }  // namespace
 
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
@@ -1399,6 +1835,16 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.node_mq = c.node_mq.as<float4>();
   a.src_u4 = c.src_u4.as<double4>();
   a.prev = prev_acc;
+  a.leaf_of_pos = nullptr;
+  a.grp_start = nullptr;
+  a.grp_rec = nullptr;
+  a.grp_list = nullptr;
+  a.grp_done = nullptr;
+  a.gauss = nullptr;
+  if (wp.gauss_lookup || wp.group_walk) {
+    if (int rc = ensureGaussTable(c, s)) return rc;
+    a.gauss = c.gauss_tab.as<double2>();
+  }
   double* acc = c.tree_acc.as<double>();
   a.out_x = acc;
   a.out_y = acc + nt;
@@ -1419,6 +1865,24 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     a.mpoly12 = (c.dpoly.terms <= 12 && c.ddpoly.terms <= 12) ? 1 : 0;
   }
   a.wp = wp;
+  uint32_t* group_count = nullptr;
+  if (wp.group_walk) {
+    if (ensure(c.grp_leaf, static_cast<size_t>(n) * 4) || ensure(c.grp_start, static_cast<size_t>(nt) * 4) ||
+        ensure(c.grp_rec, static_cast<size_t>(nt) * 2 * sizeof(double4)) ||
+        ensure(c.grp_list, static_cast<size_t>(nt) * 4) || ensure(c.grp_done, static_cast<size_t>(nt)) ||
+        ensure(c.work_counter, 16))
+      return CHUI_TREEPM_ENOMEM;
+    a.leaf_of_pos = c.grp_leaf.as<uint32_t>();
+    a.grp_start = c.grp_start.as<uint32_t>();
+    a.grp_rec = c.grp_rec.as<double4>();
+    a.grp_list = c.grp_list.as<uint32_t>();
+    a.grp_done = c.grp_done.as<unsigned char>();
+    group_count = c.work_counter.as<uint32_t>() + 1;
+    cudaMemsetAsync(c.grp_done.ptr, 0, static_cast<size_t>(nt), s);
+    cudaMemsetAsync(group_count, 0, 4, s);
+    { noteLaunch(); leafOfPosKernel<<<groupGrid(c.n_nodes, 256), 256, 0, s>>>(c.n_nodes, a.range, c.grp_leaf.as<uint32_t>()); }
+    { noteLaunch(); groupSetupKernel<<<groupGrid(nt, 256), 256, 0, s>>>(a, group_count); }
+  }
   const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
   const bool eps_zero = wp.eps == 0.0;
   if (mixed) {
@@ -1426,13 +1890,15 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     // positions base..base+31 and self pairs are excluded by the lane mask
     const bool contiguous = active == nullptr && tx == nullptr && nt == n;
     const bool diag = c.cfg.diagnostics != 0;
-    const int mode = wp.policy == CHUI_TREEPM_POLICY_ADAPTIVE ? 2 : (wp.criterion == 2 && prev_acc ? 1 : 0);
+    const int mode = wp.policy == CHUI_TREEPM_POLICY_ADAPTIVE ? (wp.group_walk ? 3 : 2)
+                                                               : (wp.criterion == 2 && prev_acc ? 1 : 0);
 #define CHUI_WALK_DISPATCH2(EPS, TERMS, ADP)                                                           \
     if (diag) return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, true, true, ADP>, a, s)     \
                                 : launchPersistent(walkFastKernel<EPS, TERMS, true, false, ADP>, a, s);   \
     return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP>, a, s)              \
                       : launchPersistent(walkFastKernel<EPS, TERMS, false, false, ADP>, a, s);
 #define CHUI_WALK_DISPATCH(EPS, TERMS)                  \
+    if (mode == 3) { CHUI_WALK_DISPATCH2(EPS, TERMS, 3) } \
     if (mode == 2) { CHUI_WALK_DISPATCH2(EPS, TERMS, 2) } \
     if (mode == 1) { CHUI_WALK_DISPATCH2(EPS, TERMS, 1) } \
     CHUI_WALK_DISPATCH2(EPS, TERMS, 0)
@@ -1444,6 +1910,20 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     CHUI_WALK_DISPATCH(false, kPolyMaxTerms)
 #undef CHUI_WALK_DISPATCH
 #undef CHUI_WALK_DISPATCH2
+  }
+  if (wp.group_walk) {
+    uint32_t n_groups = 0;
+    cudaMemcpyAsync(&n_groups, group_count, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+    if (n_groups > 0) {
+      int dev = 0, sms = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const int64_t want = (static_cast<int64_t>(n_groups) + kWalkWarpsPerBlock - 1) / kWalkWarpsPerBlock;
+      const unsigned blocks = static_cast<unsigned>(std::min<int64_t>(want, static_cast<int64_t>(sms) * 8));
+      { noteLaunch(); groupWalkKernel<<<blocks, kWalkWarpsPerBlock * 32, 0, s>>>(a, c.grp_list.as<uint32_t>(), n_groups); }
+      if (cudaGetLastError() != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+    }
   }
   return launchWalk<false, false>(a, s);
 }

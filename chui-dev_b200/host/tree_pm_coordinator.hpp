@@ -82,6 +82,8 @@ struct TreePmOptions {
   double adaptive_maximum_opening_angle = 0.25;
   TreePmAdaptiveErrorEstimator adaptive_error_estimator = TreePmAdaptiveErrorEstimator::kResidualDerivative;
   TreePmCutoffNodePolicy cutoff_node_policy = TreePmCutoffNodePolicy::kContainNode;
+  bool group_walk_enabled = false;
+  bool gaussian_pair_lookup_enabled = false;
   Precision precision = Precision::kMixed;  // B200 extension: FP64 runs the same solver in double
   int device = 0;
 };
@@ -354,6 +356,8 @@ class TreePmCoordinator {
     c.adaptive_maximum_opening_angle = o.adaptive_maximum_opening_angle;
     c.relative_force_tolerance = o.tree_options.relative_force_tolerance;
     c.relative_force_acceleration_floor = o.tree_options.relative_force_acceleration_floor_code;
+    c.group_walk_enabled = o.group_walk_enabled ? 1 : 0;
+    c.gaussian_pair_lookup = o.gaussian_pair_lookup_enabled ? 1 : 0;
     c.precision = o.precision == Precision::kFp64 ? CHUI_TREEPM_FP64 : CHUI_TREEPM_MIXED;
     c.device = o.device;
     // split scale and cutoff are in units of the mean mesh spacing (gravity_runtime.cpp:586-590)

@@ -81,6 +81,13 @@ typedef struct {
   /* relative criteria (TreeGravityOptions, tree_gravity.hpp:30-43) */
   double relative_force_tolerance;            /* alpha; 0.005 */
   double relative_force_acceleration_floor;   /* code units; 1e-30 */
+  /* TreePmOptions::group_walk_enabled: one conservative walk per leaf of targets
+   * (effective with the adaptive policy, relative_monopole and the Gaussian pair
+   * lookup, as in the reference; other cases use the per-target walk) */
+  int32_t group_walk_enabled;
+  /* TreePmOptions::gaussian_pair_lookup_enabled: direct pairs take the Gaussian
+   * long-range coefficient from the reference's cubic Hermite table */
+  int32_t gaussian_pair_lookup;
 } chui_treepm_config;
 
 /* Counters named as TreePmTraversalCounters (tree_pm_coupling.hpp:39-87) plus

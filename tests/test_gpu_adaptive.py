@@ -10,7 +10,10 @@ floor (the COM-distance fallback):
 - adaptive_monopole: the production fast deck (relative monopole,
   COM-distance cutoff nodes, alpha 0.0025, maximum angle 1.0);
 - adaptive_residual: residual-derivative estimator, contain nodes, alpha
-  0.005, maximum angle 0.5, on an active subset of 5000 targets.
+  0.005, maximum angle 0.5, on an active subset of 5000 targets;
+- group_walk, group_walk_active: the fast deck and relative monopole with
+  contain nodes under the reference's group walk (one conservative walk per
+  leaf of targets, Gaussian Hermite pair table), all targets / the subset.
 
 Bars: FP64 accelerations to FP64 round-off with the reference's traversal
 counters; mixed precision with the per-node walk: the reference's node
@@ -31,6 +34,7 @@ from conftest import golden_params, load_golden  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 CASES = ["adaptive_monopole", "adaptive_residual"]
+GROUP_CASES = ["group_walk", "group_walk_active"]
 COUNTER_KEYS = ("visited_nodes", "accepted_nodes", "opened_nodes", "direct_pair_evaluations",
                 "cutoff_pruned_nodes", "cutoff_skipped_pairs", "accepted_internal_multipoles", "accepted_leaves")
 NODE_KEYS = ("visited_nodes", "accepted_nodes", "opened_nodes", "cutoff_pruned_nodes",
@@ -50,7 +54,8 @@ def cfg_for(g, precision, diagnostics=1):
     policy, estimator, cutoff_policy = (int(v) for v in g["adaptive"])
     angle, rel_tol, floor = (float(v) for v in g["adaptive_f"])
     mesh = [int(v) for v in g["mesh"]]
-    return ct.TreePmConfig(pm_grid_nx=mesh[0], pm_grid_ny=mesh[1], pm_grid_nz=mesh[2], box_x=float(g["box"][0]),
+    group_walk, lookup = (int(v) for v in g["group"]) if "group" in g else (0, 0)
+    return ct.TreePmConfig(group_walk_enabled=group_walk, gaussian_pair_lookup=lookup,pm_grid_nx=mesh[0], pm_grid_ny=mesh[1], pm_grid_nz=mesh[2], box_x=float(g["box"][0]),
                            box_y=float(g["box"][1]), box_z=float(g["box"][2]), asmth_cells=asmth, rcut_cells=rcut,
                            opening_theta=theta, opening_criterion=criterion, multipole_order=order,
                            max_leaf_size=leaf, assignment_scheme=scheme, window_deconvolution=deconv,
@@ -72,7 +77,7 @@ def rel_err(got, ref):
     return np.linalg.norm(g - r, axis=0) / np.maximum(den, 1e-6 * scale)
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + GROUP_CASES)
 def test_fp64_adaptive_matches_reference(cuda_ok, name):
     g = load_golden(name)
     with ct.TreePmCoordinator(cfg_for(g, ct._abi.FP64)) as s:
@@ -85,7 +90,7 @@ def test_fp64_adaptive_matches_reference(cuda_ok, name):
     assert [st[k] for k in COUNTER_KEYS] == [int(v) for v in g["counters"]]
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + GROUP_CASES)
 def test_mixed_adaptive_matches_reference(cuda_ok, name):
     """Per-node mixed walk: the reference's decisions and forces. Production
     walk (subtree blocks replace some accepted multipoles by their exact
@@ -106,6 +111,7 @@ def test_mixed_adaptive_matches_reference(cuda_ok, name):
 
     strict = cfg_for(g, ct._abi.FP64)
     strict.acceptance_policy = ct._abi.POLICY_STRICT
+    strict.group_walk_enabled = strict.gaussian_pair_lookup = 0
     with ct.TreePmCoordinator(strict) as s:
         r64 = s.solve_active_set(g["x"], g["y"], g["z"], g["m"], active=_active(g))
     truth = [r64["ax"], r64["ay"], r64["az"]]
@@ -204,3 +210,41 @@ def test_adaptive_clustered_64(cuda_ok, estimator, cutoff_policy, angle, alpha):
     assert abs(out["mixed"][1]["direct_pair_evaluations"] - pairs) <= 1e-6 * pairs
     # the adaptive policy's purpose: fewer pairs than the strict walk of the same state
     assert pairs < r0["stats"]["direct_pair_evaluations"]
+
+
+@pytest.mark.parametrize("cutoff_policy", [ct._abi.CUTOFF_COM_DISTANCE, ct._abi.CUTOFF_CONTAIN_NODE])
+def test_group_walk_clustered_64(cuda_ok, cutoff_policy):
+    """Clustered 64^3 box under the group walk (fast deck settings): the mixed
+    walk's node counters equal the FP64 group walk's (groups decided in FP64 by
+    one lane per group in each warp), its forces meet the mixed bar against
+    it, and the production walk is at least as close to the strict FP64 forces
+    as the FP64 group walk."""
+    n_side, box = 64, 50.0
+    x, y, z, *_ = ics.clustered_box(n_side ** 3, box, 0.6, 120, 3.0, 0.5, 11)
+    m = np.full(len(x), 1.0 / len(x))
+    base = dict(pm_grid_nx=n_side, pm_grid_ny=n_side, pm_grid_nz=n_side, box_x=box, box_y=box, box_z=box,
+                opening_theta=0.5, max_leaf_size=16, softening=0.002)
+    with ct.TreePmCoordinator(ct.TreePmConfig(**base, precision=ct._abi.FP64)) as s:
+        r0 = s.solve_active_set(x, y, z, m)
+    prev = np.sqrt(r0["ax"] ** 2 + r0["ay"] ** 2 + r0["az"] ** 2)
+    prev[::97] = np.nan  # some groups fall back to per-target walks
+    group = dict(acceptance_policy=ct._abi.POLICY_ADAPTIVE, adaptive_error_estimator=ct._abi.ESTIMATOR_RELATIVE_MONOPOLE,
+                 cutoff_node_policy=cutoff_policy, adaptive_maximum_opening_angle=1.0, relative_force_tolerance=0.0025,
+                 group_walk_enabled=1, gaussian_pair_lookup=1)
+    out = {}
+    for key, prec, diag in (("fp64", ct._abi.FP64, 1), ("mixed", ct._abi.MIXED, 1), ("prod", ct._abi.MIXED, 0)):
+        with ct.TreePmCoordinator(ct.TreePmConfig(**base, **group, precision=prec, diagnostics=diag)) as s:
+            r = s.solve_active_set(x, y, z, m, previous_acceleration=prev)
+            out[key] = ([r[k] for k in ("ax", "ay", "az")], dict(r["stats"]))
+    ref, st64 = out["fp64"]
+    assert st64["accepted_internal_multipoles"] > 0
+    e = rel_err(out["mixed"][0], ref)
+    assert np.median(e) <= 1e-4 and np.percentile(e, 99) <= 1e-3, (np.median(e), np.percentile(e, 99))
+    assert [out["mixed"][1][k] for k in NODE_KEYS] == [st64[k] for k in NODE_KEYS]
+    pairs = st64["direct_pair_evaluations"]
+    assert abs(out["mixed"][1]["direct_pair_evaluations"] - pairs) <= 1e-6 * pairs
+    truth = [r0["ax"], r0["ay"], r0["az"]]
+    e_prod = rel_err(out["prod"][0], truth)
+    e_grp = rel_err(ref, truth)
+    assert np.median(e_prod) <= max(1e-4, 1.1 * np.median(e_grp)), (np.median(e_prod), np.median(e_grp))
+    assert np.percentile(e_prod, 99) <= max(1e-3, 1.1 * np.percentile(e_grp, 99))

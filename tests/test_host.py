@@ -44,6 +44,7 @@ def test_config_defaults_match_reference_defaults():
     assert c.cutoff_node_policy == _abi.CUTOFF_CONTAIN_NODE
     assert (c.adaptive_maximum_opening_angle, c.relative_force_tolerance,
             c.relative_force_acceleration_floor) == (0.25, 0.005, 1e-30)
+    assert c.group_walk_enabled == 0 and c.gaussian_pair_lookup == 0
     # the Python mirror carries the same defaults
     py = ct.TreePmConfig().to_c()
     for name, _ in _abi.Config._fields_:
@@ -112,6 +113,8 @@ treepm_adaptive_error_estimator = relative_monopole
 treepm_cutoff_node_policy = com_distance
 treepm_adaptive_maximum_opening_angle = 1.0
 treepm_tree_relative_force_tolerance = 0.0025
+treepm_group_walk_enabled = true
+treepm_gaussian_pair_lookup_enabled = true
 """
 
 
@@ -122,6 +125,7 @@ def test_param_deck_adaptive_keys():
     assert c.cutoff_node_policy == _abi.CUTOFF_COM_DISTANCE
     assert (c.adaptive_maximum_opening_angle, c.relative_force_tolerance) == (1.0, 0.0025)
     assert c.relative_force_acceleration_floor == 1e-30
+    assert c.group_walk_enabled == 1 and c.gaussian_pair_lookup == 1
     with pytest.raises(ValueError):
         ct.config_from_param_text(FAST_DECK.replace("relative_monopole", "bogus"))
     with pytest.raises(ValueError):
