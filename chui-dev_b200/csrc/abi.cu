@@ -64,7 +64,7 @@ __global__ void sourceReduceKernel(int64_t n, const double* __restrict__ x, cons
                                    const double* __restrict__ z, const double* __restrict__ m,
                                    unsigned long long* out, double* mass_sum, uint32_t* status) {
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-  double msum = 0.0;
+  double msum = 0.0, mlo = INFINITY, mhi = -INFINITY;
   uint32_t bad = 0;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -79,6 +79,8 @@ __global__ void sourceReduceKernel(int64_t n, const double* __restrict__ x, cons
       if (!isfinite(mi)) bad |= kStatusNonFinite;
       if (mi < 0.0) bad |= kStatusNegativeMass;
       msum += mi;
+      mlo = fmin(mlo, mi);
+      mhi = fmax(mhi, mi);
     }
   }
   for (int a = 0; a < 3; ++a) {
@@ -89,6 +91,8 @@ __global__ void sourceReduceKernel(int64_t n, const double* __restrict__ x, cons
   }
   for (int off = 16; off > 0; off >>= 1) {
     msum += __shfl_xor_sync(0xffffffffu, msum, off);
+    mlo = fmin(mlo, __shfl_xor_sync(0xffffffffu, mlo, off));
+    mhi = fmax(mhi, __shfl_xor_sync(0xffffffffu, mhi, off));
     bad |= __shfl_xor_sync(0xffffffffu, bad, off);
   }
   if ((threadIdx.x & 31) == 0) {
@@ -96,7 +100,11 @@ __global__ void sourceReduceKernel(int64_t n, const double* __restrict__ x, cons
       atomicMin(out + a, orderedBits(lo[a]));
       atomicMax(out + 3 + a, orderedBits(hi[a]));
     }
-    if (m) atomicAdd(mass_sum, msum);
+    if (m) {
+      atomicAdd(mass_sum, msum);
+      atomicMin(out + 8, orderedBits(mlo));
+      atomicMax(out + 9, orderedBits(mhi));
+    }
     if (bad) atomicOr(status, bad);
   }
 }
@@ -300,12 +308,12 @@ double hostHpp(double t) {
 // Chebyshev interpolation of f on [0, t_cut] rewritten as a polynomial in
 // s = t * 2 / t_cut - 1 (FP32 coefficients).
 template <class F>
-PolyH fitChebyshev(F func, double t_cut, double tolerance = 2.0e-6) {
+PolyH fitChebyshev(F func, double t_cut, double tolerance = 2.0e-6, int short_terms = 12) {
   PolyH best;
   best.max_rel_error = 1e300;
-  // The walk kernel evaluates either 12 terms or kPolyMaxTerms terms (unused
-  // high coefficients are zero); try 12 first, then the longest form.
-  for (int deg : {11, kPolyMaxTerms - 1}) {
+  // The kernels evaluate a short form (`short_terms`) or kPolyMaxTerms terms
+  // (unused high coefficients are zero); try the short one first.
+  for (int deg : {short_terms - 1, kPolyMaxTerms - 1}) {
     const int m = deg + 1;
     std::vector<double> f(m), cheb(m, 0.0);
     const double pi = 3.141592653589793238462643383279502884;
@@ -355,7 +363,10 @@ PolyH fitChebyshev(F func, double t_cut, double tolerance = 2.0e-6) {
   return best;
 }
 
-PolyH fitPoly(double t_cut) { return fitChebyshev(hostH, t_cut); }
+// H for the pair kernel: 10 terms (4.1e-6 relative at r_cut/r_s = 5; the
+// residual's FP32 evaluation error is of the same order) keep two FMAs per
+// pair out of the issue-bound walk; otherwise the long form.
+PolyH fitPoly(double t_cut) { return fitChebyshev(hostH, t_cut, 5.0e-6, kPairPolyTerms); }
 
 int fail(Context& c, int code, const std::string& msg) {
   c.last_error = msg;
@@ -480,15 +491,16 @@ int stageIn(Context& c, DevBuf& buf, const T* src, int64_t count, int memory, cu
 }  // namespace
 
 int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const double* z, const double* m,
-                 double lo[3], double hi[3], double* mass_sum, uint32_t* status_bits, cudaStream_t s) {
+                 double lo[3], double hi[3], double* mass_sum, uint32_t* status_bits, cudaStream_t s,
+                 double* mass_range) {
   auto* sc = c.scalars.as<unsigned long long>();
-  unsigned long long init[8] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+  unsigned long long init[10] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull, 0ull, 0ull, ~0ull, 0ull};
   cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(c.status.ptr, 0, 4, s);
   if (n > 0)
     { noteLaunch(); sourceReduceKernel<<<gridFor(n, 256), 256, 0, s>>>(n, x, y, z, m, sc, reinterpret_cast<double*>(sc + 6),
                                                        c.status.as<uint32_t>()); }
-  unsigned long long hb[8];
+  unsigned long long hb[10];
   uint32_t st = 0;
   cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(&st, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
@@ -501,6 +513,10 @@ int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const 
   std::memcpy(&ms, &hb[6], 8);
   *mass_sum = ms;
   *status_bits = st;
+  if (mass_range) {
+    mass_range[0] = (m && n > 0) ? fromOrderedBits(hb[8]) : 0.0;
+    mass_range[1] = (m && n > 0) ? fromOrderedBits(hb[9]) : 0.0;
+  }
   return 0;
 }
 
@@ -705,9 +721,9 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   if (!src->mass) m = nullptr;
 
   // validateTreePmPreflight (tree_pm_coupling.cpp:244-481)
-  double lo[3], hi[3], mass_sum = 0.0;
+  double lo[3], hi[3], mass_sum = 0.0, mass_range[2] = {0.0, 0.0};
   uint32_t st = 0;
-  if ((rc = chui::sourceBounds(c, n, x, y, z, m, lo, hi, &mass_sum, &st, s))) return rc;
+  if ((rc = chui::sourceBounds(c, n, x, y, z, m, lo, hi, &mass_sum, &st, s, mass_range))) return rc;
   if (st) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources require finite coordinates and finite non-negative masses");
   if (explicit_targets && nt > 0) {
     double tlo[3], thi[3], dummy;
@@ -784,6 +800,10 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   wp.rel_tol = c.cfg.relative_force_tolerance;
   wp.floor_ = c.cfg.relative_force_acceleration_floor;
   wp.gauss_lookup = c.cfg.gaussian_pair_lookup ? 1 : 0;
+  // one mass for every source (no mass lane, or equal entries): the walk
+  // queue then carries a lane mask instead of a mass
+  wp.uniform_mass = !m || mass_range[0] == mass_range[1];
+  wp.m0_f = static_cast<float>(m ? mass_range[0] : src->uniform_mass);
   {
     // group walk eligibility (tree_pm_coupling.cpp:3840-3870, 3922-3925, 4282-4286)
     const double inv_2a2 = (0.25 / c.rs) / c.rs, inv_8a3 = ((0.125 / c.rs) / c.rs) / c.rs;

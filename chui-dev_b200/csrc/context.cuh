@@ -50,6 +50,8 @@ struct WalkParams {
   int com_cutoff;  // adaptive with COM-distance cutoff nodes
   int group_walk;  // the group walk is active for this solve
   int gauss_lookup;  // Gaussian Hermite table for FP64 direct pairs
+  int uniform_mass;  // every source has mass m0
+  float m0_f;
   double angle;    // adaptive_maximum_opening_angle
   double rel_tol;  // relative_force_tolerance
   double floor_;   // relative_force_acceleration_floor_code
@@ -186,7 +188,7 @@ int walkVjpRun(Context& c, int64_t n, const double* sx, const double* sy, const 
 // ---- reductions / small kernels (abi.cu) ----
 int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const double* z,
                  const double* m, double lo[3], double hi[3], double* mass_sum,
-                 uint32_t* status_bits, cudaStream_t s);
+                 uint32_t* status_bits, cudaStream_t s, double* mass_range = nullptr);
 
 const char* statusText(uint32_t bits);
 

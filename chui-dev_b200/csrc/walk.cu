@@ -972,7 +972,10 @@ __device__ __forceinline__ int certainLess(float a, float b, float err = 0.f) {
 // with the group walk: lanes whose group is eligible take their group's
 // decision (made in FP64 by the group's first lane in the warp and broadcast),
 // the others the per-target adaptive decision.
-template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode>
+// kUniform (production, contiguous targets, one source mass): queue entries
+// carry the lane mask in place of the mass, so each entry is one 16-byte load
+// and the mass multiplies the flush's partial sums once.
+template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode, bool kUniform = false>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS) walkFastKernel(WalkArgs a) {
   constexpr bool kAdaptive = kMode >= 2;
   constexpr bool kGroup = kMode == 3;
@@ -996,6 +999,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   const float angle2 = static_cast<float>(w.angle * w.angle);
   const double bulk_half = kBulkHalf * w.cutoff;
   const float sc_r2 = w.inv_4rs2_f * a.poly.scale;
+  const float g_pair = kUniform ? w.G_f * w.m0_f : w.G_f;  // factor on the flush's partial sums
 
   while (true) {
     uint32_t cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0, cnt_skips = 0,
@@ -1081,7 +1085,12 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
 #pragma unroll 4
       for (int k = 0; k < qn; ++k) {
         const float4 e = q_src[warp][k];
-        const uint2 meta = q_meta[warp][k];
+        uint2 meta = make_uint2(0u, 0u);
+        if constexpr (kUniform) {
+          meta.x = __float_as_uint(e.w);
+        } else {
+          meta = q_meta[warp][k];
+        }
         const float dx = e.x - tfx, dy = e.y - tfy, dz = e.z - tfz;
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         const bool mine = kContiguous ? (meta.x & lane_bit) != 0u : ((meta.x & lane_bit) != 0u && meta.y != self_pos);
@@ -1098,14 +1107,14 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         const float k3 = fmaf(-hh, w.inv_8rs3_f, rinv * rinv * rinv);
         // coincident sources contribute nothing: with eps > 0 the kernel is
         // finite there and d = 0; with eps = 0 the zero-distance test avoids inf * 0
-        const float f = (kEpsZero ? (in && r2 > 0.f) : in) ? e.w * k3 : 0.f;
+        const float f = (kEpsZero ? (in && r2 > 0.f) : in) ? (kUniform ? k3 : e.w * k3) : 0.f;
         fx = fmaf(f, dx, fx);
         fy = fmaf(f, dy, fy);
         fz = fmaf(f, dz, fz);
       }
-      acc_x += static_cast<double>(w.G_f * fx);
-      acc_y += static_cast<double>(w.G_f * fy);
-      acc_z += static_cast<double>(w.G_f * fz);
+      acc_x += static_cast<double>(g_pair * fx);
+      acc_y += static_cast<double>(g_pair * fy);
+      acc_z += static_cast<double>(g_pair * fz);
       cnt_pairs += pairs;
       cnt_skips += skips;
       qn = 0;
@@ -1166,8 +1175,13 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
             const uint32_t rel = begin + k - base;
             if (rel < 32u) m &= ~(1u << rel);
           }
-          q_src[warp][slot_q] = e;
-          q_meta[warp][slot_q] = make_uint2(m, begin + k);
+          if constexpr (kUniform) {
+            e.w = __uint_as_float(m);
+            q_src[warp][slot_q] = e;
+          } else {
+            q_src[warp][slot_q] = e;
+            q_meta[warp][slot_q] = make_uint2(m, begin + k);
+          }
         }
         __syncwarp();
         qn += c;
@@ -1890,21 +1904,23 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     // positions base..base+31 and self pairs are excluded by the lane mask
     const bool contiguous = active == nullptr && tx == nullptr && nt == n;
     const bool diag = c.cfg.diagnostics != 0;
+    const bool uniform = wp.uniform_mass != 0;
     const int mode = wp.policy == CHUI_TREEPM_POLICY_ADAPTIVE ? (wp.group_walk ? 3 : 2)
                                                                : (wp.criterion == 2 && prev_acc ? 1 : 0);
 #define CHUI_WALK_DISPATCH2(EPS, TERMS, ADP)                                                           \
     if (diag) return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, true, true, ADP>, a, s)     \
                                 : launchPersistent(walkFastKernel<EPS, TERMS, true, false, ADP>, a, s);   \
-    return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP>, a, s)              \
-                      : launchPersistent(walkFastKernel<EPS, TERMS, false, false, ADP>, a, s);
+    if (contiguous) return uniform ? launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP, true>, a, s)  \
+                                   : launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP>, a, s);      \
+    return launchPersistent(walkFastKernel<EPS, TERMS, false, false, ADP>, a, s);
 #define CHUI_WALK_DISPATCH(EPS, TERMS)                  \
     if (mode == 3) { CHUI_WALK_DISPATCH2(EPS, TERMS, 3) } \
     if (mode == 2) { CHUI_WALK_DISPATCH2(EPS, TERMS, 2) } \
     if (mode == 1) { CHUI_WALK_DISPATCH2(EPS, TERMS, 1) } \
     CHUI_WALK_DISPATCH2(EPS, TERMS, 0)
-    if (c.poly.terms <= 12) {
-      if (eps_zero) { CHUI_WALK_DISPATCH(true, 12) }
-      CHUI_WALK_DISPATCH(false, 12)
+    if (c.poly.terms <= kPairPolyTerms) {
+      if (eps_zero) { CHUI_WALK_DISPATCH(true, kPairPolyTerms) }
+      CHUI_WALK_DISPATCH(false, kPairPolyTerms)
     }
     if (eps_zero) { CHUI_WALK_DISPATCH(true, kPolyMaxTerms) }
     CHUI_WALK_DISPATCH(false, kPolyMaxTerms)
