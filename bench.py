@@ -62,7 +62,7 @@ FLOPS_PER_VISIT = 12.0
 # DRAM bytes of one production walk launch on the workload (ncu
 # dram__bytes_read.sum + dram__bytes_write.sum, one capture of
 # `bench.py --mode profile --workload clustered256`, first walkFast launch)
-WALK_DRAM_BYTES = {"clustered256": 11645360896 + 2439870976}
+WALK_DRAM_BYTES = {"clustered256": 11471892992 + 2385204480}
 # The differentiable case: 64^3 lattice + Zel'dovich (P ~ k^-2, 0.3 spacing
 # rms) in a box of 50, mesh 64^3, theta 0.5, 10 KDK steps of 0.05 at unit mean
 # density (G = 1), softening 0.1 spacing, loss = MSE(CIC density of the final
@@ -263,16 +263,26 @@ def timed_steps(torch, solver, t, acc, factors, steps, warmup, dist=None):
     return e0.elapsed_time(e1), acc, stats, launches
 
 
-def adaptive_fast_deck(torch, ct, w, device, t, r_ref, repeats=3) -> dict:
-    """One force under the adaptive relative policy (the reference's
-    configs/treepm_evolved_snapshot_fast deck settings), production walk:
-    device time of the solve and its error against the strict FP64 forces."""
-    cfg = make_config(w, ct._abi.MIXED, device, diagnostics=0)
+def apply_fast_deck(ct, cfg, group=False):
+    """The reference's production fast deck: adaptive relative monopole,
+    COM-distance cutoff nodes, alpha 0.0025, maximum angle 1.0 (optionally
+    the group walk with the Gaussian pair table)."""
     cfg.acceptance_policy = ct._abi.POLICY_ADAPTIVE
     cfg.adaptive_error_estimator = ct._abi.ESTIMATOR_RELATIVE_MONOPOLE
     cfg.cutoff_node_policy = ct._abi.CUTOFF_COM_DISTANCE
     cfg.adaptive_maximum_opening_angle = 1.0
     cfg.relative_force_tolerance = 0.0025
+    if group:
+        cfg.group_walk_enabled = 1
+        cfg.gaussian_pair_lookup = 1
+    return cfg
+
+
+def adaptive_fast_deck(torch, ct, w, device, t, r_ref, repeats=3) -> dict:
+    """One force under the adaptive relative policy (the reference's
+    configs/treepm_evolved_snapshot_fast deck settings), production walk:
+    device time of the solve and its error against the strict FP64 forces."""
+    cfg = apply_fast_deck(ct, make_config(w, ct._abi.MIXED, device, diagnostics=0))
     prev = torch.sqrt(r_ref["ax"] ** 2 + r_ref["ay"] ** 2 + r_ref["az"] ** 2)
     n = len(t["x"])
     with ct.TreePmCoordinator(cfg) as s:
@@ -476,14 +486,24 @@ def run_profile(args) -> int:
     """Two production (mixed precision, diagnostics off) force evaluations of
     the workload (the second is the one an ncu capture selects with -s/-c),
     nothing else: for launch lists and single-kernel captures. --mode
-    profile-vjp runs two force VJPs instead."""
+    profile-vjp runs two force VJPs instead. --deck fast / fast-group: the
+    adaptive fast deck (per-target / group walk), history from a first
+    strict solve."""
     import torch
     import chui_treepm as ct
     w = WORKLOADS[args.workload]
     x, y, z, m, vx, vy, vz = make_particles(w, seed=42)
     dev = torch.device("cuda", 0)
     t = {k: torch.tensor(v, device=dev) for k, v in dict(x=x, y=y, z=z, m=m).items()}
-    with ct.TreePmCoordinator(make_config(w, ct._abi.MIXED, 0, diagnostics=0)) as s:
+    cfg = make_config(w, ct._abi.MIXED, 0, diagnostics=0)
+    prev = None
+    if args.deck != "strict":
+        with ct.TreePmCoordinator(cfg) as s:
+            r = s.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+            prev = torch.sqrt(r["ax"] ** 2 + r["ay"] ** 2 + r["az"] ** 2)
+            del r
+        apply_fast_deck(ct, cfg, group=args.deck == "fast-group")
+    with ct.TreePmCoordinator(cfg) as s:
         if args.mode == "profile-vjp":
             # two force VJPs with seeded Gaussian cotangents (the adjoint's hot call)
             g = torch.Generator(device="cpu").manual_seed(1)
@@ -494,7 +514,7 @@ def run_profile(args) -> int:
             log(json.dumps(s.last_vjp_stats))
             return 0
         for _ in range(2):
-            s.solve_active_set(t["x"], t["y"], t["z"], t["m"])
+            s.solve_active_set(t["x"], t["y"], t["z"], t["m"], previous_acceleration=prev)
         torch.cuda.synchronize()
         log(json.dumps(s.last_stats))
     return 0
@@ -630,6 +650,8 @@ def main() -> int:
     ap.add_argument("--cpu-fraction", type=float, default=1.0 / 64.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--mode", default="bench", choices=["bench", "profile", "profile-vjp", "large"])
+    ap.add_argument("--deck", default="strict", choices=["strict", "fast", "fast-group"],
+                    help="acceptance settings of --mode profile")
     args = ap.parse_args()
     if args.mode in ("profile", "profile-vjp"):
         return run_profile(args)

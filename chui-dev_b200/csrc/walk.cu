@@ -1582,7 +1582,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpA
         const bool in = valid && r2 <= cut2 && r2 > Real(0);
         Real K, Kp;
         if constexpr (sizeof(Real) == 4) {
-          const float hh = hornerR2<kTerms>(a.poly, r2, w.inv_4rs2_f * a.poly.scale);
+          // H in its pair-kernel length when it fits (the short fit has 10 terms)
+          const float hh = hornerR2<(kTerms == 12 ? kPairPolyTerms : kTerms)>(a.poly, r2, w.inv_4rs2_f * a.poly.scale);
           const float hp = hornerR2<kTerms>(a.dpoly, r2, w.inv_4rs2_f * a.dpoly.scale);
           const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
           const float rinv = rsqrtf(s2);
@@ -1981,7 +1982,7 @@ int walkVjpRun(Context& c, int64_t n, const double* sx, const double* sy, const 
   a.inv_16rs5_f = static_cast<float>(1.0 / (16.0 * rs2 * rs2 * c.rs));
   const bool eps_zero = wp.eps == 0.0;
   if (c.cfg.precision == CHUI_TREEPM_MIXED) {
-    if (c.poly.terms <= 12 && c.dpoly.terms <= 12)
+    if (c.poly.terms <= kPairPolyTerms && c.dpoly.terms <= 12)
       return eps_zero ? launchVjp(walkVjpKernel<float, true, 12>, a, s) : launchVjp(walkVjpKernel<float, false, 12>, a, s);
     return eps_zero ? launchVjp(walkVjpKernel<float, true, kPolyMaxTerms>, a, s)
                     : launchVjp(walkVjpKernel<float, false, kPolyMaxTerms>, a, s);
