@@ -38,6 +38,8 @@ class Params(C.Structure):
         ("accel_floor", C.c_double),
         ("group_walk", C.c_int32),
         ("gaussian_lookup", C.c_int32),
+        ("boundary", C.c_int32),
+        ("reserved2", C.c_int32),
     ]
 
 
@@ -49,7 +51,7 @@ class Counters(C.Structure):
 def make_params(box=(1.0, 1.0, 1.0), mesh=(16, 16, 16), asmth=1.25, rcut=6.25, theta=0.5, g=1.0,
                 eps=0.0, leaf=16, scheme=0, deconv=0, criterion=1, quadrupole=1, policy=0, estimator=0,
                 cutoff_policy=0, adaptive_angle=0.25, rel_tol=0.005, accel_floor=1e-30, group_walk=0,
-                gaussian_lookup=0) -> Params:
+                gaussian_lookup=0, boundary=0) -> Params:
     """Defaults are TreePmOptions' (include/cosmosim/gravity/tree_pm_coupling.hpp:243-332):
     strict-reference policy; the adaptive fields apply with policy=1 (estimator 0 residual
     derivative / 1 relative monopole, cutoff_policy 0 contain node / 1 COM distance)."""
@@ -74,6 +76,7 @@ def make_params(box=(1.0, 1.0, 1.0), mesh=(16, 16, 16), asmth=1.25, rcut=6.25, t
     p.accel_floor = accel_floor
     p.group_walk = group_walk
     p.gaussian_lookup = gaussian_lookup
+    p.boundary = boundary
     return p
 
 

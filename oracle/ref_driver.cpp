@@ -105,6 +105,8 @@ struct Problem {
   std::vector<double> prev;
   // optional "CHUIGRP1" block after it: group walk and Gaussian pair lookup
   std::int64_t group_walk = 0, gaussian_lookup = 0;
+  // optional "CHUIISO1" block after it: PM boundary condition (1 isolated/open)
+  std::int64_t boundary = 0;
 };
 
 Problem readProblem(const char* path) {
@@ -165,6 +167,10 @@ Problem readProblem(const char* path) {
       if (std::memcmp(tail, "CHUIGRP1", 8) != 0) throw std::runtime_error("bad trailing block");
       p.group_walk = r.get<std::int64_t>();
       p.gaussian_lookup = r.get<std::int64_t>();
+      if (std::fread(tail, 1, 8, f) == 8) {
+        if (std::memcmp(tail, "CHUIISO1", 8) != 0) throw std::runtime_error("bad trailing block");
+        p.boundary = r.get<std::int64_t>();
+      }
     }
   }
   std::fclose(f);
@@ -181,6 +187,8 @@ cg::TreePmOptions makeOptions(const Problem& p) {
   o.pm_options.gravitational_constant_code = p.g;
   o.pm_options.assignment_scheme = p.scheme == 1 ? cg::PmAssignmentScheme::kTsc : cg::PmAssignmentScheme::kCic;
   o.pm_options.enable_window_deconvolution = p.deconv != 0;
+  o.pm_options.boundary_condition =
+      p.boundary == 1 ? cg::PmBoundaryCondition::kIsolatedOpen : cg::PmBoundaryCondition::kPeriodic;
   o.tree_options.gravitational_constant_code = p.g;
   o.tree_options.opening_theta = p.theta;
   o.tree_options.opening_criterion = p.criterion == 0 ? cg::TreeOpeningCriterion::kBarnesHutGeometric
@@ -281,9 +289,11 @@ int main(int argc, char** argv) {
     const std::size_t nn = p.dump_tree ? nodes.size() : 0U;
     w.put<std::int64_t>(static_cast<std::int64_t>(nn));
     if (p.dump_tree) {
-      w.vec(coordinator.*get(TreeXTag()));
-      w.vec(coordinator.*get(TreeYTag()));
-      w.vec(coordinator.*get(TreeZTag()));
+      // isolated/open boundaries build the tree on the caller's coordinates
+      const bool unwrapped = !(coordinator.*get(TreeXTag())).empty();
+      w.vec(unwrapped ? coordinator.*get(TreeXTag()) : p.x);
+      w.vec(unwrapped ? coordinator.*get(TreeYTag()) : p.y);
+      w.vec(unwrapped ? coordinator.*get(TreeZTag()) : p.z);
       const auto anchors = coordinator.*get(AnchorTag());
       for (double a : anchors) w.put<double>(a);
       w.vec(ordering.morton_key);

@@ -62,6 +62,7 @@ class RefProblem:
     prev_acc: np.ndarray | None = None  # per active target |a_previous|
     group_walk: int = 0       # TreePmOptions::group_walk_enabled
     gaussian_lookup: int = 0  # TreePmOptions::gaussian_pair_lookup_enabled
+    boundary: int = 0         # PmBoundaryCondition: 0 periodic, 1 isolated/open
 
 
 def write_problem(path: str, p: RefProblem) -> None:
@@ -83,7 +84,7 @@ def write_problem(path: str, p: RefProblem) -> None:
                   p.vz if p.vz is not None else zeros):
             f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
         f.write(active.tobytes())
-        grp = p.group_walk or p.gaussian_lookup
+        grp = p.group_walk or p.gaussian_lookup or p.boundary
         if p.policy or p.prev_acc is not None or p.rel_tol != 0.005 or p.accel_floor != 1e-30 or grp:
             f.write(b"CHUIADP1")
             f.write(struct.pack("<4q", p.policy, p.estimator, p.cutoff_policy, int(p.prev_acc is not None)))
@@ -96,6 +97,9 @@ def write_problem(path: str, p: RefProblem) -> None:
             if grp:
                 f.write(b"CHUIGRP1")
                 f.write(struct.pack("<2q", p.group_walk, p.gaussian_lookup))
+                if p.boundary:
+                    f.write(b"CHUIISO1")
+                    f.write(struct.pack("<q", p.boundary))
 
 
 class _Buf:

@@ -149,6 +149,9 @@ void oracle_pm_cells(int64_t n, const double *x, const double *y, const double *
 
 /* assignDensityImpl serial periodic branch, pm_solver.cpp:4015-4057, then
  * the /cell_volume normalization :4544-4554. Compact (nx, ny, nz) layout. */
+/* positionInsideOpenDomain, pm_solver.cpp:117-119 */
+static int inside_open(double v, double box) { return v >= 0.0 && v < box; }
+
 void oracle_pm_density(int64_t n, const double *x, const double *y, const double *z,
                        const double *m, const oracle_params *p, double *rho) {
   const int64_t nx = p->mesh[0], ny = p->mesh[1], nz = p->mesh[2];
@@ -157,16 +160,23 @@ void oracle_pm_density(int64_t n, const double *x, const double *y, const double
   const double inv_dx = (double)nx / p->box[0];
   const double inv_dy = (double)ny / p->box[1];
   const double inv_dz = (double)nz / p->box[2];
+  const int per = p->boundary == 0;
   for (int64_t i = 0; i < n; ++i) {
-    const stencil1d sx = make_stencil(wrap_position(x[i], p->box[0]) * inv_dx, p->scheme);
-    const stencil1d sy = make_stencil(wrap_position(y[i], p->box[1]) * inv_dy, p->scheme);
-    const stencil1d sz = make_stencil(wrap_position(z[i], p->box[2]) * inv_dz, p->scheme);
+    /* isolated/open: particles outside [0, L) and stencil cells outside the mesh are skipped (:4016-4049) */
+    if (!per && !(inside_open(x[i], p->box[0]) && inside_open(y[i], p->box[1]) && inside_open(z[i], p->box[2])))
+      continue;
+    const stencil1d sx = make_stencil((per ? wrap_position(x[i], p->box[0]) : x[i]) * inv_dx, p->scheme);
+    const stencil1d sy = make_stencil((per ? wrap_position(y[i], p->box[1]) : y[i]) * inv_dy, p->scheme);
+    const stencil1d sz = make_stencil((per ? wrap_position(z[i], p->box[2]) : z[i]) * inv_dz, p->scheme);
     for (int a = 0; a < sx.count; ++a) {
-      const int64_t ix = wrap_index(sx.off[a], nx);
+      if (!per && (sx.off[a] < 0 || sx.off[a] >= nx)) continue;
+      const int64_t ix = per ? wrap_index(sx.off[a], nx) : sx.off[a];
       for (int b = 0; b < sy.count; ++b) {
-        const int64_t iy = wrap_index(sy.off[b], ny);
+        if (!per && (sy.off[b] < 0 || sy.off[b] >= ny)) continue;
+        const int64_t iy = per ? wrap_index(sy.off[b], ny) : sy.off[b];
         for (int c = 0; c < sz.count; ++c) {
-          const int64_t iz = wrap_index(sz.off[c], nz);
+          if (!per && (sz.off[c] < 0 || sz.off[c] >= nz)) continue;
+          const int64_t iz = per ? wrap_index(sz.off[c], nz) : sz.off[c];
           const double w = sx.w[a] * sy.w[b] * sz.w[c];
           rho[((size_t)ix * ny + iy) * nz + iz] += m[i] * w;
         }
@@ -187,9 +197,93 @@ static double sinc(double v) {
  * subtraction), :4712 (r2c), applyDerivedPoissonOperator :2557-2656 with the
  * axis metadata of ensureSpectralAxisMetadata :2398-2466, fillGradientSpectrum
  * :2658-2706 and the normalized c2r per axis :4865-4924. */
+/* solvePoissonIsolatedOpen single-rank path, pm_solver.cpp:4942-5337: zero-padded
+ * (2n)^3 complex convolution of the density with the split Green function
+ * -erf(r / 2 r_s) / r (r = 0: -1 / (sqrt(pi) r_s)), potential = G dV conv / pad_total,
+ * force = -gradient by central differences, one-sided second order at the faces. */
+static void pm_force_grids_isolated(int64_t n, const double *x, const double *y, const double *z,
+                                    const double *m, const oracle_params *p, double *fx, double *fy,
+                                    double *fz) {
+  const int64_t nx = p->mesh[0], ny = p->mesh[1], nz = p->mesh[2];
+  const size_t cells = (size_t)nx * ny * nz;
+  const int64_t px = 2 * nx, py = 2 * ny, pz = 2 * nz;
+  const size_t pad_total = (size_t)px * py * pz;
+  double *rho = (double *)malloc(sizeof(double) * cells);
+  oracle_pm_density(n, x, y, z, m, p, rho);
+  double *rk = (double *)calloc(2 * pad_total, sizeof(double));
+  for (int64_t ix = 0; ix < nx; ++ix)
+    for (int64_t iy = 0; iy < ny; ++iy)
+      for (int64_t iz = 0; iz < nz; ++iz) rk[2 * (((size_t)ix * py + iy) * pz + iz)] = rho[((size_t)ix * ny + iy) * nz + iz];
+  free(rho);
+  oracle_fft3d_c2c(rk, (int)px, (int)py, (int)pz, -1);
+  const double dx = p->box[0] / (double)nx, dy = p->box[1] / (double)ny, dz = p->box[2] / (double)nz;
+  const double rs = p->asmth_cells * oracle_mesh_spacing(p);
+  double *kk = (double *)calloc(2 * pad_total, sizeof(double));
+  for (int64_t ix = 0; ix < px; ++ix) {
+    const double rx = (double)(ix <= nx ? ix : ix - px) * dx;
+    for (int64_t iy = 0; iy < py; ++iy) {
+      const double ry = (double)(iy <= ny ? iy : iy - py) * dy;
+      for (int64_t iz = 0; iz < pz; ++iz) {
+        const double rz = (double)(iz <= nz ? iz : iz - pz) * dz;
+        const double r = sqrt(rx * rx + ry * ry + rz * rz);
+        double kernel;
+        if (r > 0.0) {
+          kernel = rs > 0.0 ? -erf(0.5 * r / rs) / r : -1.0 / r;
+        } else {
+          kernel = -1.0 / (sqrt(acos(-1.0)) * rs);
+        }
+        kk[2 * (((size_t)ix * py + iy) * pz + iz)] = kernel;
+      }
+    }
+  }
+  oracle_fft3d_c2c(kk, (int)px, (int)py, (int)pz, -1);
+  for (size_t i = 0; i < pad_total; ++i) {
+    const double ar = rk[2 * i], ai = rk[2 * i + 1], br = kk[2 * i], bi = kk[2 * i + 1];
+    rk[2 * i] = ar * br - ai * bi;
+    rk[2 * i + 1] = ar * bi + ai * br;
+  }
+  free(kk);
+  oracle_fft3d_c2c(rk, (int)px, (int)py, (int)pz, +1);
+  const double prefactor = p->G * (dx * dy * dz);
+  double *phi = (double *)malloc(sizeof(double) * cells);
+  for (int64_t ix = 0; ix < nx; ++ix)
+    for (int64_t iy = 0; iy < ny; ++iy)
+      for (int64_t iz = 0; iz < nz; ++iz) {
+        double value = rk[2 * (((size_t)ix * py + iy) * pz + iz)];
+        value /= (double)pad_total;
+        phi[((size_t)ix * ny + iy) * nz + iz] = prefactor * value;
+      }
+  free(rk);
+#define PHI(a, b, c) phi[((size_t)(a) * ny + (b)) * nz + (c)]
+  for (int64_t ix = 0; ix < nx; ++ix)
+    for (int64_t iy = 0; iy < ny; ++iy)
+      for (int64_t iz = 0; iz < nz; ++iz) {
+        double gx, gy, gz;
+        if (ix == 0) gx = (-3.0 * PHI(0, iy, iz) + 4.0 * PHI(1, iy, iz) - PHI(2, iy, iz)) / (2.0 * dx);
+        else if (ix + 1 == nx) gx = (3.0 * PHI(nx - 1, iy, iz) - 4.0 * PHI(nx - 2, iy, iz) + PHI(nx - 3, iy, iz)) / (2.0 * dx);
+        else gx = (PHI(ix + 1, iy, iz) - PHI(ix - 1, iy, iz)) / (2.0 * dx);
+        if (iy == 0) gy = (-3.0 * PHI(ix, 0, iz) + 4.0 * PHI(ix, 1, iz) - PHI(ix, 2, iz)) / (2.0 * dy);
+        else if (iy + 1 == ny) gy = (3.0 * PHI(ix, ny - 1, iz) - 4.0 * PHI(ix, ny - 2, iz) + PHI(ix, ny - 3, iz)) / (2.0 * dy);
+        else gy = (PHI(ix, iy + 1, iz) - PHI(ix, iy - 1, iz)) / (2.0 * dy);
+        if (iz == 0) gz = (-3.0 * PHI(ix, iy, 0) + 4.0 * PHI(ix, iy, 1) - PHI(ix, iy, 2)) / (2.0 * dz);
+        else if (iz + 1 == nz) gz = (3.0 * PHI(ix, iy, nz - 1) - 4.0 * PHI(ix, iy, nz - 2) + PHI(ix, iy, nz - 3)) / (2.0 * dz);
+        else gz = (PHI(ix, iy, iz + 1) - PHI(ix, iy, iz - 1)) / (2.0 * dz);
+        const size_t c = ((size_t)ix * ny + iy) * nz + iz;
+        fx[c] = -gx;
+        fy[c] = -gy;
+        fz[c] = -gz;
+      }
+#undef PHI
+  free(phi);
+}
+
 void oracle_pm_force_grids(int64_t n, const double *x, const double *y, const double *z,
                            const double *m, const oracle_params *p,
                            double *fx, double *fy, double *fz) {
+  if (p->boundary == 1) {
+    pm_force_grids_isolated(n, x, y, z, m, p, fx, fy, fz);
+    return;
+  }
   const int64_t nx = p->mesh[0], ny = p->mesh[1], nz = p->mesh[2];
   const size_t cells = (size_t)nx * ny * nz;
   const int64_t nzc = nz / 2 + 1;
@@ -284,18 +378,26 @@ void oracle_pm_interpolate(const oracle_params *p, const double *fx, const doubl
   const double inv_dx = (double)nx / p->box[0];
   const double inv_dy = (double)ny / p->box[1];
   const double inv_dz = (double)nz / p->box[2];
+  const int per = p->boundary == 0;
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < nt; ++i) {
-    const stencil1d sx = make_stencil(wrap_position(tx[i], p->box[0]) * inv_dx, p->scheme);
-    const stencil1d sy = make_stencil(wrap_position(ty[i], p->box[1]) * inv_dy, p->scheme);
-    const stencil1d sz = make_stencil(wrap_position(tz[i], p->box[2]) * inv_dz, p->scheme);
+    if (!per && !(inside_open(tx[i], p->box[0]) && inside_open(ty[i], p->box[1]) && inside_open(tz[i], p->box[2]))) {
+      ax[i] = ay[i] = az[i] = 0.0; /* :5905-5913 */
+      continue;
+    }
+    const stencil1d sx = make_stencil((per ? wrap_position(tx[i], p->box[0]) : tx[i]) * inv_dx, p->scheme);
+    const stencil1d sy = make_stencil((per ? wrap_position(ty[i], p->box[1]) : ty[i]) * inv_dy, p->scheme);
+    const stencil1d sz = make_stencil((per ? wrap_position(tz[i], p->box[2]) : tz[i]) * inv_dz, p->scheme);
     double gx = 0.0, gy = 0.0, gz = 0.0;
     for (int a = 0; a < sx.count; ++a) {
-      const int64_t ix = wrap_index(sx.off[a], nx);
+      if (!per && (sx.off[a] < 0 || sx.off[a] >= nx)) continue;
+      const int64_t ix = per ? wrap_index(sx.off[a], nx) : sx.off[a];
       for (int b = 0; b < sy.count; ++b) {
-        const int64_t iy = wrap_index(sy.off[b], ny);
+        if (!per && (sy.off[b] < 0 || sy.off[b] >= ny)) continue;
+        const int64_t iy = per ? wrap_index(sy.off[b], ny) : sy.off[b];
         for (int c = 0; c < sz.count; ++c) {
-          const int64_t iz = wrap_index(sz.off[c], nz);
+          if (!per && (sz.off[c] < 0 || sz.off[c] >= nz)) continue;
+          const int64_t iz = per ? wrap_index(sz.off[c], nz) : sz.off[c];
           const double w = sx.w[a] * sy.w[b] * sz.w[c];
           const size_t idx = ((size_t)ix * ny + iy) * nz + iz;
           gx += w * fx[idx];
@@ -744,6 +846,7 @@ typedef struct {
   const gauss_table *gt;      /* Gaussian pair lookup (NULL: analytic) */
   double inv_2a2, inv_8a3;    /* 1/(2 r_s)^2, 1/(8 r_s^3) */
   int scaling_ok;             /* both normal (tree_pm_coupling.cpp:3922-3925) */
+  double len[3];              /* periodic box lengths; 0 for isolated/open (:3560-3562) */
 } walk_ctx;
 
 /* monopolePlusQuadrupoleAccelPeriodicReference, tree_pm_coupling.cpp:743-827 */
@@ -922,8 +1025,8 @@ static void walk_target(const walk_ctx *w, double px, double py, double pz, uint
   const double tg[3] = {px, py, pz};
   metric sm[3], nm[3];
   for (int a = 0; a < 3; ++a) {
-    sm[a] = metric_make(w->src_lo[a], w->src_hi[a], tg[a], w->p->box[a]);
-    nm[a] = metric_make(w->node_lo[a], w->node_hi[a], tg[a], w->p->box[a]);
+    sm[a] = metric_make(w->src_lo[a], w->src_hi[a], tg[a], w->len[a]);
+    nm[a] = metric_make(w->node_lo[a], w->node_hi[a], tg[a], w->len[a]);
   }
   size_t sp = 0;
   stack[sp++] = 0;
@@ -1052,9 +1155,9 @@ static void group_build_list(const walk_ctx *w, const double center[3], const do
     const uint32_t node = stack[--sp];
     ++cnt->visited;
     const double h = t->half[node];
-    const double dc[3] = {group_nearest_image(t->cx[node] - center[0], w->p->box[0]),
-                          group_nearest_image(t->cy[node] - center[1], w->p->box[1]),
-                          group_nearest_image(t->cz[node] - center[2], w->p->box[2])};
+    const double dc[3] = {group_nearest_image(t->cx[node] - center[0], w->len[0]),
+                          group_nearest_image(t->cy[node] - center[1], w->len[1]),
+                          group_nearest_image(t->cz[node] - center[2], w->len[2])};
     double gap2 = 0.0, far2 = 0.0;
     for (int a = 0; a < 3; ++a) {
       const double ad = fabs(dc[a]);
@@ -1081,9 +1184,9 @@ static void group_build_list(const walk_ctx *w, const double center[3], const do
     }
     int accept = gap2 > 0.0 && (!contain || far2 <= w->cutoff2);
     if (accept) {
-      const double dm[3] = {group_nearest_image(t->comx[node] - center[0], w->p->box[0]),
-                            group_nearest_image(t->comy[node] - center[1], w->p->box[1]),
-                            group_nearest_image(t->comz[node] - center[2], w->p->box[2])};
+      const double dm[3] = {group_nearest_image(t->comx[node] - center[0], w->len[0]),
+                            group_nearest_image(t->comy[node] - center[1], w->len[1]),
+                            group_nearest_image(t->comz[node] - center[2], w->len[2])};
       double r_min2 = 0.0;
       for (int a = 0; a < 3; ++a) {
         const double gap = fabs(dm[a]) - half[a] > 0.0 ? fabs(dm[a]) - half[a] : 0.0;
@@ -1113,7 +1216,7 @@ static void group_build_list(const walk_ctx *w, const double center[3], const do
 static void group_pairs(const walk_ctx *w, double px, double py, double pz, size_t begin, size_t end,
                         uint32_t self_row, double acc[3], uint64_t *pairs, double *nearest) {
   const oracle_tree *t = w->t;
-  const double lx = w->p->box[0], ly = w->p->box[1], lz = w->p->box[2];
+  const double lx = w->len[0], ly = w->len[1], lz = w->len[2];
   const double hx = 0.5 * lx, hy = 0.5 * ly, hz = 0.5 * lz;
   const double t_limit = nextafter(64.0, 0.0);
   const double eps2 = w->p->epsilon * w->p->epsilon;
@@ -1151,7 +1254,7 @@ static void group_pairs(const walk_ctx *w, double px, double py, double pz, size
 static int group_evaluate(const walk_ctx *w, const double *tx, const double *ty, const double *tz,
                           const uint32_t *rows, const double *prev, const int64_t *slots, size_t count,
                           uint32_t *stack, size_t stack_cap, group_list *list, double *res, oracle_counters *cnt) {
-  const double len[3] = {w->p->box[0], w->p->box[1], w->p->box[2]};
+  const double len[3] = {w->len[0], w->len[1], w->len[2]};
   double a_min = INFINITY, ref[3] = {0, 0, 0}, low[3] = {0, 0, 0}, high[3] = {0, 0, 0};
   for (size_t i = 0; i < count; ++i) {
     const int64_t k = slots[i];
@@ -1271,7 +1374,7 @@ int oracle_treepm_solve2(int64_t n, const double *x, const double *y, const doub
     }
   }
   const double min_box = fmin(p->box[0], fmin(p->box[1], p->box[2]));
-  if (!(cutoff < nextafter(0.5 * min_box, 0.0))) return 1; /* :374-381 */
+  if (p->boundary == 0 && !(cutoff < nextafter(0.5 * min_box, 0.0))) return 1; /* :374-381 */
 
   /* targets */
   double *tx = (double *)malloc(sizeof(double) * (size_t)(na ? na : 1));
@@ -1303,6 +1406,10 @@ int oracle_treepm_solve2(int64_t n, const double *x, const double *y, const doub
   double *uz = (double *)malloc(sizeof(double) * (size_t)(n ? n : 1));
   double *u[3] = {ux, uy, uz};
   for (int a = 0; a < 3; ++a) {
+    if (p->boundary != 0) { /* isolated/open: the tree takes the caller's coordinates (:3179-3196) */
+      memcpy(u[a], pos[a], sizeof(double) * (size_t)n);
+      continue;
+    }
     const int canonical = src_lo[a] >= 0.0 && src_hi[a] < p->box[a];
     oracle_unwrap_axis(n, pos[a], p->box[a], canonical, u[a]);
   }
@@ -1321,6 +1428,7 @@ int oracle_treepm_solve2(int64_t n, const double *x, const double *y, const doub
   w.t = t;
   w.p = p;
   w.rs = rs;
+  for (int a = 0; a < 3; ++a) w.len[a] = p->boundary == 0 ? p->box[a] : 0.0;
   w.cutoff = cutoff;
   w.cutoff2 = cutoff * cutoff;
   for (int a = 0; a < 3; ++a) {

@@ -40,6 +40,8 @@ typedef struct {
   double accel_floor;    /* tree relative_force_acceleration_floor_code */
   int32_t group_walk;      /* TreePmOptions::group_walk_enabled (leaf grouping, blocks of 64) */
   int32_t gaussian_lookup; /* TreePmOptions::gaussian_pair_lookup_enabled (Hermite pair table) */
+  int32_t boundary;        /* PmBoundaryCondition: 0 periodic, 1 isolated/open */
+  int32_t reserved2;
 } oracle_params;
 
 typedef struct {

@@ -39,6 +39,8 @@ def golden_params(g):
                         adaptive_angle=angle, rel_tol=rel_tol, accel_floor=floor)
     if "group" in g:
         adaptive["group_walk"], adaptive["gaussian_lookup"] = (int(v) for v in g["group"])
+    if "boundary" in g:
+        adaptive["boundary"] = int(g["boundary"][0])
     return oracle.make_params(box=tuple(g["box"]), mesh=tuple(int(v) for v in g["mesh"]), asmth=asmth,
                               rcut=rcut, theta=theta, g=gconst, eps=eps, leaf=leaf, scheme=scheme,
                               deconv=deconv, criterion=criterion, quadrupole=1 if order == 2 else 0,

@@ -68,6 +68,8 @@ def save(name: str, p: refio.RefProblem, r: dict, extra: dict | None = None, kee
             d["prev_acc"] = np.asarray(p.prev_acc, dtype=np.float64)
         if p.group_walk or p.gaussian_lookup:
             d["group"] = np.array([p.group_walk, p.gaussian_lookup], dtype=np.int64)
+    if p.boundary:
+        d["boundary"] = np.array([p.boundary], dtype=np.int64)
     if extra:
         d.update(extra)
     np.savez_compressed(os.path.join(OUT, name + ".npz"), **d)
@@ -169,6 +171,24 @@ def main():
                          adaptive_angle=0.5, rel_tol=0.005, prev_acc=prev[active], active=active,
                          group_walk=1, gaussian_lookup=1)
     save("group_walk_active", p, refio.run(p))
+
+    # 7. isolated/open boundaries (PmBoundaryCondition::kIsolatedOpen): a clustered
+    #    distribution in the middle of the box plus particles on and beyond the faces
+    #    (outside [0, L) they take no PM force and deposit nothing), zero-padded PM,
+    #    non-periodic tree
+    x, y, z, *_ = ics.clustered_box(12 ** 3, 10.0, 0.5, 6, 2.0, 0.4, 3)
+    x, y, z = 2.5 + 0.5 * x, 2.5 + 0.5 * y, 2.5 + 0.5 * z
+    x[:6] = [-0.1, 10.2, 3.0, 9.999, 0.0, 5.0]
+    z[5] = 10.0
+    rng = np.random.default_rng(31)
+    m = rng.uniform(0.5, 1.5, len(x)) / len(x)
+    p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(16,) * 3, theta=0.5, leaf=8, boundary=1)
+    save("isolated_cic", p, refio.run(p))
+    active = np.sort(rng.choice(len(x), 600, replace=False)).astype(np.uint32)
+    active[:4] = [0, 1, 3, 5]
+    p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(16,) * 3, theta=0.6, leaf=8, eps=0.02, scheme=1,
+                         active=active, boundary=1)
+    save("isolated_tsc_active", p, refio.run(p))
 
 
 if __name__ == "__main__":
