@@ -20,6 +20,7 @@ OPEN_GEOMETRIC, OPEN_COM_DISTANCE, OPEN_RELATIVE = 0, 1, 2
 POLICY_STRICT, POLICY_ADAPTIVE = 0, 1
 ESTIMATOR_RESIDUAL_DERIVATIVE, ESTIMATOR_RELATIVE_MONOPOLE = 0, 1
 CUTOFF_CONTAIN_NODE, CUTOFF_COM_DISTANCE = 0, 1
+BOUNDARY_PERIODIC, BOUNDARY_ISOLATED_OPEN = 0, 1
 
 
 class Config(C.Structure):
@@ -37,6 +38,7 @@ class Config(C.Structure):
         ("adaptive_maximum_opening_angle", C.c_double), ("relative_force_tolerance", C.c_double),
         ("relative_force_acceleration_floor", C.c_double),
         ("group_walk_enabled", C.c_int32), ("gaussian_pair_lookup", C.c_int32),
+        ("boundary_condition", C.c_int32),
     ]
 
 

@@ -109,6 +109,14 @@ def config_from_param_text(text: str, precision: int = _abi.MIXED, device: int =
         raise ValueError(f"key 'numerics.treepm_cutoff_node_policy': invalid value '{cut}'")
     c.cutoff_node_policy = _CUTOFF_POLICIES[cut]
     c.group_walk_enabled = 1 if get("numerics.treepm_group_walk_enabled", _bool, False) else 0
+    # mode.gravity_boundary (config.cpp:1148-1160): periodic, isolated_monopole, or auto =
+    # periodic for the cosmo_cube and zoom_in modes (:3437-3439), the default mode being zoom_in
+    gb = get("mode.gravity_boundary", lambda v: v.strip().lower(), "auto")
+    if gb not in ("auto", "periodic", "isolated_monopole"):
+        raise ValueError(f"key 'mode.gravity_boundary': invalid value '{gb}'")
+    mode = get("mode.mode", lambda v: v.strip().lower(), "zoom_in")
+    periodic = gb == "periodic" or (gb == "auto" and mode in ("cosmo_cube", "zoom_in"))
+    c.boundary_condition = _abi.BOUNDARY_PERIODIC if periodic else _abi.BOUNDARY_ISOLATED_OPEN
     c.gaussian_pair_lookup = 1 if get("numerics.treepm_gaussian_pair_lookup_enabled", _bool, False) else 0
     soft = kv.get("numerics.gravity_softening")
     if soft:

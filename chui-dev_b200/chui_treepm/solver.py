@@ -94,6 +94,7 @@ class TreePmConfig:
     relative_force_acceleration_floor: float = 1.0e-30
     group_walk_enabled: int = 0
     gaussian_pair_lookup: int = 0
+    boundary_condition: int = _abi.BOUNDARY_PERIODIC
 
     def to_c(self) -> _abi.Config:
         c = _abi.Config()

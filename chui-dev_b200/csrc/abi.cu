@@ -249,9 +249,11 @@ __global__ void driftKernel(int64_t n, double* x, double* y, double* z, const do
                             double bx, double by, double bz) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    x[i] = canonicalPosition(fma(vx[i], drift, x[i]), bx);
-    y[i] = canonicalPosition(fma(vy[i], drift, y[i]), by);
-    z[i] = canonicalPosition(fma(vz[i], drift, z[i]), bz);
+    // box lengths 0: isolated/open boundaries, positions are not wrapped
+    const double nx = fma(vx[i], drift, x[i]), ny = fma(vy[i], drift, y[i]), nz = fma(vz[i], drift, z[i]);
+    x[i] = bx > 0.0 ? canonicalPosition(nx, bx) : nx;
+    y[i] = by > 0.0 ? canonicalPosition(ny, by) : ny;
+    z[i] = bz > 0.0 ? canonicalPosition(nz, bz) : nz;
   }
 }
 
@@ -411,6 +413,22 @@ int validateConfig(const chui_treepm_config& cfg, std::string& err) {
     err = "TreePM tree options are invalid";
     return CHUI_TREEPM_EINVAL;
   }
+  if (cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC &&
+      cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_ISOLATED_OPEN) {
+    err = "TreePM PM boundary condition is invalid";
+    return CHUI_TREEPM_EINVAL;
+  }
+  if (cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_ISOLATED_OPEN) {
+    // validatePmSolveOptions (pm_solver.cpp:1664-1667) and solvePoissonIsolatedOpen (:5069-5071)
+    if (cfg.window_deconvolution) {
+      err = "isolated PM currently does not support window deconvolution";
+      return CHUI_TREEPM_EINVAL;
+    }
+    if (cfg.pm_grid_nx < 3 || cfg.pm_grid_ny < 3 || cfg.pm_grid_nz < 3) {
+      err = "PmSolver::solvePoissonIsolatedOpen requires nx,ny,nz >= 3 for one-sided boundary gradients";
+      return CHUI_TREEPM_EINVAL;
+    }
+  }
   if (cfg.acceptance_policy != CHUI_TREEPM_POLICY_STRICT && cfg.acceptance_policy != CHUI_TREEPM_POLICY_ADAPTIVE) {
     err = "TreePM acceptance policy is invalid";
     return CHUI_TREEPM_EINVAL;
@@ -430,7 +448,7 @@ int validateConfig(const chui_treepm_config& cfg, std::string& err) {
                                    (cfg.box_z / cfg.pm_grid_nz));
   const double cutoff = cfg.rcut_cells * spacing;
   const double half_short = 0.5 * std::min({cfg.box_x, cfg.box_y, cfg.box_z});
-  if (cutoff >= std::nextafter(half_short, 0.0)) {
+  if (cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_PERIODIC && cutoff >= std::nextafter(half_short, 0.0)) {
     err = "Periodic TreePM requires cutoff_radius_comoving < half the shortest box axis; cutoff_radius_comoving=" +
           std::to_string(cutoff) + ", half_shortest_axis=" + std::to_string(half_short) +
           "; the short-range tree evaluates one minimum image per source";
@@ -557,6 +575,7 @@ int chui_treepm_config_default(chui_treepm_config* cfg) {
   cfg->relative_force_acceleration_floor = 1.0e-30;                           // tree_gravity.hpp:40
   cfg->group_walk_enabled = 0;                                                // tree_pm_coupling.hpp:257
   cfg->gaussian_pair_lookup = 0;                                              // tree_pm_coupling.hpp:266
+  cfg->boundary_condition = CHUI_TREEPM_BOUNDARY_PERIODIC;                    // pm_solver.hpp:236
   return 0;
 }
 
@@ -638,6 +657,7 @@ int chui_treepm_set_config(void* handle, const chui_treepm_config* cfg) {
                           cfg->window_deconvolution != c->cfg.window_deconvolution || cfg->box_x != c->cfg.box_x ||
                           cfg->box_y != c->cfg.box_y || cfg->box_z != c->cfg.box_z ||
                           cfg->asmth_cells != c->cfg.asmth_cells ||
+                          cfg->boundary_condition != c->cfg.boundary_condition ||
                           cfg->gravitational_constant != c->cfg.gravitational_constant;
   if (pm_changed) {
     cudaDeviceSynchronize();
@@ -774,9 +794,11 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
 
   // residual walk
   chui::WalkParams wp;
-  wp.box[0] = c.cfg.box_x;
-  wp.box[1] = c.cfg.box_y;
-  wp.box[2] = c.cfg.box_z;
+  // isolated/open: no periodic images (tree_pm_coupling.cpp:3560-3562)
+  const bool periodic = c.cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_PERIODIC;
+  wp.box[0] = periodic ? c.cfg.box_x : 0.0;
+  wp.box[1] = periodic ? c.cfg.box_y : 0.0;
+  wp.box[2] = periodic ? c.cfg.box_z : 0.0;
   for (int a = 0; a < 3; ++a) {
     wp.src_lo[a] = lo[a];
     wp.src_hi[a] = hi[a];
@@ -789,7 +811,7 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   wp.G = c.cfg.gravitational_constant;
   wp.eps = c.cfg.softening;
   wp.theta = c.cfg.opening_theta;
-  wp.exact_half = 0.5 * std::min({c.cfg.box_x, c.cfg.box_y, c.cfg.box_z}) - c.cutoff;
+  wp.exact_half = periodic ? 0.5 * std::min({c.cfg.box_x, c.cfg.box_y, c.cfg.box_z}) - c.cutoff : INFINITY;
   wp.criterion = c.cfg.opening_criterion;
   wp.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
   wp.policy = c.cfg.acceptance_policy;
@@ -936,6 +958,8 @@ int chui_treepm_force_vjp(void* handle, const chui_treepm_sources* src, const do
   if (!handle) return CHUI_TREEPM_EINVAL;
   Context& c = *static_cast<Context*>(handle);
   c.last_error.clear();
+  if (c.cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC)
+    return chui::fail(c, CHUI_TREEPM_ENOTSUP, "the force VJP supports periodic boundaries only");
   if (!src) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources are required");
   if (memory != CHUI_TREEPM_HOST && memory != CHUI_TREEPM_DEVICE)
     return chui::fail(c, CHUI_TREEPM_EINVAL, "memory must be CHUI_TREEPM_HOST or CHUI_TREEPM_DEVICE");
@@ -1048,6 +1072,8 @@ int chui_pm_density_vjp(void* handle, const chui_treepm_sources* src, const doub
                         double* grad_y, double* grad_z, int memory, void* stream) {
   if (!handle) return CHUI_TREEPM_EINVAL;
   Context& c = *static_cast<Context*>(handle);
+  if (c.cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC)
+    return chui::fail(c, CHUI_TREEPM_ENOTSUP, "the density VJP supports periodic boundaries only");
   if (!src || !rho_bar || (src->count > 0 && (!src->x || !src->y || !src->z || !grad_x || !grad_y || !grad_z)))
     return chui::fail(c, CHUI_TREEPM_EINVAL, "density VJP requires positions, a cotangent grid and gradients");
   if (memory != CHUI_TREEPM_HOST && memory != CHUI_TREEPM_DEVICE)
@@ -1285,6 +1311,9 @@ int chui_treepm_drift(void* handle, int64_t n, double* x, double* y, double* z, 
   Context& c = *static_cast<Context*>(handle);
   if (n == 0) return 0;
   chui::DeviceGuard guard(c.device);
+  // isolated/open boundaries: no wrap (box lengths 0 in the kernel)
+  const bool periodic = c.cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_PERIODIC;
+  const double per_box[3] = {periodic ? c.cfg.box_x : 0.0, periodic ? c.cfg.box_y : 0.0, periodic ? c.cfg.box_z : 0.0};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double *dx = x, *dy = y, *dz = z;
   const double *dvx = vx, *dvy = vy, *dvz = vz;
@@ -1305,8 +1334,8 @@ int chui_treepm_drift(void* handle, int64_t n, double* x, double* y, double* z, 
     dvy = c.out_acc[1].as<double>();
     dvz = c.out_acc[2].as<double>();
   }
-  { chui::noteLaunch(); chui::driftKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dx, dy, dz, dvx, dvy, dvz, drift_factor, c.cfg.box_x,
-                                                         c.cfg.box_y, c.cfg.box_z); }
+  { chui::noteLaunch(); chui::driftKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dx, dy, dz, dvx, dvy, dvz, drift_factor, per_box[0],
+                                                         per_box[1], per_box[2]); }
   if (memory == CHUI_TREEPM_HOST) {
     cudaMemcpyAsync(x, dx, n * 8, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(y, dy, n * 8, cudaMemcpyDeviceToHost, s);

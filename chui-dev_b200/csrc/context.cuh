@@ -74,6 +74,11 @@ struct Context {
   // PM (cuFFT, in-place padded real layout nx*ny*2*(nz/2+1))
   bool fft_ready = false;
   cufftHandle plan_r2c = 0, plan_c2r = 0;
+  // isolated/open PM: zero-padded (2nx, 2ny, 2nz) in-place real/half-spectrum
+  // array, the split Green function's (real) spectrum scaled by G dV / pad size
+  bool iso_ready = false;
+  cufftHandle iso_r2c = 0, iso_c2r = 0;
+  DevBuf iso_pad, iso_kernel;
   DevBuf grid[3];            // grid[0] holds the density then F_x; grid[1], grid[2] F_y, F_z
   DevBuf adj_grid[3];        // adjoint: cotangent grids B_x, B_y, B_z; adj_grid[0] then holds rho_bar
   DevBuf axis_tables;        // kx, ky, kz, wx, wy, wz (FP64)

@@ -36,6 +36,7 @@ struct PmGeom {
   double L[3];
   double inv_d[3];
   int scheme;
+  int periodic;  // 0: isolated/open (no wrap; cells outside the mesh dropped)
 };
 
 PmGeom geomOf(const Context& c) {
@@ -50,8 +51,12 @@ PmGeom geomOf(const Context& c) {
   g.L[2] = c.cfg.box_z;
   for (int a = 0; a < 3; ++a) g.inv_d[a] = static_cast<double>(g.n[a]) / g.L[a];
   g.scheme = c.cfg.assignment_scheme;
+  g.periodic = c.cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_PERIODIC ? 1 : 0;
   return g;
 }
+
+// positionInsideOpenDomain (pm_solver.cpp:117-119)
+__device__ __forceinline__ bool insideOpen(double v, double box) { return v >= 0.0 && v < box; }
 
 // wrapPosition (pm_solver.cpp:112-115): fmod is exact, so cell indices match.
 __device__ __forceinline__ double wrapPosition(double v, double box) {
@@ -295,16 +300,25 @@ __global__ void depositCompactKernel(int64_t n, const double* __restrict__ x, co
   const int taps = g.scheme == 0 ? 2 : 3;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const Stencil sx = makeStencil(wrapPosition(x[i], g.L[0]) * g.inv_d[0], g.scheme);
-    const Stencil sy = makeStencil(wrapPosition(y[i], g.L[1]) * g.inv_d[1], g.scheme);
-    const Stencil sz = makeStencil(wrapPosition(z[i], g.L[2]) * g.inv_d[2], g.scheme);
+    // isolated/open: particles outside [0, L) and cells outside the mesh are
+    // dropped (pm_solver.cpp:4016-4049)
+    if (!g.periodic && !(insideOpen(x[i], g.L[0]) && insideOpen(y[i], g.L[1]) && insideOpen(z[i], g.L[2]))) continue;
+    const Stencil sx = makeStencil((g.periodic ? wrapPosition(x[i], g.L[0]) : x[i]) * g.inv_d[0], g.scheme);
+    const Stencil sy = makeStencil((g.periodic ? wrapPosition(y[i], g.L[1]) : y[i]) * g.inv_d[1], g.scheme);
+    const Stencil sz = makeStencil((g.periodic ? wrapPosition(z[i], g.L[2]) : z[i]) * g.inv_d[2], g.scheme);
     const double mass = m ? m[i] : uniform_mass;
     for (int a = 0; a < taps; ++a) {
-      const int64_t ix = wrapIndex(sx.off0 + a, g.n[0]);
+      const int64_t ox = sx.off0 + a;
+      if (!g.periodic && (ox < 0 || ox >= g.n[0])) continue;
+      const int64_t ix = g.periodic ? wrapIndex(ox, g.n[0]) : ox;
       for (int b = 0; b < taps; ++b) {
-        const int64_t iy = wrapIndex(sy.off0 + b, g.n[1]);
+        const int64_t oy = sy.off0 + b;
+        if (!g.periodic && (oy < 0 || oy >= g.n[1])) continue;
+        const int64_t iy = g.periodic ? wrapIndex(oy, g.n[1]) : oy;
         for (int cc = 0; cc < taps; ++cc) {
-          const int64_t iz = wrapIndex(sz.off0 + cc, g.n[2]);
+          const int64_t oz = sz.off0 + cc;
+          if (!g.periodic && (oz < 0 || oz >= g.n[2])) continue;
+          const int64_t iz = g.periodic ? wrapIndex(oz, g.n[2]) : oz;
           const double w = sx.w[a] * sy.w[b] * sz.w[cc];
           atomicAdd(grid + (static_cast<size_t>(ix) * g.n[1] + iy) * g.n[2] + iz, mass * w);
         }
@@ -411,18 +425,31 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ activ
       py = sy[row];
       pz = sz[row];
     }
-    const Stencil s0 = makeStencil(wrapPosition(px, g.L[0]) * g.inv_d[0], g.scheme);
-    const Stencil s1 = makeStencil(wrapPosition(py, g.L[1]) * g.inv_d[1], g.scheme);
-    const Stencil s2 = makeStencil(wrapPosition(pz, g.L[2]) * g.inv_d[2], g.scheme);
+    // isolated/open: no PM force outside [0, L); cells outside the mesh skipped (pm_solver.cpp:5904-5947)
+    if (!g.periodic && !(insideOpen(px, g.L[0]) && insideOpen(py, g.L[1]) && insideOpen(pz, g.L[2]))) {
+      ax[k] = 0.0;
+      ay[k] = 0.0;
+      az[k] = 0.0;
+      continue;
+    }
+    const Stencil s0 = makeStencil((g.periodic ? wrapPosition(px, g.L[0]) : px) * g.inv_d[0], g.scheme);
+    const Stencil s1 = makeStencil((g.periodic ? wrapPosition(py, g.L[1]) : py) * g.inv_d[1], g.scheme);
+    const Stencil s2 = makeStencil((g.periodic ? wrapPosition(pz, g.L[2]) : pz) * g.inv_d[2], g.scheme);
     R gx = 0, gy = 0, gz = 0;
     for (int a = 0; a < taps; ++a) {
-      const int64_t ix = wrapIndex(s0.off0 + a, g.n[0]);
+      const int64_t ox = s0.off0 + a;
+      if (!g.periodic && (ox < 0 || ox >= g.n[0])) continue;
+      const int64_t ix = g.periodic ? wrapIndex(ox, g.n[0]) : ox;
       for (int b = 0; b < taps; ++b) {
-        const int64_t iy = wrapIndex(s1.off0 + b, g.n[1]);
+        const int64_t oy = s1.off0 + b;
+        if (!g.periodic && (oy < 0 || oy >= g.n[1])) continue;
+        const int64_t iy = g.periodic ? wrapIndex(oy, g.n[1]) : oy;
         const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
         const R wab = static_cast<R>(s0.w[a] * s1.w[b]);
         for (int cc = 0; cc < taps; ++cc) {
-          const int64_t iz = wrapIndex(s2.off0 + cc, g.n[2]);
+          const int64_t oz = s2.off0 + cc;
+          if (!g.periodic && (oz < 0 || oz >= g.n[2])) continue;
+          const int64_t iz = g.periodic ? wrapIndex(oz, g.n[2]) : oz;
           const R w = wab * static_cast<R>(s2.w[cc]);
           gx += w * fxg[row + iz];
           gy += w * fyg[row + iz];
@@ -433,6 +460,119 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ activ
     ax[k] = static_cast<double>(gx);
     ay[k] = static_cast<double>(gy);
     az[k] = static_cast<double>(gz);
+  }
+}
+
+// ---- isolated/open boundaries (solvePoissonIsolatedOpen, pm_solver.cpp:4942-5337) ----
+// Padded mesh: px = 2 nx, py = 2 ny, pz = 2 nz in the in-place real layout with
+// rows of pzp = 2 (pz/2 + 1) reals; the physical mesh is the corner ix < nx,
+// iy < ny, iz < nz.
+struct IsoGeom {
+  int64_t px, py, pz, pzp;
+};
+
+template <class R>
+__global__ void depositIsolatedKernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                                      const double* __restrict__ z, const double* __restrict__ m,
+                                      double uniform_mass, double inv_cell_volume, PmGeom g, IsoGeom q, R* pad) {
+  const int taps = g.scheme == 0 ? 2 : 3;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (!(insideOpen(x[i], g.L[0]) && insideOpen(y[i], g.L[1]) && insideOpen(z[i], g.L[2]))) continue;
+    const Stencil sx = makeStencil(x[i] * g.inv_d[0], g.scheme);
+    const Stencil sy = makeStencil(y[i] * g.inv_d[1], g.scheme);
+    const Stencil sz = makeStencil(z[i] * g.inv_d[2], g.scheme);
+    const double mass = (m ? m[i] : uniform_mass) * inv_cell_volume;
+    for (int a = 0; a < taps; ++a) {
+      const int64_t ix = sx.off0 + a;
+      if (ix < 0 || ix >= g.n[0]) continue;
+      for (int b = 0; b < taps; ++b) {
+        const int64_t iy = sy.off0 + b;
+        if (iy < 0 || iy >= g.n[1]) continue;
+        const size_t row = (static_cast<size_t>(ix) * q.py + iy) * q.pzp;
+        const double wxy = sx.w[a] * sy.w[b];
+        for (int cc = 0; cc < taps; ++cc) {
+          const int64_t iz = sz.off0 + cc;
+          if (iz < 0 || iz >= g.n[2]) continue;
+          atomicAdd(pad + row + iz, static_cast<R>(mass * (wxy * sz.w[cc])));
+        }
+      }
+    }
+  }
+}
+
+// The split Green function on the padded mesh at minimum-image separations:
+// -erf(r / 2 r_s) / r, and -1 / (sqrt(pi) r_s) at r = 0 (pm_solver.cpp:5150-5204).
+template <class R>
+__global__ void isoKernelFillKernel(PmGeom g, IsoGeom q, double dx, double dy, double dz, double rs, R* pad) {
+  const size_t total = static_cast<size_t>(q.px) * q.py * q.pz;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int64_t iz = static_cast<int64_t>(i % q.pz);
+    const int64_t iy = static_cast<int64_t>((i / q.pz) % q.py);
+    const int64_t ix = static_cast<int64_t>(i / (static_cast<size_t>(q.pz) * q.py));
+    const double rx = static_cast<double>(ix <= g.n[0] ? ix : ix - q.px) * dx;
+    const double ry = static_cast<double>(iy <= g.n[1] ? iy : iy - q.py) * dy;
+    const double rz = static_cast<double>(iz <= g.n[2] ? iz : iz - q.pz) * dz;
+    const double r = sqrt(rx * rx + ry * ry + rz * rz);
+    const double kernel = r > 0.0 ? -erf(0.5 * r / rs) / r : -1.0 / (sqrt(kPi) * rs);
+    pad[(static_cast<size_t>(ix) * q.py + iy) * q.pzp + iz] = static_cast<R>(kernel);
+  }
+}
+
+// The kernel is real and even on the padded mesh, so its spectrum is real:
+// keep the real part, scaled by G dV / (px py pz) (the convolution's prefactor
+// and the unnormalized inverse transform, pm_solver.cpp:5207-5222).
+template <class R, class C>
+__global__ void isoKernelExtractKernel(size_t count, const C* __restrict__ spec, double scale, R* out) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    out[i] = static_cast<R>(static_cast<double>(spec[i].x) * scale);
+  }
+}
+
+template <class R, class C>
+__global__ void isoMultiplyKernel(size_t count, C* spec, const R* __restrict__ kern) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const R k = kern[i];
+    C v = spec[i];
+    v.x *= k;
+    v.y *= k;
+    spec[i] = v;
+  }
+}
+
+// Force = -gradient of the potential: central differences inside, one-sided
+// second-order differences on the faces (pm_solver.cpp:5240-5265). Writes the
+// force meshes in the periodic layout the interpolation reads.
+template <class R>
+__global__ void isoGradientKernel(PmGeom g, IsoGeom q, double dx, double dy, double dz, const R* __restrict__ phi,
+                                  R* fx, R* fy, R* fz) {
+  const int64_t nx = g.n[0], ny = g.n[1], nz = g.n[2];
+  const size_t total = static_cast<size_t>(nx) * ny * nz;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int64_t iz = static_cast<int64_t>(i % nz);
+    const int64_t iy = static_cast<int64_t>((i / nz) % ny);
+    const int64_t ix = static_cast<int64_t>(i / (static_cast<size_t>(nz) * ny));
+    auto P = [&](int64_t a, int64_t b, int64_t c) -> double {
+      return static_cast<double>(phi[(static_cast<size_t>(a) * q.py + b) * q.pzp + c]);
+    };
+    double gx, gy, gz;
+    if (ix == 0) gx = (-3.0 * P(0, iy, iz) + 4.0 * P(1, iy, iz) - P(2, iy, iz)) / (2.0 * dx);
+    else if (ix + 1 == nx) gx = (3.0 * P(nx - 1, iy, iz) - 4.0 * P(nx - 2, iy, iz) + P(nx - 3, iy, iz)) / (2.0 * dx);
+    else gx = (P(ix + 1, iy, iz) - P(ix - 1, iy, iz)) / (2.0 * dx);
+    if (iy == 0) gy = (-3.0 * P(ix, 0, iz) + 4.0 * P(ix, 1, iz) - P(ix, 2, iz)) / (2.0 * dy);
+    else if (iy + 1 == ny) gy = (3.0 * P(ix, ny - 1, iz) - 4.0 * P(ix, ny - 2, iz) + P(ix, ny - 3, iz)) / (2.0 * dy);
+    else gy = (P(ix, iy + 1, iz) - P(ix, iy - 1, iz)) / (2.0 * dy);
+    if (iz == 0) gz = (-3.0 * P(ix, iy, 0) + 4.0 * P(ix, iy, 1) - P(ix, iy, 2)) / (2.0 * dz);
+    else if (iz + 1 == nz) gz = (3.0 * P(ix, iy, nz - 1) - 4.0 * P(ix, iy, nz - 2) + P(ix, iy, nz - 3)) / (2.0 * dz);
+    else gz = (P(ix, iy, iz + 1) - P(ix, iy, iz - 1)) / (2.0 * dz);
+    const size_t o = (static_cast<size_t>(ix) * ny + iy) * g.nzp + iz;
+    fx[o] = static_cast<R>(-gx);
+    fy[o] = static_cast<R>(-gy);
+    fz[o] = static_cast<R>(-gz);
   }
 }
 
@@ -673,16 +813,129 @@ void pmDestroy(Context& c) {
   if (c.plan_c2r) cufftDestroy(c.plan_c2r);
   c.plan_r2c = c.plan_c2r = 0;
   c.fft_ready = false;
+  if (c.iso_r2c) cufftDestroy(c.iso_r2c);
+  if (c.iso_c2r) cufftDestroy(c.iso_c2r);
+  c.iso_r2c = c.iso_c2r = 0;
+  c.iso_ready = false;
+  release(c.iso_pad);
+  release(c.iso_kernel);
   for (auto& b : c.grid) release(b);
   for (auto& b : c.adj_grid) release(b);
   release(c.axis_tables);
 }
+
+namespace {
+
+IsoGeom isoGeomOf(const PmGeom& g) {
+  IsoGeom q;
+  q.px = 2 * g.n[0];
+  q.py = 2 * g.n[1];
+  q.pz = 2 * g.n[2];
+  q.pzp = 2 * (q.pz / 2 + 1);
+  return q;
+}
+
+// Padded plans, buffers and the Green function's spectrum (computed once per
+// configuration, as the reference caches its kernel, pm_solver.cpp:5148-5206).
+template <class R, class C>
+int isoPrepare(Context& c, const PmGeom& g, cudaStream_t s) {
+  if (c.iso_ready) return 0;
+  const IsoGeom q = isoGeomOf(g);
+  const bool mixed = sizeof(R) == 4;
+  const size_t padded = static_cast<size_t>(q.px) * q.py * q.pzp;
+  const size_t half = static_cast<size_t>(q.px) * q.py * (q.pz / 2 + 1);
+  if (ensure(c.iso_pad, padded * sizeof(R)) != cudaSuccess || ensure(c.iso_kernel, half * sizeof(R)) != cudaSuccess) {
+    c.last_error = "isolated PM workspace allocation failed";
+    return CHUI_TREEPM_ENOMEM;
+  }
+  if (cufftPlan3d(&c.iso_r2c, static_cast<int>(q.px), static_cast<int>(q.py), static_cast<int>(q.pz),
+                  mixed ? CUFFT_R2C : CUFFT_D2Z) != CUFFT_SUCCESS ||
+      cufftPlan3d(&c.iso_c2r, static_cast<int>(q.px), static_cast<int>(q.py), static_cast<int>(q.pz),
+                  mixed ? CUFFT_C2R : CUFFT_Z2D) != CUFFT_SUCCESS) {
+    c.last_error = "cuFFT plan creation failed (isolated PM)";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  cufftSetStream(c.iso_r2c, s);
+  cufftSetStream(c.iso_c2r, s);
+  const double dx = g.L[0] / static_cast<double>(g.n[0]), dy = g.L[1] / static_cast<double>(g.n[1]),
+               dz = g.L[2] / static_cast<double>(g.n[2]);
+  const int block = 256;
+  { noteLaunch(); isoKernelFillKernel<R><<<gridFor(static_cast<size_t>(q.px) * q.py * q.pz, block), block, 0, s>>>(
+      g, q, dx, dy, dz, c.rs, c.iso_pad.as<R>()); }
+  cufftResult fr = mixed ? cufftExecR2C(c.iso_r2c, c.iso_pad.as<cufftReal>(), c.iso_pad.as<cufftComplex>())
+                         : cufftExecD2Z(c.iso_r2c, c.iso_pad.as<cufftDoubleReal>(), c.iso_pad.as<cufftDoubleComplex>());
+  if (fr != CUFFT_SUCCESS) {
+    c.last_error = "cuFFT forward transform failed (isolated PM kernel)";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  const double scale = c.cfg.gravitational_constant * (dx * dy * dz) /
+                       (static_cast<double>(q.px) * static_cast<double>(q.py) * static_cast<double>(q.pz));
+  { noteLaunch(); isoKernelExtractKernel<R, C><<<gridFor(half, block), block, 0, s>>>(half, c.iso_pad.as<C>(), scale,
+                                                                                     c.iso_kernel.as<R>()); }
+  c.iso_ready = true;
+  return 0;
+}
+
+template <class R, class C>
+int isoRefresh(Context& c, const PmGeom& g, int64_t n, const double* x, const double* y, const double* z,
+               const double* m, double uniform_mass, cudaStream_t s) {
+  int rc = isoPrepare<R, C>(c, g, s);
+  if (rc) return rc;
+  const IsoGeom q = isoGeomOf(g);
+  const bool mixed = sizeof(R) == 4;
+  const size_t padded = static_cast<size_t>(q.px) * q.py * q.pzp;
+  const size_t half = static_cast<size_t>(q.px) * q.py * (q.pz / 2 + 1);
+  const double dx = g.L[0] / static_cast<double>(g.n[0]), dy = g.L[1] / static_cast<double>(g.n[1]),
+               dz = g.L[2] / static_cast<double>(g.n[2]);
+  const int block = 256;
+  cufftSetStream(c.iso_r2c, s);
+  cufftSetStream(c.iso_c2r, s);
+  cudaMemsetAsync(c.iso_pad.ptr, 0, padded * sizeof(R), s);
+  if (n > 0)
+    { noteLaunch(); depositIsolatedKernel<R><<<gridFor(n, block), block, 0, s>>>(
+        n, x, y, z, m, uniform_mass, 1.0 / (dx * dy * dz), g, q, c.iso_pad.as<R>()); }
+  cufftResult fr = mixed ? cufftExecR2C(c.iso_r2c, c.iso_pad.as<cufftReal>(), c.iso_pad.as<cufftComplex>())
+                         : cufftExecD2Z(c.iso_r2c, c.iso_pad.as<cufftDoubleReal>(), c.iso_pad.as<cufftDoubleComplex>());
+  if (fr != CUFFT_SUCCESS) {
+    c.last_error = "cuFFT forward transform failed (isolated PM)";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  { noteLaunch(); isoMultiplyKernel<R, C><<<gridFor(half, block), block, 0, s>>>(half, c.iso_pad.as<C>(),
+                                                                                c.iso_kernel.as<R>()); }
+  fr = mixed ? cufftExecC2R(c.iso_c2r, c.iso_pad.as<cufftComplex>(), c.iso_pad.as<cufftReal>())
+             : cufftExecZ2D(c.iso_c2r, c.iso_pad.as<cufftDoubleComplex>(), c.iso_pad.as<cufftDoubleReal>());
+  if (fr != CUFFT_SUCCESS) {
+    c.last_error = "cuFFT inverse transform failed (isolated PM)";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
+  { noteLaunch(); isoGradientKernel<R><<<gridFor(cells, block), block, 0, s>>>(
+      g, q, dx, dy, dz, c.iso_pad.as<R>(), c.grid[0].as<R>(), c.grid[1].as<R>(), c.grid[2].as<R>()); }
+  return 0;
+}
+
+}  // namespace
 
 int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const double* z,
               const double* m, double uniform_mass, double total_mass, cudaStream_t s,
               const double4* tree_sources) {
   int rc = pmPrepare(c);
   if (rc) return rc;
+  if (c.cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC) {
+    const PmGeom gi = geomOf(c);
+    rc = isMixed(c) ? isoRefresh<float, cufftComplex>(c, gi, n, x, y, z, m, uniform_mass, s)
+                    : isoRefresh<double, cufftDoubleComplex>(c, gi, n, x, y, z, m, uniform_mass, s);
+    if (rc) return rc;
+    if (cudaGetLastError() != cudaSuccess) {
+      c.last_error = "PM kernel launch failed";
+      return CHUI_TREEPM_EDEVICE;
+    }
+    c.pm_field_valid = true;
+    c.pm_field_box[0] = gi.L[0];
+    c.pm_field_box[1] = gi.L[1];
+    c.pm_field_box[2] = gi.L[2];
+    return 0;
+  }
   const PmGeom g = geomOf(c);
   const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
   const size_t padded = static_cast<size_t>(g.n[0]) * g.n[1] * g.nzp;
@@ -814,6 +1067,7 @@ int pmDensityInto(const chui_treepm_config& cfg, int64_t n, const double* x, con
   g.L[2] = cfg.box_z;
   for (int a = 0; a < 3; ++a) g.inv_d[a] = static_cast<double>(g.n[a]) / g.L[a];
   g.scheme = cfg.assignment_scheme;
+  g.periodic = cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_PERIODIC ? 1 : 0;
   const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
   const int block = 256;
   if (cudaMemsetAsync(rho, 0, cells * sizeof(double), s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;

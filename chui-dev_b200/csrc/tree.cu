@@ -791,6 +791,12 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   double* u[3] = {c.ux.as<double>(), c.uy.as<double>(), c.uz.as<double>()};
   double anchors[3];
   for (int a = 0; a < 3; ++a) {
+    if (c.cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC) {
+      // isolated/open: the tree takes the caller's coordinates (tree_pm_coupling.cpp:3179-3196)
+      cudaMemcpyAsync(u[a], in[a], static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+      anchors[a] = 0.0;
+      continue;
+    }
     // canonical flag as tree_pm_coupling.cpp:3183-3194
     const int canonical = src_lo[a] >= 0.0 && src_hi[a] < box[a];
     int rc = unwrapAxis(c, n, in[a], box[a], canonical, u[a], &anchors[a], s);
@@ -855,8 +861,10 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
       c.last_error = "Tree gravity maximum depth contract exceeded";
       return CHUI_TREEPM_ERANGE;
     }
+    // bucket_max is the sorted-key scratch here; the periodic unwrap sizes it
+    // as well, but isolated/open boundaries skip the unwrap
     if (ensure(c.path_words, static_cast<size_t>(words) * n * 8) ||
-        ensure(c.keys_a, static_cast<size_t>(words) * n * 8))
+        ensure(c.keys_a, static_cast<size_t>(words) * n * 8) || ensure(c.bucket_max, static_cast<size_t>(n) * 8))
       return CHUI_TREEPM_ENOMEM;
     path = c.path_words.as<unsigned long long>();
     unsigned long long* by_rank = c.keys_a.as<unsigned long long>();

@@ -946,6 +946,10 @@ __device__ __forceinline__ void exactLeafPairs(const WalkArgs& a, double4* stage
   }
 }
 
+// Nearest image of a frame offset on an axis of length L; L = 0 (isolated/open
+// boundaries) has no images.
+__device__ __forceinline__ double frameImage(double d, double L) { return L > 0.0 ? d - L * rint(d / L) : d; }
+
 // Comparison a < b decided in FP32 with a guard band (relative, plus an
 // absolute bound `err` on the inputs' own error): returns +1 (certainly true),
 // -1 (certainly false) or 0 (too close to call in FP32).
@@ -991,7 +995,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   const uint32_t lane_bit = 1u << lane;
   uint32_t* stack = stack_sm[warp];
   const WalkParams& w = a.wp;
-  const double half_min_box = 0.5 * fmin(w.box[0], fmin(w.box[1], w.box[2]));
+  // no image ambiguity without periodic boundaries
+  const double half_min_box = w.box[0] > 0.0 ? 0.5 * fmin(w.box[0], fmin(w.box[1], w.box[2])) : INFINITY;
   const float cut2 = w.cut2_f;
   const float cut_f = static_cast<float>(w.cutoff);
   const float env2 = 0.0064f;  // 0.08^2
@@ -1029,9 +1034,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     const double ry = __shfl_sync(0xffffffffu, py, 0);
     const double rz = __shfl_sync(0xffffffffu, pz, 0);
     double ox = px - rx, oy = py - ry, oz = pz - rz;
-    ox -= w.box[0] * rint(ox / w.box[0]);
-    oy -= w.box[1] * rint(oy / w.box[1]);
-    oz -= w.box[2] * rint(oz / w.box[2]);
+    ox = frameImage(ox, w.box[0]);
+    oy = frameImage(oy, w.box[1]);
+    oz = frameImage(oz, w.box[2]);
     double rga = valid ? fmax(fabs(ox), fmax(fabs(oy), fabs(oz))) : 0.0;
     double rg2 = valid ? ox * ox + oy * oy + oz * oz : 0.0;
     for (int off = 16; off > 0; off >>= 1) {
@@ -1200,9 +1205,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       const bool is_leaf = rg4.z == 0;
       // warp-uniform FP64 centre offset from the reference target
       double cdx = g.x - rx, cdy = g.y - ry, cdz = g.z - rz;
-      cdx -= w.box[0] * rint(cdx / w.box[0]);
-      cdy -= w.box[1] * rint(cdy / w.box[1]);
-      cdz -= w.box[2] * rint(cdz / w.box[2]);
+      cdx = frameImage(cdx, w.box[0]);
+      cdy = frameImage(cdy, w.box[1]);
+      cdz = frameImage(cdz, w.box[2]);
       const double cmax = fmax(fabs(cdx), fmax(fabs(cdy), fabs(cdz)));
       const bool fast_frame = h < 64.0 * w.cutoff && cmax + rga < half_min_box * (1.0 - 1.0e-9);
       bool prune = false, accept = false, need_exact = !fast_frame;

@@ -35,6 +35,7 @@ struct PmGridShape {
 };
 
 enum class PmAssignmentScheme { kCic, kTsc };
+enum class PmBoundaryCondition { kPeriodic, kIsolatedOpen };
 enum class TreeOpeningCriterion { kBarnesHutGeometric, kBarnesHutComDistance, kRelativeForceError };
 enum class TreeMultipoleOrder { kMonopole = 0, kQuadrupole = 2 };
 enum class TreePmAcceptancePolicy { kStrictReference, kAdaptiveRelative };
@@ -52,6 +53,7 @@ struct PmSolveOptions {
   double gravitational_constant_code = 1.0;
   PmAssignmentScheme assignment_scheme = PmAssignmentScheme::kCic;
   bool enable_window_deconvolution = false;
+  PmBoundaryCondition boundary_condition = PmBoundaryCondition::kPeriodic;
 };
 
 struct TreeSofteningPolicy {
@@ -344,6 +346,9 @@ class TreePmCoordinator {
     c.max_leaf_size = static_cast<std::int64_t>(o.tree_options.max_leaf_size);
     c.assignment_scheme = o.pm_options.assignment_scheme == PmAssignmentScheme::kTsc ? CHUI_TREEPM_TSC : CHUI_TREEPM_CIC;
     c.window_deconvolution = o.pm_options.enable_window_deconvolution ? 1 : 0;
+    c.boundary_condition = o.pm_options.boundary_condition == PmBoundaryCondition::kIsolatedOpen
+                               ? CHUI_TREEPM_BOUNDARY_ISOLATED_OPEN
+                               : CHUI_TREEPM_BOUNDARY_PERIODIC;
     c.softening = o.tree_options.softening.epsilon_comoving;
     c.acceptance_policy = o.acceptance_policy == TreePmAcceptancePolicy::kStrictReference ? CHUI_TREEPM_POLICY_STRICT
                                                                                         : CHUI_TREEPM_POLICY_ADAPTIVE;

@@ -52,6 +52,8 @@ enum {
 enum { CHUI_TREEPM_POLICY_STRICT = 0, CHUI_TREEPM_POLICY_ADAPTIVE = 1 };
 enum { CHUI_TREEPM_ESTIMATOR_RESIDUAL_DERIVATIVE = 0, CHUI_TREEPM_ESTIMATOR_RELATIVE_MONOPOLE = 1 };
 enum { CHUI_TREEPM_CUTOFF_CONTAIN_NODE = 0, CHUI_TREEPM_CUTOFF_COM_DISTANCE = 1 };
+/* PmBoundaryCondition (include/cosmosim/gravity/pm_solver.hpp:78-81) */
+enum { CHUI_TREEPM_BOUNDARY_PERIODIC = 0, CHUI_TREEPM_BOUNDARY_ISOLATED_OPEN = 1 };
 
 /* Solver configuration: the `.param.txt` [numerics] treepm_* knobs
  * (include/cosmosim/core/config.hpp:776-821) after GravityRuntimeImpl's
@@ -88,6 +90,11 @@ typedef struct {
   /* TreePmOptions::gaussian_pair_lookup_enabled: direct pairs take the Gaussian
    * long-range coefficient from the reference's cubic Hermite table */
   int32_t gaussian_pair_lookup;
+  /* PmSolveOptions::boundary_condition (mode.gravity_boundary): periodic, or
+   * isolated/open -- zero-padded PM with the split Green function, the tree
+   * on the caller's coordinates and no periodic images in the walk. The
+   * adjoint entry points support periodic boundaries only. */
+  int32_t boundary_condition;
 } chui_treepm_config;
 
 /* Counters named as TreePmTraversalCounters (tree_pm_coupling.hpp:39-87) plus

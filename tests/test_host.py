@@ -45,6 +45,7 @@ def test_config_defaults_match_reference_defaults():
     assert (c.adaptive_maximum_opening_angle, c.relative_force_tolerance,
             c.relative_force_acceleration_floor) == (0.25, 0.005, 1e-30)
     assert c.group_walk_enabled == 0 and c.gaussian_pair_lookup == 0
+    assert c.boundary_condition == _abi.BOUNDARY_PERIODIC
     # the Python mirror carries the same defaults
     py = ct.TreePmConfig().to_c()
     for name, _ in _abi.Config._fields_:
@@ -58,7 +59,7 @@ def test_config_defaults_match_reference_defaults():
                                          ("relative_force_tolerance", -1.0),
                                          ("relative_force_acceleration_floor", 0.0),
                                          ("acceptance_policy", 2), ("adaptive_error_estimator", 5),
-                                         ("cutoff_node_policy", -1)])
+                                         ("cutoff_node_policy", -1), ("boundary_condition", 2)])
 def test_invalid_adaptive_options_are_rejected(field, value):
     # validateTreePmOptions (tree_pm_coupling.cpp:300-340) runs before any device work
     c = _abi.Config()
@@ -168,3 +169,27 @@ def test_fp32_kernel_polynomial_accuracy():
         cheb = np.polynomial.chebyshev.chebfit(xk, fk, m - 1)
         approx = np.polynomial.chebyshev.chebval(2 * t / t_cut - 1, cheb)
         assert np.max(np.abs(approx - h_ref) / h_ref) < tol, m
+
+
+def test_isolated_boundary_validation():
+    """Isolated/open PM (pm_solver.cpp:1664-1667, :5069-5071): no window
+    deconvolution, at least 3 cells per axis; the periodic cutoff limit does
+    not apply."""
+    lib = _abi.load()
+    for field, value, text in (("window_deconvolution", 1, "window deconvolution"),
+                               ("pm_grid_nz", 2, "nx,ny,nz >= 3")):
+        c = _abi.Config()
+        lib.chui_treepm_config_default(c)
+        c.boundary_condition = _abi.BOUNDARY_ISOLATED_OPEN
+        setattr(c, field, value)
+        h = C.c_void_p()
+        assert lib.chui_treepm_create(C.byref(c), C.byref(h)) == _abi.EINVAL, field
+        assert text in lib.chui_treepm_last_error(None).decode()
+    deck = DECK + "[mode]\ngravity_boundary = isolated_monopole\n"
+    assert ct.config_from_param_text(deck).boundary_condition == _abi.BOUNDARY_ISOLATED_OPEN
+    deck = DECK + "[mode]\nmode = isolated_galaxy\n"
+    assert ct.config_from_param_text(deck).boundary_condition == _abi.BOUNDARY_ISOLATED_OPEN
+    deck = DECK + "[mode]\nmode = cosmo_cube\n"
+    assert ct.config_from_param_text(deck).boundary_condition == _abi.BOUNDARY_PERIODIC
+    with pytest.raises(ValueError):
+        ct.config_from_param_text(DECK + "[mode]\ngravity_boundary = open\n")
