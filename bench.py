@@ -365,12 +365,14 @@ def run_gpu(args) -> int:
     hy = torch.from_numpy(y).pin_memory().numpy()
     hz = torch.from_numpy(z).pin_memory().numpy()
     hm = torch.from_numpy(m).pin_memory().numpy()
-    mixed.solve_active_set(hx, hy, hz, hm)  # warm
+    # the accelerations come back into pinned host arrays the caller keeps
+    houts = [torch.empty(n, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+    mixed.solve_active_set(hx, hy, hz, hm, out=houts)  # warm
     e2e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
     w0 = time.perf_counter()
     for _ in range(e2e_steps):
-        mixed.solve_active_set(hx, hy, hz, hm)
+        mixed.solve_active_set(hx, hy, hz, hm, out=houts)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - w0
     e2e_value = n * e2e_steps * world / max_over_ranks(torch, dist, e2e_s, dev)

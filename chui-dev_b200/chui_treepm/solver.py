@@ -143,6 +143,18 @@ class _Arrays:
         self.keep.append(arr)
         return arr.ctypes.data
 
+    def out_into(self, a, n):
+        """A caller-provided FP64 output of n entries (same memory kind as the inputs)."""
+        if self.device:
+            if not (_is_torch(a) and a.is_cuda and a.dtype.itemsize == 8 and a.is_contiguous() and a.numel() == n):
+                raise InvalidArgument(_abi.EINVAL, "output tensors must be contiguous FP64 CUDA tensors of the target count")
+            self.keep.append(a)
+            return a, a.data_ptr()
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and a.size == n):
+            raise InvalidArgument(_abi.EINVAL, "output arrays must be contiguous float64 arrays of the target count")
+        self.keep.append(a)
+        return a, a.ctypes.data
+
     def out(self, n, like=None, dtype=np.float64):
         if self.device:
             import torch
@@ -199,11 +211,13 @@ class TreePmCoordinator:
                                          targets=None, uniform_mass: float | None = None,
                                          long_range: bool = False, short_range: bool = False,
                                          nearest_pair: bool = False, previous_acceleration=None,
-                                         stream=None) -> dict:
+                                         out=None, stream=None) -> dict:
         """TreePmCoordinator::solveActiveSetWithPmCadence. Returns a dict with
         ax, ay, az (active-slot order) and the requested optional lanes.
         previous_acceleration: per active slot |a_previous| for the relative
-        criteria (NaN entries: no history for that target), or None."""
+        criteria (NaN entries: no history for that target), or None.
+        out: optional (ax, ay, az) arrays to write into (the accumulator's
+        accel spans; pinned host arrays make the device-to-host copy a DMA)."""
         arr = _Arrays(x)
         n = len(x)
         src = _abi.Sources()
@@ -236,10 +250,18 @@ class TreePmCoordinator:
             if len(previous_acceleration) != nt:
                 raise InvalidArgument(_abi.EINVAL, "TreePM force accumulator spans must have matching active-set extent")
             acc.previous_acceleration_magnitude = arr.ptr(previous_acceleration, np.float64)
+        given = out
         out = {}
-        out["ax"], acc.accel_x = arr.out(nt, x)
-        out["ay"], acc.accel_y = arr.out(nt, x)
-        out["az"], acc.accel_z = arr.out(nt, x)
+        if given is not None:
+            if len(given) != 3:
+                raise InvalidArgument(_abi.EINVAL, "out takes the three acceleration arrays")
+            out["ax"], acc.accel_x = arr.out_into(given[0], nt)
+            out["ay"], acc.accel_y = arr.out_into(given[1], nt)
+            out["az"], acc.accel_z = arr.out_into(given[2], nt)
+        else:
+            out["ax"], acc.accel_x = arr.out(nt, x)
+            out["ay"], acc.accel_y = arr.out(nt, x)
+            out["az"], acc.accel_z = arr.out(nt, x)
         if long_range:
             out["pm_ax"], acc.long_range_x = arr.out(nt, x)
             out["pm_ay"], acc.long_range_y = arr.out(nt, x)

@@ -183,6 +183,17 @@ def test_device_and_host_paths_agree(cuda_ok):
     # FP32 mesh atomics make runs differ at single-precision round-off
     for k in ("ax", "ay", "az"):
         np.testing.assert_allclose(d[k].cpu().numpy(), h[k], rtol=1e-5, atol=1e-6 * np.abs(h[k]).max())
+    # caller-provided outputs (pinned host arrays, device tensors) receive the same forces
+    with ct.TreePmCoordinator(cfg_for(g, ct._abi.FP64)) as s:
+        ref = s.solve_active_set(g["x"], g["y"], g["z"], g["m"])
+        pinned = [torch.empty(len(g["x"]), dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+        r = s.solve_active_set(g["x"], g["y"], g["z"], g["m"], out=pinned)
+        assert all(r[k] is a for k, a in zip(("ax", "ay", "az"), pinned))
+        tens = [torch.empty(len(g["x"]), dtype=torch.float64, device=dev) for _ in range(3)]
+        s.solve_active_set(*(torch.tensor(g[k], device=dev) for k in ("x", "y", "z", "m")), out=tens)
+    for k, a, t in zip(("ax", "ay", "az"), pinned, tens):
+        np.testing.assert_array_equal(a, ref[k])
+        np.testing.assert_array_equal(t.cpu().numpy(), ref[k])
 
 
 def test_explicit_targets_match_oracle_walk(cuda_ok):
