@@ -946,9 +946,13 @@ __device__ __forceinline__ void exactLeafPairs(const WalkArgs& a, double4* stage
   }
 }
 
-// Nearest image of a frame offset on an axis of length L; L = 0 (isolated/open
-// boundaries) has no images.
-__device__ __forceinline__ double frameImage(double d, double L) { return L > 0.0 ? d - L * rint(d / L) : d; }
+// Nearest image of a frame offset on an axis of length L (inv_l = 1/L); L = 0
+// (isolated/open boundaries) has no images. The reciprocal replaces a division
+// per axis and node: the shared frame is only used where offsets stay well
+// inside half a box, so the rounding of d/L cannot pick another image.
+__device__ __forceinline__ double frameImage(double d, double L, double inv_l) {
+  return L > 0.0 ? d - L * rint(d * inv_l) : d;
+}
 
 // Comparison a < b decided in FP32 with a guard band (relative, plus an
 // absolute bound `err` on the inputs' own error): returns +1 (certainly true),
@@ -997,6 +1001,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   const WalkParams& w = a.wp;
   // no image ambiguity without periodic boundaries
   const double half_min_box = w.box[0] > 0.0 ? 0.5 * fmin(w.box[0], fmin(w.box[1], w.box[2])) : INFINITY;
+  const double inv_l[3] = {1.0 / w.box[0], 1.0 / w.box[1], 1.0 / w.box[2]};
   const float cut2 = w.cut2_f;
   const float cut_f = static_cast<float>(w.cutoff);
   const float env2 = 0.0064f;  // 0.08^2
@@ -1034,9 +1039,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     const double ry = __shfl_sync(0xffffffffu, py, 0);
     const double rz = __shfl_sync(0xffffffffu, pz, 0);
     double ox = px - rx, oy = py - ry, oz = pz - rz;
-    ox = frameImage(ox, w.box[0]);
-    oy = frameImage(oy, w.box[1]);
-    oz = frameImage(oz, w.box[2]);
+    ox = frameImage(ox, w.box[0], inv_l[0]);
+    oy = frameImage(oy, w.box[1], inv_l[1]);
+    oz = frameImage(oz, w.box[2], inv_l[2]);
     double rga = valid ? fmax(fabs(ox), fmax(fabs(oy), fabs(oz))) : 0.0;
     double rg2 = valid ? ox * ox + oy * oy + oz * oz : 0.0;
     for (int off = 16; off > 0; off >>= 1) {
@@ -1205,9 +1210,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       const bool is_leaf = rg4.z == 0;
       // warp-uniform FP64 centre offset from the reference target
       double cdx = g.x - rx, cdy = g.y - ry, cdz = g.z - rz;
-      cdx = frameImage(cdx, w.box[0]);
-      cdy = frameImage(cdy, w.box[1]);
-      cdz = frameImage(cdz, w.box[2]);
+      cdx = frameImage(cdx, w.box[0], inv_l[0]);
+      cdy = frameImage(cdy, w.box[1], inv_l[1]);
+      cdz = frameImage(cdz, w.box[2], inv_l[2]);
       const double cmax = fmax(fabs(cdx), fmax(fabs(cdy), fabs(cdz)));
       const bool fast_frame = h < 64.0 * w.cutoff && cmax + rga < half_min_box * (1.0 - 1.0e-9);
       bool prune = false, accept = false, need_exact = !fast_frame;
