@@ -799,6 +799,7 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   wp.box[0] = periodic ? c.cfg.box_x : 0.0;
   wp.box[1] = periodic ? c.cfg.box_y : 0.0;
   wp.box[2] = periodic ? c.cfg.box_z : 0.0;
+  for (int a = 0; a < 3; ++a) wp.inv_box[a] = periodic ? 1.0 / wp.box[a] : 0.0;
   for (int a = 0; a < 3; ++a) {
     wp.src_lo[a] = lo[a];
     wp.src_hi[a] = hi[a];
@@ -1016,6 +1017,7 @@ int chui_treepm_force_vjp(void* handle, const chui_treepm_sources* src, const do
   wp.box[0] = c.cfg.box_x;
   wp.box[1] = c.cfg.box_y;
   wp.box[2] = c.cfg.box_z;
+  for (int a = 0; a < 3; ++a) wp.inv_box[a] = 1.0 / wp.box[a];
   wp.rs = c.rs;
   wp.cutoff = c.cutoff;
   wp.cutoff2 = c.cutoff * c.cutoff;

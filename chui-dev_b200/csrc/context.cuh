@@ -37,6 +37,7 @@ struct PolyH {
 // Per-solve scalar geometry shared with the walk kernel.
 struct WalkParams {
   double box[3];
+  double inv_box[3];              // 1/box (0 for isolated/open boundaries)
   double src_lo[3], src_hi[3];    // bounds of the caller's source coordinates
   double node_lo[3], node_hi[3];  // bounds of node centres and COMs
   double rs, cutoff, cutoff2;

@@ -282,10 +282,16 @@ __device__ __forceinline__ double gaussResidualInvR3(const WalkArgs& a, double r
   return softenedInvR3(r2, eps) - long_inv_r3;
 }
 
-// treePmGroupNearestImage (internal/tree_pm_group_walk.hpp:70-76), unfused.
-__device__ __forceinline__ double groupImage(double delta, double length) {
+// treePmGroupNearestImage (internal/tree_pm_group_walk.hpp:70-76), unfused:
+// delta - L nearbyint(delta / L). The quotient only chooses the integer; a
+// product with 1/L chooses the same one unless the quotient lies within 1e-6
+// of a half-integer (the products differ by ulps), where the division is made.
+__device__ __forceinline__ double groupImage(double delta, double length, double inv_length) {
   if (!(length > 0.0)) return delta;
-  return __dsub_rn(delta, __dmul_rn(length, rint(__ddiv_rn(delta, length))));
+  const double q = delta * inv_length;
+  double k = rint(q);
+  if (fabs(fabs(q - k) - 0.5) < 1.0e-6) k = rint(__ddiv_rn(delta, length));
+  return __dsub_rn(delta, __dmul_rn(length, k));
 }
 
 struct GroupBox {
@@ -302,7 +308,7 @@ __device__ __forceinline__ int groupDecision(const WalkArgs& a, uint32_t node, c
   const double cc[3] = {g.x, g.y, g.z};
   double gap2 = 0.0, far2 = 0.0;
   for (int ax = 0; ax < 3; ++ax) {
-    const double d = fabs(groupImage(cc[ax] - gb.c[ax], w.box[ax]));
+    const double d = fabs(groupImage(cc[ax] - gb.c[ax], w.box[ax], w.inv_box[ax]));
     const double gap = fmax(0.0, __dsub_rn(__dsub_rn(d, h), gb.h[ax]));
     const double far = __dadd_rn(__dadd_rn(d, h), gb.h[ax]);
     gap2 = __dadd_rn(gap2, __dmul_rn(gap, gap));
@@ -316,7 +322,7 @@ __device__ __forceinline__ int groupDecision(const WalkArgs& a, uint32_t node, c
     const double mc[3] = {cm.x, cm.y, cm.z};
     double r_min2 = 0.0;
     for (int ax = 0; ax < 3; ++ax) {
-      const double gap = fmax(0.0, __dsub_rn(fabs(groupImage(mc[ax] - gb.c[ax], w.box[ax])), gb.h[ax]));
+      const double gap = fmax(0.0, __dsub_rn(fabs(groupImage(mc[ax] - gb.c[ax], w.box[ax], w.inv_box[ax])), gb.h[ax]));
       r_min2 = __dadd_rn(r_min2, __dmul_rn(gap, gap));
     }
     const double width2 = 4.0 * h * h;
@@ -392,7 +398,7 @@ __global__ void groupSetupKernel(WalkArgs a, uint32_t* count) {
           ref[ax] = pos[ax];
           continue;
         }
-        const double d = groupImage(pos[ax] - ref[ax], w.box[ax]);
+        const double d = groupImage(pos[ax] - ref[ax], w.box[ax], w.inv_box[ax]);
         lo[ax] = fmin(lo[ax], d);
         hi[ax] = fmax(hi[ax], d);
       }
@@ -448,7 +454,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) groupWalkKernel(WalkA
         pz = a.tz ? a.tz[slot] : a.sz[row];
       }
       const uint32_t self_pos = (valid && row < a.n) ? a.pos_of_row[row] : kInvalid;
-      const double toff[3] = {groupImage(px - gb.c[0], lx), groupImage(py - gb.c[1], ly), groupImage(pz - gb.c[2], lz)};
+      const double toff[3] = {groupImage(px - gb.c[0], lx, w.inv_box[0]), groupImage(py - gb.c[1], ly, w.inv_box[1]),
+                                groupImage(pz - gb.c[2], lz, w.inv_box[2])};
       Metric nm[3];
       const double pt[3] = {px, py, pz};
       for (int ax = 0; ax < 3; ++ax) nm[ax] = makeMetric(w.node_lo[ax], w.node_hi[ax], pt[ax], w.box[ax]);
@@ -477,8 +484,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) groupWalkKernel(WalkA
           if (valid) {
             const double4 g = a.geom[node];
             const double h = g.w;
-            const double lc[3] = {groupImage(g.x - gb.c[0], lx), groupImage(g.y - gb.c[1], ly),
-                                  groupImage(g.z - gb.c[2], lz)};
+            const double lc[3] = {groupImage(g.x - gb.c[0], lx, w.inv_box[0]), groupImage(g.y - gb.c[1], ly, w.inv_box[1]),
+                                  groupImage(g.z - gb.c[2], lz, w.inv_box[2])};
             double g2 = 0.0;
             for (int ax = 0; ax < 3; ++ax) {
               const double off = lc[ax] - toff[ax], hl = 0.5 * w.box[ax];
@@ -1001,7 +1008,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   const WalkParams& w = a.wp;
   // no image ambiguity without periodic boundaries
   const double half_min_box = w.box[0] > 0.0 ? 0.5 * fmin(w.box[0], fmin(w.box[1], w.box[2])) : INFINITY;
-  const double inv_l[3] = {1.0 / w.box[0], 1.0 / w.box[1], 1.0 / w.box[2]};
+  const double* inv_l = w.inv_box;
   const float cut2 = w.cut2_f;
   const float cut_f = static_cast<float>(w.cutoff);
   const float env2 = 0.0064f;  // 0.08^2
