@@ -1280,7 +1280,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
             dzc = ndz + nf.z;
             const float r2c = fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc));
             const float w2 = 4.0f * hf * hf;
-            const float r2c_e = 4.0f * sqrtf(r2c) * fe;  // bound on the error of r2c
+            // bound on the error of r2c (an approximate root suffices for a bound)
+            const float r2c_e = 4.0f * (r2c * rsqrtf(r2c)) * fe;
             int env, mac;
             if constexpr (kAdaptive) {
               env = certainLess(w2, angle2 * r2c, angle2 * r2c_e);
@@ -1291,7 +1292,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
               // G M w^2 / r^4 against the allowance (relative monopole: lower <= allowance
               // accepts; residual derivative: lower > allowance rejects, else the FP64 proxy)
               const float gm = w.G_f * a.node_mq[2 * static_cast<size_t>(node)].x;
-              const float lower = gm * ((w2 / r2c) / r2c);
+              const float ir = __fdividef(1.0f, r2c);  // within the band's relative 2e-5
+              const float lower = gm * (w2 * ir) * ir;
               const int over = (allow_f > 0.f && isfinite(lower))
                                    ? certainLess(allow_f, lower, 2.0f * lower * (r2c_e / r2c))
                                    : 0;
@@ -1336,7 +1338,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
           if (w.com_cutoff) {
             const float fe = 2.4e-7f * (static_cast<float>(cmax) + rga_f + static_cast<float>(h));
             const float r2c = fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc));
-            const int beyond = certainLess(cut2, r2c, 4.0f * sqrtf(r2c) * fe);
+            const int beyond = certainLess(cut2, r2c, 4.0f * (r2c * rsqrtf(r2c)) * fe);
             if (beyond > 0) com_skip = true;
             else if (beyond == 0) exact_com = true;
           }
