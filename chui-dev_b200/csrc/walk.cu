@@ -1263,8 +1263,13 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
           if (!prune && !is_leaf) {
             // inside (target within the node cube), cutoff containment, envelope, MAC;
             // each +1 certainly true, -1 certainly false, 0 too close to call in FP32
+            // Under the strict policy the inside test never decides: a target
+            // inside the node cube is within 2 sqrt(3) h of the COM (which lies in
+            // the cube), so 2h/r >= 0.58 fails the 0.08 envelope, and without
+            // quadrupoles nothing is accepted. Only the adaptive envelope (angle
+            // up to 1) needs it.
             int cin = -1;
-            if (skip_self || kAdaptive) {
+            if (kAdaptive) {
               const int ix = certainLess(ax, hf, fe), iy = certainLess(ay, hf, fe), iz = certainLess(az, hf, fe);
               if (ix < 0 || iy < 0 || iz < 0) cin = -1;  // outside on some axis
               else cin = (ix > 0 && iy > 0 && iz > 0) ? 1 : 0;
