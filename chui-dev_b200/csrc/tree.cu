@@ -702,6 +702,25 @@ __global__ void targetKeyKernel(int64_t nt, const uint32_t* __restrict__ active,
   }
 }
 
+// Whether the path words, listed in Morton-rank order, are already in
+// non-decreasing lexicographic order (word 0 most significant): then the
+// stable path sort is the identity and is skipped.
+__global__ void pathOrderCheckKernel(int64_t n, int words, const unsigned long long* __restrict__ by_rank,
+                                     unsigned int* unsorted) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i + 1 < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    for (int w = 0; w < words; ++w) {
+      const unsigned long long a = by_rank[static_cast<size_t>(w) * n + i];
+      const unsigned long long b = by_rank[static_cast<size_t>(w) * n + i + 1];
+      if (a < b) break;
+      if (a > b) {
+        atomicOr(unsorted, 1u);
+        break;
+      }
+    }
+  }
+}
+
 __global__ void iotaKernel(int64_t n, uint32_t* v) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -875,7 +894,17 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     uint32_t* rank_in = c.idx_c.as<uint32_t>();
     uint32_t* rank_out = c.idx_d.as<uint32_t>();
     { noteLaunch(); iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in); }
-    for (int w = words - 1; w >= 0; --w) {  { noteLaunch(); // LSD over path words, each pass stable
+    // the FP64 octant path order is almost always the Morton order already
+    unsigned int* unsorted_flag = reinterpret_cast<unsigned int*>(c.scalars.as<unsigned long long>() + 12);
+    cudaMemsetAsync(unsorted_flag, 0, 4, s);
+    { noteLaunch(); pathOrderCheckKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, by_rank, unsorted_flag); }
+    unsigned int unsorted = 1;
+    cudaMemcpyAsync(&unsorted, unsorted_flag, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      c.last_error = "tree path ordering failed";
+      return CHUI_TREEPM_EDEVICE;
+    }
+    for (int w = words - 1; unsorted && w >= 0; --w) {  { noteLaunch(); // LSD over path words, each pass stable
       gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in, key_cur); }
       rc = cubSortPairsU64(c, key_cur, key_sorted, rank_in, rank_out, n, 63, s);
       if (rc) return rc;
@@ -1022,6 +1051,11 @@ int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explici
   if (ensure(c.target_order, nt * 4) || ensure(c.idx_a, std::max<int64_t>(nt, n) * 4) ||
       ensure(c.idx_c, (std::max<int64_t>(nt, n) + 1) * 4) || ensure(c.idx_d, (std::max<int64_t>(nt, n) + 1) * 4))
     return CHUI_TREEPM_ENOMEM;
+  if (!active && !explicit_targets && nt == n) {
+    // every source is a target: the visit order is the tree order itself
+    cudaMemcpyAsync(c.target_order.ptr, c.sorted_index.ptr, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToDevice, s);
+    return 0;
+  }
   uint32_t* key = c.idx_c.as<uint32_t>();
   uint32_t* slot = c.idx_a.as<uint32_t>();
   { noteLaunch(); targetKeyKernel<<<gridFor(nt, 256), 256, 0, s>>>(nt, active, n, c.pos_of_row.as<uint32_t>(), explicit_targets,
