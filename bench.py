@@ -19,8 +19,11 @@ inputs resident in HBM; `e2e` times the public C-ABI call with host buffers
 (pinned), host<->device copies inside the region. Positions (400 MB) exceed L2
 (126 MB), so no flush is needed between steps.
 
-Under torchrun with N > 1 every rank runs an independent replica (the force
-does not shard here), timing is the max over ranks.
+Under torchrun with N > 1 every rank runs an independent replica (weak
+scaling), timing is the max over ranks. `--shard` instead runs one simulation
+across the ranks (strong scaling): every rank holds all particles, walks a
+cost-balanced slice of the targets, and one NCCL all-gather per force shares
+the accelerations (chui_treepm.sharded).
 """
 from __future__ import annotations
 
@@ -453,6 +456,101 @@ def run_gpu(args) -> int:
     return 0
 
 
+def sharded_step(sharded, solver, t, acc, factors, stream):
+    """One KDK step of one simulation held by every rank: the force's walk is
+    split across the ranks, every rank kicks and drifts all particles."""
+    d, k1, k2, g1, g2 = factors
+    solver.kick(t["vx"], t["vy"], t["vz"], acc[0], acc[1], acc[2], k1, g1, stream=stream)
+    solver.drift(t["x"], t["y"], t["z"], t["vx"], t["vy"], t["vz"], d, stream=stream)
+    acc = sharded.accelerations(t["x"], t["y"], t["z"], t["m"], stream=stream)
+    solver.kick(t["vx"], t["vy"], t["vz"], acc[0], acc[1], acc[2], k2, g2, stream=stream)
+    return acc
+
+
+def run_sharded(args) -> int:
+    """--shard: one simulation across the ranks (sources replicated, the walk's
+    targets sliced by cost, one all-gather of the accelerations per force;
+    chui_treepm.sharded). Strong scaling: the particle count is fixed."""
+    import datetime
+
+    import torch
+    import chui_treepm as ct
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    # the same particles on every rank: one simulation
+    x, y, z, m, vx, vy, vz = make_particles(w, seed=42)
+    n = len(x)
+    t = {k: torch.tensor(v, device=dev) for k, v in dict(x=x, y=y, z=z, m=m, vx=vx, vy=vy, vz=vz).items()}
+    factors = ct.kdk_factors_static(args.dt)
+    solver = ct.TreePmCoordinator(make_config(w, ct._abi.MIXED, local, diagnostics=0))
+    sharded = ct.ShardedTreePm(solver, group=None if dist is not None else False)
+    stream = torch.cuda.current_stream().cuda_stream
+    acc = sharded.accelerations(t["x"], t["y"], t["z"], t["m"], stream=stream)
+    for _ in range(args.warmup):
+        acc = sharded_step(sharded, solver, t, acc, factors, stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    slices = []
+    with ClockSampler(local) as clocks:
+        e0.record()
+        for _ in range(args.steps):
+            acc = sharded_step(sharded, solver, t, acc, factors, stream)
+            launches += solver.last_stats["kernel_launches"] + 3
+            slices.append({"counts": list(sharded.last_counts), "walk_ms": list(sharded.last_walk_ms)})
+        e1.record()
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = max_over_ranks(torch, dist, e0.elapsed_time(e1), dev)
+    value = n * args.steps / (ms * 1e-3)
+    st = dict(solver.last_stats)
+    solver.close()
+    if rank == 0:
+        result = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "strong",
+            "vs_baseline": None,
+            "dtype": "f32 pair/mesh arithmetic, f64 positions/decisions/COM",
+            "data": "synthetic (seeded NFW halos + Zel'dovich lattice)",
+            "config": {"workload": f"{args.workload}: N={n}, L={w['box']} Mpc/h, mesh {w['mesh']}^3, "
+                                   f"theta={w['theta']}, leaf {w['leaf']}",
+                       "particles": n, "l2": "inputs larger than L2 (positions 400 MB)",
+                       "parallelism": f"shard{world}: sources replicated, walk targets sliced by cost, "
+                                      "one all-gather of accelerations per force"},
+            "phases_ms_rank0": {k: st[k] for k in ("pm_ms", "tree_build_ms", "walk_ms", "total_ms")},
+            "slices_last_step": slices[-1] if slices else None,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "e2e": None,
+        }
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def cpu_baseline(w, x, y, z, m, args) -> dict | None:
     """The reference's own TreePM (oracle/_ref/treepm_ref, built from its
     sources) on the host cores: full PM + tree build, residual walk on a seeded
@@ -654,6 +752,8 @@ def main() -> int:
     ap.add_argument("--mode", default="bench", choices=["bench", "profile", "profile-vjp", "large"])
     ap.add_argument("--deck", default="strict", choices=["strict", "fast", "fast-group"],
                     help="acceptance settings of --mode profile")
+    ap.add_argument("--shard", action="store_true",
+                    help="one simulation across the ranks (strong scaling) instead of one replica per rank")
     args = ap.parse_args()
     if args.mode in ("profile", "profile-vjp"):
         return run_profile(args)
@@ -665,6 +765,8 @@ def main() -> int:
         args.steps = min(args.steps, 1) if args.workload == "clustered256" else args.steps
         args.warmup = 0 if args.workload == "clustered256" else args.warmup
         return run_reference(args)
+    if args.shard:
+        return run_sharded(args)
     return run_gpu(args)
 
 

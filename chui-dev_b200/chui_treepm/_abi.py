@@ -115,6 +115,10 @@ def load(path: str | None = None):
     L.chui_treepm_last_error.restype = C.c_char_p
     L.chui_treepm_solve.argtypes = [vp, C.POINTER(Sources), C.POINTER(Accumulator), C.c_int, C.c_int, vp,
                                     C.POINTER(Stats)]
+    L.chui_treepm_solve_visit_range.argtypes = [vp, C.POINTER(Sources), C.POINTER(Accumulator), C.c_int, C.c_int,
+                                                vp, C.POINTER(Stats), C.c_int64, C.c_int64]
+    L.chui_treepm_visit_order.argtypes = [vp, C.c_int64, C.c_int64, vp, C.c_int, vp]
+    L.chui_treepm_walk_cost.argtypes = [vp, C.c_int64, C.c_int64, vp, C.c_int, vp]
     L.chui_pm_assign_density.argtypes = [vp, C.POINTER(Sources), vp, C.c_int, vp]
     L.chui_pm_cells.argtypes = [vp, C.POINTER(Sources), vp, C.c_int, vp]
     L.chui_treepm_tree_node_count.argtypes = [vp, C.POINTER(C.c_int64)]

@@ -211,13 +211,17 @@ class TreePmCoordinator:
                                          targets=None, uniform_mass: float | None = None,
                                          long_range: bool = False, short_range: bool = False,
                                          nearest_pair: bool = False, previous_acceleration=None,
-                                         out=None, stream=None) -> dict:
+                                         out=None, stream=None, visit_range=None) -> dict:
         """TreePmCoordinator::solveActiveSetWithPmCadence. Returns a dict with
         ax, ay, az (active-slot order) and the requested optional lanes.
         previous_acceleration: per active slot |a_previous| for the relative
         criteria (NaN entries: no history for that target), or None.
         out: optional (ax, ay, az) arrays to write into (the accumulator's
-        accel spans; pinned host arrays make the device-to-host copy a DMA)."""
+        accel spans; pinned host arrays make the device-to-host copy a DMA).
+        visit_range: (begin, end) walks only the targets at those visit
+        positions (chui_treepm_solve_visit_range); ax.. and pm_a.. then hold
+        end - begin entries in visit order (visit_order(begin, end) gives
+        their slots)."""
         arr = _Arrays(x)
         n = len(x)
         src = _abi.Sources()
@@ -250,22 +254,26 @@ class TreePmCoordinator:
             if len(previous_acceleration) != nt:
                 raise InvalidArgument(_abi.EINVAL, "TreePM force accumulator spans must have matching active-set extent")
             acc.previous_acceleration_magnitude = arr.ptr(previous_acceleration, np.float64)
+        nout = nt
+        if visit_range is not None:
+            begin, end = (int(v) for v in visit_range)
+            nout = max(end - begin, 0)
         given = out
         out = {}
         if given is not None:
             if len(given) != 3:
                 raise InvalidArgument(_abi.EINVAL, "out takes the three acceleration arrays")
-            out["ax"], acc.accel_x = arr.out_into(given[0], nt)
-            out["ay"], acc.accel_y = arr.out_into(given[1], nt)
-            out["az"], acc.accel_z = arr.out_into(given[2], nt)
+            out["ax"], acc.accel_x = arr.out_into(given[0], nout)
+            out["ay"], acc.accel_y = arr.out_into(given[1], nout)
+            out["az"], acc.accel_z = arr.out_into(given[2], nout)
         else:
-            out["ax"], acc.accel_x = arr.out(nt, x)
-            out["ay"], acc.accel_y = arr.out(nt, x)
-            out["az"], acc.accel_z = arr.out(nt, x)
+            out["ax"], acc.accel_x = arr.out(nout, x)
+            out["ay"], acc.accel_y = arr.out(nout, x)
+            out["az"], acc.accel_z = arr.out(nout, x)
         if long_range:
-            out["pm_ax"], acc.long_range_x = arr.out(nt, x)
-            out["pm_ay"], acc.long_range_y = arr.out(nt, x)
-            out["pm_az"], acc.long_range_z = arr.out(nt, x)
+            out["pm_ax"], acc.long_range_x = arr.out(nout, x)
+            out["pm_ay"], acc.long_range_y = arr.out(nout, x)
+            out["pm_az"], acc.long_range_z = arr.out(nout, x)
         if short_range:
             for k, attr in (("tree_ax", "short_range_x"), ("tree_ay", "short_range_y"),
                             ("tree_az", "short_range_z")):
@@ -279,9 +287,14 @@ class TreePmCoordinator:
             out["nearest_r2"] = a
             acc.nearest_pair_r2 = p
         st = _abi.Stats()
-        rc = self._lib.chui_treepm_solve(self._h, C.byref(src), C.byref(acc), 1 if refresh_long_range_field else 0,
-                                         _abi.DEVICE if arr.device else _abi.HOST,
-                                         C.c_void_p(stream) if stream else None, C.byref(st))
+        mem = _abi.DEVICE if arr.device else _abi.HOST
+        strm = C.c_void_p(stream) if stream else None
+        refresh = 1 if refresh_long_range_field else 0
+        if visit_range is None:
+            rc = self._lib.chui_treepm_solve(self._h, C.byref(src), C.byref(acc), refresh, mem, strm, C.byref(st))
+        else:
+            rc = self._lib.chui_treepm_solve_visit_range(self._h, C.byref(src), C.byref(acc), refresh, mem, strm,
+                                                         C.byref(st), begin, end)
         self._check(rc)
         self.last_stats = st.as_dict()
         out["stats"] = self.last_stats
@@ -290,6 +303,39 @@ class TreePmCoordinator:
     def solve_active_set(self, x, y, z, mass, **kw) -> dict:
         """TreePmCoordinator::solveActiveSet: the cadence variant with refresh."""
         return self.solve_active_set_with_pm_cadence(x, y, z, mass, True, **kw)
+
+    def visit_order(self, begin: int, end: int, device=None):
+        """Slots (particle rows for a full solve) at visit positions
+        [begin, end) of the last solve: a uint32 numpy array, or an int64 CUDA
+        tensor on `device`."""
+        n = max(int(end) - int(begin), 0)
+        if device is None:
+            out = np.empty(n, dtype=np.uint32)
+            self._check(self._lib.chui_treepm_visit_order(self._h, int(begin), int(end),
+                                                          C.c_void_p(out.ctypes.data), _abi.HOST, None))
+            return out
+        import torch
+        out = torch.empty(n, dtype=torch.int32, device=device)
+        self._check(self._lib.chui_treepm_visit_order(self._h, int(begin), int(end), C.c_void_p(out.data_ptr()),
+                                                      _abi.DEVICE, None))
+        # uint32 bit patterns; rows stay below 2^32 - 1
+        return out.to(torch.int64) & 0xFFFFFFFF
+
+    def walk_cost(self, begin: int, end: int, device=None):
+        """SM cycles the last solve's walk spent per 32 visit positions from
+        `begin` (a multiple of 32) to `end`: float32 numpy array, or a CUDA
+        tensor on `device`."""
+        n = (max(int(end) - int(begin), 0) + 31) // 32
+        if device is None:
+            out = np.zeros(n, dtype=np.float32)
+            self._check(self._lib.chui_treepm_walk_cost(self._h, int(begin), int(end),
+                                                        C.c_void_p(out.ctypes.data), _abi.HOST, None))
+            return out
+        import torch
+        out = torch.zeros(n, dtype=torch.float32, device=device)
+        self._check(self._lib.chui_treepm_walk_cost(self._h, int(begin), int(end), C.c_void_p(out.data_ptr()),
+                                                    _abi.DEVICE, None))
+        return out
 
     # -- PM pieces ------------------------------------------------------------
     def assign_density(self, x, y, z, mass, uniform_mass: float = 0.0):

@@ -123,17 +123,29 @@ __global__ void activeCheckKernel(int64_t nt, const uint32_t* __restrict__ activ
 // accel = PM + tree (active order); optional source-indexed tree-only and
 // nearest-pair lanes (TreePmForceAccumulatorView::addShortRangeToActiveSlot and
 // noteNearestPairToActiveSlot, tree_pm_coupling.cpp:1961-1978).
-__global__ void combineKernel(int64_t nt, const uint32_t* __restrict__ active, int64_t n,
+// Total = PM + tree per target. Over all nt slots (order == nullptr), or over
+// the count slots of a visit-order slice order[0..count), written compactly
+// (entry j of the outputs is slot order[j]; long_range copies too).
+__global__ void combineKernel(int64_t count, const uint32_t* __restrict__ order, int64_t nt,
+                              const uint32_t* __restrict__ active, int64_t n,
                               const double* __restrict__ pmx, const double* __restrict__ pmy,
                               const double* __restrict__ pmz, const double* __restrict__ tr,
                               const double* __restrict__ near, double* ax, double* ay, double* az,
+                              double* lx, double* ly, double* lz,
                               double* sx, double* sy, double* sz, double* snear) {
-  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nt;
-       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < count;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t k = order ? static_cast<int64_t>(order[j]) : j;
     const double tx = tr[k], ty = tr[nt + k], tz = tr[2 * nt + k];
-    ax[k] = (pmx ? pmx[k] : 0.0) + tx;
-    ay[k] = (pmy ? pmy[k] : 0.0) + ty;
-    az[k] = (pmz ? pmz[k] : 0.0) + tz;
+    const double px = pmx ? pmx[k] : 0.0, py = pmy ? pmy[k] : 0.0, pz = pmz ? pmz[k] : 0.0;
+    ax[j] = px + tx;
+    ay[j] = py + ty;
+    az[j] = pz + tz;
+    if (lx) {
+      lx[j] = px;
+      ly[j] = py;
+      lz[j] = pz;
+    }
     const uint32_t row = active ? active[k] : static_cast<uint32_t>(k);
     if (row < n) {
       if (sx) {
@@ -683,8 +695,12 @@ int chui_treepm_kdk_factors_static(double dt, double factors[5]) {
   return 0;
 }
 
-int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_treepm_accumulator* acc,
-                      int refresh_long_range_field, int memory, void* stream, chui_treepm_stats* stats) {
+// The solve over the visit positions [visit_begin, visit_end) of the targets
+// (ranged == false: all of them, outputs in active-slot order; ranged: outputs
+// compact in visit order).
+static int solveVisitRange(void* handle, const chui_treepm_sources* src, const chui_treepm_accumulator* acc,
+                           int refresh_long_range_field, int memory, void* stream, chui_treepm_stats* stats,
+                           int64_t visit_begin, int64_t visit_end, bool ranged) {
   if (!handle) return CHUI_TREEPM_EINVAL;
   Context& c = *static_cast<Context*>(handle);
   c.last_error.clear();
@@ -694,6 +710,18 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   const int64_t n = src->count;
   const int64_t nt = acc->active_index ? acc->active_count : (acc->target_x ? acc->active_count : n);
   if (n < 0 || nt < 0) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM requires non-negative extents");
+  if (!ranged) {
+    visit_begin = 0;
+    visit_end = nt;
+  } else if (visit_begin < 0 || visit_end < visit_begin || visit_end > nt ||
+             (visit_begin % 64 != 0 && visit_begin != nt) || (visit_end % 64 != 0 && visit_end != nt)) {
+    return chui::fail(c, CHUI_TREEPM_EINVAL,
+                      "TreePM visit range must satisfy 0 <= begin <= end <= target count with both ends multiples "
+                      "of 64 or the target count");
+  }
+  // outputs per call: every target, or the slice's targets in visit order
+  const int64_t nout = visit_end - visit_begin;
+  c.visit_count = -1;
   if (n > static_cast<int64_t>(0xFFFFFFFEu))
     return chui::fail(c, CHUI_TREEPM_ERANGE, "Tree gravity source count exceeds the 32-bit tree-index contract");
   if (n > 0 && (!src->x || !src->y || !src->z))
@@ -707,7 +735,7 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   if (!explicit_targets && (acc->target_y || acc->target_z))
     return chui::fail(c, CHUI_TREEPM_EINVAL,
                       "TreePM independent target coordinate triplet must be entirely present or absent");
-  if (nt > 0 && (!acc->accel_x || !acc->accel_y || !acc->accel_z))
+  if (nout > 0 && (!acc->accel_x || !acc->accel_y || !acc->accel_z))
     return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM force accumulator spans must have matching active-set extent");
   if (explicit_targets && (acc->short_range_x || acc->nearest_pair_r2))
     return chui::fail(c, CHUI_TREEPM_EINVAL, "Tree component output requires source-indexed full source extents");
@@ -842,7 +870,7 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   wp.eps2_f = static_cast<float>(c.cfg.softening * c.cfg.softening);
   wp.G_f = static_cast<float>(c.cfg.gravitational_constant);
   cudaMemsetAsync(c.status.ptr, 0, 4, s);
-  if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, prev, wp, n, s)))
+  if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, prev, wp, n, s, visit_begin, visit_end)))
     return chui::fail(c, rc, "residual walk launch failed");
   if (n == 0 && nt > 0) {
     if (chui::ensure(c.tree_acc, nt * 3 * 8) || chui::ensure(c.tree_near, nt * 8))
@@ -866,7 +894,7 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
     snear = acc->nearest_pair_r2;
   } else {
     for (int a = 0; a < 3; ++a)
-      if (chui::ensure(c.out_acc[a], std::max<int64_t>(nt, 1) * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+      if (chui::ensure(c.out_acc[a], std::max<int64_t>(nout, 1) * 8)) return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
     ax = c.out_acc[0].as<double>();
     ay = c.out_acc[1].as<double>();
     az = c.out_acc[2].as<double>();
@@ -886,7 +914,10 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
       cudaMemcpyAsync(snear, acc->nearest_pair_r2, n * 8, cudaMemcpyHostToDevice, s);
     }
   }
-  if (lr && memory == CHUI_TREEPM_DEVICE) {
+  // a visit range interpolates into slot-indexed scratch; the combine writes
+  // the slice's long-range lanes compactly
+  double *lx = nullptr, *ly = nullptr, *lz = nullptr;
+  if (lr && memory == CHUI_TREEPM_DEVICE && !ranged) {
     pmx = acc->long_range_x;
     pmy = acc->long_range_y;
     pmz = acc->long_range_z;
@@ -897,24 +928,40 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
     pmy = c.out_pm[1].as<double>();
     pmz = c.out_pm[2].as<double>();
   }
-  if ((rc = chui::pmInterpolate(c, nt, active, tx, ty, tz, x, y, z, pmx, pmy, pmz, s))) return rc;
-  if (nt > 0)
-    { chui::noteLaunch(); chui::combineKernel<<<chui::gridFor(nt, 256), 256, 0, s>>>(nt, active, explicit_targets ? 0 : n, pmx, pmy, pmz,
-                                                              c.tree_acc.as<double>(), c.tree_near.as<double>(), ax,
-                                                              ay, az, sx, sy, sz, snear); }
+  const uint32_t* slice = ranged && nout > 0 ? c.target_order.as<uint32_t>() + visit_begin : nullptr;
+  if (ranged && lr) {
+    if (memory == CHUI_TREEPM_DEVICE) {
+      lx = acc->long_range_x;
+      ly = acc->long_range_y;
+      lz = acc->long_range_z;
+    } else {
+      for (int a = 0; a < 3; ++a)
+        if (chui::ensure(c.out_lr[a], std::max<int64_t>(nout, 1) * 8))
+          return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
+      lx = c.out_lr[0].as<double>();
+      ly = c.out_lr[1].as<double>();
+      lz = c.out_lr[2].as<double>();
+    }
+  }
+  if ((rc = chui::pmInterpolate(c, nout, active, tx, ty, tz, x, y, z, pmx, pmy, pmz, s, slice))) return rc;
+  if (nout > 0)
+    { chui::noteLaunch(); chui::combineKernel<<<chui::gridFor(nout, 256), 256, 0, s>>>(
+          nout, slice, nt, active, explicit_targets ? 0 : n, pmx, pmy, pmz, c.tree_acc.as<double>(),
+          c.tree_near.as<double>(), ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
+  c.visit_count = nt;
   cudaEventRecord(c.ev[4], s);
   uint32_t walk_status = 0;
   cudaMemcpyAsync(&walk_status, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
   unsigned long long counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (n > 0 && nt > 0) cudaMemcpyAsync(counters, c.walk_counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, s);
-  if (memory == CHUI_TREEPM_HOST && nt > 0) {
-    cudaMemcpyAsync(acc->accel_x, ax, nt * 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(acc->accel_y, ay, nt * 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(acc->accel_z, az, nt * 8, cudaMemcpyDeviceToHost, s);
+  if (memory == CHUI_TREEPM_HOST && nout > 0) {
+    cudaMemcpyAsync(acc->accel_x, ax, nout * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(acc->accel_y, ay, nout * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(acc->accel_z, az, nout * 8, cudaMemcpyDeviceToHost, s);
     if (lr) {
-      cudaMemcpyAsync(acc->long_range_x, pmx, nt * 8, cudaMemcpyDeviceToHost, s);
-      cudaMemcpyAsync(acc->long_range_y, pmy, nt * 8, cudaMemcpyDeviceToHost, s);
-      cudaMemcpyAsync(acc->long_range_z, pmz, nt * 8, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(acc->long_range_x, ranged ? lx : pmx, nout * 8, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(acc->long_range_y, ranged ? ly : pmy, nout * 8, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(acc->long_range_z, ranged ? lz : pmz, nout * 8, cudaMemcpyDeviceToHost, s);
     }
     if (sr) {
       cudaMemcpyAsync(acc->short_range_x, sx, n * 8, cudaMemcpyDeviceToHost, s);
@@ -950,6 +997,68 @@ int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_t
   stt.total_ms = ms;
   c.last_stats = stt;
   if (stats) *stats = stt;
+  return 0;
+}
+
+int chui_treepm_solve(void* handle, const chui_treepm_sources* src, const chui_treepm_accumulator* acc,
+                      int refresh_long_range_field, int memory, void* stream, chui_treepm_stats* stats) {
+  return solveVisitRange(handle, src, acc, refresh_long_range_field, memory, stream, stats, 0, -1, false);
+}
+
+int chui_treepm_solve_visit_range(void* handle, const chui_treepm_sources* src, const chui_treepm_accumulator* acc,
+                                  int refresh_long_range_field, int memory, void* stream, chui_treepm_stats* stats,
+                                  int64_t visit_begin, int64_t visit_end) {
+  return solveVisitRange(handle, src, acc, refresh_long_range_field, memory, stream, stats, visit_begin, visit_end,
+                         true);
+}
+
+int chui_treepm_walk_cost(void* handle, int64_t begin, int64_t end, float* cost, int memory, void* stream) {
+  if (!handle) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  c.last_error.clear();
+  if (memory != CHUI_TREEPM_HOST && memory != CHUI_TREEPM_DEVICE)
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "memory must be CHUI_TREEPM_HOST or CHUI_TREEPM_DEVICE");
+  if (c.visit_count < 0) return chui::fail(c, CHUI_TREEPM_ESTATE, "TreePM walk cost requested before a solve");
+  if (begin < 0 || end < begin || end > c.visit_count || (begin % 32 != 0 && begin != end))
+    return chui::fail(c, CHUI_TREEPM_EINVAL,
+                      "TreePM walk cost range must lie in the last solve's targets and start at a multiple of 32");
+  const int64_t chunks = (end - begin + 31) / 32;
+  if (chunks == 0) return 0;
+  if (!cost) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM walk cost output is required");
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const cudaMemcpyKind kind = memory == CHUI_TREEPM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const size_t have = c.walk_cost.bytes / sizeof(float);
+  const int64_t first = begin / 32;
+  if (static_cast<size_t>(first + chunks) <= have) {
+    cudaMemcpyAsync(cost, c.walk_cost.as<float>() + first, static_cast<size_t>(chunks) * sizeof(float), kind, s);
+  } else if (memory == CHUI_TREEPM_HOST) {
+    std::fill(cost, cost + chunks, 0.0f);  // no walk ran (no sources)
+  } else {
+    cudaMemsetAsync(cost, 0, static_cast<size_t>(chunks) * sizeof(float), s);
+  }
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return chui::fail(c, CHUI_TREEPM_EDEVICE, std::string("CUDA error: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+int chui_treepm_visit_order(void* handle, int64_t begin, int64_t end, uint32_t* slots, int memory, void* stream) {
+  if (!handle) return CHUI_TREEPM_EINVAL;
+  Context& c = *static_cast<Context*>(handle);
+  c.last_error.clear();
+  if (memory != CHUI_TREEPM_HOST && memory != CHUI_TREEPM_DEVICE)
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "memory must be CHUI_TREEPM_HOST or CHUI_TREEPM_DEVICE");
+  if (c.visit_count < 0) return chui::fail(c, CHUI_TREEPM_ESTATE, "TreePM visit order requested before a solve");
+  if (begin < 0 || end < begin || end > c.visit_count)
+    return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM visit order range exceeds the last solve's target count");
+  if (end > begin && !slots) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM visit order output is required");
+  if (end == begin) return 0;
+  chui::DeviceGuard guard(c.device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaMemcpyAsync(slots, c.target_order.as<uint32_t>() + begin, static_cast<size_t>(end - begin) * 4,
+                  memory == CHUI_TREEPM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s);
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return chui::fail(c, CHUI_TREEPM_EDEVICE, std::string("CUDA error: ") + cudaGetErrorString(e));
   return 0;
 }
 
@@ -1000,6 +1109,7 @@ int chui_treepm_force_vjp(void* handle, const chui_treepm_sources* src, const do
     gz = c.out_acc[2].as<double>();
   }
   // tree for these positions, every particle a target in tree order
+  c.visit_count = -1;
   if (n > 0) {
     if ((rc = chui::treeBuild(c, n, x, y, z, m, src->uniform_mass, lo, hi, s))) {
       if (c.last_error.empty()) c.last_error = "TreePM tree build failed";

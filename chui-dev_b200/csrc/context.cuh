@@ -93,7 +93,10 @@ struct Context {
   // per-slot "evaluated by a group" flags, the Gaussian Hermite table
   DevBuf grp_leaf, grp_start, grp_rec, grp_list, grp_done, gauss_tab;
   bool gauss_ready = false;
-  DevBuf out_acc[3], out_pm[3], out_tree[3], out_near;
+  DevBuf out_acc[3], out_pm[3], out_tree[3], out_near, out_lr[3];
+  // targets of the last successful solve (its visit order is target_order);
+  // -1 before one
+  int64_t visit_count = -1;
   DevBuf status;       // uint32 status word + scalar results (reduction scratch)
   DevBuf scalars;      // reduction outputs (64 x u64)
   std::vector<unsigned long long> host_scalars;
@@ -134,6 +137,7 @@ struct Context {
 
   // walk
   DevBuf walk_counters;  // 8 x u64
+  DevBuf walk_cost;      // per 32 visit positions: SM cycles of the last walk (float)
   DevBuf work_counter;   // u32 dynamic scheduling
   DevBuf tree_acc;       // double3 per active slot (short-range part)
   DevBuf tree_near;      // double per active slot
@@ -150,10 +154,12 @@ int pmPrepare(Context& c);
 int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const double* z,
               const double* m, double uniform_mass, double total_mass, cudaStream_t s,
               const double4* tree_sources = nullptr);
-// CIC/TSC interpolation of the cached force grids at targets (active slots).
+// CIC/TSC interpolation of the cached force grids at targets (active slots);
+// with `order`, only the nt slots order[0..nt) (a visit-order slice).
 int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* tx,
                   const double* ty, const double* tz, const double* sx, const double* sy,
-                  const double* sz, double* ax, double* ay, double* az, cudaStream_t s);
+                  const double* sz, double* ax, double* ay, double* az, cudaStream_t s,
+                  const uint32_t* order = nullptr);
 int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const double* z,
                   const double* m, double uniform_mass, double* rho_out, cudaStream_t s);
 int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,
@@ -180,9 +186,12 @@ int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explici
                      cudaStream_t s);
 
 // ---- walk (walk.cu) ----
+// Targets are the visit positions [visit_begin, visit_end) of the nt targets
+// (visit_end < 0: all of them); outputs land at the targets' slots.
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
-            const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s);
+            const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s,
+            int64_t visit_begin = 0, int64_t visit_end = -1);
 
 // Adjoint of the short-range force for all n particles (targets in tree
 // order, after treeBuild and treeOrderTargets with the full set):

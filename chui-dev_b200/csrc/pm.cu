@@ -405,15 +405,18 @@ __global__ void greenGradientKernel(PmGeom g, const double* __restrict__ tab, do
 // force grids. Targets are active slots (rows of the source arrays) or
 // explicit positions.
 template <class R>
-__global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ active,
+__global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ order,
+                                  const uint32_t* __restrict__ active,
                                   const double* __restrict__ tx, const double* __restrict__ ty,
                                   const double* __restrict__ tz, const double* __restrict__ sx,
                                   const double* __restrict__ sy, const double* __restrict__ sz,
                                   PmGeom g, const R* __restrict__ fxg, const R* __restrict__ fyg,
                                   const R* __restrict__ fzg, double* ax, double* ay, double* az) {
   const int taps = g.scheme == 0 ? 2 : 3;
-  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nt;
-       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < nt;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    // slot k: the j-th target, or the j-th entry of a visit-order slice
+    const int64_t k = order ? static_cast<int64_t>(order[j]) : j;
     double px, py, pz;
     if (tx) {
       px = tx[k];
@@ -1014,17 +1017,18 @@ int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const dou
 
 int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* tx,
                   const double* ty, const double* tz, const double* sx, const double* sy,
-                  const double* sz, double* ax, double* ay, double* az, cudaStream_t s) {
+                  const double* sz, double* ax, double* ay, double* az, cudaStream_t s,
+                  const uint32_t* order) {
   if (nt == 0) return 0;
   const PmGeom g = geomOf(c);
   const int block = 256;
   if (isMixed(c)) {
     { noteLaunch(); interpolateKernel<float><<<gridFor(nt, block), block, 0, s>>>(
-        nt, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<float>(), c.grid[1].as<float>(),
+        nt, order, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<float>(), c.grid[1].as<float>(),
         c.grid[2].as<float>(), ax, ay, az); }
   } else {
     { noteLaunch(); interpolateKernel<double><<<gridFor(nt, block), block, 0, s>>>(
-        nt, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<double>(), c.grid[1].as<double>(),
+        nt, order, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<double>(), c.grid[1].as<double>(),
         c.grid[2].as<double>(), ax, ay, az); }
   }
   if (cudaGetLastError() != cudaSuccess) {

@@ -48,6 +48,8 @@ namespace {
 
 struct WalkArgs {
   int64_t nt;       // targets
+  int64_t v0, v1;   // visit positions walked: [v0, v1) of the nt
+  float* chunk_cost;  // SM cycles spent per 32 visit positions (index base / 32), nullable
   int64_t n;        // sources
   const uint32_t* order;   // visit position -> active slot
   const uint32_t* active;  // slot -> source row (nullable: slot == row)
@@ -362,7 +364,9 @@ __device__ __forceinline__ uint32_t leafOfVisit(const WalkArgs& a, int64_t v, ui
 // the floor and a bounded source metric; :4326-4368).
 __global__ void groupSetupKernel(WalkArgs a, uint32_t* count) {
   const WalkParams& w = a.wp;
-  for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < a.nt;
+  // [v0, v1) starts and ends on a residual block boundary (or at nt), so no
+  // group crosses it
+  for (int64_t v = a.v0 + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < a.v1;
        v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     uint32_t slot, row;
     const uint32_t leaf = leafOfVisit(a, v, &slot, &row);
@@ -574,6 +578,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) groupWalkKernel(WalkA
 template <bool kMixed, bool kEpsZero>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a) {
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
+  __shared__ long long item_start_sm[kWalkWarpsPerBlock];
   __shared__ float4 src_f_sm[kWalkWarpsPerBlock][32];
   __shared__ double4 src_d_sm[kWalkWarpsPerBlock][32];
   const int warp = threadIdx.x >> 5;
@@ -585,11 +590,12 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
 
   while (true) {
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(a.work, 32u);
+    if (lane == 0) base = static_cast<uint32_t>(a.v0) + atomicAdd(a.work, 32u);
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= a.nt) break;
+    if (base >= a.v1) break;
+    if (lane == 0) item_start_sm[warp] = clock64();
     const int64_t v = static_cast<int64_t>(base) + lane;
-    const bool valid = v < a.nt;
+    const bool valid = v < a.v1;
     uint32_t slot = 0, row = kInvalid;
     double px = 0.0, py = 0.0, pz = 0.0;
     if (valid) {
@@ -782,6 +788,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
       a.out_z[slot] = acc_z;
       a.out_near[slot] = nearest;
     }
+    if (lane == 0 && a.chunk_cost) a.chunk_cost[base >> 5] = static_cast<float>(clock64() - item_start_sm[warp]);
     __syncwarp();
   }
   // counters: warp reduction then one atomic each
@@ -996,6 +1003,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   constexpr bool kGroup = kMode == 3;
   constexpr bool kHistory = kMode != 0;
   constexpr int kList = kAdaptive ? kMultList : 1;
+  __shared__ long long item_start_sm[kWalkWarpsPerBlock];
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
   __shared__ float4 q_src[kWalkWarpsPerBlock][kQueue];
   __shared__ uint2 q_meta[kWalkWarpsPerBlock][kQueue];
@@ -1022,11 +1030,12 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     uint32_t cnt_visited = 0, cnt_accepted = 0, cnt_opened = 0, cnt_pairs = 0, cnt_pruned = 0, cnt_skips = 0,
              cnt_multi = 0, cnt_leaves = 0;
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(a.work, 32u);
+    if (lane == 0) base = static_cast<uint32_t>(a.v0) + atomicAdd(a.work, 32u);
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= a.nt) break;
+    if (base >= a.v1) break;
+    if (lane == 0) item_start_sm[warp] = clock64();
     const int64_t v = static_cast<int64_t>(base) + lane;
-    const bool valid = v < a.nt;
+    const bool valid = v < a.v1;
     uint32_t slot = 0, row = kInvalid;
     double px = 0.0, py = 0.0, pz = 0.0;
     if (valid) {
@@ -1474,6 +1483,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, static_cast<unsigned long long>(c[k]));
       }
     }
+    if (lane == 0 && a.chunk_cost) a.chunk_cost[base >> 5] = static_cast<float>(clock64() - item_start_sm[warp]);
     __syncwarp();
   }
 }
@@ -1778,7 +1788,7 @@ int launchPersistent(Kernel kernel, const WalkArgs& args, cudaStream_t s) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWalkWarpsPerBlock * 32, 0);
   if (per_sm < 1) per_sm = 1;
-  const int64_t warps_needed = (args.nt + 31) / 32;
+  const int64_t warps_needed = (args.v1 - args.v0 + 31) / 32;
   int64_t blocks = static_cast<int64_t>(sms) * per_sm;
   const int64_t max_useful = (warps_needed + kWalkWarpsPerBlock - 1) / kWalkWarpsPerBlock;
   if (blocks > max_useful) blocks = max_useful;
@@ -1795,7 +1805,7 @@ int launchWalk(const WalkArgs& args, cudaStream_t s) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walkKernel<kMixed, kEpsZero>,
                                                 kWalkWarpsPerBlock * 32, 0);
   if (per_sm < 1) per_sm = 1;
-  const int64_t warps_needed = (args.nt + 31) / 32;
+  const int64_t warps_needed = (args.v1 - args.v0 + 31) / 32;
   int64_t blocks = static_cast<int64_t>(sms) * per_sm;
   const int64_t max_useful = (warps_needed + kWalkWarpsPerBlock - 1) / kWalkWarpsPerBlock;
   if (blocks > max_useful) blocks = max_useful;
@@ -1843,8 +1853,15 @@ int ensureGaussTable(Context& c, cudaStream_t s) {
 
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
-            const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s) {
+            const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s,
+            int64_t visit_begin, int64_t visit_end) {
+  if (visit_end < 0) visit_end = nt;
   if (nt == 0) return 0;
+  // per-chunk walk cycles (zero for chunks outside the visit range)
+  const size_t chunks = static_cast<size_t>((nt + 31) / 32);
+  if (ensure(c.walk_cost, chunks * sizeof(float))) return CHUI_TREEPM_ENOMEM;
+  cudaMemsetAsync(c.walk_cost.ptr, 0, chunks * sizeof(float), s);
+  if (visit_end <= visit_begin) return 0;
   if (ensure(c.tree_acc, static_cast<size_t>(nt) * 3 * sizeof(double)) ||
       ensure(c.tree_near, static_cast<size_t>(nt) * sizeof(double)) ||
       ensure(c.walk_counters, 8 * sizeof(unsigned long long)) || ensure(c.work_counter, 4))
@@ -1853,6 +1870,8 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   cudaMemsetAsync(c.work_counter.ptr, 0, 4, s);
   WalkArgs a;
   a.nt = nt;
+  a.v0 = visit_begin;
+  a.v1 = visit_end;
   a.n = n;
   a.order = c.target_order.as<uint32_t>();
   a.active = active;
@@ -1891,6 +1910,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.out_near = c.tree_near.as<double>();
   a.counters = c.walk_counters.as<unsigned long long>();
   a.work = c.work_counter.as<uint32_t>();
+  a.chunk_cost = c.walk_cost.as<float>();
   a.status = c.status.as<uint32_t>();
   a.poly = c.poly;
   a.dpoly = c.dpoly;
@@ -1920,7 +1940,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     cudaMemsetAsync(c.grp_done.ptr, 0, static_cast<size_t>(nt), s);
     cudaMemsetAsync(group_count, 0, 4, s);
     { noteLaunch(); leafOfPosKernel<<<groupGrid(c.n_nodes, 256), 256, 0, s>>>(c.n_nodes, a.range, c.grp_leaf.as<uint32_t>()); }
-    { noteLaunch(); groupSetupKernel<<<groupGrid(nt, 256), 256, 0, s>>>(a, group_count); }
+    { noteLaunch(); groupSetupKernel<<<groupGrid(visit_end - visit_begin, 256), 256, 0, s>>>(a, group_count); }
   }
   const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
   const bool eps_zero = wp.eps == 0.0;

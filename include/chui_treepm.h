@@ -167,6 +167,40 @@ int chui_treepm_solve(void *handle, const chui_treepm_sources *sources,
                       const chui_treepm_accumulator *accumulator, int refresh_long_range_field,
                       int memory, void *stream, chui_treepm_stats *stats);
 
+/* One shard of a solve: the same solve restricted to the targets at visit
+ * positions [visit_begin, visit_end). No counterpart in the reference, whose
+ * ranks each own their particles (the MPI slab/LET path of
+ * tree_pm_coupling.cpp); here every process holds all sources, builds the same
+ * tree and PM field, and walks a slice of the common visit order, so the
+ * shards' union is the full solve.
+ *
+ * The visit order is the order the walk takes targets in: tree order for a
+ * full solve (no active_index, no explicit targets), else the active slots
+ * sorted by tree position. Both ends must be multiples of 64 or the target
+ * count, so that no group of targets (residual blocks of 64) is split. accel_* and long_range_* hold
+ * visit_end - visit_begin entries, entry j being the target at visit position
+ * visit_begin + j; short_range_* and nearest_pair_r2 stay source-indexed (only
+ * the slice's entries are written). chui_treepm_visit_order gives the slots. */
+int chui_treepm_solve_visit_range(void *handle, const chui_treepm_sources *sources,
+                                  const chui_treepm_accumulator *accumulator, int refresh_long_range_field,
+                                  int memory, void *stream, chui_treepm_stats *stats, int64_t visit_begin,
+                                  int64_t visit_end);
+
+/* Active slots (particle rows for a full solve) at visit positions
+ * [begin, end) of the last successful solve, into slots (end - begin
+ * entries, host or device memory). CHUI_TREEPM_ESTATE before any solve. */
+int chui_treepm_visit_order(void *handle, int64_t begin, int64_t end, uint32_t *slots, int memory,
+                            void *stream);
+
+/* Device cycles the residual walk of the last successful solve spent on each
+ * block of 32 visit positions: cost[k] covers positions begin + 32k ..
+ * begin + 32k + 31 (SM clock cycles, 0 where nothing was walked; targets
+ * taken by the group walk are not counted). begin must be a multiple of 32;
+ * cost holds ceil((end - begin) / 32) entries. No counterpart in the
+ * reference; it lets a sharded solve cut the visit order into slices of equal
+ * walk time. */
+int chui_treepm_walk_cost(void *handle, int64_t begin, int64_t end, float *cost, int memory, void *stream);
+
 /* PmSolver::assignDensity (pm_solver.hpp:469-482, pm_solver.cpp:3842-4565):
  * periodic CIC/TSC density (mass / cell volume) in compact nx*ny*nz row-major
  * order, written as FP64. */
