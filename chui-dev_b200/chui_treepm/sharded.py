@@ -106,11 +106,16 @@ def profile_bounds(chunk_cost, n: int, world: int, align: int = ALIGN) -> list[i
     return out
 
 
-def order_hash(torch, order) -> int:
+def hash_weights(torch, n: int, device):
+    """Per-position weights of `order_hash`."""
+    idx = torch.arange(n, device=device, dtype=torch.int64)
+    return (idx * 2654435761 + 97) & 0x7FFFFFFF
+
+
+def order_hash(torch, order, weights=None) -> int:
     """A 64-bit fingerprint of a visit order (weighted sum, wrapping)."""
-    idx = torch.arange(order.numel(), device=order.device, dtype=torch.int64)
-    w = (idx * 2654435761 + 97) & 0x7FFFFFFF
-    return int((order.to(torch.int64) * w).sum().item())
+    w = hash_weights(torch, order.numel(), order.device) if weights is None else weights
+    return int((order * w).sum().item())
 
 
 class ShardedTreePm:
@@ -138,6 +143,7 @@ class ShardedTreePm:
             self.rank = dist.get_rank(group)
             self.world = dist.get_world_size(group)
         self.bounds: list[int] | None = None
+        self._weights = None
         self.last_walk_ms: list[float] = []
         self.last_counts: list[int] = []
 
@@ -191,7 +197,7 @@ class ShardedTreePm:
         # the slices' accelerations, padded to the longest slice
         counts = [self.bounds[q + 1] - self.bounds[q] for q in range(self.world)]
         width = max(counts) if counts else 0
-        local = torch.zeros((3, width), dtype=torch.float64, device=x.device)
+        local = torch.empty((3, width), dtype=torch.float64, device=x.device)  # the padding is never read
         local[0, : e - b] = r["ax"]
         local[1, : e - b] = r["ay"]
         local[2, : e - b] = r["az"]
@@ -211,7 +217,11 @@ class ShardedTreePm:
                 profile = torch.from_numpy(profile)
         info = torch.zeros(3 + max(chunks), dtype=torch.float64, device=x.device)
         info[0] = walk_ms
-        h = order_hash(torch, order) if self.verify else 0
+        h = 0
+        if self.verify:
+            if self._weights is None or self._weights.numel() != n or self._weights.device != order.device:
+                self._weights = hash_weights(torch, n, order.device)
+            h = order_hash(torch, order, self._weights)
         info[1] = float(h & 0xFFFFFFFF)
         info[2] = float((h >> 32) & 0xFFFFFFFF)
         if profile is not None:

@@ -124,8 +124,8 @@ __global__ void activeCheckKernel(int64_t nt, const uint32_t* __restrict__ activ
 // nearest-pair lanes (TreePmForceAccumulatorView::addShortRangeToActiveSlot and
 // noteNearestPairToActiveSlot, tree_pm_coupling.cpp:1961-1978).
 // Total = PM + tree per target. Over all nt slots (order == nullptr), or over
-// the count slots of a visit-order slice order[0..count), written compactly
-// (entry j of the outputs is slot order[j]; long_range copies too).
+// the count targets of a visit-order slice, whose PM and tree parts and
+// outputs are all compact (entry j is slot order[j]; long_range copies too).
 __global__ void combineKernel(int64_t count, const uint32_t* __restrict__ order, int64_t nt,
                               const uint32_t* __restrict__ active, int64_t n,
                               const double* __restrict__ pmx, const double* __restrict__ pmy,
@@ -136,8 +136,8 @@ __global__ void combineKernel(int64_t count, const uint32_t* __restrict__ order,
   for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < count;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t k = order ? static_cast<int64_t>(order[j]) : j;
-    const double tx = tr[k], ty = tr[nt + k], tz = tr[2 * nt + k];
-    const double px = pmx ? pmx[k] : 0.0, py = pmy ? pmy[k] : 0.0, pz = pmz ? pmz[k] : 0.0;
+    const double tx = tr[j], ty = tr[nt + j], tz = tr[2 * nt + j];
+    const double px = pmx ? pmx[j] : 0.0, py = pmy ? pmy[j] : 0.0, pz = pmz ? pmz[j] : 0.0;
     ax[j] = px + tx;
     ay[j] = py + ty;
     az[j] = pz + tz;
@@ -153,7 +153,7 @@ __global__ void combineKernel(int64_t count, const uint32_t* __restrict__ order,
         sy[row] = ty;
         sz[row] = tz;
       }
-      if (snear) snear[row] = near[k];
+      if (snear) snear[row] = near[j];
     }
   }
 }
@@ -870,7 +870,8 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
   wp.eps2_f = static_cast<float>(c.cfg.softening * c.cfg.softening);
   wp.G_f = static_cast<float>(c.cfg.gravitational_constant);
   cudaMemsetAsync(c.status.ptr, 0, 4, s);
-  if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, prev, wp, n, s, visit_begin, visit_end)))
+  if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, prev, wp, n, s, visit_begin, visit_end,
+                                     ranged)))
     return chui::fail(c, rc, "residual walk launch failed");
   if (n == 0 && nt > 0) {
     if (chui::ensure(c.tree_acc, nt * 3 * 8) || chui::ensure(c.tree_near, nt * 8))

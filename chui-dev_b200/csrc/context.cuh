@@ -155,7 +155,8 @@ int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const dou
               const double* m, double uniform_mass, double total_mass, cudaStream_t s,
               const double4* tree_sources = nullptr);
 // CIC/TSC interpolation of the cached force grids at targets (active slots);
-// with `order`, only the nt slots order[0..nt) (a visit-order slice).
+// with `order`, only the nt slots order[0..nt) (a visit-order slice), written
+// compactly (entry j is slot order[j]).
 int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* tx,
                   const double* ty, const double* tz, const double* sx, const double* sy,
                   const double* sz, double* ax, double* ay, double* az, cudaStream_t s,
@@ -187,11 +188,12 @@ int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explici
 
 // ---- walk (walk.cu) ----
 // Targets are the visit positions [visit_begin, visit_end) of the nt targets
-// (visit_end < 0: all of them); outputs land at the targets' slots.
+// (visit_end < 0: all of them); outputs land at the targets' slots, or with
+// compact at visit position - visit_begin.
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
             const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s,
-            int64_t visit_begin = 0, int64_t visit_end = -1);
+            int64_t visit_begin = 0, int64_t visit_end = -1, bool compact = false);
 
 // Adjoint of the short-range force for all n particles (targets in tree
 // order, after treeBuild and treeOrderTargets with the full set):

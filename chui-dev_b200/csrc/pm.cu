@@ -416,6 +416,7 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ order
   for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < nt;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     // slot k: the j-th target, or the j-th entry of a visit-order slice
+    // (written at j)
     const int64_t k = order ? static_cast<int64_t>(order[j]) : j;
     double px, py, pz;
     if (tx) {
@@ -430,9 +431,9 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ order
     }
     // isolated/open: no PM force outside [0, L); cells outside the mesh skipped (pm_solver.cpp:5904-5947)
     if (!g.periodic && !(insideOpen(px, g.L[0]) && insideOpen(py, g.L[1]) && insideOpen(pz, g.L[2]))) {
-      ax[k] = 0.0;
-      ay[k] = 0.0;
-      az[k] = 0.0;
+      ax[order ? j : k] = 0.0;
+      ay[order ? j : k] = 0.0;
+      az[order ? j : k] = 0.0;
       continue;
     }
     const Stencil s0 = makeStencil((g.periodic ? wrapPosition(px, g.L[0]) : px) * g.inv_d[0], g.scheme);
@@ -460,9 +461,10 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ order
         }
       }
     }
-    ax[k] = static_cast<double>(gx);
-    ay[k] = static_cast<double>(gy);
-    az[k] = static_cast<double>(gz);
+    const int64_t o = order ? j : k;
+    ax[o] = static_cast<double>(gx);
+    ay[o] = static_cast<double>(gy);
+    az[o] = static_cast<double>(gz);
   }
 }
 

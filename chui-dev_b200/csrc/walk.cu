@@ -50,6 +50,7 @@ struct WalkArgs {
   int64_t nt;       // targets
   int64_t v0, v1;   // visit positions walked: [v0, v1) of the nt
   float* chunk_cost;  // SM cycles spent per 32 visit positions (index base / 32), nullable
+  int out_compact;    // outputs at visit position - v0 (a visit-range solve) instead of the slot
   int64_t n;        // sources
   const uint32_t* order;   // visit position -> active slot
   const uint32_t* active;  // slot -> source row (nullable: slot == row)
@@ -557,10 +558,11 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) groupWalkKernel(WalkA
       }
       if (overflow && lane == 0) atomicOr(a.status, kStatusStackOverflow);
       if (valid) {
-        a.out_x[slot] = acc_x;
-        a.out_y[slot] = acc_y;
-        a.out_z[slot] = acc_z;
-        a.out_near[slot] = nearest;
+        const int64_t o = a.out_compact ? static_cast<int64_t>(v0) + chunk + lane - a.v0 : slot;
+        a.out_x[o] = acc_x;
+        a.out_y[o] = acc_y;
+        a.out_z[o] = acc_z;
+        a.out_near[o] = nearest;
         a.grp_done[slot] = 1;
       }
       __syncwarp();
@@ -783,10 +785,11 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
     }
     if constexpr (kMixed) nearest = static_cast<double>(nearest_f);
     if (valid && !grouped) {
-      a.out_x[slot] = acc_x;
-      a.out_y[slot] = acc_y;
-      a.out_z[slot] = acc_z;
-      a.out_near[slot] = nearest;
+      const int64_t o = a.out_compact ? v - a.v0 : slot;
+      a.out_x[o] = acc_x;
+      a.out_y[o] = acc_y;
+      a.out_z[o] = acc_z;
+      a.out_near[o] = nearest;
     }
     if (lane == 0 && a.chunk_cost) a.chunk_cost[base >> 5] = static_cast<float>(clock64() - item_start_sm[warp]);
     __syncwarp();
@@ -1469,10 +1472,11 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     }
     if (overflow && lane == 0) atomicOr(a.status, kStatusStackOverflow);
     if (valid) {
-      a.out_x[slot] = acc_x;
-      a.out_y[slot] = acc_y;
-      a.out_z[slot] = acc_z;
-      a.out_near[slot] = kDiag ? static_cast<double>(nearest_f) : INFINITY;
+      const int64_t o = a.out_compact ? v - a.v0 : slot;
+      a.out_x[o] = acc_x;
+      a.out_y[o] = acc_y;
+      a.out_z[o] = acc_z;
+      a.out_near[o] = kDiag ? static_cast<double>(nearest_f) : INFINITY;
     }
     if constexpr (kDiag) {
       uint32_t c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs, cnt_pruned, cnt_skips, cnt_multi, cnt_leaves};
@@ -1854,7 +1858,7 @@ int ensureGaussTable(Context& c, cudaStream_t s) {
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
             const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s,
-            int64_t visit_begin, int64_t visit_end) {
+            int64_t visit_begin, int64_t visit_end, bool compact) {
   if (visit_end < 0) visit_end = nt;
   if (nt == 0) return 0;
   // per-chunk walk cycles (zero for chunks outside the visit range)
@@ -1872,6 +1876,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.nt = nt;
   a.v0 = visit_begin;
   a.v1 = visit_end;
+  a.out_compact = compact ? 1 : 0;
   a.n = n;
   a.order = c.target_order.as<uint32_t>();
   a.active = active;

@@ -1,13 +1,17 @@
 // Example host program: a CHUI-style caller driving the B200 solver through the
 // C++ shim exactly as GravityRuntimeImpl drives TreePmCoordinator. Reads a
 // binary problem (n, box, mesh, theta, leaf, eps, then x, y, z, m as doubles),
-// solves all particles once with refresh and once reusing the PM field, and
-// writes the accelerations of both solves as doubles.
+// solves all particles once with refresh and once reusing the PM field, checks
+// that two visit-range shards reassemble the first solve, and writes the
+// accelerations of both full solves as doubles.
 //   g++ -std=c++20 -O2 shim_example.cpp -L../_build -lchui_treepm -o shim_example
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <exception>
 #include <numeric>
+#include <utility>
 #include <vector>
 
 #include "tree_pm_coordinator.hpp"
@@ -54,6 +58,24 @@ int main(int argc, char** argv) {
     if (diag.pm_solve_count != 0 || diag.pm_reuse_count != 1) {
       std::fprintf(stderr, "unexpected PM cadence diagnostics after a reuse solve\n");
       return 5;
+    }
+    // two shards of the visit order reassemble the full solve (PM field reused)
+    {
+      const std::size_t half = (static_cast<std::size_t>(n) / 2) / 64 * 64;
+      double worst = 0.0, scale = 0.0;
+      for (double v : ax) scale = std::max(scale, std::fabs(v));
+      for (const auto [b, e] : {std::pair<std::size_t, std::size_t>{0, half},
+                                std::pair<std::size_t, std::size_t>{half, static_cast<std::size_t>(n)}}) {
+        std::vector<double> sx(e - b), sy(e - b), sz(e - b);
+        cb::TreePmForceAccumulatorView part{active, sx, sy, sz};
+        coordinator.solveVisitRange(x, y, z, m, part, options, false, b, e);
+        const std::vector<std::uint32_t> slots = coordinator.visitOrder(b, e);
+        for (std::size_t j = 0; j < slots.size(); ++j) worst = std::max(worst, std::fabs(sx[j] - ax[slots[j]]));
+      }
+      if (!(worst <= 1e-12 * scale)) {
+        std::fprintf(stderr, "visit-range shards differ from the full solve by %g\n", worst);
+        return 6;
+      }
     }
     std::FILE* o = std::fopen(argv[2], "wb");
     for (auto* v : {&ax, &ay, &az, &bx, &by, &bz}) std::fwrite(v->data(), 8, n, o);

@@ -20,6 +20,7 @@
 #include <span>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/chui_treepm.h"
 
@@ -200,6 +201,48 @@ class TreePmCoordinator {
                                    bool refresh_long_range_field, TreePmProfileEvent* profile = nullptr,
                                    TreePmDiagnostics* diagnostics = nullptr,
                                    const TreeSofteningView& softening_view = {}) {
+    solve(pos_x_comoving, pos_y_comoving, pos_z_comoving, mass_code, accumulator, options, refresh_long_range_field,
+          profile, diagnostics, softening_view, false, 0, 0);
+  }
+
+  // One shard of the solve, for processes that each hold every source (no
+  // counterpart in the reference): only the targets at visit positions
+  // [visit_begin, visit_end) of the accumulator's active set are walked, and
+  // accel_* / long_range_* hold visit_end - visit_begin entries in visit
+  // order; visitOrder() names their active slots. Both ends are multiples of
+  // 64 or the active count.
+  void solveVisitRange(std::span<const double> pos_x_comoving, std::span<const double> pos_y_comoving,
+                       std::span<const double> pos_z_comoving, std::span<const double> mass_code,
+                       const TreePmForceAccumulatorView& accumulator, const TreePmOptions& options,
+                       bool refresh_long_range_field, std::size_t visit_begin, std::size_t visit_end,
+                       TreePmProfileEvent* profile = nullptr, TreePmDiagnostics* diagnostics = nullptr) {
+    solve(pos_x_comoving, pos_y_comoving, pos_z_comoving, mass_code, accumulator, options, refresh_long_range_field,
+          profile, diagnostics, {}, true, visit_begin, visit_end);
+  }
+
+  // Active slots at visit positions [begin, end) of the last solve.
+  std::vector<std::uint32_t> visitOrder(std::size_t begin, std::size_t end) const {
+    std::vector<std::uint32_t> slots(end > begin ? end - begin : 0);
+    check(chui_treepm_visit_order(m_handle, static_cast<std::int64_t>(begin), static_cast<std::int64_t>(end),
+                                  slots.data(), CHUI_TREEPM_HOST, nullptr));
+    return slots;
+  }
+
+  void solveActiveSet(std::span<const double> pos_x_comoving, std::span<const double> pos_y_comoving,
+                      std::span<const double> pos_z_comoving, std::span<const double> mass_code,
+                      const TreePmForceAccumulatorView& accumulator, const TreePmOptions& options,
+                      TreePmProfileEvent* profile = nullptr, TreePmDiagnostics* diagnostics = nullptr,
+                      const TreeSofteningView& softening_view = {}) {
+    solveActiveSetWithPmCadence(pos_x_comoving, pos_y_comoving, pos_z_comoving, mass_code, accumulator, options,
+                                true, profile, diagnostics, softening_view);
+  }
+
+ private:
+  void solve(std::span<const double> pos_x_comoving, std::span<const double> pos_y_comoving,
+             std::span<const double> pos_z_comoving, std::span<const double> mass_code,
+             const TreePmForceAccumulatorView& accumulator, const TreePmOptions& options,
+             bool refresh_long_range_field, TreePmProfileEvent* profile, TreePmDiagnostics* diagnostics,
+             const TreeSofteningView& softening_view, bool ranged, std::size_t visit_begin, std::size_t visit_end) {
     if (!softening_view.empty()) {
       throw std::invalid_argument("B200 TreePM supports uniform softening only (per-particle softening view given)");
     }
@@ -208,8 +251,9 @@ class TreePmCoordinator {
       throw std::invalid_argument("TreePM requires position and mass spans with equal extent");
     }
     const std::size_t targets = accumulator.active_particle_index.size();
-    if (accumulator.accel_x_comoving.size() != targets || accumulator.accel_y_comoving.size() != targets ||
-        accumulator.accel_z_comoving.size() != targets) {
+    const std::size_t outputs = ranged ? (visit_end > visit_begin ? visit_end - visit_begin : 0) : targets;
+    if (accumulator.accel_x_comoving.size() != outputs || accumulator.accel_y_comoving.size() != outputs ||
+        accumulator.accel_z_comoving.size() != outputs) {
       throw std::invalid_argument("TreePM force accumulator spans must have matching active-set extent");
     }
     if (!accumulator.previous_acceleration_magnitude_code.empty() &&
@@ -261,9 +305,18 @@ class TreePmCoordinator {
     if (!accumulator.short_range_nearest_pair_r2_comoving.empty()) {
       acc.nearest_pair_r2 = accumulator.short_range_nearest_pair_r2_comoving.data();
     }
+    if (!accumulator.long_range_accel_x_comoving.empty() && accumulator.long_range_accel_x_comoving.size() != outputs) {
+      throw std::invalid_argument("TreePM force accumulator spans must have matching active-set extent");
+    }
     chui_treepm_stats stats{};
-    check(chui_treepm_solve(m_handle, &src, &acc, refresh_long_range_field ? 1 : 0, CHUI_TREEPM_HOST, nullptr,
-                            &stats));
+    if (ranged) {
+      check(chui_treepm_solve_visit_range(m_handle, &src, &acc, refresh_long_range_field ? 1 : 0, CHUI_TREEPM_HOST,
+                                          nullptr, &stats, static_cast<std::int64_t>(visit_begin),
+                                          static_cast<std::int64_t>(visit_end)));
+    } else {
+      check(chui_treepm_solve(m_handle, &src, &acc, refresh_long_range_field ? 1 : 0, CHUI_TREEPM_HOST, nullptr,
+                              &stats));
+    }
     if (diagnostics != nullptr) fillDiagnostics(stats, pos_x_comoving.size(), targets, refresh_long_range_field, *diagnostics);
     if (profile != nullptr) {
       *profile = TreePmProfileEvent{};
@@ -284,16 +337,6 @@ class TreePmCoordinator {
     }
   }
 
-  void solveActiveSet(std::span<const double> pos_x_comoving, std::span<const double> pos_y_comoving,
-                      std::span<const double> pos_z_comoving, std::span<const double> mass_code,
-                      const TreePmForceAccumulatorView& accumulator, const TreePmOptions& options,
-                      TreePmProfileEvent* profile = nullptr, TreePmDiagnostics* diagnostics = nullptr,
-                      const TreeSofteningView& softening_view = {}) {
-    solveActiveSetWithPmCadence(pos_x_comoving, pos_y_comoving, pos_z_comoving, mass_code, accumulator, options,
-                                true, profile, diagnostics, softening_view);
-  }
-
- private:
   void fillDiagnostics(const chui_treepm_stats& s, std::size_t sources, std::size_t targets, bool refresh,
                        TreePmDiagnostics& d) const {
     d = TreePmDiagnostics{};
