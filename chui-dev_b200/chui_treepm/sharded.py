@@ -23,9 +23,9 @@ cycles it spent on every block of 32 visit positions (`chui_treepm_walk_cost`),
 the ranks exchange their slices' profiles, and the next boundaries cut the
 cumulative cost into equal parts (rounded to the 64-target blocks the walk
 groups targets in). Visit positions map to the same regions of the box from
-one step to the next (tree order), so the profile carries over. A solver
-without the profile is balanced on each slice's total walk time instead, the
-cost spread evenly over the slice.
+one step to the next (tree order), so the profile carries over. Where no profile is recorded (a solver
+without one, diagnostics on, several masses) the slices are balanced on their
+total walk times instead, each spread evenly over its slice.
 
 The visit order itself must be the same on every rank (same positions, same
 tree); each force checks it with a hash compared across ranks and raises
@@ -233,9 +233,11 @@ class ShardedTreePm:
                                 torch.equal(infos[:, 2], infos[:1, 2].expand(self.world))):
             raise RuntimeError("ranks disagree on the visit order: the replicated particle state has diverged")
         if self.balance and self.world > 1:
+            full = None
             if profile is not None:
                 full = torch.cat([infos[q, 3 : 3 + chunks[q]] for q in range(self.world)]).numpy()
+            if full is not None and full.sum() > 0.0:
                 self.bounds = profile_bounds(full, n, self.world)
-            else:
+            else:  # no profile recorded (diagnostics on, several masses, ...): slice totals
                 self.bounds = balanced_bounds(self.bounds, self.last_walk_ms)
         return acc[0], acc[1], acc[2]

@@ -595,7 +595,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
     if (lane == 0) base = static_cast<uint32_t>(a.v0) + atomicAdd(a.work, 32u);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= a.v1) break;
-    if (lane == 0) item_start_sm[warp] = clock64();
+    if (lane == 0 && a.chunk_cost) item_start_sm[warp] = clock64();
     const int64_t v = static_cast<int64_t>(base) + lane;
     const bool valid = v < a.v1;
     uint32_t slot = 0, row = kInvalid;
@@ -1000,7 +1000,8 @@ __device__ __forceinline__ int certainLess(float a, float b, float err = 0.f) {
 // kUniform (production, contiguous targets, one source mass): queue entries
 // carry the lane mask in place of the mass, so each entry is one 16-byte load
 // and the mass multiplies the flush's partial sums once.
-template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode, bool kUniform = false>
+template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode, bool kUniform = false,
+          bool kCost = false>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS) walkFastKernel(WalkArgs a) {
   constexpr bool kAdaptive = kMode >= 2;
   constexpr bool kGroup = kMode == 3;
@@ -1036,7 +1037,11 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     if (lane == 0) base = static_cast<uint32_t>(a.v0) + atomicAdd(a.work, 32u);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= a.v1) break;
-    if (lane == 0) item_start_sm[warp] = clock64();
+    if constexpr (kCost) {
+      // reading the clock costs the walk ~1.5 % in code generation, so only
+      // the instances behind a visit-range solve do it
+      if (lane == 0) item_start_sm[warp] = clock64();
+    }
     const int64_t v = static_cast<int64_t>(base) + lane;
     const bool valid = v < a.v1;
     uint32_t slot = 0, row = kInvalid;
@@ -1487,7 +1492,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         for (int k = 0; k < 8; ++k) atomicAdd(a.counters + k, static_cast<unsigned long long>(c[k]));
       }
     }
-    if (lane == 0 && a.chunk_cost) a.chunk_cost[base >> 5] = static_cast<float>(clock64() - item_start_sm[warp]);
+    if constexpr (kCost) {
+      if (lane == 0) a.chunk_cost[base >> 5] = static_cast<float>(clock64() - item_start_sm[warp]);
+    }
     __syncwarp();
   }
 }
@@ -1915,7 +1922,9 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.out_near = c.tree_near.as<double>();
   a.counters = c.walk_counters.as<unsigned long long>();
   a.work = c.work_counter.as<uint32_t>();
-  a.chunk_cost = c.walk_cost.as<float>();
+  // per-block cycles for visit-range solves (FP64 walk, and the mixed walk's
+  // production instances: no diagnostics, every source a target, one mass)
+  a.chunk_cost = compact ? c.walk_cost.as<float>() : nullptr;
   a.status = c.status.as<uint32_t>();
   a.poly = c.poly;
   a.dpoly = c.dpoly;
@@ -1960,8 +1969,10 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
 #define CHUI_WALK_DISPATCH2(EPS, TERMS, ADP)                                                           \
     if (diag) return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, true, true, ADP>, a, s)     \
                                 : launchPersistent(walkFastKernel<EPS, TERMS, true, false, ADP>, a, s);   \
-    if (contiguous) return uniform ? launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP, true>, a, s)  \
-                                   : launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP>, a, s);      \
+    if (contiguous && uniform)                                                                         \
+      return a.chunk_cost ? launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP, true, true>, a, s)    \
+                          : launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP, true>, a, s);         \
+    if (contiguous) return launchPersistent(walkFastKernel<EPS, TERMS, false, true, ADP>, a, s);             \
     return launchPersistent(walkFastKernel<EPS, TERMS, false, false, ADP>, a, s);
 #define CHUI_WALK_DISPATCH(EPS, TERMS)                  \
     if (mode == 3) { CHUI_WALK_DISPATCH2(EPS, TERMS, 3) } \

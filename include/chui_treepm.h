@@ -194,8 +194,10 @@ int chui_treepm_visit_order(void *handle, int64_t begin, int64_t end, uint32_t *
 
 /* Device cycles the residual walk of the last successful solve spent on each
  * block of 32 visit positions: cost[k] covers positions begin + 32k ..
- * begin + 32k + 31 (SM clock cycles, 0 where nothing was walked; targets
- * taken by the group walk are not counted). begin must be a multiple of 32;
+ * begin + 32k + 31 (SM clock cycles). Recorded by visit-range solves in FP64
+ * and by the mixed walk's production form (diagnostics off, every source a
+ * target, one mass for all sources); 0 elsewhere, where nothing was walked,
+ * and for targets taken by the group walk. begin must be a multiple of 32;
  * cost holds ceil((end - begin) / 32) entries. No counterpart in the
  * reference; it lets a sharded solve cut the visit order into slices of equal
  * walk time. */

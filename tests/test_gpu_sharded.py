@@ -75,7 +75,10 @@ def test_slices_reassemble_the_full_solve(cuda_ok, precision, diagnostics, shard
             cost = s.walk_cost(0, n)
             inside = cost[b // 32:(e + 31) // 32]
             outside = np.concatenate([cost[: b // 32], cost[(e + 31) // 32:]])
-            assert (inside > 0).all() and (outside == 0).all()
+            assert (outside == 0).all()
+            # recorded by the FP64 walk and the mixed production walk (no diagnostics)
+            recorded = precision == ct._abi.FP64 or not diagnostics
+            assert (inside > 0).all() if recorded else (inside == 0).all()
     scale = max(float(full[k].abs().max()) for k in ("ax", "ay", "az"))
     tol = 1e-12 if precision == ct._abi.FP64 else 1e-6
     for k in ("ax", "ay", "az"):
