@@ -304,9 +304,9 @@ struct GroupBox {
 // Node decision of the group walk (buildTreePmGroupInteractionList,
 // internal/tree_pm_group_walk.hpp:78-154): 0 prune, 1 accept (leaf or
 // multipole), 2 open. The reference's FP64 arithmetic, unfused.
-__device__ __forceinline__ int groupDecision(const WalkArgs& a, uint32_t node, const GroupBox& gb) {
+__device__ __forceinline__ int groupDecisionNode(const WalkArgs& a, uint32_t node, const GroupBox& gb,
+                                                 const double4 g, bool is_leaf) {
   const WalkParams& w = a.wp;
-  const double4 g = a.geom[node];
   const double h = g.w;
   const double cc[3] = {g.x, g.y, g.z};
   double gap2 = 0.0, far2 = 0.0;
@@ -318,7 +318,7 @@ __device__ __forceinline__ int groupDecision(const WalkArgs& a, uint32_t node, c
     far2 = __dadd_rn(far2, __dmul_rn(far, far));
   }
   if (gap2 > w.cutoff2) return 0;
-  if (a.range[node].z == 0) return 1;
+  if (is_leaf) return 1;
   bool accept = gap2 > 0.0 && (w.com_cutoff || far2 <= w.cutoff2);
   if (accept) {
     const double4 cm = a.com[node];
@@ -334,6 +334,10 @@ __device__ __forceinline__ int groupDecision(const WalkArgs& a, uint32_t node, c
              cm.w * width2 <= rel_over_g * gb.a_min * r_min2 * r_min2;
   }
   return accept ? 1 : 2;
+}
+
+__device__ __forceinline__ int groupDecision(const WalkArgs& a, uint32_t node, const GroupBox& gb) {
+  return groupDecisionNode(a, node, gb, a.geom[node], a.range[node].z == 0);
 }
 
 inline unsigned groupGrid(int64_t n, int block) {
@@ -1013,6 +1017,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   __shared__ uint2 q_meta[kWalkWarpsPerBlock][kQueue];
   __shared__ float4 m_list[kWalkWarpsPerBlock][kList][32];
   __shared__ double4 exact_sm[kWalkWarpsPerBlock][32];
+  // group walk: each deciding lane's group box {centre, half, a_min}, read at
+  // every node visit (components outermost: no bank conflicts)
+  __shared__ double gbox_sm[kGroup ? 7 : 1][kWalkWarpsPerBlock][32];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const uint32_t lane_bit = 1u << lane;
@@ -1093,6 +1100,18 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       const unsigned run_start = __ballot_sync(0xffffffffu, lane == 0 || up != g_start);
       leader = 31 - __clz(run_start & ((2u << lane) - 1u));
       count_walk = in_group && leader == lane && static_cast<int64_t>(g_start) == v;
+      if (in_group && leader == lane) {
+        const double4 r0 = a.grp_rec[2 * static_cast<size_t>(g_start)];
+        const double4 r1 = a.grp_rec[2 * static_cast<size_t>(g_start) + 1];
+        gbox_sm[0][warp][lane] = r0.x;
+        gbox_sm[1][warp][lane] = r0.y;
+        gbox_sm[2][warp][lane] = r0.z;
+        gbox_sm[3][warp][lane] = r1.x;
+        gbox_sm[4][warp][lane] = r1.y;
+        gbox_sm[5][warp][lane] = r1.z;
+        gbox_sm[6][warp][lane] = r0.w;
+      }
+      __syncwarp();
     }
     // relative criterion in FP32: the allowance alpha |a_prev| (adaptive, with
     // usable history) or alpha max(|a_prev|, floor) (strict relative MAC, any
@@ -1246,12 +1265,13 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
         int gd = 0;
         if (__any_sync(0xffffffffu, lead)) {
           if (lead) {
-            const double4 r0 = a.grp_rec[2 * static_cast<size_t>(g_start)];
-            const double4 r1 = a.grp_rec[2 * static_cast<size_t>(g_start) + 1];
             GroupBox gb;
-            gb.c[0] = r0.x; gb.c[1] = r0.y; gb.c[2] = r0.z; gb.a_min = r0.w;
-            gb.h[0] = r1.x; gb.h[1] = r1.y; gb.h[2] = r1.z;
-            gd = groupDecision(a, node, gb);
+            for (int c = 0; c < 3; ++c) {
+              gb.c[c] = gbox_sm[c][warp][lane];
+              gb.h[c] = gbox_sm[3 + c][warp][lane];
+            }
+            gb.a_min = gbox_sm[6][warp][lane];
+            gd = groupDecisionNode(a, node, gb, g, is_leaf);
           }
         }
         gd = __shfl_sync(0xffffffffu, gd, leader);
