@@ -802,8 +802,11 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
     return chui::fail(c, CHUI_TREEPM_ESTATE, "TreePM long-range reuse requested without a compatible PM field");
   }
 
-  // periodic tree build (first: the PM deposit reads the tree-ordered sources)
-  if ((rc = chui::treeBuild(c, n, x, y, z, m, src->uniform_mass, lo, hi, s))) {
+  // periodic tree build (first: the PM deposit reads the tree-ordered sources);
+  // equal masses travel as one value instead of a lane of scattered reads
+  const bool equal_masses = m && mass_range[0] == mass_range[1];
+  if ((rc = chui::treeBuild(c, n, x, y, z, equal_masses ? nullptr : m,
+                            equal_masses ? mass_range[0] : src->uniform_mass, lo, hi, s))) {
     if (c.last_error.empty()) c.last_error = "TreePM tree build failed";
     return rc;
   }

@@ -130,7 +130,7 @@ struct Context {
   DevBuf pos_of_row;   // u32 per caller row: tree position
   DevBuf src_f4;       // float4 per tree position: offset from leaf centre (FP32) + mass
   DevBuf src_d4;       // double4 per tree position: caller position + mass (FP64 path)
-  DevBuf src_u4;       // double4 per tree position: unwrapped (tree frame) position + mass (mixed path)
+  DevBuf src_u4;       // double4 per tree position: unwrapped (tree frame) position + mass (moments, walk)
   DevBuf src_cot;      // double4 per tree position: force cotangent (adjoint walk)
   DevBuf target_order; // visit order of active slots
   DevBuf morton_sorted;  // sorted Morton keys (diagnostic parity output)

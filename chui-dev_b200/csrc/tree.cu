@@ -51,18 +51,26 @@ __device__ __forceinline__ double bitsd(unsigned long long b) {
 // Canonical wrap of unwrapPeriodicAxis (tree_pm_coupling.cpp:166-183), then
 // bucket min/max of the non-negative IEEE bits (buckets stored reversed so a
 // forward exclusive min-scan yields "smallest value in any later bucket").
+// The canonical periodic coordinate of the unwrap's first pass. One compiled
+// copy (not inlined) serves the unwrap and the source packing, which
+// recomputes the tree-frame coordinate and must get the same bits.
+__device__ __noinline__ double canonicalCoordinate(double x, double box, int canonical) {
+  double v = canonical ? x : x - box * floor(x / box);
+  if (v >= box) {
+    v = 0.0;
+  } else if (v < 0.0) {
+    v += box;
+  }
+  if (v == 0.0) v = 0.0;
+  return v;
+}
+
 __global__ void wrapBucketKernel(int64_t n, const double* __restrict__ in, double box, int canonical,
                                  double* out, unsigned long long nb, double bucket_scale,
                                  unsigned long long* bmin_rev, unsigned long long* bmax) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    double v = canonical ? in[i] : in[i] - box * floor(in[i] / box);
-    if (v >= box) {
-      v = 0.0;
-    } else if (v < 0.0) {
-      v += box;
-    }
-    if (v == 0.0) v = 0.0;
+    const double v = canonicalCoordinate(in[i], box, canonical);
     out[i] = v;
     unsigned long long b = static_cast<unsigned long long>(v * bucket_scale);
     if (b >= nb) b = nb - 1;
@@ -482,12 +490,7 @@ __global__ void leafKeyKernel(int64_t n, const uint32_t* __restrict__ inv_rank,
 }
 
 struct MomentIn {
-  const double* ux;
-  const double* uy;
-  const double* uz;
-  const double* m;
-  double uniform_mass;
-  const uint32_t* sorted;
+  const double4* u4;  // tree-ordered tree-frame positions and masses
   int quadrupole;
 };
 
@@ -495,12 +498,12 @@ __device__ void leafMoments(int64_t node, const MomentIn& in, const double4 g, c
                             double4* com_out, double* quad_out) {
   double total = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
   for (uint32_t t = r.x; t < r.x + r.y; ++t) {
-    const uint32_t s = in.sorted[t];
-    const double ms = in.m ? in.m[s] : in.uniform_mass;
+    const double4 p = in.u4[t];
+    const double ms = p.w;
     total += ms;
-    wx += ms * in.ux[s];
-    wy += ms * in.uy[s];
-    wz += ms * in.uz[s];
+    wx += ms * p.x;
+    wy += ms * p.y;
+    wz += ms * p.z;
   }
   double cx = g.x, cy = g.y, cz = g.z;
   if (total > 0.0) {
@@ -512,9 +515,9 @@ __device__ void leafMoments(int64_t node, const MomentIn& in, const double4 g, c
   if (in.quadrupole && total > 0.0) {
     double ixx = 0, ixy = 0, ixz = 0, iyy = 0, iyz = 0, izz = 0;
     for (uint32_t t = r.x; t < r.x + r.y; ++t) {
-      const uint32_t s = in.sorted[t];
-      const double ms = in.m ? in.m[s] : in.uniform_mass;
-      const double rx = in.ux[s] - cx, ry = in.uy[s] - cy, rz = in.uz[s] - cz;
+      const double4 p = in.u4[t];
+      const double ms = p.w;
+      const double rx = p.x - cx, ry = p.y - cy, rz = p.z - cz;
       ixx += ms * rx * rx;
       ixy += ms * rx * ry;
       ixz += ms * rx * rz;
@@ -667,10 +670,28 @@ __global__ void nodeBoundsKernel(int64_t nodes, const double4* __restrict__ geom
 // Tree-ordered source records. Mixed precision: FP32 offset of the unwrapped
 // position from its leaf's FP64 centre, plus mass. FP64: the caller's
 // position (the reference's source lanes, :3736-3800) plus mass.
+// How the tree frame follows from the caller's coordinates, per axis: the
+// canonical coordinate plus one box below the anchor (periodic), or the
+// coordinate itself (isolated/open).
+struct FrameSpec {
+  double box[3], anchor[3];
+  int canonical[3];
+  int periodic;
+};
+
+__device__ __forceinline__ double treeFrameCoordinate(double x, const FrameSpec& f, int a) {
+  if (!f.periodic) return x;
+  double v = canonicalCoordinate(x, f.box[a], f.canonical[a]);
+  if (v < f.anchor[a]) v += f.box[a];  // applyAnchorKernel
+  return v;
+}
+
+// Tree-ordered source records. The tree-frame coordinates are recomputed from
+// the gathered caller coordinates (the same arithmetic as the unwrap), so a
+// source costs three scattered position reads (four with a mass lane).
 __global__ void packSourcesKernel(int64_t n, const uint32_t* __restrict__ sorted,
                                   const uint32_t* __restrict__ leaf_of_pos,
-                                  const double4* __restrict__ geom, const double* __restrict__ ux,
-                                  const double* __restrict__ uy, const double* __restrict__ uz,
+                                  const double4* __restrict__ geom, FrameSpec frame,
                                   const double* __restrict__ x, const double* __restrict__ y,
                                   const double* __restrict__ z, const double* __restrict__ m,
                                   double uniform_mass, float4* f4, double4* d4, double4* u4,
@@ -680,13 +701,17 @@ __global__ void packSourcesKernel(int64_t n, const uint32_t* __restrict__ sorted
     const uint32_t s = sorted[t];
     const double ms = m ? m[s] : uniform_mass;
     pos_of_row[s] = static_cast<uint32_t>(t);
+    const double px = x[s], py = y[s], pz = z[s];
+    const double ux = treeFrameCoordinate(px, frame, 0);
+    const double uy = treeFrameCoordinate(py, frame, 1);
+    const double uz = treeFrameCoordinate(pz, frame, 2);
     if (f4) {
       const double4 g = geom[leaf_of_pos[t]];
-      f4[t] = make_float4(static_cast<float>(ux[s] - g.x), static_cast<float>(uy[s] - g.y),
-                          static_cast<float>(uz[s] - g.z), static_cast<float>(ms));
+      f4[t] = make_float4(static_cast<float>(ux - g.x), static_cast<float>(uy - g.y), static_cast<float>(uz - g.z),
+                          static_cast<float>(ms));
     }
-    if (d4) d4[t] = make_double4(x[s], y[s], z[s], ms);
-    if (u4) u4[t] = make_double4(ux[s], uy[s], uz[s], ms);
+    if (d4) d4[t] = make_double4(px, py, pz, ms);
+    if (u4) u4[t] = make_double4(ux, uy, uz, ms);
   }
 }
 
@@ -809,7 +834,11 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   const double* in[3] = {x, y, z};
   double* u[3] = {c.ux.as<double>(), c.uy.as<double>(), c.uz.as<double>()};
   double anchors[3];
+  FrameSpec frame;
+  frame.periodic = c.cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_PERIODIC ? 1 : 0;
   for (int a = 0; a < 3; ++a) {
+    frame.box[a] = box[a];
+    frame.canonical[a] = src_lo[a] >= 0.0 && src_hi[a] < box[a];
     if (c.cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC) {
       // isolated/open: the tree takes the caller's coordinates (tree_pm_coupling.cpp:3179-3196)
       cudaMemcpyAsync(u[a], in[a], static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
@@ -821,6 +850,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     int rc = unwrapAxis(c, n, in[a], box[a], canonical, u[a], &anchors[a], s);
     if (rc) return rc;
   }
+  for (int a = 0; a < 3; ++a) frame.anchor[a] = anchors[a];
   // bounds of the unwrapped frame
   auto* sc = c.scalars.as<unsigned long long>();
   unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
@@ -975,15 +1005,22 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   rc = cubSortPairsU32(c, leaf_key, c.idx_d.as<uint32_t>(), perm_m, c.sorted_index.as<uint32_t>(), n,
                        bitsFor(total_nodes), s);
   if (rc) return rc;
-  // moments
+  // tree-ordered source records
+  const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
+  if (mixed) {
+    if (ensure(c.src_f4, n * sizeof(float4))) return CHUI_TREEPM_ENOMEM;
+  }
+  if (ensure(c.src_d4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
+  if (ensure(c.src_u4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
+  { noteLaunch(); packSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), out.leaf_of_pos, out.geom,
+                                                    frame, x, y, z, m, uniform_mass,
+                                                    mixed ? c.src_f4.as<float4>() : nullptr,
+                                                    c.src_d4.as<double4>(), c.src_u4.as<double4>(),
+                                                    c.pos_of_row.as<uint32_t>()); }
+  // moments (leaves read the tree-ordered records written above)
   cudaMemsetAsync(c.node_counter.ptr, 0, total_nodes * 4, s);
   MomentIn mi;
-  mi.ux = u[0];
-  mi.uy = u[1];
-  mi.uz = u[2];
-  mi.m = m;
-  mi.uniform_mass = uniform_mass;
-  mi.sorted = c.sorted_index.as<uint32_t>();
+  mi.u4 = c.src_u4.as<double4>();
   mi.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
   { noteLaunch(); momentsKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(total_nodes, mi, out.geom, out.range, out.parent,
                                                           out.child, c.node_counter.as<uint32_t>(),
@@ -993,18 +1030,6 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   { noteLaunch(); nodeFrameKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.geom, c.node_com.as<double4>(),
                                                             c.node_quad.as<double>(), c.node_f4.as<float4>(),
                                                             c.node_mq.as<float4>()); }
-  // tree-ordered source records
-  const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
-  if (mixed) {
-    if (ensure(c.src_f4, n * sizeof(float4))) return CHUI_TREEPM_ENOMEM;
-  }
-  if (ensure(c.src_d4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
-  if (mixed && ensure(c.src_u4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
-  { noteLaunch(); packSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), out.leaf_of_pos, out.geom,
-                                                    u[0], u[1], u[2], x, y, z, m, uniform_mass,
-                                                    mixed ? c.src_f4.as<float4>() : nullptr,
-                                                    c.src_d4.as<double4>(), mixed ? c.src_u4.as<double4>() : nullptr,
-                                                    c.pos_of_row.as<uint32_t>()); }
   // maximum depth (for stack sizing and stats)
   {
     size_t bytes = 0;

@@ -70,7 +70,7 @@ struct WalkArgs {
   const double4* src_d4;
   const float4* node_f4;
   const float4* node_mq;   // per node 2 x float4: {mass, Mxx, Mxy, Mxz}, {Myy, Myz, Mzz, trace}
-  const double4* src_u4;   // tree-ordered unwrapped positions + mass (mixed)
+  const double4* src_u4;   // tree-ordered unwrapped positions + mass
   const double* prev;      // per slot |a_previous| (nullable: no history)
   // group walk
   const uint32_t* leaf_of_pos;  // tree position -> leaf node
