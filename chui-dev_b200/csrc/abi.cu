@@ -641,13 +641,14 @@ void chui_treepm_destroy(void* handle) {
                             &c->out_acc[0], &c->out_acc[1], &c->out_acc[2], &c->out_pm[0], &c->out_pm[1],
                             &c->out_pm[2], &c->out_tree[0], &c->out_tree[1], &c->out_tree[2], &c->out_near,
                             &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max,
-                            &c->bucket_next, &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
+                            &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
                             &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
                             &c->leaf_of_pos, &c->inv_pos, &c->cub_temp, &c->node_geom, &c->node_com,
                             &c->node_quad, &c->node_f4, &c->node_mq, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
                             &c->node_counter, &c->sorted_index, &c->pos_of_row, &c->src_f4, &c->src_d4, &c->src_u4, &c->src_cot,
                             &c->target_order, &c->morton_sorted, &c->walk_counters, &c->work_counter,
-                            &c->tree_acc, &c->tree_near};
+                            &c->tree_acc, &c->tree_near, &c->walk_cost, &c->out_lr[0], &c->out_lr[1],
+                            &c->out_lr[2]};
     for (auto* b : bufs) chui::release(*b);
     if (c->events_ready)
       for (auto& e : c->ev) cudaEventDestroy(e);
@@ -957,7 +958,8 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
   uint32_t walk_status = 0;
   cudaMemcpyAsync(&walk_status, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
   unsigned long long counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (n > 0 && nt > 0) cudaMemcpyAsync(counters, c.walk_counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, s);
+  if (n > 0 && nt > 0 && c.walk_counters.ptr)
+    cudaMemcpyAsync(counters, c.walk_counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, s);
   if (memory == CHUI_TREEPM_HOST && nout > 0) {
     cudaMemcpyAsync(acc->accel_x, ax, nout * 8, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(acc->accel_y, ay, nout * 8, cudaMemcpyDeviceToHost, s);

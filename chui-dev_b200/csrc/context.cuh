@@ -103,7 +103,7 @@ struct Context {
 
   // tree construction
   DevBuf ux, uy, uz;             // unwrapped FP64 coordinates (tree frame)
-  DevBuf bucket_min, bucket_max, bucket_next;
+  DevBuf bucket_min, bucket_max;  // unwrap sort keys; bucket_max is also tree-path sort scratch
   DevBuf keys_a, keys_b, idx_a, idx_b, idx_c, idx_d;
   DevBuf path_words;             // kMaxPathWords * n u64
   DevBuf common_prefix;          // int8/int32 per sorted position

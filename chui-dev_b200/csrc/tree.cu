@@ -48,11 +48,12 @@ __device__ __forceinline__ double bitsd(unsigned long long b) {
 
 // ---------------------------------------------------------------- unwrap
 
-// Canonical wrap of unwrapPeriodicAxis (tree_pm_coupling.cpp:166-183), then
-// bucket min/max of the non-negative IEEE bits (buckets stored reversed so a
-// forward exclusive min-scan yields "smallest value in any later bucket").
-// The canonical periodic coordinate of the unwrap's first pass. One compiled
-// copy (not inlined) serves the unwrap and the source packing, which
+// unwrapPeriodicAxis (tree_pm_coupling.cpp:94-218): canonical wrap, the
+// coordinates sorted by their non-negative IEEE bits, the largest circular gap
+// between neighbours, and one box added below the value after it.
+//
+// The canonical periodic coordinate (tree_pm_coupling.cpp:166-183). One
+// compiled copy (not inlined) serves the unwrap and the source packing, which
 // recomputes the tree-frame coordinate and must get the same bits.
 __device__ __noinline__ double canonicalCoordinate(double x, double box, int canonical) {
   double v = canonical ? x : x - box * floor(x / box);
@@ -65,53 +66,39 @@ __device__ __noinline__ double canonicalCoordinate(double x, double box, int can
   return v;
 }
 
-__global__ void wrapBucketKernel(int64_t n, const double* __restrict__ in, double box, int canonical,
-                                 double* out, unsigned long long nb, double bucket_scale,
-                                 unsigned long long* bmin_rev, unsigned long long* bmax) {
+__global__ void canonicalKeysKernel(int64_t n, const double* __restrict__ in, double box, int canonical,
+                                    double* out, unsigned long long* keys) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const double v = canonicalCoordinate(in[i], box, canonical);
     out[i] = v;
-    unsigned long long b = static_cast<unsigned long long>(v * bucket_scale);
-    if (b >= nb) b = nb - 1;
-    const unsigned long long bits = dbits(v);
-    atomicMin(bmin_rev + (nb - 1 - b), bits);
-    atomicMax(bmax + b, bits);
+    keys[i] = dbits(v);
   }
 }
 
-// Largest circular gap over occupied buckets: gap = next - current with the
-// wrap-around next = first + L (tree_pm_coupling.cpp:189-207). Pass 0 finds
-// the largest gap (gaps are >= 0, so their bit patterns order like the
-// values; reduced per block, one atomic per block); pass 1 takes the smallest
-// anchor among the buckets whose gap equals it.
-__global__ void __launch_bounds__(256) bucketGapKernel(unsigned long long nb, const unsigned long long* __restrict__ bmin_rev,
-                                const unsigned long long* __restrict__ bmax,
-                                const unsigned long long* __restrict__ later_min_rev, double box,
-                                unsigned long long global_min, unsigned long long* best_gap,
-                                int pass, unsigned long long* best_anchor) {
+// Circular gaps of the sorted coordinates: gap_i = v[i+1] - v[i], and
+// v[0] + L - v[n-1] around the box (tree_pm_coupling.cpp:189-207). Pass 0
+// finds the largest (gaps are >= 0, so their bits order like the values;
+// reduced per block, one atomic per block); pass 1 takes the smallest value
+// after a gap equal to it as the anchor.
+__global__ void __launch_bounds__(256) sortedGapKernel(int64_t n, const unsigned long long* __restrict__ sorted,
+                                                        double box, unsigned long long* best_gap, int pass,
+                                                        unsigned long long* best_anchor) {
   unsigned long long local = 0ull;
   const unsigned long long target = pass == 0 ? 0ull : *best_gap;
-  for (unsigned long long b = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x;
-       b < nb; b += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
-    const unsigned long long rb = nb - 1 - b;
-    if (bmin_rev[rb] == ~0ull) continue;
-    const double cur = bitsd(bmax[b]);
-    const unsigned long long later = later_min_rev[rb];
-    double cand, next;
-    if (later == ~0ull) {
-      cand = bitsd(global_min);
-      next = cand + box;
-    } else {
-      cand = bitsd(later);
-      next = cand;
-    }
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double cur = bitsd(sorted[i]);
+    const bool around = i + 1 == n;
+    const unsigned long long after = around ? sorted[0] : sorted[i + 1];
+    const double cand = bitsd(after);
+    const double next = around ? cand + box : cand;
     const double gap = next - cur;
     if (pass == 0) {
       const unsigned long long g = dbits(gap);
       local = g > local ? g : local;
     } else if (dbits(gap) == target) {
-      atomicMin(best_anchor, dbits(cand));
+      atomicMin(best_anchor, after);
     }
   }
   if (pass != 0) return;
@@ -138,11 +125,6 @@ __global__ void applyAnchorKernel(int64_t n, double* u, double box, const unsign
   }
 }
 
-struct MinU64 {
-  __device__ __forceinline__ unsigned long long operator()(unsigned long long a, unsigned long long b) const {
-    return a < b ? a : b;
-  }
-};
 
 // ------------------------------------------------------------- bounds
 
@@ -790,31 +772,23 @@ static int unwrapAxis(Context& c, int64_t n, const double* in, double box, int c
     *anchor = 0.0;
     return 0;
   }
-  const unsigned long long nb = 2ull * static_cast<unsigned long long>(n);
-  if (ensure(c.bucket_min, nb * 8) || ensure(c.bucket_max, nb * 8) || ensure(c.bucket_next, nb * 8))
+  if (ensure(c.bucket_min, static_cast<size_t>(n) * 8) || ensure(c.bucket_max, static_cast<size_t>(n) * 8))
     return CHUI_TREEPM_ENOMEM;
-  auto* bmin = c.bucket_min.as<unsigned long long>();
-  auto* bmax = c.bucket_max.as<unsigned long long>();
-  auto* later = c.bucket_next.as<unsigned long long>();
-  cudaMemsetAsync(bmin, 0xFF, nb * 8, s);
-  cudaMemsetAsync(bmax, 0x00, nb * 8, s);
-  const double scale = static_cast<double>(nb) / box;
-  { noteLaunch(); wrapBucketKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in, box, canonical, out, nb, scale, bmin, bmax); }
+  auto* keys = c.bucket_min.as<unsigned long long>();
+  auto* sorted = c.bucket_max.as<unsigned long long>();
+  { noteLaunch(); canonicalKeysKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in, box, canonical, out, keys); }
+  // canonical coordinates are non-negative: bit 63 is zero
   size_t bytes = 0;
-  cub::DeviceScan::ExclusiveScan(nullptr, bytes, bmin, later, MinU64(), ~0ull, static_cast<int>(nb), s);
+  cub::DeviceRadixSort::SortKeys(nullptr, bytes, keys, sorted, static_cast<int>(n), 0, 63, s);
   if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
-  cub::DeviceScan::ExclusiveScan(c.cub_temp.ptr, bytes, bmin, later, MinU64(), ~0ull, static_cast<int>(nb), s);
-  // global minimum = min(later[nb-1], bmin[nb-1]) (bucket 0 is the last reversed slot)
-  unsigned long long tail[2];
-  cudaMemcpyAsync(&tail[0], later + nb - 1, 8, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(&tail[1], bmin + nb - 1, 8, cudaMemcpyDeviceToHost, s);
-  cudaStreamSynchronize(s);
-  const unsigned long long gmin = tail[0] < tail[1] ? tail[0] : tail[1];
+  if (cub::DeviceRadixSort::SortKeys(c.cub_temp.ptr, bytes, keys, sorted, static_cast<int>(n), 0, 63, s) !=
+      cudaSuccess)
+    return CHUI_TREEPM_EDEVICE;
   auto* sc = c.scalars.as<unsigned long long>();
   unsigned long long init[2] = {0ull, ~0ull};
   cudaMemcpyAsync(sc, init, 16, cudaMemcpyHostToDevice, s);
-  { noteLaunch(); bucketGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, later, box, gmin, sc, 0, sc + 1); }
-  { noteLaunch(); bucketGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, later, box, gmin, sc, 1, sc + 1); }
+  { noteLaunch(); sortedGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, sorted, box, sc, 0, sc + 1); }
+  { noteLaunch(); sortedGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, sorted, box, sc, 1, sc + 1); }
   { noteLaunch(); applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out, box, sc + 1); }
   unsigned long long ab = 0;
   cudaMemcpyAsync(&ab, sc + 1, 8, cudaMemcpyDeviceToHost, s);

@@ -1888,16 +1888,17 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
             int64_t visit_begin, int64_t visit_end, bool compact) {
   if (visit_end < 0) visit_end = nt;
   if (nt == 0) return 0;
-  // per-chunk walk cycles (zero for chunks outside the visit range)
+  // counters and per-chunk walk cycles start at zero even when the visit
+  // range is empty (the solve reads the counters back either way)
   const size_t chunks = static_cast<size_t>((nt + 31) / 32);
-  if (ensure(c.walk_cost, chunks * sizeof(float))) return CHUI_TREEPM_ENOMEM;
+  if (ensure(c.walk_cost, chunks * sizeof(float)) || ensure(c.walk_counters, 8 * sizeof(unsigned long long)))
+    return CHUI_TREEPM_ENOMEM;
   cudaMemsetAsync(c.walk_cost.ptr, 0, chunks * sizeof(float), s);
+  cudaMemsetAsync(c.walk_counters.ptr, 0, 8 * sizeof(unsigned long long), s);
   if (visit_end <= visit_begin) return 0;
   if (ensure(c.tree_acc, static_cast<size_t>(nt) * 3 * sizeof(double)) ||
-      ensure(c.tree_near, static_cast<size_t>(nt) * sizeof(double)) ||
-      ensure(c.walk_counters, 8 * sizeof(unsigned long long)) || ensure(c.work_counter, 4))
+      ensure(c.tree_near, static_cast<size_t>(nt) * sizeof(double)) || ensure(c.work_counter, 4))
     return CHUI_TREEPM_ENOMEM;
-  cudaMemsetAsync(c.walk_counters.ptr, 0, 8 * sizeof(unsigned long long), s);
   cudaMemsetAsync(c.work_counter.ptr, 0, 4, s);
   WalkArgs a;
   a.nt = nt;
