@@ -317,7 +317,8 @@ class TreePmCoordinator {
       check(chui_treepm_solve(m_handle, &src, &acc, refresh_long_range_field ? 1 : 0, CHUI_TREEPM_HOST, nullptr,
                               &stats));
     }
-    if (diagnostics != nullptr) fillDiagnostics(stats, pos_x_comoving.size(), targets, refresh_long_range_field, *diagnostics);
+    // a visit-range solve walks only its slice's targets
+    if (diagnostics != nullptr) fillDiagnostics(stats, pos_x_comoving.size(), outputs, refresh_long_range_field, *diagnostics);
     if (profile != nullptr) {
       *profile = TreePmProfileEvent{};
       profile->pm_ms = stats.pm_ms;
@@ -332,7 +333,7 @@ class TreePmCoordinator {
       t.accepted_nodes = stats.accepted_nodes;
       t.opened_nodes = stats.opened_nodes;
       t.particle_particle_interactions = stats.direct_pair_evaluations;
-      t.traversed_target_count = targets;
+      t.traversed_target_count = outputs;
       t.actual_node_count = stats.node_count;
     }
   }
