@@ -810,7 +810,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
 }
 
 constexpr int kQueue = 64;   // sources per warp batch
-constexpr int kMultList = 8; // accepted multipoles per lane before a flush
+constexpr int kMultList = 4; // accepted multipoles per lane before a flush (4 against 8: group walk 209 -> 202 ms)
 
 // Subtree blocks of the production walk (diagnostics off): an opened node
 // with at most kBulkCount sources and half-size at most kBulkHalf * r_cut is
@@ -1011,10 +1011,10 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   constexpr bool kGroup = kMode == 3;
   constexpr bool kHistory = kMode != 0;
   constexpr int kList = kAdaptive ? kMultList : 1;
-  // sources per warp batch: longer for the strict walk (fewer flushes; 221.4
-  // against 224.1 ms at 256^3), the adaptive instances' shared memory (lane
-  // multipole lists) keeps them at 64 for occupancy
-  constexpr int kQueueLen = kAdaptive ? kQueue : 2 * kQueue;
+  // sources per warp batch: longer for the strict walk (fewer flushes; 256
+  // against 64 took 224.1 to 219.8 ms at 256^3), the adaptive instances'
+  // shared memory (lane multipole lists) keeps them at 64 for occupancy
+  constexpr int kQueueLen = kAdaptive ? kQueue : 4 * kQueue;
   __shared__ long long item_start_sm[kWalkWarpsPerBlock];
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
   __shared__ float4 q_src[kWalkWarpsPerBlock][kQueueLen];
