@@ -64,7 +64,7 @@ int main(int argc, char** argv) {
       const std::size_t half = (static_cast<std::size_t>(n) / 2) / 64 * 64;
       double worst = 0.0, scale = 0.0;
       for (double v : ax) scale = std::max(scale, std::fabs(v));
-      for (const auto [b, e] : {std::pair<std::size_t, std::size_t>{0, half},
+      for (const auto& [b, e] : {std::pair<std::size_t, std::size_t>{0, half},
                                 std::pair<std::size_t, std::size_t>{half, static_cast<std::size_t>(n)}}) {
         std::vector<double> sx(e - b), sy(e - b), sz(e - b);
         cb::TreePmForceAccumulatorView part{active, sx, sy, sz};

@@ -193,3 +193,20 @@ def test_isolated_boundary_validation():
     assert ct.config_from_param_text(deck).boundary_condition == _abi.BOUNDARY_PERIODIC
     with pytest.raises(ValueError):
         ct.config_from_param_text(DECK + "[mode]\ngravity_boundary = open\n")
+
+
+def test_cpp_shim_compiles_and_links(tmp_path):
+    """The C++20 shim (the class a CHUI build compiles in place of the
+    reference's TreePmCoordinator) and its example program build against the
+    C-ABI header and link against the library; running it needs a GPU
+    (tests/test_gpu_cpp_shim.py)."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    host = os.path.join(ROOT, "chui-dev_b200", "host")
+    build = os.path.dirname(_abi.LIB_PATH)
+    exe = tmp_path / "shim_example"
+    subprocess.run(["g++", "-std=c++20", "-O1", "-Wall", "-Werror", os.path.join(host, "shim_example.cpp"),
+                    f"-L{build}", "-lchui_treepm", "-o", str(exe)], check=True)
+    assert exe.exists()
