@@ -876,7 +876,10 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
   cudaMemsetAsync(c.status.ptr, 0, 4, s);
   if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, prev, wp, n, s, visit_begin, visit_end,
                                      ranged)))
-    return chui::fail(c, rc, "residual walk launch failed");
+    return chui::fail(c, rc, rc == CHUI_TREEPM_ENOTSUP
+                                 ? "the mixed-precision pair kernel's constants (H(t)/(8 r_s^3)) overflow FP32 for "
+                                   "this split scale; use precision FP64"
+                                 : "residual walk launch failed");
   if (n == 0 && nt > 0) {
     if (chui::ensure(c.tree_acc, nt * 3 * 8) || chui::ensure(c.tree_near, nt * 8))
       return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");

@@ -93,6 +93,14 @@ struct WalkArgs {
   float inv_32rs7_f;
   int mult_f32;    // accepted multipoles in FP32 (the split constants are normal floats)
   int mpoly12;     // H' and H'' fits have at most 12 terms
+  // Packed (f32x2) operands of the pair loop, each value in both halves, so
+  // that two queued sources share every FP32 instruction: the coefficients
+  // of -H(t)/(8 r_s^3) (minus the long-range kernel K_long), the scale and
+  // offset taking r^2 + eps^2 to the polynomial variable s = r^2 sc - 1, and
+  // eps^2. cut2e = r_cut^2 + eps^2 is the cutoff test on r^2 + eps^2.
+  float2 pk2[kPolyMaxTerms];
+  float2 sc2, soff2, eps2_2;
+  float cut2e;
   WalkParams wp;
 };
 
@@ -821,6 +829,12 @@ constexpr int kMultList = 4; // accepted multipoles per lane before a flush (4 a
 #ifndef CHUI_BULK_HALF
 #define CHUI_BULK_HALF 1.0
 #endif
+#ifndef CHUI_PAIR_UNROLL
+#define CHUI_PAIR_UNROLL 4  // source pairs per unrolled step of the pair loop
+#endif
+#ifndef CHUI_WALK_MIN_BLOCKS_STRICT
+#define CHUI_WALK_MIN_BLOCKS_STRICT 6  // the strict, uniform-mass production instances (80 registers)
+#endif
 #ifndef CHUI_WALK_MIN_BLOCKS
 #define CHUI_WALK_MIN_BLOCKS 5  // resident blocks per SM the register budget is sized for
 #endif
@@ -833,6 +847,7 @@ constexpr int kMultList = 4; // accepted multipoles per lane before a flush (4 a
 constexpr uint32_t kBulkCount = CHUI_BULK_COUNT;
 constexpr uint32_t kBulkCountAdaptive = CHUI_BULK_COUNT_ADAPTIVE;
 constexpr double kBulkHalf = CHUI_BULK_HALF;
+constexpr int kPairUnroll = CHUI_PAIR_UNROLL;
 
 // The fitted polynomial at t = r^2 / (4 r_s^2), straight from r^2: s =
 // r^2 * sc - 1 with sc = scale / (4 r_s^2), then Horner (kTerms - 1 FMAs).
@@ -844,6 +859,18 @@ __device__ __forceinline__ float hornerR2(const PolyH& p, float r2, float sc) {
   float h = p.c[kTerms - 1];
 #pragma unroll
   for (int k = kTerms - 2; k >= 0; --k) h = fmaf(h, s, p.c[k]);
+  return h;
+}
+
+// The same Horner chain for two sources at once (packed FP32: one f32x2 FMA
+// per term serves both halves); c2 holds each coefficient in both halves,
+// s = r2 * sc2 + off2.
+template <int kTerms>
+__device__ __forceinline__ float2 hornerR2x2(const float2* c2, float2 r2, float2 sc2, float2 off2) {
+  const float2 s = __ffma2_rn(r2, sc2, off2);
+  float2 h = c2[kTerms - 1];
+#pragma unroll
+  for (int k = kTerms - 2; k >= 0; --k) h = __ffma2_rn(h, s, c2[k]);
   return h;
 }
 
@@ -1006,7 +1033,9 @@ __device__ __forceinline__ int certainLess(float a, float b, float err = 0.f) {
 // and the mass multiplies the flush's partial sums once.
 template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode, bool kUniform = false,
           bool kCost = false>
-__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS) walkFastKernel(WalkArgs a) {
+__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUniform) ? CHUI_WALK_MIN_BLOCKS_STRICT
+                                                                                  : CHUI_WALK_MIN_BLOCKS)
+    walkFastKernel(WalkArgs a) {
   constexpr bool kAdaptive = kMode >= 2;
   constexpr bool kGroup = kMode == 3;
   constexpr bool kHistory = kMode != 0;
@@ -1015,12 +1044,21 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
   // against 64 took 224.1 to 219.8 ms at 256^3), the adaptive instances'
   // shared memory (lane multipole lists) keeps them at 64 for occupancy
   constexpr int kQueueLen = kAdaptive ? kQueue : 4 * kQueue;
+  static_assert(kQueueLen % 2 == 0, "the queue holds pairs of sources");
   __shared__ long long item_start_sm[kWalkWarpsPerBlock];
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
+  // The queue holds sources in pairs, laid out for packed FP32 evaluation:
+  // pair p is q_src[2p] = {x0, x1, y0, y1}, q_src[2p+1] = {z0, z1, w0, w1}
+  // (w: mass, or the lane mask under kUniform), and q_meta[p] = {mask0,
+  // mask1, tree position 0, tree position 1} when masses travel separately.
   __shared__ float4 q_src[kWalkWarpsPerBlock][kQueueLen];
-  __shared__ uint2 q_meta[kWalkWarpsPerBlock][kQueueLen];
+  __shared__ uint4 q_meta[kWalkWarpsPerBlock][kQueueLen / 2];
   __shared__ float4 m_list[kWalkWarpsPerBlock][kList][32];
   __shared__ double4 exact_sm[kWalkWarpsPerBlock][32];
+  // per-lane FP64 target position and accumulators, kept in shared memory
+  // rather than registers: they are touched once per flush or exact decision,
+  // and the registers they would hold buy the pair loop occupancy and ILP
+  __shared__ double lane_sm[6][kWalkWarpsPerBlock][32];
   // group walk: each deciding lane's group box {centre, half, a_min}, read at
   // every node visit (components outermost: no bank conflicts)
   __shared__ double gbox_sm[kGroup ? 7 : 1][kWalkWarpsPerBlock][32];
@@ -1056,7 +1094,12 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     const int64_t v = static_cast<int64_t>(base) + lane;
     const bool valid = v < a.v1;
     uint32_t slot = 0, row = kInvalid;
-    double px = 0.0, py = 0.0, pz = 0.0;
+    double& px = lane_sm[0][warp][lane];
+    double& py = lane_sm[1][warp][lane];
+    double& pz = lane_sm[2][warp][lane];
+    px = 0.0;
+    py = 0.0;
+    pz = 0.0;
     if (valid) {
       slot = a.order[v];
       row = a.active ? a.active[slot] : slot;
@@ -1126,7 +1169,12 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
       allow_f = static_cast<float>(kAdaptive ? w.rel_tol * hist.mag : w.rel_tol * fmax(fabs(hist.mag), w.floor_));
       if (!(allow_f >= FLT_MIN && allow_f <= FLT_MAX)) allow_f = 0.f;  // FP32 cannot decide: exact path
     }
-    double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
+    double& acc_x = lane_sm[3][warp][lane];
+    double& acc_y = lane_sm[4][warp][lane];
+    double& acc_z = lane_sm[5][warp][lane];
+    acc_x = 0.0;
+    acc_y = 0.0;
+    acc_z = 0.0;
     float nearest_f = INFINITY;
     uint32_t skip_until = 0;
     int qn = 0;  // warp's source queue length
@@ -1136,42 +1184,78 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
     __syncwarp();
     bool overflow = false;
 
+    // Pair loop over the queue, two sources per step in packed FP32 (f32x2
+    // FMA/ADD/MUL: one instruction serves both sources of a pair); lane
+    // masks, cutoff tests and rsqrt stay per source.
     auto flush = [&]() {
-      float fx = 0.f, fy = 0.f, fz = 0.f;
+      if (qn & 1) {
+        // pad to whole pairs with an entry no lane takes (mask 0, mass 0)
+        if (lane == 0) {
+          float* qf = reinterpret_cast<float*>(&q_src[warp][qn - 1]);
+          qf[1] = 0.f;
+          qf[3] = 0.f;
+          qf[5] = 0.f;
+          qf[7] = 0.f;
+          if constexpr (!kUniform) {
+            uint32_t* qm = reinterpret_cast<uint32_t*>(&q_meta[warp][qn >> 1]);
+            qm[1] = 0u;
+            qm[3] = kInvalid;
+          }
+        }
+        __syncwarp();
+      }
+      const float2 ntx = make_float2(-tfx, -tfx), nty = make_float2(-tfy, -tfy), ntz = make_float2(-tfz, -tfz);
+      float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
       uint32_t pairs = 0, skips = 0;
-#pragma unroll 4
-      for (int k = 0; k < qn; ++k) {
-        const float4 e = q_src[warp][k];
-        uint2 meta = make_uint2(0u, 0u);
+      const int np = (qn + 1) >> 1;
+      auto pairStep = [&](int p, float2& fx, float2& fy, float2& fz) {
+        const float4 A = q_src[warp][2 * p];
+        const float4 B = q_src[warp][2 * p + 1];
+        const float2 dx = __fadd2_rn(make_float2(A.x, A.y), ntx);
+        const float2 dy = __fadd2_rn(make_float2(A.z, A.w), nty);
+        const float2 dz = __fadd2_rn(make_float2(B.x, B.y), ntz);
+        // r^2 + eps^2 in one chain (eps^2 is the first addend); the polynomial
+        // variable and the cutoff test take it with eps^2 folded into their
+        // constants. Diagnostics test the cutoff on r^2 itself, as the
+        // reference does, and report it for the nearest pair.
+        const float2 r2e = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, a.eps2_2)));
+        const float2 r2 = kDiag ? __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz))) : r2e;
+        const float cut_t = kDiag ? cut2 : a.cut2e;
+        bool mine0, mine1;
         if constexpr (kUniform) {
-          meta.x = __float_as_uint(e.w);
+          mine0 = (__float_as_uint(B.z) & lane_bit) != 0u;
+          mine1 = (__float_as_uint(B.w) & lane_bit) != 0u;
         } else {
-          meta = q_meta[warp][k];
+          const uint4 M = q_meta[warp][p];
+          mine0 = kContiguous ? (M.x & lane_bit) != 0u : ((M.x & lane_bit) != 0u && M.z != self_pos);
+          mine1 = kContiguous ? (M.y & lane_bit) != 0u : ((M.y & lane_bit) != 0u && M.w != self_pos);
         }
-        const float dx = e.x - tfx, dy = e.y - tfy, dz = e.z - tfz;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const bool mine = kContiguous ? (meta.x & lane_bit) != 0u : ((meta.x & lane_bit) != 0u && meta.y != self_pos);
-        const bool in = mine && r2 <= cut2;
+        const bool in0 = mine0 && r2.x <= cut_t;
+        const bool in1 = mine1 && r2.y <= cut_t;
         if constexpr (kDiag) {
-          pairs += in ? 1u : 0u;
+          pairs += (in0 ? 1u : 0u) + (in1 ? 1u : 0u);
           // the group walk's pair kernel counts no skipped pairs
-          skips += (mine && !in && !in_group) ? 1u : 0u;
-          nearest_f = in ? fminf(nearest_f, r2) : nearest_f;
+          skips += ((mine0 && !in0 && !in_group) ? 1u : 0u) + ((mine1 && !in1 && !in_group) ? 1u : 0u);
+          nearest_f = in0 ? fminf(nearest_f, r2.x) : nearest_f;
+          nearest_f = in1 ? fminf(nearest_f, r2.y) : nearest_f;
         }
-        const float hh = hornerR2<kTerms>(a.poly, r2, sc_r2);
-        const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
-        const float rinv = rsqrtf(s2);
-        const float k3 = fmaf(-hh, w.inv_8rs3_f, rinv * rinv * rinv);
+        const float2 klong = hornerR2x2<kTerms>(a.pk2, r2e, a.sc2, a.soff2);  // -K_long
+        const float2 rinv = make_float2(rsqrtf(r2e.x), rsqrtf(r2e.y));
+        float2 k3 = __ffma2_rn(__fmul2_rn(rinv, rinv), rinv, klong);  // K_soft - K_long
+        if constexpr (!kUniform) k3 = __fmul2_rn(k3, make_float2(B.z, B.w));
         // coincident sources contribute nothing: with eps > 0 the kernel is
         // finite there and d = 0; with eps = 0 the zero-distance test avoids inf * 0
-        const float f = (kEpsZero ? (in && r2 > 0.f) : in) ? (kUniform ? k3 : e.w * k3) : 0.f;
-        fx = fmaf(f, dx, fx);
-        fy = fmaf(f, dy, fy);
-        fz = fmaf(f, dz, fz);
-      }
-      acc_x += static_cast<double>(g_pair * fx);
-      acc_y += static_cast<double>(g_pair * fy);
-      acc_z += static_cast<double>(g_pair * fz);
+        const float2 f = make_float2((kEpsZero ? (in0 && r2e.x > 0.f) : in0) ? k3.x : 0.f,
+                                     (kEpsZero ? (in1 && r2e.y > 0.f) : in1) ? k3.y : 0.f);
+        fx = __ffma2_rn(f, dx, fx);
+        fy = __ffma2_rn(f, dy, fy);
+        fz = __ffma2_rn(f, dz, fz);
+      };
+#pragma unroll (kPairUnroll)
+      for (int p = 0; p < np; ++p) pairStep(p, fx, fy, fz);
+      acc_x += static_cast<double>(g_pair * (fx.x + fx.y));
+      acc_y += static_cast<double>(g_pair * (fy.x + fy.y));
+      acc_z += static_cast<double>(g_pair * (fz.x + fz.y));
       cnt_pairs += pairs;
       cnt_skips += skips;
       qn = 0;
@@ -1232,12 +1316,17 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, CHUI_WALK_MIN_BLOCKS)
             const uint32_t rel = begin + k - base;
             if (rel < 32u) m &= ~(1u << rel);
           }
-          if constexpr (kUniform) {
-            e.w = __uint_as_float(m);
-            q_src[warp][slot_q] = e;
-          } else {
-            q_src[warp][slot_q] = e;
-            q_meta[warp][slot_q] = make_uint2(m, begin + k);
+          // pair layout (see q_src): entry slot_q is half (slot_q & 1) of pair slot_q / 2
+          float* qf = reinterpret_cast<float*>(&q_src[warp][slot_q & ~1]);
+          const int hq = slot_q & 1;
+          qf[hq] = e.x;
+          qf[2 + hq] = e.y;
+          qf[4 + hq] = e.z;
+          qf[6 + hq] = kUniform ? __uint_as_float(m) : e.w;
+          if constexpr (!kUniform) {
+            uint32_t* qm = reinterpret_cast<uint32_t*>(&q_meta[warp][slot_q >> 1]);
+            qm[hq] = m;
+            qm[2 + hq] = begin + k;
           }
         }
         __syncwarp();
@@ -1961,6 +2050,23 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     a.inv_32rs7_f = static_cast<float>(i7);
     a.mult_f32 = (i5 >= FLT_MIN && i5 <= 1.0e30 && i7 >= FLT_MIN && i7 <= 1.0e30) ? 1 : 0;
     a.mpoly12 = (c.dpoly.terms <= 12 && c.ddpoly.terms <= 12) ? 1 : 0;
+  }
+  {
+    // K_long = H(t)/(8 r_s^3): the pair loop evaluates -K_long directly from
+    // the H coefficients scaled by -1/(8 r_s^3), at s = (r^2 + eps^2) sc + soff
+    // with soff = -1 - eps^2 sc (that is s = r^2 sc - 1, eps^2 folded in)
+    const double kscale = -0.125 / (c.rs * c.rs * c.rs);
+    for (int k = 0; k < kPolyMaxTerms; ++k) {
+      const float v = static_cast<float>(static_cast<double>(c.poly.c[k]) * kscale);
+      if (!std::isfinite(v)) return CHUI_TREEPM_ENOTSUP;  // r_s outside the FP32 pair kernel's range
+      a.pk2[k] = make_float2(v, v);
+    }
+    const float sc = wp.inv_4rs2_f * c.poly.scale;  // the r^2 -> s scale, rounded as the multipoles round it
+    a.sc2 = make_float2(sc, sc);
+    const float soff = static_cast<float>(-1.0 - static_cast<double>(wp.eps2_f) * static_cast<double>(sc));
+    a.soff2 = make_float2(soff, soff);
+    a.eps2_2 = make_float2(wp.eps2_f, wp.eps2_f);
+    a.cut2e = wp.cut2_f + wp.eps2_f;
   }
   a.wp = wp;
   uint32_t* group_count = nullptr;
