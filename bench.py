@@ -157,6 +157,78 @@ def rel_errors(a, b):
     return num / np.maximum(den, 1e-300)
 
 
+def error_summary(e) -> dict:
+    return {"median_rel": float(np.median(e)), "p99_rel": float(np.percentile(e, 99)), "max_rel": float(np.max(e))}
+
+
+def error_map(err, a_ref, x, y, z, box, cells=64) -> dict:
+    """The force-error map of the headline state: the mixed-vs-FP64 relative
+    error binned by the FP64 force magnitude (deciles) and by the local number
+    density (particles per cell of a 64^3 grid over the mean, by decade)."""
+    amag = np.sqrt((a_ref ** 2).sum(axis=0))
+    edges = np.quantile(amag, np.linspace(0.0, 1.0, 11))
+    by_a = []
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        sel = (amag >= lo) & (amag <= hi)
+        by_a.append({"a_min": float(lo), "a_max": float(hi), "n": int(sel.sum()), **error_summary(err[sel])})
+    idx = [np.minimum((np.asarray(c) / box * cells).astype(np.int64), cells - 1) for c in (x, y, z)]
+    flat = (idx[0] * cells + idx[1]) * cells + idx[2]
+    counts = np.bincount(flat, minlength=cells ** 3)
+    dens = counts[flat] / (len(x) / cells ** 3)
+    by_rho = []
+    for lo, hi in ((0.0, 0.1), (0.1, 1.0), (1.0, 10.0), (10.0, 100.0), (100.0, np.inf)):
+        sel = (dens >= lo) & (dens < hi)
+        if sel.any():
+            by_rho.append({"overdensity_min": lo, "overdensity_max": None if np.isinf(hi) else hi,
+                           "n": int(sel.sum()), **error_summary(err[sel])})
+    return {"by_force_decile": by_a, "by_local_density": by_rho,
+            "density_grid": f"{cells}^3 cells, particle count over the mean"}
+
+
+def ewald_accuracy(ct, device: int) -> dict:
+    """GPU TreePM forces (production mixed walk and FP64) against the direct
+    FP64 Ewald sums stored with the reference's outputs in tests/golden (the
+    32^3 configuration and the 64000-particle clustered box with the headline
+    settings), next to the reference TreePM's own error on the same targets."""
+    out = {}
+    for name in ("config32", "clustered64k_cic"):
+        path = os.path.join(ROOT, "tests", "golden", name + ".npz")
+        if not os.path.isfile(path):
+            continue
+        g = dict(np.load(path))
+        k = len(g["ewald_ax"])
+        ew = np.stack([g["ewald_ax"], g["ewald_ay"], g["ewald_az"]])
+        asmth, rcut, theta, gconst, eps = (float(v) for v in g["params"])
+        leaf, scheme, deconv, criterion, order = (int(v) for v in g["iparams"])
+        mesh = [int(v) for v in g["mesh"]]
+        rec = {"targets": k, "reference_rel_l2": float(np.linalg.norm(
+            np.stack([g["ax"][:k], g["ay"][:k], g["az"][:k]]) - ew) / np.linalg.norm(ew))}
+        for label, precision, diag in (("mixed_production", ct._abi.MIXED, 0), ("fp64", ct._abi.FP64, 1)):
+            cfg = ct.TreePmConfig(pm_grid_nx=mesh[0], pm_grid_ny=mesh[1], pm_grid_nz=mesh[2], box_x=float(g["box"][0]),
+                                  box_y=float(g["box"][1]), box_z=float(g["box"][2]), asmth_cells=asmth,
+                                  rcut_cells=rcut, opening_theta=theta, opening_criterion=criterion,
+                                  multipole_order=order, max_leaf_size=leaf, assignment_scheme=scheme,
+                                  window_deconvolution=deconv, gravitational_constant=gconst, softening=eps,
+                                  precision=precision, device=device, diagnostics=diag)
+            with ct.TreePmCoordinator(cfg) as s:
+                r = s.solve_active_set(g["x"], g["y"], g["z"], g["m"])
+            got = np.stack([r["ax"][:k], r["ay"][:k], r["az"][:k]])
+            per = np.linalg.norm(got - ew, axis=0) / np.linalg.norm(ew, axis=0)
+            rec[label] = {"rel_l2": float(np.linalg.norm(got - ew) / np.linalg.norm(ew)),
+                          "median_rel": float(np.median(per)), "max_rel": float(per.max())}
+        out[name] = rec
+    return out
+
+
+def bench_config(args, w, n, world) -> dict:
+    """The workload description both arms print (the same for the reference arm)."""
+    return {"workload": f"{args.workload}: N={n}, L={w['box']} Mpc/h, mesh {w['mesh']}^3, "
+                        f"r_s=1.25 cells, r_cut=6.25 cells, theta={w['theta']}, leaf {w['leaf']}, "
+                        f"CIC+deconvolution, eps={w['eps']}",
+            "particles": n, "l2": "inputs larger than L2 (positions 400 MB)",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
+
+
 def gpu_step(solver, t, acc, factors, stream):
     d, k1, k2, g1, g2 = factors
     solver.kick(t["vx"], t["vy"], t["vz"], acc["ax"], acc["ay"], acc["az"], k1, g1, stream=stream)
@@ -336,8 +408,10 @@ def run_gpu(args) -> int:
     # accuracy of the production walk against the FP64 walk on the initial state
     r_m = mixed.solve_active_set(t["x"], t["y"], t["z"], t["m"])
     r_d = fp64.solve_active_set(t["x"], t["y"], t["z"], t["m"])
-    err = rel_errors([r_m[k].cpu().numpy() for k in ("ax", "ay", "az")],
-                     [r_d[k].cpu().numpy() for k in ("ax", "ay", "az")])
+    a_mixed = np.stack([r_m[k].cpu().numpy() for k in ("ax", "ay", "az")])
+    a_fp64 = np.stack([r_d[k].cpu().numpy() for k in ("ax", "ay", "az")])
+    err = rel_errors(a_mixed, a_fp64)
+    err_map = error_map(err, a_fp64, x, y, z, w["box"])
     # the reference's traversal counters (pairs inside r_cut etc.) come from the FP64 walk
     stats0 = dict(fp64.last_stats)
     log(f"[rank {rank}] mixed vs fp64 median {np.median(err):.3e} p99 {np.percentile(err, 99):.3e}; "
@@ -363,22 +437,29 @@ def run_gpu(args) -> int:
     ms = max_over_ranks(torch, dist, ms, dev)
     value = n * args.steps * world / (ms * 1e-3)
 
-    # end to end through the C-ABI with pinned host buffers
-    hx = torch.from_numpy(x).pin_memory().numpy()
-    hy = torch.from_numpy(y).pin_memory().numpy()
-    hz = torch.from_numpy(z).pin_memory().numpy()
-    hm = torch.from_numpy(m).pin_memory().numpy()
+    # end to end through the C-ABI with pinned host buffers: the same KDK step
+    # (kick, drift, force, kick), every call staging its host arrays in and
+    # its results out
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    h = {k: pinned(v) for k, v in dict(x=x, y=y, z=z, m=m, vx=vx, vy=vy, vz=vz).items()}
     # the accelerations come back into pinned host arrays the caller keeps
-    houts = [torch.empty(n, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
-    mixed.solve_active_set(hx, hy, hz, hm, out=houts)  # warm
+    houts = [pinned(np.zeros(n)) for _ in range(3)]
+    mixed.solve_active_set(h["x"], h["y"], h["z"], h["m"], out=houts)  # warm
     e2e_steps = max(1, min(args.steps, 3))
+    d_f, k1_f, k2_f, g1_f, g2_f = factors
     torch.cuda.synchronize()
     w0 = time.perf_counter()
     for _ in range(e2e_steps):
-        mixed.solve_active_set(hx, hy, hz, hm, out=houts)
+        mixed.kick(h["vx"], h["vy"], h["vz"], houts[0], houts[1], houts[2], k1_f, g1_f)
+        mixed.drift(h["x"], h["y"], h["z"], h["vx"], h["vy"], h["vz"], d_f)
+        mixed.solve_active_set(h["x"], h["y"], h["z"], h["m"], out=houts)
+        mixed.kick(h["vx"], h["vy"], h["vz"], houts[0], houts[1], houts[2], k2_f, g2_f)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - w0
     e2e_value = n * e2e_steps * world / max_over_ranks(torch, dist, e2e_s, dev)
+    del h, houts
 
     # roofline of the dominant kernel (residual walk, FP32 pipes)
     peak = ct.probe_fp32_peak_tflops(local)
@@ -417,14 +498,10 @@ def run_gpu(args) -> int:
             "vs_baseline": None,
             "dtype": "f32 pair/mesh arithmetic, f64 positions/decisions/COM",
             "data": "synthetic (seeded NFW halos + Zel'dovich lattice)",
-            "config": {"workload": f"{args.workload}: N={n}, L={w['box']} Mpc/h, mesh {w['mesh']}^3, "
-                                   f"r_s=1.25 cells, r_cut=6.25 cells, theta={w['theta']}, leaf {w['leaf']}, "
-                                   f"CIC+deconvolution, eps={w['eps']}",
-                       "particles": n, "l2": "inputs larger than L2 (positions 400 MB)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "config": bench_config(args, w, n, world),
             "accuracy_vs_fp64_gpu": {"median_rel": float(np.median(err)),
                                      "p99_rel": float(np.percentile(err, 99)),
-                                     "max_rel": float(np.max(err))},
+                                     "max_rel": float(np.max(err)), "error_map": err_map},
             "fp64_gpu": {"value": fp64_value, "unit": UNIT, "steps": max(1, args.fp64_steps),
                          "speedup_mixed_over_fp64": value / world / fp64_value},
             "phases_ms": {k: st[k] for k in ("pm_ms", "tree_build_ms", "walk_ms", "total_ms")},
@@ -442,13 +519,27 @@ def run_gpu(args) -> int:
                                               "visit": FLOPS_PER_VISIT},
                          "traffic": WALK_DRAM_BYTES.get(args.workload),
                          "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 32,
-                    "d2h_bytes_per_step": n * 24, "steps": e2e_steps},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    # kick (v, a in; v out), drift (x, v in; x out), force (x, m in; a out), kick
+                    "h2d_bytes_per_step": n * (48 + 48 + 32 + 48), "d2h_bytes_per_step": n * (24 + 24 + 24 + 24),
+                    "steps": e2e_steps, "step": "one KDK step through the C-ABI with pinned host buffers"},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
         if args.cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(w, x, y, z, m, args)
+            cb, ref, act = cpu_baseline(w, x, y, z, m, args)
+            if cb is not None:
+                result["cpu_baseline"] = cb
+                a_ref = np.stack([ref["ax"], ref["ay"], ref["az"]])
+                result["accuracy_vs_reference"] = {
+                    "targets": int(len(act)),
+                    "sample": "the reference's own TreePM accelerations at the CPU baseline's seeded targets, "
+                              "same initial state and settings",
+                    "mixed_production": error_summary(rel_errors(a_mixed[:, act], a_ref)),
+                    "fp64_gpu": error_summary(rel_errors(a_fp64[:, act], a_ref)),
+                    "reference_vs_fp64_gpu_max_abs_over_max": float(
+                        np.abs(a_fp64[:, act] - a_ref).max() / np.abs(a_ref).max())}
+        result["accuracy_vs_ewald"] = ewald_accuracy(ct, local)
         print(json.dumps(result), flush=True)
     if dist is not None:
         dist.barrier()
@@ -551,35 +642,49 @@ def run_sharded(args) -> int:
     return 0
 
 
-def cpu_baseline(w, x, y, z, m, args) -> dict | None:
+def cpu_baseline(w, x, y, z, m, args, warmup: int = 1, steps: int = 1):
     """The reference's own TreePM (oracle/_ref/treepm_ref, built from its
-    sources) on the host cores: full PM + tree build, residual walk on a seeded
-    1/64 target subset scaled to all N targets."""
+    sources) on the host cores, all in one process: full PM + tree build, and
+    the residual walk on a seeded 1/64 target subset whose traversal time is
+    scaled to all N targets. The process's first solve and the next
+    warmup - 1 are warm-up; the value is the median of the estimates of the
+    following `steps` solves. Returns (summary, reference result, targets),
+    or (None, None, None) without the reference build."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refio
     if not refio.available():
-        return None
+        return None, None, None
     n = len(x)
     frac = args.cpu_fraction
     rng = np.random.default_rng(7)
     k = max(1, int(n * frac))
     act = np.sort(rng.choice(n, k, replace=False)).astype(np.uint32)
+    warmup = max(1, warmup)
     p = refio.RefProblem(x, y, z, m, box=(w["box"],) * 3, mesh=(w["mesh"],) * 3, theta=w["theta"], leaf=w["leaf"],
-                         eps=w["eps"], deconv=1, active=act, dump_tree=0)
+                         eps=w["eps"], deconv=1, active=act, dump_tree=0, repeats=warmup - 1 + steps)
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
     r = refio.run(p, threads=cores)
     wall = time.perf_counter() - t0
-    total = r["first_ms"]
-    fixed = r["pm_ms"] + r["build_ms"]
-    walk = max(total - fixed, 0.0)
-    est_ms = fixed + walk * (n / k)
-    return {"value": n / (est_ms * 1e-3), "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"full PM ({w['mesh']}^3, FFT via the repo's FFTW-API shim) + full tree build, "
-                      f"walk on {k} seeded targets ({frac:.4f} of N) scaled by N/{k}",
-            "phases_ms": {"pm": r["pm_ms"], "tree_build": r["build_ms"], "walk_sample": walk,
-                          "walk_scaled": walk * n / k},
-            "process_wall_s": wall}
+    ph = r["repeat_phases_ms"][warmup - 1:]
+    tot = r["repeat_ms"][warmup - 1:]
+    # per solve: everything as measured, except the traversal (per target),
+    # which is scaled from the k sampled targets to all n
+    est = [float(t - trav + trav * n / k) for t, (pm, build, trav) in zip(tot, ph)]
+    est_ms = statistics.median(est)
+    i = est.index(sorted(est)[len(est) // 2]) if len(est) % 2 else 0
+    pm, build, trav = (float(v) for v in ph[i])
+    summary = {"value": n / (est_ms * 1e-3), "unit": UNIT, "cores": cores, "kind": "reference",
+               "cpu_model": refio.host_cpu(), "build": f"g++ -O3 -fopenmp -march={refio.build_arch()}",
+               "warmup": warmup, "steps": steps, "solve_ms_estimates": est,
+               "sample": f"one process: {warmup} warm-up + {steps} timed full solves (PM {w['mesh']}^3 with the "
+                         f"FFT of the repository's FFTW-API shim, full tree build), residual walk on {k} seeded "
+                         f"targets ({frac:.4f} of N) with its traversal time scaled by N/{k}; median of the timed "
+                         f"solves",
+               "phases_ms": {"pm": pm, "tree_build": build, "walk_sample": trav, "walk_scaled": trav * n / k,
+                             "rest": float(tot[i]) - pm - build - trav},
+               "process_wall_s": wall}
+    return summary, r, act
 
 
 def run_profile(args) -> int:
@@ -621,6 +726,11 @@ def run_profile(args) -> int:
 
 
 def run_reference(args) -> int:
+    """The reference arm: the reference's CPU TreePM (cpu_baseline) on the
+    same workload, one warm-up and a median over timed solves in one process.
+    At 256^3 a full solve takes ~20 s on 16 host cores (the tree build and PM
+    alone are most of it), so the arm times at most 3 solves after 1 warm-up
+    whatever --steps/--warmup ask, to end within a few minutes."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -633,19 +743,16 @@ def run_reference(args) -> int:
         return 0
     x, y, z, m, vx, vy, vz = make_particles(w, seed=42)
     n = len(x)
-    values = []
-    cb = None
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(w, x, y, z, m, args)
-        if i >= args.warmup:
-            values.append(cb["value"])
-    value = statistics.median(values)
-    cb["value"] = value
+    big = args.workload in ("clustered256", "clustered512")
+    steps = min(args.steps, 3) if big else args.steps
+    warmup = min(max(args.warmup, 1), 1) if big else max(args.warmup, 1)
+    cb, _, _ = cpu_baseline(w, x, y, z, m, args, warmup=warmup, steps=steps)
+    value = cb["value"]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "steps": steps, "warmup": warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded NFW halos + Zel'dovich lattice)",
-        "config": {"workload": args.workload, "particles": n},
+        "config": bench_config(args, w, n, 1),
         "cpu_baseline": cb,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -762,8 +869,6 @@ def main() -> int:
             args.workload = "clustered512"
         return run_large(args)
     if args.impl == "reference":
-        args.steps = min(args.steps, 1) if args.workload == "clustered256" else args.steps
-        args.warmup = 0 if args.workload == "clustered256" else args.warmup
         return run_reference(args)
     if args.shard:
         return run_sharded(args)

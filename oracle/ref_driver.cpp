@@ -251,12 +251,15 @@ int main(int argc, char** argv) {
     coordinator.solveActiveSet(p.x, p.y, p.z, p.m, acc, options, &profile, &diagnostics);
     const double first_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 
-    std::vector<double> times;
+    std::vector<double> times, rep_phases;  // rep_phases: {pm, tree build, traversal} ms per repeat
     for (std::int64_t rep = 0; rep < p.repeats; ++rep) {
       cg::TreePmProfileEvent prof{};
       const auto t1 = std::chrono::steady_clock::now();
       coordinator.solveActiveSet(p.x, p.y, p.z, p.m, acc, options, &prof, nullptr);
       times.push_back(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count());
+      rep_phases.push_back(prof.pm_profile.total_ms);
+      rep_phases.push_back(prof.tree_profile.full_rebuild_ms);
+      rep_phases.push_back(prof.tree_profile.traversal_ms);
     }
 
     FILE* f = std::fopen(argv[2], "wb");
@@ -383,6 +386,10 @@ int main(int argc, char** argv) {
       for (std::size_t k = 0; k < nt; ++k) { ex[k] = e[k].x; ey[k] = e[k].y; ez[k] = e[k].z; }
       w.vec(ex); w.vec(ey); w.vec(ez);
     }
+    // per-repeat phase times (trailing block, read when present)
+    std::fwrite("CHUIREP1", 1, 8, f);
+    w.put<std::int64_t>(static_cast<std::int64_t>(times.size()));
+    w.vec(rep_phases);
     std::fclose(f);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "treepm_ref error: %s\n", e.what());

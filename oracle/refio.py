@@ -16,7 +16,42 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_BINARY = os.path.join(HERE, "_ref", "treepm_ref")
+REF_BINARY = os.path.join(HERE, "_ref", "treepm_ref")          # x86-64-v3 (AVX2)
+REF_BINARY_V4 = os.path.join(HERE, "_ref", "v4", "treepm_ref")  # x86-64-v4 (AVX-512)
+_V4_FLAGS = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
+
+
+def _cpuinfo() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            return f.read()
+    except OSError:
+        return ""
+
+
+def host_cpu() -> str:
+    """The host CPU's model name (first processor entry)."""
+    for line in _cpuinfo().splitlines():
+        if line.startswith("model name"):
+            return line.split(":", 1)[1].strip()
+    return "unknown"
+
+
+def binary() -> str:
+    """The reference build for this host: the AVX-512 one where the CPU has
+    AVX-512 and it was built, else the AVX2 one."""
+    flags = set()
+    for line in _cpuinfo().splitlines():
+        if line.startswith("flags"):
+            flags = set(line.split(":", 1)[1].split())
+            break
+    if all(f in flags for f in _V4_FLAGS) and os.access(REF_BINARY_V4, os.X_OK):
+        return REF_BINARY_V4
+    return REF_BINARY
+
+
+def build_arch() -> str:
+    return "x86-64-v4" if binary() == REF_BINARY_V4 else "x86-64-v3"
 
 
 @dataclass
@@ -162,6 +197,11 @@ def read_result(path: str) -> dict:
         nt = min(ew, na)
         for k in ("ewald_ax", "ewald_ay", "ewald_az"):
             r[k] = b.arr(np.float64, nt)
+    if b.d[b.o:b.o + 8] == b"CHUIREP1":
+        b.o += 8
+        reps = b.q()
+        # per repeat: PM, tree build and traversal milliseconds
+        r["repeat_phases_ms"] = b.arr(np.float64, 3 * reps).reshape(reps, 3)
     return r
 
 
@@ -180,5 +220,5 @@ def run(p: RefProblem, threads: int | None = None, timeout: float | None = None)
         fin = os.path.join(td, "in.bin")
         fout = os.path.join(td, "out.bin")
         write_problem(fin, p)
-        subprocess.run([REF_BINARY, fin, fout], check=True, env=env, timeout=timeout)
+        subprocess.run([binary(), fin, fout], check=True, env=env, timeout=timeout)
         return read_result(fout)

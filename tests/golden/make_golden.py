@@ -190,6 +190,24 @@ def main():
                          active=active, boundary=1)
     save("isolated_tsc_active", p, refio.run(p))
 
+    # 8. the headline configuration's settings on a clustered periodic box of
+    #    40^3 = 64000 particles at the 256^3 case's mean spacing (L = 31.25):
+    #    50 % in 8 NFW halos over 3 decades, CIC with window deconvolution,
+    #    theta 0.6, leaf 16, eps 0.001, mesh 40^3, r_s = 1.25 cells; Ewald
+    #    sums at 16 targets
+    x, y, z, *_ = ics.clustered_box(40 ** 3, 31.25, 0.5, 8, 3.0, 0.5, 81)
+    m = np.full(len(x), 1.0 / len(x))
+    p = refio.RefProblem(x, y, z, m, box=(31.25,) * 3, mesh=(40,) * 3, theta=0.6, leaf=16, eps=0.001,
+                         scheme=0, deconv=1, dump_density=1, ewald=16)
+    save("clustered64k_cic", p, refio.run(p))
+    #    the large configuration's tree: theta 0.7, leaf 32, 60 % in 8 halos
+    #    over 4 decades, same box, mesh and scheme
+    x, y, z, *_ = ics.clustered_box(40 ** 3, 31.25, 0.6, 8, 4.0, 0.5, 82)
+    m = np.full(len(x), 1.0 / len(x))
+    p = refio.RefProblem(x, y, z, m, box=(31.25,) * 3, mesh=(40,) * 3, theta=0.7, leaf=32, eps=0.001,
+                         scheme=0, deconv=1)
+    save("clustered64k_t07_leaf32", p, refio.run(p))
+
 
 if __name__ == "__main__":
     main()

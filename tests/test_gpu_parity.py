@@ -19,7 +19,11 @@ from conftest import golden_params, load_golden  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["lattice16_cic", "clustered_tsc", "rect_active", "two_body", "quasi24", "duplicates", "config32"]
+# clustered64k_*: the headline settings (CIC with window deconvolution, theta
+# 0.6, leaf 16) and the large configuration's tree (theta 0.7, leaf 32) on a
+# clustered periodic box of 64000 particles
+CASES = ["lattice16_cic", "clustered_tsc", "rect_active", "two_body", "quasi24", "duplicates", "config32",
+         "clustered64k_cic", "clustered64k_t07_leaf32"]
 COUNTER_KEYS = ("visited_nodes", "accepted_nodes", "opened_nodes", "direct_pair_evaluations",
                 "cutoff_pruned_nodes", "cutoff_skipped_pairs", "accepted_internal_multipoles", "accepted_leaves")
 

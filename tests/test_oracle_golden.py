@@ -14,7 +14,7 @@ from conftest import golden_params, load_golden
 
 CASES = ["lattice16_cic", "clustered_tsc", "rect_active", "two_body", "quasi24", "duplicates", "config32",
          "adaptive_monopole", "adaptive_residual", "group_walk", "group_walk_active", "isolated_cic",
-         "isolated_tsc_active"]
+         "isolated_tsc_active", "clustered64k_cic", "clustered64k_t07_leaf32"]
 COUNTER_KEYS = ("visited", "accepted", "opened", "pairs", "pruned", "pair_skips", "multipoles", "leaves")
 
 
