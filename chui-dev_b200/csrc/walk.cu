@@ -1031,11 +1031,19 @@ __device__ __forceinline__ int certainLess(float a, float b, float err = 0.f) {
 // kUniform (production, contiguous targets, one source mass): queue entries
 // carry the lane mask in place of the mass, so each entry is one 16-byte load
 // and the mass multiplies the flush's partial sums once.
+//
+// kF64 (strict policy, no diagnostics): the same traversal, decisions and
+// subtree blocks with every pair in FP64 -- queue entries are FP64 offsets
+// formed from the tree-frame FP64 positions, pairs take the reference's
+// formulas (erf/exp residual, or its Gaussian table) and accepted multipoles
+// the FP64 screened quadrupole. This is the production solver in FP64, the
+// comparator for the mixed-precision speed-up.
 template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode, bool kUniform = false,
-          bool kCost = false>
+          bool kCost = false, bool kF64 = false>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUniform) ? CHUI_WALK_MIN_BLOCKS_STRICT
                                                                                   : CHUI_WALK_MIN_BLOCKS)
     walkFastKernel(WalkArgs a) {
+  static_assert(!kF64 || (kMode <= 1 && !kDiag && !kUniform), "FP64 production walk: strict policy only");
   constexpr bool kAdaptive = kMode >= 2;
   constexpr bool kGroup = kMode == 3;
   constexpr bool kHistory = kMode != 0;
@@ -1051,14 +1059,18 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
   // pair p is q_src[2p] = {x0, x1, y0, y1}, q_src[2p+1] = {z0, z1, w0, w1}
   // (w: mass, or the lane mask under kUniform), and q_meta[p] = {mask0,
   // mask1, tree position 0, tree position 1} when masses travel separately.
-  __shared__ float4 q_src[kWalkWarpsPerBlock][kQueueLen];
-  __shared__ uint4 q_meta[kWalkWarpsPerBlock][kQueueLen / 2];
+  __shared__ float4 q_src[kWalkWarpsPerBlock][kF64 ? 2 : kQueueLen];
+  __shared__ uint4 q_meta[kWalkWarpsPerBlock][kF64 ? 1 : kQueueLen / 2];
+  // kF64: FP64 offsets + mass, and {lane mask, tree position}
+  constexpr int kQ64 = kF64 ? kQueueLen / 2 : 1;
+  __shared__ double4 q64[kWalkWarpsPerBlock][kQ64];
+  __shared__ uint2 q64m[kWalkWarpsPerBlock][kQ64];
   __shared__ float4 m_list[kWalkWarpsPerBlock][kList][32];
   __shared__ double4 exact_sm[kWalkWarpsPerBlock][32];
   // per-lane FP64 target position and accumulators, kept in shared memory
   // rather than registers: they are touched once per flush or exact decision,
   // and the registers they would hold buy the pair loop occupancy and ILP
-  __shared__ double lane_sm[6][kWalkWarpsPerBlock][32];
+  __shared__ double lane_sm[kF64 ? 9 : 6][kWalkWarpsPerBlock][32];
   // group walk: each deciding lane's group box {centre, half, a_min}, read at
   // every node visit (components outermost: no bank conflicts)
   __shared__ double gbox_sm[kGroup ? 7 : 1][kWalkWarpsPerBlock][32];
@@ -1127,6 +1139,13 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
       rg2 = fmax(rg2, __shfl_xor_sync(0xffffffffu, rg2, off));
     }
     const float tfx = static_cast<float>(ox), tfy = static_cast<float>(oy), tfz = static_cast<float>(oz);
+    if constexpr (kF64) {
+      lane_sm[6][warp][lane] = ox;
+      lane_sm[7][warp][lane] = oy;
+      lane_sm[8][warp][lane] = oz;
+    }
+    // FP64 cull radius of the queue (kF64): r_cut + the warp's target spread
+    const double cull2d = kF64 ? (w.cutoff + sqrt(rg2)) * (w.cutoff + sqrt(rg2)) * (1.0 + 1.0e-12) : 0.0;
     const float cull = static_cast<float>(w.cutoff + sqrt(rg2));
     const float cull2 = cull * cull * 1.0001f;
     const float rga_f = static_cast<float>(rga);
@@ -1187,7 +1206,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
     // Pair loop over the queue, two sources per step in packed FP32 (f32x2
     // FMA/ADD/MUL: one instruction serves both sources of a pair); lane
     // masks, cutoff tests and rsqrt stay per source.
-    auto flush = [&]() {
+    auto flush32 = [&]() {
       if (qn & 1) {
         // pad to whole pairs with an entry no lane takes (mask 0, mass 0)
         if (lane == 0) {
@@ -1262,6 +1281,36 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
       __syncwarp();
     };
 
+    // kF64: every queued source in FP64 with the reference's pair formula.
+    auto flush64 = [&]() {
+      const double tx = lane_sm[6][warp][lane], ty = lane_sm[7][warp][lane], tz = lane_sm[8][warp][lane];
+      double fx = 0.0, fy = 0.0, fz = 0.0;
+      for (int k = 0; k < qn; ++k) {
+        const double4 e = q64[warp][k];
+        const uint2 meta = q64m[warp][k];
+        const double dx = e.x - tx, dy = e.y - ty, dz = e.z - tz;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const bool mine = (meta.x & lane_bit) != 0u && (kContiguous || meta.y != self_pos);
+        const bool in = mine && r2 <= w.cutoff2 && (!kEpsZero || r2 > 0.0);
+        if (in) {
+          const double kr = w.gauss_lookup ? gaussResidualInvR3(a, r2, w.eps) : residualInvR3(r2, w.eps, w.rs);
+          const double f = kr * e.w;
+          fx += f * dx;
+          fy += f * dy;
+          fz += f * dz;
+        }
+      }
+      acc_x += w.G * fx;
+      acc_y += w.G * fy;
+      acc_z += w.G * fz;
+      qn = 0;
+      __syncwarp();
+    };
+    auto flush = [&]() {
+      if constexpr (kF64) flush64();
+      else flush32();
+    };
+
     // Accepted multipoles wait in a per-lane list and are evaluated together:
     // the lanes step through their own lists in lockstep, so a warp pays for
     // the longest list rather than for every node some lane accepted.
@@ -1288,6 +1337,34 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
     // way the offset is formed in FP64 and rounded once.
     auto enqueue = [&](uint32_t begin, uint32_t count, uint32_t mask, bool whole, const double4& g, double cdx,
                        double cdy, double cdz) {
+      if constexpr (kF64) {
+        for (uint32_t chunk = 0; chunk < count; chunk += 32) {
+          const uint32_t k = chunk + lane;
+          double4 e = make_double4(0.0, 0.0, 0.0, 0.0);
+          bool keep = false;
+          if (k < count) {
+            const double4 u = a.src_u4[begin + k];
+            e = make_double4((u.x - g.x) + cdx, (u.y - g.y) + cdy, (u.z - g.z) + cdz, u.w);
+            keep = e.x * e.x + e.y * e.y + e.z * e.z <= cull2d;
+          }
+          const uint32_t keep_mask = __ballot_sync(0xffffffffu, keep);
+          const int c = __popc(keep_mask);
+          if (qn + c > kQ64) flush();
+          if (keep) {
+            const int slot_q = qn + __popc(keep_mask & (lane_bit - 1u));
+            uint32_t m = mask;
+            if constexpr (kContiguous) {
+              const uint32_t rel = begin + k - base;
+              if (rel < 32u) m &= ~(1u << rel);
+            }
+            q64[warp][slot_q] = e;
+            q64m[warp][slot_q] = make_uint2(m, begin + k);
+          }
+          __syncwarp();
+          qn += c;
+        }
+        return;
+      }
       for (uint32_t chunk = 0; chunk < count; chunk += 32) {
         const uint32_t k = chunk + lane;
         float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1534,7 +1611,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         }
       }
       if (do_accept && !com_skip) {
-        if (a.mult_f32 && fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc)) >= fmaxf(1.0e-8f * cut2, 1.0e-10f)) {
+        if (!kF64 && a.mult_f32 && fmaf(dxc, dxc, fmaf(dyc, dyc, dzc * dzc)) >= fmaxf(1.0e-8f * cut2, 1.0e-10f)) {
           if constexpr (kAdaptive) {
             m_list[warp][mn][lane] = make_float4(dxc, dyc, dzc, __uint_as_float(node));
             ++mn;
@@ -2118,6 +2195,22 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     CHUI_WALK_DISPATCH(false, kPolyMaxTerms)
 #undef CHUI_WALK_DISPATCH
 #undef CHUI_WALK_DISPATCH2
+  }
+  if (!mixed && c.cfg.diagnostics == 0 && wp.policy == CHUI_TREEPM_POLICY_STRICT && !wp.group_walk &&
+      !(wp.criterion == 2 && prev_acc)) {
+    // the production solver in FP64 (same traversal and subtree blocks as the
+    // mixed walk, FP64 pairs and multipoles)
+    const bool contiguous = active == nullptr && tx == nullptr && nt == n;
+#define CHUI_WALK64(EPS, CONT, COST) walkFastKernel<EPS, kPairPolyTerms, false, CONT, 0, false, COST, true>
+    if (contiguous) {
+      if (a.chunk_cost) return eps_zero ? launchPersistent(CHUI_WALK64(true, true, true), a, s)
+                                        : launchPersistent(CHUI_WALK64(false, true, true), a, s);
+      return eps_zero ? launchPersistent(CHUI_WALK64(true, true, false), a, s)
+                      : launchPersistent(CHUI_WALK64(false, true, false), a, s);
+    }
+    return eps_zero ? launchPersistent(CHUI_WALK64(true, false, false), a, s)
+                    : launchPersistent(CHUI_WALK64(false, false, false), a, s);
+#undef CHUI_WALK64
   }
   if (wp.group_walk) {
     uint32_t n_groups = 0;

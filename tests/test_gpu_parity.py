@@ -254,3 +254,27 @@ def test_uniform_mass_lane_matches_explicit_masses(cuda_ok):
         b = s.solve_active_set(g["x"], g["y"], g["z"], None, uniform_mass=float(g["m"][0]))
     for k in ("ax", "ay", "az"):
         np.testing.assert_allclose(a[k], b[k], rtol=1e-5, atol=1e-6 * np.abs(a[k]).max())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_production_matches_reference(cuda_ok, name):
+    """The production solver in FP64 (diagnostics off: the mixed walk's
+    traversal and subtree blocks with FP64 pairs and multipoles). Subtree
+    blocks sum as pairs what the reference may accept as a strict multipole,
+    so it equals the reference to FP64 round-off where no multipole is
+    accepted and otherwise within the quadrupole truncation error."""
+    g = load_golden(name)
+    act = _active(g)
+    cfg = cfg_for(g, ct._abi.FP64)
+    cfg.diagnostics = 0
+    with ct.TreePmCoordinator(cfg) as s:
+        r = s.solve_active_set(g["x"], g["y"], g["z"], g["m"], active=act)
+    e = rel_err([r["ax"], r["ay"], r["az"]], [g["ax"], g["ay"], g["az"]])
+    print(f"{name}: FP64 production vs reference median {np.median(e):.2e} p99 {np.percentile(e, 99):.2e} "
+          f"max {e.max():.2e}")
+    if int(g["counters"][6]) == 0:  # no accepted multipoles
+        scale = np.abs(np.concatenate([g["ax"], g["ay"], g["az"]])).max()
+        for k in ("ax", "ay", "az"):
+            assert np.abs(r[k] - g[k]).max() <= 1e-9 * scale, k
+    assert np.median(e) <= 1e-8, np.median(e)
+    assert np.percentile(e, 99) <= 1e-5, np.percentile(e, 99)
