@@ -86,7 +86,7 @@ class TreePmConfig:
     acceptance_policy: int = _abi.POLICY_STRICT
     precision: int = _abi.MIXED
     device: int = 0
-    diagnostics: int = 1
+    diagnostics: int = 0
     adaptive_error_estimator: int = _abi.ESTIMATOR_RESIDUAL_DERIVATIVE
     cutoff_node_policy: int = _abi.CUTOFF_CONTAIN_NODE
     adaptive_maximum_opening_angle: float = 0.25

@@ -441,6 +441,11 @@ int validateConfig(const chui_treepm_config& cfg, std::string& err) {
       return CHUI_TREEPM_EINVAL;
     }
   }
+  if (cfg.diagnostics < 0 || cfg.diagnostics > 2) {
+    err = "diagnostics must be 0 (production walk), 1 (the reference's per-node walk and counters) or 2 "
+          "(production walk with its own counters and the nearest-pair lane)";
+    return CHUI_TREEPM_EINVAL;
+  }
   if (cfg.acceptance_policy != CHUI_TREEPM_POLICY_STRICT && cfg.acceptance_policy != CHUI_TREEPM_POLICY_ADAPTIVE) {
     err = "TreePM acceptance policy is invalid";
     return CHUI_TREEPM_EINVAL;
@@ -579,7 +584,7 @@ int chui_treepm_config_default(chui_treepm_config* cfg) {
   cfg->acceptance_policy = CHUI_TREEPM_POLICY_STRICT;            // tree_pm_coupling.hpp:247
   cfg->precision = CHUI_TREEPM_MIXED;
   cfg->device = 0;
-  cfg->diagnostics = 1;
+  cfg->diagnostics = 0;  // the production walk
   cfg->adaptive_error_estimator = CHUI_TREEPM_ESTIMATOR_RESIDUAL_DERIVATIVE;  // tree_pm_coupling.hpp:249
   cfg->cutoff_node_policy = CHUI_TREEPM_CUTOFF_CONTAIN_NODE;                  // tree_pm_coupling.hpp:250
   cfg->adaptive_maximum_opening_angle = 0.25;                                 // tree_pm_coupling.hpp:248
@@ -874,6 +879,9 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
   wp.eps2_f = static_cast<float>(c.cfg.softening * c.cfg.softening);
   wp.G_f = static_cast<float>(c.cfg.gravitational_constant);
   cudaMemsetAsync(c.status.ptr, 0, 4, s);
+  // the production walk also counts and records nearest pairs when asked to,
+  // or when the caller wants the nearest-pair lane
+  c.walk_instrument = c.cfg.diagnostics == 2 || acc->nearest_pair_r2 != nullptr;
   if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, prev, wp, n, s, visit_begin, visit_end,
                                      ranged)))
     return chui::fail(c, rc, rc == CHUI_TREEPM_ENOTSUP

@@ -141,6 +141,9 @@ struct Context {
   DevBuf work_counter;   // u32 dynamic scheduling
   DevBuf tree_acc;       // double3 per active slot (short-range part)
   DevBuf tree_near;      // double per active slot
+  // the production walk counts its traversal and pairs and records the
+  // nearest-pair r^2 (diagnostics 2, or a nearest-pair lane requested)
+  bool walk_instrument = false;
 
   cudaEvent_t ev[8] = {};
   bool events_ready = false;

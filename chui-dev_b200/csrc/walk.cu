@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "context.cuh"
@@ -101,6 +102,11 @@ struct WalkArgs {
   float2 pk2[kPolyMaxTerms];
   float2 sc2, soff2, eps2_2;
   float cut2e;
+  // diagnostics 2 (or a requested nearest-pair lane): the counting instances
+  // walk with subtree blocks (the production traversal) -- blocks -- and the
+  // FP64 production walk counts and records nearest pairs -- instrument
+  int blocks;
+  int instrument;
   WalkParams wp;
 };
 
@@ -959,7 +965,7 @@ __device__ __forceinline__ ExactDecision exactNodeDecision(const WalkArgs& a, ui
 // per-pair source metric): used where the shared FP32 frame cannot serve.
 __device__ __forceinline__ void exactLeafPairs(const WalkArgs& a, double4* stage, uint32_t begin, uint32_t count,
                                             bool want, double px, double py, double pz, uint32_t self_pos,
-                                            double& ax, double& ay, double& az, float& nearest,
+                                            double& ax, double& ay, double& az, double& nearest,
                                             unsigned long long& pairs, unsigned long long& skips) {
   const WalkParams& w = a.wp;
   const int lane = threadIdx.x & 31;
@@ -981,7 +987,7 @@ __device__ __forceinline__ void exactLeafPairs(const WalkArgs& a, double4* stage
           ++skips;
           continue;
         }
-        nearest = fminf(nearest, static_cast<float>(r2));
+        nearest = fmin(nearest, r2);
         ++pairs;
         if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
         const double f = residualInvR3(r2, w.eps, w.rs) * w.G;
@@ -1044,6 +1050,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
                                                                                   : CHUI_WALK_MIN_BLOCKS)
     walkFastKernel(WalkArgs a) {
   static_assert(!kF64 || (kMode <= 1 && !kDiag && !kUniform), "FP64 production walk: strict policy only");
+  // counters and the nearest-pair lane: the counting instances (kDiag), and
+  // the FP64 production walk on request
+  const bool inst = kDiag || (kF64 && a.instrument != 0);
   constexpr bool kAdaptive = kMode >= 2;
   constexpr bool kGroup = kMode == 3;
   constexpr bool kHistory = kMode != 0;
@@ -1195,6 +1204,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
     acc_y = 0.0;
     acc_z = 0.0;
     float nearest_f = INFINITY;
+    double nearest_d = INFINITY;  // FP64 pairs (exact leaf pairs, the FP64 production walk)
     uint32_t skip_until = 0;
     int qn = 0;  // warp's source queue length
     int mn = 0;  // this lane's multipole list length
@@ -1227,7 +1237,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
       float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;
       uint32_t pairs = 0, skips = 0;
       const int np = (qn + 1) >> 1;
-      auto pairStep = [&](int p, float2& fx, float2& fy, float2& fz) {
+      auto pairStep = [&](auto count_tag, int p, float2& fx, float2& fy, float2& fz) {
+        constexpr bool kCount = decltype(count_tag)::value;
         const float4 A = q_src[warp][2 * p];
         const float4 B = q_src[warp][2 * p + 1];
         const float2 dx = __fadd2_rn(make_float2(A.x, A.y), ntx);
@@ -1251,7 +1262,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         }
         const bool in0 = mine0 && r2.x <= cut_t;
         const bool in1 = mine1 && r2.y <= cut_t;
-        if constexpr (kDiag) {
+        if constexpr (kCount) {
           pairs += (in0 ? 1u : 0u) + (in1 ? 1u : 0u);
           // the group walk's pair kernel counts no skipped pairs
           skips += ((mine0 && !in0 && !in_group) ? 1u : 0u) + ((mine1 && !in1 && !in_group) ? 1u : 0u);
@@ -1271,7 +1282,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         fz = __ffma2_rn(f, dz, fz);
       };
 #pragma unroll (kPairUnroll)
-      for (int p = 0; p < np; ++p) pairStep(p, fx, fy, fz);
+      for (int p = 0; p < np; ++p) pairStep(std::integral_constant<bool, kDiag>{}, p, fx, fy, fz);
       acc_x += static_cast<double>(g_pair * (fx.x + fx.y));
       acc_y += static_cast<double>(g_pair * (fy.x + fy.y));
       acc_z += static_cast<double>(g_pair * (fz.x + fz.y));
@@ -1292,6 +1303,11 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         const double r2 = dx * dx + dy * dy + dz * dz;
         const bool mine = (meta.x & lane_bit) != 0u && (kContiguous || meta.y != self_pos);
         const bool in = mine && r2 <= w.cutoff2 && (!kEpsZero || r2 > 0.0);
+        if (inst) {
+          cnt_pairs += in ? 1u : 0u;
+          cnt_skips += (mine && !in) ? 1u : 0u;
+          nearest_d = in ? fmin(nearest_d, r2) : nearest_d;
+        }
         if (in) {
           const double kr = w.gauss_lookup ? gaussResidualInvR3(a, r2, w.eps) : residualInvR3(r2, w.eps, w.rs);
           const double f = kr * e.w;
@@ -1565,7 +1581,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
           dyc = static_cast<float>(ey);
           dzc = static_cast<float>(ez);
         }
-        if (kDiag && com_skip) ++cnt_pruned;
+        if (inst && com_skip) ++cnt_pruned;
       }
       if (act && need_exact) {
         const ExactDecision d = exactNodeDecision<kAdaptive>(a, node, px, py, pz, skip_self, hist);
@@ -1577,7 +1593,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
       }
       // node counters: per lane, or once per group under the group walk
       const bool count_node = !kGroup || !in_group || count_walk;
-      if (kDiag && act && count_node) {
+      if (inst && act && count_node) {
         ++cnt_visited;
         cnt_pruned += prune ? 1 : 0;
       }
@@ -1585,7 +1601,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         const bool want = act && !prune;
         const uint32_t mask = __ballot_sync(0xffffffffu, want);
         if (mask == 0u) continue;
-        if (kDiag && want && count_node) {
+        if (inst && want && count_node) {
           ++cnt_accepted;
           ++cnt_leaves;
         }
@@ -1595,7 +1611,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         } else {
           unsigned long long p = 0, sk = 0;
           exactLeafPairs(a, exact_sm[warp], begin, count, want, px, py, pz, self_pos, acc_x, acc_y, acc_z,
-                         nearest_f, p, sk);
+                         nearest_d, p, sk);
           cnt_pairs += static_cast<uint32_t>(p);
           cnt_skips += static_cast<uint32_t>(sk);
         }
@@ -1605,7 +1621,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
       const bool do_accept = act && !prune && accept;
       const bool open = act && !prune && !accept;
       if (do_accept) {
-        if (kDiag && count_node) {
+        if (inst && count_node) {
           ++cnt_accepted;
           ++cnt_multi;
         }
@@ -1634,10 +1650,10 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         if (__any_sync(0xffffffffu, mn == kList)) mflush();
       }
       if (act && (prune || accept)) skip_until = rg4.w;
-      if (kDiag && open && count_node) ++cnt_opened;
+      if (inst && open && count_node) ++cnt_opened;
       if (__any_sync(0xffffffffu, open)) {
         constexpr uint32_t kBlock = kAdaptive ? kBulkCountAdaptive : kBulkCount;
-        if constexpr (!kDiag && kBlock > 0) {
+        if (kBlock > 0 && (!kDiag || a.blocks)) {
           // Subtree block: the lanes that opened this small node take every
           // source in it within r_cut (per-pair test, as in the leaf path)
           // instead of descending. This is the reference's pair set except
@@ -1671,9 +1687,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
       a.out_x[o] = acc_x;
       a.out_y[o] = acc_y;
       a.out_z[o] = acc_z;
-      a.out_near[o] = kDiag ? static_cast<double>(nearest_f) : INFINITY;
+      a.out_near[o] = inst ? fmin(static_cast<double>(nearest_f), nearest_d) : INFINITY;
     }
-    if constexpr (kDiag) {
+    if (inst) {
       uint32_t c[8] = {cnt_visited, cnt_accepted, cnt_opened, cnt_pairs, cnt_pruned, cnt_skips, cnt_multi, cnt_leaves};
       for (int k = 0; k < 8; ++k) {
         for (int off = 16; off > 0; off >>= 1) c[k] += __shfl_xor_sync(0xffffffffu, c[k], off);
@@ -2145,6 +2161,9 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     a.eps2_2 = make_float2(wp.eps2_f, wp.eps2_f);
     a.cut2e = wp.cut2_f + wp.eps2_f;
   }
+  // diagnostics 2 or a nearest-pair lane: counted walk over the production traversal
+  a.instrument = c.walk_instrument ? 1 : 0;
+  a.blocks = c.cfg.diagnostics != 1 ? 1 : 0;
   a.wp = wp;
   uint32_t* group_count = nullptr;
   if (wp.group_walk) {
@@ -2170,7 +2189,9 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     // full solves visit targets in tree order, so a warp's targets are tree
     // positions base..base+31 and self pairs are excluded by the lane mask
     const bool contiguous = active == nullptr && tx == nullptr && nt == n;
-    const bool diag = c.cfg.diagnostics != 0;
+    // the counting instances: diagnostics 1 (per node) and 2 or a nearest-pair
+    // lane (with subtree blocks: the production traversal)
+    const bool diag = c.cfg.diagnostics == 1 || c.walk_instrument;
     const bool uniform = wp.uniform_mass != 0;
     const int mode = wp.policy == CHUI_TREEPM_POLICY_ADAPTIVE ? (wp.group_walk ? 3 : 2)
                                                                : (wp.criterion == 2 && prev_acc ? 1 : 0);
@@ -2196,7 +2217,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
 #undef CHUI_WALK_DISPATCH
 #undef CHUI_WALK_DISPATCH2
   }
-  if (!mixed && c.cfg.diagnostics == 0 && wp.policy == CHUI_TREEPM_POLICY_STRICT && !wp.group_walk &&
+  if (!mixed && c.cfg.diagnostics != 1 && wp.policy == CHUI_TREEPM_POLICY_STRICT && !wp.group_walk &&
       !(wp.criterion == 2 && prev_acc)) {
     // the production solver in FP64 (same traversal and subtree blocks as the
     // mixed walk, FP64 pairs and multipoles)

@@ -74,8 +74,13 @@ typedef struct {
   int32_t acceptance_policy;                  /* CHUI_TREEPM_POLICY_*: treepm_adaptive_acceptance_enabled */
   int32_t precision;                          /* CHUI_TREEPM_MIXED or CHUI_TREEPM_FP64 */
   int32_t device;                             /* CUDA device ordinal */
-  int32_t diagnostics;                        /* 1: per-pair counters and nearest-pair r^2 (default);
-                                                 0: skipped in the walk (production timing) */
+  int32_t diagnostics;                        /* 0 (default): the production walk (subtree blocks), no
+                                                 counters; it still fills a requested nearest-pair lane.
+                                                 1: the reference's per-node walk, traversal counters
+                                                 equal to the reference's, nearest-pair r^2.
+                                                 2: the production walk with its own counters (its
+                                                 traversal's node visits and in-cutoff pairs) and the
+                                                 nearest-pair lane */
   /* adaptive-relative policy (TreePmOptions, tree_pm_coupling.hpp:243-332) */
   int32_t adaptive_error_estimator;           /* CHUI_TREEPM_ESTIMATOR_*: treepm_adaptive_error_estimator */
   int32_t cutoff_node_policy;                 /* CHUI_TREEPM_CUTOFF_*: treepm_cutoff_node_policy */

@@ -184,7 +184,7 @@ def test_adaptive_clustered_64(cuda_ok, estimator, cutoff_policy, angle, alpha):
     m = np.full(len(x), 1.0 / len(x))
     base = dict(pm_grid_nx=n_side, pm_grid_ny=n_side, pm_grid_nz=n_side, box_x=box, box_y=box, box_z=box,
                 opening_theta=0.5, max_leaf_size=16, softening=0.002)
-    with ct.TreePmCoordinator(ct.TreePmConfig(**base, precision=ct._abi.FP64)) as s:
+    with ct.TreePmCoordinator(ct.TreePmConfig(**base, precision=ct._abi.FP64, diagnostics=1)) as s:
         r0 = s.solve_active_set(x, y, z, m)
     prev = np.sqrt(r0["ax"] ** 2 + r0["ay"] ** 2 + r0["az"] ** 2)
     adaptive = dict(acceptance_policy=ct._abi.POLICY_ADAPTIVE, adaptive_error_estimator=estimator,
@@ -224,7 +224,7 @@ def test_group_walk_clustered_64(cuda_ok, cutoff_policy):
     m = np.full(len(x), 1.0 / len(x))
     base = dict(pm_grid_nx=n_side, pm_grid_ny=n_side, pm_grid_nz=n_side, box_x=box, box_y=box, box_z=box,
                 opening_theta=0.5, max_leaf_size=16, softening=0.002)
-    with ct.TreePmCoordinator(ct.TreePmConfig(**base, precision=ct._abi.FP64)) as s:
+    with ct.TreePmCoordinator(ct.TreePmConfig(**base, precision=ct._abi.FP64, diagnostics=1)) as s:
         r0 = s.solve_active_set(x, y, z, m)
     prev = np.sqrt(r0["ax"] ** 2 + r0["ay"] ** 2 + r0["az"] ** 2)
     prev[::97] = np.nan  # some groups fall back to per-target walks

@@ -36,7 +36,7 @@ def cfg_for(g, precision):
                            box_y=float(g["box"][1]), box_z=float(g["box"][2]), asmth_cells=asmth, rcut_cells=rcut,
                            opening_theta=theta, opening_criterion=criterion, multipole_order=order,
                            max_leaf_size=leaf, assignment_scheme=scheme, window_deconvolution=deconv,
-                           gravitational_constant=gconst, softening=eps, precision=precision)
+                           gravitational_constant=gconst, softening=eps, precision=precision, diagnostics=1)
 
 
 def _active(g):
@@ -278,3 +278,42 @@ def test_fp64_production_matches_reference(cuda_ok, name):
             assert np.abs(r[k] - g[k]).max() <= 1e-9 * scale, k
     assert np.median(e) <= 1e-8, np.median(e)
     assert np.percentile(e, 99) <= 1e-5, np.percentile(e, 99)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("precision", [ct._abi.MIXED, ct._abi.FP64])
+def test_production_walk_nearest_pair_and_counters(cuda_ok, name, precision):
+    """The production walk (diagnostics 0) fills a requested nearest-pair lane
+    and, with diagnostics 2, reports its own traversal counters. Its pairs are
+    every source inside r_cut of the target (subtree blocks also sum what the
+    reference accepts as far multipoles), a superset of the reference's
+    direct pairs: the nearest pair is the reference's, or nearer."""
+    g = load_golden(name)
+    act = _active(g)
+    rows = act if act is not None else np.arange(len(g["x"]))
+    near_ref = g["nearest_r2"][rows]
+    for diagnostics in (0, 2):
+        cfg = cfg_for(g, precision)
+        cfg.diagnostics = diagnostics
+        with ct.TreePmCoordinator(cfg) as s:
+            r = s.solve_active_set(g["x"], g["y"], g["z"], g["m"], active=act, nearest_pair=True)
+        near = r["nearest_r2"][rows]
+        fin = np.isfinite(near_ref)
+        assert np.isfinite(near[fin]).all()
+        # mixed: r^2 from FP32 offsets in the warp's frame (absolute error
+        # ~1e-7 of the frame's extent), so the closest pairs carry up to
+        # ~1e-4 relative error; the lane feeds a timestep criterion
+        # (FP64: offsets formed in the warp's frame, ~1e-16 of its extent)
+        tol = 1e-3 if precision == ct._abi.MIXED else 1e-9
+        assert (near[fin] <= near_ref[fin] * (1 + tol) + 1e-30).all()
+        same = np.abs(near[fin] - near_ref[fin]) <= tol * near_ref[fin] + 1e-30
+        assert same.mean() >= 0.99, same.mean()
+        st = r["stats"]
+        if diagnostics == 2:
+            ref = dict(zip(COUNTER_KEYS, (int(v) for v in g["counters"])))
+            assert st["direct_pair_evaluations"] >= 0.99 * ref["direct_pair_evaluations"]
+            assert st["visited_nodes"] > 0  # (small trees may be one subtree block: no accepted nodes)
+    # the lane comes back without being asked for a counted walk, and the
+    # forces are the production walk's
+    e = rel_err([r["ax"], r["ay"], r["az"]], [g["ax"], g["ay"], g["az"]])
+    assert np.median(e) <= 1e-4 and np.percentile(e, 99) <= 1e-3
