@@ -62,7 +62,7 @@ U32P = C.POINTER(C.c_uint32)
 
 class Sources(C.Structure):
     _fields_ = [("count", C.c_int64), ("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p),
-                ("mass", C.c_void_p), ("uniform_mass", C.c_double)]
+                ("mass", C.c_void_p), ("uniform_mass", C.c_double), ("softening", C.c_void_p)]
 
 
 class Accumulator(C.Structure):
@@ -71,7 +71,8 @@ class Accumulator(C.Structure):
                 ("target_x", C.c_void_p), ("target_y", C.c_void_p), ("target_z", C.c_void_p),
                 ("long_range_x", C.c_void_p), ("long_range_y", C.c_void_p), ("long_range_z", C.c_void_p),
                 ("short_range_x", C.c_void_p), ("short_range_y", C.c_void_p), ("short_range_z", C.c_void_p),
-                ("nearest_pair_r2", C.c_void_p), ("previous_acceleration_magnitude", C.c_void_p)]
+                ("nearest_pair_r2", C.c_void_p), ("previous_acceleration_magnitude", C.c_void_p),
+                ("target_softening", C.c_void_p)]
 
 
 class TreeDump(C.Structure):

@@ -211,7 +211,8 @@ class TreePmCoordinator:
                                          targets=None, uniform_mass: float | None = None,
                                          long_range: bool = False, short_range: bool = False,
                                          nearest_pair: bool = False, previous_acceleration=None,
-                                         out=None, stream=None, visit_range=None) -> dict:
+                                         out=None, stream=None, visit_range=None, softening=None,
+                                         target_softening=None) -> dict:
         """TreePmCoordinator::solveActiveSetWithPmCadence. Returns a dict with
         ax, ay, az (active-slot order) and the requested optional lanes.
         previous_acceleration: per active slot |a_previous| for the relative
@@ -221,7 +222,10 @@ class TreePmCoordinator:
         visit_range: (begin, end) walks only the targets at those visit
         positions (chui_treepm_solve_visit_range); ax.. and pm_a.. then hold
         end - begin entries in visit order (visit_order(begin, end) gives
-        their slots)."""
+        their slots).
+        softening / target_softening: resolved per-source and per-active-slot
+        Plummer epsilons (chui_treepm.softening resolves a TreeSofteningView
+        into them), or None for config.softening."""
         arr = _Arrays(x)
         n = len(x)
         src = _abi.Sources()
@@ -250,6 +254,14 @@ class TreePmCoordinator:
             nt = n if active is None else len(active)
         acc.active_count = nt
         acc.active_index = arr.ptr(active, np.uint32) if active is not None else None
+        if softening is not None:
+            if len(softening) != n:
+                raise InvalidArgument(_abi.EINVAL, "TreePM source softening sidecar size must match source particle count")
+            src.softening = arr.ptr(softening, np.float64)
+        if target_softening is not None:
+            if len(target_softening) != nt:
+                raise InvalidArgument(_abi.EINVAL, "TreePM target softening sidecar size must match active-set size")
+            acc.target_softening = arr.ptr(target_softening, np.float64)
         if previous_acceleration is not None:
             if len(previous_acceleration) != nt:
                 raise InvalidArgument(_abi.EINVAL, "TreePM force accumulator spans must have matching active-set extent")
@@ -413,14 +425,17 @@ class TreePmCoordinator:
 def _adjoint_methods():
     """Reverse-mode entry points, attached to TreePmCoordinator below."""
 
-    def force_vjp(self, x, y, z, mass, cot_x, cot_y, cot_z, uniform_mass: float = 0.0):
-        """J_a(x)^T cot for the full-set TreePM acceleration (chui_treepm_force_vjp)."""
+    def force_vjp(self, x, y, z, mass, cot_x, cot_y, cot_z, uniform_mass: float = 0.0, softening=None):
+        """J_a(x)^T cot for the full-set TreePM acceleration (chui_treepm_force_vjp;
+        uniform softening only: a softening lane raises NotSupported)."""
         arr = _Arrays(x)
         src = _abi.Sources()
         src.count = len(x)
         src.x, src.y, src.z = arr.ptr(x, np.float64), arr.ptr(y, np.float64), arr.ptr(z, np.float64)
         src.mass = arr.ptr(mass, np.float64) if mass is not None else None
         src.uniform_mass = uniform_mass
+        if softening is not None:
+            src.softening = arr.ptr(softening, np.float64)
         cps = [arr.ptr(c, np.float64) for c in (cot_x, cot_y, cot_z)]
         outs = [arr.out(len(x), x) for _ in range(3)]
         st = _abi.Stats()

@@ -120,6 +120,18 @@ __global__ void activeCheckKernel(int64_t nt, const uint32_t* __restrict__ activ
   if (bad) atomicOr(status, bad);
 }
 
+// Softening lanes must be finite and non-negative
+// (validateTreePmPreflight, tree_pm_coupling.cpp:440-449).
+__global__ void softeningCheckKernel(int64_t n, const double* __restrict__ eps, uint32_t* status) {
+  uint32_t bad = 0;
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double e = eps[k];
+    if (!(isfinite(e) && e >= 0.0)) bad = kStatusNonFinite;
+  }
+  if (bad) atomicOr(status, bad);
+}
+
 // accel = PM + tree (active order); optional source-indexed tree-only and
 // nearest-pair lanes (TreePmForceAccumulatorView::addShortRangeToActiveSlot and
 // noteNearestPairToActiveSlot, tree_pm_coupling.cpp:1961-1978).
@@ -773,6 +785,28 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
        (rc = chui::stageIn(c, c.in_tz, acc->target_z, nt, memory, s, &tz))))
     return rc;
   if (!src->mass) m = nullptr;
+  // per-particle softening lanes (resolved epsilons)
+  c.soft_rows = nullptr;
+  c.soft_targets = nullptr;
+  if (explicit_targets && src->softening && !acc->target_softening)
+    return chui::fail(c, CHUI_TREEPM_EINVAL,
+                      "TreePM independent targets require target-owned softening/species sidecars when source "
+                      "sidecars are present");
+  if (src->softening && (rc = chui::stageIn(c, c.in_eps, src->softening, n, memory, s, &c.soft_rows))) return rc;
+  if (acc->target_softening &&
+      (rc = chui::stageIn(c, c.in_teps, acc->target_softening, nt, memory, s, &c.soft_targets)))
+    return rc;
+  if (c.soft_rows || c.soft_targets) {
+    uint32_t bits = 0;
+    cudaMemsetAsync(c.status.ptr, 0, 4, s);
+    if (c.soft_rows && n > 0)
+      { chui::noteLaunch(); chui::softeningCheckKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, c.soft_rows, c.status.as<uint32_t>()); }
+    if (c.soft_targets && nt > 0)
+      { chui::noteLaunch(); chui::softeningCheckKernel<<<chui::gridFor(nt, 256), 256, 0, s>>>(nt, c.soft_targets, c.status.as<uint32_t>()); }
+    cudaMemcpyAsync(&bits, c.status.ptr, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return chui::fail(c, CHUI_TREEPM_EDEVICE, "CUDA error");
+    if (bits) return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM softening sidecars require finite non-negative values");
+  }
 
   // validateTreePmPreflight (tree_pm_coupling.cpp:244-481)
   double lo[3], hi[3], mass_sum = 0.0, mass_range[2] = {0.0, 0.0};
@@ -868,7 +902,9 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
     // group walk eligibility (tree_pm_coupling.cpp:3840-3870, 3922-3925, 4282-4286)
     const double inv_2a2 = (0.25 / c.rs) / c.rs, inv_8a3 = ((0.125 / c.rs) / c.rs) / c.rs;
     const double t_cut = (0.25 * wp.cutoff2 / c.rs) / c.rs;
-    wp.group_walk = c.cfg.group_walk_enabled && c.cfg.acceptance_policy == CHUI_TREEPM_POLICY_ADAPTIVE &&
+    // (no group walk with per-particle softening: tree_pm_coupling.cpp:3858-3859)
+    wp.group_walk = !c.soft_rows && !c.soft_targets && c.cfg.group_walk_enabled &&
+                    c.cfg.acceptance_policy == CHUI_TREEPM_POLICY_ADAPTIVE &&
                     c.cfg.adaptive_error_estimator == CHUI_TREEPM_ESTIMATOR_RELATIVE_MONOPOLE &&
                     c.cfg.gaussian_pair_lookup && std::isnormal(inv_2a2) && std::isnormal(inv_8a3) &&
                     std::isfinite(t_cut) && t_cut < 63.0;
@@ -1098,6 +1134,10 @@ int chui_treepm_force_vjp(void* handle, const chui_treepm_sources* src, const do
     return chui::fail(c, CHUI_TREEPM_EINVAL, "force VJP requires positions, cotangents and gradients of equal extent");
   if (!src->mass && !(std::isfinite(src->uniform_mass) && src->uniform_mass >= 0.0))
     return chui::fail(c, CHUI_TREEPM_EINVAL, "TreePM sources require finite coordinates and finite non-negative masses");
+  if (src->softening)
+    return chui::fail(c, CHUI_TREEPM_ENOTSUP, "the force VJP supports uniform softening only");
+  c.soft_rows = nullptr;
+  c.soft_targets = nullptr;
   chui::DeviceGuard guard(c.device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const uint64_t launches_before = chui::launchCount();

@@ -88,6 +88,12 @@ struct Context {
 
   // staged inputs / outputs
   DevBuf in_x, in_y, in_z, in_m, in_active, in_tx, in_ty, in_tz, in_prev;
+  // per-particle softening of the current solve: row-order source epsilons and
+  // active-slot target epsilons (staged inputs), the tree-order copy, and each
+  // node's {min, max} source epsilon
+  DevBuf in_eps, in_teps, src_eps, node_soft;
+  const double* soft_rows = nullptr;     // null: uniform (config) source softening
+  const double* soft_targets = nullptr;  // null: targets take their source row's epsilon
   // group walk: leaf per tree position, per visit position the group start and
   // the group record (centre + a_min, half + flags), the eligible group starts,
   // per-slot "evaluated by a group" flags, the Gaussian Hermite table

@@ -474,7 +474,22 @@ __global__ void leafKeyKernel(int64_t n, const uint32_t* __restrict__ inv_rank,
 struct MomentIn {
   const double4* u4;  // tree-ordered tree-frame positions and masses
   int quadrupole;
+  const double* eps;  // tree-ordered source softening (nullable: uniform)
+  double2* soft;      // per node {min, max} source softening (when eps is given)
 };
+
+// Source softening range of a node (accumulateMultipoles,
+// tree_gravity.cpp:1215-1240, 1320-1323): leaves over their sources, parents
+// over their children; a node without sources keeps {+inf, 0}.
+__device__ __forceinline__ double2 leafSoftening(const MomentIn& in, const uint4 r) {
+  double lo = INFINITY, hi = 0.0;
+  for (uint32_t t = r.x; t < r.x + r.y; ++t) {
+    const double e = in.eps[t];
+    lo = fmin(lo, e);
+    hi = fmax(hi, e);
+  }
+  return make_double2(lo, hi);
+}
 
 __device__ void leafMoments(int64_t node, const MomentIn& in, const double4 g, const uint4 r,
                             double4* com_out, double* quad_out) {
@@ -588,6 +603,7 @@ __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restr
     leafMoments(k, in, geom[k], r, &cm, q);
     com[k] = cm;
     for (int t = 0; t < 8; ++t) quad[8 * k + t] = q[t];
+    if (in.eps) in.soft[k] = leafSoftening(in, r);
     int64_t node = k;
     while (true) {
       __threadfence();
@@ -599,6 +615,17 @@ __global__ void momentsKernel(int64_t nodes, MomentIn in, const double4* __restr
       internalMoments(p, geom[p], child, com, quad, in.quadrupole, &cm, q);
       com[p] = cm;
       for (int t = 0; t < 8; ++t) quad[8 * static_cast<size_t>(p) + t] = q[t];
+      if (in.eps) {
+        double lo = INFINITY, hi = 0.0;
+        for (int o = 0; o < 8; ++o) {
+          const uint32_t ch = __ldcg(child + 8 * static_cast<size_t>(p) + o);
+          if (ch == kInvalid) continue;
+          const double2 cs = __ldcg(in.soft + ch);
+          lo = fmin(lo, cs.x);
+          hi = fmax(hi, cs.y);
+        }
+        in.soft[p] = make_double2(lo, hi);
+      }
       node = p;
     }
   }
@@ -677,7 +704,7 @@ __global__ void packSourcesKernel(int64_t n, const uint32_t* __restrict__ sorted
                                   const double* __restrict__ x, const double* __restrict__ y,
                                   const double* __restrict__ z, const double* __restrict__ m,
                                   double uniform_mass, float4* f4, double4* d4, double4* u4,
-                                  uint32_t* pos_of_row) {
+                                  uint32_t* pos_of_row, const double* __restrict__ eps_rows, double* eps_tree) {
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < n;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const uint32_t s = sorted[t];
@@ -694,6 +721,7 @@ __global__ void packSourcesKernel(int64_t n, const uint32_t* __restrict__ sorted
     }
     if (d4) d4[t] = make_double4(px, py, pz, ms);
     if (u4) u4[t] = make_double4(ux, uy, uz, ms);
+    if (eps_rows) eps_tree[t] = eps_rows[s];
   }
 }
 
@@ -986,16 +1014,21 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   }
   if (ensure(c.src_d4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
   if (ensure(c.src_u4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
+  if (c.soft_rows && (ensure(c.src_eps, n * sizeof(double)) || ensure(c.node_soft, total_nodes * sizeof(double2))))
+    return CHUI_TREEPM_ENOMEM;
   { noteLaunch(); packSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), out.leaf_of_pos, out.geom,
                                                     frame, x, y, z, m, uniform_mass,
                                                     mixed ? c.src_f4.as<float4>() : nullptr,
                                                     c.src_d4.as<double4>(), c.src_u4.as<double4>(),
-                                                    c.pos_of_row.as<uint32_t>()); }
+                                                    c.pos_of_row.as<uint32_t>(), c.soft_rows,
+                                                    c.soft_rows ? c.src_eps.as<double>() : nullptr); }
   // moments (leaves read the tree-ordered records written above)
   cudaMemsetAsync(c.node_counter.ptr, 0, total_nodes * 4, s);
   MomentIn mi;
   mi.u4 = c.src_u4.as<double4>();
   mi.quadrupole = c.cfg.multipole_order == 2 ? 1 : 0;
+  mi.eps = c.soft_rows ? c.src_eps.as<double>() : nullptr;
+  mi.soft = c.soft_rows ? c.node_soft.as<double2>() : nullptr;
   { noteLaunch(); momentsKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(total_nodes, mi, out.geom, out.range, out.parent,
                                                           out.child, c.node_counter.as<uint32_t>(),
                                                           c.node_com.as<double4>(), c.node_quad.as<double>()); }

@@ -73,6 +73,12 @@ struct WalkArgs {
   const float4* node_mq;   // per node 2 x float4: {mass, Mxx, Mxy, Mxz}, {Myy, Myz, Mzz, trace}
   const double4* src_u4;   // tree-ordered unwrapped positions + mass
   const double* prev;      // per slot |a_previous| (nullable: no history)
+  // per-particle softening (all nullable: uniform wp.eps): tree-order and
+  // row-order source epsilons, per-slot target epsilons, per-node {min, max}
+  const double* src_eps;
+  const double* row_eps;
+  const double* tgt_eps;
+  const double2* node_soft;
   // group walk
   const uint32_t* leaf_of_pos;  // tree position -> leaf node
   uint32_t* grp_start;          // visit position -> visit position of its group's first target
@@ -101,6 +107,7 @@ struct WalkArgs {
   // eps^2. cut2e = r_cut^2 + eps^2 is the cutoff test on r^2 + eps^2.
   float2 pk2[kPolyMaxTerms];
   float2 sc2, soff2, eps2_2;
+  float2 mone2;  // {-1, -1}: s from r^2 itself (per-pair softening)
   float cut2e;
   // diagnostics 2 (or a requested nearest-pair lane): the counting instances
   // walk with subtree blocks (the production traversal) -- blocks -- and the
@@ -136,7 +143,8 @@ __device__ __forceinline__ void multipoleForce(const WalkArgs& a, uint32_t node,
   const double r2 = dx * dx + dy * dy + dz * dz;
   const double safe_r2 = fmax(r2, 1.0e-30);
   const double r = sqrt(safe_r2);
-  const double pe = fmax(w.eps, eps_t);
+  // max(node softening maximum, target) (tree_pm_coupling.cpp:749-757)
+  const double pe = fmax(a.node_soft ? a.node_soft[node].y : w.eps, eps_t);
   const double denom = fmax(r2 + pe * pe, 1.0e-30);
   const double soft = 1.0 / (denom * sqrt(denom));
   const double split = shortRangeFactor(r, rs);
@@ -229,15 +237,48 @@ __device__ __noinline__ double residualProxy(double G, double eps, double rs, do
   return isfinite(proxy) && proxy >= 0.0 ? proxy : INFINITY;
 }
 
+// A target's softening: its own lane, else its source row's epsilon, else
+// the configured one (targetSofteningEpsilonUnchecked, tree_softening.hpp:90-110).
+__device__ __forceinline__ double targetEps(const WalkArgs& a, uint32_t slot, uint32_t row, bool valid) {
+  if (!valid) return a.wp.eps;
+  if (a.tgt_eps) return a.tgt_eps[slot];
+  if (a.row_eps && row < a.n) return a.row_eps[row];
+  return a.wp.eps;
+}
+
+// A source's softening by tree position.
+__device__ __forceinline__ double sourceEps(const WalkArgs& a, uint32_t pos) {
+  return a.src_eps ? a.src_eps[pos] : a.wp.eps;
+}
+
+// max(node softening maximum, target): the multipole and proxy softening.
+__device__ __forceinline__ double nodeEps(const WalkArgs& a, uint32_t node, double eps_t) {
+  return fmax(a.node_soft ? a.node_soft[node].y : a.wp.eps, eps_t);
+}
+
+// passesSofteningEnvelopeGuard (internal/tree_interaction_common.hpp:77-89)
+// at r = sqrt(max(r^2, 1e-30)): nodes whose sources' softenings differ are
+// accepted only beyond 2h + 2 max(node maximum, target).
+__device__ __forceinline__ bool softeningGuard(const WalkArgs& a, uint32_t node, double half, double r2,
+                                               double eps_t) {
+  if (!a.node_soft) return true;
+  const double2 ns = a.node_soft[node];
+  if (ns.y - ns.x <= 1.0e-12) return true;
+  return sqrt(fmax(r2, 1.0e-30)) > 2.0 * half + 2.0 * fmax(ns.y, eps_t);
+}
+
 // Acceptance of an internal node (acceptTreePmNode, internal/tree_pm_acceptance.hpp:53-139,
 // with acceptNodeByMac and acceptNodeByComDistanceMac of
 // internal/tree_interaction_common.hpp:36-75). Softening is uniform, so the
 // softening envelope guard passes.
 template <bool kAdaptive>
 __device__ __forceinline__ bool acceptNode(const WalkParams& w, double half, double com_offset, double mass,
-                                           bool inside, bool within, double r2, const History& hist) {
+                                           bool inside, bool within, double r2, const History& hist,
+                                           bool soft_ok = true, double eps_node = -1.0) {
   const double r = sqrt(fmax(r2, 1.0e-30));
   const double width = 2.0 * half;
+  if (eps_node < 0.0) eps_node = w.eps;
+  if (!soft_ok) return false;  // passesSofteningEnvelopeGuard
   if constexpr (!kAdaptive) {
     const bool envelope_ok = w.quadrupole && (width / r) < 0.08;
     bool mac_ok;
@@ -261,7 +302,7 @@ __device__ __forceinline__ bool acceptNode(const WalkParams& w, double half, dou
     const double lower = w.G * mass * (width * width * inv_r4);
     if (isfinite(allowance) && isfinite(lower) && lower > allowance) return false;
     if (w.estimator == 1) return isfinite(allowance) && isfinite(lower);
-    const double est = residualProxy(w.G, w.eps, w.rs, half, com_offset, mass, r2);
+    const double est = residualProxy(w.G, eps_node, w.rs, half, com_offset, mass, r2);
     return isfinite(est) && isfinite(allowance) && est <= allowance;
   }
   return ((width + com_offset) / sqrt(r2 + 1.0e-30)) < w.theta;
@@ -633,7 +674,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
     }
     const bool skip_self = valid && row < a.n;
     const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
-    const double eps_t = w.eps;
+    const double eps_t = targetEps(a, slot, row, valid);
     const History hist = loadHistory(a.prev, slot, valid);
     // targets the group walk evaluated take no per-target walk
     const bool grouped = valid && a.grp_done != nullptr && a.grp_done[slot] != 0;
@@ -739,8 +780,10 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
                 nearest_mixed = fminf(nearest_mixed, static_cast<float>(r2));
                 ++cnt_pairs;
                 if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
-                const double f = (w.gauss_lookup && r2 > 0.0 ? gaussResidualInvR3(a, r2, fmax(w.eps, eps_t))
-                                                             : residualInvR3(r2, fmax(w.eps, eps_t), w.rs)) *
+                // max(source, target) softening (tree_pm_coupling.cpp:4208-4212)
+                const double pe = fmax(sourceEps(a, begin + chunk + j), eps_t);
+                const double f = (w.gauss_lookup && r2 > 0.0 ? gaussResidualInvR3(a, r2, pe)
+                                                             : residualInvR3(r2, pe, w.rs)) *
                                  w.G;
                 acc_x += f * s.w * dx;
                 acc_y += f * s.w * dy;
@@ -765,8 +808,10 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32) walkKernel(WalkArgs a
       const double dz = applyMetric(nm[2], cm.z - pz);
       const double r2 = norm2rn(dx, dy, dz);
       bool accept = act && !prune &&
-                    (w.policy == 1 ? acceptNode<true>(w, h, off, cm.w, inside, within, r2, hist)
-                                   : acceptNode<false>(w, h, off, cm.w, inside, within, r2, hist));
+                    (w.policy == 1 ? acceptNode<true>(w, h, off, cm.w, inside, within, r2, hist,
+                                                      softeningGuard(a, node, h, r2, eps_t), nodeEps(a, node, eps_t))
+                                   : acceptNode<false>(w, h, off, cm.w, inside, within, r2, hist,
+                                                       softeningGuard(a, node, h, r2, eps_t), nodeEps(a, node, eps_t)));
       // COM-distance cutoff nodes: accepted beyond r_cut means pruned (:4129-4132)
       if (accept && w.com_cutoff && r2 > w.cutoff2) {
         accept = false;
@@ -888,10 +933,10 @@ __device__ __forceinline__ float2 hornerR2x2(const float2* c2, float2 r2, float2
 // M K d + f1 (Md + tr d / 2) + cr (d.Md) d / 2 with f1 = K'/r, cr the last.
 template <bool kEpsZero, int kTerms>
 __device__ __forceinline__ void multipoleF32(const WalkArgs& a, uint32_t node, float dx, float dy, float dz, float sc,
-                                             float& fx, float& fy, float& fz) {
+                                             float& fx, float& fy, float& fz, float eps2) {
   const float4 q0 = a.node_mq[2 * static_cast<size_t>(node)];
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float den = kEpsZero ? r2 : r2 + a.wp.eps2_f;
+  const float den = kEpsZero ? r2 : r2 + eps2;
   const float rinv = rsqrtf(den);
   const float rinv2 = rinv * rinv;
   const float rinv3 = rinv2 * rinv;
@@ -929,7 +974,8 @@ struct ExactDecision {
 
 template <bool kAdaptive>
 __device__ __forceinline__ ExactDecision exactNodeDecision(const WalkArgs& a, uint32_t node, double px, double py,
-                                                        double pz, bool skip_self, const History& hist) {
+                                                        double pz, bool skip_self, const History& hist,
+                                                        double eps_t) {
   const WalkParams& w = a.wp;
   ExactDecision d{};
   const double4 g = a.geom[node];
@@ -953,7 +999,8 @@ __device__ __forceinline__ ExactDecision exactNodeDecision(const WalkArgs& a, ui
   d.dy = applyMetric(my, cm.y - py);
   d.dz = applyMetric(mz, cm.z - pz);
   const double r2 = norm2rn(d.dx, d.dy, d.dz);
-  d.accept = acceptNode<kAdaptive>(w, h, off, cm.w, inside, within, r2, hist);
+  d.accept = acceptNode<kAdaptive>(w, h, off, cm.w, inside, within, r2, hist, softeningGuard(a, node, h, r2, eps_t),
+                                   nodeEps(a, node, eps_t));
   if (kAdaptive && d.accept && w.com_cutoff && r2 > w.cutoff2) {  // accepted beyond r_cut: pruned
     d.accept = false;
     d.prune = true;
@@ -964,7 +1011,7 @@ __device__ __forceinline__ ExactDecision exactNodeDecision(const WalkArgs& a, ui
 // Exact FP64 pairs of one leaf for the lanes in `want` (reference formulas,
 // per-pair source metric): used where the shared FP32 frame cannot serve.
 __device__ __forceinline__ void exactLeafPairs(const WalkArgs& a, double4* stage, uint32_t begin, uint32_t count,
-                                            bool want, double px, double py, double pz, uint32_t self_pos,
+                                            bool want, double px, double py, double pz, uint32_t self_pos, double eps_t,
                                             double& ax, double& ay, double& az, double& nearest,
                                             unsigned long long& pairs, unsigned long long& skips) {
   const WalkParams& w = a.wp;
@@ -990,7 +1037,7 @@ __device__ __forceinline__ void exactLeafPairs(const WalkArgs& a, double4* stage
         nearest = fmin(nearest, r2);
         ++pairs;
         if (dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
-        const double f = residualInvR3(r2, w.eps, w.rs) * w.G;
+        const double f = residualInvR3(r2, fmax(sourceEps(a, begin + chunk + j), eps_t), w.rs) * w.G;
         ax += f * sv.w * dx;
         ay += f * sv.w * dy;
         az += f * sv.w * dz;
@@ -1044,12 +1091,18 @@ __device__ __forceinline__ int certainLess(float a, float b, float err = 0.f) {
 // formulas (erf/exp residual, or its Gaussian table) and accepted multipoles
 // the FP64 screened quadrupole. This is the production solver in FP64, the
 // comparator for the mixed-precision speed-up.
+//
+// kSoft: per-particle softening -- each queued source carries its epsilon,
+// pairs take max(source, target), multipoles max(node maximum, target), and
+// nodes whose sources' softenings differ are decided in FP64 (the envelope
+// guard); masses travel with the sources.
 template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode, bool kUniform = false,
-          bool kCost = false, bool kF64 = false>
+          bool kCost = false, bool kF64 = false, bool kSoft = false>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUniform) ? CHUI_WALK_MIN_BLOCKS_STRICT
                                                                                   : CHUI_WALK_MIN_BLOCKS)
     walkFastKernel(WalkArgs a) {
   static_assert(!kF64 || (kMode <= 1 && !kDiag && !kUniform), "FP64 production walk: strict policy only");
+  static_assert(!kSoft || (!kUniform && !kEpsZero && !kF64 && kMode <= 2), "per-particle softening instances");
   // counters and the nearest-pair lane: the counting instances (kDiag), and
   // the FP64 production walk on request
   const bool inst = kDiag || (kF64 && a.instrument != 0);
@@ -1070,6 +1123,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
   // mask1, tree position 0, tree position 1} when masses travel separately.
   __shared__ float4 q_src[kWalkWarpsPerBlock][kF64 ? 2 : kQueueLen];
   __shared__ uint4 q_meta[kWalkWarpsPerBlock][kF64 ? 1 : kQueueLen / 2];
+  // kSoft: each queued source's softening (entry k at [k]; a pair reads a float2)
+  __shared__ __align__(8) float q_eps[kWalkWarpsPerBlock][kSoft ? kQueueLen : 2];
   // kF64: FP64 offsets + mass, and {lane mask, tree position}
   constexpr int kQ64 = kF64 ? kQueueLen / 2 : 1;
   __shared__ double4 q64[kWalkWarpsPerBlock][kQ64];
@@ -1161,6 +1216,9 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
     const bool skip_self = valid && row < a.n;
     const uint32_t self_pos = skip_self ? a.pos_of_row[row] : kInvalid;
     const History hist = loadHistory(kHistory ? a.prev : nullptr, slot, valid);
+    // the target's softening (uniform: the configured one)
+    const double eps_t_d = kSoft ? targetEps(a, slot, row, valid) : w.eps;
+    const float eps_t_f = static_cast<float>(eps_t_d);
     // group walk: the lane's group (start visit position), eligibility, and the
     // lane deciding for it in this warp (the group's first lane here); only the
     // warp holding a group's first target counts the group walk's node counters
@@ -1230,6 +1288,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
             qm[1] = 0u;
             qm[3] = kInvalid;
           }
+          if constexpr (kSoft) q_eps[warp][qn] = 0.f;
         }
         __syncwarp();
       }
@@ -1248,9 +1307,18 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         // variable and the cutoff test take it with eps^2 folded into their
         // constants. Diagnostics test the cutoff on r^2 itself, as the
         // reference does, and report it for the nearest pair.
-        const float2 r2e = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, a.eps2_2)));
-        const float2 r2 = kDiag ? __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz))) : r2e;
-        const float cut_t = kDiag ? cut2 : a.cut2e;
+        // kSoft: r^2, then r^2 + max(eps_source, eps_target)^2 per source
+        float2 r2e, r2;
+        if constexpr (kSoft) {
+          r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+          const float2 es = *reinterpret_cast<const float2*>(&q_eps[warp][2 * p]);
+          const float2 ep = make_float2(fmaxf(es.x, eps_t_f), fmaxf(es.y, eps_t_f));
+          r2e = __ffma2_rn(ep, ep, r2);
+        } else {
+          r2e = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, a.eps2_2)));
+          r2 = kDiag ? __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz))) : r2e;
+        }
+        const float cut_t = (kDiag || kSoft) ? cut2 : a.cut2e;
         bool mine0, mine1;
         if constexpr (kUniform) {
           mine0 = (__float_as_uint(B.z) & lane_bit) != 0u;
@@ -1269,7 +1337,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
           nearest_f = in0 ? fminf(nearest_f, r2.x) : nearest_f;
           nearest_f = in1 ? fminf(nearest_f, r2.y) : nearest_f;
         }
-        const float2 klong = hornerR2x2<kTerms>(a.pk2, r2e, a.sc2, a.soff2);  // -K_long
+        const float2 klong = kSoft ? hornerR2x2<kTerms>(a.pk2, r2, a.sc2, a.mone2)     // -K_long
+                                   : hornerR2x2<kTerms>(a.pk2, r2e, a.sc2, a.soff2);
         const float2 rinv = make_float2(rsqrtf(r2e.x), rsqrtf(r2e.y));
         float2 k3 = __ffma2_rn(__fmul2_rn(rinv, rinv), rinv, klong);  // K_soft - K_long
         if constexpr (!kUniform) k3 = __fmul2_rn(k3, make_float2(B.z, B.w));
@@ -1309,7 +1378,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
           nearest_d = in ? fmin(nearest_d, r2) : nearest_d;
         }
         if (in) {
-          const double kr = w.gauss_lookup ? gaussResidualInvR3(a, r2, w.eps) : residualInvR3(r2, w.eps, w.rs);
+          const double pe = fmax(sourceEps(a, meta.y), eps_t_d);
+          const double kr = w.gauss_lookup ? gaussResidualInvR3(a, r2, pe) : residualInvR3(r2, pe, w.rs);
           const double f = kr * e.w;
           fx += f * dx;
           fy += f * dy;
@@ -1336,7 +1406,13 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
       for (int k = 0; k < kmax; ++k) {
         if (k < mn) {
           const float4 e = m_list[warp][k][lane];
-          multipoleF32<kEpsZero, kTerms>(a, __float_as_uint(e.w), e.x, e.y, e.z, sc_r2, fx, fy, fz);
+          const uint32_t mnode = __float_as_uint(e.w);
+          float me2 = w.eps2_f;
+          if constexpr (kSoft) {
+            const float me = static_cast<float>(nodeEps(a, mnode, eps_t_d));
+            me2 = me * me;
+          }
+          multipoleF32<kEpsZero, kTerms>(a, mnode, e.x, e.y, e.z, sc_r2, fx, fy, fz, me2);
         }
       }
       acc_x += static_cast<double>(w.G_f * fx);
@@ -1421,6 +1497,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
             qm[hq] = m;
             qm[2 + hq] = begin + k;
           }
+          if constexpr (kSoft) q_eps[warp][slot_q] = static_cast<float>(sourceEps(a, begin + k));
         }
         __syncwarp();
         qn += c;
@@ -1583,8 +1660,16 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         }
         if (inst && com_skip) ++cnt_pruned;
       }
+      if constexpr (kSoft) {
+        // a node whose sources' softenings differ: the envelope guard decides
+        // with the reference's FP64 arithmetic
+        if (act && !is_leaf && !prune && !in_group && a.node_soft) {
+          const double2 ns = a.node_soft[node];
+          if (ns.y - ns.x > 1.0e-12) need_exact = true;
+        }
+      }
       if (act && need_exact) {
-        const ExactDecision d = exactNodeDecision<kAdaptive>(a, node, px, py, pz, skip_self, hist);
+        const ExactDecision d = exactNodeDecision<kAdaptive>(a, node, px, py, pz, skip_self, hist, eps_t_d);
         prune = d.prune;
         accept = d.accept;
         dxc = static_cast<float>(d.dx);
@@ -1610,7 +1695,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
           enqueue(begin, count, mask, false, g, cdx, cdy, cdz);
         } else {
           unsigned long long p = 0, sk = 0;
-          exactLeafPairs(a, exact_sm[warp], begin, count, want, px, py, pz, self_pos, acc_x, acc_y, acc_z,
+          exactLeafPairs(a, exact_sm[warp], begin, count, want, px, py, pz, self_pos, eps_t_d, acc_x, acc_y, acc_z,
                          nearest_d, p, sk);
           cnt_pairs += static_cast<uint32_t>(p);
           cnt_skips += static_cast<uint32_t>(sk);
@@ -1634,7 +1719,12 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
           } else {
             // few multipoles under the strict policy: evaluated where accepted
             float fx = 0.f, fy = 0.f, fz = 0.f;
-            multipoleF32<kEpsZero, kTerms>(a, node, dxc, dyc, dzc, sc_r2, fx, fy, fz);
+            float me2 = w.eps2_f;
+            if constexpr (kSoft) {
+              const float me = static_cast<float>(nodeEps(a, node, eps_t_d));
+              me2 = me * me;
+            }
+            multipoleF32<kEpsZero, kTerms>(a, node, dxc, dyc, dzc, sc_r2, fx, fy, fz, me2);
             acc_x += static_cast<double>(w.G_f * fx);
             acc_y += static_cast<double>(w.G_f * fy);
             acc_z += static_cast<double>(w.G_f * fz);
@@ -1642,8 +1732,8 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUnifo
         } else {
           // FP64 multipole: FP32 powers of 1/r could overflow this close to the
           // COM, or the FP32 split constants are out of range for this r_s
-          const ExactDecision d = exactNodeDecision<kAdaptive>(a, node, px, py, pz, skip_self, hist);
-          multipoleForce(a, node, d.dx, d.dy, d.dz, w.eps, acc_x, acc_y, acc_z);
+          const ExactDecision d = exactNodeDecision<kAdaptive>(a, node, px, py, pz, skip_self, hist, eps_t_d);
+          multipoleForce(a, node, d.dx, d.dy, d.dz, eps_t_d, acc_x, acc_y, acc_z);
         }
       }
       if constexpr (kAdaptive) {
@@ -2112,6 +2202,11 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.node_mq = c.node_mq.as<float4>();
   a.src_u4 = c.src_u4.as<double4>();
   a.prev = prev_acc;
+  const bool soft = c.soft_rows != nullptr || c.soft_targets != nullptr;
+  a.src_eps = c.soft_rows ? c.src_eps.as<double>() : nullptr;
+  a.row_eps = c.soft_rows;
+  a.tgt_eps = c.soft_targets;
+  a.node_soft = c.soft_rows ? c.node_soft.as<double2>() : nullptr;
   a.leaf_of_pos = nullptr;
   a.grp_start = nullptr;
   a.grp_rec = nullptr;
@@ -2160,6 +2255,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     a.soff2 = make_float2(soff, soff);
     a.eps2_2 = make_float2(wp.eps2_f, wp.eps2_f);
     a.cut2e = wp.cut2_f + wp.eps2_f;
+    a.mone2 = make_float2(-1.0f, -1.0f);
   }
   // diagnostics 2 or a nearest-pair lane: counted walk over the production traversal
   a.instrument = c.walk_instrument ? 1 : 0;
@@ -2195,6 +2291,22 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
     const bool uniform = wp.uniform_mass != 0;
     const int mode = wp.policy == CHUI_TREEPM_POLICY_ADAPTIVE ? (wp.group_walk ? 3 : 2)
                                                                : (wp.criterion == 2 && prev_acc ? 1 : 0);
+    if (soft) {
+      // per-particle softening: masses travel with the sources, the long H
+      // form (any configuration), no group walk
+#define CHUI_WALK_SOFT(DIAG, CONT, MODE) \
+  walkFastKernel<false, kPolyMaxTerms, DIAG, CONT, MODE, false, false, false, true>
+#define CHUI_WALK_SOFT2(MODE)                                                                          \
+  if (diag) return contiguous ? launchPersistent(CHUI_WALK_SOFT(true, true, MODE), a, s)                  \
+                              : launchPersistent(CHUI_WALK_SOFT(true, false, MODE), a, s);                \
+  return contiguous ? launchPersistent(CHUI_WALK_SOFT(false, true, MODE), a, s)                          \
+                    : launchPersistent(CHUI_WALK_SOFT(false, false, MODE), a, s);
+      if (mode >= 2) { CHUI_WALK_SOFT2(2) }
+      if (mode == 1) { CHUI_WALK_SOFT2(1) }
+      CHUI_WALK_SOFT2(0)
+#undef CHUI_WALK_SOFT2
+#undef CHUI_WALK_SOFT
+    }
 #define CHUI_WALK_DISPATCH2(EPS, TERMS, ADP)                                                           \
     if (diag) return contiguous ? launchPersistent(walkFastKernel<EPS, TERMS, true, true, ADP>, a, s)     \
                                 : launchPersistent(walkFastKernel<EPS, TERMS, true, false, ADP>, a, s);   \
@@ -2217,7 +2329,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
 #undef CHUI_WALK_DISPATCH
 #undef CHUI_WALK_DISPATCH2
   }
-  if (!mixed && c.cfg.diagnostics != 1 && wp.policy == CHUI_TREEPM_POLICY_STRICT && !wp.group_walk &&
+  if (!mixed && !soft && c.cfg.diagnostics != 1 && wp.policy == CHUI_TREEPM_POLICY_STRICT && !wp.group_walk &&
       !(wp.criterion == 2 && prev_acc)) {
     // the production solver in FP64 (same traversal and subtree blocks as the
     // mixed walk, FP64 pairs and multipoles)

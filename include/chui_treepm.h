@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define CHUI_TREEPM_ABI_VERSION 1
+#define CHUI_TREEPM_ABI_VERSION 2
 
 enum {
   CHUI_TREEPM_OK = 0,
@@ -115,12 +115,21 @@ typedef struct {
 } chui_treepm_stats;
 
 /* Sources: TreePmCoordinator::solveActiveSet's pos_{x,y,z}_comoving and
- * mass_code spans. mass may be NULL for a uniform mass population. */
+ * mass_code spans. mass may be NULL for a uniform mass population.
+ * softening (optional): each source's resolved Plummer epsilon (comoving),
+ * the materialized lane of TreeGravitySolver::resolvedSourceSoftening
+ * (include/cosmosim/gravity/tree_softening.hpp:46-67, resolved from a
+ * TreeSofteningView by resolveSourceSofteningEpsilon, :152-180); NULL: every
+ * source takes config.softening. A pair uses max(epsilon_source,
+ * epsilon_target) and an accepted node max(node maximum, epsilon_target)
+ * (:229-233); nodes whose sources' epsilons differ are accepted only beyond
+ * 2h + 2 max(node maximum, epsilon_target) (passesSofteningEnvelopeGuard). */
 typedef struct {
   int64_t count;
   const double *x, *y, *z;
   const double *mass;
   double uniform_mass;
+  const double *softening;
 } chui_treepm_sources;
 
 /* Accumulator: TreePmForceAccumulatorView (tree_pm_coupling.hpp:127-165).
@@ -142,6 +151,12 @@ typedef struct {
    * relative criteria, or NULL (no history). Non-finite entries mean "no
    * history" for that target: the COM-distance fallback. */
   const double *previous_acceleration_magnitude;
+  /* target_softening (optional): per active slot, the target's resolved
+   * epsilon (resolveTargetSofteningEpsilon, tree_softening.hpp:182-226);
+   * NULL: a target that is a source takes its source epsilon, others
+   * config.softening. Explicit targets with a source softening lane need it
+   * (tree_pm_coupling.cpp:3962-3971). */
+  const double *target_softening;
 } chui_treepm_accumulator;
 
 /* Defaults of TreePmOptions / TreeGravityOptions (tree_gravity.hpp:30-43,

@@ -107,6 +107,10 @@ struct Problem {
   std::int64_t group_walk = 0, gaussian_lookup = 0;
   // optional "CHUIISO1" block after it: PM boundary condition (1 isolated/open)
   std::int64_t boundary = 0;
+  // optional "CHUISOF1" block: per-particle softening sidecars of a
+  // TreeSofteningView (source epsilon + override mask, target epsilon + mask)
+  std::vector<double> src_eps, tgt_eps;
+  std::vector<std::uint8_t> src_mask, tgt_mask;
 };
 
 Problem readProblem(const char* path) {
@@ -152,25 +156,32 @@ Problem readProblem(const char* path) {
   p.vy = r.vec<double>(n);
   p.vz = r.vec<double>(n);
   p.active = r.vec<std::uint32_t>(static_cast<std::size_t>(p.n_active));
+  // tagged trailing blocks, in any order
   char tail[8];
-  if (std::fread(tail, 1, 8, f) == 8) {
-    if (std::memcmp(tail, "CHUIADP1", 8) != 0) throw std::runtime_error("bad trailing block");
-    p.policy = r.get<std::int64_t>();
-    p.estimator = r.get<std::int64_t>();
-    p.cutoff_policy = r.get<std::int64_t>();
-    p.has_prev = r.get<std::int64_t>();
-    p.adaptive_angle = r.get<double>();
-    p.rel_tol = r.get<double>();
-    p.accel_floor = r.get<double>();
-    if (p.has_prev) p.prev = r.vec<double>(static_cast<std::size_t>(p.n_active ? p.n_active : p.n));
-    if (std::fread(tail, 1, 8, f) == 8) {
-      if (std::memcmp(tail, "CHUIGRP1", 8) != 0) throw std::runtime_error("bad trailing block");
+  while (std::fread(tail, 1, 8, f) == 8) {
+    if (std::memcmp(tail, "CHUIADP1", 8) == 0) {
+      p.policy = r.get<std::int64_t>();
+      p.estimator = r.get<std::int64_t>();
+      p.cutoff_policy = r.get<std::int64_t>();
+      p.has_prev = r.get<std::int64_t>();
+      p.adaptive_angle = r.get<double>();
+      p.rel_tol = r.get<double>();
+      p.accel_floor = r.get<double>();
+      if (p.has_prev) p.prev = r.vec<double>(static_cast<std::size_t>(p.n_active ? p.n_active : p.n));
+    } else if (std::memcmp(tail, "CHUIGRP1", 8) == 0) {
       p.group_walk = r.get<std::int64_t>();
       p.gaussian_lookup = r.get<std::int64_t>();
-      if (std::fread(tail, 1, 8, f) == 8) {
-        if (std::memcmp(tail, "CHUIISO1", 8) != 0) throw std::runtime_error("bad trailing block");
-        p.boundary = r.get<std::int64_t>();
-      }
+    } else if (std::memcmp(tail, "CHUIISO1", 8) == 0) {
+      p.boundary = r.get<std::int64_t>();
+    } else if (std::memcmp(tail, "CHUISOF1", 8) == 0) {
+      const auto ns = static_cast<std::size_t>(r.get<std::int64_t>());
+      p.src_eps = r.vec<double>(ns);
+      p.src_mask = r.vec<std::uint8_t>(ns);
+      const auto nt = static_cast<std::size_t>(r.get<std::int64_t>());
+      p.tgt_eps = r.vec<double>(nt);
+      p.tgt_mask = r.vec<std::uint8_t>(nt);
+    } else {
+      throw std::runtime_error("bad trailing block");
     }
   }
   std::fclose(f);
@@ -247,15 +258,20 @@ int main(int argc, char** argv) {
 
     cg::TreePmProfileEvent profile{};
     cg::TreePmDiagnostics diagnostics{};
+    cg::TreeSofteningView softening{};
+    softening.source_particle_epsilon_comoving = p.src_eps;
+    softening.source_particle_epsilon_override_mask = p.src_mask;
+    softening.target_particle_epsilon_comoving = p.tgt_eps;
+    softening.target_particle_epsilon_override_mask = p.tgt_mask;
     const auto t0 = std::chrono::steady_clock::now();
-    coordinator.solveActiveSet(p.x, p.y, p.z, p.m, acc, options, &profile, &diagnostics);
+    coordinator.solveActiveSet(p.x, p.y, p.z, p.m, acc, options, &profile, &diagnostics, softening);
     const double first_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 
     std::vector<double> times, rep_phases;  // rep_phases: {pm, tree build, traversal} ms per repeat
     for (std::int64_t rep = 0; rep < p.repeats; ++rep) {
       cg::TreePmProfileEvent prof{};
       const auto t1 = std::chrono::steady_clock::now();
-      coordinator.solveActiveSet(p.x, p.y, p.z, p.m, acc, options, &prof, nullptr);
+      coordinator.solveActiveSet(p.x, p.y, p.z, p.m, acc, options, &prof, nullptr, softening);
       times.push_back(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count());
       rep_phases.push_back(prof.pm_profile.total_ms);
       rep_phases.push_back(prof.tree_profile.full_rebuild_ms);

@@ -98,6 +98,12 @@ class RefProblem:
     group_walk: int = 0       # TreePmOptions::group_walk_enabled
     gaussian_lookup: int = 0  # TreePmOptions::gaussian_pair_lookup_enabled
     boundary: int = 0         # PmBoundaryCondition: 0 periodic, 1 isolated/open
+    # TreeSofteningView sidecars: source epsilon + override mask (per source),
+    # target epsilon + override mask (per active slot)
+    src_eps: np.ndarray | None = None
+    src_mask: np.ndarray | None = None
+    tgt_eps: np.ndarray | None = None
+    tgt_mask: np.ndarray | None = None
 
 
 def write_problem(path: str, p: RefProblem) -> None:
@@ -135,6 +141,14 @@ def write_problem(path: str, p: RefProblem) -> None:
                 if p.boundary:
                     f.write(b"CHUIISO1")
                     f.write(struct.pack("<q", p.boundary))
+        if p.src_eps is not None or p.tgt_eps is not None:
+            f.write(b"CHUISOF1")
+            for eps, mask in ((p.src_eps, p.src_mask), (p.tgt_eps, p.tgt_mask)):
+                e = np.ascontiguousarray(eps if eps is not None else [], dtype=np.float64)
+                mk = np.ascontiguousarray(mask if mask is not None else np.ones(len(e)), dtype=np.uint8)
+                f.write(struct.pack("<q", len(e)))
+                f.write(e.tobytes())
+                f.write(mk.tobytes())
 
 
 class _Buf:

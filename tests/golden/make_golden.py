@@ -33,9 +33,13 @@ TREE_KEYS = ("ux", "uy", "uz", "anchors", "morton_key", "sorted_index", "center_
 ONLY = set(sys.argv[1:])
 
 
-def save(name: str, p: refio.RefProblem, r: dict, extra: dict | None = None, keep_tree=True):
+def save(name: str, p: refio.RefProblem, r, extra: dict | None = None, keep_tree=True):
+    """r: the reference's result, or a callable producing it (run only for
+    the selected fixtures)."""
     if ONLY and name not in ONLY:
         return
+    if callable(r):
+        r = r()
     d = {
         "x": p.x, "y": p.y, "z": p.z, "m": p.m,
         "vx": p.vx if p.vx is not None else np.zeros_like(p.x),
@@ -83,7 +87,7 @@ def main():
     p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(16,) * 3, theta=0.5, leaf=16,
                          dump_density=1, kdk=1, drift=0.02, kick1=0.01, kick2=0.01,
                          vx=vx, vy=vy, vz=vz, ewald=32)
-    save("lattice16_cic", p, refio.run(p))
+    save("lattice16_cic", p, lambda: refio.run(p))
 
     # 2. clustered: lattice + NFW halos, TSC + deconvolution, softened (accepted multipoles)
     x, y, z, vx, vy, vz = ics.zeldovich_lattice(20, 50.0, 0.3, seed=12)
@@ -92,7 +96,7 @@ def main():
     m = np.full(len(x), 2.0 / len(x))
     p = refio.RefProblem(x, y, z, m, box=(50.0,) * 3, mesh=(16,) * 3, theta=0.7, leaf=16, eps=0.05,
                          scheme=1, deconv=1, dump_density=1)
-    save("clustered_tsc", p, refio.run(p))
+    save("clustered_tsc", p, lambda: refio.run(p))
 
     # 3. rectangular box, non-power-of-two mesh, non-canonical coordinates, active subset
     rng = np.random.default_rng(14)
@@ -109,23 +113,23 @@ def main():
     active[:3] = [0, 3, 4]
     p = refio.RefProblem(x, y, z, m, box=box, mesh=(12, 10, 16), theta=0.5, leaf=8, eps=0.02, rcut=4.5,
                          active=active, dump_density=1)
-    save("rect_active", p, refio.run(p))
+    save("rect_active", p, lambda: refio.run(p))
 
     # 4. tiny cases: two-body, 24-particle quasi-uniform, duplicates deeper than a leaf
     p = refio.RefProblem(np.array([1.0, 1.7]), np.array([2.0, 2.1]), np.array([3.0, 2.6]),
                          np.array([1.0, 0.5]), box=(10.0,) * 3, mesh=(16,) * 3, theta=0.5, leaf=1)
-    save("two_body", p, refio.run(p))
+    save("two_body", p, lambda: refio.run(p))
     rng = np.random.default_rng(15)
     x, y, z = (rng.uniform(0, 4.0, 24) for _ in range(3))
     p = refio.RefProblem(x, y, z, np.full(24, 1.0 / 24), box=(4.0,) * 3, mesh=(8,) * 3, theta=0.5,
                          leaf=4, eps=0.01, rcut=3.9)
-    save("quasi24", p, refio.run(p))
+    save("quasi24", p, lambda: refio.run(p))
     x = np.concatenate([np.full(20, 1.25), rng.uniform(0, 5.0, 200)])
     y = np.concatenate([np.full(20, 2.5), rng.uniform(0, 5.0, 200)])
     z = np.concatenate([np.full(20, 3.75), rng.uniform(0, 5.0, 200)])
     p = refio.RefProblem(x, y, z, np.full(220, 1.0 / 220), box=(5.0,) * 3, mesh=(8,) * 3, theta=0.5,
                          leaf=4, eps=0.02, rcut=3.9)
-    save("duplicates", p, refio.run(p))
+    save("duplicates", p, lambda: refio.run(p))
 
     # 5. the 32^3 configuration: L = 10 Mpc/h, lattice + Zel'dovich (P ~ k^-2, rms 0.2
     #    spacing), mesh 64^3, r_s = 1.25 cells, theta = 0.5, leaf 16, CIC, unsoftened,
@@ -134,7 +138,7 @@ def main():
     m = np.full(len(x), 1.0 / len(x))
     p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(64,) * 3, theta=0.5, leaf=16,
                          kdk=1, drift=0.02, kick1=0.01, kick2=0.01, vx=vx, vy=vy, vz=vz, ewald=8)
-    save("config32", p, refio.run(p))
+    save("config32", p, lambda: refio.run(p))
 
     # 6. adaptive relative policy (TreePmOptions::acceptance_policy = kAdaptiveRelative) on a
     #    clustered box: lattice + NFW halos, softened, leaf 8. The acceleration history is the
@@ -155,22 +159,22 @@ def main():
     #    alpha 0.0025, maximum angle 1.0
     p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=1, cutoff_policy=1,
                          adaptive_angle=1.0, rel_tol=0.0025, prev_acc=prev)
-    save("adaptive_monopole", p, refio.run(p))
+    save("adaptive_monopole", p, lambda: refio.run(p))
     #    the default adaptive estimator: residual derivative, contain nodes, alpha 0.005,
     #    maximum angle 0.5; an active subset carries its own history slots
     active = np.sort(rng.choice(len(x), 5000, replace=False)).astype(np.uint32)
     p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=0, cutoff_policy=0,
                          adaptive_angle=0.5, rel_tol=0.005, prev_acc=prev[active], active=active)
-    save("adaptive_residual", p, refio.run(p))
+    save("adaptive_residual", p, lambda: refio.run(p))
     #    the group walk (one conservative walk per leaf of targets, Gaussian Hermite pair
     #    table) on the fast deck, over all targets and over the active subset
     p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=1, cutoff_policy=1,
                          adaptive_angle=1.0, rel_tol=0.0025, prev_acc=prev, group_walk=1, gaussian_lookup=1)
-    save("group_walk", p, refio.run(p))
+    save("group_walk", p, lambda: refio.run(p))
     p = refio.RefProblem(x, y, z, m, **common, policy=1, estimator=1, cutoff_policy=0,
                          adaptive_angle=0.5, rel_tol=0.005, prev_acc=prev[active], active=active,
                          group_walk=1, gaussian_lookup=1)
-    save("group_walk_active", p, refio.run(p))
+    save("group_walk_active", p, lambda: refio.run(p))
 
     # 7. isolated/open boundaries (PmBoundaryCondition::kIsolatedOpen): a clustered
     #    distribution in the middle of the box plus particles on and beyond the faces
@@ -183,12 +187,12 @@ def main():
     rng = np.random.default_rng(31)
     m = rng.uniform(0.5, 1.5, len(x)) / len(x)
     p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(16,) * 3, theta=0.5, leaf=8, boundary=1)
-    save("isolated_cic", p, refio.run(p))
+    save("isolated_cic", p, lambda: refio.run(p))
     active = np.sort(rng.choice(len(x), 600, replace=False)).astype(np.uint32)
     active[:4] = [0, 1, 3, 5]
     p = refio.RefProblem(x, y, z, m, box=(10.0,) * 3, mesh=(16,) * 3, theta=0.6, leaf=8, eps=0.02, scheme=1,
                          active=active, boundary=1)
-    save("isolated_tsc_active", p, refio.run(p))
+    save("isolated_tsc_active", p, lambda: refio.run(p))
 
     # 8. the headline configuration's settings on a clustered periodic box of
     #    40^3 = 64000 particles at the 256^3 case's mean spacing (L = 31.25):
@@ -199,14 +203,40 @@ def main():
     m = np.full(len(x), 1.0 / len(x))
     p = refio.RefProblem(x, y, z, m, box=(31.25,) * 3, mesh=(40,) * 3, theta=0.6, leaf=16, eps=0.001,
                          scheme=0, deconv=1, dump_density=1, ewald=16)
-    save("clustered64k_cic", p, refio.run(p))
+    save("clustered64k_cic", p, lambda: refio.run(p))
     #    the large configuration's tree: theta 0.7, leaf 32, 60 % in 8 halos
     #    over 4 decades, same box, mesh and scheme
     x, y, z, *_ = ics.clustered_box(40 ** 3, 31.25, 0.6, 8, 4.0, 0.5, 82)
     m = np.full(len(x), 1.0 / len(x))
     p = refio.RefProblem(x, y, z, m, box=(31.25,) * 3, mesh=(40,) * 3, theta=0.7, leaf=32, eps=0.001,
                          scheme=0, deconv=1)
-    save("clustered64k_t07_leaf32", p, refio.run(p))
+    save("clustered64k_t07_leaf32", p, lambda: refio.run(p))
+
+    # 9. per-particle softening (TreeSofteningView): a clustered box whose halo
+    #    particles take epsilon 0.02 and lattice particles 0.08 by override,
+    #    with 5 % of the overrides off (the configured 0.05 applies); nodes
+    #    mixing the two see the softening envelope guard. CIC + deconvolution,
+    #    theta 0.7, leaf 16, quadrupoles (accepted multipoles).
+    x, y, z, vx, vy, vz = ics.zeldovich_lattice(20, 50.0, 0.3, seed=91)
+    hx, hy, hz = ics.nfw_halos(4000, 8, 50.0, 2.0, seed=92, total_particles=len(x) + 4000)
+    n_lat = len(x)
+    x, y, z = np.concatenate([x, hx]), np.concatenate([y, hy]), np.concatenate([z, hz])
+    m = np.full(len(x), 2.0 / len(x))
+    rng = np.random.default_rng(93)
+    src_eps = np.where(np.arange(len(x)) < n_lat, 0.08, 0.02)
+    src_mask = (rng.random(len(x)) >= 0.05).astype(np.uint8)
+    common = dict(box=(50.0,) * 3, mesh=(16,) * 3, theta=0.7, leaf=16, eps=0.05, deconv=1)
+    p = refio.RefProblem(x, y, z, m, **common, src_eps=src_eps, src_mask=src_mask)
+    save("softening_mixed", p, lambda: refio.run(p), extra={"src_eps": src_eps, "src_mask": src_mask})
+    #    an active subset with target sidecars: some targets override to 0.1 or
+    #    0.0, the rest (mask 0) take the configured epsilon
+    active = np.sort(rng.choice(len(x), 2500, replace=False)).astype(np.uint32)
+    tgt_eps = rng.choice([0.1, 0.0, 0.03], len(active))
+    tgt_mask = (rng.random(len(active)) >= 0.3).astype(np.uint8)
+    p = refio.RefProblem(x, y, z, m, **common, active=active, src_eps=src_eps, src_mask=src_mask,
+                         tgt_eps=tgt_eps, tgt_mask=tgt_mask, dump_tree=0)
+    save("softening_active", p, lambda: refio.run(p), keep_tree=False,
+         extra={"src_eps": src_eps, "src_mask": src_mask, "tgt_eps": tgt_eps, "tgt_mask": tgt_mask})
 
 
 if __name__ == "__main__":
