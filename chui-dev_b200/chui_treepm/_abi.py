@@ -38,7 +38,7 @@ class Config(C.Structure):
         ("adaptive_maximum_opening_angle", C.c_double), ("relative_force_tolerance", C.c_double),
         ("relative_force_acceleration_floor", C.c_double),
         ("group_walk_enabled", C.c_int32), ("gaussian_pair_lookup", C.c_int32),
-        ("boundary_condition", C.c_int32),
+        ("boundary_condition", C.c_int32), ("short_range_only", C.c_int32),
     ]
 
 

@@ -95,6 +95,7 @@ class TreePmConfig:
     group_walk_enabled: int = 0
     gaussian_pair_lookup: int = 0
     boundary_condition: int = _abi.BOUNDARY_PERIODIC
+    short_range_only: int = 0
 
     def to_c(self) -> _abi.Config:
         c = _abi.Config()

@@ -605,6 +605,7 @@ int chui_treepm_config_default(chui_treepm_config* cfg) {
   cfg->group_walk_enabled = 0;                                                // tree_pm_coupling.hpp:257
   cfg->gaussian_pair_lookup = 0;                                              // tree_pm_coupling.hpp:266
   cfg->boundary_condition = CHUI_TREEPM_BOUNDARY_PERIODIC;                    // pm_solver.hpp:236
+  cfg->short_range_only = 0;                                                  // tree_pm_coupling.hpp:292
   return 0;
 }
 
@@ -835,8 +836,11 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
   }
   const double total_mass = m ? mass_sum : static_cast<double>(n) * src->uniform_mass;
 
+  // short-range only: no PM refresh, interpolation or reuse
+  const bool short_only = c.cfg.short_range_only != 0;
+  if (short_only) refresh_long_range_field = 0;
   // cached-field reuse needs a compatible field (tree_pm_coupling.cpp:2483-2532)
-  if (!refresh_long_range_field &&
+  if (!refresh_long_range_field && !short_only &&
       (!c.pm_field_valid || c.pm_field_box[0] != c.cfg.box_x || c.pm_field_box[1] != c.cfg.box_y ||
        c.pm_field_box[2] != c.cfg.box_z)) {
     return chui::fail(c, CHUI_TREEPM_ESTATE, "TreePM long-range reuse requested without a compatible PM field");
@@ -995,7 +999,11 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
       lz = c.out_lr[2].as<double>();
     }
   }
-  if ((rc = chui::pmInterpolate(c, nout, active, tx, ty, tz, x, y, z, pmx, pmy, pmz, s, slice))) return rc;
+  if (short_only) {
+    for (double* p : {pmx, pmy, pmz}) cudaMemsetAsync(p, 0, static_cast<size_t>(nt) * 8, s);
+  } else if ((rc = chui::pmInterpolate(c, nout, active, tx, ty, tz, x, y, z, pmx, pmy, pmz, s, slice))) {
+    return rc;
+  }
   if (nout > 0)
     { chui::noteLaunch(); chui::combineKernel<<<chui::gridFor(nout, 256), 256, 0, s>>>(
           nout, slice, nt, active, explicit_targets ? 0 : n, pmx, pmy, pmz, c.tree_acc.as<double>(),

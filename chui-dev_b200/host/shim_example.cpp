@@ -52,6 +52,28 @@ int main(int argc, char** argv) {
       std::fprintf(stderr, "unexpected diagnostics after a refresh solve\n");
       return 4;
     }
+    // the default walk is the production one (subtree blocks): fewer node
+    // visits than the per-node walk whose counters equal the reference's
+    {
+      cb::TreePmOptions per_node = options;
+      per_node.walk_diagnostics = cb::WalkDiagnostics::kReferenceCounters;
+      std::vector<double> px(n), py(n), pz(n);
+      cb::TreePmForceAccumulatorView pacc{active, px, py, pz};
+      cb::TreePmDiagnostics ref_diag;
+      coordinator.solveActiveSet(x, y, z, m, pacc, per_node, nullptr, &ref_diag);
+      // (pairs: the production set is a superset, up to FP32 rounding at r_cut)
+      const auto& pt = diag.local_traversal;
+      const auto& rt = ref_diag.local_traversal;
+      if (!(pt.visited_nodes < rt.visited_nodes) ||
+          static_cast<double>(pt.direct_pair_evaluations) < 0.999 * static_cast<double>(rt.direct_pair_evaluations)) {
+        std::fprintf(stderr, "the default walk is not the production walk: visits %llu vs %llu, pairs %llu vs %llu\n",
+                     static_cast<unsigned long long>(pt.visited_nodes), static_cast<unsigned long long>(rt.visited_nodes),
+                     static_cast<unsigned long long>(pt.direct_pair_evaluations),
+                     static_cast<unsigned long long>(rt.direct_pair_evaluations));
+        return 7;
+      }
+      coordinator.solveActiveSet(x, y, z, m, acc, options, &profile, &diag);
+    }
     cb::TreePmForceAccumulatorView acc2{active, bx, by, bz};
     coordinator.solveActiveSetWithPmCadence(x, y, z, m, acc2, options, false, nullptr, &diag);
     // the integrator's cadence check (gravity_runtime.cpp:2418-2424)
@@ -68,7 +90,9 @@ int main(int argc, char** argv) {
                                 std::pair<std::size_t, std::size_t>{half, static_cast<std::size_t>(n)}}) {
         std::vector<double> sx(e - b), sy(e - b), sz(e - b);
         cb::TreePmForceAccumulatorView part{active, sx, sy, sz};
-        coordinator.solveVisitRange(x, y, z, m, part, options, false, b, e);
+        // the same walk as the full solve (counted: diagnostics requested)
+        cb::TreePmDiagnostics shard_diag;
+        coordinator.solveVisitRange(x, y, z, m, part, options, false, b, e, nullptr, &shard_diag);
         const std::vector<std::uint32_t> slots = coordinator.visitOrder(b, e);
         for (std::size_t j = 0; j < slots.size(); ++j) worst = std::max(worst, std::fabs(sx[j] - ax[slots[j]]));
       }

@@ -13,6 +13,8 @@
 // std::runtime_error, std::bad_alloc).
 #pragma once
 
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -43,6 +45,11 @@ enum class TreePmAcceptancePolicy { kStrictReference, kAdaptiveRelative };
 enum class TreePmAdaptiveErrorEstimator { kResidualDerivative, kRelativeMonopole };
 enum class TreePmCutoffNodePolicy { kContainNode, kComDistance };
 enum class Precision { kMixed, kFp64 };
+// B200 extension: which walk serves the solve. kAuto: the production walk,
+// counting its own traversal (kProductionCounters) when the caller passes a
+// TreePmDiagnostics, else uncounted (kProduction). kReferenceCounters: the
+// per-node walk whose counters equal the reference's (parity checks).
+enum class WalkDiagnostics { kAuto, kProduction, kReferenceCounters, kProductionCounters };
 
 // The option fields the periodic TreePM path consumes (tree_pm_coupling.hpp:243-332,
 // tree_gravity.hpp:30-43, pm_solver.hpp:223-254, tree_pm_split_kernel.hpp:20-27).
@@ -87,7 +94,9 @@ struct TreePmOptions {
   TreePmCutoffNodePolicy cutoff_node_policy = TreePmCutoffNodePolicy::kContainNode;
   bool group_walk_enabled = false;
   bool gaussian_pair_lookup_enabled = false;
+  bool short_range_only = false;  // the integrator's split operator: residual only, no PM
   Precision precision = Precision::kMixed;  // B200 extension: FP64 runs the same solver in double
+  WalkDiagnostics walk_diagnostics = WalkDiagnostics::kAuto;  // B200 extension
   int device = 0;
 };
 
@@ -110,8 +119,9 @@ struct TreePmForceAccumulatorView {
   std::span<double> short_range_nearest_pair_r2_comoving{};
 };
 
-// The TreePmTraversalCounters fields the periodic strict walk produces
-// (tree_pm_coupling.hpp:39-60); counts are equal to the reference's.
+// The TreePmTraversalCounters fields the walk produces (tree_pm_coupling.hpp:39-60):
+// equal to the reference's with WalkDiagnostics::kReferenceCounters; the
+// production walk's own traversal (subtree blocks) with kProductionCounters.
 struct TreePmTraversalCounters {
   std::uint64_t visited_nodes = 0;
   std::uint64_t accepted_nodes = 0;
@@ -170,8 +180,16 @@ struct TreePmProfileEvent {
   double source_preprocess_ms = 0.0;
 };
 
-// tree_softening.hpp:31-47. Only uniform softening (options) is supported;
-// a non-empty per-particle view is rejected.
+// tree_softening.hpp:26-47: per-particle softening sidecars. Resolved here
+// into the C-ABI's epsilon lanes with the reference's rules
+// (resolveSourceSofteningEpsilon :152-180, targetSofteningEpsilonUnchecked
+// :90-110, sourceSofteningIsProvablyUniform tree_gravity.cpp:82-94).
+struct TreeSofteningSpeciesPolicy {
+  static constexpr std::size_t kSpeciesCapacity = 6;  // core::k_particle_species_count
+  std::array<double, kSpeciesCapacity> epsilon_comoving_by_species{};
+  bool enabled = false;
+};
+
 struct TreeSofteningView {
   std::span<const std::uint32_t> source_species_tag{};
   std::span<const double> source_particle_epsilon_comoving{};
@@ -179,12 +197,76 @@ struct TreeSofteningView {
   std::span<const std::uint32_t> target_species_tag{};
   std::span<const double> target_particle_epsilon_comoving{};
   std::span<const std::uint8_t> target_particle_epsilon_override_mask{};
-  [[nodiscard]] bool empty() const noexcept {
-    return source_species_tag.empty() && source_particle_epsilon_comoving.empty() &&
-           source_particle_epsilon_override_mask.empty() && target_species_tag.empty() &&
-           target_particle_epsilon_comoving.empty() && target_particle_epsilon_override_mask.empty();
-  }
+  TreeSofteningSpeciesPolicy species_policy{};
 };
+
+namespace softening_detail {
+
+inline double validated(double v, const char* what) {
+  if (!std::isfinite(v) || v < 0.0) throw std::invalid_argument(std::string(what) + " must be finite and non-negative");
+  return v;
+}
+
+inline double speciesEpsilon(const TreeSofteningSpeciesPolicy& p, std::uint32_t tag, const char* what) {
+  if (tag >= p.epsilon_comoving_by_species.size())
+    throw std::invalid_argument("species tag is outside the canonical species range");
+  return validated(p.epsilon_comoving_by_species[tag], what);
+}
+
+// Per-source epsilons, or empty when the sources are provably uniform.
+inline std::vector<double> resolveSources(std::size_t n, double fallback, const TreeSofteningView& v) {
+  const bool species = v.species_policy.enabled && !v.source_species_tag.empty();
+  if (v.source_particle_epsilon_comoving.empty() && v.source_particle_epsilon_override_mask.empty() && !species)
+    return {};
+  if ((!v.source_particle_epsilon_comoving.empty() && v.source_particle_epsilon_comoving.size() != n) ||
+      (!v.source_particle_epsilon_override_mask.empty() && v.source_particle_epsilon_override_mask.size() != n) ||
+      (!v.source_species_tag.empty() && v.source_species_tag.size() != n))
+    throw std::invalid_argument("TreePM softening/species sidecar extent mismatch");
+  std::vector<double> eps(n, validated(fallback, "Tree softening epsilon_comoving"));
+  for (std::size_t i = 0; i < n; ++i) {
+    if (!v.source_particle_epsilon_comoving.empty() && !v.source_particle_epsilon_override_mask.empty() &&
+        v.source_particle_epsilon_override_mask[i] != 0U) {
+      eps[i] = validated(v.source_particle_epsilon_comoving[i], "source softening override");
+    } else if (species) {
+      eps[i] = speciesEpsilon(v.species_policy, v.source_species_tag[i], "source species softening");
+    }
+  }
+  return eps;
+}
+
+// Per-active-slot target epsilons, or empty when the library's default (a
+// target that is a source takes its source epsilon, others the configured
+// one) gives the same values.
+inline std::vector<double> resolveTargets(std::span<const std::uint32_t> rows, std::size_t sources,
+                                          const std::vector<double>& source_eps, double fallback,
+                                          const TreeSofteningView& v) {
+  const bool target_species = v.species_policy.enabled && !v.target_species_tag.empty();
+  if (v.target_particle_epsilon_comoving.empty() && !target_species) return {};
+  const std::size_t nt = rows.size();
+  if ((!v.target_particle_epsilon_comoving.empty() && v.target_particle_epsilon_comoving.size() != nt) ||
+      (!v.target_particle_epsilon_override_mask.empty() && v.target_particle_epsilon_override_mask.size() != nt) ||
+      (!v.target_species_tag.empty() && v.target_species_tag.size() != nt))
+    throw std::invalid_argument("TreePM softening/species sidecar extent mismatch");
+  std::vector<double> eps(nt);
+  for (std::size_t k = 0; k < nt; ++k) {
+    const std::size_t row = rows[k];
+    if (!v.target_particle_epsilon_comoving.empty() && !v.target_particle_epsilon_override_mask.empty() &&
+        v.target_particle_epsilon_override_mask[k] != 0U) {
+      eps[k] = validated(v.target_particle_epsilon_comoving[k], "target softening override");
+    } else if (target_species) {
+      eps[k] = speciesEpsilon(v.species_policy, v.target_species_tag[k], "target species softening");
+    } else if (v.target_particle_epsilon_comoving.empty() && row < sources) {
+      eps[k] = source_eps.empty() ? fallback : source_eps[row];
+    } else if (v.species_policy.enabled && row < v.source_species_tag.size()) {
+      eps[k] = speciesEpsilon(v.species_policy, v.source_species_tag[row], "target species softening");
+    } else {
+      eps[k] = fallback;
+    }
+  }
+  return eps;
+}
+
+}  // namespace softening_detail
 
 class TreePmCoordinator {
  public:
@@ -243,9 +325,6 @@ class TreePmCoordinator {
              const TreePmForceAccumulatorView& accumulator, const TreePmOptions& options,
              bool refresh_long_range_field, TreePmProfileEvent* profile, TreePmDiagnostics* diagnostics,
              const TreeSofteningView& softening_view, bool ranged, std::size_t visit_begin, std::size_t visit_end) {
-    if (!softening_view.empty()) {
-      throw std::invalid_argument("B200 TreePM supports uniform softening only (per-particle softening view given)");
-    }
     if (pos_x_comoving.size() != pos_y_comoving.size() || pos_x_comoving.size() != pos_z_comoving.size() ||
         pos_x_comoving.size() != mass_code.size()) {
       throw std::invalid_argument("TreePM requires position and mass spans with equal extent");
@@ -260,19 +339,26 @@ class TreePmCoordinator {
         accumulator.previous_acceleration_magnitude_code.size() != targets) {
       throw std::invalid_argument("TreePM force accumulator spans must have matching active-set extent");
     }
-    configure(options);
+    configure(options, diagnostics != nullptr);
+    // per-particle softening: resolved epsilon lanes
+    const double eps0 = options.tree_options.softening.epsilon_comoving;
+    m_source_eps = softening_detail::resolveSources(pos_x_comoving.size(), eps0, softening_view);
+    m_target_eps = softening_detail::resolveTargets(accumulator.active_particle_index, pos_x_comoving.size(),
+                                                    m_source_eps, eps0, softening_view);
     chui_treepm_sources src{};
     src.count = static_cast<std::int64_t>(pos_x_comoving.size());
     src.x = pos_x_comoving.data();
     src.y = pos_y_comoving.data();
     src.z = pos_z_comoving.data();
     src.mass = mass_code.data();
+    src.softening = m_source_eps.empty() ? nullptr : m_source_eps.data();
     chui_treepm_accumulator acc{};
     acc.active_count = static_cast<std::int64_t>(targets);
     acc.active_index = accumulator.active_particle_index.data();
     acc.accel_x = accumulator.accel_x_comoving.data();
     acc.accel_y = accumulator.accel_y_comoving.data();
     acc.accel_z = accumulator.accel_z_comoving.data();
+    acc.target_softening = m_target_eps.empty() ? nullptr : m_target_eps.data();
     if (!accumulator.previous_acceleration_magnitude_code.empty()) {
       acc.previous_acceleration_magnitude = accumulator.previous_acceleration_magnitude_code.data();
     }
@@ -355,8 +441,9 @@ class TreePmCoordinator {
     d.local_source_count = sources;
     d.local_active_target_count = targets;
     d.local_tree_node_count = s.node_count;
-    d.pm_solve_count = refresh ? 1U : 0U;
-    d.pm_reuse_count = refresh ? 0U : 1U;
+    // short-range only: neither a PM solve nor a reuse (gravity_runtime.cpp:2418-2424)
+    d.pm_solve_count = refresh && !m_short_only ? 1U : 0U;
+    d.pm_reuse_count = refresh || m_short_only ? 0U : 1U;
     d.mesh_spacing_comoving = m_spacing;
     d.asmth_cells = m_asmth;
     d.rcut_cells = m_rcut;
@@ -368,7 +455,7 @@ class TreePmCoordinator {
     d.local_pair_evaluations = s.direct_pair_evaluations;
   }
 
-  void configure(const TreePmOptions& o) {
+  void configure(const TreePmOptions& o, bool counters_wanted) {
     chui_treepm_config c{};
     chui_treepm_config_default(&c);
     c.pm_grid_nx = static_cast<std::int64_t>(m_shape.nx);
@@ -408,6 +495,14 @@ class TreePmCoordinator {
     c.group_walk_enabled = o.group_walk_enabled ? 1 : 0;
     c.gaussian_pair_lookup = o.gaussian_pair_lookup_enabled ? 1 : 0;
     c.precision = o.precision == Precision::kFp64 ? CHUI_TREEPM_FP64 : CHUI_TREEPM_MIXED;
+    c.short_range_only = o.short_range_only ? 1 : 0;
+    m_short_only = o.short_range_only;
+    switch (o.walk_diagnostics) {
+      case WalkDiagnostics::kAuto: c.diagnostics = counters_wanted ? 2 : 0; break;
+      case WalkDiagnostics::kProduction: c.diagnostics = 0; break;
+      case WalkDiagnostics::kReferenceCounters: c.diagnostics = 1; break;
+      case WalkDiagnostics::kProductionCounters: c.diagnostics = 2; break;
+    }
     c.device = o.device;
     // split scale and cutoff are in units of the mean mesh spacing (gravity_runtime.cpp:586-590)
     m_spacing = std::cbrt((c.box_x / c.pm_grid_nx) * (c.box_y / c.pm_grid_ny) * (c.box_z / c.pm_grid_nz));
@@ -441,6 +536,8 @@ class TreePmCoordinator {
 
   PmGridShape m_shape;
   void* m_handle = nullptr;
+  std::vector<double> m_source_eps, m_target_eps;
+  bool m_short_only = false;
   double m_spacing = 0.0;
   double m_asmth = 0.0;
   double m_rcut = 0.0;

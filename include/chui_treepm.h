@@ -100,6 +100,10 @@ typedef struct {
    * on the caller's coordinates and no periodic images in the walk. The
    * adjoint entry points support periodic boundaries only. */
   int32_t boundary_condition;
+  /* TreePmOptions::short_range_only (tree_pm_coupling.hpp:289-292): the
+   * integrator's split operator -- only the short-range residual force, no PM
+   * refresh, interpolation or reuse (long-range lanes are zero). */
+  int32_t short_range_only;
 } chui_treepm_config;
 
 /* Counters named as TreePmTraversalCounters (tree_pm_coupling.hpp:39-87) plus

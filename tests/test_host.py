@@ -210,3 +210,28 @@ def test_cpp_shim_compiles_and_links(tmp_path):
     subprocess.run(["g++", "-std=c++20", "-O1", "-Wall", "-Werror", os.path.join(host, "shim_example.cpp"),
                     f"-L{build}", "-lchui_treepm", "-o", str(exe)], check=True)
     assert exe.exists()
+
+
+def test_cosmosim_adapter_compiles_against_the_reference_headers(tmp_path):
+    """The coordinator over the reference's own types
+    (chui-dev_b200/host/cosmosim_tree_pm_coordinator.hpp) and an example that
+    calls solveActiveSetWithPmCadence the way GravityRuntimeImpl does
+    (gravity_runtime.cpp:2383-2424) compile against the reference's headers,
+    warning-free in their own code, and link against libchui_treepm.so alone.
+    Needs the reference checkout (CHUI_REFERENCE); running it needs a GPU
+    (tests/test_gpu_cpp_shim.py)."""
+    import shutil
+    import subprocess
+    import sys
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as ge
+    ref = os.environ.get("CHUI_REFERENCE", ge.REFERENCE)
+    if shutil.which("g++") is None or not os.path.isfile(
+            os.path.join(ref, "include", "cosmosim", "gravity", "tree_pm_coupling.hpp")):
+        pytest.skip("reference headers not present")
+    exe = tmp_path / "cosmosim_example"
+    r = subprocess.run(ge.cosmosim_example_command(ref, str(exe)), capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    own = [ln for ln in r.stderr.splitlines() if "warning" in ln and "chui-dev_b200/host" in ln]
+    assert not own, own
+    assert exe.exists()
