@@ -7,10 +7,11 @@ from . import _abi, softening
 from .config import config_from_param_file, config_from_param_text
 from .sharded import ShardedTreePm
 from .solver import (AllocationError, DeviceError, InvalidArgument, NotSupported, OutOfRange, StateError,
-                     TreePmConfig, TreePmCoordinator, TreePmError, kdk_factors_static, probe_fp32_peak_tflops)
+                     TreePmConfig, TreePmCoordinator, TreePmError, kdk_factors_lcdm, kdk_factors_static,
+                     probe_fp32_peak_tflops)
 
 __all__ = [
     "TreePmConfig", "TreePmCoordinator", "TreePmError", "InvalidArgument", "OutOfRange", "StateError",
     "DeviceError", "AllocationError", "NotSupported", "config_from_param_file", "config_from_param_text",
-    "kdk_factors_static", "probe_fp32_peak_tflops", "ShardedTreePm", "_abi", "softening",
+    "kdk_factors_static", "kdk_factors_lcdm", "probe_fp32_peak_tflops", "ShardedTreePm", "_abi", "softening",
 ]

@@ -510,3 +510,28 @@ def kdk_factors_static(dt: float):
     if rc != 0:
         raise InvalidArgument(rc, "dt must be finite and positive")
     return tuple(float(v) for v in f)
+
+
+def kdk_factors_lcdm(scale_factor: float, dt: float, hubble_param: float = 0.674, omega_matter: float = 0.315,
+                     omega_lambda: float = 0.685, omega_radiation: float = 0.0, omega_curvature: float = 0.0,
+                     time_si_per_code: float = 3.0856775814913673e17) -> dict:
+    """CosmologicalTimeline::prepareStep with a Lambda-CDM background
+    (chui_treepm_kdk_factors_lcdm): the KDK factors of one step of dt (code
+    time) from scale_factor. `factors` = (D, K1, K2, drag1, drag2) for the
+    kick/drift calls; the rest are the source-kick factors and the midpoint
+    and end scale factors."""
+    class _Cosmo(C.Structure):
+        _fields_ = [(k, C.c_double) for k in ("hubble_param", "omega_matter", "omega_lambda", "omega_radiation",
+                                               "omega_curvature", "time_si_per_code")]
+    c = _Cosmo(hubble_param, omega_matter, omega_lambda, omega_radiation, omega_curvature, time_si_per_code)
+    f = np.zeros(10)
+    rc = _abi.load().chui_treepm_kdk_factors_lcdm(C.byref(c), scale_factor, dt, f.ctypes.data)
+    if rc == _abi.EINVAL:
+        raise InvalidArgument(rc, "invalid background, scale factor or step")
+    if rc != 0:
+        raise OutOfRange(rc, "scale-factor advance could not be bracketed")
+    keys = ("drift", "kick1", "kick2", "drag1", "drag2", "source_kick1", "source_kick2", "a_midpoint", "a_end",
+            "drag")
+    out = {k: float(v) for k, v in zip(keys, f)}
+    out["factors"] = tuple(float(v) for v in f[:5])
+    return out

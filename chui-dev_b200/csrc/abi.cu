@@ -576,6 +576,60 @@ namespace {
 thread_local std::string g_create_error;
 }  // namespace
 
+// ---- Lambda-CDM step factors (host) ----
+namespace lcdm {
+
+// H(a) in s^-1 for the background (LambdaCdmBackground::hubbleSi without
+// radiation species).
+struct Background {
+  double h0_si, om, ol, orad, ok;
+  double hubble(double a) const {
+    const double a2 = a * a, a3 = a2 * a, a4 = a2 * a2;
+    return h0_si * std::sqrt(orad / a4 + om / a3 + ok / a2 + ol);
+  }
+};
+
+// Midpoint rule over [a0, a1] with `samples` cells of integrand(a_mid).
+template <class F>
+double midpoint(double a0, double a1, unsigned samples, F integrand) {
+  const double da = (a1 - a0) / static_cast<double>(samples);
+  if (da == 0.0) return 0.0;
+  double sum = 0.0;
+  for (unsigned i = 0; i < samples; ++i) sum += integrand(a0 + (static_cast<double>(i) + 0.5) * da);
+  return sum * da;
+}
+
+// Cosmic time from a0 to a1: integral da / (a H).
+double cosmicTime(const Background& b, double a0, double a1, unsigned samples) {
+  return midpoint(a0, a1, samples, [&](double a) { return 1.0 / (a * b.hubble(a)); });
+}
+
+// Scale factor after dt seconds from a0: bracket by doubling, then bisect.
+int advanceScaleFactor(const Background& b, double a0, double dt_si, double* out) {
+  if (dt_si == 0.0) {
+    *out = a0;
+    return 0;
+  }
+  constexpr unsigned kSamples = 64;
+  double hi = a0 * 1.001;
+  if (hi <= a0) hi = a0 + 1.0e-12;
+  for (int iter = 0; iter < 256 && cosmicTime(b, a0, hi, kSamples) < dt_si; ++iter) {
+    hi *= 2.0;
+    if (!std::isfinite(hi) || hi > 1.0e12) return CHUI_TREEPM_ERANGE;
+  }
+  if (cosmicTime(b, a0, hi, kSamples) < dt_si) return CHUI_TREEPM_ERANGE;
+  double lo = a0;
+  for (int iter = 0; iter < 96; ++iter) {
+    const double mid = 0.5 * (lo + hi);
+    if (cosmicTime(b, a0, mid, kSamples) < dt_si) lo = mid;
+    else hi = mid;
+  }
+  *out = 0.5 * (lo + hi);
+  return 0;
+}
+
+}  // namespace lcdm
+
 extern "C" {
 
 int chui_treepm_config_default(chui_treepm_config* cfg) {
@@ -702,6 +756,50 @@ int chui_treepm_set_config(void* handle, const chui_treepm_config* cfg) {
 const char* chui_treepm_last_error(const void* handle) {
   if (!handle) return g_create_error.c_str();
   return static_cast<const Context*>(handle)->last_error.c_str();
+}
+
+int chui_treepm_kdk_factors_lcdm(const chui_treepm_cosmology* cosmo, double a, double dt, double factors[10]) {
+  if (!cosmo || !factors) return CHUI_TREEPM_EINVAL;
+  const chui_treepm_cosmology& c = *cosmo;
+  const double dens[4] = {c.omega_matter, c.omega_lambda, c.omega_radiation, c.omega_curvature};
+  for (double d : dens)
+    if (!std::isfinite(d)) return CHUI_TREEPM_EINVAL;
+  if (!(std::isfinite(c.hubble_param) && c.hubble_param > 0.0) || c.omega_matter < 0.0 || c.omega_lambda < 0.0 ||
+      c.omega_radiation < 0.0 ||
+      std::fabs(c.omega_matter + c.omega_lambda + c.omega_radiation + c.omega_curvature - 1.0) > 1.0e-10 ||
+      !(std::isfinite(c.time_si_per_code) && c.time_si_per_code > 0.0) || !(std::isfinite(a) && a > 0.0) ||
+      !(std::isfinite(dt) && dt > 0.0))
+    return CHUI_TREEPM_EINVAL;
+  // 100 km/s/Mpc in s^-1 (1 pc = 3.0856775814913673e16 m)
+  const double h100_si = (100.0 * 1.0e3) / (1.0e6 * 3.0856775814913673e16);
+  const lcdm::Background b{c.hubble_param * h100_si, c.omega_matter, c.omega_lambda, c.omega_radiation,
+                     c.omega_curvature};
+  const double dt_si = dt * c.time_si_per_code;
+  double a_mid = 0.0, a_end = 0.0;
+  int rc = lcdm::advanceScaleFactor(b, a, 0.5 * dt_si, &a_mid);
+  if (!rc) rc = lcdm::advanceScaleFactor(b, a, dt_si, &a_end);
+  if (rc) return rc;
+  constexpr unsigned kSamples = 64;
+  // integral dt / a = integral da / (a^2 H); kick factors divide by the end scale factor
+  const auto drift_like = [&](double a0, double a1) {
+    return lcdm::midpoint(a0, a1, kSamples, [&](double x) { return 1.0 / (x * x * b.hubble(x)); });
+  };
+  const auto source_like = [&](double a0, double a1) {
+    return lcdm::midpoint(a0, a1, kSamples, [&](double x) { return 1.0 / (x * x * x * b.hubble(x)); });
+  };
+  factors[0] = drift_like(a, a_end) / c.time_si_per_code;
+  factors[1] = drift_like(a, a_mid) / a_mid / c.time_si_per_code;
+  factors[2] = drift_like(a_mid, a_end) / a_end / c.time_si_per_code;
+  factors[3] = a / a_mid;
+  factors[4] = a_mid / a_end;
+  factors[5] = source_like(a, a_mid) / c.time_si_per_code;
+  factors[6] = source_like(a_mid, a_end) / c.time_si_per_code;
+  factors[7] = a_mid;
+  factors[8] = a_end;
+  factors[9] = a / a_end;
+  for (int k = 0; k < 10; ++k)
+    if (!std::isfinite(factors[k])) return CHUI_TREEPM_ERANGE;
+  return 0;
 }
 
 int chui_treepm_kdk_factors_static(double dt, double factors[5]) {

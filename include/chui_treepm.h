@@ -301,6 +301,28 @@ int chui_treepm_drift(void *handle, int64_t n, double *x, double *y, double *z,
  * drag = 1. factors = {drift, kick1, kick2, drag1, drag2}. */
 int chui_treepm_kdk_factors_static(double dt, double factors[5]);
 
+/* Flat or curved Lambda-CDM background without radiation species
+ * (CosmologyBackgroundConfig, include/cosmosim/core/cosmology.hpp:49-56):
+ * E(a)^2 = Omega_r a^-4 + Omega_m a^-3 + Omega_k a^-2 + Omega_Lambda, the
+ * densities summing to 1 within 1e-10; H0 = h x 100 km/s/Mpc. */
+typedef struct {
+  double hubble_param;
+  double omega_matter, omega_lambda, omega_radiation, omega_curvature;
+  double time_si_per_code; /* seconds per code time unit */
+} chui_treepm_cosmology;
+
+/* Cosmological KDK factors of one step of dt_code from scale factor a
+ * (CosmologicalTimeline::prepareStep with a background,
+ * src/core/time_integration.cpp:409-458; the factors of
+ * computeComovingDriftFactor / KickFactor / SourceKickFactor /
+ * HubbleDragFactor, :3530-3595, as 64-sample midpoint integrals over a; the
+ * midpoint and end scale factors by advanceScaleFactorByCosmicTime,
+ * :3469-3517). factors = {drift, kick1, kick2, drag1, drag2, source_kick1,
+ * source_kick2, a_midpoint, a_end, drag (whole step)}: the kick and drift of
+ * chui_treepm_kick / chui_treepm_drift take factors[0..4]. */
+int chui_treepm_kdk_factors_lcdm(const chui_treepm_cosmology *cosmology, double scale_factor, double dt_code,
+                                 double factors[10]);
+
 /* Global FP64 momentum and energy checks over n particles: out = {sum m v_x,
  * sum m v_y, sum m v_z, sum m a_x, sum m a_y, sum m a_z, sum m |v|^2 / 2,
  * sum m}. mass may be NULL (uniform_mass); a_* may all be NULL. Reductions run

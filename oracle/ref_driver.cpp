@@ -25,7 +25,9 @@
 #include <string>
 #include <vector>
 
+#include "cosmosim/core/cosmology.hpp"
 #include "cosmosim/core/periodic_domain.hpp"
+#include "cosmosim/core/time_integration.hpp"
 #include "cosmosim/gravity/pm_solver.hpp"
 #include "cosmosim/gravity/tree_pm_coupling.hpp"
 #include "support/periodic_ewald_reference.hpp"
@@ -226,7 +228,35 @@ cg::TreePmOptions makeOptions(const Problem& p) {
   return o;
 }
 
+// --kdk-factors h omega_m omega_lambda omega_r omega_k time_si_per_code a dt:
+// the reference's CosmologicalTimeline::prepareStep factors, one per line.
+int kdkFactors(char** argv) {
+  cosmosim::core::CosmologyBackgroundConfig cfg;
+  cfg.hubble_param = std::stod(argv[2]);
+  cfg.omega_matter = std::stod(argv[3]);
+  cfg.omega_lambda = std::stod(argv[4]);
+  cfg.omega_radiation = std::stod(argv[5]);
+  cfg.omega_curvature = std::stod(argv[6]);
+  const cosmosim::core::LambdaCdmBackground background(cfg);
+  const cosmosim::core::CosmologicalTimeline timeline(&background, std::stod(argv[7]));
+  const auto st = timeline.prepareStep(0.0, std::stod(argv[8]), std::stod(argv[9]));
+  const double v[10] = {st.drift_factor_code, st.first_kick_factor_code, st.second_kick_factor_code,
+                        st.first_hubble_drag_factor, st.second_hubble_drag_factor, st.first_source_kick_factor_code,
+                        st.second_source_kick_factor_code, st.scale_factor_midpoint, st.scale_factor_end,
+                        st.hubble_drag_factor};
+  for (double x : v) std::printf("%.17g\n", x);
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 10 && std::strcmp(argv[1], "--kdk-factors") == 0) {
+    try {
+      return kdkFactors(argv);
+    } catch (const std::exception& e) {
+      std::fprintf(stderr, "treepm_ref error: %s\n", e.what());
+      return 1;
+    }
+  }
   if (argc != 3) {
     std::fprintf(stderr, "usage: treepm_ref <input.bin> <output.bin>\n");
     return 2;

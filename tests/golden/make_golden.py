@@ -239,5 +239,27 @@ def main():
          extra={"src_eps": src_eps, "src_mask": src_mask, "tgt_eps": tgt_eps, "tgt_mask": tgt_mask})
 
 
+def kdk_factors():
+    """The reference's CosmologicalTimeline::prepareStep factors for several
+    backgrounds, scale factors and steps (flat LCDM, an open model with
+    radiation, matter only), from the reference driver's --kdk-factors mode."""
+    import subprocess
+    if ONLY and "kdk_factors" not in ONLY:
+        return
+    cosmos = [(0.674, 0.315, 0.685, 0.0, 0.0), (0.7, 0.25, 0.7, 1e-4, 0.0499), (0.5, 1.0, 0.0, 0.0, 0.0)]
+    steps = [(0.02, 1e-3), (0.1, 0.02), (0.5, 0.01), (1.0, 0.05), (0.9, 1e-6)]
+    tspc = 3.0856775814913673e17  # seconds per code time unit (a kpc/(km/s) unit system)
+    rows, out = [], []
+    for c in cosmos:
+        for a, dt in steps:
+            r = subprocess.run([refio.binary(), "--kdk-factors", *(repr(v) for v in c), repr(tspc), repr(a), repr(dt)],
+                               check=True, capture_output=True, text=True)
+            rows.append(list(c) + [tspc, a, dt])
+            out.append([float(v) for v in r.stdout.split()])
+    np.savez_compressed(os.path.join(OUT, "kdk_factors.npz"), inputs=np.array(rows), factors=np.array(out))
+    print("kdk_factors", len(rows))
+
+
 if __name__ == "__main__":
     main()
+    kdk_factors()

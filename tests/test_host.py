@@ -235,3 +235,22 @@ def test_cosmosim_adapter_compiles_against_the_reference_headers(tmp_path):
     own = [ln for ln in r.stderr.splitlines() if "warning" in ln and "chui-dev_b200/host" in ln]
     assert not own, own
     assert exe.exists()
+
+
+def test_lcdm_kdk_factors_match_reference():
+    """chui_treepm_kdk_factors_lcdm against the reference's
+    CosmologicalTimeline::prepareStep (tests/golden/kdk_factors.npz, from the
+    reference built here): three backgrounds, scale factors 0.02-1, steps
+    1e-6-0.05."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "kdk_factors.npz"))
+    for row, ref in zip(g["inputs"], g["factors"]):
+        h, om, ol, orad, ok, tspc, a, dt = (float(v) for v in row)
+        f = ct.kdk_factors_lcdm(a, dt, hubble_param=h, omega_matter=om, omega_lambda=ol, omega_radiation=orad,
+                                omega_curvature=ok, time_si_per_code=tspc)
+        got = [f[k] for k in ("drift", "kick1", "kick2", "drag1", "drag2", "source_kick1", "source_kick2",
+                              "a_midpoint", "a_end", "drag")]
+        np.testing.assert_allclose(got, ref, rtol=1e-13, atol=0.0)
+    with pytest.raises(ct.InvalidArgument):
+        ct.kdk_factors_lcdm(0.5, 0.01, omega_matter=0.3, omega_lambda=0.6)  # densities do not sum to 1
+    with pytest.raises(ct.InvalidArgument):
+        ct.kdk_factors_lcdm(-1.0, 0.01)
