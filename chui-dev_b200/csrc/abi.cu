@@ -3,7 +3,6 @@
 // and the orchestration of one solve (TreePmCoordinator::solveActiveSetWithPmCadence,
 // tree_pm_coupling.cpp:2282-3518): PM refresh -> periodic tree build ->
 // residual walk -> PM interpolation -> accumulation.
-#include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -715,7 +714,8 @@ void chui_treepm_destroy(void* handle) {
                             &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max,
                             &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
                             &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
-                            &c->leaf_of_pos, &c->inv_pos, &c->cub_temp, &c->node_geom, &c->node_com,
+                            &c->leaf_of_pos, &c->inv_pos, &c->sort_hist, &c->sort_counts,
+                            &c->sort_totals, &c->sort_keys, &c->sort_vals, &c->node_geom, &c->node_com,
                             &c->node_quad, &c->node_f4, &c->node_mq, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
                             &c->node_counter, &c->sorted_index, &c->pos_of_row, &c->src_f4, &c->src_d4, &c->src_u4, &c->src_cot,
                             &c->target_order, &c->morton_sorted, &c->walk_counters, &c->work_counter,

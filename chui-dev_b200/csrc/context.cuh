@@ -115,7 +115,8 @@ struct Context {
   DevBuf common_prefix;          // int8/int32 per sorted position
   DevBuf node_count_per_pos, node_offset;  // per sorted position (n+1)
   DevBuf leaf_of_pos, inv_pos;
-  DevBuf cub_temp;
+  // radix sort and scan scratch (sort.cu)
+  DevBuf sort_hist, sort_counts, sort_totals, sort_keys, sort_vals;
   int64_t n_nodes = 0;
   uint32_t max_depth = 0;
   int path_words_used = 0;
@@ -194,6 +195,20 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
 int treeNodeBounds(Context& c, double lo[3], double hi[3], cudaStream_t s);
 int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explicit_targets, int64_t n,
                      cudaStream_t s);
+
+// ---- sort and scan (sort.cu) ----
+// Stable LSD radix sorts by the low end_bit bits (8-bit digits; digits equal
+// for every key are skipped); kin and kout must differ.
+int radixSortPairsU64(Context& c, const unsigned long long* kin, unsigned long long* kout, const uint32_t* vin,
+                      uint32_t* vout, int64_t n, int end_bit, cudaStream_t s);
+// batch (<= 3) independent keys-only sorts of n keys each, in the same launches
+int radixSortKeysU64(Context& c, int batch, const unsigned long long* const* kin, unsigned long long* const* kout,
+                     int64_t n, int end_bit, cudaStream_t s);
+int radixSortPairsU32(Context& c, const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout,
+                      int64_t n, int end_bit, cudaStream_t s);
+int exclusiveScanU32(Context& c, const uint32_t* in, uint32_t* out, int64_t n, cudaStream_t s);
+// Maximum of n values, returned to the host (synchronises the stream).
+int maxU32(Context& c, const uint32_t* in, int64_t n, uint32_t* result, cudaStream_t s);
 
 // ---- walk (walk.cu) ----
 // Targets are the visit positions [visit_begin, visit_end) of the nt targets

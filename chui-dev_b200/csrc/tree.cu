@@ -21,7 +21,6 @@
 //  5. stable sort of Morton order by leaf id gives the final particle order;
 //  6. FP64 multipoles bottom-up, each parent reduced once, children in octant
 //     order, by the last child to finish.
-#include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -763,28 +762,6 @@ __global__ void iotaKernel(int64_t n, uint32_t* v) {
   }
 }
 
-int cubSortPairsU64(Context& c, const unsigned long long* kin, unsigned long long* kout,
-                    const uint32_t* vin, uint32_t* vout, int64_t n, int end_bit, cudaStream_t s) {
-  size_t bytes = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, static_cast<int>(n), 0, end_bit, s);
-  if (ensure(c.cub_temp, bytes) != cudaSuccess) return CHUI_TREEPM_ENOMEM;
-  if (cub::DeviceRadixSort::SortPairs(c.cub_temp.ptr, bytes, kin, kout, vin, vout, static_cast<int>(n), 0,
-                                      end_bit, s) != cudaSuccess)
-    return CHUI_TREEPM_EDEVICE;
-  return 0;
-}
-
-int cubSortPairsU32(Context& c, const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout,
-                    int64_t n, int end_bit, cudaStream_t s) {
-  size_t bytes = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, static_cast<int>(n), 0, end_bit, s);
-  if (ensure(c.cub_temp, bytes) != cudaSuccess) return CHUI_TREEPM_ENOMEM;
-  if (cub::DeviceRadixSort::SortPairs(c.cub_temp.ptr, bytes, kin, kout, vin, vout, static_cast<int>(n), 0,
-                                      end_bit, s) != cudaSuccess)
-    return CHUI_TREEPM_EDEVICE;
-  return 0;
-}
-
 int bitsFor(uint64_t maxval) {
   int b = 1;
   while (b < 32 && (1ull << b) <= maxval) ++b;
@@ -793,35 +770,42 @@ int bitsFor(uint64_t maxval) {
 
 }  // namespace
 
-// Unwrap one axis into `out` (tree frame), returning the anchor.
-static int unwrapAxis(Context& c, int64_t n, const double* in, double box, int canonical, double* out,
-                      double* anchor, cudaStream_t s) {
-  if (n == 0) {
-    *anchor = 0.0;
+// Unwrap the axes into `out` (tree frame), returning each axis's anchor: the
+// canonical coordinates of all axes are sorted together (one batched radix
+// sort), then each axis finds its largest circular gap.
+static int unwrapAxes(Context& c, int64_t n, int axes, const int* axis, const double* const* in, const double* box,
+                      const int* canonical, double* const* out, double* anchor, cudaStream_t s) {
+  if (n == 0 || axes == 0) {
+    for (int k = 0; k < axes; ++k) anchor[axis[k]] = 0.0;
     return 0;
   }
-  if (ensure(c.bucket_min, static_cast<size_t>(n) * 8) || ensure(c.bucket_max, static_cast<size_t>(n) * 8))
+  if (ensure(c.bucket_min, static_cast<size_t>(axes) * n * 8) || ensure(c.bucket_max, static_cast<size_t>(axes) * n * 8))
     return CHUI_TREEPM_ENOMEM;
-  auto* keys = c.bucket_min.as<unsigned long long>();
-  auto* sorted = c.bucket_max.as<unsigned long long>();
-  { noteLaunch(); canonicalKeysKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in, box, canonical, out, keys); }
+  const unsigned long long* keys[3];
+  unsigned long long* sorted[3];
+  for (int k = 0; k < axes; ++k) {
+    const int a = axis[k];
+    auto* kk = c.bucket_min.as<unsigned long long>() + static_cast<size_t>(k) * n;
+    keys[k] = kk;
+    sorted[k] = c.bucket_max.as<unsigned long long>() + static_cast<size_t>(k) * n;
+    { noteLaunch(); canonicalKeysKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in[a], box[a], canonical[a], out[a], kk); }
+  }
   // canonical coordinates are non-negative: bit 63 is zero
-  size_t bytes = 0;
-  cub::DeviceRadixSort::SortKeys(nullptr, bytes, keys, sorted, static_cast<int>(n), 0, 63, s);
-  if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
-  if (cub::DeviceRadixSort::SortKeys(c.cub_temp.ptr, bytes, keys, sorted, static_cast<int>(n), 0, 63, s) !=
-      cudaSuccess)
-    return CHUI_TREEPM_EDEVICE;
+  if (int rc = radixSortKeysU64(c, axes, keys, sorted, n, 63, s)) return rc;
   auto* sc = c.scalars.as<unsigned long long>();
-  unsigned long long init[2] = {0ull, ~0ull};
-  cudaMemcpyAsync(sc, init, 16, cudaMemcpyHostToDevice, s);
-  { noteLaunch(); sortedGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, sorted, box, sc, 0, sc + 1); }
-  { noteLaunch(); sortedGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, sorted, box, sc, 1, sc + 1); }
-  { noteLaunch(); applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out, box, sc + 1); }
-  unsigned long long ab = 0;
-  cudaMemcpyAsync(&ab, sc + 1, 8, cudaMemcpyDeviceToHost, s);
-  cudaStreamSynchronize(s);
-  std::memcpy(anchor, &ab, 8);
+  unsigned long long init[6] = {0ull, ~0ull, 0ull, ~0ull, 0ull, ~0ull};
+  cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  for (int k = 0; k < axes; ++k) {
+    const int a = axis[k];
+    unsigned long long* g = sc + 2 * k;
+    { noteLaunch(); sortedGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, sorted[k], box[a], g, 0, g + 1); }
+    { noteLaunch(); sortedGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, sorted[k], box[a], g, 1, g + 1); }
+    { noteLaunch(); applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out[a], box[a], g + 1); }
+  }
+  unsigned long long ab[6];
+  cudaMemcpyAsync(ab, sc, sizeof(ab), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  for (int k = 0; k < axes; ++k) std::memcpy(&anchor[axis[k]], &ab[2 * k + 1], 8);
   return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
 }
 
@@ -838,20 +822,21 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   double anchors[3];
   FrameSpec frame;
   frame.periodic = c.cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_PERIODIC ? 1 : 0;
+  int canonical[3], axis[3], axes = 0;
   for (int a = 0; a < 3; ++a) {
     frame.box[a] = box[a];
-    frame.canonical[a] = src_lo[a] >= 0.0 && src_hi[a] < box[a];
+    // canonical flag as tree_pm_coupling.cpp:3183-3194
+    canonical[a] = src_lo[a] >= 0.0 && src_hi[a] < box[a];
+    frame.canonical[a] = canonical[a];
     if (c.cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC) {
       // isolated/open: the tree takes the caller's coordinates (tree_pm_coupling.cpp:3179-3196)
       cudaMemcpyAsync(u[a], in[a], static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
       anchors[a] = 0.0;
       continue;
     }
-    // canonical flag as tree_pm_coupling.cpp:3183-3194
-    const int canonical = src_lo[a] >= 0.0 && src_hi[a] < box[a];
-    int rc = unwrapAxis(c, n, in[a], box[a], canonical, u[a], &anchors[a], s);
-    if (rc) return rc;
+    axis[axes++] = a;
   }
+  if (int rc = unwrapAxes(c, n, axes, axis, in, box, canonical, u, anchors, s)) return rc;
   for (int a = 0; a < 3; ++a) frame.anchor[a] = anchors[a];
   // bounds of the unwrapped frame
   auto* sc = c.scalars.as<unsigned long long>();
@@ -875,7 +860,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     return CHUI_TREEPM_ENOMEM;
   { noteLaunch(); mortonKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], lo[0], lo[1], lo[2], extent,
                                                c.keys_a.as<unsigned long long>(), c.idx_a.as<uint32_t>()); }
-  int rc = cubSortPairsU64(c, c.keys_a.as<unsigned long long>(), c.keys_b.as<unsigned long long>(),
+  int rc = radixSortPairsU64(c, c.keys_a.as<unsigned long long>(), c.keys_b.as<unsigned long long>(),
                            c.idx_a.as<uint32_t>(), c.idx_b.as<uint32_t>(), n, 63, s);
   if (rc) return rc;
   // keys_b: sorted Morton keys; idx_b: perm_m (Morton rank -> particle)
@@ -938,7 +923,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     }
     for (int w = words - 1; unsorted && w >= 0; --w) {  { noteLaunch(); // LSD over path words, each pass stable
       gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in, key_cur); }
-      rc = cubSortPairsU64(c, key_cur, key_sorted, rank_in, rank_out, n, 63, s);
+      rc = radixSortPairsU64(c, key_cur, key_sorted, rank_in, rank_out, n, 63, s);
       if (rc) return rc;
       uint32_t* t = rank_in;
       rank_in = rank_out;
@@ -953,10 +938,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     plan.depth_max = kLevelsPerWord * words;
     cudaMemsetAsync(status, 0, 4, s);
     { noteLaunch(); nodeCountKernel<<<gridFor(n + 1, 256), 256, 0, s>>>(plan, cp, counts, status); }
-    size_t bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, bytes, counts, offset, static_cast<int>(n + 1), s);
-    if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
-    cub::DeviceScan::ExclusiveSum(c.cub_temp.ptr, bytes, counts, offset, static_cast<int>(n + 1), s);
+    if ((rc = exclusiveScanU32(c, counts, offset, n + 1, s))) return rc;
     uint32_t hs[2];
     cudaMemcpyAsync(&hs[0], status, 4, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&hs[1], offset + n, 4, cudaMemcpyDeviceToHost, s);
@@ -1004,7 +986,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   // final order: stable sort of Morton order by leaf id
   uint32_t* leaf_key = c.idx_a.as<uint32_t>();
   { noteLaunch(); leafKeyKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.inv_pos.as<uint32_t>(), out.leaf_of_pos, leaf_key); }
-  rc = cubSortPairsU32(c, leaf_key, c.idx_d.as<uint32_t>(), perm_m, c.sorted_index.as<uint32_t>(), n,
+  rc = radixSortPairsU32(c, leaf_key, c.idx_d.as<uint32_t>(), perm_m, c.sorted_index.as<uint32_t>(), n,
                        bitsFor(total_nodes), s);
   if (rc) return rc;
   // tree-ordered source records
@@ -1039,14 +1021,8 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
                                                             c.node_mq.as<float4>()); }
   // maximum depth (for stack sizing and stats)
   {
-    size_t bytes = 0;
-    uint32_t* dmax = c.idx_a.as<uint32_t>();
-    cub::DeviceReduce::Max(nullptr, bytes, out.depth, dmax, static_cast<int>(total_nodes), s);
-    if (ensure(c.cub_temp, bytes)) return CHUI_TREEPM_ENOMEM;
-    cub::DeviceReduce::Max(c.cub_temp.ptr, bytes, out.depth, dmax, static_cast<int>(total_nodes), s);
     uint32_t hd = 0;
-    cudaMemcpyAsync(&hd, dmax, 4, cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) {
+    if (maxU32(c, out.depth, total_nodes, &hd, s)) {
       c.last_error = "tree build kernels failed";
       return CHUI_TREEPM_EDEVICE;
     }
@@ -1092,7 +1068,7 @@ int treeOrderTargets(Context& c, int64_t nt, const uint32_t* active, int explici
   uint32_t* slot = c.idx_a.as<uint32_t>();
   { noteLaunch(); targetKeyKernel<<<gridFor(nt, 256), 256, 0, s>>>(nt, active, n, c.pos_of_row.as<uint32_t>(), explicit_targets,
                                                    key, slot); }
-  return cubSortPairsU32(c, key, c.idx_d.as<uint32_t>(), slot, c.target_order.as<uint32_t>(), nt, 32, s);
+  return radixSortPairsU32(c, key, c.idx_d.as<uint32_t>(), slot, c.target_order.as<uint32_t>(), nt, 32, s);
 }
 
 }  // namespace chui
