@@ -1020,8 +1020,9 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
   // the production walk also counts and records nearest pairs when asked to,
   // or when the caller wants the nearest-pair lane
   c.walk_instrument = c.cfg.diagnostics == 2 || acc->nearest_pair_r2 != nullptr;
+  // outputs at slots (a slice's compactly, with per-block cycles)
   if (n > 0 && (rc = chui::walkRun(c, nt, active, tx, ty, tz, x, y, z, prev, wp, n, s, visit_begin, visit_end,
-                                     ranged)))
+                                     ranged, ranged)))
     return chui::fail(c, rc, rc == CHUI_TREEPM_ENOTSUP
                                  ? "the mixed-precision pair kernel's constants (H(t)/(8 r_s^3)) overflow FP32 for "
                                    "this split scale; use precision FP64"
@@ -1097,15 +1098,25 @@ static int solveVisitRange(void* handle, const chui_treepm_sources* src, const c
       lz = c.out_lr[2].as<double>();
     }
   }
-  if (short_only) {
-    for (double* p : {pmx, pmy, pmz}) cudaMemsetAsync(p, 0, static_cast<size_t>(nt) * 8, s);
-  } else if ((rc = chui::pmInterpolate(c, nout, active, tx, ty, tz, x, y, z, pmx, pmy, pmz, s, slice))) {
-    return rc;
+  if (!ranged) {
+    // interpolation and the total in one pass over the slots
+    if (nt > 0 &&
+        (rc = chui::pmInterpolateCombine(c, nt, active, tx, ty, tz, explicit_targets ? 0 : n, x, y, z, !short_only,
+                                         c.tree_acc.as<double>(), c.tree_near.as<double>(), ax, ay, az,
+                                         lr ? pmx : nullptr, lr ? pmy : nullptr, lr ? pmz : nullptr, sx, sy, sz, snear,
+                                         s)))
+      return rc;
+  } else {
+    if (short_only) {
+      for (double* p : {pmx, pmy, pmz}) cudaMemsetAsync(p, 0, static_cast<size_t>(nt) * 8, s);
+    } else if ((rc = chui::pmInterpolate(c, nout, active, tx, ty, tz, x, y, z, pmx, pmy, pmz, s, slice))) {
+      return rc;
+    }
+    if (nout > 0)
+      { chui::noteLaunch(); chui::combineKernel<<<chui::gridFor(nout, 256), 256, 0, s>>>(
+            nout, slice, nt, active, explicit_targets ? 0 : n, pmx, pmy, pmz, c.tree_acc.as<double>(),
+            c.tree_near.as<double>(), ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
   }
-  if (nout > 0)
-    { chui::noteLaunch(); chui::combineKernel<<<chui::gridFor(nout, 256), 256, 0, s>>>(
-          nout, slice, nt, active, explicit_targets ? 0 : n, pmx, pmy, pmz, c.tree_acc.as<double>(),
-          c.tree_near.as<double>(), ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
   c.visit_count = nt;
   cudaEventRecord(c.ev[4], s);
   uint32_t walk_status = 0;

@@ -171,6 +171,16 @@ int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* 
                   const double* ty, const double* tz, const double* sx, const double* sy,
                   const double* sz, double* ax, double* ay, double* az, cudaStream_t s,
                   const uint32_t* order = nullptr);
+// Interpolation and the solve's total force over the nt active slots (tree:
+// the walk's slot-indexed output, 3 lanes of nt; positions: explicit targets
+// or the sources' rows): the accel (and optional long-range) lanes at slots,
+// the optional source-indexed short-range and nearest-pair lanes at rows
+// below n.
+int pmInterpolateCombine(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
+                         const double* tz, int64_t n, const double* px, const double* py, const double* pz,
+                         bool with_pm, const double* tree, const double* near, double* ax, double* ay, double* az,
+                         double* lx, double* ly, double* lz, double* sx, double* sy, double* sz, double* snear,
+                         cudaStream_t s);
 int pmDensityOnly(Context& c, int64_t n, const double* x, const double* y, const double* z,
                   const double* m, double uniform_mass, double* rho_out, cudaStream_t s);
 int pmCells(Context& c, int64_t n, const double* x, const double* y, const double* z,
@@ -217,7 +227,7 @@ int maxU32(Context& c, const uint32_t* in, int64_t n, uint32_t* result, cudaStre
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
             const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s,
-            int64_t visit_begin = 0, int64_t visit_end = -1, bool compact = false);
+            int64_t visit_begin = 0, int64_t visit_end = -1, bool compact = false, bool record_cost = false);
 
 // Adjoint of the short-range force for all n particles (targets in tree
 // order, after treeBuild and treeOrderTargets with the full set):

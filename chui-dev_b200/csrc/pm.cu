@@ -401,6 +401,95 @@ __global__ void greenGradientKernel(PmGeom g, const double* __restrict__ tab, do
   }
 }
 
+// taps^3 stencil gathers of the three padded force grids at one position
+// (interpolateForcesImpl, pm_solver.cpp:5735-5953); isolated/open
+// boundaries: no force outside [0, L), cells outside the mesh skipped.
+template <class R>
+__device__ __forceinline__ void gatherForce(const PmGeom& g, const R* __restrict__ fxg, const R* __restrict__ fyg,
+                                            const R* __restrict__ fzg, double px, double py, double pz, R& gx,
+                                            R& gy, R& gz) {
+  gx = gy = gz = R(0);
+  if (!g.periodic && !(insideOpen(px, g.L[0]) && insideOpen(py, g.L[1]) && insideOpen(pz, g.L[2]))) return;
+  const int taps = g.scheme == 0 ? 2 : 3;
+  const Stencil s0 = makeStencil((g.periodic ? wrapPosition(px, g.L[0]) : px) * g.inv_d[0], g.scheme);
+  const Stencil s1 = makeStencil((g.periodic ? wrapPosition(py, g.L[1]) : py) * g.inv_d[1], g.scheme);
+  const Stencil s2 = makeStencil((g.periodic ? wrapPosition(pz, g.L[2]) : pz) * g.inv_d[2], g.scheme);
+  for (int a = 0; a < taps; ++a) {
+    const int64_t ox = s0.off0 + a;
+    if (!g.periodic && (ox < 0 || ox >= g.n[0])) continue;
+    const int64_t ix = g.periodic ? wrapIndex(ox, g.n[0]) : ox;
+    for (int b = 0; b < taps; ++b) {
+      const int64_t oy = s1.off0 + b;
+      if (!g.periodic && (oy < 0 || oy >= g.n[1])) continue;
+      const int64_t iy = g.periodic ? wrapIndex(oy, g.n[1]) : oy;
+      const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
+      const R wab = static_cast<R>(s0.w[a] * s1.w[b]);
+      for (int cc = 0; cc < taps; ++cc) {
+        const int64_t oz = s2.off0 + cc;
+        if (!g.periodic && (oz < 0 || oz >= g.n[2])) continue;
+        const int64_t iz = g.periodic ? wrapIndex(oz, g.n[2]) : oz;
+        const R w = wab * static_cast<R>(s2.w[cc]);
+        gx += w * fxg[row + iz];
+        gy += w * fyg[row + iz];
+        gz += w * fzg[row + iz];
+      }
+    }
+  }
+}
+
+// Interpolation and the total force of a solve in one pass over the active
+// slots: the stencil gathers, the walk's part (written at the slot), and the
+// total and optional lanes written once (TreePmForceAccumulatorView's accel,
+// long-range, short-range and nearest-pair lanes, tree_pm_coupling.cpp:1961-1978),
+// with no long-range lane round trip through memory.
+template <class R>
+__global__ void interpolateCombineKernel(int64_t nt, const uint32_t* __restrict__ active,
+                                         const double* __restrict__ tx, const double* __restrict__ ty,
+                                         const double* __restrict__ tz, int64_t n, const double* __restrict__ sx_pos,
+                                         const double* __restrict__ sy_pos, const double* __restrict__ sz_pos,
+                                         PmGeom g, const R* __restrict__ fxg, const R* __restrict__ fyg,
+                                         const R* __restrict__ fzg, int with_pm, const double* __restrict__ tree,
+                                         const double* __restrict__ near, double* ax, double* ay, double* az,
+                                         double* lx, double* ly, double* lz, double* sx, double* sy, double* sz,
+                                         double* snear) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nt;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t row = tx ? kInvalid : (active ? active[k] : static_cast<uint32_t>(k));
+    R gx = R(0), gy = R(0), gz = R(0);
+    if (with_pm) {
+      double px, py, pz;
+      if (tx) {
+        px = tx[k];
+        py = ty[k];
+        pz = tz[k];
+      } else {
+        px = sx_pos[row];
+        py = sy_pos[row];
+        pz = sz_pos[row];
+      }
+      gatherForce<R>(g, fxg, fyg, fzg, px, py, pz, gx, gy, gz);
+    }
+    const double pmx = static_cast<double>(gx), pmy = static_cast<double>(gy), pmz = static_cast<double>(gz);
+    const double trx = tree[k], try_ = tree[nt + k], trz = tree[2 * nt + k];
+    ax[k] = pmx + trx;
+    ay[k] = pmy + try_;
+    az[k] = pmz + trz;
+    if (lx) {
+      lx[k] = pmx;
+      ly[k] = pmy;
+      lz[k] = pmz;
+    }
+    if (row < n) {
+      if (sx) {
+        sx[row] = trx;
+        sy[row] = try_;
+        sz[row] = trz;
+      }
+      if (snear) snear[row] = near[k];
+    }
+  }
+}
+
 // Force interpolation at targets: taps^3 gathers from the three padded
 // force grids. Targets are active slots (rows of the source arrays) or
 // explicit positions.
@@ -412,7 +501,6 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ order
                                   const double* __restrict__ sy, const double* __restrict__ sz,
                                   PmGeom g, const R* __restrict__ fxg, const R* __restrict__ fyg,
                                   const R* __restrict__ fzg, double* ax, double* ay, double* az) {
-  const int taps = g.scheme == 0 ? 2 : 3;
   for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < nt;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     // slot k: the j-th target, or the j-th entry of a visit-order slice
@@ -429,38 +517,8 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ order
       py = sy[row];
       pz = sz[row];
     }
-    // isolated/open: no PM force outside [0, L); cells outside the mesh skipped (pm_solver.cpp:5904-5947)
-    if (!g.periodic && !(insideOpen(px, g.L[0]) && insideOpen(py, g.L[1]) && insideOpen(pz, g.L[2]))) {
-      ax[order ? j : k] = 0.0;
-      ay[order ? j : k] = 0.0;
-      az[order ? j : k] = 0.0;
-      continue;
-    }
-    const Stencil s0 = makeStencil((g.periodic ? wrapPosition(px, g.L[0]) : px) * g.inv_d[0], g.scheme);
-    const Stencil s1 = makeStencil((g.periodic ? wrapPosition(py, g.L[1]) : py) * g.inv_d[1], g.scheme);
-    const Stencil s2 = makeStencil((g.periodic ? wrapPosition(pz, g.L[2]) : pz) * g.inv_d[2], g.scheme);
-    R gx = 0, gy = 0, gz = 0;
-    for (int a = 0; a < taps; ++a) {
-      const int64_t ox = s0.off0 + a;
-      if (!g.periodic && (ox < 0 || ox >= g.n[0])) continue;
-      const int64_t ix = g.periodic ? wrapIndex(ox, g.n[0]) : ox;
-      for (int b = 0; b < taps; ++b) {
-        const int64_t oy = s1.off0 + b;
-        if (!g.periodic && (oy < 0 || oy >= g.n[1])) continue;
-        const int64_t iy = g.periodic ? wrapIndex(oy, g.n[1]) : oy;
-        const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.nzp;
-        const R wab = static_cast<R>(s0.w[a] * s1.w[b]);
-        for (int cc = 0; cc < taps; ++cc) {
-          const int64_t oz = s2.off0 + cc;
-          if (!g.periodic && (oz < 0 || oz >= g.n[2])) continue;
-          const int64_t iz = g.periodic ? wrapIndex(oz, g.n[2]) : oz;
-          const R w = wab * static_cast<R>(s2.w[cc]);
-          gx += w * fxg[row + iz];
-          gy += w * fyg[row + iz];
-          gz += w * fzg[row + iz];
-        }
-      }
-    }
+    R gx, gy, gz;
+    gatherForce<R>(g, fxg, fyg, fzg, px, py, pz, gx, gy, gz);
     const int64_t o = order ? j : k;
     ax[o] = static_cast<double>(gx);
     ay[o] = static_cast<double>(gy);
@@ -1032,6 +1090,30 @@ int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* 
     { noteLaunch(); interpolateKernel<double><<<gridFor(nt, block), block, 0, s>>>(
         nt, order, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<double>(), c.grid[1].as<double>(),
         c.grid[2].as<double>(), ax, ay, az); }
+  }
+  if (cudaGetLastError() != cudaSuccess) {
+    c.last_error = "PM interpolation launch failed";
+    return CHUI_TREEPM_EDEVICE;
+  }
+  return 0;
+}
+
+int pmInterpolateCombine(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
+                         const double* tz, int64_t n, const double* px, const double* py, const double* pz,
+                         bool with_pm, const double* tree, const double* near, double* ax, double* ay, double* az,
+                         double* lx, double* ly, double* lz, double* sx, double* sy, double* sz, double* snear,
+                         cudaStream_t s) {
+  if (nt == 0) return 0;
+  const PmGeom g = geomOf(c);
+  const int block = 256;
+  if (isMixed(c)) {
+    { noteLaunch(); interpolateCombineKernel<float><<<gridFor(nt, block), block, 0, s>>>(
+        nt, active, tx, ty, tz, n, px, py, pz, g, c.grid[0].as<float>(), c.grid[1].as<float>(),
+        c.grid[2].as<float>(), with_pm ? 1 : 0, tree, near, ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
+  } else {
+    { noteLaunch(); interpolateCombineKernel<double><<<gridFor(nt, block), block, 0, s>>>(
+        nt, active, tx, ty, tz, n, px, py, pz, g, c.grid[0].as<double>(), c.grid[1].as<double>(),
+        c.grid[2].as<double>(), with_pm ? 1 : 0, tree, near, ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
   }
   if (cudaGetLastError() != cudaSuccess) {
     c.last_error = "PM interpolation launch failed";

@@ -38,7 +38,12 @@ constexpr int kSortWarps = kSortThreads / 32;
 #define CHUI_SORT_ITEMS 16  // keys per thread of a tile
 #endif
 #ifndef CHUI_SORT_MIN_BLOCKS
-#define CHUI_SORT_MIN_BLOCKS 1  // resident downsweep blocks per SM the register budget is sized for
+#define CHUI_SORT_MIN_BLOCKS 0  // resident downsweep blocks per SM to size registers for (0: the compiler's choice)
+#endif
+#if CHUI_SORT_MIN_BLOCKS > 0
+#define CHUI_SORT_BOUNDS __launch_bounds__(kSortThreads, CHUI_SORT_MIN_BLOCKS)
+#else
+#define CHUI_SORT_BOUNDS __launch_bounds__(kSortThreads)
 #endif
 constexpr int kItemsPerThread = CHUI_SORT_ITEMS;
 constexpr int kTile = kSortThreads * kItemsPerThread;  // 4096 keys per tile
@@ -159,7 +164,7 @@ constexpr size_t downsweepSmem() {
 
 // Rank, stage and scatter one tile for one digit.
 template <class K, bool kValues>
-__global__ void __launch_bounds__(kSortThreads, CHUI_SORT_MIN_BLOCKS) downsweepKernel(int64_t n, SortJob job, SortJob dst, int shift,
+__global__ void CHUI_SORT_BOUNDS downsweepKernel(int64_t n, SortJob job, SortJob dst, int shift,
                                                               int64_t tiles, const uint32_t* __restrict__ counts,
                                                               const uint32_t* __restrict__ totals) {
   __shared__ uint32_t wcount[kSortWarps][256];  // per-warp digit counts, then prefixes

@@ -2161,7 +2161,7 @@ int ensureGaussTable(Context& c, cudaStream_t s) {
 int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, const double* ty,
             const double* tz, const double* sx, const double* sy, const double* sz,
             const double* prev_acc, const WalkParams& wp, int64_t n, cudaStream_t s,
-            int64_t visit_begin, int64_t visit_end, bool compact) {
+            int64_t visit_begin, int64_t visit_end, bool compact, bool record_cost) {
   if (visit_end < 0) visit_end = nt;
   if (nt == 0) return 0;
   // counters and per-chunk walk cycles start at zero even when the visit
@@ -2226,7 +2226,7 @@ int walkRun(Context& c, int64_t nt, const uint32_t* active, const double* tx, co
   a.work = c.work_counter.as<uint32_t>();
   // per-block cycles for visit-range solves (FP64 walk, and the mixed walk's
   // production instances: no diagnostics, every source a target, one mass)
-  a.chunk_cost = compact ? c.walk_cost.as<float>() : nullptr;
+  a.chunk_cost = record_cost ? c.walk_cost.as<float>() : nullptr;
   a.status = c.status.as<uint32_t>();
   a.poly = c.poly;
   a.dpoly = c.dpoly;

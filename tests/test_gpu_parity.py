@@ -317,3 +317,24 @@ def test_production_walk_nearest_pair_and_counters(cuda_ok, name, precision):
     # forces are the production walk's
     e = rel_err([r["ax"], r["ay"], r["az"]], [g["ax"], g["ay"], g["az"]])
     assert np.median(e) <= 1e-4 and np.percentile(e, 99) <= 1e-3
+
+
+@pytest.mark.parametrize("name", ["lattice16_cic", "clustered64k_cic", "rect_active"])
+def test_short_range_only_is_the_tree_part(cuda_ok, name):
+    """TreePmOptions::short_range_only (the integrator's split operator): the
+    solve returns the short-range residual alone -- the reference's
+    source-indexed tree-only lanes -- with zero long-range lanes, and needs no
+    PM field (a reuse request does not fail)."""
+    g = load_golden(name)
+    act = _active(g)
+    rows = act if act is not None else np.arange(len(g["x"]))
+    cfg = cfg_for(g, ct._abi.FP64)
+    cfg.short_range_only = 1
+    scale = np.abs(np.concatenate([g["tree_ax"][rows], g["tree_ay"][rows], g["tree_az"][rows]])).max()
+    with ct.TreePmCoordinator(cfg) as s:
+        for refresh in (False, True):
+            r = s.solve_active_set_with_pm_cadence(g["x"], g["y"], g["z"], g["m"], refresh, active=act,
+                                                   long_range=True)
+            for k in ("x", "y", "z"):
+                assert np.abs(r["a" + k] - g["tree_a" + k][rows]).max() <= 1e-9 * scale, k
+                assert np.all(r["pm_a" + k] == 0.0)
