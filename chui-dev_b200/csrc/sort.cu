@@ -137,23 +137,40 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* war
 }
 
 // For each digit of each sort (block (v, y)): exclusive prefix over tiles in
-// place and the digit's total; each thread takes a run of consecutive tiles.
+// place and the digit's total. The row is staged through shared memory in
+// coalesced chunks of kScanRow; each thread scans a run of consecutive
+// entries there.
+constexpr int kScanRow = 4096;
 __global__ void __launch_bounds__(kSortThreads) tileScanKernel(int64_t tiles, uint32_t* counts, uint32_t* totals) {
   __shared__ uint32_t warp_sums[kSortWarps];
+  __shared__ uint32_t row_sm[kScanRow + kScanRow / 32];  // one pad word per 32: no bank conflicts
   const int64_t row = static_cast<int64_t>(blockIdx.y) * 256 + blockIdx.x;
   uint32_t* c = counts + row * tiles;
-  const int64_t per = (tiles + kSortThreads - 1) / kSortThreads;
-  const int64_t b = threadIdx.x * per, e = b + per < tiles ? b + per : tiles;
-  uint32_t sum = 0u;
-  for (int64_t i = b; i < e; ++i) sum += c[i];
-  uint32_t total;
-  uint32_t run = blockExclusiveScan(sum, warp_sums, &total);
-  for (int64_t i = b; i < e; ++i) {
-    const uint32_t v = c[i];
-    c[i] = run;
-    run += v;
+  constexpr int kPer = kScanRow / kSortThreads;  // 16 entries per thread
+  uint32_t carry = 0u;
+  for (int64_t b = 0; b < tiles; b += kScanRow) {
+    const int len = tiles - b < kScanRow ? static_cast<int>(tiles - b) : kScanRow;
+    for (int i = threadIdx.x; i < kScanRow; i += kSortThreads) row_sm[i + i / 32] = i < len ? c[b + i] : 0u;
+    __syncthreads();
+    uint32_t sum = 0u;
+    for (int i = 0; i < kPer; ++i) {
+      const int q = threadIdx.x * kPer + i;
+      sum += row_sm[q + q / 32];
+    }
+    uint32_t total;
+    uint32_t run = carry + blockExclusiveScan(sum, warp_sums, &total);
+    for (int i = 0; i < kPer; ++i) {
+      const int q = threadIdx.x * kPer + i;
+      const uint32_t v = row_sm[q + q / 32];
+      row_sm[q + q / 32] = run;
+      run += v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < len; i += kSortThreads) c[b + i] = row_sm[i + i / 32];
+    carry += total;
+    __syncthreads();
   }
-  if (threadIdx.x == 0) totals[row] = total;
+  if (threadIdx.x == 0) totals[row] = carry;
 }
 
 // Dynamic shared memory of the downsweep: the staged tile (keys, values).

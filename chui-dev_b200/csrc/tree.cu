@@ -694,33 +694,38 @@ __device__ __forceinline__ double treeFrameCoordinate(double x, const FrameSpec&
   return v;
 }
 
-// Tree-ordered source records. The tree-frame coordinates are recomputed from
-// the gathered caller coordinates (the same arithmetic as the unwrap), so a
-// source costs three scattered position reads (four with a mass lane).
-__global__ void packSourcesKernel(int64_t n, const uint32_t* __restrict__ sorted,
-                                  const uint32_t* __restrict__ leaf_of_pos,
-                                  const double4* __restrict__ geom, FrameSpec frame,
-                                  const double* __restrict__ x, const double* __restrict__ y,
-                                  const double* __restrict__ z, const double* __restrict__ m,
-                                  double uniform_mass, float4* f4, double4* d4, double4* u4,
-                                  uint32_t* pos_of_row, const double* __restrict__ eps_rows, double* eps_tree) {
+// Tree-ordered source records, written from row order: each row's caller
+// position, mass and softening are read contiguously and its records are
+// scattered to its tree position (whole 32-byte records: no partial
+// sectors); the tree-frame coordinates are recomputed from the caller's
+// (the same arithmetic as the unwrap).
+__global__ void scatterSourcesKernel(int64_t n, const uint32_t* __restrict__ pos_of_row, FrameSpec frame,
+                                     const double* __restrict__ x, const double* __restrict__ y,
+                                     const double* __restrict__ z, const double* __restrict__ m, double uniform_mass,
+                                     double4* d4, double4* u4, const double* __restrict__ eps_rows,
+                                     double* eps_tree) {
+  for (int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; s < n;
+       s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t t = pos_of_row[s];
+    const double ms = m ? m[s] : uniform_mass;
+    const double px = x[s], py = y[s], pz = z[s];
+    d4[t] = make_double4(px, py, pz, ms);
+    u4[t] = make_double4(treeFrameCoordinate(px, frame, 0), treeFrameCoordinate(py, frame, 1),
+                         treeFrameCoordinate(pz, frame, 2), ms);
+    if (eps_rows) eps_tree[t] = eps_rows[s];
+  }
+}
+
+// Mixed precision: each source's FP32 offset from its leaf's FP64 centre, in
+// tree order (a leaf's sources are consecutive).
+__global__ void leafOffsetsKernel(int64_t n, const uint32_t* __restrict__ leaf_of_pos,
+                                  const double4* __restrict__ geom, const double4* __restrict__ u4, float4* f4) {
   for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < n;
        t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const uint32_t s = sorted[t];
-    const double ms = m ? m[s] : uniform_mass;
-    pos_of_row[s] = static_cast<uint32_t>(t);
-    const double px = x[s], py = y[s], pz = z[s];
-    const double ux = treeFrameCoordinate(px, frame, 0);
-    const double uy = treeFrameCoordinate(py, frame, 1);
-    const double uz = treeFrameCoordinate(pz, frame, 2);
-    if (f4) {
-      const double4 g = geom[leaf_of_pos[t]];
-      f4[t] = make_float4(static_cast<float>(ux - g.x), static_cast<float>(uy - g.y), static_cast<float>(uz - g.z),
-                          static_cast<float>(ms));
-    }
-    if (d4) d4[t] = make_double4(px, py, pz, ms);
-    if (u4) u4[t] = make_double4(ux, uy, uz, ms);
-    if (eps_rows) eps_tree[t] = eps_rows[s];
+    const double4 u = u4[t];
+    const double4 g = geom[leaf_of_pos[t]];
+    f4[t] = make_float4(static_cast<float>(u.x - g.x), static_cast<float>(u.y - g.y), static_cast<float>(u.z - g.z),
+                        static_cast<float>(u.w));
   }
 }
 
@@ -998,12 +1003,14 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   if (ensure(c.src_u4, n * sizeof(double4))) return CHUI_TREEPM_ENOMEM;
   if (c.soft_rows && (ensure(c.src_eps, n * sizeof(double)) || ensure(c.node_soft, total_nodes * sizeof(double2))))
     return CHUI_TREEPM_ENOMEM;
-  { noteLaunch(); packSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), out.leaf_of_pos, out.geom,
-                                                    frame, x, y, z, m, uniform_mass,
-                                                    mixed ? c.src_f4.as<float4>() : nullptr,
-                                                    c.src_d4.as<double4>(), c.src_u4.as<double4>(),
-                                                    c.pos_of_row.as<uint32_t>(), c.soft_rows,
-                                                    c.soft_rows ? c.src_eps.as<double>() : nullptr); }
+  // tree position of each row, then the records scattered from row order
+  { noteLaunch(); invertKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), c.pos_of_row.as<uint32_t>()); }
+  { noteLaunch(); scatterSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.pos_of_row.as<uint32_t>(), frame, x, y, z, m,
+                                                       uniform_mass, c.src_d4.as<double4>(), c.src_u4.as<double4>(),
+                                                       c.soft_rows, c.soft_rows ? c.src_eps.as<double>() : nullptr); }
+  if (mixed)
+    { noteLaunch(); leafOffsetsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out.leaf_of_pos, out.geom, c.src_u4.as<double4>(),
+                                                      c.src_f4.as<float4>()); }
   // moments (leaves read the tree-ordered records written above)
   cudaMemsetAsync(c.node_counter.ptr, 0, total_nodes * 4, s);
   MomentIn mi;
