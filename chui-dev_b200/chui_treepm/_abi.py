@@ -87,7 +87,7 @@ EXPORTED = (
     "chui_treepm_config_default", "chui_treepm_create", "chui_treepm_destroy",
     "chui_treepm_set_config", "chui_treepm_last_error", "chui_treepm_solve",
     "chui_pm_assign_density", "chui_pm_cells", "chui_treepm_tree_node_count",
-    "chui_treepm_dump_tree", "chui_treepm_dump_particles", "chui_treepm_kick", "chui_treepm_drift",
+    "chui_treepm_dump_tree", "chui_treepm_tree_build_info", "chui_treepm_dump_particles", "chui_treepm_kick", "chui_treepm_drift",
     "chui_treepm_kdk_factors_static", "chui_treepm_kdk_factors_lcdm", "chui_treepm_probe_fp32_peak", "chui_pm_assign_density_static",
     "chui_treepm_force_vjp", "chui_pm_density_vjp", "chui_treepm_kdk_adjoint", "chui_treepm_momentum_energy",
 )
@@ -125,6 +125,7 @@ def load(path: str | None = None):
     L.chui_treepm_tree_node_count.argtypes = [vp, C.POINTER(C.c_int64)]
     L.chui_treepm_dump_tree.argtypes = [vp, C.POINTER(TreeDump)]
     L.chui_treepm_dump_particles.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp]
+    L.chui_treepm_tree_build_info.argtypes = [vp, vp]
     L.chui_treepm_kick.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, vp]
     L.chui_treepm_drift.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp, C.c_double, C.c_int, vp]
     L.chui_treepm_kdk_factors_static.argtypes = [C.c_double, vp]

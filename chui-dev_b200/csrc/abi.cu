@@ -711,14 +711,14 @@ void chui_treepm_destroy(void* handle) {
                             &c->grp_leaf, &c->grp_start, &c->grp_rec, &c->grp_list, &c->grp_done, &c->gauss_tab,
                             &c->out_acc[0], &c->out_acc[1], &c->out_acc[2], &c->out_pm[0], &c->out_pm[1],
                             &c->out_pm[2], &c->out_tree[0], &c->out_tree[1], &c->out_tree[2], &c->out_near,
-                            &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max,
+                            &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max, &c->gap_min, &c->gap_max, &c->gap_flag, &c->gap_off,
                             &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
                             &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
                             &c->leaf_of_pos, &c->inv_pos, &c->sort_hist, &c->sort_counts,
                             &c->sort_totals, &c->sort_keys, &c->sort_vals, &c->node_geom, &c->node_com,
                             &c->node_quad, &c->node_f4, &c->node_mq, &c->node_child, &c->node_range, &c->node_parent, &c->node_depth,
                             &c->node_counter, &c->sorted_index, &c->pos_of_row, &c->src_f4, &c->src_d4, &c->src_u4, &c->src_cot,
-                            &c->target_order, &c->morton_sorted, &c->walk_counters, &c->work_counter,
+                            &c->target_order, &c->morton_keys, &c->walk_counters, &c->work_counter,
                             &c->tree_acc, &c->tree_near, &c->walk_cost, &c->out_lr[0], &c->out_lr[1],
                             &c->out_lr[2]};
     for (auto* b : bufs) chui::release(*b);
@@ -1493,6 +1493,14 @@ int chui_pm_cells(void* handle, const chui_treepm_sources* src, int64_t* cells, 
   return rc;
 }
 
+int chui_treepm_tree_build_info(const void* handle, int32_t info[2]) {
+  if (!handle || !info) return CHUI_TREEPM_EINVAL;
+  const Context& c = *static_cast<const Context*>(handle);
+  info[0] = c.unwrap_sorted_axes;
+  info[1] = c.large_leaf;
+  return 0;
+}
+
 int chui_treepm_tree_node_count(const void* handle, int64_t* node_count) {
   if (!handle || !node_count) return CHUI_TREEPM_EINVAL;
   *node_count = static_cast<const Context*>(handle)->n_nodes;
@@ -1549,7 +1557,14 @@ int chui_treepm_dump_particles(void* handle, int64_t n, double* ux, double* uy, 
   if (ux) cudaMemcpy(ux, c.ux.ptr, n * 8, cudaMemcpyDeviceToHost);
   if (uy) cudaMemcpy(uy, c.uy.ptr, n * 8, cudaMemcpyDeviceToHost);
   if (uz) cudaMemcpy(uz, c.uz.ptr, n * 8, cudaMemcpyDeviceToHost);
-  if (morton_sorted) cudaMemcpy(morton_sorted, c.morton_sorted.ptr, n * 8, cudaMemcpyDeviceToHost);
+  if (morton_sorted) {
+    // the tree build keeps each particle's key; the sorted list is formed here
+    if (chui::ensure(c.keys_b, n * 8)) return CHUI_TREEPM_ENOMEM;
+    const unsigned long long* kin = c.morton_keys.as<unsigned long long>();
+    unsigned long long* kout = c.keys_b.as<unsigned long long>();
+    if (int rc = chui::radixSortKeysU64(c, 1, &kin, &kout, n, 63, nullptr)) return rc;
+    if (cudaMemcpy(morton_sorted, kout, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  }
   if (sorted_index) cudaMemcpy(sorted_index, c.sorted_index.ptr, n * 4, cudaMemcpyDeviceToHost);
   if (anchors)
     for (int a = 0; a < 3; ++a) anchors[a] = c.tree_anchor[a];

@@ -12,6 +12,7 @@ namespace chui {
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr int kMaxDepth = 64;            // tree_gravity.hpp:17 (kMaximumTreeDepth)
 constexpr int kLevelsPerWord = 21;       // 3 octant bits per level, 63 bits per path word
+constexpr int kLeafOrderMax = 1024;      // largest leaf ordered in place (larger: one more global sort)
 constexpr int kMaxPathWords = 4;         // 84 levels > kMaxDepth
 constexpr int kWalkWarpsPerBlock = 4;
 constexpr int kStackCap = 1 + 7 * kMaxDepth;  // tree_pm_coupling.cpp:899-925 stack bound
@@ -27,6 +28,7 @@ enum StatusBits : uint32_t {
   kStatusNeedMorePathWords = 1u << 3,
   kStatusNegativeMass = 1u << 4,
   kStatusIndexRange = 1u << 5,
+  kStatusLargeLeaf = 1u << 6,  // a leaf above the within-leaf ordering limit (not an error)
 };
 
 // Periodic nearest-image metric (internal/tree_pm_geometry.hpp:12-32): bounded

@@ -109,7 +109,8 @@ struct Context {
 
   // tree construction
   DevBuf ux, uy, uz;             // unwrapped FP64 coordinates (tree frame)
-  DevBuf bucket_min, bucket_max;  // unwrap sort keys; bucket_max is also tree-path sort scratch
+  DevBuf bucket_min, bucket_max;  // unwrap gap buckets {min, max}; bucket_max is also tree-path sort scratch
+  DevBuf gap_min, gap_max, gap_flag, gap_off;  // non-empty gap buckets in order, their flags and offsets
   DevBuf keys_a, keys_b, idx_a, idx_b, idx_c, idx_d;
   DevBuf path_words;             // kMaxPathWords * n u64
   DevBuf common_prefix;          // int8/int32 per sorted position
@@ -120,6 +121,8 @@ struct Context {
   int64_t n_nodes = 0;
   uint32_t max_depth = 0;
   int path_words_used = 0;
+  int unwrap_sorted_axes = 0;  // axes whose unwrap sorted the coordinates (bit a)
+  int large_leaf = 0;          // the last build ordered a leaf above kLeafOrderMax globally
   double tree_anchor[3] = {0, 0, 0};
 
   // nodes (SoA, FP64 geometry/moments)
@@ -140,7 +143,7 @@ struct Context {
   DevBuf src_u4;       // double4 per tree position: unwrapped (tree frame) position + mass (moments, walk)
   DevBuf src_cot;      // double4 per tree position: force cotangent (adjoint walk)
   DevBuf target_order; // visit order of active slots
-  DevBuf morton_sorted;  // sorted Morton keys (diagnostic parity output)
+  DevBuf morton_keys;  // Morton key of each particle (row order)
 
   // walk
   DevBuf walk_counters;  // 8 x u64

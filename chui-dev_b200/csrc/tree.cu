@@ -65,42 +65,97 @@ __device__ __noinline__ double canonicalCoordinate(double x, double box, int can
   return v;
 }
 
-__global__ void canonicalKeysKernel(int64_t n, const double* __restrict__ in, double box, int canonical,
-                                    double* out, unsigned long long* keys) {
+// Gap bucket of a canonical coordinate: floor(v * nb / L), clamped. The map is
+// monotone in v (a product with a positive factor and a truncation both
+// keep order), so every value of bucket k is <= every value of bucket k+1.
+__device__ __forceinline__ uint32_t gapBucket(double v, double scale, uint32_t nb) {
+  const double f = v * scale;
+  if (!(f > 0.0)) return 0u;
+  return f >= static_cast<double>(nb) ? nb - 1u : static_cast<uint32_t>(f);
+}
+
+// The canonical coordinate of every particle, and per gap bucket the
+// smallest and largest value, as bits (non-negative doubles order like their
+// bits). A plain read first skips the atomics that cannot change the bucket
+// (a stale read only ever asks for an atomic that was not needed): particles
+// in row order often share a bucket across a warp.
+__global__ void canonicalBucketsKernel(int64_t n, const double* __restrict__ in, double box, int canonical,
+                                       double* out, double scale, uint32_t nb, unsigned long long* bmin,
+                                       unsigned long long* bmax) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const double v = canonicalCoordinate(in[i], box, canonical);
     out[i] = v;
-    keys[i] = dbits(v);
+    const uint32_t k = gapBucket(v, scale, nb);
+    const unsigned long long b = dbits(v);
+    if (b < bmin[k]) atomicMin(bmin + k, b);
+    if (b > bmax[k]) atomicMax(bmax + k, b);
   }
 }
 
-// Circular gaps of the sorted coordinates: gap_i = v[i+1] - v[i], and
-// v[0] + L - v[n-1] around the box (tree_pm_coupling.cpp:189-207). Pass 0
-// finds the largest (gaps are >= 0, so their bits order like the values;
-// reduced per block, one atomic per block); pass 1 takes the smallest value
-// after a gap equal to it as the anchor.
-__global__ void __launch_bounds__(256) sortedGapKernel(int64_t n, const unsigned long long* __restrict__ sorted,
-                                                        double box, unsigned long long* best_gap, int pass,
-                                                        unsigned long long* best_anchor) {
+// flag[k] = 1 for a non-empty bucket (flag[nb] = 0: the scan's total slot)
+__global__ void bucketFlagsKernel(uint32_t nb, const unsigned long long* __restrict__ bmin, uint32_t* flag) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k <= nb;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    flag[k] = k < nb && bmin[k] != ~0ull ? 1u : 0u;
+  }
+}
+
+// The non-empty buckets' {min, max}, in bucket (= value) order.
+__global__ void bucketCompactKernel(uint32_t nb, const unsigned long long* __restrict__ bmin,
+                                    const unsigned long long* __restrict__ bmax, const uint32_t* __restrict__ off,
+                                    unsigned long long* cmin, unsigned long long* cmax) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nb;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const unsigned long long lo = bmin[k];
+    if (lo == ~0ull) continue;
+    const uint32_t j = off[k];
+    if (j < nb) {  // always true; a guard on the computed index
+      cmin[j] = lo;
+      cmax[j] = bmax[k];
+    }
+  }
+}
+
+// Circular gaps between consecutive runs of sorted coordinates: run i holds
+// values lo[i] .. hi[i], gap_i = lo[i+1] - hi[i], and lo[0] + L - hi[m-1]
+// around the box (tree_pm_coupling.cpp:189-207). With the fully sorted
+// coordinates every run is one value (lo == hi); with gap buckets a run is a
+// bucket, and a bucket whose own extent hi - lo is not below the largest gap
+// found could hide a larger or equal gap inside it: pass 1 then raises
+// *suspect and the axis is sorted instead. Pass 0 finds the largest gap (gaps
+// are >= 0, so their bits order like the values; one atomic per block); pass
+// 1 takes the smallest value after a gap equal to it as the anchor. The run
+// count is m, or *m_dev when given.
+__global__ void __launch_bounds__(256) runGapKernel(int64_t m, const uint32_t* __restrict__ m_dev,
+                                                    const unsigned long long* __restrict__ lo,
+                                                    const unsigned long long* __restrict__ hi, double box,
+                                                    unsigned long long* best_gap, int pass,
+                                                    unsigned long long* best_anchor, unsigned long long* suspect) {
+  if (m_dev) m = *m_dev;
   unsigned long long local = 0ull;
   const unsigned long long target = pass == 0 ? 0ull : *best_gap;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+  bool hidden = false;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < m;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const double cur = bitsd(sorted[i]);
-    const bool around = i + 1 == n;
-    const unsigned long long after = around ? sorted[0] : sorted[i + 1];
+    const double cur = bitsd(hi[i]);
+    const bool around = i + 1 == m;
+    const unsigned long long after = around ? lo[0] : lo[i + 1];
     const double cand = bitsd(after);
     const double next = around ? cand + box : cand;
     const double gap = next - cur;
     if (pass == 0) {
       const unsigned long long g = dbits(gap);
       local = g > local ? g : local;
-    } else if (dbits(gap) == target) {
-      atomicMin(best_anchor, after);
+    } else {
+      if (dbits(gap) == target) atomicMin(best_anchor, after);
+      if (suspect && lo[i] != hi[i] && dbits(cur - bitsd(lo[i])) >= target) hidden = true;
     }
   }
-  if (pass != 0) return;
+  if (pass != 0) {
+    if (hidden) atomicOr(suspect, 1ull);
+    return;
+  }
   for (int off = 16; off > 0; off >>= 1) {
     const unsigned long long o = __shfl_xor_sync(0xffffffffu, local, off);
     local = o > local ? o : local;
@@ -116,7 +171,10 @@ __global__ void __launch_bounds__(256) sortedGapKernel(int64_t n, const unsigned
   }
 }
 
-__global__ void applyAnchorKernel(int64_t n, double* u, double box, const unsigned long long* anchor_bits) {
+// u += L below the anchor; skipped while the axis's bucket gaps are suspect.
+__global__ void applyAnchorKernel(int64_t n, double* u, double box, const unsigned long long* anchor_bits,
+                                  const unsigned long long* suspect) {
+  if (suspect && *suspect) return;
   const double anchor = bitsd(*anchor_bits);
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -193,7 +251,7 @@ __global__ void mortonKernel(int64_t n, const double* __restrict__ ux, const dou
 
 // ------------------------------------------------------------ paths
 
-// Octant path of each particle (in Morton order) by the reference's centre
+// Octant path of each particle (row order, or perm[j] for entry j) by the reference's centre
 // recurrence: digit d compares against the level-(d-1) centre, then
 // centre += +-half/2 (tree_gravity.cpp:50-61, :1181-1185). Word w holds levels
 // 21w+1 .. 21w+21, level 1 in the top digit.
@@ -203,7 +261,7 @@ __global__ void pathKernel(int64_t n, int words, const uint32_t* __restrict__ pe
                            double half0, unsigned long long* path /* words * n */) {
   for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < n;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const uint32_t p = perm[j];
+    const uint32_t p = perm ? perm[j] : static_cast<uint32_t>(j);
     const double px = ux[p], py = uy[p], pz = uz[p];
     double cx = cx0, cy = cy0, cz = cz0, h = half0;
     for (int w = 0; w < words; ++w) {
@@ -440,6 +498,7 @@ __global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* 
       }
       if (d == l) {
         for (int64_t k = i; k < end; ++k) out.leaf_of_pos[k] = node;
+        if (count > kLeafOrderMax) atomicOr(status, kStatusLargeLeaf);
       }
     }
   }
@@ -462,11 +521,41 @@ __global__ void invertKernel(int64_t n, const uint32_t* __restrict__ perm, uint3
 }
 
 // key for the final stable sort: leaf id of each particle, listed in Morton order
-__global__ void leafKeyKernel(int64_t n, const uint32_t* __restrict__ inv_rank,
+// Within-leaf order. The reference partitions the Morton-sorted particles
+// into octants, so a leaf's particles keep their Morton order (key, then row:
+// the radix sort is stable over rows; tree_gravity.cpp:1081-1206,
+// tree_ordering.cpp:13-71). Here the octant paths are sorted directly, and
+// each particle's place in its leaf is its rank by (Morton key, row) among
+// the leaf's particles: positions [begin, begin + count) of the path order.
+__global__ void leafOrderKernel(int64_t n, const uint32_t* __restrict__ leaf_of_pos, const uint4* __restrict__ range,
+                                const uint32_t* __restrict__ row_of_pos, const unsigned long long* __restrict__ key_of_pos,
+                                uint32_t* sorted_index, uint32_t* status) {
+  for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint4 r = range[leaf_of_pos[p]];
+    if (r.y > static_cast<uint32_t>(kLeafOrderMax) || p < r.x || p >= static_cast<int64_t>(r.x) + r.y ||
+        static_cast<int64_t>(r.x) + r.y > n) {
+      atomicOr(status, kStatusIndexRange);
+      continue;
+    }
+    const unsigned long long k = key_of_pos[p];
+    const uint32_t row = row_of_pos[p];
+    uint32_t rank = 0u;
+    for (uint32_t q = r.x; q < r.x + r.y; ++q) {
+      const unsigned long long kq = key_of_pos[q];
+      rank += (kq < k || (kq == k && row_of_pos[q] < row)) ? 1u : 0u;
+    }
+    sorted_index[r.x + rank] = row;
+  }
+}
+
+// Leaf of each particle in Morton order (the large-leaf path: a stable sort
+// of the Morton order by leaf gives the same order).
+__global__ void leafKeyKernel(int64_t n, const uint32_t* __restrict__ perm_m, const uint32_t* __restrict__ pos_of_particle,
                               const uint32_t* __restrict__ leaf_of_pos, uint32_t* key) {
   for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < n;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    key[j] = leaf_of_pos[inv_rank[j]];
+    key[j] = leaf_of_pos[pos_of_particle[perm_m[j]]];
   }
 }
 
@@ -741,25 +830,6 @@ __global__ void targetKeyKernel(int64_t nt, const uint32_t* __restrict__ active,
   }
 }
 
-// Whether the path words, listed in Morton-rank order, are already in
-// non-decreasing lexicographic order (word 0 most significant): then the
-// stable path sort is the identity and is skipped.
-__global__ void pathOrderCheckKernel(int64_t n, int words, const unsigned long long* __restrict__ by_rank,
-                                     unsigned int* unsorted) {
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i + 1 < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    for (int w = 0; w < words; ++w) {
-      const unsigned long long a = by_rank[static_cast<size_t>(w) * n + i];
-      const unsigned long long b = by_rank[static_cast<size_t>(w) * n + i + 1];
-      if (a < b) break;
-      if (a > b) {
-        atomicOr(unsorted, 1u);
-        break;
-      }
-    }
-  }
-}
-
 __global__ void iotaKernel(int64_t n, uint32_t* v) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -775,42 +845,87 @@ int bitsFor(uint64_t maxval) {
 
 }  // namespace
 
-// Unwrap the axes into `out` (tree frame), returning each axis's anchor: the
-// canonical coordinates of all axes are sorted together (one batched radix
-// sort), then each axis finds its largest circular gap.
+// Unwrap the axes into `out` (tree frame), returning each axis's anchor. Per
+// axis, the canonical coordinates go into about n/4 gap buckets (min and max
+// per bucket), the non-empty buckets are listed in order, and the largest
+// circular gap is taken between consecutive buckets. When every bucket's own
+// extent is below that gap no gap inside a bucket can reach it, so it is the
+// largest gap of the sorted coordinates and the anchor is theirs. Otherwise
+// (few particles, or a bucket holding the largest gap) the axis's
+// coordinates are sorted and the gaps taken between consecutive values, as
+// the reference does.
 static int unwrapAxes(Context& c, int64_t n, int axes, const int* axis, const double* const* in, const double* box,
                       const int* canonical, double* const* out, double* anchor, cudaStream_t s) {
   if (n == 0 || axes == 0) {
     for (int k = 0; k < axes; ++k) anchor[axis[k]] = 0.0;
     return 0;
   }
-  if (ensure(c.bucket_min, static_cast<size_t>(axes) * n * 8) || ensure(c.bucket_max, static_cast<size_t>(axes) * n * 8))
+  uint32_t nb = 1;
+  while (nb < static_cast<uint64_t>(n) / 4 && nb < (1u << 30)) nb <<= 1;
+  if (ensure(c.bucket_min, static_cast<size_t>(nb) * 8) || ensure(c.bucket_max, static_cast<size_t>(nb) * 8) ||
+      ensure(c.gap_min, static_cast<size_t>(nb) * 8) || ensure(c.gap_max, static_cast<size_t>(nb) * 8) ||
+      ensure(c.gap_flag, (static_cast<size_t>(nb) + 1) * 4) || ensure(c.gap_off, (static_cast<size_t>(nb) + 1) * 4))
     return CHUI_TREEPM_ENOMEM;
-  const unsigned long long* keys[3];
-  unsigned long long* sorted[3];
-  for (int k = 0; k < axes; ++k) {
-    const int a = axis[k];
-    auto* kk = c.bucket_min.as<unsigned long long>() + static_cast<size_t>(k) * n;
-    keys[k] = kk;
-    sorted[k] = c.bucket_max.as<unsigned long long>() + static_cast<size_t>(k) * n;
-    { noteLaunch(); canonicalKeysKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in[a], box[a], canonical[a], out[a], kk); }
-  }
-  // canonical coordinates are non-negative: bit 63 is zero
-  if (int rc = radixSortKeysU64(c, axes, keys, sorted, n, 63, s)) return rc;
   auto* sc = c.scalars.as<unsigned long long>();
+  unsigned long long* suspect = sc + 16;  // one flag per axis slot
   unsigned long long init[6] = {0ull, ~0ull, 0ull, ~0ull, 0ull, ~0ull};
   cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(suspect, 0, 3 * 8, s);
+  unsigned long long* bmin = c.bucket_min.as<unsigned long long>();
+  unsigned long long* bmax = c.bucket_max.as<unsigned long long>();
+  uint32_t* flag = c.gap_flag.as<uint32_t>();
+  uint32_t* off = c.gap_off.as<uint32_t>();
   for (int k = 0; k < axes; ++k) {
     const int a = axis[k];
     unsigned long long* g = sc + 2 * k;
-    { noteLaunch(); sortedGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, sorted[k], box[a], g, 0, g + 1); }
-    { noteLaunch(); sortedGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, sorted[k], box[a], g, 1, g + 1); }
-    { noteLaunch(); applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out[a], box[a], g + 1); }
+    cudaMemsetAsync(bmin, 0xFF, static_cast<size_t>(nb) * 8, s);
+    cudaMemsetAsync(bmax, 0, static_cast<size_t>(nb) * 8, s);
+    const double scale = static_cast<double>(nb) / box[a];
+    { noteLaunch(); canonicalBucketsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in[a], box[a], canonical[a], out[a], scale,
+                                                                       nb, bmin, bmax); }
+    { noteLaunch(); bucketFlagsKernel<<<gridFor(static_cast<size_t>(nb) + 1, 256), 256, 0, s>>>(nb, bmin, flag); }
+    if (int rc = exclusiveScanU32(c, flag, off, static_cast<int64_t>(nb) + 1, s)) return rc;
+    { noteLaunch(); bucketCompactKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, bmin, bmax, off, c.gap_min.as<unsigned long long>(),
+                                                                     c.gap_max.as<unsigned long long>()); }
+    for (int pass = 0; pass < 2; ++pass) {
+      noteLaunch();
+      runGapKernel<<<gridFor(nb, 256), 256, 0, s>>>(nb, off + nb, c.gap_min.as<unsigned long long>(),
+                                                    c.gap_max.as<unsigned long long>(), box[a], g, pass, g + 1,
+                                                    suspect + k);
+    }
+    { noteLaunch(); applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out[a], box[a], g + 1, suspect + k); }
   }
-  unsigned long long ab[6];
+  unsigned long long ab[6], sus[3];
   cudaMemcpyAsync(ab, sc, sizeof(ab), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(sus, suspect, sizeof(sus), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
-  for (int k = 0; k < axes; ++k) std::memcpy(&anchor[axis[k]], &ab[2 * k + 1], 8);
+  bool resorted = false;
+  for (int k = 0; k < axes; ++k) {
+    if (!sus[k]) continue;
+    // out[a] still holds the canonical coordinates (the anchor was skipped)
+    const int a = axis[k];
+    if (ensure(c.keys_b, static_cast<size_t>(n) * 8)) return CHUI_TREEPM_ENOMEM;
+    const unsigned long long* kin = reinterpret_cast<const unsigned long long*>(out[a]);
+    unsigned long long* sorted = c.keys_b.as<unsigned long long>();
+    // canonical coordinates are non-negative: bit 63 is zero
+    if (int rc = radixSortKeysU64(c, 1, &kin, &sorted, n, 63, s)) return rc;
+    unsigned long long* g = sc + 2 * k;
+    const unsigned long long reset[2] = {0ull, ~0ull};
+    cudaMemcpyAsync(g, reset, sizeof(reset), cudaMemcpyHostToDevice, s);
+    for (int pass = 0; pass < 2; ++pass) {
+      noteLaunch();
+      runGapKernel<<<gridFor(n, 256), 256, 0, s>>>(n, nullptr, sorted, sorted, box[a], g, pass, g + 1, nullptr);
+    }
+    { noteLaunch(); applyAnchorKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out[a], box[a], g + 1, nullptr); }
+    cudaMemcpyAsync(&ab[2 * k], g, 16, cudaMemcpyDeviceToHost, s);
+    resorted = true;
+  }
+  if (resorted && cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+  c.unwrap_sorted_axes = 0;
+  for (int k = 0; k < axes; ++k) {
+    std::memcpy(&anchor[axis[k]], &ab[2 * k + 1], 8);
+    if (sus[k]) c.unwrap_sorted_axes |= 1 << axis[k];
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
 }
 
@@ -819,6 +934,8 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
               cudaStream_t s) {
   c.n_nodes = 0;
   c.max_depth = 0;
+  c.unwrap_sorted_axes = 0;
+  c.large_leaf = 0;
   if (n == 0) return 0;
   const double box[3] = {c.cfg.box_x, c.cfg.box_y, c.cfg.box_z};
   if (ensure(c.ux, n * 8) || ensure(c.uy, n * 8) || ensure(c.uz, n * 8)) return CHUI_TREEPM_ENOMEM;
@@ -858,20 +975,17 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   }
   const double max_extent = std::fmax(hi[0] - lo[0], std::fmax(hi[1] - lo[1], hi[2] - lo[2]));
 
-  // Morton keys + stable sort (tree_ordering.cpp:152-172)
+  // Morton keys (tree_ordering.cpp:152-172). The reference sorts them and
+  // partitions the sorted list into octants; here the octant paths are sorted
+  // directly and the Morton keys only order each leaf's particles.
   const double extent = std::fmax(max_extent, 1.0e-12);
   if (ensure(c.keys_a, n * 8) || ensure(c.keys_b, n * 8) || ensure(c.idx_a, n * 4) || ensure(c.idx_b, n * 4) ||
-      ensure(c.idx_c, (n + 1) * 4) || ensure(c.idx_d, (n + 1) * 4))
+      ensure(c.idx_c, (n + 1) * 4) || ensure(c.idx_d, (n + 1) * 4) || ensure(c.morton_keys, n * 8))
     return CHUI_TREEPM_ENOMEM;
+  unsigned long long* morton = c.morton_keys.as<unsigned long long>();
   { noteLaunch(); mortonKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], lo[0], lo[1], lo[2], extent,
-                                               c.keys_a.as<unsigned long long>(), c.idx_a.as<uint32_t>()); }
-  int rc = radixSortPairsU64(c, c.keys_a.as<unsigned long long>(), c.keys_b.as<unsigned long long>(),
-                           c.idx_a.as<uint32_t>(), c.idx_b.as<uint32_t>(), n, 63, s);
-  if (rc) return rc;
-  // keys_b: sorted Morton keys; idx_b: perm_m (Morton rank -> particle)
-  if (ensure(c.morton_sorted, n * 8)) return CHUI_TREEPM_ENOMEM;
-  cudaMemcpyAsync(c.morton_sorted.ptr, c.keys_b.ptr, n * 8, cudaMemcpyDeviceToDevice, s);
-  const uint32_t* perm_m = c.idx_b.as<uint32_t>();
+                                               morton, c.idx_a.as<uint32_t>()); }
+  int rc = 0;
 
   // root (tree_gravity.cpp:448-452)
   const double mext = std::fmax(max_extent, 1.0e-10);
@@ -891,6 +1005,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   uint32_t* counts = c.node_count_per_pos.as<uint32_t>();
   uint32_t* offset = c.node_offset.as<uint32_t>();
   unsigned long long* path = nullptr;
+  uint32_t* row_of_pos = nullptr;
   uint32_t total_nodes = 0;
   int words = 1;
   NodePlan plan;
@@ -908,37 +1023,34 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
         ensure(c.keys_a, static_cast<size_t>(words) * n * 8) || ensure(c.bucket_max, static_cast<size_t>(n) * 8))
       return CHUI_TREEPM_ENOMEM;
     path = c.path_words.as<unsigned long long>();
-    unsigned long long* by_rank = c.keys_a.as<unsigned long long>();
+    unsigned long long* by_row = c.keys_a.as<unsigned long long>();
     unsigned long long* key_cur = c.keys_b.as<unsigned long long>();
     unsigned long long* key_sorted = c.bucket_max.as<unsigned long long>();
-    { noteLaunch(); pathKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, perm_m, u[0], u[1], u[2], cx0, cy0, cz0, half0,
-                                               by_rank); }
+    { noteLaunch(); pathKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, nullptr, u[0], u[1], u[2], cx0, cy0, cz0, half0,
+                                               by_row); }
     uint32_t* rank_in = c.idx_c.as<uint32_t>();
     uint32_t* rank_out = c.idx_d.as<uint32_t>();
     { noteLaunch(); iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in); }
-    // the FP64 octant path order is almost always the Morton order already
-    unsigned int* unsorted_flag = reinterpret_cast<unsigned int*>(c.scalars.as<unsigned long long>() + 12);
-    cudaMemsetAsync(unsorted_flag, 0, 4, s);
-    { noteLaunch(); pathOrderCheckKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, by_rank, unsorted_flag); }
-    unsigned int unsorted = 1;
-    cudaMemcpyAsync(&unsorted, unsorted_flag, 4, cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) {
-      c.last_error = "tree path ordering failed";
-      return CHUI_TREEPM_EDEVICE;
-    }
-    for (int w = words - 1; unsorted && w >= 0; --w) {  { noteLaunch(); // LSD over path words, each pass stable
-      gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in, key_cur); }
-      rc = radixSortPairsU64(c, key_cur, key_sorted, rank_in, rank_out, n, 63, s);
+    // LSD over path words, each pass a stable sort; the first pass reads the
+    // words in row order and the last writes the sorted first word in place
+    for (int w = words - 1; w >= 0; --w) {
+      const unsigned long long* key_in = by_row + static_cast<size_t>(w) * n;
+      if (w != words - 1) {
+        noteLaunch();
+        gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, key_in, rank_in, key_cur);
+        key_in = key_cur;
+      }
+      rc = radixSortPairsU64(c, key_in, w == 0 ? path : key_sorted, rank_in, rank_out, n, 63, s);
       if (rc) return rc;
       uint32_t* t = rank_in;
       rank_in = rank_out;
       rank_out = t;
     }
-    // rank_in: path position -> Morton rank
-    for (int w = 0; w < words; ++w)
-      { noteLaunch(); gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_rank + static_cast<size_t>(w) * n, rank_in,
+    // rank_in: path position -> row
+    row_of_pos = rank_in;
+    for (int w = 1; w < words; ++w)
+      { noteLaunch(); gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_row + static_cast<size_t>(w) * n, rank_in,
                                                       path + static_cast<size_t>(w) * n); }
-    { noteLaunch(); invertKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in, c.inv_pos.as<uint32_t>()); }
     { noteLaunch(); commonPrefixKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, path, cp); }
     plan.depth_max = kLevelsPerWord * words;
     cudaMemsetAsync(status, 0, 4, s);
@@ -976,24 +1088,44 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   cudaMemsetAsync(out.leaf_of_pos, 0, n * 4, s);
   cudaMemsetAsync(out.child, 0xFF, static_cast<size_t>(total_nodes) * 8 * 4, s);  // all slots empty
   cudaMemsetAsync(status, 0, 4, s);
+  bool large_leaf = false;
   { noteLaunch(); nodeEmitKernel<<<gridFor(n, 128), 128, 0, s>>>(plan, words, path, cp, counts, offset, cx0, cy0, cz0, half0,
                                                  total_nodes, out, status); }
   {
     uint32_t est = 0;
     cudaMemcpyAsync(&est, status, 4, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
-    if (est) {
+    if (est & ~static_cast<uint32_t>(kStatusLargeLeaf)) {
       c.last_error = "tree node enumeration produced an inconsistent node range";
       return CHUI_TREEPM_EDEVICE;
     }
+    large_leaf = (est & kStatusLargeLeaf) != 0;
+    c.large_leaf = large_leaf ? 1 : 0;
   }
   { noteLaunch(); childCountKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.child, out.range); }
-  // final order: stable sort of Morton order by leaf id
-  uint32_t* leaf_key = c.idx_a.as<uint32_t>();
-  { noteLaunch(); leafKeyKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.inv_pos.as<uint32_t>(), out.leaf_of_pos, leaf_key); }
-  rc = radixSortPairsU32(c, leaf_key, c.idx_d.as<uint32_t>(), perm_m, c.sorted_index.as<uint32_t>(), n,
-                       bitsFor(total_nodes), s);
-  if (rc) return rc;
+  // final order: each leaf's particles in Morton order
+  if (!large_leaf) {
+    unsigned long long* key_of_pos = c.keys_b.as<unsigned long long>();
+    { noteLaunch(); gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, morton, row_of_pos, key_of_pos); }
+    { noteLaunch(); leafOrderKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out.leaf_of_pos, out.range, row_of_pos, key_of_pos,
+                                                    c.sorted_index.as<uint32_t>(), status); }
+  } else {
+    // a leaf above the in-place limit (particles at the depth limit): the
+    // stable Morton sort, then a stable sort of that order by leaf
+    { noteLaunch(); iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.idx_a.as<uint32_t>()); }
+    rc = radixSortPairsU64(c, morton, c.keys_b.as<unsigned long long>(), c.idx_a.as<uint32_t>(),
+                           c.idx_b.as<uint32_t>(), n, 63, s);
+    if (rc) return rc;
+    const uint32_t* perm_m = c.idx_b.as<uint32_t>();
+    { noteLaunch(); invertKernel<<<gridFor(n, 256), 256, 0, s>>>(n, row_of_pos, c.inv_pos.as<uint32_t>()); }
+    uint32_t* leaf_key = c.idx_a.as<uint32_t>();
+    { noteLaunch(); leafKeyKernel<<<gridFor(n, 256), 256, 0, s>>>(n, perm_m, c.inv_pos.as<uint32_t>(), out.leaf_of_pos,
+                                                  leaf_key); }
+    // row_of_pos may share idx_d with the sort's key output: it is not read again
+    rc = radixSortPairsU32(c, leaf_key, c.idx_d.as<uint32_t>(), perm_m, c.sorted_index.as<uint32_t>(), n,
+                           bitsFor(total_nodes), s);
+    if (rc) return rc;
+  }
   // tree-ordered source records
   const bool mixed = c.cfg.precision == CHUI_TREEPM_MIXED;
   if (mixed) {
@@ -1026,11 +1158,17 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   { noteLaunch(); nodeFrameKernel<<<gridFor(total_nodes, 256), 256, 0, s>>>(total_nodes, out.geom, c.node_com.as<double4>(),
                                                             c.node_quad.as<double>(), c.node_f4.as<float4>(),
                                                             c.node_mq.as<float4>()); }
-  // maximum depth (for stack sizing and stats)
+  // maximum depth (for stack sizing and stats); the status of the
+  // within-leaf ordering is read at the same synchronisation
   {
-    uint32_t hd = 0;
+    uint32_t hd = 0, est = 0;
+    cudaMemcpyAsync(&est, status, 4, cudaMemcpyDeviceToHost, s);
     if (maxU32(c, out.depth, total_nodes, &hd, s)) {
       c.last_error = "tree build kernels failed";
+      return CHUI_TREEPM_EDEVICE;
+    }
+    if (est & ~static_cast<uint32_t>(kStatusLargeLeaf)) {
+      c.last_error = "tree leaf ordering produced an inconsistent index";
       return CHUI_TREEPM_EDEVICE;
     }
     c.max_depth = hd;

@@ -338,3 +338,54 @@ def test_short_range_only_is_the_tree_part(cuda_ok, name):
             for k in ("x", "y", "z"):
                 assert np.abs(r["a" + k] - g["tree_a" + k][rows]).max() <= 1e-9 * scale, k
                 assert np.all(r["pm_a" + k] == 0.0)
+
+
+def _forms_case(kind, seed=11):
+    """Particle sets that take each form of the tree build: evenly spaced
+    distinct x (the gap buckets could hide the largest gap, so the unwrap
+    sorts that axis), 1500 coincident particles (one leaf above the in-place
+    ordering limit at the depth limit), and a clustered set (neither)."""
+    rng = np.random.default_rng(seed)
+    if kind == "spaced_x":
+        n = 4096
+        x = (rng.permutation(n) + 0.5) / n
+        y, z = rng.random(n), rng.random(n)
+    elif kind == "large_leaf":
+        p = rng.random(3)
+        x = np.concatenate([np.full(1500, p[0]), rng.random(2000)])
+        y = np.concatenate([np.full(1500, p[1]), rng.random(2000)])
+        z = np.concatenate([np.full(1500, p[2]), rng.random(2000)])
+    else:
+        c = rng.random((40, 3))
+        pts = (c[rng.integers(0, 40, 20000)] + 0.02 * rng.standard_normal((20000, 3))) % 1.0
+        x, y, z = pts[:, 0].copy(), pts[:, 1].copy(), pts[:, 2].copy()
+        x[:50] -= 1.0  # some coordinates outside [0, L): the canonical map applies
+    m = np.full(len(x), 1.0 / len(x))
+    return x, y, z, m
+
+
+@pytest.mark.parametrize("kind", ["spaced_x", "large_leaf", "clustered"])
+@pytest.mark.parametrize("precision", [ct._abi.FP64, ct._abi.MIXED])
+def test_tree_build_forms_match_oracle(cuda_ok, kind, precision):
+    x, y, z, m = _forms_case(kind)
+    p = oracle.make_params(box=(1.0, 1.0, 1.0), mesh=(16, 16, 16), eps=0.01, leaf=16)
+    cfg = ct.TreePmConfig(pm_grid_nx=16, pm_grid_ny=16, pm_grid_nz=16, box_x=1.0, box_y=1.0, box_z=1.0,
+                          asmth_cells=1.25, rcut_cells=6.25, opening_theta=0.5, opening_criterion=1,
+                          multipole_order=2, max_leaf_size=16, softening=0.01, precision=precision)
+    with ct.TreePmCoordinator(cfg) as s:
+        s.solve_active_set(x, y, z, m)
+        t = s.dump_tree(len(x))
+    u = []
+    for a, v in enumerate((x, y, z)):
+        ua, anchor = oracle.unwrap_axis(v, 1.0, bool(v.min() >= 0.0 and v.max() < 1.0))
+        assert np.array_equal(t["u" + "xyz"[a]], ua), a
+        assert t["anchors"][a] == anchor, a
+        u.append(ua)
+    o = oracle.tree_build(u[0], u[1], u[2], m, p)
+    assert t["n_nodes"] == o["n_nodes"]
+    for k in ("morton_key", "sorted_index", "particle_begin", "particle_count", "child_count", "child_index"):
+        assert np.array_equal(t[k], o[k]), k
+    assert np.array_equal(t["half_size"], o["half"])
+    expect_sorted = 1 if kind == "spaced_x" else 0
+    assert t["unwrap_sorted_axes"] == expect_sorted
+    assert t["large_leaf"] == (kind == "large_leaf")
