@@ -396,10 +396,10 @@ class TreePmCoordinator:
         anchors = np.zeros(3)
         self._check(self._lib.chui_treepm_dump_particles(self._h, n, ux.ctypes.data, uy.ctypes.data, uz.ctypes.data,
                                                          mk.ctypes.data, si.ctypes.data, anchors.ctypes.data))
-        info = np.zeros(2, dtype=np.int32)
+        info = np.zeros(3, dtype=np.int32)
         self._check(self._lib.chui_treepm_tree_build_info(self._h, info.ctypes.data))
         r.update(ux=ux, uy=uy, uz=uz, morton_key=mk, sorted_index=si, anchors=anchors, n_nodes=nn,
-                 unwrap_sorted_axes=int(info[0]), large_leaf=bool(info[1]))
+                 unwrap_sorted_axes=int(info[0]), large_leaf=bool(info[1]), path_levels_retried=bool(info[2]))
         return r
 
     # -- KDK ------------------------------------------------------------------

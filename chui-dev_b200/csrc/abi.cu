@@ -388,10 +388,14 @@ PolyH fitChebyshev(F func, double t_cut, double tolerance = 2.0e-6, int short_te
   return best;
 }
 
-// H for the pair kernel: 10 terms (4.1e-6 relative at r_cut/r_s = 5; the
-// residual's FP32 evaluation error is of the same order) keep two FMAs per
-// pair out of the issue-bound walk; otherwise the long form.
-PolyH fitPoly(double t_cut) { return fitChebyshev(hostH, t_cut, 5.0e-6, kPairPolyTerms); }
+// H for the pair kernel: 9 terms (2.9e-5 relative at r_cut/r_s = 5) keep
+// FMAs out of the issue-bound walk; at 256^3 the forces then differ from the
+// FP64 solve by median 2.5e-7, p99 3.0e-6 (10 terms: 1.9e-7, 2.0e-6);
+// configurations the short form cannot fit take the long one.
+#ifndef CHUI_PAIR_TOLERANCE
+#define CHUI_PAIR_TOLERANCE 5.0e-5
+#endif
+PolyH fitPoly(double t_cut) { return fitChebyshev(hostH, t_cut, CHUI_PAIR_TOLERANCE, kPairPolyTerms); }
 
 int fail(Context& c, int code, const std::string& msg) {
   c.last_error = msg;
@@ -711,7 +715,7 @@ void chui_treepm_destroy(void* handle) {
                             &c->grp_leaf, &c->grp_start, &c->grp_rec, &c->grp_list, &c->grp_done, &c->gauss_tab,
                             &c->out_acc[0], &c->out_acc[1], &c->out_acc[2], &c->out_pm[0], &c->out_pm[1],
                             &c->out_pm[2], &c->out_tree[0], &c->out_tree[1], &c->out_tree[2], &c->out_near,
-                            &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max, &c->gap_min, &c->gap_max, &c->gap_flag, &c->gap_off,
+                            &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max, &c->gap_min, &c->gap_max, &c->gap_flag, &c->gap_off, &c->cp_levels,
                             &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
                             &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
                             &c->leaf_of_pos, &c->inv_pos, &c->sort_hist, &c->sort_counts,
@@ -1493,11 +1497,12 @@ int chui_pm_cells(void* handle, const chui_treepm_sources* src, int64_t* cells, 
   return rc;
 }
 
-int chui_treepm_tree_build_info(const void* handle, int32_t info[2]) {
+int chui_treepm_tree_build_info(const void* handle, int32_t info[3]) {
   if (!handle || !info) return CHUI_TREEPM_EINVAL;
   const Context& c = *static_cast<const Context*>(handle);
   info[0] = c.unwrap_sorted_axes;
   info[1] = c.large_leaf;
+  info[2] = c.path_levels_retried;
   return 0;
 }
 

@@ -17,7 +17,10 @@ constexpr int kMaxPathWords = 4;         // 84 levels > kMaxDepth
 constexpr int kWalkWarpsPerBlock = 4;
 constexpr int kStackCap = 1 + 7 * kMaxDepth;  // tree_pm_coupling.cpp:899-925 stack bound
 constexpr int kPolyMaxTerms = 20;
-constexpr int kPairPolyTerms = 10;  // short form of the pair kernel's H(t) polynomial
+#ifndef CHUI_PAIR_TERMS
+#define CHUI_PAIR_TERMS 9
+#endif
+constexpr int kPairPolyTerms = CHUI_PAIR_TERMS;  // short form of the pair kernel's H(t) polynomial
 
 // Status bits written by kernels instead of trapping.
 enum StatusBits : uint32_t {

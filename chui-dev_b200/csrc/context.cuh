@@ -114,6 +114,7 @@ struct Context {
   DevBuf keys_a, keys_b, idx_a, idx_b, idx_c, idx_d;
   DevBuf path_words;             // kMaxPathWords * n u64
   DevBuf common_prefix;          // int8/int32 per sorted position
+  DevBuf cp_levels;              // block minima of the common prefix (levels 1..)
   DevBuf node_count_per_pos, node_offset;  // per sorted position (n+1)
   DevBuf leaf_of_pos, inv_pos;
   // radix sort and scan scratch (sort.cu)
@@ -122,7 +123,9 @@ struct Context {
   uint32_t max_depth = 0;
   int path_words_used = 0;
   int unwrap_sorted_axes = 0;  // axes whose unwrap sorted the coordinates (bit a)
-  int large_leaf = 0;          // the last build ordered a leaf above kLeafOrderMax globally
+  int prev_tree_depth = 0;     // depth of the previous tree built by this context (0: none)
+  int large_leaf = 0;
+  int path_levels_retried = 0;  // the last build repeated the path sort with every level          // the last build ordered a leaf above kLeafOrderMax globally
   double tree_anchor[3] = {0, 0, 0};
 
   // nodes (SoA, FP64 geometry/moments)

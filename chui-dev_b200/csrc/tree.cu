@@ -23,6 +23,8 @@
 //     order, by the last child to finish.
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -51,9 +53,9 @@ __device__ __forceinline__ double bitsd(unsigned long long b) {
 // coordinates sorted by their non-negative IEEE bits, the largest circular gap
 // between neighbours, and one box added below the value after it.
 //
-// The canonical periodic coordinate (tree_pm_coupling.cpp:166-183). One
-// compiled copy (not inlined) serves the unwrap and the source packing, which
-// recomputes the tree-frame coordinate and must get the same bits.
+// The canonical periodic coordinate (tree_pm_coupling.cpp:166-183), one
+// compiled copy (not inlined, so that no caller's contraction changes its
+// bits).
 __device__ __noinline__ double canonicalCoordinate(double x, double box, int canonical) {
   double v = canonical ? x : x - box * floor(x / box);
   if (v >= box) {
@@ -258,7 +260,7 @@ __global__ void mortonKernel(int64_t n, const double* __restrict__ ux, const dou
 __global__ void pathKernel(int64_t n, int words, const uint32_t* __restrict__ perm,
                            const double* __restrict__ ux, const double* __restrict__ uy,
                            const double* __restrict__ uz, double cx0, double cy0, double cz0,
-                           double half0, unsigned long long* path /* words * n */) {
+                           double half0, unsigned long long mask0, unsigned long long* path /* words * n */) {
   for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < n;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const uint32_t p = perm ? perm[j] : static_cast<uint32_t>(j);
@@ -275,7 +277,7 @@ __global__ void pathKernel(int64_t n, int words, const uint32_t* __restrict__ pe
         cz = __dadd_rn(cz, (o & 1u) ? ch : -ch);
         h = ch;
       }
-      path[static_cast<size_t>(w) * n + j] = word;
+      path[static_cast<size_t>(w) * n + j] = w == 0 ? word & mask0 : word;
     }
   }
 }
@@ -296,7 +298,7 @@ __device__ __forceinline__ unsigned digitAt(const unsigned long long* path, int6
 }
 
 // Number of leading equal digits of the paths at sorted positions i-1, i.
-__global__ void commonPrefixKernel(int64_t n, int words, const unsigned long long* __restrict__ path,
+__global__ void commonPrefixKernel(int64_t n, int words, int levels, const unsigned long long* __restrict__ path,
                                    int* cp) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -304,7 +306,7 @@ __global__ void commonPrefixKernel(int64_t n, int words, const unsigned long lon
       cp[0] = -1;
       continue;
     }
-    int c = kLevelsPerWord * words;
+    int c = levels;  // equal through every resolved level
     for (int w = 0; w < words; ++w) {
       const unsigned long long x = path[static_cast<size_t>(w) * n + i - 1] ^ path[static_cast<size_t>(w) * n + i];
       if (x != 0) {
@@ -376,56 +378,73 @@ __global__ void nodeCountKernel(NodePlan p, const int* __restrict__ cp, uint32_t
   }
 }
 
-// First sorted position > i whose path differs from path[i] within `d` levels.
-__device__ int64_t runEnd(const unsigned long long* __restrict__ path, int64_t n, int words,
-                          const int* __restrict__ cp, int64_t i, int d, int leaf) {
-  for (int64_t k = i + 1; k < n && k <= i + leaf; ++k) {
-    if (cp[k] < d) return k;
+// Block minima of the common-prefix lengths: level 0 is cp itself, entry b of
+// level L+1 the minimum of entries 32b .. 32b+31 of level L. Node ends and
+// run starts are then nearest-smaller queries that scan at most 32 entries
+// per level up and down instead of searching the path words.
+constexpr int kCpLevels = 7;
+struct CpLevels {
+  const int* lv[kCpLevels];
+  int64_t len[kCpLevels];
+  int count;  // levels in use; the top one is scanned whole
+};
+
+__global__ void cpBlockMinKernel(int64_t len, const int* __restrict__ in, int* out) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t whole = (len + 31) / 32 * 32;  // whole warps: every lane takes part in the reduction
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < whole; i += stride) {
+    const int v = i < len ? in[i] : INT_MAX;
+    const int m = __reduce_min_sync(0xffffffffu, v);
+    if ((threadIdx.x & 31) == 0) out[i >> 5] = m;
   }
-  if (i + leaf + 1 >= n) return n;
-  // binary search on the sorted paths for the end of the d-digit prefix
-  int64_t lo = i + leaf, hi = n;  // cp[...] >= d through lo
-  while (hi - lo > 1) {
-    const int64_t mid = lo + (hi - lo) / 2;
-    // prefix equal through d digits <=> common prefix of (i, mid) >= d
-    int common = kLevelsPerWord * words;
-    for (int w = 0; w < words; ++w) {
-      const unsigned long long x = path[static_cast<size_t>(w) * n + i] ^ path[static_cast<size_t>(w) * n + mid];
-      if (x != 0) {
-        common = kLevelsPerWord * w + (__clzll(static_cast<long long>(x)) - 1) / 3;
-        break;
-      }
-    }
-    if (common >= d) lo = mid;
-    else hi = mid;
-  }
-  return hi;
 }
 
-// First sorted position <= i whose d-digit prefix equals path[i]'s.
-__device__ int64_t runStart(const unsigned long long* __restrict__ path, int64_t n, int words,
-                            const int* __restrict__ cp, int64_t i, int d) {
+// First position k > i with cp[k] < t, or n.
+__device__ int64_t nextBelow(const CpLevels& c, int64_t i, int t) {
+  int64_t k = i + 1;
+  int level = 0;
+  for (;;) {
+    const int64_t len = c.len[level];
+    const int64_t end = level + 1 == c.count ? len : ((k >> 5) + 1) << 5;
+    const int64_t stop = end < len ? end : len;
+    for (; k < stop; ++k)
+      if (c.lv[level][k] < t) goto found;
+    if (stop >= len) return c.len[0];
+    k = stop >> 5;
+    ++level;
+  }
+found:
+  while (level > 0) {
+    --level;
+    const int64_t b = k << 5;
+    const int64_t e = b + 32 < c.len[level] ? b + 32 : c.len[level];
+    for (k = b; k < e; ++k)
+      if (c.lv[level][k] < t) break;
+  }
+  return k;
+}
+
+// Last position k <= i with cp[k] < t, or -1.
+__device__ int64_t prevBelow(const CpLevels& c, int64_t i, int t) {
   int64_t k = i;
-  for (int step = 0; step < 64 && k > 0; ++step) {
-    if (cp[k] < d) return k;
-    --k;
+  int level = 0;
+  for (;;) {
+    const int64_t beg = level + 1 == c.count ? 0 : (k >> 5) << 5;
+    for (; k >= beg; --k)
+      if (c.lv[level][k] < t) goto found;
+    if (beg == 0) return -1;
+    k = (beg >> 5) - 1;
+    ++level;
   }
-  if (k == 0) return 0;
-  int64_t lo = -1, hi = k;  // answer in (lo, hi]
-  while (hi - lo > 1) {
-    const int64_t mid = lo + (hi - lo) / 2;
-    int common = kLevelsPerWord * words;
-    for (int w = 0; w < words; ++w) {
-      const unsigned long long x = path[static_cast<size_t>(w) * n + i] ^ path[static_cast<size_t>(w) * n + mid];
-      if (x != 0) {
-        common = kLevelsPerWord * w + (__clzll(static_cast<long long>(x)) - 1) / 3;
-        break;
-      }
-    }
-    if (common >= d) hi = mid;
-    else lo = mid;
+found:
+  while (level > 0) {
+    --level;
+    const int64_t b = k << 5;
+    const int64_t e = b + 32 < c.len[level] ? b + 32 : c.len[level];
+    for (k = e - 1; k >= b; --k)
+      if (c.lv[level][k] < t) break;
   }
-  return hi;
+  return k;
 }
 
 struct NodeOut {
@@ -440,8 +459,8 @@ struct NodeOut {
 // Emit the chain of nodes started at each sorted position, in preorder.
 __global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* __restrict__ path,
                                const int* __restrict__ cp, const uint32_t* __restrict__ counts,
-                               const uint32_t* __restrict__ offset, double cx0, double cy0, double cz0,
-                               double half0, uint32_t total_nodes, NodeOut out, uint32_t* status) {
+                               const uint32_t* __restrict__ offset, CpLevels lv, double cx0, double cy0,
+                               double cz0, double half0, uint32_t total_nodes, NodeOut out, uint32_t* status) {
   const int64_t n = p.n;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -470,7 +489,8 @@ __global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* 
         h = ch;
       }
       const uint32_t node = offset[i] + static_cast<uint32_t>(d - d0);
-      const int64_t end = (d == 0) ? n : runEnd(path, n, words, cp, i, d, p.leaf);
+      // the run of the d-digit prefix ends where the common prefix drops below d
+      const int64_t end = (d == 0) ? n : nextBelow(lv, i, d);
       if (node >= total_nodes || end > n || end <= i) {
         atomicOr(status, kStatusIndexRange);
         return;
@@ -486,7 +506,12 @@ __global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* 
         if (d > d0) {
           parent = node - 1;
         } else {
-          const int64_t s = runStart(path, n, words, cp, i, d - 1);
+          // the parent's run starts at the last position whose prefix differs within d - 1 digits
+          const int64_t s = prevBelow(lv, i, d - 1);
+          if (s < 0) {
+            atomicOr(status, kStatusIndexRange);
+            return;
+          }
           parent = offset[s] + static_cast<uint32_t>((d - 1) - (cp[s] + 1));
         }
         if (parent >= total_nodes) {
@@ -764,43 +789,23 @@ __global__ void nodeBoundsKernel(int64_t nodes, const double4* __restrict__ geom
   }
 }
 
-// Tree-ordered source records. Mixed precision: FP32 offset of the unwrapped
-// position from its leaf's FP64 centre, plus mass. FP64: the caller's
-// position (the reference's source lanes, :3736-3800) plus mass.
-// How the tree frame follows from the caller's coordinates, per axis: the
-// canonical coordinate plus one box below the anchor (periodic), or the
-// coordinate itself (isolated/open).
-struct FrameSpec {
-  double box[3], anchor[3];
-  int canonical[3];
-  int periodic;
-};
-
-__device__ __forceinline__ double treeFrameCoordinate(double x, const FrameSpec& f, int a) {
-  if (!f.periodic) return x;
-  double v = canonicalCoordinate(x, f.box[a], f.canonical[a]);
-  if (v < f.anchor[a]) v += f.box[a];  // applyAnchorKernel
-  return v;
-}
-
-// Tree-ordered source records, written from row order: each row's caller
-// position, mass and softening are read contiguously and its records are
-// scattered to its tree position (whole 32-byte records: no partial
-// sectors); the tree-frame coordinates are recomputed from the caller's
-// (the same arithmetic as the unwrap).
-__global__ void scatterSourcesKernel(int64_t n, const uint32_t* __restrict__ pos_of_row, FrameSpec frame,
+// Tree-ordered source records (the reference's source lanes,
+// tree_pm_coupling.cpp:3736-3800), written from row order: each row's caller
+// position, tree-frame position (the unwrapped coordinates), mass and
+// softening are read contiguously and its records are scattered to its tree
+// position (whole 32-byte records: no partial sectors).
+__global__ void scatterSourcesKernel(int64_t n, const uint32_t* __restrict__ pos_of_row,
                                      const double* __restrict__ x, const double* __restrict__ y,
-                                     const double* __restrict__ z, const double* __restrict__ m, double uniform_mass,
-                                     double4* d4, double4* u4, const double* __restrict__ eps_rows,
-                                     double* eps_tree) {
+                                     const double* __restrict__ z, const double* __restrict__ ux,
+                                     const double* __restrict__ uy, const double* __restrict__ uz,
+                                     const double* __restrict__ m, double uniform_mass, double4* d4, double4* u4,
+                                     const double* __restrict__ eps_rows, double* eps_tree) {
   for (int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; s < n;
        s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const uint32_t t = pos_of_row[s];
     const double ms = m ? m[s] : uniform_mass;
-    const double px = x[s], py = y[s], pz = z[s];
-    d4[t] = make_double4(px, py, pz, ms);
-    u4[t] = make_double4(treeFrameCoordinate(px, frame, 0), treeFrameCoordinate(py, frame, 1),
-                         treeFrameCoordinate(pz, frame, 2), ms);
+    d4[t] = make_double4(x[s], y[s], z[s], ms);
+    u4[t] = make_double4(ux[s], uy[s], uz[s], ms);
     if (eps_rows) eps_tree[t] = eps_rows[s];
   }
 }
@@ -936,20 +941,17 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   c.max_depth = 0;
   c.unwrap_sorted_axes = 0;
   c.large_leaf = 0;
+  c.path_levels_retried = 0;
   if (n == 0) return 0;
   const double box[3] = {c.cfg.box_x, c.cfg.box_y, c.cfg.box_z};
   if (ensure(c.ux, n * 8) || ensure(c.uy, n * 8) || ensure(c.uz, n * 8)) return CHUI_TREEPM_ENOMEM;
   const double* in[3] = {x, y, z};
   double* u[3] = {c.ux.as<double>(), c.uy.as<double>(), c.uz.as<double>()};
   double anchors[3];
-  FrameSpec frame;
-  frame.periodic = c.cfg.boundary_condition == CHUI_TREEPM_BOUNDARY_PERIODIC ? 1 : 0;
   int canonical[3], axis[3], axes = 0;
   for (int a = 0; a < 3; ++a) {
-    frame.box[a] = box[a];
     // canonical flag as tree_pm_coupling.cpp:3183-3194
     canonical[a] = src_lo[a] >= 0.0 && src_hi[a] < box[a];
-    frame.canonical[a] = canonical[a];
     if (c.cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC) {
       // isolated/open: the tree takes the caller's coordinates (tree_pm_coupling.cpp:3179-3196)
       cudaMemcpyAsync(u[a], in[a], static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
@@ -959,7 +961,6 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     axis[axes++] = a;
   }
   if (int rc = unwrapAxes(c, n, axes, axis, in, box, canonical, u, anchors, s)) return rc;
-  for (int a = 0; a < 3; ++a) frame.anchor[a] = anchors[a];
   // bounds of the unwrapped frame
   auto* sc = c.scalars.as<unsigned long long>();
   unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
@@ -1012,6 +1013,17 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   plan.n = n;
   plan.leaf = static_cast<int>(c.cfg.max_leaf_size);
   plan.depth_half = depth_half;
+  // The first attempt resolves only the levels the previous tree of this
+  // context needed (plus one): the lower digits of the path word are zeroed,
+  // so the sort skips them. A node that needs a deeper level raises the
+  // same status as a missing path word, and the build repeats with every
+  // level of the word.
+  int masked_levels = kLevelsPerWord;
+  if (c.prev_tree_depth > 0) {
+    const int need = c.prev_tree_depth + 1 < kLevelsPerWord ? c.prev_tree_depth + 1 : kLevelsPerWord;
+    const int zero_digits = (3 * kLevelsPerWord - 3 * need) / 8;  // whole 8-bit digits below the kept levels
+    masked_levels = (3 * kLevelsPerWord - 8 * zero_digits) / 3;
+  }
   for (;; ++words) {
     if (words > kMaxPathWords) {
       c.last_error = "Tree gravity maximum depth contract exceeded";
@@ -1026,8 +1038,11 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     unsigned long long* by_row = c.keys_a.as<unsigned long long>();
     unsigned long long* key_cur = c.keys_b.as<unsigned long long>();
     unsigned long long* key_sorted = c.bucket_max.as<unsigned long long>();
+    const bool masked = words == 1 && masked_levels < kLevelsPerWord;
+    const int levels = masked ? masked_levels : kLevelsPerWord * words;
+    const unsigned long long mask0 = masked ? ~((1ull << (3 * (kLevelsPerWord - masked_levels))) - 1ull) : ~0ull;
     { noteLaunch(); pathKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, nullptr, u[0], u[1], u[2], cx0, cy0, cz0, half0,
-                                               by_row); }
+                                               mask0, by_row); }
     uint32_t* rank_in = c.idx_c.as<uint32_t>();
     uint32_t* rank_out = c.idx_d.as<uint32_t>();
     { noteLaunch(); iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(n, rank_in); }
@@ -1051,8 +1066,8 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     for (int w = 1; w < words; ++w)
       { noteLaunch(); gatherU64Kernel<<<gridFor(n, 256), 256, 0, s>>>(n, by_row + static_cast<size_t>(w) * n, rank_in,
                                                       path + static_cast<size_t>(w) * n); }
-    { noteLaunch(); commonPrefixKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, path, cp); }
-    plan.depth_max = kLevelsPerWord * words;
+    { noteLaunch(); commonPrefixKernel<<<gridFor(n, 256), 256, 0, s>>>(n, words, levels, path, cp); }
+    plan.depth_max = levels;
     cudaMemsetAsync(status, 0, 4, s);
     { noteLaunch(); nodeCountKernel<<<gridFor(n + 1, 256), 256, 0, s>>>(plan, cp, counts, status); }
     if ((rc = exclusiveScanU32(c, counts, offset, n + 1, s))) return rc;
@@ -1063,7 +1078,14 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
       c.last_error = "tree node enumeration failed";
       return CHUI_TREEPM_EDEVICE;
     }
-    if (hs[0] & kStatusNeedMorePathWords) continue;
+    if (hs[0] & kStatusNeedMorePathWords) {
+      if (masked) {
+        masked_levels = kLevelsPerWord;  // the same word count with every level
+        c.path_levels_retried = 1;
+        --words;
+      }
+      continue;
+    }
     if (hs[0] & kStatusDepthExceeded) {
       c.last_error = "Tree gravity maximum depth contract exceeded";
       return CHUI_TREEPM_ERANGE;
@@ -1089,8 +1111,30 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   cudaMemsetAsync(out.child, 0xFF, static_cast<size_t>(total_nodes) * 8 * 4, s);  // all slots empty
   cudaMemsetAsync(status, 0, 4, s);
   bool large_leaf = false;
-  { noteLaunch(); nodeEmitKernel<<<gridFor(n, 128), 128, 0, s>>>(plan, words, path, cp, counts, offset, cx0, cy0, cz0, half0,
-                                                 total_nodes, out, status); }
+  // block minima of the common-prefix lengths for the run queries
+  CpLevels lv{};
+  {
+    size_t total = 0;
+    int64_t len = n;
+    lv.lv[0] = cp;
+    lv.len[0] = n;
+    lv.count = 1;
+    while (len > 32 && lv.count < kCpLevels) {
+      len = (len + 31) / 32;
+      lv.len[lv.count++] = len;
+      total += static_cast<size_t>(len);
+    }
+    if (ensure(c.cp_levels, (total + 1) * sizeof(int))) return CHUI_TREEPM_ENOMEM;
+    int* dst = c.cp_levels.as<int>();
+    for (int l = 1; l < lv.count; ++l) {
+      noteLaunch();
+      cpBlockMinKernel<<<gridFor(lv.len[l - 1], 256), 256, 0, s>>>(lv.len[l - 1], lv.lv[l - 1], dst);
+      lv.lv[l] = dst;
+      dst += lv.len[l];
+    }
+  }
+  { noteLaunch(); nodeEmitKernel<<<gridFor(n, 128), 128, 0, s>>>(plan, words, path, cp, counts, offset, lv, cx0, cy0, cz0,
+                                                 half0, total_nodes, out, status); }
   {
     uint32_t est = 0;
     cudaMemcpyAsync(&est, status, 4, cudaMemcpyDeviceToHost, s);
@@ -1137,9 +1181,10 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
     return CHUI_TREEPM_ENOMEM;
   // tree position of each row, then the records scattered from row order
   { noteLaunch(); invertKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.sorted_index.as<uint32_t>(), c.pos_of_row.as<uint32_t>()); }
-  { noteLaunch(); scatterSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.pos_of_row.as<uint32_t>(), frame, x, y, z, m,
-                                                       uniform_mass, c.src_d4.as<double4>(), c.src_u4.as<double4>(),
-                                                       c.soft_rows, c.soft_rows ? c.src_eps.as<double>() : nullptr); }
+  { noteLaunch(); scatterSourcesKernel<<<gridFor(n, 256), 256, 0, s>>>(n, c.pos_of_row.as<uint32_t>(), x, y, z, u[0], u[1],
+                                                       u[2], m, uniform_mass, c.src_d4.as<double4>(),
+                                                       c.src_u4.as<double4>(), c.soft_rows,
+                                                       c.soft_rows ? c.src_eps.as<double>() : nullptr); }
   if (mixed)
     { noteLaunch(); leafOffsetsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, out.leaf_of_pos, out.geom, c.src_u4.as<double4>(),
                                                       c.src_f4.as<float4>()); }
@@ -1172,6 +1217,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
       return CHUI_TREEPM_EDEVICE;
     }
     c.max_depth = hd;
+    c.prev_tree_depth = static_cast<int>(hd);
   }
   c.tree_anchor[0] = anchors[0];
   c.tree_anchor[1] = anchors[1];

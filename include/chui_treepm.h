@@ -279,8 +279,10 @@ int chui_treepm_dump_tree(void *handle, const chui_treepm_tree_dump *dump);
  * tree is the same either way): info[0] has bit a set when axis a's periodic
  * unwrap sorted the coordinates because its gap buckets could hide the
  * largest gap; info[1] is 1 when a leaf held more particles than the
- * in-place within-leaf ordering takes and the Morton order was sorted. */
-int chui_treepm_tree_build_info(const void *handle, int32_t info[2]);
+ * in-place within-leaf ordering takes and the Morton order was sorted;
+ * info[2] is 1 when the octant paths, first sorted by the levels the
+ * context's previous tree needed, were sorted again by every level. */
+int chui_treepm_tree_build_info(const void *handle, int32_t info[3]);
 
 /* Particle-level parity dump after the last solve of n sources: unwrapped
  * tree-frame coordinates (m_tree_source_{x,y,z}_comoving), Morton keys in

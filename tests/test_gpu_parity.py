@@ -364,17 +364,7 @@ def _forms_case(kind, seed=11):
     return x, y, z, m
 
 
-@pytest.mark.parametrize("kind", ["spaced_x", "large_leaf", "clustered"])
-@pytest.mark.parametrize("precision", [ct._abi.FP64, ct._abi.MIXED])
-def test_tree_build_forms_match_oracle(cuda_ok, kind, precision):
-    x, y, z, m = _forms_case(kind)
-    p = oracle.make_params(box=(1.0, 1.0, 1.0), mesh=(16, 16, 16), eps=0.01, leaf=16)
-    cfg = ct.TreePmConfig(pm_grid_nx=16, pm_grid_ny=16, pm_grid_nz=16, box_x=1.0, box_y=1.0, box_z=1.0,
-                          asmth_cells=1.25, rcut_cells=6.25, opening_theta=0.5, opening_criterion=1,
-                          multipole_order=2, max_leaf_size=16, softening=0.01, precision=precision)
-    with ct.TreePmCoordinator(cfg) as s:
-        s.solve_active_set(x, y, z, m)
-        t = s.dump_tree(len(x))
+def _check_tree_against_oracle(t, x, y, z, m, p):
     u = []
     for a, v in enumerate((x, y, z)):
         ua, anchor = oracle.unwrap_axis(v, 1.0, bool(v.min() >= 0.0 and v.max() < 1.0))
@@ -386,6 +376,32 @@ def test_tree_build_forms_match_oracle(cuda_ok, kind, precision):
     for k in ("morton_key", "sorted_index", "particle_begin", "particle_count", "child_count", "child_index"):
         assert np.array_equal(t[k], o[k]), k
     assert np.array_equal(t["half_size"], o["half"])
-    expect_sorted = 1 if kind == "spaced_x" else 0
-    assert t["unwrap_sorted_axes"] == expect_sorted
-    assert t["large_leaf"] == (kind == "large_leaf")
+
+
+@pytest.mark.parametrize("kind", ["spaced_x", "large_leaf", "clustered"])
+@pytest.mark.parametrize("precision", [ct._abi.FP64, ct._abi.MIXED])
+def test_tree_build_forms_match_oracle(cuda_ok, kind, precision):
+    """Each form of the build gives the oracle's tree: the unwrap by gap
+    buckets or by sorting, the in-place or global within-leaf order, and the
+    path sort by the previous tree's levels, repeated with every level when
+    the tree is deeper (a shallow set first), or kept (the same set again)."""
+    x, y, z, m = _forms_case(kind)
+    p = oracle.make_params(box=(1.0, 1.0, 1.0), mesh=(16, 16, 16), eps=0.01, leaf=16)
+    cfg = ct.TreePmConfig(pm_grid_nx=16, pm_grid_ny=16, pm_grid_nz=16, box_x=1.0, box_y=1.0, box_z=1.0,
+                          asmth_cells=1.25, rcut_cells=6.25, opening_theta=0.5, opening_criterion=1,
+                          multipole_order=2, max_leaf_size=16, softening=0.01, precision=precision)
+    rng = np.random.default_rng(5)
+    shallow = rng.random((3, 24))  # a root and its octants: depth 1
+    with ct.TreePmCoordinator(cfg) as s:
+        s.solve_active_set(shallow[0], shallow[1], shallow[2], np.full(24, 1.0 / 24))
+        assert s.dump_tree(24)["n_nodes"] <= 9
+        trees = []
+        for _ in range(2):
+            s.solve_active_set(x, y, z, m)
+            trees.append(s.dump_tree(len(x)))
+    for t in trees:
+        _check_tree_against_oracle(t, x, y, z, m, p)
+        assert t["unwrap_sorted_axes"] == (1 if kind == "spaced_x" else 0)
+        assert t["large_leaf"] == (kind == "large_leaf")
+    # the shallow tree's levels do not resolve these trees; the repeat's own do
+    assert trees[0]["path_levels_retried"] and not trees[1]["path_levels_retried"]
