@@ -248,10 +248,10 @@ int chui_pm_assign_density(void *handle, const chui_treepm_sources *sources, dou
  * is host or device memory as density_memory says. The call zeroes the
  * scratch grid itself; nothing has to start at zero.
  *
- * The first call on a device looks up the scratch address (per-device set-up);
- * make it before any stream capture on that device. All calls on a device in
- * one process share the scratch grid and overlapping calls would race, so each
- * call holds a process-wide lock and waits for its stream before returning.
+ * The first call on a device also looks up the scratch address (a one-time
+ * per-device set-up). All calls on a device in one process share the scratch
+ * grid and overlapping calls would race, so each call holds a process-wide
+ * lock and synchronises its stream (cudaStreamSynchronize) before returning.
  * Errors: chui_treepm_last_error(NULL) describes the last failure. */
 #define CHUI_PM_STATIC_MAX_CELLS 262144
 int chui_pm_assign_density_static(const chui_treepm_config *config, const chui_treepm_sources *sources,
