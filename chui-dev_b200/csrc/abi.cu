@@ -548,7 +548,7 @@ int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const 
   cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(c.status.ptr, 0, 4, s);
   if (n > 0)
-    { noteLaunch(); sourceReduceKernel<<<gridFor(n, 256), 256, 0, s>>>(n, x, y, z, m, sc, reinterpret_cast<double*>(sc + 6),
+    { noteLaunch(); sourceReduceKernel<<<std::min(gridFor(n, 256), kReduceBlocks), 256, 0, s>>>(n, x, y, z, m, sc, reinterpret_cast<double*>(sc + 6),
                                                        c.status.as<uint32_t>()); }
   unsigned long long hb[10];
   uint32_t st = 0;

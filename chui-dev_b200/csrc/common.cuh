@@ -12,6 +12,10 @@ namespace chui {
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr int kMaxDepth = 64;            // tree_gravity.hpp:17 (kMaximumTreeDepth)
 constexpr int kLevelsPerWord = 21;       // 3 octant bits per level, 63 bits per path word
+// Grid of the reductions whose warps end in atomics on a few adjacent words:
+// four blocks per SM keep those atomics (serialised on one L2 line) to a few
+// thousand while the grid-stride loops still stream at full bandwidth.
+constexpr unsigned kReduceBlocks = 148u * 4u;
 constexpr int kLeafOrderMax = 1024;      // largest leaf ordered in place (larger: one more global sort)
 constexpr int kMaxPathWords = 4;         // 84 levels > kMaxDepth
 constexpr int kWalkWarpsPerBlock = 4;

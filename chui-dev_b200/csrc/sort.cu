@@ -17,6 +17,7 @@
 //    by digit, and writes each digit's run to consecutive addresses.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -442,7 +443,7 @@ int maxU32(Context& c, const uint32_t* in, int64_t n, uint32_t* result, cudaStre
   if (n <= 0) return 0;
   uint32_t* d = reinterpret_cast<uint32_t*>(c.scalars.as<unsigned long long>() + 14);
   cudaMemsetAsync(d, 0, 4, s);
-  { noteLaunch(); maxKernel<<<gridFor(n, 256), 256, 0, s>>>(n, in, d); }
+  { noteLaunch(); maxKernel<<<std::min(gridFor(n, 256), kReduceBlocks), 256, 0, s>>>(n, in, d); }
   cudaMemcpyAsync(result, d, 4, cudaMemcpyDeviceToHost, s);
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
 }

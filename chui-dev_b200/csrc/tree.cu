@@ -26,6 +26,7 @@
 #include <climits>
 
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -965,7 +966,7 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
   auto* sc = c.scalars.as<unsigned long long>();
   unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
   cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
-  { noteLaunch(); boundsKernel<<<gridFor(n, 256), 256, 0, s>>>(n, u[0], u[1], u[2], sc); }
+  { noteLaunch(); boundsKernel<<<std::min(gridFor(n, 256), kReduceBlocks), 256, 0, s>>>(n, u[0], u[1], u[2], sc); }
   unsigned long long hb[6];
   cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
@@ -1230,7 +1231,7 @@ int treeNodeBounds(Context& c, double lo[3], double hi[3], cudaStream_t s) {
   unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
   cudaMemcpyAsync(sc, init, sizeof(init), cudaMemcpyHostToDevice, s);
   if (c.n_nodes > 0)
-    { noteLaunch(); nodeBoundsKernel<<<gridFor(c.n_nodes, 256), 256, 0, s>>>(c.n_nodes, c.node_geom.as<double4>(),
+    { noteLaunch(); nodeBoundsKernel<<<std::min(gridFor(c.n_nodes, 256), kReduceBlocks), 256, 0, s>>>(c.n_nodes, c.node_geom.as<double4>(),
                                                               c.node_com.as<double4>(), sc); }
   unsigned long long hb[6];
   cudaMemcpyAsync(hb, sc, sizeof(hb), cudaMemcpyDeviceToHost, s);

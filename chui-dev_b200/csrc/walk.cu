@@ -875,7 +875,7 @@ constexpr int kMultList = 4; // accepted multipoles per lane before a flush (4 a
 // with at most kBulkCount sources and half-size at most kBulkHalf * r_cut is
 // evaluated as one block of sources by the lanes that opened it.
 #ifndef CHUI_BULK_COUNT
-#define CHUI_BULK_COUNT 1024
+#define CHUI_BULK_COUNT 2048  // 1024: 192.8 ms, 2048: 190.3, 4096: 190.4 at 256^3 (strict, packed pair loop)
 #endif
 #ifndef CHUI_BULK_HALF
 #define CHUI_BULK_HALF 1.0
@@ -896,6 +896,7 @@ constexpr int kMultList = 4; // accepted multipoles per lane before a flush (4 a
 #define CHUI_BULK_COUNT_ADAPTIVE 256
 #endif
 constexpr uint32_t kBulkCount = CHUI_BULK_COUNT;
+constexpr uint32_t kBulkCountVjp = 1024;  // the adjoint walk's blocks (measured there at this size)
 constexpr uint32_t kBulkCountAdaptive = CHUI_BULK_COUNT_ADAPTIVE;
 constexpr double kBulkHalf = CHUI_BULK_HALF;
 constexpr int kPairUnroll = CHUI_PAIR_UNROLL;
@@ -1843,7 +1844,7 @@ struct VjpQueue<double> {
 //
 // Traversal: a node is kept while the r_cut sphere of some lane may reach its
 // cube (each lane with its own minimum image, so groups of targets that are
-// far apart in the box still prune); leaves and nodes of at most kBulkCount
+// far apart in the box still prune); leaves and nodes of at most kBulkCountVjp
 // sources are enqueued whole, keeping sources inside the sphere of the lanes
 // that need the node; every pair decision is the per-pair cutoff test. Queue
 // entries are FP64-formed minimum-image offsets from the warp's reference
@@ -2036,7 +2037,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpA
       }
       const uint32_t need_mask = __ballot_sync(0xffffffffu, need);
       if (need_mask == 0u) continue;
-      if (rg4.z == 0 || (rg4.y <= kBulkCount && h <= bulk_half)) {
+      if (rg4.z == 0 || (rg4.y <= kBulkCountVjp && h <= bulk_half)) {
         enqueue(rg4.x, rg4.y, need_mask);
         continue;
       }

@@ -125,24 +125,35 @@ def test_mixed_precision_matches_reference(cuda_ok, name, diagnostics):
 
 @pytest.mark.parametrize("n_side,halos", [(48, 60), (64, 120)])
 def test_production_walk_matches_diagnostic_walk(cuda_ok, n_side, halos):
-    """Clustered boxes where many opened nodes qualify as subtree blocks: the
-    production walk sums the same pairs as the per-node walk (FP32 summation
-    order differs), and both agree with the FP64 walk to the mixed bar."""
+    """Clustered boxes where many opened nodes qualify as subtree blocks. The
+    production walk's pair set is the per-node walk's, except that strict
+    multipoles inside a block are summed as the pairs they stand for: against
+    the FP64 production walk (the same pair set) it differs only by FP32
+    arithmetic; against the per-node walk also by those multipoles'
+    truncation; and against the reference-exact FP64 per-node walk it meets
+    the mixed bar. The lanes compared are the tree-only residual forces, a
+    fraction of the total force, so their relative FP32 error is larger than
+    the total force's (the total's is median 2.5e-7, p99 2.9e-6 at 256^3):
+    the bars here are 1e-5 at the median and 3e-4 at the 99th percentile."""
     from chui_treepm import ics
     box = 50.0
     x, y, z, *_ = ics.clustered_box(n_side ** 3, box, 0.6, halos, 3.0, 0.5, 7)
     m = np.full(len(x), 1.0 / len(x))
     res = {}
-    for key, prec, diag in (("d1", ct._abi.MIXED, 1), ("d0", ct._abi.MIXED, 0), ("f64", ct._abi.FP64, 1)):
+    for key, prec, diag in (("d1", ct._abi.MIXED, 1), ("d0", ct._abi.MIXED, 0), ("f64", ct._abi.FP64, 1),
+                            ("f64p", ct._abi.FP64, 0)):
         cfg = ct.TreePmConfig(pm_grid_nx=n_side, pm_grid_ny=n_side, pm_grid_nz=n_side, box_x=box, box_y=box,
                               box_z=box, opening_theta=0.6, max_leaf_size=16, softening=0.002, precision=prec,
                               diagnostics=diag)
         with ct.TreePmCoordinator(cfg) as s:
             r = s.solve_active_set(x, y, z, m, short_range=True)
             res[key] = [r["tree_ax"], r["tree_ay"], r["tree_az"]]
-    e_order = rel_err(res["d0"], res["d1"])
-    assert np.median(e_order) <= 1e-5, np.median(e_order)
-    assert np.percentile(e_order, 99) <= 1e-4, np.percentile(e_order, 99)
+    e_fp32 = rel_err(res["d0"], res["f64p"])
+    assert np.median(e_fp32) <= 1e-5, np.median(e_fp32)
+    assert np.percentile(e_fp32, 99) <= 3e-4, np.percentile(e_fp32, 99)
+    e_blocks = rel_err(res["d0"], res["d1"])
+    assert np.median(e_blocks) <= 1e-5, np.median(e_blocks)
+    assert np.percentile(e_blocks, 99) <= 3e-4, np.percentile(e_blocks, 99)
     e64 = rel_err(res["d0"], res["f64"])
     assert np.median(e64) <= 1e-4, np.median(e64)
     assert np.percentile(e64, 99) <= 1e-3, np.percentile(e64, 99)
