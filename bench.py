@@ -64,8 +64,8 @@ FLOPS_PER_MULTIPOLE = 90.0
 FLOPS_PER_VISIT = 12.0
 # DRAM bytes of one production walk launch on the workload (ncu
 # dram__bytes_read.sum + dram__bytes_write.sum, one capture of
-# `bench.py --mode profile --workload clustered256`, first walkFast launch)
-WALK_DRAM_BYTES = {"clustered256": 11648765696 + 2503527936}
+# `bench.py --mode profile --workload clustered256`, second walkFast launch)
+WALK_DRAM_BYTES = {"clustered256": 11676495872 + 2522083072}
 # The differentiable case: 64^3 lattice + Zel'dovich (P ~ k^-2, 0.3 spacing
 # rms) in a box of 50, mesh 64^3, theta 0.5, 10 KDK steps of 0.05 at unit mean
 # density (G = 1), softening 0.1 spacing, loss = MSE(CIC density of the final

@@ -715,7 +715,7 @@ void chui_treepm_destroy(void* handle) {
                             &c->grp_leaf, &c->grp_start, &c->grp_rec, &c->grp_list, &c->grp_done, &c->gauss_tab,
                             &c->out_acc[0], &c->out_acc[1], &c->out_acc[2], &c->out_pm[0], &c->out_pm[1],
                             &c->out_pm[2], &c->out_tree[0], &c->out_tree[1], &c->out_tree[2], &c->out_near,
-                            &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max, &c->gap_min, &c->gap_max, &c->gap_flag, &c->gap_off, &c->cp_levels,
+                            &c->status, &c->scalars, &c->ux, &c->uy, &c->uz, &c->bucket_min, &c->bucket_max, &c->gap_min, &c->gap_max, &c->gap_flag, &c->gap_off, &c->grid_f4, &c->cp_levels,
                             &c->keys_a, &c->keys_b, &c->idx_a, &c->idx_b, &c->idx_c, &c->idx_d,
                             &c->path_words, &c->common_prefix, &c->node_count_per_pos, &c->node_offset,
                             &c->leaf_of_pos, &c->inv_pos, &c->sort_hist, &c->sort_counts,
@@ -752,6 +752,7 @@ int chui_treepm_set_config(void* handle, const chui_treepm_config* cfg) {
     cudaDeviceSynchronize();
     chui::pmDestroy(*c);
     c->pm_field_valid = false;
+    c->pm_f4_ready = false;
   }
   chui::applyConfig(*c, *cfg);
   return 0;

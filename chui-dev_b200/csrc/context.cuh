@@ -81,6 +81,8 @@ struct Context {
   cufftHandle iso_r2c = 0, iso_c2r = 0;
   DevBuf iso_pad, iso_kernel;
   DevBuf grid[3];            // grid[0] holds the density then F_x; grid[1], grid[2] F_y, F_z
+  DevBuf grid_f4;            // periodic mixed: {F_x, F_y, F_z, 0} per cell for the interpolation
+  bool pm_f4_ready = false;  // grid_f4 holds the current field
   DevBuf adj_grid[3];        // adjoint: cotangent grids B_x, B_y, B_z; adj_grid[0] then holds rho_bar
   DevBuf axis_tables;        // kx, ky, kz, wx, wy, wz (FP64)
   bool pm_field_valid = false;

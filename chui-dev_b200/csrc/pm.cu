@@ -16,6 +16,8 @@
 // spectrum; grid[1], grid[2] receive F_y, F_z. Mixed precision keeps the mesh
 // in FP32; the FP64 configuration uses double grids and Z2D/D2Z plans.
 #include <cuda_runtime.h>
+
+#include <type_traits>
 #include <cufft.h>
 
 #include <algorithm>
@@ -437,6 +439,47 @@ __device__ __forceinline__ void gatherForce(const PmGeom& g, const R* __restrict
   }
 }
 
+// The same gathers from the interleaved field of a periodic mixed-precision
+// mesh: one 16-byte record {F_x, F_y, F_z, 0} per cell, row-major without the
+// FFT padding, so each stencil cell costs one sector instead of one in each
+// of three grids. Weights, products and sums are those of gatherForce<float>.
+__device__ __forceinline__ void gatherForce4(const PmGeom& g, const float4* __restrict__ f4, double px, double py,
+                                             double pz, float& gx, float& gy, float& gz) {
+  gx = gy = gz = 0.f;
+  const int taps = g.scheme == 0 ? 2 : 3;
+  const Stencil s0 = makeStencil(wrapPosition(px, g.L[0]) * g.inv_d[0], g.scheme);
+  const Stencil s1 = makeStencil(wrapPosition(py, g.L[1]) * g.inv_d[1], g.scheme);
+  const Stencil s2 = makeStencil(wrapPosition(pz, g.L[2]) * g.inv_d[2], g.scheme);
+  for (int a = 0; a < taps; ++a) {
+    const int64_t ix = wrapIndex(s0.off0 + a, g.n[0]);
+    for (int b = 0; b < taps; ++b) {
+      const int64_t iy = wrapIndex(s1.off0 + b, g.n[1]);
+      const size_t row = (static_cast<size_t>(ix) * g.n[1] + iy) * g.n[2];
+      const float wab = static_cast<float>(s0.w[a] * s1.w[b]);
+      for (int cc = 0; cc < taps; ++cc) {
+        const int64_t iz = wrapIndex(s2.off0 + cc, g.n[2]);
+        const float w = wab * static_cast<float>(s2.w[cc]);
+        const float4 v = f4[row + iz];
+        gx += w * v.x;
+        gy += w * v.y;
+        gz += w * v.z;
+      }
+    }
+  }
+}
+
+// {F_x, F_y, F_z, 0} per cell from the three padded real grids.
+__global__ void interleaveForceKernel(PmGeom g, const float* __restrict__ fx, const float* __restrict__ fy,
+                                      const float* __restrict__ fz, float4* out) {
+  const size_t cells = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < cells;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t row = i / static_cast<size_t>(g.n[2]);
+    const size_t src = row * static_cast<size_t>(g.nzp) + (i - row * static_cast<size_t>(g.n[2]));
+    out[i] = make_float4(fx[src], fy[src], fz[src], 0.f);
+  }
+}
+
 // Interpolation and the total force of a solve in one pass over the active
 // slots: the stencil gathers, the walk's part (written at the slot), and the
 // total and optional lanes written once (TreePmForceAccumulatorView's accel,
@@ -448,7 +491,8 @@ __global__ void interpolateCombineKernel(int64_t nt, const uint32_t* __restrict_
                                          const double* __restrict__ tz, int64_t n, const double* __restrict__ sx_pos,
                                          const double* __restrict__ sy_pos, const double* __restrict__ sz_pos,
                                          PmGeom g, const R* __restrict__ fxg, const R* __restrict__ fyg,
-                                         const R* __restrict__ fzg, int with_pm, const double* __restrict__ tree,
+                                         const R* __restrict__ fzg, const float4* __restrict__ f4, int with_pm,
+                                         const double* __restrict__ tree,
                                          const double* __restrict__ near, double* ax, double* ay, double* az,
                                          double* lx, double* ly, double* lz, double* sx, double* sy, double* sz,
                                          double* snear) {
@@ -467,7 +511,12 @@ __global__ void interpolateCombineKernel(int64_t nt, const uint32_t* __restrict_
         py = sy_pos[row];
         pz = sz_pos[row];
       }
-      gatherForce<R>(g, fxg, fyg, fzg, px, py, pz, gx, gy, gz);
+      if constexpr (std::is_same<R, float>::value) {
+        if (f4) gatherForce4(g, f4, px, py, pz, gx, gy, gz);
+        else gatherForce<R>(g, fxg, fyg, fzg, px, py, pz, gx, gy, gz);
+      } else {
+        gatherForce<R>(g, fxg, fyg, fzg, px, py, pz, gx, gy, gz);
+      }
     }
     const double pmx = static_cast<double>(gx), pmy = static_cast<double>(gy), pmz = static_cast<double>(gz);
     const double trx = tree[k], try_ = tree[nt + k], trz = tree[2 * nt + k];
@@ -500,7 +549,8 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ order
                                   const double* __restrict__ tz, const double* __restrict__ sx,
                                   const double* __restrict__ sy, const double* __restrict__ sz,
                                   PmGeom g, const R* __restrict__ fxg, const R* __restrict__ fyg,
-                                  const R* __restrict__ fzg, double* ax, double* ay, double* az) {
+                                  const R* __restrict__ fzg, const float4* __restrict__ f4, double* ax, double* ay,
+                                  double* az) {
   for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < nt;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     // slot k: the j-th target, or the j-th entry of a visit-order slice
@@ -518,7 +568,12 @@ __global__ void interpolateKernel(int64_t nt, const uint32_t* __restrict__ order
       pz = sz[row];
     }
     R gx, gy, gz;
-    gatherForce<R>(g, fxg, fyg, fzg, px, py, pz, gx, gy, gz);
+    if constexpr (std::is_same<R, float>::value) {
+      if (f4) gatherForce4(g, f4, px, py, pz, gx, gy, gz);
+      else gatherForce<R>(g, fxg, fyg, fzg, px, py, pz, gx, gy, gz);
+    } else {
+      gatherForce<R>(g, fxg, fyg, fzg, px, py, pz, gx, gy, gz);
+    }
     const int64_t o = order ? j : k;
     ax[o] = static_cast<double>(gx);
     ay[o] = static_cast<double>(gy);
@@ -982,6 +1037,7 @@ int isoRefresh(Context& c, const PmGeom& g, int64_t n, const double* x, const do
 int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const double* z,
               const double* m, double uniform_mass, double total_mass, cudaStream_t s,
               const double4* tree_sources) {
+  c.pm_f4_ready = false;
   int rc = pmPrepare(c);
   if (rc) return rc;
   if (c.cfg.boundary_condition != CHUI_TREEPM_BOUNDARY_PERIODIC) {
@@ -1046,6 +1102,14 @@ int pmRefresh(Context& c, int64_t n, const double* x, const double* y, const dou
         return CHUI_TREEPM_EDEVICE;
       }
     }
+    // the interpolation's interleaved copy of the field
+    if (ensure(c.grid_f4, cells * sizeof(float4))) {
+      c.last_error = "PM interleaved field allocation failed";
+      return CHUI_TREEPM_ENOMEM;
+    }
+    { noteLaunch(); interleaveForceKernel<<<gridFor(cells, block), block, 0, s>>>(
+        g, c.grid[0].as<float>(), c.grid[1].as<float>(), c.grid[2].as<float>(), c.grid_f4.as<float4>()); }
+    c.pm_f4_ready = true;
   } else {
     fr = cufftExecD2Z(c.plan_r2c, c.grid[0].as<cufftDoubleReal>(), c.grid[0].as<cufftDoubleComplex>());
     if (fr != CUFFT_SUCCESS) {
@@ -1085,11 +1149,11 @@ int pmInterpolate(Context& c, int64_t nt, const uint32_t* active, const double* 
   if (isMixed(c)) {
     { noteLaunch(); interpolateKernel<float><<<gridFor(nt, block), block, 0, s>>>(
         nt, order, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<float>(), c.grid[1].as<float>(),
-        c.grid[2].as<float>(), ax, ay, az); }
+        c.grid[2].as<float>(), c.pm_f4_ready ? c.grid_f4.as<float4>() : nullptr, ax, ay, az); }
   } else {
     { noteLaunch(); interpolateKernel<double><<<gridFor(nt, block), block, 0, s>>>(
         nt, order, active, tx, ty, tz, sx, sy, sz, g, c.grid[0].as<double>(), c.grid[1].as<double>(),
-        c.grid[2].as<double>(), ax, ay, az); }
+        c.grid[2].as<double>(), nullptr, ax, ay, az); }
   }
   if (cudaGetLastError() != cudaSuccess) {
     c.last_error = "PM interpolation launch failed";
@@ -1109,11 +1173,11 @@ int pmInterpolateCombine(Context& c, int64_t nt, const uint32_t* active, const d
   if (isMixed(c)) {
     { noteLaunch(); interpolateCombineKernel<float><<<gridFor(nt, block), block, 0, s>>>(
         nt, active, tx, ty, tz, n, px, py, pz, g, c.grid[0].as<float>(), c.grid[1].as<float>(),
-        c.grid[2].as<float>(), with_pm ? 1 : 0, tree, near, ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
+        c.grid[2].as<float>(), c.pm_f4_ready ? c.grid_f4.as<float4>() : nullptr, with_pm ? 1 : 0, tree, near, ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
   } else {
     { noteLaunch(); interpolateCombineKernel<double><<<gridFor(nt, block), block, 0, s>>>(
         nt, active, tx, ty, tz, n, px, py, pz, g, c.grid[0].as<double>(), c.grid[1].as<double>(),
-        c.grid[2].as<double>(), with_pm ? 1 : 0, tree, near, ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
+        c.grid[2].as<double>(), nullptr, with_pm ? 1 : 0, tree, near, ax, ay, az, lx, ly, lz, sx, sy, sz, snear); }
   }
   if (cudaGetLastError() != cudaSuccess) {
     c.last_error = "PM interpolation launch failed";
