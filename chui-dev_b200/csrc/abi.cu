@@ -579,6 +579,57 @@ namespace {
 thread_local std::string g_create_error;
 }  // namespace
 
+namespace chui {
+namespace {
+
+// One array of a host-memory elementwise step: copied in (host_in), updated
+// on the device (dev), copied back (host_out, or NULL for inputs only).
+struct HostLane {
+  const double* host_in;
+  double* dev;
+  double* host_out;
+};
+
+// Host-memory kick and drift in chunks on two streams: each chunk's copies
+// in, its kernel and its copies out are ordered on one stream, so a chunk's
+// host-to-device copy overlaps the previous chunk's kernel and device-to-host
+// copy (the copy engines move both directions at once). The caller's stream
+// orders the whole step: the two streams start after its pending work and it
+// waits for both before the call returns.
+template <class Launch>
+int pipelineHostStep(Context& c, int64_t n, cudaStream_t s, const HostLane* lanes, int count, Launch launch) {
+  if (!c.pipe_ready) {
+    for (auto& st : c.pipe_stream)
+      if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+    for (auto& e : c.pipe_ev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return CHUI_TREEPM_EDEVICE;
+    c.pipe_ready = true;
+  }
+  cudaEventRecord(c.pipe_ev[2], s);
+  for (auto& st : c.pipe_stream) cudaStreamWaitEvent(st, c.pipe_ev[2], 0);
+  constexpr int64_t kChunk = int64_t(1) << 22;  // 4 Mi elements: 32 MiB per array
+  int64_t k = 0;
+  for (int64_t b = 0; b < n; b += kChunk, ++k) {
+    cudaStream_t st = c.pipe_stream[k & 1];
+    const int64_t len = n - b < kChunk ? n - b : kChunk;
+    for (int l = 0; l < count; ++l)
+      cudaMemcpyAsync(lanes[l].dev + b, lanes[l].host_in + b, static_cast<size_t>(len) * 8, cudaMemcpyHostToDevice, st);
+    launch(b, len, st);
+    for (int l = 0; l < count; ++l)
+      if (lanes[l].host_out)
+        cudaMemcpyAsync(lanes[l].host_out + b, lanes[l].dev + b, static_cast<size_t>(len) * 8, cudaMemcpyDeviceToHost,
+                        st);
+  }
+  for (int j = 0; j < 2; ++j) {
+    cudaEventRecord(c.pipe_ev[j], c.pipe_stream[j]);
+    cudaStreamWaitEvent(s, c.pipe_ev[j], 0);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : CHUI_TREEPM_EDEVICE;
+}
+
+}  // namespace
+}  // namespace chui
+
 // ---- Lambda-CDM step factors (host) ----
 namespace lcdm {
 
@@ -728,6 +779,10 @@ void chui_treepm_destroy(void* handle) {
     for (auto* b : bufs) chui::release(*b);
     if (c->events_ready)
       for (auto& e : c->ev) cudaEventDestroy(e);
+    if (c->pipe_ready) {
+      for (auto& st : c->pipe_stream) cudaStreamDestroy(st);
+      for (auto& e : c->pipe_ev) cudaEventDestroy(e);
+    }
   }
   delete c;
 }
@@ -1590,25 +1645,19 @@ int chui_treepm_kick(void* handle, int64_t n, double* vx, double* vy, double* vz
     if (chui::ensure(c.in_x, n * 8) || chui::ensure(c.in_y, n * 8) || chui::ensure(c.in_z, n * 8) ||
         chui::ensure(c.out_acc[0], n * 8) || chui::ensure(c.out_acc[1], n * 8) || chui::ensure(c.out_acc[2], n * 8))
       return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
-    dvx = c.in_x.as<double>();
-    dvy = c.in_y.as<double>();
-    dvz = c.in_z.as<double>();
-    cudaMemcpyAsync(dvx, vx, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dvy, vy, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dvz, vz, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(c.out_acc[0].ptr, ax, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(c.out_acc[1].ptr, ay, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(c.out_acc[2].ptr, az, n * 8, cudaMemcpyHostToDevice, s);
-    dax = c.out_acc[0].as<double>();
-    day = c.out_acc[1].as<double>();
-    daz = c.out_acc[2].as<double>();
+    double* v[3] = {c.in_x.as<double>(), c.in_y.as<double>(), c.in_z.as<double>()};
+    double* a[3] = {c.out_acc[0].as<double>(), c.out_acc[1].as<double>(), c.out_acc[2].as<double>()};
+    const chui::HostLane lanes[6] = {{vx, v[0], vx}, {vy, v[1], vy}, {vz, v[2], vz},
+                                     {ax, a[0], nullptr}, {ay, a[1], nullptr}, {az, a[2], nullptr}};
+    const int rc = chui::pipelineHostStep(c, n, s, lanes, 6, [&](int64_t b, int64_t len, cudaStream_t st) {
+      chui::noteLaunch();
+      chui::kickKernel<<<chui::gridFor(len, 256), 256, 0, st>>>(len, v[0] + b, v[1] + b, v[2] + b, a[0] + b, a[1] + b,
+                                                                a[2] + b, kick_factor, drag_factor);
+    });
+    if (rc) return chui::fail(c, rc, "kick failed");
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "kick failed");
   }
   { chui::noteLaunch(); chui::kickKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dvx, dvy, dvz, dax, day, daz, kick_factor, drag_factor); }
-  if (memory == CHUI_TREEPM_HOST) {
-    cudaMemcpyAsync(vx, dvx, n * 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(vy, dvy, n * 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(vz, dvz, n * 8, cudaMemcpyDeviceToHost, s);
-  }
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "kick failed");
 }
 
@@ -1628,25 +1677,21 @@ int chui_treepm_drift(void* handle, int64_t n, double* x, double* y, double* z, 
     if (chui::ensure(c.in_x, n * 8) || chui::ensure(c.in_y, n * 8) || chui::ensure(c.in_z, n * 8) ||
         chui::ensure(c.out_acc[0], n * 8) || chui::ensure(c.out_acc[1], n * 8) || chui::ensure(c.out_acc[2], n * 8))
       return chui::fail(c, CHUI_TREEPM_ENOMEM, "allocation failed");
-    dx = c.in_x.as<double>();
-    dy = c.in_y.as<double>();
-    dz = c.in_z.as<double>();
-    cudaMemcpyAsync(dx, x, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dy, y, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dz, z, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(c.out_acc[0].ptr, vx, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(c.out_acc[1].ptr, vy, n * 8, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(c.out_acc[2].ptr, vz, n * 8, cudaMemcpyHostToDevice, s);
-    dvx = c.out_acc[0].as<double>();
-    dvy = c.out_acc[1].as<double>();
-    dvz = c.out_acc[2].as<double>();
-  }
-  { chui::noteLaunch(); chui::driftKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dx, dy, dz, dvx, dvy, dvz, drift_factor, per_box[0],
-                                                         per_box[1], per_box[2]); }
-  if (memory == CHUI_TREEPM_HOST) {
-    cudaMemcpyAsync(x, dx, n * 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(y, dy, n * 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(z, dz, n * 8, cudaMemcpyDeviceToHost, s);
+    double* p[3] = {c.in_x.as<double>(), c.in_y.as<double>(), c.in_z.as<double>()};
+    double* v[3] = {c.out_acc[0].as<double>(), c.out_acc[1].as<double>(), c.out_acc[2].as<double>()};
+    const chui::HostLane lanes[6] = {{x, p[0], x}, {y, p[1], y}, {z, p[2], z},
+                                     {vx, v[0], nullptr}, {vy, v[1], nullptr}, {vz, v[2], nullptr}};
+    const int rc = chui::pipelineHostStep(c, n, s, lanes, 6, [&](int64_t b, int64_t len, cudaStream_t st) {
+      chui::noteLaunch();
+      chui::driftKernel<<<chui::gridFor(len, 256), 256, 0, st>>>(len, p[0] + b, p[1] + b, p[2] + b, v[0] + b, v[1] + b,
+                                                                 v[2] + b, drift_factor, per_box[0], per_box[1],
+                                                                 per_box[2]);
+    });
+    if (rc) return chui::fail(c, rc, "drift failed");
+  } else {
+    chui::noteLaunch();
+    chui::driftKernel<<<chui::gridFor(n, 256), 256, 0, s>>>(n, dx, dy, dz, dvx, dvy, dvz, drift_factor, per_box[0],
+                                                           per_box[1], per_box[2]);
   }
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : chui::fail(c, CHUI_TREEPM_EDEVICE, "drift failed");
 }

@@ -162,6 +162,10 @@ struct Context {
 
   cudaEvent_t ev[8] = {};
   bool events_ready = false;
+  // host-memory kick and drift: two copy/compute streams and their events
+  cudaStream_t pipe_stream[2] = {};
+  cudaEvent_t pipe_ev[3] = {};
+  bool pipe_ready = false;
   chui_treepm_stats last_stats{};
 };
 

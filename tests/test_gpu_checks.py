@@ -1,6 +1,7 @@
 """FP64 global momentum / energy checks on the device
-(chui_treepm_momentum_energy) against numpy sums, and momentum conservation
-of the full TreePM force (net force ~ 0)."""
+(chui_treepm_momentum_energy) against numpy sums, momentum conservation of
+the full TreePM force (net force ~ 0), and the host-memory kick and drift
+against the device path."""
 import numpy as np
 import pytest
 
@@ -54,3 +55,35 @@ def test_total_force_conserves_momentum(cuda_ok, precision):
     # pair forces cancel pairwise up to rounding and the few strict multipoles
     assert np.abs(tree["net_force"]).max() <= 1e-5 * tree_scale
     assert np.abs(tot["net_force"]).max() <= 1e-3 * scale
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_kick_and_drift_match_device(cuda_ok, pinned):
+    """Host-memory kick and drift run in chunks of 4 Mi elements on two
+    streams; over several chunks and a ragged tail (pinned or pageable host
+    arrays) they give the device path's results bit for bit, and the caller's
+    stream sees the finished arrays."""
+    n = (1 << 23) + 12345  # two whole chunks and a tail
+    rng = np.random.default_rng(3)
+    box = 10.0
+    cfg = ct.TreePmConfig(pm_grid_nx=16, pm_grid_ny=16, pm_grid_nz=16, box_x=box, box_y=box, box_z=box)
+
+    def host(a):
+        if not pinned:
+            return np.ascontiguousarray(a)
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    p = [host(rng.random(n) * box) for _ in range(3)]
+    v = [host(rng.standard_normal(n)) for _ in range(3)]
+    a = [host(rng.standard_normal(n)) for _ in range(3)]
+    dp = [torch.tensor(q, device="cuda") for q in p]
+    dv = [torch.tensor(q, device="cuda") for q in v]
+    da = [torch.tensor(q, device="cuda") for q in a]
+    with ct.TreePmCoordinator(cfg) as s:
+        s.kick(*v, *a, 0.3, 0.97)
+        s.drift(*p, *v, 0.7)
+        s.kick(*dv, *da, 0.3, 0.97)
+        s.drift(*dp, *dv, 0.7)
+        torch.cuda.synchronize()
+    for h_arr, d_arr in zip(v + p, dv + dp):
+        assert np.array_equal(h_arr, d_arr.cpu().numpy())
