@@ -1823,6 +1823,11 @@ struct VjpArgs {
   PolyH dpoly;
   WalkParams wp;
   float inv_16rs5_f;
+  // the FP32 instance's packed pair loop: each coefficient in both halves, the
+  // polynomial variables' scales and the kernel constants as pairs
+  float2 pk2[kPolyMaxTerms];
+  float2 dk2[kPolyMaxTerms];
+  float2 sc2, dsc2, mone2, eps2_2, m8_2, m16_2, mthree2;
 };
 
 template <class Real>
@@ -1853,9 +1858,13 @@ struct VjpQueue<double> {
 template <class Real, bool kEpsZero, int kTerms>
 __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpArgs a) {
   using V4 = typename VjpQueue<Real>::V4;
+  // FP32: sources in pairs for packed arithmetic, pair p = {x0, x1, y0, y1},
+  // {z0, z1, m0, m1}, {cx0, cx1, cy0, cy1}, {cz0, cz1, -, -} (cotangents c)
+  constexpr bool kPacked = sizeof(Real) == 4;
   __shared__ uint32_t stack_sm[kWalkWarpsPerBlock][kStackCap];
-  __shared__ V4 q_pos[kWalkWarpsPerBlock][kQueue];
-  __shared__ V4 q_cot[kWalkWarpsPerBlock][kQueue];
+  __shared__ V4 q_pos[kWalkWarpsPerBlock][kPacked ? 1 : kQueue];
+  __shared__ V4 q_cot[kWalkWarpsPerBlock][kPacked ? 1 : kQueue];
+  __shared__ float4 q_pair[4][kWalkWarpsPerBlock][kPacked ? kQueue / 2 : 1];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   uint32_t* stack = stack_sm[warp];
@@ -1908,12 +1917,88 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpA
     __syncwarp();
     bool overflow = false;
 
+    // entry k of the queue (either layout)
+    auto entryAt = [&](int k, V4& e, V4& cj) {
+      if constexpr (kPacked) {
+        const int h = k & 1;
+        const float* qa = reinterpret_cast<const float*>(&q_pair[0][warp][k >> 1]);
+        const float* qb = reinterpret_cast<const float*>(&q_pair[1][warp][k >> 1]);
+        const float* qc = reinterpret_cast<const float*>(&q_pair[2][warp][k >> 1]);
+        const float* qd = reinterpret_cast<const float*>(&q_pair[3][warp][k >> 1]);
+        e = make_float4(qa[h], qa[2 + h], qb[h], qb[2 + h]);
+        cj = make_float4(qc[h], qc[2 + h], qd[h], 0.f);
+      } else {
+        e = q_pos[warp][k];
+        cj = q_cot[warp][k];
+      }
+    };
+
     auto flush = [&]() {
       Real gx = 0, gy = 0, gz = 0;
+      if constexpr (kPacked) {
+        if (!pair_image) {
+          // two sources per step in packed FP32; an odd queue's last pair has
+          // a second half of zero mass and zero cotangent (it adds exactly 0)
+          if (qn & 1) {
+            if (lane == 0) {
+              for (int t = 0; t < 4; ++t) {
+                float* q = reinterpret_cast<float*>(&q_pair[t][warp][qn >> 1]);
+                q[1] = 0.f;
+                q[3] = 0.f;
+              }
+            }
+            __syncwarp();
+          }
+          const float2 ntx = make_float2(-tx, -tx), nty = make_float2(-ty, -ty), ntz = make_float2(-tz, -tz);
+          const float2 mk2 = make_float2(mkr, mkr);
+          const float2 nck0 = make_float2(-ckxr, -ckxr), nck1 = make_float2(-ckyr, -ckyr),
+                       nck2 = make_float2(-ckzr, -ckzr);
+          float2 g0 = make_float2(0.f, 0.f), g1 = g0, g2 = g0;
+          const int np = (qn + 1) >> 1;
+#pragma unroll 2
+          for (int p = 0; p < np; ++p) {
+            const float4 A = q_pair[0][warp][p];
+            const float4 B = q_pair[1][warp][p];
+            const float4 C = q_pair[2][warp][p];
+            const float4 D = q_pair[3][warp][p];
+            const float2 dx = __fadd2_rn(make_float2(A.x, A.y), ntx);
+            const float2 dy = __fadd2_rn(make_float2(A.z, A.w), nty);
+            const float2 dz = __fadd2_rn(make_float2(B.x, B.y), ntz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            const bool in0 = valid && r2.x <= cut2 && r2.x > 0.f;
+            const bool in1 = valid && r2.y <= cut2 && r2.y > 0.f;
+            const float2 hh = hornerR2x2<(kTerms == 12 ? kPairPolyTerms : kTerms)>(a.pk2, r2, a.sc2, a.mone2);
+            const float2 hp = hornerR2x2<kTerms>(a.dk2, r2, a.dsc2, a.mone2);
+            const float2 s2 = kEpsZero ? r2 : __fadd2_rn(r2, a.eps2_2);
+            const float2 rinv = make_float2(rsqrtf(s2.x), rsqrtf(s2.y));
+            const float2 rinv2 = __fmul2_rn(rinv, rinv);
+            const float2 rinv3 = __fmul2_rn(rinv2, rinv);
+            const float2 K = __ffma2_rn(hh, a.m8_2, rinv3);  // r^-3 - H/(8 r_s^3)
+            const float2 Kp = __ffma2_rn(hp, a.m16_2, __fmul2_rn(__fmul2_rn(rinv3, rinv2), a.mthree2));
+            const float2 mj = make_float2(B.z, B.w);
+            const float2 c0 = __ffma2_rn(mk2, make_float2(C.x, C.y), __fmul2_rn(mj, nck0));
+            const float2 c1 = __ffma2_rn(mk2, make_float2(C.z, C.w), __fmul2_rn(mj, nck1));
+            const float2 c2 = __ffma2_rn(mk2, make_float2(D.x, D.y), __fmul2_rn(mj, nck2));
+            const float2 dc = __fmul2_rn(__ffma2_rn(dx, c0, __ffma2_rn(dy, c1, __fmul2_rn(dz, c2))), Kp);
+            // select, not multiply: K and K' are infinite for the excluded self pair
+            const float2 Ks = make_float2(in0 ? K.x : 0.f, in1 ? K.y : 0.f);
+            const float2 dcs = make_float2(in0 ? dc.x : 0.f, in1 ? dc.y : 0.f);
+            g0 = __ffma2_rn(Ks, c0, __ffma2_rn(dcs, dx, g0));
+            g1 = __ffma2_rn(Ks, c1, __ffma2_rn(dcs, dy, g1));
+            g2 = __ffma2_rn(Ks, c2, __ffma2_rn(dcs, dz, g2));
+          }
+          acc_x += static_cast<double>(g0.x + g0.y);
+          acc_y += static_cast<double>(g1.x + g1.y);
+          acc_z += static_cast<double>(g2.x + g2.y);
+          qn = 0;
+          __syncwarp();
+          return;
+        }
+      }
 #pragma unroll 2
       for (int k = 0; k < qn; ++k) {
-        const V4 e = q_pos[warp][k];
-        const V4 cj = q_cot[warp][k];
+        V4 e, cj;
+        entryAt(k, e, cj);
         Real dx = static_cast<Real>(e.x) - tx, dy = static_cast<Real>(e.y) - ty, dz = static_cast<Real>(e.z) - tz;
         if (pair_image) {
           dx -= box_r[0] * rint(dx * inv_box_r[0]);
@@ -2007,8 +2092,23 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpA
           cj.y = static_cast<Real>(cv.y);
           cj.z = static_cast<Real>(cv.z);
           cj.w = Real(0);
-          q_pos[warp][slot_q] = e;
-          q_cot[warp][slot_q] = cj;
+          if constexpr (kPacked) {
+            const int hq = slot_q & 1;
+            float* qa = reinterpret_cast<float*>(&q_pair[0][warp][slot_q >> 1]);
+            float* qb = reinterpret_cast<float*>(&q_pair[1][warp][slot_q >> 1]);
+            float* qc = reinterpret_cast<float*>(&q_pair[2][warp][slot_q >> 1]);
+            float* qd = reinterpret_cast<float*>(&q_pair[3][warp][slot_q >> 1]);
+            qa[hq] = e.x;
+            qa[2 + hq] = e.y;
+            qb[hq] = e.z;
+            qb[2 + hq] = e.w;
+            qc[hq] = cj.x;
+            qc[2 + hq] = cj.y;
+            qd[hq] = cj.z;
+          } else {
+            q_pos[warp][slot_q] = e;
+            q_cot[warp][slot_q] = cj;
+          }
         }
         __syncwarp();
         qn += c;
@@ -2398,6 +2498,18 @@ int walkVjpRun(Context& c, int64_t n, const double* sx, const double* sy, const 
   a.wp = wp;
   const double rs2 = c.rs * c.rs;
   a.inv_16rs5_f = static_cast<float>(1.0 / (16.0 * rs2 * rs2 * c.rs));
+  for (int k = 0; k < kPolyMaxTerms; ++k) {
+    a.pk2[k] = make_float2(c.poly.c[k], c.poly.c[k]);
+    a.dk2[k] = make_float2(c.dpoly.c[k], c.dpoly.c[k]);
+  }
+  const float sc = wp.inv_4rs2_f * c.poly.scale, dsc = wp.inv_4rs2_f * c.dpoly.scale;
+  a.sc2 = make_float2(sc, sc);
+  a.dsc2 = make_float2(dsc, dsc);
+  a.mone2 = make_float2(-1.f, -1.f);
+  a.eps2_2 = make_float2(wp.eps2_f, wp.eps2_f);
+  a.m8_2 = make_float2(-wp.inv_8rs3_f, -wp.inv_8rs3_f);
+  a.m16_2 = make_float2(-a.inv_16rs5_f, -a.inv_16rs5_f);
+  a.mthree2 = make_float2(-3.f, -3.f);
   const bool eps_zero = wp.eps == 0.0;
   if (c.cfg.precision == CHUI_TREEPM_MIXED) {
     if (c.poly.terms <= kPairPolyTerms && c.dpoly.terms <= 12)
