@@ -896,7 +896,10 @@ constexpr int kMultList = 4; // accepted multipoles per lane before a flush (4 a
 #define CHUI_BULK_COUNT_ADAPTIVE 256
 #endif
 constexpr uint32_t kBulkCount = CHUI_BULK_COUNT;
-constexpr uint32_t kBulkCountVjp = 1024;  // the adjoint walk's blocks (measured there at this size)
+#ifndef CHUI_BULK_COUNT_VJP
+#define CHUI_BULK_COUNT_VJP 1024  // the adjoint walk's blocks
+#endif
+constexpr uint32_t kBulkCountVjp = CHUI_BULK_COUNT_VJP;
 constexpr uint32_t kBulkCountAdaptive = CHUI_BULK_COUNT_ADAPTIVE;
 constexpr double kBulkHalf = CHUI_BULK_HALF;
 constexpr int kPairUnroll = CHUI_PAIR_UNROLL;
