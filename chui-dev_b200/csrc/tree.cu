@@ -458,15 +458,37 @@ struct NodeOut {
 };
 
 // Emit the chain of nodes started at each sorted position, in preorder.
+// The sorted positions that start a chain of nodes (counts[i] > 0), listed in
+// order: starts[pos_off[i]] = i. The emission then runs one thread per chain
+// instead of one per position (most positions start none).
+__global__ void chainFlagsKernel(int64_t n, const uint32_t* __restrict__ counts, uint32_t* flag) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i <= n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    flag[i] = i < n && counts[i] > 0u ? 1u : 0u;
+}
+
+__global__ void chainListKernel(int64_t n, const uint32_t* __restrict__ counts, const uint32_t* __restrict__ pos_off,
+                                uint32_t* starts) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    if (counts[i] > 0u) starts[pos_off[i]] = static_cast<uint32_t>(i);
+}
+
 __global__ void nodeEmitKernel(NodePlan p, int words, const unsigned long long* __restrict__ path,
                                const int* __restrict__ cp, const uint32_t* __restrict__ counts,
-                               const uint32_t* __restrict__ offset, CpLevels lv, double cx0, double cy0,
+                               const uint32_t* __restrict__ offset, const uint32_t* __restrict__ starts,
+                               const uint32_t* __restrict__ chains, CpLevels lv, double cx0, double cy0,
                                double cz0, double half0, uint32_t total_nodes, NodeOut out, uint32_t* status) {
   const int64_t n = p.n;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const uint32_t cnt = counts[i];
-    if (cnt == 0) continue;
+  const int64_t m = *chains;  // chain starts
+  for (int64_t j = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; j < m;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = starts[j];
+    const uint32_t cnt = i < n ? counts[i] : 0u;
+    if (cnt == 0) {
+      atomicOr(status, kStatusIndexRange);
+      return;
+    }
     const int ci = cp[i];
     const int d0 = ci + 1;
     const int l = d0 + static_cast<int>(cnt) - 1;
@@ -1134,8 +1156,18 @@ int treeBuild(Context& c, int64_t n, const double* x, const double* y, const dou
       dst += lv.len[l];
     }
   }
-  { noteLaunch(); nodeEmitKernel<<<gridFor(n, 128), 128, 0, s>>>(plan, words, path, cp, counts, offset, lv, cx0, cy0, cz0,
-                                                 half0, total_nodes, out, status); }
+  // the chain starts, listed (at most one per node)
+  if (ensure(c.idx_a, (n + 1) * 4) || ensure(c.idx_b, (n + 1) * 4) || ensure(c.inv_pos, n * 4))
+    return CHUI_TREEPM_ENOMEM;
+  uint32_t* chain_flag = c.idx_b.as<uint32_t>();
+  uint32_t* chain_off = c.idx_a.as<uint32_t>();
+  uint32_t* chain_start = c.inv_pos.as<uint32_t>();
+  { noteLaunch(); chainFlagsKernel<<<gridFor(n + 1, 256), 256, 0, s>>>(n, counts, chain_flag); }
+  if ((rc = exclusiveScanU32(c, chain_flag, chain_off, n + 1, s))) return rc;
+  { noteLaunch(); chainListKernel<<<gridFor(n, 256), 256, 0, s>>>(n, counts, chain_off, chain_start); }
+  { noteLaunch(); nodeEmitKernel<<<gridFor(total_nodes, 128), 128, 0, s>>>(plan, words, path, cp, counts, offset,
+                                                 chain_start, chain_off + n, lv, cx0, cy0, cz0, half0, total_nodes,
+                                                 out, status); }
   {
     uint32_t est = 0;
     cudaMemcpyAsync(&est, status, 4, cudaMemcpyDeviceToHost, s);
