@@ -255,7 +255,7 @@ int sourceBounds(Context& c, int64_t n, const double* x, const double* y, const 
 
 const char* statusText(uint32_t bits);
 
-// Count of this library's own kernel launches (cuFFT/CUB internals excluded),
+// Count of this library's own kernel launches (cuFFT internals excluded),
 // reported per solve in chui_treepm_stats::kernel_launches.
 void noteLaunch();
 uint64_t launchCount();

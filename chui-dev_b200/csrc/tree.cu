@@ -10,15 +10,20 @@
 // stably partitions each node's particles by (x >= cx, y >= cy, z >= cz)
 // against FP64 centres obtained by repeated centre +- half/2, stopping at
 // count <= leaf or half <= 1e-12. The same tree is produced here in parallel:
-//  1. unwrap each axis (largest circular gap, found with a 2N-bucket max-gap
-//     pass instead of a sort: the largest gap always exceeds a bucket width);
-//  2. Morton keys + stable radix sort (the reference's within-leaf order);
+//  1. unwrap each axis (largest circular gap of the canonical coordinates):
+//     per-bucket {min, max} over about n/4 buckets find it when no bucket's
+//     own extent can hide it, else the axis is sorted;
+//  2. Morton keys per particle (they order particles within a leaf);
 //  3. per particle, the geometric octant path (3 bits/level, 21 levels per
-//     64-bit word) by the same FP64 centre recurrence; stable sort by path;
+//     64-bit word) by the same FP64 centre recurrence; stable sort by path,
+//     resolving first only the levels the previous tree needed;
 //  4. nodes = maximal runs of equal path prefix whose parent run has more
-//     than `leaf` particles; they are enumerated in preorder directly from the
-//     common-prefix lengths of neighbouring sorted paths;
-//  5. stable sort of Morton order by leaf id gives the final particle order;
+//     than `leaf` particles; they are enumerated in preorder from the
+//     common-prefix lengths of neighbouring sorted paths (node ends and
+//     parents by nearest-smaller queries on block minima of those lengths);
+//  5. within each leaf, particles ranked by (Morton key, row): the
+//     reference's order (a leaf above 1024 particles takes a stable sort of
+//     the Morton order by leaf instead);
 //  6. FP64 multipoles bottom-up, each parent reduced once, children in octant
 //     order, by the last child to finish.
 #include <cuda_runtime.h>
@@ -568,7 +573,6 @@ __global__ void invertKernel(int64_t n, const uint32_t* __restrict__ perm, uint3
   }
 }
 
-// key for the final stable sort: leaf id of each particle, listed in Morton order
 // Within-leaf order. The reference partitions the Morton-sorted particles
 // into octants, so a leaf's particles keep their Morton order (key, then row:
 // the radix sort is stable over rows; tree_gravity.cpp:1081-1206,

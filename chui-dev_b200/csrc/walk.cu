@@ -2012,7 +2012,7 @@ __global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, 4) walkVjpKernel(VjpA
         const bool in = valid && r2 <= cut2 && r2 > Real(0);
         Real K, Kp;
         if constexpr (sizeof(Real) == 4) {
-          // H in its pair-kernel length when it fits (the short fit has 10 terms)
+          // H in its pair-kernel length when it fits (the short fit has 9 terms)
           const float hh = hornerR2<(kTerms == 12 ? kPairPolyTerms : kTerms)>(a.poly, r2, w.inv_4rs2_f * a.poly.scale);
           const float hp = hornerR2<kTerms>(a.dpoly, r2, w.inv_4rs2_f * a.dpoly.scale);
           const float s2 = kEpsZero ? r2 : r2 + w.eps2_f;
