@@ -889,6 +889,9 @@ constexpr int kMultList = 4; // accepted multipoles per lane before a flush (4 a
 #ifndef CHUI_WALK_MIN_BLOCKS
 #define CHUI_WALK_MIN_BLOCKS 5  // resident blocks per SM the register budget is sized for
 #endif
+#ifndef CHUI_WALK_MIN_BLOCKS_ADAPTIVE
+#define CHUI_WALK_MIN_BLOCKS_ADAPTIVE 6  // the adaptive, uniform-mass production instances (fast deck: 149.8 -> 147.2 ms at 256^3)
+#endif
 // Under the adaptive policy most opened nodes have deeper accepted
 // multipoles, so blocks pay only for small nodes; evaluating their sources as
 // pairs is at least as accurate as the multipoles it replaces.
@@ -1102,8 +1105,10 @@ __device__ __forceinline__ int certainLess(float a, float b, float err = 0.f) {
 // guard); masses travel with the sources.
 template <bool kEpsZero, int kTerms, bool kDiag, bool kContiguous, int kMode, bool kUniform = false,
           bool kCost = false, bool kF64 = false, bool kSoft = false>
-__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32, (kMode == 0 && kUniform) ? CHUI_WALK_MIN_BLOCKS_STRICT
-                                                                                  : CHUI_WALK_MIN_BLOCKS)
+__global__ void __launch_bounds__(kWalkWarpsPerBlock * 32,
+                                  (kMode == 0 && kUniform)   ? CHUI_WALK_MIN_BLOCKS_STRICT
+                                  : (kMode == 2 && kUniform) ? CHUI_WALK_MIN_BLOCKS_ADAPTIVE
+                                                             : CHUI_WALK_MIN_BLOCKS)
     walkFastKernel(WalkArgs a) {
   static_assert(!kF64 || (kMode <= 1 && !kDiag && !kUniform), "FP64 production walk: strict policy only");
   static_assert(!kSoft || (!kUniform && !kEpsZero && !kF64 && kMode <= 2), "per-particle softening instances");
